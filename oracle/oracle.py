@@ -1,0 +1,133 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the CPU-baseline
+leg of bench.py, always as the checker or the timed CPU reference, never as the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+
+
+class OrcMat(C.Structure):
+    _fields_ = [("n", C.c_int), ("nnz", C.c_int), ("istart", C.c_int),
+                ("rowptr", C.c_void_p), ("col", C.c_void_p), ("val", C.c_void_p)]
+
+
+class OrcParams(C.Structure):
+    _fields_ = [("solver", C.c_int), ("ipreflag", C.c_int), ("ILU_method", C.c_int),
+                ("precon_thblock", C.c_int), ("itrmax", C.c_int), ("rtolmax", C.c_double),
+                ("GMRES_m", C.c_int), ("GMRES_GSflag", C.c_int),
+                ("CAGMRES_sstep", C.c_int), ("CAGMRES_tstep", C.c_int),
+                ("CAGMRES_basis", C.c_int), ("CAGMRES_QRflag", C.c_int)]
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(_LIB) or (
+            os.path.getmtime(_LIB) < os.path.getmtime(os.path.join(_HERE, "parcel_oracle.cpp"))):
+        subprocess.run(["make", "-C", _HERE, "-s", "-B" if force else "liboracle.so"], check=True)
+    return _LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = C.CDLL(_LIB)
+        L.orc_solve.argtypes = [C.POINTER(OrcMat), C.POINTER(OrcParams), C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.orc_solve.restype = C.c_int
+        L.orc_spmv.argtypes = [C.POINTER(OrcMat), C.c_void_p, C.c_void_p]
+        L.orc_dot.argtypes = [C.c_long, C.c_void_p, C.c_void_p]
+        L.orc_dot.restype = C.c_double
+        L.orc_precon_apply.argtypes = [C.POINTER(OrcMat), C.POINTER(OrcParams), C.c_void_p, C.c_void_p]
+        L.orc_precon_apply.restype = C.c_int
+        L.orc_precon_dinv.argtypes = [C.POINTER(OrcMat), C.POINTER(OrcParams), C.c_void_p]
+        L.orc_precon_dinv.restype = C.c_int
+        L.orc_true_relres.argtypes = [C.POINTER(OrcMat), C.c_void_p, C.c_void_p]
+        L.orc_true_relres.restype = C.c_double
+        L.orc_num_threads.restype = C.c_int
+        L.orc_set_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Matrix:
+    """Keeps the numpy arrays alive while the C struct points at them."""
+
+    def __init__(self, A):
+        self.rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
+        self.col = np.ascontiguousarray(A.col, dtype=np.int32)
+        self.val = np.ascontiguousarray(A.val, dtype=np.float64)
+        self.n = int(A.n)
+        self.s = OrcMat(self.n, int(self.col.shape[0]), int(getattr(A, "istart", 1)),
+                        _ptr(self.rowptr), _ptr(self.col), _ptr(self.val))
+
+
+def params(solver=1, ipreflag=0, ILU_method=1, precon_thblock=-1, itrmax=1000, rtolmax=1e-8,
+           GMRES_m=30, GMRES_GSflag=1, sstep=4, tstep=1, basis=0, qrflag=3) -> OrcParams:
+    return OrcParams(solver, ipreflag, ILU_method, precon_thblock, itrmax, rtolmax,
+                     GMRES_m, GMRES_GSflag, sstep, tstep, basis, qrflag)
+
+
+def solve(A, b, x0=None, **kw):
+    """Runs the oracle solve; returns (x, reshistory[:niter], niter, iret)."""
+    M = A if isinstance(A, Matrix) else Matrix(A)
+    p = params(**kw)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros(M.n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+    hist = np.zeros(max(p.itrmax, 1) + 1)
+    niter, iret = C.c_int(0), C.c_int(0)
+    rc = lib().orc_solve(C.byref(M.s), C.byref(p), _ptr(b), _ptr(x), _ptr(hist),
+                         C.byref(niter), C.byref(iret))
+    if rc != 0:
+        return x, hist[:0], 0, rc
+    return x, hist[:niter.value].copy(), niter.value, iret.value
+
+
+def spmv(A, x):
+    M = A if isinstance(A, Matrix) else Matrix(A)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty(M.n)
+    lib().orc_spmv(C.byref(M.s), _ptr(x), _ptr(y))
+    return y
+
+
+def precon_apply(A, r, **kw):
+    M = A if isinstance(A, Matrix) else Matrix(A)
+    p = params(**kw)
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    s = np.zeros(M.n)
+    rc = lib().orc_precon_apply(C.byref(M.s), C.byref(p), _ptr(r), _ptr(s))
+    if rc != 0:
+        raise RuntimeError(f"oracle preconditioner setup failed: {rc}")
+    return s
+
+
+def true_relres(A, b, x) -> float:
+    M = A if isinstance(A, Matrix) else Matrix(A)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    return lib().orc_true_relres(C.byref(M.s), _ptr(b), _ptr(x))
+
+
+def set_threads(t: int) -> None:
+    lib().orc_set_threads(int(t))
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
