@@ -1,0 +1,261 @@
+/* parcel_b.h -- C ABI of libparcelb, a B200 (sm_100a) implementation of PARCEL-legacy's
+ * single-process preconditioned Krylov solve on CRS matrices.
+ *
+ * Every entry point is `extern "C"` with plain pointers and sizes.  Two families:
+ *
+ *  1. Drop-in shims with the reference's C-callable signatures (every argument by
+ *     reference, CRS 1-based with global column ids, int32 indices, real*8 values):
+ *       parcel_init_c_, parcel_free_c_, parcel_dcg_c_, parcel_dbicgstab_c_,
+ *       parcel_dgmres_c_, parcel_dcagmres_c_          (host arrays: the CPU-build ABI)
+ *       parcel_d*_gpu_c_                              (device pointers: the GPU-build ABI)
+ *  2. The native API: parcel_b_solve (PARCEL_KSP_CRS with the KSP_INPUT_PARAM struct),
+ *     the split setup/solve handle API, and kernel-level entries used by tests.
+ *
+ * Pointer arguments of parcel_b_solve and the split API may be host or device memory;
+ * the library detects which (cudaPointerGetAttributes) and copies host data in and out.
+ *
+ * Return convention: `iret` 0 = converged, 1 = iteration limit reached, as in the
+ * reference (src/define.f90:101-102).  Where the reference stops the process
+ * (zero pivot, matrix.f90:8018-8021; allocation failure, cu_common.h:119-124), this
+ * library returns a negative PARCEL_B_E_* code in iret instead.
+ */
+#ifndef PARCEL_B_H
+#define PARCEL_B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------------- */
+#define PARCEL_B_OK 0
+#define PARCEL_B_MAXITER 1
+#define PARCEL_B_E_ZERO_PIVOT (-1)   /* reference: `stop` in ILU / D-ILU setup        */
+#define PARCEL_B_E_ARG (-2)          /* invalid argument                               */
+#define PARCEL_B_E_CUDA (-3)         /* CUDA runtime error                             */
+#define PARCEL_B_E_BREAKDOWN (-4)    /* NaN / Inf in the iteration                     */
+#define PARCEL_B_E_UNSUPPORTED (-5)  /* option this single-GPU build does not provide  */
+#define PARCEL_B_E_NOMEM (-6)        /* device allocation failed                       */
+#define PARCEL_B_E_NOT_INIT (-7)
+
+/* ---- constants of src/define.f90:14-102 ------------------------------------------ */
+#define PARCEL_B_SOLVER_CG 1
+#define PARCEL_B_SOLVER_BICG 2
+#define PARCEL_B_SOLVER_GMRES 3
+#define PARCEL_B_SOLVER_CAGMRES 4
+#define PARCEL_B_PRECON_NONE 0
+#define PARCEL_B_PRECON_POINTJACOBI 1
+#define PARCEL_B_PRECON_BLOCKJACOBI 2
+#define PARCEL_B_PRECON_ADDITIVESCHWARZ 3
+#define PARCEL_B_ILU0 0
+#define PARCEL_B_ILUD 1
+#define PARCEL_B_MLUD 2
+#define PARCEL_B_GS_MGS 1
+#define PARCEL_B_GS_CGS 2
+#define PARCEL_B_BASIS_MONOMIAL 0
+#define PARCEL_B_BASIS_NEWTON 1
+#define PARCEL_B_QR_MGS 1
+#define PARCEL_B_QR_CGS 2
+#define PARCEL_B_QR_TSQR 3
+#define PARCEL_B_QR_CHOLQR 4
+#define PARCEL_B_QR_CHOLQR2 5
+
+/* Inner arithmetic of the Krylov iteration (extension; the reference is FP64 only). */
+#define PARCEL_B_INNER_FP64 0
+#define PARCEL_B_INNER_FP32_REFINE 1 /* FP32 Krylov + FP32 preconditioner inside an
+                                        FP64 / double-double iterative refinement loop */
+
+/* KSP_INPUT_PARAM (src/type.f90:907-946), field for field and in the same order, followed
+ * by this library's extensions.  A value of -1 selects the reference default
+ * (PARCEL_KSP_Default_Setting, type.f90:949-1132; INIT_PARCEL_INPUT, wrapper.f90:5-45). */
+typedef struct parcel_b_input {
+  int ipreflag;
+  int ILU_method;
+  int addL;
+  int iflagAS;
+  int solver;
+  int iovlflag;
+  int GMRES_m;
+  int GMRES_GSflag;
+  int CAGMRES_sstep;
+  int CAGMRES_tstep;
+  int CAGMRES_basis;
+  int CAGMRES_QRflag;
+  int CBCG_kstep;
+  int CBCG_Eigenflag;
+  int power_method_itrmax;
+  int CAARNOLDI_sstep;
+  int CAARNOLDI_tstep;
+  int CAARNOLDI_basis;
+  int CAARNOLDI_QRflag;
+  int machineflag;
+  int dataflag;
+  int calcflag;
+  int Neuman_itr;
+  int Neuman_local;
+  int itrmax;
+  double rtolmax;
+  double abstolmax;
+  int independ_nvec;
+  int precon_thblock;
+  int nBlock;
+  int PRECISION_A;
+  int PRECISION_b;
+  int PRECISION_x;
+  int PRECISION_PRECONDITION;
+  /* ---- extensions ---- */
+  int inner_precision;    /* PARCEL_B_INNER_*                                     */
+  int residual_dd;        /* 1: outer residual b - A x in double-double            */
+  double inner_rtol;      /* relative tolerance of each inner solve (FP32 path)     */
+  int max_refine;         /* outer refinement steps (FP32 path)                     */
+  int reserved[7];
+} parcel_b_input;
+
+/* Fills every field with -1 / defaults (INIT_PARCEL_INPUT, wrapper.f90:5-45). */
+void parcel_b_input_init(parcel_b_input* p);
+
+/* CRS matrix of one process, reference layout: rowptr has n+1 entries with
+ * rowptr[0] = 1, col holds 1-based global column ids sorted within each row, istart is
+ * the 1-based global id of the first row (1 on one process). */
+typedef struct parcel_b_crs {
+  int32_t n;
+  int32_t gn;
+  int64_t nnz;
+  int32_t istart;
+  const int32_t* rowptr;
+  const int32_t* col;
+  const double* val;
+} parcel_b_crs;
+
+/* Per-solve statistics (extension). */
+typedef struct parcel_b_stats {
+  double setup_s;           /* preconditioner + layout setup, wall seconds           */
+  double solve_s;           /* Krylov iteration, wall seconds                        */
+  double total_s;
+  double true_relres;       /* ||b - A x|| / ||b|| in FP64 at exit                   */
+  double true_relres_dd;    /* same, residual computed in double-double (if asked)   */
+  int niter;
+  int iret;
+  int refine_steps;         /* FP32 path: outer refinement steps                     */
+  int kernel_launches;      /* kernels this library launched for the solve           */
+  int ilu_levels_max;       /* longest wavefront (levels) of any block-Jacobi block  */
+  int ilu_nblocks;
+  int reserved[6];
+} parcel_b_stats;
+
+/* ---- lifecycle: PARCEL_Init / PARCEL_Free (src/c_krylov_wrapper.f90:6-23,
+ *      src/example/c2fortran_kernel.f90:1-10) -------------------------------------- */
+void parcel_init_c_(int* myrank);
+void parcel_free_c_(void);
+/* Selects the CUDA stream the library launches on (NULL: a private non-blocking stream). */
+int parcel_b_set_stream(void* cuda_stream);
+void* parcel_b_get_stream(void);
+/* Last error message and code of this thread's most recent failing call. */
+int parcel_b_last_error(char* buf, int buflen);
+/* Statistics of the most recent solve. */
+int parcel_b_last_stats(parcel_b_stats* out);
+
+/* ---- generic entry: PARCEL_KSP_CRS (src/wrapper.f90:47-222) ------------------------
+ * x holds x0 on entry and the solution on exit; reshistory has itrmax entries;
+ * niter returns the iterations used; iret as described above. */
+int parcel_b_solve(const parcel_b_input* prm, const parcel_b_crs* A, const double* b,
+                   double* x, double* reshistory, int* niter, int* iret);
+
+/* ---- drop-in shims, CPU-build ABI (host arrays; src/example/c2fortran_kernel.f90) ----
+ * parcel_dcg_c       : c2fortran_kernel.f90:334-432  -> parcel_dcg (wrapper.f90:1995)
+ * parcel_dbicgstab_c : c2fortran_kernel.f90:434-521  -> parcel_dbicgstab (wrapper.f90:1813)
+ * parcel_dgmres_c    : c2fortran_kernel.f90:523-618  -> parcel_dgmres (wrapper.f90:2179)
+ * parcel_dcagmres_c  : c2fortran_kernel.f90:901-1004 -> parcel_dcagmres (wrapper.f90:2807)
+ * niter: in = itrmax, out = iterations used (wrapper.f90:630). */
+void parcel_dcg_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int32_t* gn,
+                   int32_t* nnz, int32_t* istart, double* crsa, int32_t* crsrow_ptr,
+                   int32_t* crscol, int* ipreflag, int* ilu_method, int* addl, int* iflagas,
+                   int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                   int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock,
+                   int* iret);
+void parcel_dbicgstab_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int32_t* gn,
+                         int32_t* nnz, int32_t* istart, double* crsa, int32_t* crsrow_ptr,
+                         int32_t* crscol, int* ipreflag, int* ilu_method, int* addl,
+                         int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                         int* iovlflag, int* precon_thblock, int* neuman_itr,
+                         int* independ_nvec, int* nblock, int* iret);
+void parcel_dgmres_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int32_t* gn,
+                      int32_t* nnz, int32_t* istart, double* crsa, int32_t* crsrow_ptr,
+                      int32_t* crscol, int* ipreflag, int* ilu_method, int* addl,
+                      int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                      int* iovlflag, int* precon_thblock, int* neuman_itr,
+                      int* independ_nvec, int* nblock, int* restart, int* gmres_gsflag,
+                      int* iret);
+void parcel_dcagmres_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int32_t* gn,
+                        int32_t* nnz, int32_t* istart, double* crsa, int32_t* crsrow_ptr,
+                        int32_t* crscol, int* ipreflag, int* ilu_method, int* addl,
+                        int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                        int* iovlflag, int* precon_thblock, int* neuman_itr,
+                        int* independ_nvec, int* nblock, int* cagmres_sstep,
+                        int* cagmres_tstep, int* cagmres_basis, int* cagmres_qrflag,
+                        int* iret);
+
+/* ---- drop-in shims, GPU-build ABI: vecx, vecb, crsa, crsrow_ptr and crscol are passed
+ * as `devicemem*` (src/CUDA/src/cu_common.h:37-42), whose first member is the device
+ * pointer; a `void**` pointing at the device pointer is the same thing. ------------- */
+void parcel_dcg_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn,
+                       int32_t* nnz, int32_t* istart, void** crsa, void** crsrow_ptr,
+                       void** crscol, int* ipreflag, int* ilu_method, int* addl,
+                       int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                       int* iovlflag, int* precon_thblock, int* neuman_itr,
+                       int* independ_nvec, int* nblock, int* iret);
+void parcel_dbicgstab_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn,
+                             int32_t* nnz, int32_t* istart, void** crsa, void** crsrow_ptr,
+                             void** crscol, int* ipreflag, int* ilu_method, int* addl,
+                             int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                             int* iovlflag, int* precon_thblock, int* neuman_itr,
+                             int* independ_nvec, int* nblock, int* iret);
+void parcel_dgmres_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn,
+                          int32_t* nnz, int32_t* istart, void** crsa, void** crsrow_ptr,
+                          void** crscol, int* ipreflag, int* ilu_method, int* addl,
+                          int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                          int* iovlflag, int* precon_thblock, int* neuman_itr,
+                          int* independ_nvec, int* nblock, int* restart, int* gmres_gsflag,
+                          int* iret);
+void parcel_dcagmres_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn,
+                            int32_t* nnz, int32_t* istart, void** crsa, void** crsrow_ptr,
+                            void** crscol, int* ipreflag, int* ilu_method, int* addl,
+                            int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                            int* iovlflag, int* precon_thblock, int* neuman_itr,
+                            int* independ_nvec, int* nblock, int* cagmres_sstep,
+                            int* cagmres_tstep, int* cagmres_basis, int* cagmres_qrflag,
+                            int* iret);
+
+/* ---- split setup / solve (set_ksp_crs_c, start_ksp_solver_crs_c, get_vecx_ksp_crs_c,
+ *      get_reshistory_ksp_crs_c: src/example/c2fortran_kernel.f90:2855-2961) ----------
+ * A handle keeps the matrix layout and preconditioner on the device between solves. */
+typedef struct parcel_b_handle_s* parcel_b_handle;
+int parcel_b_setup(const parcel_b_input* prm, const parcel_b_crs* A, parcel_b_handle* out);
+int parcel_b_start(parcel_b_handle h, const double* b, double* x, double* reshistory,
+                   int* niter, int* iret);
+int parcel_b_release(parcel_b_handle h);
+
+/* ---- kernel-level entries (tests and benchmarks) ---------------------------------- */
+/* y = A x with the library's CRS SpMV (MatVec_crs, matrix.f90:1348-1512); device arrays. */
+int parcel_b_spmv(const parcel_b_crs* A, const double* x, double* y);
+/* y = A x in FP32 values and vectors (the mixed-precision inner SpMV); device arrays. */
+int parcel_b_spmv_f32(int32_t n, int64_t nnz, int32_t istart, const int32_t* rowptr,
+                      const int32_t* col, const float* val, const float* x, float* y);
+/* s = M^-1 r for the preconditioner described by prm (setup + one application);
+ * host or device arrays. */
+int parcel_b_precon_apply(const parcel_b_input* prm, const parcel_b_crs* A, const double* r,
+                          double* s);
+/* Deterministic dot product of two device vectors. */
+int parcel_b_dot(int64_t n, const double* x, const double* y, double* out_host);
+/* r = b - A x in double-double with the reference's dd add / mul order
+ * (dd_func.f90:5-98); A values, b and x given as (hi, lo) pairs, lo may be NULL. Device
+ * arrays; returns r as (r_hi, r_lo). */
+int parcel_b_residual_dd(const parcel_b_crs* A, const double* x_hi, const double* x_lo,
+                         const double* b_hi, const double* b_lo, double* r_hi, double* r_lo);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PARCEL_B_H */

@@ -1,0 +1,716 @@
+// pb_ilu.cu -- block-Jacobi ILU(0) and D-ILU on B200.
+//
+// Reference algorithms (restated, not translated):
+//   * blocks: contiguous row ranges from divide_region (src/common.f90:125-182);
+//   * ILU(0): IKJ factorisation of each block's in-block submatrix, L unit-diagonal,
+//     U with its diagonal (src/matrix.f90:7970-8072, 8249-8392); sweeps
+//     solve_LU_crs (matrix.f90:8548-8747);
+//   * D-ILU: K = (D+L) D^-1 (D+U) with D matched to the diagonal (ILUD) or the row sum
+//     (MLUD) (DILU_DInv_crs, matrix.f90:3482-3648); sweeps solve_ILU_crs
+//     (matrix.f90:4987-5163).
+// The reference runs each block's sweeps sequentially on one OpenMP thread (CPU) or one
+// cuSPARSE csrsv2 solve per process (src/CUDA/src/cusparse.cu:712-787).
+//
+// B200 design.  Rows of every block are grouped into wavefront levels (row i depends on
+// the in-block rows it couples to with a smaller index), and the library stores every
+// Krylov vector in a permuted, level-major layout where each level is contiguous and
+// starts on a 16-byte boundary.  One CTA sweeps one block.  A producer warp streams each
+// level's packed coefficients and its input-vector slice into a ring of shared-memory
+// stages with bulk asynchronous copies (cp.async.bulk + mbarrier); the consumer warps
+// solve the level's rows from shared memory, keeping the last W levels of the solution in
+// a shared-memory ring, so a level step costs shared-memory latency and one named
+// barrier.  The arithmetic of every row is the reference's: same operands, same order.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "pb_device.cuh"
+#include "pb_ilu.cuh"
+
+namespace pb {
+
+namespace {
+
+inline int align4(int x) { return (x + 3) & ~3; }
+inline int64_t align16(int64_t x) { return (x + 15) & ~int64_t(15); }
+
+void divide_region(int r, int np, long idown, long iup, long* lo, long* hi) {
+  if (iup == idown) { *lo = idown; *hi = iup; return; }
+  long region = iup - idown + 1, blk = region / np, over = region % np;
+  if (r < over) { *lo = idown + blk * r + r; *hi = *lo + blk; }
+  else { *lo = idown + blk * r + over; *hi = *lo + blk - 1; }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host plan
+void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P) {
+  const int n = A.n;
+  P.n = n;
+  P.nb = nb;
+  P.lev.assign(n, 0);
+  P.pos.assign(n, 0);
+  P.blk_lo.resize(nb);
+  P.blk_hi.resize(nb);
+  for (int b = 0; b < nb; ++b) {
+    long lo, hi;
+    divide_region(b, nb, 1, n, &lo, &hi);
+    P.blk_lo[b] = (int)(lo - 1);
+    P.blk_hi[b] = (int)hi;
+  }
+  std::vector<int> nlev(nb, 0), gap(nb, 0), missing_diag(nb, 0);
+  std::vector<int> cL(n, 0), cU(n, 0);
+  const int* rp = A.rowptr;
+  const int* ci = A.col;
+  const int cb = A.istart;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int b = 0; b < nb; ++b) {
+    const int lo = P.blk_lo[b], hi = P.blk_hi[b];
+    std::vector<int> lb(hi - lo, 0);
+    int maxlev = 0, g = 0;
+    for (int i = lo; i < hi; ++i) {
+      int L = lb[i - lo];
+      int nl = 0, nu = 0;
+      bool diag = false;
+      for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
+        int c = ci[j] - cb;
+        if (c < lo || c >= hi) continue;
+        if (c < i) { L = std::max(L, P.lev[c] + 1); ++nl; }
+        else if (c > i) ++nu;
+        else diag = true;
+      }
+      if (!diag) missing_diag[b] = 1;
+      P.lev[i] = L;
+      cL[i] = nl; cU[i] = nu;
+      maxlev = std::max(maxlev, L);
+      // an upper entry (i, c) makes c wait for i in the backward sweep order as well
+      for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
+        int c = ci[j] - cb;
+        if (c > i && c < hi) lb[c - lo] = std::max(lb[c - lo], L + 1);
+      }
+    }
+    for (int i = lo; i < hi; ++i)
+      for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
+        int c = ci[j] - cb;
+        if (c < lo || c >= hi || c == i) continue;
+        g = std::max(g, std::abs(P.lev[i] - P.lev[c]));
+      }
+    nlev[b] = maxlev + 1;
+    gap[b] = g;
+  }
+  for (int b = 0; b < nb; ++b)
+    if (missing_diag[b]) {
+      set_last_error(PARCEL_B_E_ZERO_PIVOT,
+                     "block-Jacobi block %d has a row without an in-block diagonal entry", b);
+      throw Error{PARCEL_B_E_ZERO_PIVOT, "missing diagonal"};
+    }
+  // level widths and starts; permuted layout, block by block, level by level
+  P.blk_lvl.assign(nb + 1, 0);
+  for (int b = 0; b < nb; ++b) P.blk_lvl[b + 1] = P.blk_lvl[b] + nlev[b];
+  const int totlev = P.blk_lvl[nb];
+  std::vector<int> width(totlev, 0);
+  for (int b = 0; b < nb; ++b)
+    for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) width[P.blk_lvl[b] + P.lev[i]]++;
+  P.lvl_start.assign(totlev, 0);
+  int cursor = 0, maxw = 0;
+  for (int b = 0; b < nb; ++b)
+    for (int l = 0; l < nlev[b]; ++l) {
+      int gl = P.blk_lvl[b] + l;
+      cursor = align4(cursor);
+      P.lvl_start[gl] = cursor;
+      cursor += width[gl];
+      maxw = std::max(maxw, width[gl]);
+    }
+  P.np = align4(cursor);
+  P.maxWp = align4(maxw);
+  P.max_levels = *std::max_element(nlev.begin(), nlev.end());
+  P.W = *std::max_element(gap.begin(), gap.end()) + 1;
+  // positions, stable by natural index within a level
+  std::vector<int> fill(totlev, 0);
+  P.rowAt.assign(P.np, -1);
+  for (int b = 0; b < nb; ++b)
+    for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) {
+      int gl = P.blk_lvl[b] + P.lev[i];
+      int q = P.lvl_start[gl] + fill[gl]++;
+      P.pos[i] = q;
+      P.rowAt[q] = i;
+    }
+  // chunks
+  P.chunks.clear();
+  P.blk_chunk.assign(nb + 1, 0);
+  int64_t offF = 0, offB = 0;
+  for (int b = 0; b < nb; ++b) {
+    P.blk_chunk[b] = (int)P.chunks.size();
+    for (int l = 0; l < nlev[b]; ++l) {
+      int gl = P.blk_lvl[b] + l;
+      for (int o = 0; o < width[gl]; o += kIluChunk) {
+        IluChunk c;
+        c.start = P.lvl_start[gl] + o;
+        c.w = std::min(kIluChunk, width[gl] - o);
+        c.wpad = align4(c.w);
+        c.KL = 0; c.KU = 0;
+        for (int p = 0; p < c.w; ++p) {
+          int i = P.rowAt[c.start + p];
+          c.KL = std::max(c.KL, cL[i]);
+          c.KU = std::max(c.KU, cU[i]);
+        }
+        c.lvl = l;
+        c.off_in_level = o;
+        c.blk = b;
+        c.offF = offF;
+        c.offB = offB;
+        P.chunks.push_back(c);
+      }
+    }
+  }
+  P.blk_chunk[nb] = (int)P.chunks.size();
+  // permuted row pointer (0-based)
+  P.rowptrP.assign(P.np + 1, 0);
+  for (int q = 0; q < P.np; ++q) {
+    int i = P.rowAt[q];
+    P.rowptrP[q + 1] = P.rowptrP[q] + (i >= 0 ? rp[i + 1] - rp[i] : 0);
+  }
+}
+
+// ------------------------------------------------------------------ permuted matrix
+template <class VT>
+__global__ void k_permute_matrix(int np, const int* __restrict__ rowAt, const int* __restrict__ pos,
+                                 const int* __restrict__ rp, const int* __restrict__ ci,
+                                 const double* __restrict__ va, int rbase, int cbase,
+                                 const int* __restrict__ rpP, int* __restrict__ ciP,
+                                 VT* __restrict__ vaP) {
+  const int lanes = 8;
+  int g = (blockIdx.x * blockDim.x + threadIdx.x) / lanes;
+  int l = threadIdx.x % lanes;
+  int ng = gridDim.x * blockDim.x / lanes;
+  for (int q = g; q < np; q += ng) {
+    int i = rowAt[q];
+    if (i < 0) continue;
+    int a = rp[i] - rbase, z = rp[i + 1] - rbase;
+    int o = rpP[q];
+    for (int j = a + l; j < z; j += lanes) {
+      ciP[o + (j - a)] = pos[ci[j] - cbase];
+      vaP[o + (j - a)] = (VT)va[j];
+    }
+  }
+}
+
+template <class VT>
+void ilu_permute_matrix(const IluPlan& P, const DevMat<double>& A, const int* d_pos,
+                        const int* d_rowAt, PermMat<VT>& out, int64_t nnz) {
+  out.rowptr.alloc(sizeof(int) * (P.np + 1));
+  h2d(out.rowptr.p, P.rowptrP.data(), sizeof(int) * (P.np + 1));
+  out.col.alloc(sizeof(int) * std::max<int64_t>(nnz, 1));
+  out.val.alloc(sizeof(VT) * std::max<int64_t>(nnz, 1));
+  int blocks = 8 * num_sms();
+  k_permute_matrix<VT><<<blocks, 256, 0, stream()>>>(P.np, d_rowAt, d_pos, A.rowptr, A.col, A.val,
+                                                     A.rbase, A.cbase, dp<int>(out.rowptr),
+                                                     dp<int>(out.col), dp<VT>(out.val));
+  PB_CUDA(cudaGetLastError());
+}
+
+template void ilu_permute_matrix<double>(const IluPlan&, const DevMat<double>&, const int*,
+                                         const int*, PermMat<double>&, int64_t);
+template void ilu_permute_matrix<float>(const IluPlan&, const DevMat<double>&, const int*,
+                                        const int*, PermMat<float>&, int64_t);
+
+// ------------------------------------------------------------------ factorisation
+// In-block column range of natural row i (columns sorted): [first, last) positions.
+__device__ __forceinline__ void inblock_range(const int* rp, const int* ci, int rbase, int cbase,
+                                              int i, int lo, int hi, int* ja, int* jz, int* jd) {
+  int a = rp[i] - rbase, z = rp[i + 1] - rbase;
+  int s = z, e = z, d = -1;
+  for (int j = a; j < z; ++j) {
+    int c = ci[j] - cbase;
+    if (c >= lo && s == z) s = j;
+    if (c >= hi) { e = j; break; }
+    if (c == i) d = j;
+  }
+  if (s > e) s = e;
+  *ja = s; *jz = e; *jd = d;
+}
+
+// ILU(0) IKJ factorisation of every block, level by level; one CTA per block.
+// ILU_LU_crs (matrix.f90:7970-8072).  Explicit roundings keep the reference's
+// two-rounding a - b*c.
+__global__ void k_ilu0_factor(const IluChunk* __restrict__ ch, const int* __restrict__ blk_chunk,
+                              const int* __restrict__ blk_lo, const int* __restrict__ blk_hi,
+                              const int* __restrict__ rowAt, const int* __restrict__ rp,
+                              const int* __restrict__ ci, int rbase, int cbase, double* lu) {
+  const int b = blockIdx.x;
+  const int lo = blk_lo[b], hi = blk_hi[b];
+  for (int c = blk_chunk[b]; c < blk_chunk[b + 1]; ++c) {
+    const IluChunk C = ch[c];
+    for (int p = threadIdx.x; p < C.w; p += blockDim.x) {
+      int i = rowAt[C.start + p];
+      int ia, iz, idg;
+      inblock_range(rp, ci, rbase, cbase, i, lo, hi, &ia, &iz, &idg);
+      for (int kc = ia; kc < iz; ++kc) {
+        int k = ci[kc] - cbase;
+        if (k > i - 1) break;
+        int ka, kz, kk;
+        inblock_range(rp, ci, rbase, cbase, k, lo, hi, &ka, &kz, &kk);
+        double lik = __ddiv_rn(lu[kc], lu[kk]);
+        lu[kc] = lik;
+        for (int jc = kc + 1; jc < iz; ++jc) {
+          int j = ci[jc] - cbase;
+          for (int kj = kk; kj < kz; ++kj) {
+            int cj = ci[kj] - cbase;
+            if (cj == j) { lu[jc] = __dsub_rn(lu[jc], __dmul_rn(lik, lu[kj])); break; }
+            if (cj > j) break;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// D-ILU diagonal, level by level; DILU_DInv_crs (matrix.f90:3482-3648).
+__global__ void k_dilu_diag(const IluChunk* __restrict__ ch, const int* __restrict__ blk_chunk,
+                            const int* __restrict__ blk_lo, const int* __restrict__ blk_hi,
+                            const int* __restrict__ rowAt, const int* __restrict__ rp,
+                            const int* __restrict__ ci, const double* __restrict__ va, int rbase,
+                            int cbase, int mlud, double* D, double* Dinv) {
+  const int b = blockIdx.x;
+  const int lo = blk_lo[b], hi = blk_hi[b];
+  for (int c = blk_chunk[b]; c < blk_chunk[b + 1]; ++c) {
+    const IluChunk C = ch[c];
+    for (int p = threadIdx.x; p < C.w; p += blockDim.x) {
+      int k = rowAt[C.start + p];
+      int ia, iz, idg;
+      inblock_range(rp, ci, rbase, cbase, k, lo, hi, &ia, &iz, &idg);
+      double d = va[idg];
+      for (int jr = ia; jr < idg; ++jr) {
+        int kr = ci[jr] - cbase;
+        int ra, rz, rd;
+        inblock_range(rp, ci, rbase, cbase, kr, lo, hi, &ra, &rz, &rd);
+        double dk = D[kr];
+        for (int i = ra; i < rz; ++i) {
+          int rc = ci[i] - cbase;
+          if (!mlud) {
+            if (rc == k) { d = __dsub_rn(d, __ddiv_rn(__dmul_rn(va[jr], va[i]), dk)); break; }
+          } else if (kr < rc) {
+            d = __dsub_rn(d, __ddiv_rn(__dmul_rn(va[jr], va[i]), dk));
+          }
+        }
+      }
+      D[k] = d;
+      Dinv[k] = __ddiv_rn(1.0, d);
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ packing
+// Packed chunk layout (bytes, every section 16-byte aligned):
+//   header int[8] = {start, w, wpad, K, lvl, off_in_level, 0, 0}
+//   diag   T[wpad]          forward: 1 (ILU(0)) or D^-1 (D-ILU); backward: U_kk or D^-1
+//   val    T[K * wpad]      entry k of row p at k*wpad + p
+//   slot   int[K * wpad]    ring slot (or permuted position) of the coupled row, -1 = none
+template <class T>
+__host__ __device__ inline int64_t chunk_bytes(int wpad, int K) {
+  return kIluHeader + (int64_t)wpad * sizeof(T) * (1 + K) + (int64_t)4 * K * wpad;
+}
+
+template <class T>
+__global__ void k_ilu_pack(const IluChunk* __restrict__ ch, int nchunks,
+                           const int* __restrict__ blk_lo, const int* __restrict__ blk_hi,
+                           const int* __restrict__ blk_lvl, const int* __restrict__ lvl_start,
+                           const int* __restrict__ rowAt, const int* __restrict__ pos,
+                           const int* __restrict__ lev, const int* __restrict__ rp,
+                           const int* __restrict__ ci, int rbase, int cbase,
+                           const double* __restrict__ vL,    // values of L entries
+                           const double* __restrict__ vU,    // values of U entries
+                           const double* __restrict__ Dinv,  // D-ILU only
+                           int dilu, int ring, int W, int maxWp,
+                           unsigned char* packF, unsigned char* packB) {
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const IluChunk C = ch[c];
+    const int lo = blk_lo[C.blk], hi = blk_hi[C.blk];
+    unsigned char* f = packF + C.offF;
+    unsigned char* g = packB + C.offB;
+    if (threadIdx.x == 0) {
+      int* hf = (int*)f;
+      int* hb = (int*)g;
+      hf[0] = C.start; hf[1] = C.w; hf[2] = C.wpad; hf[3] = C.KL; hf[4] = C.lvl;
+      hf[5] = C.off_in_level; hf[6] = 0; hf[7] = 0;
+      hb[0] = C.start; hb[1] = C.w; hb[2] = C.wpad; hb[3] = C.KU; hb[4] = C.lvl;
+      hb[5] = C.off_in_level; hb[6] = 0; hb[7] = 0;
+    }
+    T* dF = (T*)(f + kIluHeader);
+    T* valF = dF + C.wpad;
+    int* slF = (int*)(valF + (size_t)C.KL * C.wpad);
+    T* dB = (T*)(g + kIluHeader);
+    T* valB = dB + C.wpad;
+    int* slB = (int*)(valB + (size_t)C.KU * C.wpad);
+    for (int p = threadIdx.x; p < C.wpad; p += blockDim.x) {
+      if (p >= C.w) {
+        dF[p] = (T)0; dB[p] = (T)0;
+        for (int k = 0; k < C.KL; ++k) { valF[k * C.wpad + p] = (T)0; slF[k * C.wpad + p] = -1; }
+        for (int k = 0; k < C.KU; ++k) { valB[k * C.wpad + p] = (T)0; slB[k * C.wpad + p] = -1; }
+        continue;
+      }
+      int i = rowAt[C.start + p];
+      int ia, iz, idg;
+      inblock_range(rp, ci, rbase, cbase, i, lo, hi, &ia, &iz, &idg);
+      auto slot_of = [&](int cnat) -> int {
+        int q = pos[cnat];
+        if (!ring) return q;
+        int l = lev[cnat];
+        return (l % W) * maxWp + (q - lvl_start[blk_lvl[C.blk] + l]);
+      };
+      // forward: strictly lower in-block entries, increasing column
+      int k = 0;
+      for (int j = ia; j < idg; ++j, ++k) {
+        valF[k * C.wpad + p] = (T)vL[j];
+        slF[k * C.wpad + p] = slot_of(ci[j] - cbase);
+      }
+      for (; k < C.KL; ++k) { valF[k * C.wpad + p] = (T)0; slF[k * C.wpad + p] = -1; }
+      dF[p] = dilu ? (T)Dinv[i] : (T)1;
+      // backward: strictly upper in-block entries; ILU(0) increasing column
+      // (solve_LU_crs), D-ILU decreasing column (solve_ILU_crs runs Ustart down to Uend)
+      k = 0;
+      if (!dilu) {
+        for (int j = idg + 1; j < iz; ++j, ++k) {
+          valB[k * C.wpad + p] = (T)vU[j];
+          slB[k * C.wpad + p] = slot_of(ci[j] - cbase);
+        }
+        dB[p] = (T)vU[idg];
+      } else {
+        for (int j = iz - 1; j > idg; --j, ++k) {
+          valB[k * C.wpad + p] = (T)vU[j];
+          slB[k * C.wpad + p] = slot_of(ci[j] - cbase);
+        }
+        dB[p] = (T)Dinv[i];
+      }
+      for (; k < C.KU; ++k) { valB[k * C.wpad + p] = (T)0; slB[k * C.wpad + p] = -1; }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ the sweep kernel
+constexpr int kIluProducerWarps = 1;
+constexpr int kIluConsumerThreads = 256;
+constexpr int kIluThreads = 32 * kIluProducerWarps + kIluConsumerThreads;
+constexpr unsigned kWaitLimit = 1u << 20;   // polls of one mbarrier wait before giving up
+
+// What the producer needs per chunk, in the order it streams them:
+// {packed offset / 16, first permuted row, packed bytes, vector-slice bytes}.
+struct ProdDesc { int off16, start, cbytes, vbytes; };
+
+template <class T>
+struct IluSolveArgs {
+  const ProdDesc* tabF;   // per chunk, forward order
+  const ProdDesc* tabB;   // per chunk, forward order (read backwards)
+  const int* blk_chunk;
+  const unsigned char* packF;
+  const unsigned char* packB;
+  const T* r;
+  T* y;
+  T* s;
+  T* accum;
+  int W, maxWp, stage_bytes, nstages, ring_elems;
+  const int* gate;
+  int* err;
+};
+
+template <class T, bool DILU, bool RING>
+__global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve(IluSolveArgs<T> a) {
+  if (gated(a.gate)) return;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int NST = a.nstages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + NST;
+  volatile int* sflags = reinterpret_cast<volatile int*>(empty + NST);   // [0] abort, [1] consumed
+  T* ring = reinterpret_cast<T*>(smem + ((16 * NST + 16 + 127) & ~127));
+  unsigned char* stages =
+      reinterpret_cast<unsigned char*>(ring) + (((size_t)a.ring_elems * sizeof(T) + 127) & ~size_t(127));
+
+  const int b = blockIdx.x;
+  const int c0 = a.blk_chunk[b], c1 = a.blk_chunk[b + 1];
+  const int nc = c1 - c0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool producer = warp < kIluProducerWarps;
+  const int ctid = threadIdx.x - 32 * kIluProducerWarps;
+  int issued = 0;   // producer lane 0: copies issued so far (over both phases)
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NST; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
+    sflags[0] = 0;
+    sflags[1] = 0;
+    mbar_fence_init();
+  }
+  if (RING) {
+    for (int i = threadIdx.x; i < a.ring_elems; i += blockDim.x) ring[i] = T(0);
+  }
+  __syncthreads();
+
+  for (int phase = 0; phase < 2; ++phase) {
+    const bool fwd = phase == 0;
+    const unsigned char* pack = fwd ? a.packF : a.packB;
+    const T* vin = fwd ? a.r : a.y;
+    T* vout = fwd ? a.y : a.s;
+    const int gbase = phase * nc;
+    if (producer) {
+      // The whole warp walks the chunk list: 32 descriptors per coalesced load, prefetched
+      // one batch ahead and broadcast with shuffles; lane 0 issues the bulk copies.
+      const ProdDesc* tab = fwd ? a.tabF : a.tabB;
+      auto fetch = [&](int i) -> ProdDesc {
+        if (i >= nc) return ProdDesc{0, 0, 0, 0};
+        return tab[fwd ? c0 + i : c1 - 1 - i];
+      };
+      ProdDesc cur = fetch(lane);
+      for (int i0 = 0; i0 < nc; i0 += 32) {
+        ProdDesc nxt = fetch(i0 + 32 + lane);
+        const int kmax = min(32, nc - i0);
+        bool stop = false;
+        for (int k = 0; k < kmax; ++k) {
+          ProdDesc d;
+          d.off16 = __shfl_sync(kFull, cur.off16, k);
+          d.start = __shfl_sync(kFull, cur.start, k);
+          d.cbytes = __shfl_sync(kFull, cur.cbytes, k);
+          d.vbytes = __shfl_sync(kFull, cur.vbytes, k);
+          if (lane == 0) {
+            const int g = gbase + i0 + k;
+            const int st = g % NST;
+            const int use = g / NST;
+            if (sflags[0]) {
+              stop = true;
+            } else if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1, kWaitLimit)) {
+              atomicExch(a.err, 2);
+              sflags[0] = 1;
+              stop = true;
+            } else {
+              unsigned char* dst = stages + (size_t)st * a.stage_bytes;
+              mbar_arrive_expect_tx(&full[st], (unsigned)(d.cbytes + d.vbytes));
+              bulk_g2s(dst, pack + (size_t)d.off16 * 16, (unsigned)d.cbytes, &full[st]);
+              bulk_g2s(dst + d.cbytes, vin + d.start, (unsigned)d.vbytes, &full[st]);
+              ++issued;
+            }
+          }
+          stop = __shfl_sync(kFull, stop, 0);
+          if (stop) break;
+        }
+        if (stop) break;
+        cur = nxt;
+      }
+    } else {
+      for (int i = 0; i < nc; ++i) {
+        const int g = gbase + i;
+        const int st = g % NST;
+        const bool ok = mbar_wait(&full[st], (g / NST) & 1, kWaitLimit);
+        if (!ok) {
+          atomicExch(a.err, 3);
+          sflags[0] = 1;
+        } else {
+          const unsigned char* sp = stages + (size_t)st * a.stage_bytes;
+          const int* hdr = reinterpret_cast<const int*>(sp);
+          const int start = hdr[0], w = hdr[1], wpad = hdr[2], K = hdr[3], lvl = hdr[4], off = hdr[5];
+          const T* dg = reinterpret_cast<const T*>(sp + kIluHeader);
+          const T* val = dg + wpad;
+          const int* slot = reinterpret_cast<const int*>(val + (size_t)K * wpad);
+          const T* xin = reinterpret_cast<const T*>(sp + chunk_bytes<T>(wpad, K));
+          const T* dep = RING ? ring : vout;
+          T* rslot = ring + (size_t)(lvl % a.W) * a.maxWp + off;
+          for (int p = ctid; p < w; p += kIluConsumerThreads) {
+            T out;
+            if (fwd) {
+              T acc = xin[p];
+              for (int k = 0; k < K; ++k) {
+                int sl = slot[k * wpad + p];
+                if (sl >= 0) acc = acc - val[k * wpad + p] * dep[sl];
+              }
+              out = DILU ? dg[p] * acc : acc;
+            } else if (DILU) {
+              T zz = T(0);
+              for (int k = 0; k < K; ++k) {
+                int sl = slot[k * wpad + p];
+                if (sl >= 0) zz = zz + dep[sl] * val[k * wpad + p];
+              }
+              out = xin[p] - dg[p] * zz;
+            } else {
+              T acc = xin[p];
+              for (int k = 0; k < K; ++k) {
+                int sl = slot[k * wpad + p];
+                if (sl >= 0) acc = acc - dep[sl] * val[k * wpad + p];
+              }
+              out = acc / dg[p];
+            }
+            if (RING) rslot[p] = out;
+            vout[start + p] = out;
+            if (!fwd && a.accum) a.accum[start + p] += out;
+          }
+        }
+        named_bar_sync(1, kIluConsumerThreads);
+        if (ctid == 0) {
+          if (ok) mbar_arrive(&empty[st]);
+          sflags[1] = g + 1;
+        }
+        if (sflags[0]) break;   // uniform: read after the barrier
+      }
+      if (fwd) fence_proxy_async_global();
+    }
+    __syncthreads();
+    if (sflags[0]) break;
+  }
+  // After an abort, wait (bounded) for copies that were issued but never consumed so no
+  // bulk copy is still writing into this CTA's shared memory when it exits.
+  if (sflags[0] && threadIdx.x == 0) {
+    for (int g = sflags[1]; g < issued; ++g) mbar_wait(&full[g % NST], (g / NST) & 1, kWaitLimit);
+  }
+}
+
+// ------------------------------------------------------------------ host side
+template <class T>
+int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
+                     const int* d_pos, const int* d_rowAt, const int* d_lev, IluDev<T>& D) {
+  cudaStream_t st = stream();
+  D.nb = P.nb; D.np = P.np; D.n = P.n;
+  D.dilu = ilu_method != 0;
+  D.W = P.W;
+  D.maxWp = std::max(4, P.maxWp);
+  // chunk byte offsets for this value type
+  std::vector<IluChunk> ch = P.chunks;
+  int64_t oF = 0, oB = 0;
+  int64_t max_stage = 0;
+  for (auto& c : ch) {
+    c.offF = oF; c.offB = oB;
+    int64_t bf = chunk_bytes<T>(c.wpad, c.KL), bb = chunk_bytes<T>(c.wpad, c.KU);
+    oF += align16(bf); oB += align16(bb);
+    max_stage = std::max(max_stage, std::max(bf, bb) + (int64_t)c.wpad * (int64_t)sizeof(T));
+  }
+  D.packF_bytes = std::max<int64_t>(oF, 16);
+  D.packB_bytes = std::max<int64_t>(oB, 16);
+  D.stage_bytes = (int)((max_stage + 127) & ~int64_t(127));
+  // shared memory budget: barriers + ring + stages
+  int dev_smem = 0;
+  PB_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx().device));
+  const int budget = std::min(dev_smem, 220 * 1024);
+  int64_t ring_bytes = (int64_t)D.W * D.maxWp * sizeof(T);
+  D.ring = ring_bytes <= 64 * 1024;
+  int64_t ring_alloc = D.ring ? ((ring_bytes + 127) & ~int64_t(127)) : 0;
+  int nst = 8;
+  auto need = [&](int k) { return (int64_t)((16 * k + 16 + 127) & ~127) + ring_alloc + (int64_t)k * D.stage_bytes; };
+  while (nst > 2 && need(nst) > budget) --nst;
+  PB_CHECK(need(nst) <= budget, PARCEL_B_E_UNSUPPORTED,
+           "block-Jacobi level too wide for shared memory (stage %d bytes)", D.stage_bytes);
+  D.nstages = nst;
+  D.smem_bytes = (int)need(nst);
+
+  D.chunks.alloc(sizeof(IluChunk) * std::max<size_t>(ch.size(), 1));
+  h2d(D.chunks.p, ch.data(), sizeof(IluChunk) * ch.size());
+  {
+    std::vector<ProdDesc> tf(ch.size()), tb(ch.size());
+    for (size_t i = 0; i < ch.size(); ++i) {
+      const IluChunk& c = ch[i];
+      PB_CHECK(c.offF / 16 < INT32_MAX && c.offB / 16 < INT32_MAX, PARCEL_B_E_UNSUPPORTED,
+               "packed preconditioner larger than 32 GiB");
+      tf[i] = ProdDesc{(int)(c.offF / 16), c.start, (int)chunk_bytes<T>(c.wpad, c.KL),
+                       (int)(c.wpad * sizeof(T))};
+      tb[i] = ProdDesc{(int)(c.offB / 16), c.start, (int)chunk_bytes<T>(c.wpad, c.KU),
+                       (int)(c.wpad * sizeof(T))};
+    }
+    D.tabF.alloc(sizeof(ProdDesc) * std::max<size_t>(ch.size(), 1));
+    D.tabB.alloc(sizeof(ProdDesc) * std::max<size_t>(ch.size(), 1));
+    h2d(D.tabF.p, tf.data(), sizeof(ProdDesc) * ch.size());
+    h2d(D.tabB.p, tb.data(), sizeof(ProdDesc) * ch.size());
+  }
+  D.blk_chunk.alloc(sizeof(int) * (P.nb + 1));
+  h2d(D.blk_chunk.p, P.blk_chunk.data(), sizeof(int) * (P.nb + 1));
+  DBuf blo(sizeof(int) * P.nb), bhi(sizeof(int) * P.nb);
+  h2d(blo.p, P.blk_lo.data(), sizeof(int) * P.nb);
+  h2d(bhi.p, P.blk_hi.data(), sizeof(int) * P.nb);
+  DBuf blvl(sizeof(int) * (P.nb + 1)), lst(sizeof(int) * std::max<size_t>(P.lvl_start.size(), 1));
+  h2d(blvl.p, P.blk_lvl.data(), sizeof(int) * (P.nb + 1));
+  h2d(lst.p, P.lvl_start.data(), sizeof(int) * P.lvl_start.size());
+
+  // factorisation in natural CSR order
+  const int64_t nnz = A.nnz;
+  DBuf lu, Dd, Di;
+  const double* vL = A.val;
+  const double* vU = A.val;
+  if (!D.dilu) {
+    lu.alloc(sizeof(double) * nnz);
+    d2d(lu.p, A.val, sizeof(double) * nnz);
+    k_ilu0_factor<<<P.nb, 256, 0, st>>>(dp<IluChunk>(D.chunks), dp<int>(D.blk_chunk), dp<int>(blo),
+                                        dp<int>(bhi), d_rowAt, A.rowptr, A.col, A.rbase, A.cbase,
+                                        dp<double>(lu));
+    PB_CUDA(cudaGetLastError());
+    vL = dp<double>(lu);
+    vU = dp<double>(lu);
+  } else {
+    Dd.alloc(sizeof(double) * P.n);
+    Di.alloc(sizeof(double) * P.n);
+    k_dilu_diag<<<P.nb, 256, 0, st>>>(dp<IluChunk>(D.chunks), dp<int>(D.blk_chunk), dp<int>(blo),
+                                      dp<int>(bhi), d_rowAt, A.rowptr, A.col, A.val, A.rbase, A.cbase,
+                                      ilu_method == 2 ? 1 : 0, dp<double>(Dd), dp<double>(Di));
+    PB_CUDA(cudaGetLastError());
+  }
+  D.packF.alloc(D.packF_bytes);
+  D.packB.alloc(D.packB_bytes);
+  k_ilu_pack<T><<<std::min<int>((int)ch.size(), 65535) > 0 ? std::min<int>((int)ch.size(), 65535) : 1,
+                  128, 0, st>>>(
+      dp<IluChunk>(D.chunks), (int)ch.size(), dp<int>(blo), dp<int>(bhi), dp<int>(blvl),
+      dp<int>(lst), d_rowAt, d_pos, d_lev, A.rowptr, A.col, A.rbase, A.cbase, vL, vU,
+      D.dilu ? dp<double>(Di) : nullptr, D.dilu ? 1 : 0, D.ring ? 1 : 0, D.W, D.maxWp,
+      dp<unsigned char>(D.packF), dp<unsigned char>(D.packB));
+  PB_CUDA(cudaGetLastError());
+  D.ytmp.alloc(sizeof(T) * (P.np + 4));
+  PB_CUDA(cudaMemsetAsync(D.ytmp.p, 0, sizeof(T) * (P.np + 4), st));
+  D.err.alloc(sizeof(int));
+  PB_CUDA(cudaMemsetAsync(D.err.p, 0, sizeof(int), st));
+  // temporaries (lu, Dd, Di, blo, ...) are freed when this function returns: make sure
+  // the kernels that read them have finished.
+  sync();
+  return 0;
+}
+
+template <class T, bool DILU, bool RING>
+static void launch_ilu(const IluDev<T>& D, const IluSolveArgs<T>& a, cudaStream_t st) {
+  auto kern = k_ilu_solve<T, DILU, RING>;
+  static int configured = 0;
+  if (configured < D.smem_bytes) {
+    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    configured = 227 * 1024;
+  }
+  kern<<<D.nb, kIluThreads, D.smem_bytes, st>>>(a);
+}
+
+template <class T>
+void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, cudaStream_t st) {
+  IluSolveArgs<T> a;
+  a.tabF = dp<ProdDesc>(D.tabF);
+  a.tabB = dp<ProdDesc>(D.tabB);
+  a.blk_chunk = dp<int>(D.blk_chunk);
+  a.packF = dp<unsigned char>(D.packF);
+  a.packB = dp<unsigned char>(D.packB);
+  a.r = r;
+  a.y = dp<T>(D.ytmp);
+  a.s = s;
+  a.accum = accum;
+  a.W = D.W;
+  a.maxWp = D.maxWp;
+  a.stage_bytes = D.stage_bytes;
+  a.nstages = D.nstages;
+  a.ring_elems = D.ring ? D.W * D.maxWp : 0;
+  a.gate = gate;
+  a.err = dp<int>(D.err);
+  if (D.dilu) {
+    if (D.ring) launch_ilu<T, true, true>(D, a, st); else launch_ilu<T, true, false>(D, a, st);
+  } else {
+    if (D.ring) launch_ilu<T, false, true>(D, a, st); else launch_ilu<T, false, false>(D, a, st);
+  }
+  PB_CUDA(cudaGetLastError());
+}
+
+template int ilu_setup_device<double>(const IluPlan&, const DevMat<double>&, int, const int*,
+                                      const int*, const int*, IluDev<double>&);
+template int ilu_setup_device<float>(const IluPlan&, const DevMat<double>&, int, const int*,
+                                     const int*, const int*, IluDev<float>&);
+template void ilu_apply<double>(const IluDev<double>&, const double*, double*, double*,
+                                const int*, cudaStream_t);
+template void ilu_apply<float>(const IluDev<float>&, const float*, float*, float*, const int*,
+                               cudaStream_t);
+
+}  // namespace pb

@@ -1,0 +1,109 @@
+// pb_ilu.cuh -- block-Jacobi ILU(0) / D-ILU preconditioner on the level-major layout.
+#pragma once
+
+#include "pb_common.cuh"
+
+namespace pb {
+
+// Device matrix view.  Row pointers and columns may be 1-based (the reference's arrays,
+// rbase = 1, cbase = istart) or 0-based (internal copies, rbase = cbase = 0).
+template <class VT>
+struct DevMat {
+  int n = 0;
+  int64_t nnz = 0;
+  const int* rowptr = nullptr;
+  const int* col = nullptr;
+  const VT* val = nullptr;
+  int rbase = 0;
+  int cbase = 0;
+};
+
+// One chunk = up to kIluChunk rows of one wavefront level of one block.
+struct IluChunk {
+  int start;         // permuted position of the first row (multiple of 4)
+  int w;             // rows
+  int wpad;          // rows rounded up to 4
+  int KL, KU;        // max strictly-lower / strictly-upper in-block entries of its rows
+  int lvl;           // level index within the block
+  int off_in_level;  // position of the chunk's first row within its level
+  int blk;           // block-Jacobi block
+  int64_t offF, offB;   // byte offsets of the packed forward / backward data
+};
+constexpr int kIluChunk = 1024;     // rows per chunk (multiple of 4)
+constexpr int kIluHeader = 32;      // bytes of the per-chunk header in the packed data
+
+// Host-side plan: wavefront levels of every block and the permuted, padded layout.
+struct IluPlan {
+  int n = 0;            // natural rows
+  int np = 0;           // permuted length incl. padding
+  int nb = 0;           // blocks
+  int W = 1;            // ring depth in levels
+  int maxWp = 0;        // widest chunk (padded)
+  int max_levels = 0;
+  std::vector<int> pos;         // natural row -> permuted position
+  std::vector<int> lev;         // natural row -> level within its block
+  std::vector<int> rowAt;       // permuted position -> natural row, -1 = padding
+  std::vector<int> rowptrP;     // permuted 0-based row pointer (np + 1)
+  std::vector<IluChunk> chunks;
+  std::vector<int> blk_chunk;   // nb + 1
+  std::vector<int> blk_lo, blk_hi;   // natural row ranges [lo, hi)
+  std::vector<int> lvl_start;   // per block-level (global index) permuted start
+  std::vector<int> blk_lvl;     // nb + 1 index into lvl_start
+};
+
+// Device-resident preconditioner.
+template <class T>
+struct IluDev {
+  int nb = 0, np = 0, n = 0;
+  int W = 1, maxWp = 0;
+  bool ring = true;
+  bool dilu = false;
+  int stage_bytes = 0, nstages = 0, smem_bytes = 0;
+  DBuf chunks;      // IluChunk[]
+  DBuf tabF, tabB;  // per-chunk producer descriptors
+  DBuf blk_chunk;   // int[nb+1]
+  DBuf packF, packB;
+  int64_t packF_bytes = 0, packB_bytes = 0;
+  DBuf ytmp;        // forward result, np + 1 entries
+  DBuf err;         // int error flag
+};
+
+// Permuted matrix (0-based) in the layout of the plan.
+template <class VT>
+struct PermMat {
+  DBuf rowptr, col, val;
+  DevMat<VT> view(int np, int64_t nnz) const {
+    DevMat<VT> m;
+    m.n = np; m.nnz = nnz;
+    m.rowptr = dp<int>(rowptr); m.col = dp<int>(col); m.val = dp<VT>(val);
+    return m;
+  }
+};
+
+struct HostCSR {
+  int n = 0;
+  int64_t nnz = 0;
+  int istart = 1;
+  const int* rowptr = nullptr;   // 1-based
+  const int* col = nullptr;      // 1-based global
+};
+
+void ilu_build_plan(const HostCSR& A, int nblocks, IluPlan& P);
+
+// Builds the permuted copy of A (values cast to VT) on the device.
+template <class VT>
+void ilu_permute_matrix(const IluPlan& P, const DevMat<double>& A, const int* d_pos,
+                        const int* d_rowAt, PermMat<VT>& out, int64_t nnz);
+
+// Factorises (ILU(0)) or computes the D-ILU diagonal on the device and packs the sweep
+// data.  ilu_method: 0 ILU(0), 1 ILUD, 2 MLUD (define.f90:40-42).  Returns a status.
+template <class T>
+int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
+                     const int* d_pos, const int* d_rowAt, const int* d_lev, IluDev<T>& D);
+
+// s = M^-1 r on permuted vectors (np entries each).  If `accum` is non-null the result
+// is added into it instead of being written to s (s may then be null).
+template <class T>
+void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, cudaStream_t st);
+
+}  // namespace pb

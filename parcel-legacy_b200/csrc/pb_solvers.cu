@@ -1,0 +1,477 @@
+// pb_solvers.cu -- PCG, BiCGStab and GMRES(m) drivers on B200.
+//
+// Reference loops (restated): KSP_pCG (src/pcg.f90:224-892), KSP_pBiCG
+// (src/pbicg.f90:280-698), KSP_pGMRES (src/pgmres.f90:62-525) with GivensRotations and
+// update_xVec (src/pcagmres.f90:190-242, 1136-1236).
+//
+// The reference's GPU path synchronises the device and moves a scalar across PCIe for
+// every dot product and axpy (src/CUDA/src/cu_common.cu:412-446,
+// src/parcel_vec.f90:466-470).  Here every scalar stays on the device (KState) and the
+// solver logic runs in the epilogue of the reduction that produces it, so an iteration
+// is a fixed sequence of kernel launches.  Each kernel first reads a device flag and
+// returns at once after the reference loop has exited, which lets a whole restart cycle
+// (GMRES) or a chunk of iterations (CG, BiCGStab) be captured once into a CUDA graph and
+// replayed; the host looks at the flag once per replay.
+#include <algorithm>
+#include <chrono>
+#include <type_traits>
+
+#include "pb_solvers.cuh"
+
+namespace pb {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// ------------------------------------------------------------------ options
+Options resolve_options(const parcel_b_input* p) {
+  Options o;
+  if (!p) return o;
+  if (p->solver > 0) o.solver = p->solver;
+  if (p->ipreflag >= 0) o.precon = p->ipreflag;
+  if (o.precon == PARCEL_B_PRECON_ADDITIVESCHWARZ) o.precon = PARCEL_B_PRECON_BLOCKJACOBI;
+  if (p->ILU_method >= 0) o.ilu_method = p->ILU_method;
+  if (p->precon_thblock > 0) o.nblocks = p->precon_thblock;
+  if (p->GMRES_m > 0) o.m = p->GMRES_m;
+  if (p->GMRES_GSflag > 0) o.gs = p->GMRES_GSflag;
+  if (p->itrmax > 0) o.itrmax = p->itrmax;
+  if (p->rtolmax != -1.0) o.rtol = p->rtolmax;
+  if (p->abstolmax > 0.0) o.abstol = p->abstolmax;
+  if (p->CAGMRES_sstep > 0) o.sstep = p->CAGMRES_sstep;
+  if (p->CAGMRES_tstep > 0) o.tstep = p->CAGMRES_tstep;
+  if (p->CAGMRES_basis >= 0) o.basis = p->CAGMRES_basis;
+  if (p->CAGMRES_QRflag > 0) o.qrflag = p->CAGMRES_QRflag;
+  if (p->inner_precision > 0) o.inner = p->inner_precision;
+  if (p->residual_dd > 0) o.residual_dd = 1;
+  if (p->inner_rtol > 0.0) o.inner_rtol = p->inner_rtol;
+  if (p->max_refine > 0) o.max_refine = p->max_refine;
+  if (p->independ_nvec > 0) o.independ_nvec = p->independ_nvec;
+  if (p->reserved[0] == 1) o.use_graphs = false;
+  return o;
+}
+
+// ------------------------------------------------------------------ workspace
+void Workspace::init() {
+  part.alloc(sizeof(double) * (size_t)red_blocks() * kMaxRed);
+  ticket.alloc(sizeof(unsigned) * 4);
+  state.alloc(sizeof(KState));
+  PB_CUDA(cudaMemsetAsync(ticket.p, 0, sizeof(unsigned) * 4, stream()));
+  PB_CUDA(cudaMemsetAsync(state.p, 0, sizeof(KState), stream()));
+}
+
+Red Workspace::red(int epi) const {
+  Red r;
+  r.part = dp<double>(part);
+  r.ticket = dp<unsigned>(ticket);
+  r.epi = epi;
+  r.ea.st = st();
+  return r;
+}
+
+// ------------------------------------------------------------------ preconditioner
+template <class T>
+__global__ void k_pj_dinv(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                          const double* __restrict__ va, int rbase, int cbase, T* __restrict__ dinv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = 0.0;
+    for (int j = rp[i] - rbase; j < rp[i + 1] - rbase; ++j)
+      if (ci[j] - cbase == i) d = va[j];
+    if (d == 0.0) d = 1.0e-300;   // get_DInv_crs (matrix.f90:3104-3144)
+    dinv[i] = (T)(1.0 / d);
+  }
+}
+
+template <class T>
+void Precon<T>::apply(int64_t np, const T* r, T* s, const int* gate, cudaStream_t st) const {
+  switch (kind) {
+    case PARCEL_B_PRECON_NONE:
+      lincomb<T>(np, s, r, cimm(1.0), nullptr, cimm(0.0), nullptr, cimm(0.0), gate, st);
+      break;
+    case PARCEL_B_PRECON_POINTJACOBI:
+      scale<T>(np, s, dp<T>(dinv), r, gate, st);
+      break;
+    case PARCEL_B_PRECON_BLOCKJACOBI:
+      ilu_apply<T>(ilu, r, s, nullptr, gate, st);
+      break;
+  }
+}
+
+// ------------------------------------------------------------------ system setup
+template <class T>
+void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& S) {
+  cudaStream_t st = stream();
+  S.n = A.n;
+  S.nnz = A.nnz;
+  const int* rp = A.rowptr;
+  const int* ci = A.col;
+  const double* va = A.val;
+  if (!dev) {
+    S.up_rowptr.alloc(sizeof(int) * (A.n + 1));
+    S.up_col.alloc(sizeof(int) * std::max<int64_t>(A.nnz, 1));
+    S.up_val.alloc(sizeof(double) * std::max<int64_t>(A.nnz, 1));
+    h2d(S.up_rowptr.p, A.rowptr, sizeof(int) * (A.n + 1));
+    h2d(S.up_col.p, A.col, sizeof(int) * A.nnz);
+    h2d(S.up_val.p, A.val, sizeof(double) * A.nnz);
+    rp = dp<int>(S.up_rowptr);
+    ci = dp<int>(S.up_col);
+    va = dp<double>(S.up_val);
+  }
+  S.Anat.n = A.n;
+  S.Anat.nnz = A.nnz;
+  S.Anat.rowptr = rp;
+  S.Anat.col = ci;
+  S.Anat.val = va;
+  S.Anat.rbase = 1;
+  S.Anat.cbase = A.istart;
+  S.M.kind = o.precon;
+
+  if (o.precon == PARCEL_B_PRECON_BLOCKJACOBI) {
+    // The wavefront analysis needs the sparsity structure on the host.
+    std::vector<int> hrp, hci;
+    const int* hrpp = A.rowptr;
+    const int* hcip = A.col;
+    if (dev) {
+      hrp.resize(A.n + 1);
+      hci.resize(A.nnz);
+      d2h(hrp.data(), A.rowptr, sizeof(int) * (A.n + 1));
+      d2h(hci.data(), A.col, sizeof(int) * A.nnz);
+      hrpp = hrp.data();
+      hcip = hci.data();
+    }
+    HostCSR H;
+    H.n = A.n; H.nnz = A.nnz; H.istart = A.istart; H.rowptr = hrpp; H.col = hcip;
+    IluPlan P;
+    ilu_build_plan(H, std::max(1, std::min(o.nblocks, A.n)), P);
+    S.np = P.np;
+    S.permuted = true;
+    S.ilu_levels_max = P.max_levels;
+    S.ilu_nblocks = P.nb;
+    S.pos.alloc(sizeof(int) * A.n);
+    S.lev.alloc(sizeof(int) * A.n);
+    S.rowAt.alloc(sizeof(int) * P.np);
+    h2d(S.pos.p, P.pos.data(), sizeof(int) * A.n);
+    h2d(S.lev.p, P.lev.data(), sizeof(int) * A.n);
+    h2d(S.rowAt.p, P.rowAt.data(), sizeof(int) * P.np);
+    ilu_permute_matrix<T>(P, S.Anat, dp<int>(S.pos), dp<int>(S.rowAt), S.Ap, A.nnz);
+    S.A = S.Ap.view(P.np, A.nnz);
+    ilu_setup_device<T>(P, S.Anat, o.ilu_method, dp<int>(S.pos), dp<int>(S.rowAt),
+                        dp<int>(S.lev), S.M.ilu);
+  } else {
+    S.np = A.n;
+    S.permuted = false;
+    if constexpr (std::is_same<T, double>::value) {
+      S.A = S.Anat;
+    } else {
+      S.Aval_T.alloc(sizeof(T) * std::max<int64_t>(A.nnz, 1));
+      convert<T, double>(A.nnz, dp<T>(S.Aval_T), va, st);
+      S.A.n = A.n; S.A.nnz = A.nnz; S.A.rowptr = rp; S.A.col = ci;
+      S.A.val = dp<T>(S.Aval_T); S.A.rbase = 1; S.A.cbase = A.istart;
+    }
+    if (o.precon == PARCEL_B_PRECON_POINTJACOBI) {
+      S.M.dinv.alloc(sizeof(T) * A.n);
+      k_pj_dinv<T><<<8 * num_sms(), 256, 0, st>>>(A.n, rp, ci, va, 1, A.istart, dp<T>(S.M.dinv));
+      PB_CUDA(cudaGetLastError());
+    }
+  }
+}
+
+// ------------------------------------------------------------------ graph replay
+struct GraphRunner {
+  cudaGraphExec_t exec = nullptr;
+  int launches = 0;
+  GraphRunner() = default;
+  GraphRunner(const GraphRunner&) = delete;
+  ~GraphRunner() { if (exec) cudaGraphExecDestroy(exec); }
+  template <class F>
+  void launch(F&& f, bool use_graph, cudaStream_t st) {
+    if (!use_graph) { f(); return; }
+    if (!exec) {
+      cudaGraph_t g = nullptr;
+      PB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        f();
+      } catch (...) {
+        cudaGraph_t g2 = nullptr;
+        cudaStreamEndCapture(st, &g2);
+        if (g2) cudaGraphDestroy(g2);
+        throw;
+      }
+      PB_CUDA(cudaStreamEndCapture(st, &g));
+      PB_CUDA(cudaGraphInstantiate(&exec, g, 0));
+      cudaGraphDestroy(g);
+    }
+    PB_CUDA(cudaGraphLaunch(exec, st));
+  }
+};
+
+static int read_done(const KState* st, cudaStream_t s) {
+  static int* pinned = nullptr;
+  if (!pinned) PB_CUDA(cudaMallocHost(&pinned, sizeof(int)));
+  PB_CUDA(cudaMemcpyAsync(pinned, &st->done, sizeof(int), cudaMemcpyDeviceToHost, s));
+  PB_CUDA(cudaStreamSynchronize(s));
+  return *pinned;
+}
+
+static KState read_state(const KState* st) {
+  KState h;
+  d2h(&h, st, sizeof(KState));
+  return h;
+}
+
+static void init_state(Workspace& W, int itr0) {
+  KState h;
+  memset(&h, 0, sizeof(h));
+  h.itr = itr0;
+  h.last_inner = 1;
+  h2d(W.state.p, &h, sizeof(KState));
+}
+
+// ------------------------------------------------------------------ PCG
+template <class T>
+static SolveOut run_pcg(const Options& o, const System<T>& S, const T* b, T* x, double* hist,
+                        Workspace& W) {
+  cudaStream_t st = stream();
+  const int64_t np = S.np;
+  DBuf r(sizeof(T) * np), p(sizeof(T) * np), q(sizeof(T) * np), s(sizeof(T) * np);
+  T* R = dp<T>(r); T* P = dp<T>(p); T* Q = dp<T>(q); T* Sv = dp<T>(s);
+  KState* K = W.st();
+  init_state(W, 1);
+  const int* gdone = &K->done;
+  auto red = [&](int epi) {
+    Red rr = W.red(epi);
+    rr.ea.hist = hist; rr.ea.itrmax = o.itrmax; rr.ea.rtol = o.rtol; rr.ea.abstol = o.abstol;
+    return rr;
+  };
+  int launches = 0;
+  // r = b - A x; s = M^-1 r; bnorm, rnorm, rho0 = <s, r>   (pcg.f90:442-478)
+  spmv<T, T>(S.A, x, R, SPMV_RES, b, nullptr, st);
+  S.M.apply(np, R, Sv, nullptr, st);
+  PB_CUDA(cudaMemsetAsync(P, 0, sizeof(T) * np, st));
+  DotSel sel;
+  sel.a[0] = 1; sel.b[0] = 1;   // <b, b>
+  sel.a[1] = 2; sel.b[1] = 2;   // <r, r>
+  sel.a[2] = 3; sel.b[2] = 2;   // <s, r>
+  lincomb_dot<T>(np, nullptr, b, cimm(0), R, cimm(0), Sv, cimm(0), nullptr, nullptr, sel, 3,
+                 red(EPI_CG_INIT), nullptr, st);
+  launches += 3;
+  const int chunk = 16;
+  auto iterations = [&] {
+    for (int it = 0; it < chunk; ++it) {
+      cg_axpy2<T>(np, x, P, Sv, K, gdone, st);                            // x += alpha p; p = s + beta p
+      int sa[2] = {1, 0}, sb[2] = {0, 0};
+      spmv_dot<T, T>(S.A, P, Q, SPMV_Y, nullptr, nullptr, 1, sa, sb, red(EPI_CG_GAMMA), gdone, st);
+      lincomb<T>(np, R, Q, cdev(&K->tmp[0]), R, cimm(1.0), nullptr, cimm(0), gdone, st);  // r = -alpha q + r
+      S.M.apply(np, R, Sv, gdone, st);                                    // s = M^-1 r
+      DotSel d2;
+      d2.a[0] = 1; d2.b[0] = 2;   // <s, r>
+      d2.a[1] = 2; d2.b[1] = 2;   // <r, r>
+      lincomb_dot<T>(np, nullptr, Sv, cimm(0), R, cimm(0), nullptr, cimm(0), nullptr, nullptr, d2, 2,
+                     red(EPI_CG_DOT2), gdone, st);
+    }
+  };
+  GraphRunner G;
+  const int max_chunks = o.itrmax / chunk + 2;
+  for (int c = 0; c < max_chunks; ++c) {
+    if (read_done(K, st)) break;
+    G.launch(iterations, o.use_graphs, st);
+    launches += 5 * chunk;
+  }
+  // x = alpha p + x   (pcg.f90:733)
+  lincomb<T>(np, x, P, cdev(&K->alpha), x, cimm(1.0), nullptr, cimm(0), nullptr, st);
+  launches += 1;
+  KState h = read_state(K);
+  SolveOut out;
+  out.niter = h.niter;
+  out.iret = h.iret;
+  out.breakdown = h.breakdown;
+  out.launches = launches;
+  return out;
+}
+
+// ------------------------------------------------------------------ BiCGStab
+template <class T>
+static SolveOut run_bicg(const Options& o, const System<T>& S, const T* b, T* x, double* hist,
+                         Workspace& W) {
+  cudaStream_t st = stream();
+  const int64_t np = S.np;
+  const size_t vb = sizeof(T) * np;
+  DBuf r(vb), r0(vb), p(vb), q(vb), pp(vb), e(vb), pe(vb), v(vb);
+  T *R = dp<T>(r), *R0 = dp<T>(r0), *P = dp<T>(p), *Q = dp<T>(q), *PP = dp<T>(pp),
+    *E = dp<T>(e), *PE = dp<T>(pe), *V = dp<T>(v);
+  KState* K = W.st();
+  init_state(W, 1);
+  const int* gdone = &K->done;
+  auto red = [&](int epi) {
+    Red rr = W.red(epi);
+    rr.ea.hist = hist; rr.ea.itrmax = o.itrmax; rr.ea.rtol = o.rtol;
+    return rr;
+  };
+  int launches = 0;
+  spmv<T, T>(S.A, x, R, SPMV_RES, b, nullptr, st);
+  DotSel sel;
+  sel.a[0] = 1; sel.b[0] = 1;   // <b, b>
+  sel.a[1] = 2; sel.b[1] = 2;   // <r, r>
+  lincomb_dot<T>(np, nullptr, b, cimm(0), R, cimm(0), nullptr, cimm(0), nullptr, nullptr, sel, 2,
+                 red(EPI_BICG_INIT), nullptr, st);
+  d2d(R0, R, vb);
+  d2d(P, R, vb);
+  launches += 2;
+  const int chunk = 8;
+  auto iterations = [&] {
+    for (int it = 0; it < chunk; ++it) {
+      S.M.apply(np, P, PP, gdone, st);                                        // pp = M^-1 p
+      int sa[2] = {2, 0}, sb[2] = {0, 0};
+      spmv_dot<T, T>(S.A, PP, Q, SPMV_Y, nullptr, R0, 1, sa, sb, red(EPI_BICG_C2), gdone, st);  // q, c2
+      lincomb<T>(np, E, R, cimm(1.0), Q, cdev(&K->tmp[0]), nullptr, cimm(0), gdone, st);      // e = r - alpha q
+      S.M.apply(np, E, PE, gdone, st);                                        // pe = M^-1 e
+      int sa2[2] = {2, 0}, sb2[2] = {0, 0};
+      spmv_dot<T, T>(S.A, PE, V, SPMV_Y, nullptr, E, 2, sa2, sb2, red(EPI_BICG_C3), gdone, st);  // v, <e,v>, <v,v>
+      lincomb<T>(np, x, PP, cdev(&K->alpha), PE, cdev(&K->c3), x, cimm(1.0), gdone, st);   // x += alpha pp + c3 pe
+      DotSel d3;
+      d3.a[0] = 0; d3.b[0] = 4;   // <r, r0>
+      d3.a[1] = 0; d3.b[1] = 0;   // <r, r>
+      lincomb_dot<T>(np, R, E, cimm(1.0), V, cdev(&K->tmp[1]), nullptr, cimm(0), R0, nullptr, d3, 2,
+                     red(EPI_BICG_END), gdone, st);                           // r = e - c3 v
+      lincomb<T>(np, P, R, cimm(1.0), Q, cdev(&K->tmp[2]), P, cdev(&K->beta), gdone, st);  // p = r - beta c3 q + beta p
+    }
+  };
+  GraphRunner G;
+  const int max_chunks = o.itrmax / chunk + 2;
+  for (int c = 0; c < max_chunks; ++c) {
+    if (read_done(K, st)) break;
+    G.launch(iterations, o.use_graphs, st);
+    launches += 8 * chunk;
+  }
+  KState h = read_state(K);
+  SolveOut out;
+  out.niter = h.niter;
+  out.iret = h.iret;
+  out.breakdown = h.breakdown;
+  out.launches = launches;
+  return out;
+}
+
+// ------------------------------------------------------------------ GMRES(m)
+template <class T>
+static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x, double* hist,
+                          Workspace& W) {
+  cudaStream_t st = stream();
+  const int64_t np = S.np;
+  const int m = o.m;
+  PB_CHECK(m >= 1 && m < kMaxRed, PARCEL_B_E_ARG, "GMRES restart length %d outside [1, %d)", m, kMaxRed);
+  const int64_t ldv = (np + 31) & ~int64_t(31);
+  const size_t vb = sizeof(T) * np;
+  DBuf r(vb), Vb(sizeof(T) * ldv * (m + 1)), pv(vb), w(vb), v0(vb), x0(vb);
+  DBuf hb(sizeof(double) * (m + 1) * m), eb(sizeof(double) * (m + 1)), csb(sizeof(double) * (m + 1)),
+      snb(sizeof(double) * (m + 1)), yb(sizeof(double) * (m + 1));
+  T *R = dp<T>(r), *V = dp<T>(Vb), *PV = dp<T>(pv), *Wv = dp<T>(w), *V0 = dp<T>(v0),
+    *X0 = dp<T>(x0);
+  PB_CUDA(cudaMemsetAsync(V, 0, sizeof(T) * ldv * (m + 1), st));
+  KState* K = W.st();
+  init_state(W, 1);
+  const int* gdone = &K->done;
+  const int* gskip = &K->skip_inner;
+  auto red = [&](int epi, int k = 0, int j = 0) {
+    Red rr = W.red(epi);
+    rr.ea.hist = hist; rr.ea.itrmax = o.itrmax; rr.ea.rtol = o.rtol; rr.ea.abstol = o.abstol;
+    rr.ea.h = dp<double>(hb); rr.ea.e = dp<double>(eb); rr.ea.cs = dp<double>(csb);
+    rr.ea.sn = dp<double>(snb); rr.ea.m = m; rr.ea.k = k; rr.ea.j = j;
+    return rr;
+  };
+  int launches = 0;
+  {  // bnorm = ||b||
+    Red rr = red(EPI_NORM2);
+    rr.ea.out = &K->bnorm;
+    DotSel sel;
+    sel.a[0] = 1; sel.b[0] = 1;
+    lincomb_dot<T>(np, nullptr, b, cimm(0), nullptr, cimm(0), nullptr, cimm(0), nullptr, nullptr, sel, 1,
+                   rr, nullptr, st);
+    launches += 1;
+  }
+  int per_cycle = 0;
+  auto cycle = [&] {
+    per_cycle = 0;
+    int sa[2] = {0, 0}, sb[2] = {0, 0};
+    spmv_dot<T, T>(S.A, x, R, SPMV_RES, b, nullptr, 1, sa, sb, red(EPI_GM_RESTART), gdone, st);
+    ++per_cycle;
+    for (int j = 1; j <= m; ++j) {
+      T* Vj = V + (size_t)(j - 1) * ldv;
+      if (j == 1) {
+        lincomb<T>(np, Vj, R, cdev(&K->tmp[0]), nullptr, cimm(0), nullptr, cimm(0), gskip, st);
+        ++per_cycle;
+      }
+      S.M.apply(np, Vj, PV, gskip, st);
+      ++per_cycle;
+      if (o.gs == PARCEL_B_GS_CGS) {
+        spmv<T, T>(S.A, PV, Wv, SPMV_Y, nullptr, gskip, st);
+        multidot<T>(np, j, Wv, V, ldv, red(EPI_GM_HCGS, 0, j), gskip, st);
+        cgs_update<T>(np, j, Wv, V, ldv, dp<double>(hb) + (size_t)(j - 1) * (m + 1), red(EPI_GM_NORM, 0, j),
+                      gskip, st);
+        per_cycle += 3;
+      } else {
+        int sa1[2] = {0, 0}, sb1[2] = {2, 0};   // <w, v_1>
+        spmv_dot<T, T>(S.A, PV, Wv, SPMV_Y, nullptr, V, 1, sa1, sb1, red(EPI_GM_H, 1, j), gskip, st);
+        ++per_cycle;
+        for (int k = 1; k <= j; ++k) {
+          const T* Vk = V + (size_t)(k - 1) * ldv;
+          DotSel d;
+          if (k < j) { d.a[0] = 0; d.b[0] = 4; }   // <w, v_{k+1}>
+          else { d.a[0] = 0; d.b[0] = 0; }         // <w, w>
+          const T* Vnext = (k < j) ? V + (size_t)k * ldv : nullptr;
+          lincomb_dot<T>(np, Wv, Vk, cdev(&K->tmp[1]), Wv, cimm(1.0), nullptr, cimm(0), Vnext, nullptr, d, 1,
+                         (k < j) ? red(EPI_GM_H, k + 1, j) : red(EPI_GM_NORM, 0, j), gskip, st);
+          ++per_cycle;
+        }
+      }
+      if (j < m) {
+        lincomb<T>(np, V + (size_t)j * ldv, Wv, cdev(&K->tmp[2]), nullptr, cimm(0), nullptr, cimm(0), gskip, st);
+        ++per_cycle;
+      }
+    }
+    // update_xVec: y = H^-1 e; v0 = V y; x0 = M^-1 v0; x = x0 + x
+    gm_backsolve(dp<double>(hb), dp<double>(eb), dp<double>(yb), m, K, gdone, st);
+    sum_vec<T>(np, V0, V, ldv, dp<double>(yb), K, gdone, st);
+    S.M.apply(np, V0, X0, gdone, st);
+    lincomb<T>(np, x, X0, cimm(1.0), x, cimm(1.0), nullptr, cimm(0), gdone, st);
+    gm_post(K, m, o.itrmax, st);
+    per_cycle += 5;
+  };
+  GraphRunner G;
+  const int max_cycles = o.itrmax / m + 2;
+  for (int c = 0; c < max_cycles; ++c) {
+    if (read_done(K, st)) break;
+    G.launch(cycle, o.use_graphs, st);
+    launches += per_cycle;
+  }
+  KState h = read_state(K);
+  SolveOut out;
+  out.niter = h.niter;
+  out.iret = h.iret;
+  out.breakdown = h.breakdown;
+  out.launches = launches;
+  return out;
+}
+
+template <class T>
+SolveOut run_krylov(const Options& o, const System<T>& S, const T* b, T* x, double* hist_dev) {
+  Workspace W;
+  W.init();
+  switch (o.solver) {
+    case PARCEL_B_SOLVER_CG: return run_pcg<T>(o, S, b, x, hist_dev, W);
+    case PARCEL_B_SOLVER_BICG: return run_bicg<T>(o, S, b, x, hist_dev, W);
+    case PARCEL_B_SOLVER_GMRES: return run_gmres<T>(o, S, b, x, hist_dev, W);
+    default:
+      PB_CHECK(false, PARCEL_B_E_UNSUPPORTED, "solver %d is not provided by this build", o.solver);
+  }
+  return SolveOut{};
+}
+
+template void build_system<double>(const Options&, const parcel_b_crs&, bool, System<double>&);
+template void build_system<float>(const Options&, const parcel_b_crs&, bool, System<float>&);
+template SolveOut run_krylov<double>(const Options&, const System<double>&, const double*, double*,
+                                     double*);
+template SolveOut run_krylov<float>(const Options&, const System<float>&, const float*, float*,
+                                    double*);
+
+}  // namespace pb

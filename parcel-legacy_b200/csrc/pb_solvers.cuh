@@ -1,0 +1,88 @@
+// pb_solvers.cuh -- solver drivers (pb_solvers.cu).
+#pragma once
+
+#include <chrono>
+#include <memory>
+
+#include "pb_blas.cuh"
+#include "pb_ilu.cuh"
+#include "pb_spmv.cuh"
+
+namespace pb {
+
+// Resolved options (KSP_INPUT_PARAM after PARCEL_KSP_Default_Setting, type.f90:949-1132).
+struct Options {
+  int solver = PARCEL_B_SOLVER_GMRES;
+  int precon = PARCEL_B_PRECON_NONE;
+  int ilu_method = PARCEL_B_ILUD;
+  int nblocks = 1;
+  int m = 4;
+  int gs = PARCEL_B_GS_MGS;
+  int itrmax = 100;
+  double rtol = 1e-8;
+  double abstol = 0.0;
+  int sstep = 4, tstep = 1, basis = PARCEL_B_BASIS_MONOMIAL, qrflag = PARCEL_B_QR_CHOLQR;
+  int inner = PARCEL_B_INNER_FP64;
+  int residual_dd = 0;
+  double inner_rtol = 1e-4;
+  int max_refine = 50;
+  int independ_nvec = 1;
+  bool use_graphs = true;
+};
+
+Options resolve_options(const parcel_b_input* p);
+
+// Preconditioner on iteration-layout vectors.
+template <class T>
+struct Precon {
+  int kind = PARCEL_B_PRECON_NONE;
+  DBuf dinv;
+  IluDev<T> ilu;
+  int launches_per_apply() const { return 1; }
+  void apply(int64_t np, const T* r, T* s, const int* gate, cudaStream_t st) const;
+};
+
+// Everything a solve needs on the device, in the iteration layout.
+template <class T>
+struct System {
+  int n = 0;            // natural rows
+  int np = 0;           // iteration-layout length
+  int64_t nnz = 0;
+  bool permuted = false;
+  DevMat<double> Anat;  // natural matrix (reference layout)
+  DBuf up_rowptr, up_col, up_val;   // uploaded copies of host inputs
+  PermMat<T> Ap;        // permuted matrix (block Jacobi)
+  DevMat<T> A;          // matrix of the iteration
+  DBuf Aval_T;          // natural values cast to T (FP32 path, no permutation)
+  DBuf pos, rowAt, lev; // layout maps (block Jacobi)
+  Precon<T> M;
+  int ilu_levels_max = 0;
+  int ilu_nblocks = 0;
+};
+
+template <class T>
+void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& S);
+
+struct SolveOut {
+  int niter = 0;
+  int iret = 0;
+  int launches = 0;
+  int breakdown = 0;
+};
+
+// Runs the Krylov iteration on iteration-layout vectors x (in/out) and b.  hist_dev has
+// itrmax+1 entries on the device.
+template <class T>
+SolveOut run_krylov(const Options& o, const System<T>& S, const T* b, T* x, double* hist_dev);
+
+// Workspace shared by the drivers.
+struct Workspace {
+  DBuf part, ticket, state;
+  Red red(int epi) const;
+  KState* st() const { return dp<KState>(state); }
+  void init();
+};
+
+double now_s();
+
+}  // namespace pb

@@ -1,0 +1,164 @@
+// pb_spmv.cu -- CRS sparse matrix-vector product for B200.
+//
+// Replaces MatVec_crs (src/matrix.f90:1348-1512) on the CPU and cusparse_SpMV
+// (src/CUDA/src/cusparse.cu:632-672) on the GPU, which the reference calls with four
+// device synchronisations and a DnVec descriptor re-creation per product
+// (src/krylov_h.f90:11-78).
+//
+// Layout: LPR lanes of a warp share a row (LPR from the mean row length: 8 for the
+// 7-point stencils), so a warp covers 32/LPR consecutive rows whose nonzeros are
+// contiguous and every value/column load is coalesced; each warp keeps UNR such row
+// groups in flight to hide HBM latency.  Values and columns stream with evict-first loads
+// (they are read once per product); x is gathered through the read-only path, where its
+// stencil locality turns into L1/L2 hits.  The product can be fused with the residual
+// b - A x and with one or two dot products that are reduced deterministically on the
+// device.
+#include "pb_device.cuh"
+#include "pb_epilogue.cuh"
+#include "pb_spmv.cuh"
+
+namespace pb {
+
+int spmv_lanes(int n, int64_t nnz) {
+  double avg = n > 0 ? (double)nnz / n : 1.0;
+  if (avg <= 2.0) return 2;
+  if (avg <= 4.0) return 4;
+  if (avg <= 10.0) return 8;
+  if (avg <= 20.0) return 16;
+  return 32;
+}
+
+template <class T> __device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
+
+template <int LPR, int UNR, class VT, class XT, int ND, bool RES>
+__global__ void __launch_bounds__(kRedThreads) k_spmv(int n, const int* __restrict__ rp,
+                                                      const int* __restrict__ ci,
+                                                      const VT* __restrict__ va, int rbase,
+                                                      int cbase, const XT* __restrict__ x,
+                                                      XT* __restrict__ y, const XT* __restrict__ b,
+                                                      const XT* __restrict__ d, int sa0, int sb0,
+                                                      int sa1, int sb1, Red red, const int* gate) {
+  if (gated(gate)) return;
+  constexpr int G = 32 / LPR;
+  constexpr int TILE = G * UNR;
+  const int lane = threadIdx.x & 31;
+  const int g = lane / LPR, lg = lane % LPR;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  double acc[ND > 0 ? ND : 1];
+#pragma unroll
+  for (int k = 0; k < (ND > 0 ? ND : 1); ++k) acc[k] = 0.0;
+
+  for (int64_t base = warp * TILE; base < n; base += nwarps * TILE) {
+    int beg[UNR], len[UNR];
+    int maxlen = 0;
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      int64_t row = base + u * G + g;
+      if (row < n) {
+        beg[u] = __ldg(rp + row) - rbase;
+        len[u] = __ldg(rp + row + 1) - rbase - beg[u];
+      } else {
+        beg[u] = 0;
+        len[u] = 0;
+      }
+      maxlen = max(maxlen, len[u]);
+    }
+    XT sum[UNR];
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) sum[u] = XT(0);
+    for (int k = lg; k < maxlen; k += LPR) {
+      VT v[UNR];
+      int c[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        if (k < len[u]) {
+          v[u] = ld_stream(va + beg[u] + k);
+          c[u] = ld_stream(ci + beg[u] + k) - cbase;
+        } else {
+          v[u] = VT(0);
+          c[u] = -1;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < UNR; ++u)
+        if (c[u] >= 0) sum[u] += (XT)v[u] * __ldg(x + c[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) sum[u] += __shfl_xor_sync(kFull, sum[u], o);
+    }
+    if (lg == 0) {
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        int64_t row = base + u * G + g;
+        if (row < n) {
+          XT yv = RES ? b[row] - sum[u] : sum[u];
+          y[row] = yv;
+          if constexpr (ND > 0) {
+            XT src[3] = {yv, x[row], d ? d[row] : XT(0)};
+            acc[0] += (double)(src[sa0] * src[sb0]);
+            if (ND > 1) acc[ND > 1 ? 1 : 0] += (double)(src[sa1] * src[sb1]);
+          }
+        }
+      }
+    }
+  }
+  if constexpr (ND > 0) reduce_and_finish<ND>(acc, red);
+}
+
+template <class VT, class XT, int ND, bool RES>
+static void launch_spmv(const DevMat<VT>& A, const XT* x, XT* y, const XT* b, const XT* d,
+                        const int* sa, const int* sb, const Red& red, const int* gate,
+                        cudaStream_t st) {
+  const int lpr = spmv_lanes(A.n, A.nnz);
+  const int grid = red_blocks();
+  int a0 = sa ? sa[0] : 0, b0 = sb ? sb[0] : 0, a1 = sa ? sa[1] : 0, b1 = sb ? sb[1] : 0;
+#define L(LPR_, UNR_)                                                                         \
+  k_spmv<LPR_, UNR_, VT, XT, ND, RES><<<grid, kRedThreads, 0, st>>>(                          \
+      A.n, A.rowptr, A.col, A.val, A.rbase, A.cbase, x, y, b, d, a0, b0, a1, b1, red, gate)
+  switch (lpr) {
+    case 2: L(2, 4); break;
+    case 4: L(4, 4); break;
+    case 8: L(8, 4); break;
+    case 16: L(16, 2); break;
+    default: L(32, 1); break;
+  }
+#undef L
+  PB_CUDA(cudaGetLastError());
+}
+
+template <class VT, class XT>
+void spmv(const DevMat<VT>& A, const XT* x, XT* y, int mode, const XT* b, const int* gate,
+          cudaStream_t st) {
+  Red red{};
+  if (mode == SPMV_RES) launch_spmv<VT, XT, 0, true>(A, x, y, b, nullptr, nullptr, nullptr, red, gate, st);
+  else launch_spmv<VT, XT, 0, false>(A, x, y, b, nullptr, nullptr, nullptr, red, gate, st);
+}
+
+template <class VT, class XT>
+void spmv_dot(const DevMat<VT>& A, const XT* x, XT* y, int mode, const XT* b, const XT* d,
+              int nd, const int* sa, const int* sb, const Red& red, const int* gate,
+              cudaStream_t st) {
+  if (nd == 1) {
+    if (mode == SPMV_RES) launch_spmv<VT, XT, 1, true>(A, x, y, b, d, sa, sb, red, gate, st);
+    else launch_spmv<VT, XT, 1, false>(A, x, y, b, d, sa, sb, red, gate, st);
+  } else {
+    if (mode == SPMV_RES) launch_spmv<VT, XT, 2, true>(A, x, y, b, d, sa, sb, red, gate, st);
+    else launch_spmv<VT, XT, 2, false>(A, x, y, b, d, sa, sb, red, gate, st);
+  }
+}
+
+template void spmv<double, double>(const DevMat<double>&, const double*, double*, int,
+                                   const double*, const int*, cudaStream_t);
+template void spmv<float, float>(const DevMat<float>&, const float*, float*, int, const float*,
+                                 const int*, cudaStream_t);
+template void spmv_dot<double, double>(const DevMat<double>&, const double*, double*, int,
+                                       const double*, const double*, int, const int*, const int*,
+                                       const Red&, const int*, cudaStream_t);
+template void spmv_dot<float, float>(const DevMat<float>&, const float*, float*, int,
+                                     const float*, const float*, int, const int*, const int*,
+                                     const Red&, const int*, cudaStream_t);
+
+}  // namespace pb

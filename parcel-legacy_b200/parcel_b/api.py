@@ -1,0 +1,175 @@
+"""Python mirror of PARCEL's solver interface on top of libparcelb.
+
+The functions keep the reference's names and argument meaning:
+
+* ``parcel_dcg``, ``parcel_dbicgstab``, ``parcel_dgmres``, ``parcel_dcagmres`` follow the
+  Fortran wrappers of src/wrapper.f90 (CPU build 1813-2900, GPU build 362-1455) and their C
+  forms in src/example/c2fortran_kernel.f90: CRS 1-based with global column ids, ``vecx``
+  holds x0 on entry and the solution on exit, ``reshistory`` (length ``itrmax``) receives
+  the relative residual history, and the call returns ``(niter, iret)`` with iret 0 =
+  converged, 1 = iteration limit (src/define.f90:101-102) or a negative error code where
+  the reference would stop.  Arrays may be numpy (host memory: the C-ABI copies them to
+  the GPU and back) or CUDA torch tensors (device memory).
+* ``solve`` is PARCEL_KSP_CRS (src/wrapper.f90:47-222) with keyword options named after
+  the fields of KSP_INPUT_PARAM.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import Crs, load, new_input
+
+
+def _ptr(a) -> int:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _check_types(vecx, vecb, crsA, crsRow_ptr, crsCol):
+    for name, a, dt in (("vecx", vecx, "float64"), ("vecb", vecb, "float64"), ("crsA", crsA, "float64"),
+                        ("crsRow_ptr", crsRow_ptr, "int32"), ("crsCol", crsCol, "int32")):
+        got = str(a.dtype).replace("torch.", "")
+        if got != dt:
+            raise TypeError(f"{name} must be {dt}, got {got}")
+
+
+def _i(v):
+    return C.byref(C.c_int(int(v)))
+
+
+def _call_shim(fn, vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU_method,
+               addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag, precon_thblock, Neuman_itr,
+               independ_nvec, nBlock, extra=()):
+    _check_types(vecx, vecb, crsA, crsRow_ptr, crsCol)
+    niter = C.c_int(int(itrmax))
+    iret = C.c_int(0)
+    hist = reshistory if reshistory is not None else np.zeros(int(itrmax))
+    args = [_i(0), _ptr(vecx), _ptr(vecb), C.byref(C.c_int32(n)), C.byref(C.c_int32(gn)),
+            C.byref(C.c_int32(nnz)), C.byref(C.c_int32(istart)), _ptr(crsA), _ptr(crsRow_ptr),
+            _ptr(crsCol), _i(ipreflag), _i(ILU_method), _i(addL), _i(iflagAS), C.byref(niter),
+            C.byref(C.c_double(rtolmax)), _ptr(hist), _i(iovlflag), _i(precon_thblock),
+            _i(Neuman_itr), _i(independ_nvec), _i(nBlock)]
+    args += [_i(e) for e in extra]
+    args += [C.byref(iret)]
+    fn(*args)
+    return niter.value, iret.value
+
+
+def _shim_name(base: str, vecx) -> str:
+    return base + ("_gpu_c_" if hasattr(vecx, "is_cuda") and vecx.is_cuda else "_c_")
+
+
+def _devptr_args(vecx, vecb, crsA, crsRow_ptr, crsCol):
+    """GPU-build ABI: each array is passed as a pointer to its device pointer."""
+    return [C.byref(C.c_void_p(_ptr(a))) for a in (vecx, vecb, crsA, crsRow_ptr, crsCol)]
+
+
+def _dispatch(base, vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU_method,
+              addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag, precon_thblock, Neuman_itr,
+              independ_nvec, nBlock, extra=()):
+    L = load()
+    if hasattr(vecx, "is_cuda") and vecx.is_cuda:
+        _check_types(vecx, vecb, crsA, crsRow_ptr, crsCol)
+        fn = getattr(L, base + "_gpu_c_")
+        niter = C.c_int(int(itrmax))
+        iret = C.c_int(0)
+        hist = reshistory if reshistory is not None else np.zeros(int(itrmax))
+        vx, vb, va, vr, vc = _devptr_args(vecx, vecb, crsA, crsRow_ptr, crsCol)
+        args = [_i(0), vx, vb, C.byref(C.c_int32(n)), C.byref(C.c_int32(gn)), C.byref(C.c_int32(nnz)),
+                C.byref(C.c_int32(istart)), va, vr, vc, _i(ipreflag), _i(ILU_method), _i(addL),
+                _i(iflagAS), C.byref(niter), C.byref(C.c_double(rtolmax)), _ptr(hist), _i(iovlflag),
+                _i(precon_thblock), _i(Neuman_itr), _i(independ_nvec), _i(nBlock)]
+        args += [_i(e) for e in extra] + [C.byref(iret)]
+        fn.argtypes = None
+        fn(*args)
+        return niter.value, iret.value
+    return _call_shim(getattr(L, base + "_c_"), vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr,
+                      crsCol, ipreflag, ILU_method, addL, iflagAS, itrmax, rtolmax, reshistory,
+                      iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, extra)
+
+
+def parcel_dcg(vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU_method, addL,
+               iflagAS, itrmax, rtolmax, reshistory, iovlflag=0, precon_thblock=-1, Neuman_itr=1,
+               independ_nvec=-1, nBlock=2000):
+    """PCG (parcel_dcg, src/wrapper.f90:1995 / :544).  Returns (niter, iret)."""
+    return _dispatch("parcel_dcg", vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag,
+                     ILU_method, addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag, precon_thblock,
+                     Neuman_itr, independ_nvec, nBlock)
+
+
+def parcel_dbicgstab(vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU_method,
+                     addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag=0, precon_thblock=-1,
+                     Neuman_itr=1, independ_nvec=-1, nBlock=2000):
+    """BiCGStab (parcel_dbicgstab, src/wrapper.f90:1813 / :362).  Returns (niter, iret)."""
+    return _dispatch("parcel_dbicgstab", vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol,
+                     ipreflag, ILU_method, addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag,
+                     precon_thblock, Neuman_itr, independ_nvec, nBlock)
+
+
+def parcel_dgmres(vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU_method, addL,
+                  iflagAS, itrmax, rtolmax, reshistory, iovlflag=0, precon_thblock=-1, Neuman_itr=1,
+                  independ_nvec=-1, nBlock=2000, GMRES_m=4, GMRES_GSflag=1):
+    """GMRES(m) (parcel_dgmres, src/wrapper.f90:2179 / :727).  Returns (niter, iret)."""
+    return _dispatch("parcel_dgmres", vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag,
+                     ILU_method, addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag, precon_thblock,
+                     Neuman_itr, independ_nvec, nBlock, extra=(GMRES_m, GMRES_GSflag))
+
+
+def parcel_dcagmres(vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU_method,
+                    addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag=0, precon_thblock=-1,
+                    Neuman_itr=1, independ_nvec=-1, nBlock=2000, CAGMRES_sstep=4, CAGMRES_tstep=1,
+                    CAGMRES_basis=0, CAGMRES_QRflag=4):
+    """CA-GMRES(s,t) (parcel_dcagmres, src/wrapper.f90:2807 / :1355).  Returns (niter, iret)."""
+    return _dispatch("parcel_dcagmres", vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol,
+                     ipreflag, ILU_method, addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag,
+                     precon_thblock, Neuman_itr, independ_nvec, nBlock,
+                     extra=(CAGMRES_sstep, CAGMRES_tstep, CAGMRES_basis, CAGMRES_QRflag))
+
+
+def crs_struct(A, rowptr=None, col=None, val=None) -> Crs:
+    """parcel_b_crs for a problems.CRS (host) or explicit (device) arrays."""
+    rowptr = A.rowptr if rowptr is None else rowptr
+    col = A.col if col is None else col
+    val = A.val if val is None else val
+    return Crs(int(A.n), int(A.n), int(col.shape[0]), int(getattr(A, "istart", 1)), _ptr(rowptr),
+               _ptr(col), _ptr(val))
+
+
+def solve(A, b, x0=None, *, rowptr=None, col=None, val=None, **options):
+    """PARCEL_KSP_CRS: solves A x = b with the options of KSP_INPUT_PARAM given as keywords
+    (solver, ipreflag, ILU_method, precon_thblock, itrmax, rtolmax, GMRES_m, GMRES_GSflag,
+    CAGMRES_*, inner_precision, residual_dd, inner_rtol, max_refine).  Returns a dict with
+    x, reshistory, niter, iret and the library's statistics.  Raises on a negative iret."""
+    L = load()
+    p = new_input(**options)
+    S = crs_struct(A, rowptr, col, val)
+    on_dev = hasattr(b, "is_cuda") and b.is_cuda
+    if x0 is None:
+        if on_dev:
+            import torch
+            x = torch.zeros_like(b)
+        else:
+            x = np.zeros(A.n)
+    else:
+        x = x0.clone() if on_dev else np.array(x0, dtype=np.float64, copy=True)
+    itrmax = p.itrmax if p.itrmax > 0 else 100
+    hist = np.zeros(itrmax)
+    niter, iret = C.c_int(0), C.c_int(0)
+    rc = L.parcel_b_solve(C.byref(p), C.byref(S), _ptr(b), _ptr(x), _ptr(hist), C.byref(niter),
+                          C.byref(iret))
+    if rc < 0:
+        raise RuntimeError(f"parcel_b_solve failed: {_lib.last_error()}")
+    return {"x": x, "reshistory": hist[: niter.value].copy(), "niter": niter.value, "iret": iret.value,
+            "stats": _lib.last_stats()}

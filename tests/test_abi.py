@@ -1,0 +1,58 @@
+"""CPU-side checks of the C-ABI: the library loads and exports every function that
+include/parcel_b.h declares, and the ctypes mirrors of its structs have the C layout."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+from parcel_b import _lib
+
+HEADER = os.path.join(ROOT, "include", "parcel_b.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:[\w\*]+\s+)+\**(\w+)\s*\(", src, flags=re.M)
+    return sorted(set(n for n in names if n.startswith(("parcel", "PARCEL"))))
+
+
+def test_header_declares_the_reference_entry_points():
+    names = declared_functions()
+    for n in ("parcel_dcg_c_", "parcel_dbicgstab_c_", "parcel_dgmres_c_", "parcel_dcagmres_c_",
+              "parcel_init_c_", "parcel_free_c_", "parcel_b_solve"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.load()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_ctypes_signatures_cover_the_header():
+    assert set(declared_functions()) <= set(_lib.SIGNATURES)
+
+
+def test_struct_layouts_match_c(tmp_path):
+    src = tmp_path / "sz.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "parcel_b.h"\n'
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(parcel_b_input), '
+                   'sizeof(parcel_b_stats), sizeof(parcel_b_crs), offsetof(parcel_b_input, rtolmax), '
+                   'offsetof(parcel_b_input, inner_rtol), offsetof(parcel_b_crs, rowptr));return 0;}\n')
+    exe = tmp_path / "sz"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    want = [C.sizeof(_lib.Input), C.sizeof(_lib.Stats), C.sizeof(_lib.Crs), _lib.Input.rtolmax.offset,
+            _lib.Input.inner_rtol.offset, _lib.Crs.rowptr.offset]
+    assert [int(v) for v in out] == want
+
+
+def test_input_defaults_are_minus_one():
+    p = _lib.new_input()
+    for f in ("ipreflag", "ILU_method", "solver", "GMRES_m", "itrmax", "precon_thblock", "independ_nvec"):
+        assert getattr(p, f) == -1
+    assert p.rtolmax == -1.0
