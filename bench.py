@@ -1,0 +1,316 @@
+"""Benchmark: time to a 1e-10 true relative residual for PARCEL's drop-in GMRES path.
+
+Workload (one "step" = one complete solve): 3D 7-point upwind convection-diffusion on a
+128^3 grid (n = 2,097,152, nnz = 14,581,760, CRS int32), -Lap u + Pe v.grad u with
+v = (1, 0.5, 0.25), Pe = 10, h = 1/129; b ~ N(0,1) (seed 2); x0 = 0; GMRES(30) with
+modified Gram-Schmidt (the reference default) and block-Jacobi ILU(0) over 64
+contiguous-row blocks; stop at relative residual 1e-10.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value : device time (CUDA events on the library stream) of the whole solve call
+        (setup + iteration) through the GPU-build C-ABI (parcel_dgmres_gpu_c_) with the
+        matrix and vectors already in HBM.
+e2e   : the same solve through the CPU-build C-ABI (parcel_dgmres_c_) with host arrays,
+        host<->device copies inside the timed region.
+roofline : the CRS SpMV kernel (the metric's "SpMV HBM GB/s"), algorithmic bytes
+        (8+4) nnz + 4 (n+1) + 8 n + 8 n per launch over its CUDA-event time.
+--impl reference : the reference's CPU algorithm (the oracle port of KSP_pGMRES with
+        block-Jacobi ILU(0)) on the host cores, same workload and metric.
+With torchrun (N > 1) every rank solves its own copy of the problem on its GPU (replicas;
+the solve is not split across GPUs), and the slowest rank's time is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "parcel-legacy_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+N_GRID = 128
+NBLOCKS = 64
+GMRES_M = 30
+RTOL = 1e-10
+ITRMAX = 5000
+SEED_B = 2
+METRIC = "time-to-1e-10 true rel. residual (s) vs plain FP64 GPU path; SpMV HBM GB/s"
+WORKLOAD = ("PGMRES(30) FP64, block-Jacobi ILU(0) 64 blocks, 3D 7-pt upwind convection-diffusion "
+            "128^3 (Pe=10, v=(1,0.5,0.25)), b~N(0,1), tol 1e-10")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def problem():
+    from parcel_b import problems
+    A = problems.convdiff3d_upwind(N_GRID)
+    b = problems.rhs_normal(A.n, SEED_B)
+    return A, b
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.strip().split(", ") for l in open(self.f.name) if l.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        load = [s for s in sm if s > 300] or sm
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def dist_setup(ngpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from parcel_b import _lib, api
+    L = _lib.load()
+    A, b = problem()
+    dev = torch.device("cuda", local)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    rp, ci, va, bd = t(A.rowptr), t(A.col), t(A.val), t(b)
+    x = torch.zeros(A.n, dtype=torch.float64, device=dev)
+    hist = np.zeros(ITRMAX)
+    stream = torch.cuda.ExternalStream(L.parcel_b_get_stream(), device=dev)
+
+    def solve_dev():
+        x.zero_()
+        torch.cuda.synchronize()
+        return api.parcel_dgmres(x, bd, A.n, A.n, A.nnz, 1, va, rp, ci, 2, 0, 0, 1, ITRMAX, RTOL, hist,
+                                 precon_thblock=NBLOCKS, GMRES_m=GMRES_M, GMRES_GSflag=1)
+
+    # pinned host copies for the end-to-end arm
+    hp = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    h_rp, h_ci, h_va, h_b = hp(A.rowptr), hp(A.col), hp(A.val), hp(b)
+    h_x = torch.zeros(A.n, dtype=torch.float64).pin_memory().numpy()
+
+    def solve_host():
+        h_x[:] = 0.0
+        return api.parcel_dgmres(h_x, h_b, A.n, A.n, A.nnz, 1, h_va, h_rp, h_ci, 2, 0, 0, 1, ITRMAX, RTOL,
+                                 hist, precon_thblock=NBLOCKS, GMRES_m=GMRES_M, GMRES_GSflag=1)
+
+    for _ in range(args.warmup):
+        niter, iret = solve_dev()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    times, stats = [], []
+    for _ in range(args.steps):
+        x.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        niter, iret = api.parcel_dgmres(x, bd, A.n, A.n, A.nnz, 1, va, rp, ci, 2, 0, 0, 1, ITRMAX, RTOL, hist,
+                                        precon_thblock=NBLOCKS, GMRES_m=GMRES_M, GMRES_GSflag=1)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+        stats.append(_lib.last_stats())
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    step_s = max(times)
+    if dist:
+        tt = torch.tensor([step_s, sum(times)], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        step_s, tot = float(tt[0]), float(tt[1])
+    else:
+        tot = sum(times)
+    value = tot / args.steps
+    relres = stats[-1]["true_relres"]
+
+    # end-to-end: host arrays through the CPU-build ABI, copies inside the timed region
+    solve_host()
+    torch.cuda.synchronize()
+    e2e = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        n2, i2 = solve_host()
+        e2e.append(time.perf_counter() - t0)
+    h2d = A.rowptr.nbytes + A.col.nbytes + A.val.nbytes + 2 * A.n * 8
+    d2h = A.n * 8 + ITRMAX * 8
+
+    # kernel timing for the roofline (CUDA events on the library stream)
+    ms_spmv, ms_pre = C.c_double(0), C.c_double(0)
+    p = _lib.new_input(solver=3, ipreflag=2, ILU_method=0, precon_thblock=NBLOCKS, GMRES_m=GMRES_M)
+    S = api.crs_struct(A, rp, ci, va)
+    rc = L.parcel_b_bench_kernels(C.byref(p), C.byref(S), 50, C.byref(ms_spmv), C.byref(ms_pre))
+    assert rc == 0, _lib.last_error()
+    hbm, peak_kind = peaks()
+    spmv_bytes = 12 * A.nnz + 4 * (A.n + 1) + 16 * A.n
+    achieved = spmv_bytes / (ms_spmv.value * 1e-3) / 1e9
+    ilu_bytes = None
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": A.n, "nnz": A.nnz, "blocks": NBLOCKS, "restart": GMRES_M,
+                   "orthogonalization": "MGS", "l2": "inputs larger than L2 (217 MB matrix, 126 MB L2)",
+                   "parallelism": f"replicas x{world}"},
+        "iterations": niter, "iret": iret, "true_relres": relres,
+        "setup_s": stats[-1]["setup_s"], "solve_s": stats[-1]["solve_s"],
+        "e2e": {"value": sum(e2e) / len(e2e), "unit": "s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "kernel": "k_spmv<8,4,double,double> (CRS SpMV, permuted level layout)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes": int(spmv_bytes),
+                     "us_per_launch": ms_spmv.value * 1e3},
+        "kernels_us": {"spmv": ms_spmv.value * 1e3, "bj_ilu0_apply": ms_pre.value * 1e3},
+        "clocks": clocks,
+        "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(A, b)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def cpu_baseline(A, b):
+    import oracle
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    t0 = time.perf_counter()
+    x, h, niter, iret = oracle.solve(A, b, solver=3, ipreflag=2, ILU_method=0, precon_thblock=NBLOCKS,
+                                     itrmax=ITRMAX, rtolmax=RTOL, GMRES_m=GMRES_M, GMRES_GSflag=1)
+    dt = time.perf_counter() - t0
+    return {"value": dt, "unit": "s", "cores": cores, "kind": "port",
+            "sample": f"one full oracle solve of the same workload ({niter} GMRES iterations, iret {iret})"}
+
+
+def run_reference(args):
+    rank, world, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import oracle
+    A, b = problem()
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    M = oracle.Matrix(A)
+    times = []
+    niter = 0
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        x, h, niter, iret = oracle.solve(M, b, solver=3, ipreflag=2, ILU_method=0, precon_thblock=NBLOCKS,
+                                         itrmax=ITRMAX, rtolmax=RTOL, GMRES_m=GMRES_M, GMRES_GSflag=1)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    value = sum(times) / len(times)
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "n": A.n, "nnz": A.nnz, "blocks": NBLOCKS, "restart": GMRES_M},
+           "iterations": niter,
+           "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port",
+                            "sample": "full solves of the same workload by the C++/OpenMP restatement of "
+                                      "KSP_pGMRES + block-Jacobi ILU(0) (the reference's Fortran cannot be "
+                                      "built here)"},
+           "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def run_kernels_only(args):
+    """Times the SpMV and the block-Jacobi ILU(0) application of the benchmark workload
+    (CUDA events on the library stream), without solving; used for kernel profiles."""
+    import torch
+    from parcel_b import _lib, api
+    L = _lib.load()
+    A, b = problem()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    rp, ci, va = t(A.rowptr), t(A.col), t(A.val)
+    ms_spmv, ms_pre = C.c_double(0), C.c_double(0)
+    p = _lib.new_input(solver=3, ipreflag=2, ILU_method=args.ilu_method, precon_thblock=NBLOCKS,
+                       GMRES_m=GMRES_M)
+    rc = L.parcel_b_bench_kernels(C.byref(p), C.byref(api.crs_struct(A, rp, ci, va)), args.steps,
+                                  C.byref(ms_spmv), C.byref(ms_pre))
+    assert rc == 0, _lib.last_error()
+    spmv_bytes = 12 * A.nnz + 4 * (A.n + 1) + 16 * A.n
+    print(json.dumps({"spmv_us": ms_spmv.value * 1e3, "precon_us": ms_pre.value * 1e3,
+                      "spmv_gbs": spmv_bytes / (ms_spmv.value * 1e-3) / 1e9, "reps": args.steps}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels-only", action="store_true")
+    ap.add_argument("--ilu-method", type=int, default=0)
+    args = ap.parse_args()
+    if args.kernels_only:
+        run_kernels_only(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

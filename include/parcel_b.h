@@ -255,6 +255,13 @@ int parcel_b_dot(int64_t n, const double* x, const double* y, double* out_host);
 int parcel_b_residual_dd(const parcel_b_crs* A, const double* x_hi, const double* x_lo,
                          const double* b_hi, const double* b_lo, double* r_hi, double* r_lo);
 
+/* Kernel timing for benchmarks: builds the solver layout and preconditioner described by
+ * prm (setup excluded from the timing), then launches `reps` back-to-back SpMVs and `reps`
+ * preconditioner applications on the library stream and returns the mean milliseconds per
+ * launch of each, measured with CUDA events on that stream.  Host or device matrix. */
+int parcel_b_bench_kernels(const parcel_b_input* prm, const parcel_b_crs* A, int reps,
+                           double* ms_spmv, double* ms_precon);
+
 #ifdef __cplusplus
 }
 #endif

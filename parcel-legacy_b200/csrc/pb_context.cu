@@ -56,7 +56,7 @@ cudaStream_t stream() { ensure_init(); return g_ctx.stream; }
 
 int num_sms() { ensure_init(); return g_sms; }
 
-int red_blocks() { return 2 * num_sms(); }
+int red_blocks() { return 4 * num_sms(); }
 
 void DBuf::alloc(size_t b) {
   release();

@@ -342,13 +342,14 @@ __global__ void k_ilu_pack(const IluChunk* __restrict__ ch, int nchunks,
     T* valF = dF + C.wpad;
     int* slF = (int*)(valF + (size_t)C.KL * C.wpad);
     T* dB = (T*)(g + kIluHeader);
+    const int zslot = ring ? W * maxWp : -1;   // ring mode: a slot that always holds 0
     T* valB = dB + C.wpad;
     int* slB = (int*)(valB + (size_t)C.KU * C.wpad);
     for (int p = threadIdx.x; p < C.wpad; p += blockDim.x) {
       if (p >= C.w) {
         dF[p] = (T)0; dB[p] = (T)0;
-        for (int k = 0; k < C.KL; ++k) { valF[k * C.wpad + p] = (T)0; slF[k * C.wpad + p] = -1; }
-        for (int k = 0; k < C.KU; ++k) { valB[k * C.wpad + p] = (T)0; slB[k * C.wpad + p] = -1; }
+        for (int k = 0; k < C.KL; ++k) { valF[k * C.wpad + p] = (T)0; slF[k * C.wpad + p] = zslot; }
+        for (int k = 0; k < C.KU; ++k) { valB[k * C.wpad + p] = (T)0; slB[k * C.wpad + p] = zslot; }
         continue;
       }
       int i = rowAt[C.start + p];
@@ -366,7 +367,7 @@ __global__ void k_ilu_pack(const IluChunk* __restrict__ ch, int nchunks,
         valF[k * C.wpad + p] = (T)vL[j];
         slF[k * C.wpad + p] = slot_of(ci[j] - cbase);
       }
-      for (; k < C.KL; ++k) { valF[k * C.wpad + p] = (T)0; slF[k * C.wpad + p] = -1; }
+      for (; k < C.KL; ++k) { valF[k * C.wpad + p] = (T)0; slF[k * C.wpad + p] = zslot; }
       dF[p] = dilu ? (T)Dinv[i] : (T)1;
       // backward: strictly upper in-block entries; ILU(0) increasing column
       // (solve_LU_crs), D-ILU decreasing column (solve_ILU_crs runs Ustart down to Uend)
@@ -384,7 +385,7 @@ __global__ void k_ilu_pack(const IluChunk* __restrict__ ch, int nchunks,
         }
         dB[p] = (T)Dinv[i];
       }
-      for (; k < C.KU; ++k) { valB[k * C.wpad + p] = (T)0; slB[k * C.wpad + p] = -1; }
+      for (; k < C.KU; ++k) { valB[k * C.wpad + p] = (T)0; slB[k * C.wpad + p] = zslot; }
     }
   }
 }
@@ -394,6 +395,7 @@ constexpr int kIluProducerWarps = 1;
 constexpr int kIluConsumerThreads = 256;
 constexpr int kIluThreads = 32 * kIluProducerWarps + kIluConsumerThreads;
 constexpr unsigned kWaitLimit = 1u << 20;   // polls of one mbarrier wait before giving up
+constexpr int kIluKUnroll = 4;            // coupled entries gathered per step
 
 // What the producer needs per chunk, in the order it streams them:
 // {packed offset / 16, first permuted row, packed bytes, vector-slice bytes}.
@@ -515,28 +517,34 @@ __global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve(IluSolveArgs<T> a)
           T* rslot = ring + (size_t)(lvl % a.W) * a.maxWp + off;
           for (int p = ctid; p < w; p += kIluConsumerThreads) {
             T out;
-            if (fwd) {
-              T acc = xin[p];
-              for (int k = 0; k < K; ++k) {
-                int sl = slot[k * wpad + p];
-                if (sl >= 0) acc = acc - val[k * wpad + p] * dep[sl];
+            // Gather the K coupled values first (independent loads), then accumulate in
+            // the reference's order.
+            T dv[kIluKUnroll], av[kIluKUnroll];
+            T acc = (fwd || !DILU) ? xin[p] : T(0);
+            for (int k0 = 0; k0 < K; k0 += kIluKUnroll) {
+#pragma unroll
+              for (int u = 0; u < kIluKUnroll; ++u) {
+                const int k = k0 + u;
+                dv[u] = T(0);
+                av[u] = T(0);
+                if (k < K) {
+                  const int sl = slot[k * wpad + p];
+                  av[u] = val[k * wpad + p];
+                  if (RING || sl >= 0) dv[u] = dep[sl];
+                }
               }
-              out = DILU ? dg[p] * acc : acc;
-            } else if (DILU) {
-              T zz = T(0);
-              for (int k = 0; k < K; ++k) {
-                int sl = slot[k * wpad + p];
-                if (sl >= 0) zz = zz + dep[sl] * val[k * wpad + p];
+#pragma unroll
+              for (int u = 0; u < kIluKUnroll; ++u) {
+                if (k0 + u < K) {
+                  if (fwd) acc = acc - av[u] * dv[u];
+                  else if (DILU) acc = acc + dv[u] * av[u];
+                  else acc = acc - dv[u] * av[u];
+                }
               }
-              out = xin[p] - dg[p] * zz;
-            } else {
-              T acc = xin[p];
-              for (int k = 0; k < K; ++k) {
-                int sl = slot[k * wpad + p];
-                if (sl >= 0) acc = acc - dep[sl] * val[k * wpad + p];
-              }
-              out = acc / dg[p];
             }
+            if (fwd) out = DILU ? dg[p] * acc : acc;
+            else if (DILU) out = xin[p] - dg[p] * acc;
+            else out = acc / dg[p];
             if (RING) rslot[p] = out;
             vout[start + p] = out;
             if (!fwd && a.accum) a.accum[start + p] += out;
@@ -587,10 +595,10 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   int dev_smem = 0;
   PB_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx().device));
   const int budget = std::min(dev_smem, 220 * 1024);
-  int64_t ring_bytes = (int64_t)D.W * D.maxWp * sizeof(T);
+  int64_t ring_bytes = ((int64_t)D.W * D.maxWp + 1) * sizeof(T);
   D.ring = ring_bytes <= 64 * 1024;
   int64_t ring_alloc = D.ring ? ((ring_bytes + 127) & ~int64_t(127)) : 0;
-  int nst = 8;
+  int nst = 16;
   auto need = [&](int k) { return (int64_t)((16 * k + 16 + 127) & ~127) + ring_alloc + (int64_t)k * D.stage_bytes; };
   while (nst > 2 && need(nst) > budget) --nst;
   PB_CHECK(need(nst) <= budget, PARCEL_B_E_UNSUPPORTED,
@@ -693,7 +701,7 @@ void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, 
   a.maxWp = D.maxWp;
   a.stage_bytes = D.stage_bytes;
   a.nstages = D.nstages;
-  a.ring_elems = D.ring ? D.W * D.maxWp : 0;
+  a.ring_elems = D.ring ? D.W * D.maxWp + 1 : 0;
   a.gate = gate;
   a.err = dp<int>(D.err);
   if (D.dilu) {

@@ -31,7 +31,7 @@ int spmv_lanes(int n, int64_t nnz) {
 template <class T> __device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
 
 template <int LPR, int UNR, class VT, class XT, int ND, bool RES>
-__global__ void __launch_bounds__(kRedThreads) k_spmv(int n, const int* __restrict__ rp,
+__global__ void __launch_bounds__(kRedThreads, 4) k_spmv(int n, const int* __restrict__ rp,
                                                       const int* __restrict__ ci,
                                                       const VT* __restrict__ va, int rbase,
                                                       int cbase, const XT* __restrict__ x,

@@ -58,6 +58,7 @@ P = C.c_void_p
 IP = C.POINTER(C.c_int)
 I32P = C.POINTER(C.c_int32)
 DP = C.POINTER(C.c_double)
+PP = C.POINTER(C.c_void_p)
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -77,13 +78,13 @@ SIGNATURES = {
                                 P, IP, IP, IP, IP, IP, IP, IP, IP]),
     "parcel_dcagmres_c_": (None, [IP, P, P, I32P, I32P, I32P, I32P, P, P, P, IP, IP, IP, IP, IP,
                                   DP, P, IP, IP, IP, IP, IP, IP, IP, IP, IP, IP]),
-    "parcel_dcg_gpu_c_": (None, [IP, P, P, I32P, I32P, I32P, I32P, P, P, P, IP, IP, IP, IP, IP, DP,
+    "parcel_dcg_gpu_c_": (None, [IP, PP, PP, I32P, I32P, I32P, I32P, PP, PP, PP, IP, IP, IP, IP, IP, DP,
                                  P, IP, IP, IP, IP, IP, IP]),
-    "parcel_dbicgstab_gpu_c_": (None, [IP, P, P, I32P, I32P, I32P, I32P, P, P, P, IP, IP, IP, IP,
+    "parcel_dbicgstab_gpu_c_": (None, [IP, PP, PP, I32P, I32P, I32P, I32P, PP, PP, PP, IP, IP, IP, IP,
                                        IP, DP, P, IP, IP, IP, IP, IP, IP]),
-    "parcel_dgmres_gpu_c_": (None, [IP, P, P, I32P, I32P, I32P, I32P, P, P, P, IP, IP, IP, IP, IP,
+    "parcel_dgmres_gpu_c_": (None, [IP, PP, PP, I32P, I32P, I32P, I32P, PP, PP, PP, IP, IP, IP, IP, IP,
                                     DP, P, IP, IP, IP, IP, IP, IP, IP, IP]),
-    "parcel_dcagmres_gpu_c_": (None, [IP, P, P, I32P, I32P, I32P, I32P, P, P, P, IP, IP, IP, IP,
+    "parcel_dcagmres_gpu_c_": (None, [IP, PP, PP, I32P, I32P, I32P, I32P, PP, PP, PP, IP, IP, IP, IP,
                                       IP, DP, P, IP, IP, IP, IP, IP, IP, IP, IP, IP, IP]),
     "parcel_b_setup": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.POINTER(P)]),
     "parcel_b_start": (C.c_int, [P, P, P, P, IP, IP]),
@@ -93,6 +94,7 @@ SIGNATURES = {
     "parcel_b_precon_apply": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), P, P]),
     "parcel_b_dot": (C.c_int, [C.c_int64, P, P, DP]),
     "parcel_b_residual_dd": (C.c_int, [C.POINTER(Crs), P, P, P, P, P, P]),
+    "parcel_b_bench_kernels": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, DP, DP]),
 }
 
 _lib = None

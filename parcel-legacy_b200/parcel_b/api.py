@@ -71,11 +71,6 @@ def _shim_name(base: str, vecx) -> str:
     return base + ("_gpu_c_" if hasattr(vecx, "is_cuda") and vecx.is_cuda else "_c_")
 
 
-def _devptr_args(vecx, vecb, crsA, crsRow_ptr, crsCol):
-    """GPU-build ABI: each array is passed as a pointer to its device pointer."""
-    return [C.byref(C.c_void_p(_ptr(a))) for a in (vecx, vecb, crsA, crsRow_ptr, crsCol)]
-
-
 def _dispatch(base, vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU_method,
               addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag, precon_thblock, Neuman_itr,
               independ_nvec, nBlock, extra=()):
@@ -86,13 +81,13 @@ def _dispatch(base, vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ip
         niter = C.c_int(int(itrmax))
         iret = C.c_int(0)
         hist = reshistory if reshistory is not None else np.zeros(int(itrmax))
-        vx, vb, va, vr, vc = _devptr_args(vecx, vecb, crsA, crsRow_ptr, crsCol)
+        keep = [C.c_void_p(_ptr(a)) for a in (vecx, vecb, crsA, crsRow_ptr, crsCol)]
+        vx, vb, va, vr, vc = (C.byref(k) for k in keep)
         args = [_i(0), vx, vb, C.byref(C.c_int32(n)), C.byref(C.c_int32(gn)), C.byref(C.c_int32(nnz)),
                 C.byref(C.c_int32(istart)), va, vr, vc, _i(ipreflag), _i(ILU_method), _i(addL),
                 _i(iflagAS), C.byref(niter), C.byref(C.c_double(rtolmax)), _ptr(hist), _i(iovlflag),
                 _i(precon_thblock), _i(Neuman_itr), _i(independ_nvec), _i(nBlock)]
         args += [_i(e) for e in extra] + [C.byref(iret)]
-        fn.argtypes = None
         fn(*args)
         return niter.value, iret.value
     return _call_shim(getattr(L, base + "_c_"), vecx, vecb, n, gn, nnz, istart, crsA, crsRow_ptr,
