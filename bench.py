@@ -213,7 +213,7 @@ def run_ours(args):
         "setup_s": stats[-1]["setup_s"], "solve_s": stats[-1]["solve_s"],
         "e2e": {"value": sum(e2e) / len(e2e), "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "hbm", "kernel": "k_spmv<8,4,double,double> (CRS SpMV, permuted level layout)",
+        "roofline": {"bound": "hbm", "kernel": "k_spmv_sell<double,double> (sliced-ELLPACK SpMV, level-major layout)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes": int(spmv_bytes),
                      "us_per_launch": ms_spmv.value * 1e3},

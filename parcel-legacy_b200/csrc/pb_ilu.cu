@@ -417,6 +417,176 @@ struct IluSolveArgs {
   int* err;
 };
 
+// Operands of one row of one chunk, staged from shared memory into registers.
+template <class T, int KM>
+struct RowOps {
+  T xin, dg;
+  T val[KM];
+  int slot[KM];
+  int start, w, K, rbase;   // chunk header; rbase = ring offset of the chunk's first row
+};
+
+template <class T, int KM>
+__device__ __forceinline__ void load_ops(RowOps<T, KM>& o, const unsigned char* sp, int ctid, int W,
+                                         int maxWp) {
+  const int* hdr = reinterpret_cast<const int*>(sp);
+  const int4 h0 = *reinterpret_cast<const int4*>(hdr);
+  const int2 h1 = *reinterpret_cast<const int2*>(hdr + 4);
+  o.start = h0.x; o.w = h0.y; o.K = h0.w;
+  const int wpad = h0.z;
+  o.rbase = (h1.x % W) * maxWp + h1.y;
+  const T* dg = reinterpret_cast<const T*>(sp + kIluHeader);
+  const T* val = dg + wpad;
+  const int* slot = reinterpret_cast<const int*>(val + (size_t)o.K * wpad);
+  const T* xin = reinterpret_cast<const T*>(sp + chunk_bytes<T>(wpad, o.K));
+  const int p = ctid;
+  if (p < o.w) {
+    o.xin = xin[p];
+    o.dg = dg[p];
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+      if (k < o.K) { o.val[k] = val[k * wpad + p]; o.slot[k] = slot[k * wpad + p]; }
+    }
+  }
+}
+
+// Ring-mode consumer loop with the next chunk's operands loaded while the current chunk
+// is solved; requires every chunk to have at most kIluConsumerThreads rows and at most
+// KM coupled entries per row.
+template <class T, bool DILU, bool FWD, int KM>
+__device__ __forceinline__ void consume_pipelined(const IluSolveArgs<T>& a, uint64_t* full,
+                                                  uint64_t* empty, volatile int* sflags,
+                                                  unsigned char* stages, T* ring, int nc, int gbase,
+                                                  int ctid, T* vout) {
+  const int NST = a.nstages;
+  RowOps<T, KM> cur, nxt;
+  bool ok = mbar_wait(&full[gbase % NST], (gbase / NST) & 1, kWaitLimit);
+  if (!ok) { atomicExch(a.err, 3); sflags[0] = 1; }
+  else load_ops<T, KM>(cur, stages + (size_t)(gbase % NST) * a.stage_bytes, ctid, a.W, a.maxWp);
+  named_bar_sync(1, kIluConsumerThreads);
+  if (ctid == 0) { if (ok) mbar_arrive(&empty[gbase % NST]); sflags[1] = gbase + 1; }
+  if (sflags[0]) return;
+  for (int i = 0; i < nc; ++i) {
+    const int g1 = gbase + i + 1;
+    bool ok1 = true;
+    if (i + 1 < nc) {
+      ok1 = mbar_wait(&full[g1 % NST], (g1 / NST) & 1, kWaitLimit);
+      if (!ok1) { atomicExch(a.err, 3); sflags[0] = 1; }
+      else load_ops<T, KM>(nxt, stages + (size_t)(g1 % NST) * a.stage_bytes, ctid, a.W, a.maxWp);
+    }
+    if (ctid < cur.w) {
+      T dv[KM];
+#pragma unroll
+      for (int k = 0; k < KM; ++k) dv[k] = (k < cur.K) ? ring[cur.slot[k]] : T(0);
+      T acc = (FWD || !DILU) ? cur.xin : T(0);
+#pragma unroll
+      for (int k = 0; k < KM; ++k) {
+        if (k < cur.K) {
+          if (FWD) acc = acc - cur.val[k] * dv[k];
+          else if (DILU) acc = acc + dv[k] * cur.val[k];
+          else acc = acc - dv[k] * cur.val[k];
+        }
+      }
+      T out;
+      if (FWD) out = DILU ? cur.dg * acc : acc;
+      else if (DILU) out = cur.xin - cur.dg * acc;
+      else out = acc / cur.dg;
+      ring[cur.rbase + ctid] = out;
+      vout[cur.start + ctid] = out;
+      if (!FWD && a.accum) a.accum[cur.start + ctid] += out;
+    }
+    named_bar_sync(1, kIluConsumerThreads);
+    if (ctid == 0 && i + 1 < nc) { if (ok1) mbar_arrive(&empty[g1 % NST]); sflags[1] = g1 + 1; }
+    if (sflags[0]) return;
+    cur = nxt;
+  }
+}
+
+template <class T, bool DILU, int KM>
+__global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve_fast(IluSolveArgs<T> a) {
+  if (gated(a.gate)) return;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int NST = a.nstages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + NST;
+  volatile int* sflags = reinterpret_cast<volatile int*>(empty + NST);
+  T* ring = reinterpret_cast<T*>(smem + ((16 * NST + 16 + 127) & ~127));
+  unsigned char* stages =
+      reinterpret_cast<unsigned char*>(ring) + (((size_t)a.ring_elems * sizeof(T) + 127) & ~size_t(127));
+  const int b = blockIdx.x;
+  const int c0 = a.blk_chunk[b], c1 = a.blk_chunk[b + 1];
+  const int nc = c1 - c0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool producer = warp < kIluProducerWarps;
+  const int ctid = threadIdx.x - 32 * kIluProducerWarps;
+  int issued = 0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NST; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
+    sflags[0] = 0;
+    sflags[1] = 0;
+    mbar_fence_init();
+  }
+  for (int i = threadIdx.x; i < a.ring_elems; i += blockDim.x) ring[i] = T(0);
+  __syncthreads();
+  for (int phase = 0; phase < 2; ++phase) {
+    const bool fwd = phase == 0;
+    const int gbase = phase * nc;
+    if (producer) {
+      const unsigned char* pack = fwd ? a.packF : a.packB;
+      const T* vin = fwd ? a.r : a.y;
+      const ProdDesc* tab = fwd ? a.tabF : a.tabB;
+      auto fetch = [&](int i) -> ProdDesc {
+        if (i >= nc) return ProdDesc{0, 0, 0, 0};
+        return tab[fwd ? c0 + i : c1 - 1 - i];
+      };
+      ProdDesc cur = fetch(lane);
+      for (int i0 = 0; i0 < nc; i0 += 32) {
+        ProdDesc nxt = fetch(i0 + 32 + lane);
+        const int kmax = min(32, nc - i0);
+        bool stop = false;
+        for (int k = 0; k < kmax; ++k) {
+          ProdDesc d;
+          d.off16 = __shfl_sync(kFull, cur.off16, k);
+          d.start = __shfl_sync(kFull, cur.start, k);
+          d.cbytes = __shfl_sync(kFull, cur.cbytes, k);
+          d.vbytes = __shfl_sync(kFull, cur.vbytes, k);
+          if (lane == 0) {
+            const int g = gbase + i0 + k;
+            const int st = g % NST;
+            const int use = g / NST;
+            if (sflags[0]) {
+              stop = true;
+            } else if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1, kWaitLimit)) {
+              atomicExch(a.err, 2);
+              sflags[0] = 1;
+              stop = true;
+            } else {
+              unsigned char* dst = stages + (size_t)st * a.stage_bytes;
+              mbar_arrive_expect_tx(&full[st], (unsigned)(d.cbytes + d.vbytes));
+              bulk_g2s(dst, pack + (size_t)d.off16 * 16, (unsigned)d.cbytes, &full[st]);
+              bulk_g2s(dst + d.cbytes, vin + d.start, (unsigned)d.vbytes, &full[st]);
+              ++issued;
+            }
+          }
+          stop = __shfl_sync(kFull, stop, 0);
+          if (stop) break;
+        }
+        if (stop) break;
+        cur = nxt;
+      }
+    } else if (nc > 0) {
+      if (fwd) consume_pipelined<T, DILU, true, KM>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.y);
+      else consume_pipelined<T, DILU, false, KM>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.s);
+      if (fwd) fence_proxy_async_global();
+    }
+    __syncthreads();
+    if (sflags[0]) break;
+  }
+  if (sflags[0] && threadIdx.x == 0) {
+    for (int g = sflags[1]; g < issued; ++g) mbar_wait(&full[g % NST], (g / NST) & 1, kWaitLimit);
+  }
+}
+
 template <class T, bool DILU, bool RING>
 __global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve(IluSolveArgs<T> a) {
   if (gated(a.gate)) return;
@@ -605,6 +775,12 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
            "block-Jacobi level too wide for shared memory (stage %d bytes)", D.stage_bytes);
   D.nstages = nst;
   D.smem_bytes = (int)need(nst);
+  {
+    int maxw = 0, maxk = 0;
+    for (const auto& c : ch) { maxw = std::max(maxw, c.w); maxk = std::max(maxk, std::max(c.KL, c.KU)); }
+    D.fast_km = 0;
+    if (D.ring && maxw <= kIluConsumerThreads) D.fast_km = maxk <= 4 ? 4 : (maxk <= 8 ? 8 : 0);
+  }
 
   D.chunks.alloc(sizeof(IluChunk) * std::max<size_t>(ch.size(), 1));
   h2d(D.chunks.p, ch.data(), sizeof(IluChunk) * ch.size());
@@ -685,6 +861,17 @@ static void launch_ilu(const IluDev<T>& D, const IluSolveArgs<T>& a, cudaStream_
   kern<<<D.nb, kIluThreads, D.smem_bytes, st>>>(a);
 }
 
+template <class T, bool DILU, int KM>
+static void launch_fast(const IluDev<T>& D, const IluSolveArgs<T>& a, cudaStream_t st) {
+  auto kern = k_ilu_solve_fast<T, DILU, KM>;
+  static bool configured = false;
+  if (!configured) {
+    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    configured = true;
+  }
+  kern<<<D.nb, kIluThreads, D.smem_bytes, st>>>(a);
+}
+
 template <class T>
 void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, cudaStream_t st) {
   IluSolveArgs<T> a;
@@ -704,7 +891,11 @@ void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, 
   a.ring_elems = D.ring ? D.W * D.maxWp + 1 : 0;
   a.gate = gate;
   a.err = dp<int>(D.err);
-  if (D.dilu) {
+  if (D.fast_km == 4) {
+    if (D.dilu) launch_fast<T, true, 4>(D, a, st); else launch_fast<T, false, 4>(D, a, st);
+  } else if (D.fast_km == 8) {
+    if (D.dilu) launch_fast<T, true, 8>(D, a, st); else launch_fast<T, false, 8>(D, a, st);
+  } else if (D.dilu) {
     if (D.ring) launch_ilu<T, true, true>(D, a, st); else launch_ilu<T, true, false>(D, a, st);
   } else {
     if (D.ring) launch_ilu<T, false, true>(D, a, st); else launch_ilu<T, false, false>(D, a, st);

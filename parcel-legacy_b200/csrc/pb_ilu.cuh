@@ -16,7 +16,28 @@ struct DevMat {
   const VT* val = nullptr;
   int rbase = 0;
   int cbase = 0;
+  // Sliced ELLPACK copy (32-row slices, column-major within a slice) used by the SpMV
+  // when present: entry k of row r lives at s_off[r/32] + 32 k + r%32.
+  int nslices = 0;
+  const int* s_off = nullptr;
+  const int* s_w = nullptr;
+  const int* s_col = nullptr;
+  const VT* s_val = nullptr;
 };
+
+template <class VT>
+struct SellBuf {
+  DBuf off, w, col, val;
+};
+
+// Builds the sliced-ELLPACK copy of the natural CRS matrix A in the row order
+// rowAt (permuted position -> natural row, -1 = empty row; null = identity) with columns
+// mapped through pos (natural -> permuted; null = identity).  row_len holds the host-side
+// length of every natural row.  Fills M's SELL fields.
+template <class VT>
+void build_sell(const DevMat<double>& A, int np, const std::vector<int>& rowAt_h,
+                const int* rowAt_d, const int* pos_d, const std::vector<int>& row_len,
+                SellBuf<VT>& buf, DevMat<VT>& M);
 
 // One chunk = up to kIluChunk rows of one wavefront level of one block.
 struct IluChunk {
@@ -58,6 +79,7 @@ struct IluDev {
   int W = 1, maxWp = 0;
   bool ring = true;
   bool dilu = false;
+  int fast_km = 0;  // >0: pipelined ring-mode sweep with at most fast_km couplings per row
   int stage_bytes = 0, nstages = 0, smem_bytes = 0;
   DBuf chunks;      // IluChunk[]
   DBuf tabF, tabB;  // per-chunk producer descriptors

@@ -16,6 +16,7 @@
 #include <chrono>
 #include <type_traits>
 
+#include "pb_mgs.cuh"
 #include "pb_solvers.cuh"
 
 namespace pb {
@@ -48,6 +49,7 @@ Options resolve_options(const parcel_b_input* p) {
   if (p->max_refine > 0) o.max_refine = p->max_refine;
   if (p->independ_nvec > 0) o.independ_nvec = p->independ_nvec;
   if (p->reserved[0] == 1) o.use_graphs = false;
+  if (p->reserved[1] == 1) o.fused_mgs = false;
   return o;
 }
 
@@ -153,8 +155,13 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
     h2d(S.pos.p, P.pos.data(), sizeof(int) * A.n);
     h2d(S.lev.p, P.lev.data(), sizeof(int) * A.n);
     h2d(S.rowAt.p, P.rowAt.data(), sizeof(int) * P.np);
-    ilu_permute_matrix<T>(P, S.Anat, dp<int>(S.pos), dp<int>(S.rowAt), S.Ap, A.nnz);
-    S.A = S.Ap.view(P.np, A.nnz);
+    {
+      std::vector<int> len(A.n);
+      for (int i = 0; i < A.n; ++i) len[i] = hrpp[i + 1] - hrpp[i];
+      S.A = DevMat<T>{};
+      S.A.nnz = A.nnz;
+      build_sell<T>(S.Anat, P.np, P.rowAt, dp<int>(S.rowAt), dp<int>(S.pos), len, S.Asell, S.A);
+    }
     ilu_setup_device<T>(P, S.Anat, o.ilu_method, dp<int>(S.pos), dp<int>(S.rowAt),
                         dp<int>(S.lev), S.M.ilu);
   } else {
@@ -167,6 +174,15 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
       convert<T, double>(A.nnz, dp<T>(S.Aval_T), va, st);
       S.A.n = A.n; S.A.nnz = A.nnz; S.A.rowptr = rp; S.A.col = ci;
       S.A.val = dp<T>(S.Aval_T); S.A.rbase = 1; S.A.cbase = A.istart;
+    }
+    {
+      std::vector<int> hrp(A.n + 1), len(A.n);
+      if (dev) d2h(hrp.data(), A.rowptr, sizeof(int) * (A.n + 1));
+      else memcpy(hrp.data(), A.rowptr, sizeof(int) * (A.n + 1));
+      for (int i = 0; i < A.n; ++i) len[i] = hrp[i + 1] - hrp[i];
+      DevMat<T> M = S.A;
+      build_sell<T>(S.Anat, A.n, std::vector<int>(), nullptr, nullptr, len, S.Asell, M);
+      S.A = M;
     }
     if (o.precon == PARCEL_B_PRECON_POINTJACOBI) {
       S.M.dinv.alloc(sizeof(T) * A.n);
@@ -389,9 +405,18 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
                    rr, nullptr, st);
     launches += 1;
   }
+  // Fused one-launch MGS (pb_mgs.cu) when the vector fits its register tiling.
+  const bool fused_mgs = o.gs != PARCEL_B_GS_CGS && o.fused_mgs && mgs_supported<T>(np);
+  DBuf mparts(sizeof(double) * 2 * (size_t)std::max(1, mgs_grid<T>())),
+      mctr(sizeof(unsigned) * (size_t)m * (m + 2)), merr(sizeof(int));
+  PB_CUDA(cudaMemsetAsync(merr.p, 0, sizeof(int), st));
   int per_cycle = 0;
   auto cycle = [&] {
     per_cycle = 0;
+    if (fused_mgs) {
+      PB_CUDA(cudaMemsetAsync(mctr.p, 0, sizeof(unsigned) * (size_t)m * (m + 2), st));
+      ++per_cycle;
+    }
     int sa[2] = {0, 0}, sb[2] = {0, 0};
     spmv_dot<T, T>(S.A, x, R, SPMV_RES, b, nullptr, 1, sa, sb, red(EPI_GM_RESTART), gdone, st);
     ++per_cycle;
@@ -409,6 +434,18 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
         cgs_update<T>(np, j, Wv, V, ldv, dp<double>(hb) + (size_t)(j - 1) * (m + 1), red(EPI_GM_NORM, 0, j),
                       gskip, st);
         per_cycle += 3;
+      } else if (fused_mgs) {
+        spmv<T, T>(S.A, PV, Wv, SPMV_Y, nullptr, gskip, st);
+        MgsArgs<T> ma;
+        ma.np = np; ma.j = j; ma.w = Wv; ma.V = V; ma.ldv = ldv;
+        ma.vnext = (j < m) ? V + (size_t)j * ldv : nullptr;
+        ma.parts = dp<double>(mparts);
+        ma.ctr = dp<unsigned>(mctr) + (size_t)(j - 1) * (m + 2);
+        ma.err = dp<int>(merr);
+        ma.gate = gskip;
+        ma.red = red(EPI_GM_NORM, 0, j);
+        mgs_column<T>(ma, st);
+        per_cycle += 2;
       } else {
         int sa1[2] = {0, 0}, sb1[2] = {2, 0};   // <w, v_1>
         spmv_dot<T, T>(S.A, PV, Wv, SPMV_Y, nullptr, V, 1, sa1, sb1, red(EPI_GM_H, 1, j), gskip, st);
@@ -424,7 +461,7 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
           ++per_cycle;
         }
       }
-      if (j < m) {
+      if (j < m && !(fused_mgs && o.gs != PARCEL_B_GS_CGS)) {
         lincomb<T>(np, V + (size_t)j * ldv, Wv, cdev(&K->tmp[2]), nullptr, cimm(0), nullptr, cimm(0), gskip, st);
         ++per_cycle;
       }
@@ -445,6 +482,9 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
     launches += per_cycle;
   }
   KState h = read_state(K);
+  int merr_h = 0;
+  d2h(&merr_h, merr.p, sizeof(int));
+  PB_CHECK(merr_h == 0, PARCEL_B_E_CUDA, "MGS grid barrier timed out");
   SolveOut out;
   out.niter = h.niter;
   out.iret = h.iret;

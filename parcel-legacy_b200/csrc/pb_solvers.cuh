@@ -28,6 +28,7 @@ struct Options {
   int max_refine = 50;
   int independ_nvec = 1;
   bool use_graphs = true;
+  bool fused_mgs = true;
 };
 
 Options resolve_options(const parcel_b_input* p);
@@ -52,6 +53,7 @@ struct System {
   DevMat<double> Anat;  // natural matrix (reference layout)
   DBuf up_rowptr, up_col, up_val;   // uploaded copies of host inputs
   PermMat<T> Ap;        // permuted matrix (block Jacobi)
+  SellBuf<T> Asell;     // sliced-ELLPACK copy used by the SpMV
   DevMat<T> A;          // matrix of the iteration
   DBuf Aval_T;          // natural values cast to T (FP32 path, no permutation)
   DBuf pos, rowAt, lev; // layout maps (block Jacobi)

@@ -108,6 +108,59 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_spmv(int n, const int* __res
   if constexpr (ND > 0) reduce_and_finish<ND>(acc, red);
 }
 
+// Sliced-ELLPACK SpMV: one thread per row, all of a row's value/column loads issued
+// before its x gathers.
+template <class VT, class XT, int ND, bool RES>
+__global__ void __launch_bounds__(kRedThreads, 4) k_spmv_sell(int n, int nslices, const int* __restrict__ soff,
+                                                           const int* __restrict__ sw,
+                                                           const int* __restrict__ ci,
+                                                           const VT* __restrict__ va,
+                                                           const XT* __restrict__ x, XT* __restrict__ y,
+                                                           const XT* __restrict__ b, const XT* __restrict__ d,
+                                                           int sa0, int sb0, int sa1, int sb1, Red red,
+                                                           const int* gate) {
+  if (gated(gate)) return;
+  constexpr int U = 8;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double acc[ND > 0 ? ND : 1];
+#pragma unroll
+  for (int k = 0; k < (ND > 0 ? ND : 1); ++k) acc[k] = 0.0;
+  for (int s = warp; s < nslices; s += nwarps) {
+    const int off = __ldg(soff + s) + lane;
+    const int w = __ldg(sw + s);
+    const int row = s * 32 + lane;
+    XT sum = XT(0);
+    for (int k0 = 0; k0 < w; k0 += U) {
+      VT v[U];
+      int c[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (k0 + u < w) {
+          v[u] = __ldcs(va + off + (k0 + u) * 32);
+          c[u] = __ldcs(ci + off + (k0 + u) * 32);
+        } else {
+          v[u] = VT(0);
+          c[u] = row < n ? row : 0;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) sum += (XT)v[u] * __ldg(x + c[u]);
+    }
+    if (row < n) {
+      XT yv = RES ? b[row] - sum : sum;
+      y[row] = yv;
+      if constexpr (ND > 0) {
+        XT src[3] = {yv, x[row], d ? d[row] : XT(0)};
+        acc[0] += (double)(src[sa0] * src[sb0]);
+        if (ND > 1) acc[ND > 1 ? 1 : 0] += (double)(src[sa1] * src[sb1]);
+      }
+    }
+  }
+  if constexpr (ND > 0) reduce_and_finish<ND>(acc, red);
+}
+
 template <class VT, class XT, int ND, bool RES>
 static void launch_spmv(const DevMat<VT>& A, const XT* x, XT* y, const XT* b, const XT* d,
                         const int* sa, const int* sb, const Red& red, const int* gate,
@@ -115,6 +168,13 @@ static void launch_spmv(const DevMat<VT>& A, const XT* x, XT* y, const XT* b, co
   const int lpr = spmv_lanes(A.n, A.nnz);
   const int grid = red_blocks();
   int a0 = sa ? sa[0] : 0, b0 = sb ? sb[0] : 0, a1 = sa ? sa[1] : 0, b1 = sb ? sb[1] : 0;
+  if (A.s_val) {
+    k_spmv_sell<VT, XT, ND, RES><<<grid, kRedThreads, 0, st>>>(A.n, A.nslices, A.s_off, A.s_w, A.s_col,
+                                                              A.s_val, x, y, b, d, a0, b0, a1, b1, red,
+                                                              gate);
+    PB_CUDA(cudaGetLastError());
+    return;
+  }
 #define L(LPR_, UNR_)                                                                         \
   k_spmv<LPR_, UNR_, VT, XT, ND, RES><<<grid, kRedThreads, 0, st>>>(                          \
       A.n, A.rowptr, A.col, A.val, A.rbase, A.cbase, x, y, b, d, a0, b0, a1, b1, red, gate)
@@ -149,6 +209,74 @@ void spmv_dot(const DevMat<VT>& A, const XT* x, XT* y, int mode, const XT* b, co
     else launch_spmv<VT, XT, 2, false>(A, x, y, b, d, sa, sb, red, gate, st);
   }
 }
+
+template <class VT>
+__global__ void k_fill_sell(int np, const int* __restrict__ rowAt, const int* __restrict__ pos,
+                            const int* __restrict__ rp, const int* __restrict__ ci,
+                            const double* __restrict__ va, int rbase, int cbase,
+                            const int* __restrict__ soff, const int* __restrict__ sw,
+                            int* __restrict__ scol, VT* __restrict__ sval) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ((np + 31) & ~31); q += gridDim.x * blockDim.x) {
+    const int s = q >> 5, lane = q & 31;
+    const int w = sw[s];
+    const int base = soff[s] + lane;
+    int i = (q < np) ? (rowAt ? rowAt[q] : q) : -1;
+    int a = 0, len = 0;
+    if (i >= 0) { a = rp[i] - rbase; len = rp[i + 1] - rbase - a; }
+    const int self = q < np ? q : 0;
+    for (int k = 0; k < w; ++k) {
+      if (k < len) {
+        const int c = ci[a + k] - cbase;
+        scol[base + 32 * k] = pos ? pos[c] : c;
+        sval[base + 32 * k] = (VT)va[a + k];
+      } else {
+        scol[base + 32 * k] = self;
+        sval[base + 32 * k] = VT(0);
+      }
+    }
+  }
+}
+
+template <class VT>
+void build_sell(const DevMat<double>& A, int np, const std::vector<int>& rowAt_h, const int* rowAt_d,
+                const int* pos_d, const std::vector<int>& row_len, SellBuf<VT>& buf, DevMat<VT>& M) {
+  const int ns = (np + 31) / 32;
+  std::vector<int> off(ns + 1, 0), w(ns, 0);
+  for (int s = 0; s < ns; ++s) {
+    int mx = 0;
+    for (int l = 0; l < 32; ++l) {
+      const int q = s * 32 + l;
+      if (q >= np) break;
+      const int i = rowAt_h.empty() ? q : rowAt_h[q];
+      if (i >= 0) mx = std::max(mx, row_len[i]);
+    }
+    w[s] = mx;
+    PB_CHECK((int64_t)off[s] + 32LL * mx < INT32_MAX, PARCEL_B_E_UNSUPPORTED, "matrix too large for int32 SELL");
+    off[s + 1] = off[s] + 32 * mx;
+  }
+  const int64_t total = std::max(off[ns], 1);
+  buf.off.alloc(sizeof(int) * (ns + 1));
+  buf.w.alloc(sizeof(int) * std::max(ns, 1));
+  buf.col.alloc(sizeof(int) * total);
+  buf.val.alloc(sizeof(VT) * total);
+  h2d(buf.off.p, off.data(), sizeof(int) * (ns + 1));
+  h2d(buf.w.p, w.data(), sizeof(int) * ns);
+  k_fill_sell<VT><<<8 * num_sms(), 256, 0, stream()>>>(np, rowAt_d, pos_d, A.rowptr, A.col, A.val, A.rbase,
+                                                       A.cbase, dp<int>(buf.off), dp<int>(buf.w),
+                                                       dp<int>(buf.col), dp<VT>(buf.val));
+  PB_CUDA(cudaGetLastError());
+  M.nslices = ns;
+  M.s_off = dp<int>(buf.off);
+  M.s_w = dp<int>(buf.w);
+  M.s_col = dp<int>(buf.col);
+  M.s_val = dp<VT>(buf.val);
+  M.n = np;
+}
+
+template void build_sell<double>(const DevMat<double>&, int, const std::vector<int>&, const int*, const int*,
+                                 const std::vector<int>&, SellBuf<double>&, DevMat<double>&);
+template void build_sell<float>(const DevMat<double>&, int, const std::vector<int>&, const int*, const int*,
+                                const std::vector<int>&, SellBuf<float>&, DevMat<float>&);
 
 template void spmv<double, double>(const DevMat<double>&, const double*, double*, int,
                                    const double*, const int*, cudaStream_t);
