@@ -305,7 +305,8 @@ __global__ void k_dilu_diag(const IluChunk* __restrict__ ch, const int* __restri
 // ------------------------------------------------------------------ packing
 // Packed chunk layout (bytes, every section 16-byte aligned):
 //   header int[8] = {start, w, wpad, K, lvl, off_in_level, 0, 0}
-//   diag   T[wpad]          forward: 1 (ILU(0)) or D^-1 (D-ILU); backward: U_kk or D^-1
+//   header int[6] = ring offset of the chunk's first row: (lvl % W) * maxWp + off_in_level
+//   diag   T[wpad]          forward: 1 (ILU(0)) or D^-1 (D-ILU); backward: 1/U_kk or D^-1
 //   val    T[K * wpad]      entry k of row p at k*wpad + p
 //   slot   int[K * wpad]    ring slot (or permuted position) of the coupled row, -1 = none
 template <class T>
@@ -334,9 +335,9 @@ __global__ void k_ilu_pack(const IluChunk* __restrict__ ch, int nchunks,
       int* hf = (int*)f;
       int* hb = (int*)g;
       hf[0] = C.start; hf[1] = C.w; hf[2] = C.wpad; hf[3] = C.KL; hf[4] = C.lvl;
-      hf[5] = C.off_in_level; hf[6] = 0; hf[7] = 0;
+      hf[5] = C.off_in_level; hf[6] = (C.lvl % W) * maxWp + C.off_in_level; hf[7] = 0;
       hb[0] = C.start; hb[1] = C.w; hb[2] = C.wpad; hb[3] = C.KU; hb[4] = C.lvl;
-      hb[5] = C.off_in_level; hb[6] = 0; hb[7] = 0;
+      hb[5] = C.off_in_level; hb[6] = (C.lvl % W) * maxWp + C.off_in_level; hb[7] = 0;
     }
     T* dF = (T*)(f + kIluHeader);
     T* valF = dF + C.wpad;
@@ -377,7 +378,7 @@ __global__ void k_ilu_pack(const IluChunk* __restrict__ ch, int nchunks,
           valB[k * C.wpad + p] = (T)vU[j];
           slB[k * C.wpad + p] = slot_of(ci[j] - cbase);
         }
-        dB[p] = (T)vU[idg];
+        dB[p] = (T)(1.0 / vU[idg]);   // reciprocal of U_kk: the sweep multiplies
       } else {
         for (int j = iz - 1; j > idg; --j, ++k) {
           valB[k * C.wpad + p] = (T)vU[j];
@@ -417,89 +418,107 @@ struct IluSolveArgs {
   int* err;
 };
 
-// Operands of one row of one chunk, staged from shared memory into registers.
+// Operands of one row of one chunk, staged from shared memory into registers.  Every
+// chunk of a sweep carries exactly KM coupled entries per row (shorter rows are padded
+// with the ring's zero slot), so the loops below have compile-time trip counts.
 template <class T, int KM>
 struct RowOps {
   T xin, dg;
   T val[KM];
   int slot[KM];
-  int start, w, K, rbase;   // chunk header; rbase = ring offset of the chunk's first row
+  int start, w, rbase;
 };
 
 template <class T, int KM>
-__device__ __forceinline__ void load_ops(RowOps<T, KM>& o, const unsigned char* sp, int ctid, int W,
-                                         int maxWp) {
-  const int* hdr = reinterpret_cast<const int*>(sp);
-  const int4 h0 = *reinterpret_cast<const int4*>(hdr);
-  const int2 h1 = *reinterpret_cast<const int2*>(hdr + 4);
-  o.start = h0.x; o.w = h0.y; o.K = h0.w;
+__device__ __forceinline__ void load_ops(RowOps<T, KM>& o, const unsigned char* sp, int p) {
+  const int4 h0 = *reinterpret_cast<const int4*>(sp);
+  const int rb = *reinterpret_cast<const int*>(sp + 24);
+  o.start = h0.x;
+  o.w = h0.y;
+  o.rbase = rb;
   const int wpad = h0.z;
-  o.rbase = (h1.x % W) * maxWp + h1.y;
   const T* dg = reinterpret_cast<const T*>(sp + kIluHeader);
   const T* val = dg + wpad;
-  const int* slot = reinterpret_cast<const int*>(val + (size_t)o.K * wpad);
-  const T* xin = reinterpret_cast<const T*>(sp + chunk_bytes<T>(wpad, o.K));
-  const int p = ctid;
+  const int* slot = reinterpret_cast<const int*>(val + KM * wpad);
+  const T* xin = reinterpret_cast<const T*>(slot + KM * wpad);
   if (p < o.w) {
     o.xin = xin[p];
     o.dg = dg[p];
 #pragma unroll
-    for (int k = 0; k < KM; ++k) {
-      if (k < o.K) { o.val[k] = val[k * wpad + p]; o.slot[k] = slot[k * wpad + p]; }
-    }
+    for (int k = 0; k < KM; ++k) { o.val[k] = val[k * wpad + p]; o.slot[k] = slot[k * wpad + p]; }
   }
 }
 
-// Ring-mode consumer loop with the next chunk's operands loaded while the current chunk
-// is solved; requires every chunk to have at most kIluConsumerThreads rows and at most
-// KM coupled entries per row.
+template <class T, bool DILU, bool FWD, int KM>
+__device__ __forceinline__ void solve_rows(const RowOps<T, KM>& c, const T* ring, T* ringw, T* vout,
+                                           T* accum, int p) {
+  if (p >= c.w) return;
+  T dv[KM];
+#pragma unroll
+  for (int k = 0; k < KM; ++k) dv[k] = ring[c.slot[k]];
+  T acc = (FWD || !DILU) ? c.xin : T(0);
+#pragma unroll
+  for (int k = 0; k < KM; ++k) {
+    if (FWD) acc = acc - c.val[k] * dv[k];
+    else if (DILU) acc = acc + dv[k] * c.val[k];
+    else acc = acc - dv[k] * c.val[k];
+  }
+  T out;
+  if (FWD) out = DILU ? c.dg * acc : acc;
+  else if (DILU) out = c.xin - c.dg * acc;
+  else out = acc * c.dg;
+  ringw[c.rbase + p] = out;
+  vout[c.start + p] = out;
+  if (!FWD && accum) accum[c.start + p] += out;
+}
+
+// Ring-mode consumer loop: chunk i+1's operands are loaded from its stage while chunk i
+// is solved, so after each level barrier only the ring gathers, the multiply-add chain
+// and the stores remain on the critical path.  Two register sets alternate.
 template <class T, bool DILU, bool FWD, int KM>
 __device__ __forceinline__ void consume_pipelined(const IluSolveArgs<T>& a, uint64_t* full,
                                                   uint64_t* empty, volatile int* sflags,
                                                   unsigned char* stages, T* ring, int nc, int gbase,
                                                   int ctid, T* vout) {
   const int NST = a.nstages;
-  RowOps<T, KM> cur, nxt;
-  bool ok = mbar_wait(&full[gbase % NST], (gbase / NST) & 1, kWaitLimit);
-  if (!ok) { atomicExch(a.err, 3); sflags[0] = 1; }
-  else load_ops<T, KM>(cur, stages + (size_t)(gbase % NST) * a.stage_bytes, ctid, a.W, a.maxWp);
+  RowOps<T, KM> A, B;
+  int done = 0;
+  auto wait_load = [&](RowOps<T, KM>& o, int g) -> bool {
+    const int st = g % NST;
+    if (!mbar_wait(&full[st], (g / NST) & 1, kWaitLimit)) {
+      atomicExch(a.err, 3);
+      sflags[0] = 1;
+      return false;
+    }
+    load_ops<T, KM>(o, stages + (size_t)st * a.stage_bytes, ctid);
+    return true;
+  };
+  auto release = [&](bool ok, int g) {
+    if (ctid == 0 && ok) mbar_arrive(&empty[g % NST]);
+  };
+  bool ok = wait_load(A, gbase);
   named_bar_sync(1, kIluConsumerThreads);
-  if (ctid == 0) { if (ok) mbar_arrive(&empty[gbase % NST]); sflags[1] = gbase + 1; }
-  if (sflags[0]) return;
-  for (int i = 0; i < nc; ++i) {
-    const int g1 = gbase + i + 1;
-    bool ok1 = true;
-    if (i + 1 < nc) {
-      ok1 = mbar_wait(&full[g1 % NST], (g1 / NST) & 1, kWaitLimit);
-      if (!ok1) { atomicExch(a.err, 3); sflags[0] = 1; }
-      else load_ops<T, KM>(nxt, stages + (size_t)(g1 % NST) * a.stage_bytes, ctid, a.W, a.maxWp);
+  release(ok, gbase);
+  done = 1;
+  if (!sflags[0]) {
+    for (int i = 0; i < nc; i += 2) {
+      // chunk i in A, prefetch i+1 into B
+      bool okB = true;
+      if (i + 1 < nc) okB = wait_load(B, gbase + i + 1);
+      solve_rows<T, DILU, FWD, KM>(A, ring, ring, vout, a.accum, ctid);
+      named_bar_sync(1, kIluConsumerThreads);
+      if (i + 1 >= nc || sflags[0]) { done = i + 1; break; }
+      release(okB, gbase + i + 1);
+      // chunk i+1 in B, prefetch i+2 into A
+      bool okA = true;
+      if (i + 2 < nc) okA = wait_load(A, gbase + i + 2);
+      solve_rows<T, DILU, FWD, KM>(B, ring, ring, vout, a.accum, ctid);
+      named_bar_sync(1, kIluConsumerThreads);
+      if (i + 2 >= nc || sflags[0]) { done = i + 2; break; }
+      release(okA, gbase + i + 2);
     }
-    if (ctid < cur.w) {
-      T dv[KM];
-#pragma unroll
-      for (int k = 0; k < KM; ++k) dv[k] = (k < cur.K) ? ring[cur.slot[k]] : T(0);
-      T acc = (FWD || !DILU) ? cur.xin : T(0);
-#pragma unroll
-      for (int k = 0; k < KM; ++k) {
-        if (k < cur.K) {
-          if (FWD) acc = acc - cur.val[k] * dv[k];
-          else if (DILU) acc = acc + dv[k] * cur.val[k];
-          else acc = acc - dv[k] * cur.val[k];
-        }
-      }
-      T out;
-      if (FWD) out = DILU ? cur.dg * acc : acc;
-      else if (DILU) out = cur.xin - cur.dg * acc;
-      else out = acc / cur.dg;
-      ring[cur.rbase + ctid] = out;
-      vout[cur.start + ctid] = out;
-      if (!FWD && a.accum) a.accum[cur.start + ctid] += out;
-    }
-    named_bar_sync(1, kIluConsumerThreads);
-    if (ctid == 0 && i + 1 < nc) { if (ok1) mbar_arrive(&empty[g1 % NST]); sflags[1] = g1 + 1; }
-    if (sflags[0]) return;
-    cur = nxt;
   }
+  if (ctid == 0) sflags[1] = gbase + done;
 }
 
 template <class T, bool DILU, int KM>
@@ -714,7 +733,7 @@ __global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve(IluSolveArgs<T> a)
             }
             if (fwd) out = DILU ? dg[p] * acc : acc;
             else if (DILU) out = xin[p] - dg[p] * acc;
-            else out = acc / dg[p];
+            else out = acc * dg[p];
             if (RING) rslot[p] = out;
             vout[start + p] = out;
             if (!fwd && a.accum) a.accum[start + p] += out;
@@ -748,8 +767,15 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   D.dilu = ilu_method != 0;
   D.W = P.W;
   D.maxWp = std::max(4, P.maxWp);
-  // chunk byte offsets for this value type
+  // chunk byte offsets for this value type; every chunk carries the same number of
+  // coupled entries per row (the matrix-wide maximum, rounded up to a supported count)
   std::vector<IluChunk> ch = P.chunks;
+  int kmax = 0;
+  for (const auto& c : ch) kmax = std::max(kmax, std::max(c.KL, c.KU));
+  int kuni = kmax;
+  for (int c : {1, 2, 3, 4, 6, 8})
+    if (kmax <= c) { kuni = c; break; }
+  for (auto& c : ch) { c.KL = kuni; c.KU = kuni; }
   int64_t oF = 0, oB = 0;
   int64_t max_stage = 0;
   for (auto& c : ch) {
@@ -776,10 +802,9 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   D.nstages = nst;
   D.smem_bytes = (int)need(nst);
   {
-    int maxw = 0, maxk = 0;
-    for (const auto& c : ch) { maxw = std::max(maxw, c.w); maxk = std::max(maxk, std::max(c.KL, c.KU)); }
-    D.fast_km = 0;
-    if (D.ring && maxw <= kIluConsumerThreads) D.fast_km = maxk <= 4 ? 4 : (maxk <= 8 ? 8 : 0);
+    int maxw = 0;
+    for (const auto& c : ch) maxw = std::max(maxw, c.w);
+    D.fast_km = (D.ring && maxw <= kIluConsumerThreads && kuni <= 8) ? kuni : 0;
   }
 
   D.chunks.alloc(sizeof(IluChunk) * std::max<size_t>(ch.size(), 1));
@@ -891,10 +916,15 @@ void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, 
   a.ring_elems = D.ring ? D.W * D.maxWp + 1 : 0;
   a.gate = gate;
   a.err = dp<int>(D.err);
-  if (D.fast_km == 4) {
-    if (D.dilu) launch_fast<T, true, 4>(D, a, st); else launch_fast<T, false, 4>(D, a, st);
-  } else if (D.fast_km == 8) {
-    if (D.dilu) launch_fast<T, true, 8>(D, a, st); else launch_fast<T, false, 8>(D, a, st);
+#define FAST(KM_)                                                                 \
+  case KM_:                                                                       \
+    if (D.dilu) launch_fast<T, true, KM_>(D, a, st); else launch_fast<T, false, KM_>(D, a, st); \
+    break;
+  if (D.fast_km > 0) {
+    switch (D.fast_km) {
+      FAST(1) FAST(2) FAST(3) FAST(4) FAST(6) FAST(8)
+      default: PB_CHECK(false, PARCEL_B_E_ARG, "unsupported coupling count %d", D.fast_km);
+    }
   } else if (D.dilu) {
     if (D.ring) launch_ilu<T, true, true>(D, a, st); else launch_ilu<T, true, false>(D, a, st);
   } else {
