@@ -210,6 +210,7 @@ def run_ours(args):
                    "orthogonalization": "MGS", "l2": "inputs larger than L2 (217 MB matrix, 126 MB L2)",
                    "parallelism": f"replicas x{world}"},
         "iterations": niter, "iret": iret, "true_relres": relres,
+        "step_times_s": [round(t_, 6) for t_ in times],
         "setup_s": stats[-1]["setup_s"], "solve_s": stats[-1]["solve_s"],
         "e2e": {"value": sum(e2e) / len(e2e), "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},

@@ -57,6 +57,10 @@ def lib():
         L.orc_true_relres.argtypes = [C.POINTER(OrcMat), C.c_void_p, C.c_void_p]
         L.orc_true_relres.restype = C.c_double
         L.orc_num_threads.restype = C.c_int
+        L.orc_precon_create.argtypes = [C.POINTER(OrcMat), C.POINTER(OrcParams), C.POINTER(C.c_int)]
+        L.orc_precon_create.restype = C.c_void_p
+        L.orc_precon_apply_h.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_precon_destroy.argtypes = [C.c_void_p]
         L.orc_set_threads.argtypes = [C.c_int]
         _lib = L
     return _lib
@@ -131,3 +135,26 @@ def set_threads(t: int) -> None:
 
 def num_threads() -> int:
     return lib().orc_num_threads()
+
+
+class Precon:
+    """Persistent oracle preconditioner (setup once, apply many times)."""
+
+    def __init__(self, M: "Matrix", **kw):
+        self.M = M
+        self.p = params(**kw)
+        err = C.c_int(0)
+        self.h = lib().orc_precon_create(C.byref(M.s), C.byref(self.p), C.byref(err))
+        if not self.h:
+            raise RuntimeError(f"oracle preconditioner setup failed: {err.value}")
+
+    def __call__(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        s = np.empty_like(r)
+        lib().orc_precon_apply_h(self.h, _ptr(r), _ptr(s))
+        return s
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_precon_destroy(self.h)
+            self.h = None

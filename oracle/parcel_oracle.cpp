@@ -649,4 +649,19 @@ double orc_true_relres(const OrcMat* A, const double* b, const double* x) {
   return std::sqrt(dot(A->n, r.data(), r.data())) / std::sqrt(dot(A->n, b, b));
 }
 
+// Persistent preconditioner for the numpy CA-GMRES oracle (oracle/cagmres.py).
+void* orc_precon_create(const OrcMat* A, const OrcParams* prm, int* err) {
+  Precon* P = new Precon();
+  int e = setup_precon(*A, *prm, *P);
+  if (err) *err = e;
+  if (e) { delete P; return nullptr; }
+  return P;
+}
+
+void orc_precon_apply_h(void* h, const double* r, double* s) {
+  apply_precon(*static_cast<Precon*>(h), r, s);
+}
+
+void orc_precon_destroy(void* h) { delete static_cast<Precon*>(h); }
+
 }  // extern "C"

@@ -20,6 +20,15 @@ namespace pb {
 #define GRID_LOOP(i, n) \
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
+// Grid-stride loop over groups of kU elements per thread (i0 + u*stride, u < kU): the
+// loads of a group are issued before any result is stored, which keeps kU independent
+// loads per operand in flight for the HBM-bound vector kernels.
+constexpr int kU = 4;
+#define GRID_LOOP_U(i0, st, n)                                                            \
+  for (int64_t st = (int64_t)gridDim.x * blockDim.x,                                       \
+               i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;                       \
+       i0 < (n); i0 += kU * st)
+
 __device__ __forceinline__ double cval(const Coef& c) { return c.p ? (*c.p) * c.mul : c.v; }
 
 // out = c0*x0 + c1*x1 (+ c2*x2), evaluated left to right as the reference's axpy
@@ -30,11 +39,26 @@ __global__ void k_lincomb(int64_t n, T* __restrict__ out, const T* __restrict__ 
                           Coef c2, const int* gate) {
   if (gated(gate)) return;
   const T a0 = (T)cval(c0), a1 = (T)cval(c1), a2 = (T)cval(c2);
-  GRID_LOOP(i, n) {
-    T v = a0 * x0[i];
-    if (x1) v = v + a1 * x1[i];
-    if (x2) v = v + a2 * x2[i];
-    out[i] = v;
+  GRID_LOOP_U(i0, st, n) {
+    T v0[kU], v1[kU], v2[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int64_t i = i0 + u * st;
+      const bool ok = i < n;
+      v0[u] = ok ? x0[i] : T(0);
+      v1[u] = (ok && x1) ? x1[i] : T(0);
+      v2[u] = (ok && x2) ? x2[i] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int64_t i = i0 + u * st;
+      if (i < n) {
+        T v = a0 * v0[u];
+        if (x1) v = v + a1 * v1[u];
+        if (x2) v = v + a2 * v2[u];
+        out[i] = v;
+      }
+    }
   }
 }
 
@@ -53,20 +77,33 @@ __global__ void __launch_bounds__(kRedThreads) k_lincomb_dot(int64_t n, T* __res
   double acc[ND > 0 ? ND : 1];
 #pragma unroll
   for (int k = 0; k < ND; ++k) acc[k] = 0.0;
-  GRID_LOOP(i, n) {
-    T v;
-    if (out) {
-      v = a0 * x0[i];
-      if (x1) v = v + a1 * x1[i];
-      if (x2) v = v + a2 * x2[i];
-      out[i] = v;
-    } else {
-      v = T(0);
-    }
-    T src[6] = {v, x0 ? x0[i] : T(0), x1 ? x1[i] : T(0), x2 ? x2[i] : T(0), d0 ? d0[i] : T(0),
-                d1 ? d1[i] : T(0)};
+  GRID_LOOP_U(i0, st, n) {
+    T s0[kU], s1[kU], s2[kU], s4[kU], s5[kU];
 #pragma unroll
-    for (int k = 0; k < ND; ++k) acc[k] += (double)(src[sel.a[k]] * src[sel.b[k]]);
+    for (int u = 0; u < kU; ++u) {
+      const int64_t i = i0 + u * st;
+      const bool ok = i < n;
+      s0[u] = (ok && x0) ? x0[i] : T(0);
+      s1[u] = (ok && x1) ? x1[i] : T(0);
+      s2[u] = (ok && x2) ? x2[i] : T(0);
+      s4[u] = (ok && d0) ? d0[i] : T(0);
+      s5[u] = (ok && d1) ? d1[i] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int64_t i = i0 + u * st;
+      if (i >= n) continue;
+      T v = T(0);
+      if (out) {
+        v = a0 * s0[u];
+        if (x1) v = v + a1 * s1[u];
+        if (x2) v = v + a2 * s2[u];
+        out[i] = v;
+      }
+      T src[6] = {v, s0[u], s1[u], s2[u], s4[u], s5[u]};
+#pragma unroll
+      for (int k = 0; k < ND; ++k) acc[k] += (double)(src[sel.a[k]] * src[sel.b[k]]);
+    }
   }
   reduce_and_finish<ND>(acc, red);
 }
@@ -77,10 +114,24 @@ __global__ void k_cg_axpy2(int64_t n, T* __restrict__ x, T* __restrict__ p, cons
                            const KState* st, const int* gate) {
   if (gated(gate)) return;
   const T alpha = (T)st->alpha, beta = (T)st->beta;
-  GRID_LOOP(i, n) {
-    T pi = p[i];
-    x[i] = x[i] + alpha * pi;
-    p[i] = s[i] + beta * pi;
+  GRID_LOOP_U(i0, stp, n) {
+    T pv[kU], xv[kU], sv[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int64_t i = i0 + u * stp;
+      const bool ok = i < n;
+      pv[u] = ok ? p[i] : T(0);
+      xv[u] = ok ? x[i] : T(0);
+      sv[u] = ok ? s[i] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int64_t i = i0 + u * stp;
+      if (i < n) {
+        x[i] = xv[u] + alpha * pv[u];
+        p[i] = sv[u] + beta * pv[u];
+      }
+    }
   }
 }
 
@@ -89,7 +140,21 @@ template <class T>
 __global__ void k_scale(int64_t n, T* __restrict__ s, const T* __restrict__ d, const T* __restrict__ r,
                         const int* gate) {
   if (gated(gate)) return;
-  GRID_LOOP(i, n) s[i] = r[i] * d[i];
+  GRID_LOOP_U(i0, st, n) {
+    T rv[kU], dv[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int64_t i = i0 + u * st;
+      const bool ok = i < n;
+      rv[u] = ok ? r[i] : T(0);
+      dv[u] = ok ? d[i] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int64_t i = i0 + u * st;
+      if (i < n) s[i] = rv[u] * dv[u];
+    }
+  }
 }
 
 // CGS multi-dot h(k) = <w, v_k>, k = 1..j (cuda_CGS_Orth dot phase, cu_qrdecomposition.cu:45)

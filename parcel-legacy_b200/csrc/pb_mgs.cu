@@ -58,12 +58,25 @@ __global__ void __launch_bounds__(kMgsThreads, 2) k_gm_mgs(MgsArgs<T> a) {
     const T* vcur = a.V + (size_t)(p - 1) * a.ldv;
     const T mh = (T)(-hprev);
     double part = 0.0;
+    // Batches of EB elements: all loads of a batch are issued before any is used, so
+    // every thread keeps 2*EB loads in flight.
+    constexpr int EB = ELEMS < 8 ? ELEMS : 8;
+    const bool upd = p > 1, dotv = p <= j;
 #pragma unroll
-    for (int e = 0; e < ELEMS; ++e) {
-      const int64_t i = tid + e * nthr;
-      if (i < a.np) {
-        if (p > 1) w[e] = mh * vprev[i] + w[e];              // w = -h v + 1*w
-        part += (p <= j) ? (double)(w[e] * vcur[i]) : (double)(w[e] * w[e]);
+    for (int e0 = 0; e0 < ELEMS; e0 += EB) {
+      T vp[EB], vc[EB];
+#pragma unroll
+      for (int u = 0; u < EB; ++u) {
+        const int64_t i = tid + (e0 + u) * nthr;
+        const bool ok = i < a.np;
+        vp[u] = (upd && ok) ? __ldcg(vprev + i) : T(0);
+        vc[u] = (dotv && ok) ? __ldcs(vcur + i) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < EB; ++u) {
+        T& we = w[e0 + u];
+        if (upd) we = mh * vp[u] + we;                          // w = -h v + 1*w
+        part += dotv ? (double)(we * vc[u]) : (double)(we * we);
       }
     }
 #pragma unroll
