@@ -143,6 +143,9 @@ __global__ void __launch_bounds__(256) k_tsqr_local(int64_t nrows, int c, const 
   const int lane = threadIdx.x & 31;
   const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t r0 = w * rows_per_warp;
+  // The grid is rounded up to whole blocks: warps past the last row own no R factor and
+  // must not write one (Rout holds exactly ceil(nrows / rows_per_warp) factors).
+  if (r0 >= nrows) return;
   const int64_t r1 = min(nrows, r0 + rows_per_warp);
   double R[CM];
 #pragma unroll

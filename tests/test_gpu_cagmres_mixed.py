@@ -58,7 +58,9 @@ def test_residual_dd_matches_numpy_oracle():
     rh_ref, rl_ref = dd.residual(A, x, None, b, None)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     rh, rl = torch.zeros(A.n, dtype=torch.float64, device="cuda"), torch.zeros(A.n, dtype=torch.float64, device="cuda")
-    S = api.crs_struct(A, t(A.rowptr), t(A.col), t(A.val))
+    # the device copies must outlive the call: the struct holds raw pointers only
+    rp, ci, va = t(A.rowptr), t(A.col), t(A.val)
+    S = api.crs_struct(A, rp, ci, va)
     xd, bd = t(x), t(b)
     rc = _lib.load().parcel_b_residual_dd(C.byref(S), xd.data_ptr(), None, bd.data_ptr(), None, rh.data_ptr(),
                                           rl.data_ptr())
