@@ -249,6 +249,20 @@ int parcel_b_precon_apply(const parcel_b_input* prm, const parcel_b_crs* A, cons
                           double* s);
 /* Deterministic dot product of two device vectors. */
 int parcel_b_dot(int64_t n, const double* x, const double* y, double* out_host);
+/* Dot product of two device vectors that allocates nothing (no counterpart in the
+ * reference).  For callers that may not allocate device memory while they run (their
+ * own memory pool owns the GPU, or a cudaMalloc would synchronise a pipeline): scratch
+ * is a fixed file-scope device array, the kernel runs on `stream` (a cudaStream_t, NULL
+ * for the legacy default stream) and writes *result_dev (device memory) without a host
+ * synchronisation.  Same result as parcel_b_dot up to rounding (different block size).
+ *   - n <= 67,108,864 (one partial per 16,384 elements, 4,096 partials); larger n
+ *     returns PARCEL_B_E_ARG;
+ *   - one scratch array per device shared by all calls: calls that overlap on the GPU
+ *     race; serialise them;
+ *   - the first call on a device resolves the array's address on the current device:
+ *     make it before any stream capture. */
+int parcel_b_dot_noalloc(int64_t n, const double* x, const double* y, double* result_dev,
+                         void* stream);
 /* r = b - A x in double-double with the reference's dd add / mul order
  * (dd_func.f90:5-98); A values, b and x given as (hi, lo) pairs, lo may be NULL. Device
  * arrays; returns r as (r_hi, r_lo). */

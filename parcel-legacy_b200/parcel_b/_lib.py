@@ -93,6 +93,7 @@ SIGNATURES = {
     "parcel_b_spmv_f32": (C.c_int, [C.c_int32, C.c_int64, C.c_int32, P, P, P, P, P]),
     "parcel_b_precon_apply": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), P, P]),
     "parcel_b_dot": (C.c_int, [C.c_int64, P, P, DP]),
+    "parcel_b_dot_noalloc": (C.c_int, [C.c_int64, P, P, P, P]),
     "parcel_b_residual_dd": (C.c_int, [C.POINTER(Crs), P, P, P, P, P, P]),
     "parcel_b_bench_kernels": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, DP, DP]),
 }
