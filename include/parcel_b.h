@@ -142,7 +142,8 @@ typedef struct parcel_b_stats {
   int kernel_launches;      /* kernels this library launched for the solve           */
   int ilu_levels_max;       /* longest wavefront (levels) of any block-Jacobi block  */
   int ilu_nblocks;
-  int reserved[6];
+  int fallback;             /* learned solve: 1 if the plain PGMRES/ILU path finished it */
+  int reserved[5];
 } parcel_b_stats;
 
 /* ---- lifecycle: PARCEL_Init / PARCEL_Free (src/c_krylov_wrapper.f90:6-23,
@@ -275,6 +276,46 @@ int parcel_b_residual_dd(const parcel_b_crs* A, const double* x_hi, const double
  * launch of each, measured with CUDA events on that stream.  Host or device matrix. */
 int parcel_b_bench_kernels(const parcel_b_input* prm, const parcel_b_crs* A, int reps,
                            double* ms_spmv, double* ms_precon);
+
+/* ---- learned coarse-grid preconditioner stage (no counterpart in the reference) -----
+ * Flexible GMRES with z = M^-1 r followed by a learned coarse correction:
+ *   t = r - A z,  z += (sigma / s) P Net([R t / sigma, dhat]),  sigma = rms(R t),
+ * R = mean over coarsen^3 blocks of the natural grid (row = (z ny + y) nx + x), P =
+ * cell-centred trilinear interpolation, dhat = normalised coarse log|diag A|, s = the
+ * target scale fixed from the training pairs.  Net: six BF16 3x3x3 convolutions,
+ * 2 -> 32 -> 32 -> 32 -> 32 -> 32 -> 1 channels, ReLU between, zero padding, FP32 sums.
+ * Parameters (FP32): for layer l = 0..5, W_l[27][C_in][C_out] (tap 9(dz+1)+3(dy+1)+(dx+1))
+ * then b_l[C_out]. */
+typedef struct parcel_b_learned_s* parcel_b_learned;
+int parcel_b_learned_create(int nx, int ny, int nz, int coarsen, uint64_t seed, parcel_b_learned* out);
+int parcel_b_learned_destroy(parcel_b_learned h);
+int64_t parcel_b_learned_num_params(void);
+/* FP32 master parameters (host or device array of num_params) and the target scale s. */
+int parcel_b_learned_get_params(parcel_b_learned h, float* params, double* target_scale);
+/* params may be NULL (keep); target_scale <= 0 keeps the current one. */
+int parcel_b_learned_set_params(parcel_b_learned h, const float* params, double target_scale);
+/* The network alone on `batch` coarse grids: u [batch][V][2] FP32 (rounded to BF16 on
+ * entry), y [batch][V]; V = (nx ny nz) / coarsen^3; host or device arrays. */
+int parcel_b_learned_forward(parcel_b_learned h, int batch, const float* u, float* y);
+/* loss = 1/(2 M) sum (y - target)^2 over the M = batch V outputs and its gradient with
+ * respect to every parameter (FP32, parameter layout), kept for parcel_b_learned_adam. */
+int parcel_b_learned_grad(parcel_b_learned h, int batch, const float* u, const float* target,
+                          double* loss, float* grad);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) with the last gradient. */
+int parcel_b_learned_adam(parcel_b_learned h, double lr);
+/* Solves A x = b with the plain GMRES of prm (x0 = 0) and appends up to max_pairs
+ * training pairs from the iterates after each restart cycle (x_0 = 0 included). */
+int parcel_b_learned_collect(parcel_b_learned h, const parcel_b_input* prm, const parcel_b_crs* A,
+                             const double* b, int max_pairs, int* npairs);
+int parcel_b_learned_num_pairs(parcel_b_learned h);
+/* Adam over the collected pairs: `steps` steps of `batch` pairs drawn with `seed`. */
+int parcel_b_learned_train(parcel_b_learned h, int steps, int batch, double lr, uint64_t seed,
+                           double* first_loss, double* last_loss);
+/* Flexible GMRES(GMRES_m) with M from prm and the learned stage (h NULL: M alone), FP64
+ * or, with inner_precision = 1, FP32 inside the FP64 refinement loop.  If the FP64 true
+ * residual misses rtolmax, plain PGMRES with M continues from x (stats.fallback = 1). */
+int parcel_b_solve_learned(const parcel_b_input* prm, const parcel_b_crs* A, parcel_b_learned h,
+                           const double* b, double* x, double* reshistory, int* niter, int* iret);
 
 #ifdef __cplusplus
 }

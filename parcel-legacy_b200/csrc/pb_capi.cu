@@ -10,33 +10,18 @@
 #include <memory>
 #include <mutex>
 
-#include "pb_mixed.cuh"
-#include "pb_solvers.cuh"
+#include "pb_api.cuh"
 
 namespace pb {
 
 namespace {
 std::mutex g_stats_mu;
 parcel_b_stats g_stats;
+}  // namespace
 
 void set_stats(const parcel_b_stats& s) {
   std::lock_guard<std::mutex> lk(g_stats_mu);
   g_stats = s;
-}
-
-template <class F>
-int guarded(F&& f) {
-  try {
-    return f();
-  } catch (const Error& e) {
-    return e.code;
-  } catch (const std::bad_alloc&) {
-    set_last_error(PARCEL_B_E_NOMEM, "host allocation failed");
-    return PARCEL_B_E_NOMEM;
-  } catch (...) {
-    set_last_error(PARCEL_B_E_ARG, "unexpected exception");
-    return PARCEL_B_E_ARG;
-  }
 }
 
 void validate(const parcel_b_crs* A) {
@@ -51,8 +36,6 @@ void validate(const parcel_b_crs* A) {
   PB_CHECK(A->istart == 1, PARCEL_B_E_UNSUPPORTED,
            "istart=%d: one process owns rows 1..n", A->istart);
 }
-
-}  // namespace
 
 // Deterministic dot of two device vectors, result on the host.
 template <class T>
@@ -82,21 +65,9 @@ double true_relres(const DevMat<double>& A, const double* b, const double* x) {
   return std::sqrt(rr) / std::sqrt(bb);
 }
 
-// Natural-layout vector on the device: the caller's pointer or an uploaded copy.
-struct NatVec {
-  DBuf own;
-  double* p = nullptr;
-  NatVec(const double* src, int n, bool dev) {
-    if (dev) { p = const_cast<double*>(src); return; }
-    own.alloc(sizeof(double) * n);
-    h2d(own.p, src, sizeof(double) * n);
-    p = dp<double>(own);
-  }
-};
-
 // One FP64 solve on a built system.  b, x natural-layout device arrays; x in/out.
-static SolveOut solve_on_system(const Options& o, System<double>& S, const double* b_dev,
-                                double* x_dev, std::vector<double>& hist_out, double* setup_t) {
+SolveOut solve_on_system(const Options& o, System<double>& S, const double* b_dev, double* x_dev,
+                         std::vector<double>& hist_out, double* setup_t) {
   cudaStream_t st = stream();
   const int np = S.np;
   DBuf bb, xb;

@@ -1,0 +1,891 @@
+// pb_cnn.cu -- kernels of the learned coarse-grid preconditioner stage.
+//
+// The four 32 -> 32 convolutions (and their transposes in the backward pass) are implicit
+// GEMMs on the tensor cores: a CTA stages a halo brick of BF16 activations (34 x 6 x 4
+// voxels x 64 B) and all 27 taps of packed weights in shared memory with cp.async, and
+// each warp issues m16n8k16 BF16 MMAs with FP32 accumulation for one line of 32 output
+// voxels x 32 channels.  The weight gradient is the same product with the voxel axis as
+// the reduction axis (ldmatrix.trans on both operands); every CTA writes a partial and a
+// second kernel sums the partials in CTA order, so gradients are deterministic.  The
+// 2 -> 32 input layer and the 32 -> 1 output layer have too few MACs per voxel for the
+// tensor cores and run on the CUDA cores.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <random>
+#include <vector>
+
+#include "pb_cnn.cuh"
+#include "pb_device.cuh"
+
+namespace pb {
+namespace cnn {
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int TX = 32, TY = 4, TZ = 2;                 // output tile of one CTA
+constexpr int BX = TX + 2, BY = TY + 2, BZ = TZ + 2;   // halo brick
+constexpr int kBrickRows = BX * BY * BZ;               // 816 voxels
+constexpr int kTileVox = TX * TY * TZ;                 // 256 voxels
+constexpr int kBrickBytes = kBrickRows * 64;           // 52,224 B
+constexpr int kWBytes = kTaps * kCh * 64;              // 55,296 B
+constexpr int kConvSmem = kBrickBytes + kWBytes + kCh * 4;
+constexpr int kWgSmem = kBrickBytes + kTileVox * 64;
+constexpr int kConvThreads = 256;                      // 8 warps: 4 (y) x 2 (z) lines
+constexpr int kWgThreads = 288;                        // 9 warps: 3 taps each
+constexpr int kWgPart = kTaps * kCh * kCh + kCh;       // W then b of one 32 -> 32 layer
+constexpr int kL1Part = kTaps * kCin * kCh + kCh;      // 1,760
+constexpr int kL6Part = kTaps * kCh + 1;               // 865
+
+struct Tiles {
+  int ntx, nty, ntz;
+  int64_t per_sample, total;
+};
+__host__ __device__ inline Tiles tiles_of(const Geo& g, int batch) {
+  Tiles t;
+  t.ntx = (g.gx + TX - 1) / TX;
+  t.nty = (g.gy + TY - 1) / TY;
+  t.ntz = (g.gz + TZ - 1) / TZ;
+  t.per_sample = (int64_t)t.ntx * t.nty * t.ntz;
+  t.total = t.per_sample * batch;
+  return t;
+}
+
+// 64-byte rows (32 BF16 channels) of four 16-byte chunks; the chunk index is XORed with
+// bits 1..2 of the row so that ldmatrix over any 8 consecutive rows is conflict-free.
+__device__ __forceinline__ uint32_t swz(int row, int chunk) {
+  return (uint32_t)row * 64u + ((uint32_t)(chunk ^ ((row >> 1) & 3)) << 4);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], uint32_t addr) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(addr) : "memory");
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], uint32_t addr) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(addr) : "memory");
+}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Keeps each BF16 half of v where the matching half of m is > 0 (ReLU derivative).
+__device__ __forceinline__ uint32_t mask_pairs(uint32_t v, uint32_t m) {
+  const uint32_t lo = ((int16_t)(m & 0xFFFFu) > 0) ? 0x0000FFFFu : 0u;
+  const uint32_t hi = ((int16_t)(m >> 16) > 0) ? 0xFFFF0000u : 0u;
+  return v & (lo | hi);
+}
+
+__device__ __forceinline__ void tile_origin(const Tiles& T, int64_t tile, int64_t& b, int& x0, int& y0, int& z0) {
+  b = tile / T.per_sample;
+  const int64_t rem = tile - b * T.per_sample;
+  x0 = (int)(rem % T.ntx) * TX;
+  y0 = (int)((rem / T.ntx) % T.nty) * TY;
+  z0 = (int)(rem / ((int64_t)T.ntx * T.nty)) * TZ;
+}
+
+// Halo brick of 32-channel BF16 voxels (zero outside the grid) into shared memory.
+__device__ __forceinline__ void load_brick(uint32_t sb, const bf16* in, const Geo& g, int64_t vbase, int x0,
+                                           int y0, int z0) {
+  for (int idx = threadIdx.x; idx < kBrickRows * 4; idx += blockDim.x) {
+    const int row = idx >> 2, ch = idx & 3;
+    const int bx = row % BX, r2 = row / BX, by = r2 % BY, bz = r2 / BY;
+    const int x = x0 + bx - 1, y = y0 + by - 1, z = z0 + bz - 1;
+    const bool ok = (unsigned)x < (unsigned)g.gx && (unsigned)y < (unsigned)g.gy && (unsigned)z < (unsigned)g.gz;
+    const bf16* src = ok ? in + ((vbase + ((int64_t)z * g.gy + y) * g.gx + x) * kCh + ch * 8) : in;
+    cp_async16(sb + swz(row, ch), src, ok);
+  }
+}
+
+// ---------------------------------------------------------------- 32 -> 32 convolution
+// out = relu(conv3(in, W) + b)                          (forward)
+// out = conv3(in, W') where mask > 0, else 0            (transposed convolution, W' mirrored)
+template <bool DGRAD>
+__global__ void __launch_bounds__(kConvThreads, 2)
+    k_conv32(Geo g, int batch, const bf16* __restrict__ in, const bf16* __restrict__ wpk,
+             const float* __restrict__ bias, const bf16* __restrict__ mask, bf16* __restrict__ out,
+             const int* gate) {
+  if (gated(gate)) return;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const uint32_t sb = smem_u32(smem), sw = sb + kBrickBytes;
+  float* sbias = reinterpret_cast<float*>(smem + kBrickBytes + kWBytes);
+  for (int idx = threadIdx.x; idx < kTaps * kCh * 4; idx += kConvThreads) {
+    const int row = idx >> 2, ch = idx & 3;
+    cp_async16(sw + swz(row, ch), wpk + row * kCh + ch * 8, true);
+  }
+  if (threadIdx.x < kCh) sbias[threadIdx.x] = DGRAD ? 0.f : bias[threadIdx.x];
+  const Tiles T = tiles_of(g, batch);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wy = warp & 3, wz = warp >> 2;
+  const int q = lane >> 3, rr = lane & 7, gq = lane >> 2, tq = lane & 3;
+  const int64_t V = g.V();
+  for (int64_t tile = blockIdx.x; tile < T.total; tile += gridDim.x) {
+    int64_t b;
+    int x0, y0, z0;
+    tile_origin(T, tile, b, x0, y0, z0);
+    load_brick(sb, in, g, b * V, x0, y0, z0);
+    cp_async_wait_all();
+    __syncthreads();
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.f;
+#pragma unroll 1
+    for (int t = 0; t < kTaps; ++t) {
+      const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+      const int rbase = ((wz + 1 + dz) * BY + (wy + 1 + dy)) * BX + 1 + dx;
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks) {
+        uint32_t a[2][4], bq[4][2];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) ldsm_x4(a[mt], sb + swz(rbase + mt * 16 + (q & 1) * 8 + rr, ks * 2 + (q >> 1)));
+#pragma unroll
+        for (int np = 0; np < 2; ++np) {
+          uint32_t r[4];
+          ldsm_x4(r, sw + swz(t * kCh + (np * 2 + (q >> 1)) * 8 + rr, ks * 2 + (q & 1)));
+          bq[np * 2][0] = r[0];
+          bq[np * 2][1] = r[1];
+          bq[np * 2 + 1][0] = r[2];
+          bq[np * 2 + 1][1] = r[3];
+        }
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[mt][nt], a[mt], bq[nt][0], bq[nt][1]);
+      }
+    }
+    __syncthreads();   // the brick is free: stage the BF16 results there
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int tv = (wz * TY + wy) * TX + mt * 16 + gq + h * 8;
+          const int co = nt * 8 + tq * 2;
+          float v0 = acc[mt][nt][h * 2], v1 = acc[mt][nt][h * 2 + 1];
+          if (!DGRAD) {
+            v0 = fmaxf(v0 + sbias[co], 0.f);
+            v1 = fmaxf(v1 + sbias[co + 1], 0.f);
+          }
+          *reinterpret_cast<__nv_bfloat162*>(smem + swz(tv, nt) + tq * 4) = __floats2bfloat162_rn(v0, v1);
+        }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kTileVox * 4; idx += kConvThreads) {
+      const int tv = idx >> 2, ch = idx & 3;
+      const int x = x0 + tv % TX, y = y0 + (tv / TX) % TY, z = z0 + tv / (TX * TY);
+      if (x < g.gx && y < g.gy && z < g.gz) {
+        const int64_t o = (b * V + ((int64_t)z * g.gy + y) * g.gx + x) * kCh + ch * 8;
+        uint4 v = *reinterpret_cast<const uint4*>(smem + swz(tv, ch));
+        if (DGRAD) {
+          const uint4 m = *reinterpret_cast<const uint4*>(mask + o);
+          v.x = mask_pairs(v.x, m.x);
+          v.y = mask_pairs(v.y, m.y);
+          v.z = mask_pairs(v.z, m.z);
+          v.w = mask_pairs(v.w, m.w);
+        }
+        *reinterpret_cast<uint4*>(out + o) = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- 32 -> 32 weight gradient
+// part[cta] = ( dW[t][ci][co] = sum_v a[v + d_t][ci] g[v][co],  db[co] = sum_v g[v][co] )
+// over the tiles of this CTA.  Warp w owns taps w, w + 9, w + 18.
+__global__ void __launch_bounds__(kWgThreads, 1)
+    k_wgrad32(Geo g, int batch, const bf16* __restrict__ a_in, const bf16* __restrict__ gout, float* __restrict__ part) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ float sdb[kWgThreads / 32][kCh];
+  const uint32_t sb = smem_u32(smem), sg = sb + kBrickBytes;
+  const Tiles T = tiles_of(g, batch);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = lane >> 3, rr = lane & 7, gq = lane >> 2, tq = lane & 3;
+  const int64_t V = g.V();
+  float acc[3][2][4][4];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) acc[i][j][k][l] = 0.f;
+  float db = 0.f;
+  for (int64_t tile = blockIdx.x; tile < T.total; tile += gridDim.x) {
+    int64_t b;
+    int x0, y0, z0;
+    tile_origin(T, tile, b, x0, y0, z0);
+    load_brick(sb, a_in, g, b * V, x0, y0, z0);
+    for (int idx = threadIdx.x; idx < kTileVox * 4; idx += kWgThreads) {
+      const int tv = idx >> 2, ch = idx & 3;
+      const int x = x0 + tv % TX, y = y0 + (tv / TX) % TY, z = z0 + tv / (TX * TY);
+      const bool ok = x < g.gx && y < g.gy && z < g.gz;
+      const bf16* src = ok ? gout + ((b * V + ((int64_t)z * g.gy + y) * g.gx + x) * kCh + ch * 8) : gout;
+      cp_async16(sg + swz(tv, ch), src, ok);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    {
+      const int co = threadIdx.x & 31;
+      for (int v = warp; v < kTileVox; v += kWgThreads / 32)
+        db += __bfloat162float(*reinterpret_cast<const bf16*>(smem + kBrickBytes + swz(v, co >> 3) + (co & 7) * 2));
+    }
+#pragma unroll 1
+    for (int L = 0; L < TY * TZ; ++L) {
+      const int wy = L % TY, wz = L / TY;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int tvb = L * TX + h * 16;
+        uint32_t bq[4][2];
+#pragma unroll
+        for (int np = 0; np < 2; ++np) {
+          uint32_t r[4];
+          ldsm_x4_t(r, sg + swz(tvb + (q & 1) * 8 + rr, np * 2 + (q >> 1)));
+          bq[np * 2][0] = r[0];
+          bq[np * 2][1] = r[1];
+          bq[np * 2 + 1][0] = r[2];
+          bq[np * 2 + 1][1] = r[3];
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const int t = warp + 9 * i;
+          const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+          const int rbase = ((wz + 1 + dz) * BY + (wy + 1 + dy)) * BX + 1 + dx + h * 16;
+#pragma unroll
+          for (int mt = 0; mt < 2; ++mt) {
+            uint32_t a[4];
+            ldsm_x4_t(a, sb + swz(rbase + (q >> 1) * 8 + rr, mt * 2 + (q & 1)));
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[i][mt][nt], a, bq[nt][0], bq[nt][1]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  float* P = part + (size_t)blockIdx.x * kWgPart;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int t = warp + 9 * i;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int ci = mt * 16 + gq + (r >> 1) * 8, co = nt * 8 + tq * 2 + (r & 1);
+          P[(t * kCh + ci) * kCh + co] = acc[i][mt][nt][r];
+        }
+  }
+  sdb[warp][threadIdx.x & 31] = db;
+  __syncthreads();
+  if (threadIdx.x < kCh) {
+    float s = 0.f;
+    for (int w = 0; w < kWgThreads / 32; ++w) s += sdb[w][threadIdx.x];
+    P[kTaps * kCh * kCh + threadIdx.x] = s;
+  }
+}
+
+// Sums `nparts` partials of `count` floats (stride `stride`) in partial order.
+__global__ void k_reduce_parts(const float* __restrict__ part, int nparts, int stride, int count, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  double s = 0.0;
+  for (int c = 0; c < nparts; ++c) s += part[(size_t)c * stride + i];
+  out[i] = (float)s;
+}
+
+__device__ __forceinline__ void voxel_xyz(const Geo& g, int64_t v, int& x, int& y, int& z) {
+  x = (int)(v % g.gx);
+  y = (int)((v / g.gx) % g.gy);
+  z = (int)(v / ((int64_t)g.gx * g.gy));
+}
+__device__ __forceinline__ bool nb_of(const Geo& g, int x, int y, int z, int t, int sgn, int64_t& nb) {
+  const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+  const int xx = x + sgn * dx, yy = y + sgn * dy, zz = z + sgn * dz;
+  if ((unsigned)xx >= (unsigned)g.gx || (unsigned)yy >= (unsigned)g.gy || (unsigned)zz >= (unsigned)g.gz) return false;
+  nb = ((int64_t)zz * g.gy + yy) * g.gx + xx;
+  return true;
+}
+
+// ---------------------------------------------------------------- input layer 2 -> 32
+__global__ void __launch_bounds__(256) k_l1_fwd(Geo g, int batch, const __nv_bfloat162* __restrict__ u,
+                                                const float* __restrict__ w0, const float* __restrict__ b0,
+                                                bf16* __restrict__ out, const int* gate) {
+  if (gated(gate)) return;
+  __shared__ float sw[kTaps * kCin * kCh];
+  __shared__ float sbv[kCh];
+  for (int i = threadIdx.x; i < kTaps * kCin * kCh; i += blockDim.x) sw[i] = w0[i];
+  if (threadIdx.x < kCh) sbv[threadIdx.x] = b0[threadIdx.x];
+  __syncthreads();
+  const int64_t V = g.V();
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V * batch) return;
+  const int64_t b = i / V, v = i - b * V;
+  int x, y, z;
+  voxel_xyz(g, v, x, y, z);
+  float acc[kCh];
+#pragma unroll
+  for (int c = 0; c < kCh; ++c) acc[c] = sbv[c];
+  for (int t = 0; t < kTaps; ++t) {
+    int64_t nb;
+    if (!nb_of(g, x, y, z, t, 1, nb)) continue;
+    const float2 uv = __bfloat1622float2(u[b * V + nb]);
+#pragma unroll
+    for (int c = 0; c < kCh; ++c) {
+      acc[c] = fmaf(uv.x, sw[(t * kCin + 0) * kCh + c], acc[c]);
+      acc[c] = fmaf(uv.y, sw[(t * kCin + 1) * kCh + c], acc[c]);
+    }
+  }
+  uint4* o = reinterpret_cast<uint4*>(out + i * kCh);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    uint32_t w[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      __nv_bfloat162 p = __floats2bfloat162_rn(fmaxf(acc[k * 8 + j * 2], 0.f), fmaxf(acc[k * 8 + j * 2 + 1], 0.f));
+      w[j] = *reinterpret_cast<uint32_t*>(&p);
+    }
+    o[k] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+__device__ __forceinline__ void unpack32(const bf16* row, float (&a)[kCh]) {
+  const uint4* p = reinterpret_cast<const uint4*>(row);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint4 q = p[k];
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[j]));
+      a[k * 8 + j * 2] = f.x;
+      a[k * 8 + j * 2 + 1] = f.y;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- output layer 32 -> 1
+__global__ void __launch_bounds__(256) k_l6_fwd(Geo g, int batch, const bf16* __restrict__ a5,
+                                                const float* __restrict__ w5, const float* __restrict__ b5,
+                                                float* __restrict__ y, const int* gate) {
+  if (gated(gate)) return;
+  __shared__ float sw[kTaps * kCh];
+  for (int i = threadIdx.x; i < kTaps * kCh; i += blockDim.x) sw[i] = w5[i];
+  __syncthreads();
+  const int64_t V = g.V();
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V * batch) return;
+  const int64_t b = i / V, v = i - b * V;
+  int x, yy, z;
+  voxel_xyz(g, v, x, yy, z);
+  float acc = b5[0];
+  for (int t = 0; t < kTaps; ++t) {
+    int64_t nb;
+    if (!nb_of(g, x, yy, z, t, 1, nb)) continue;
+    float a[kCh];
+    unpack32(a5 + (b * V + nb) * kCh, a);
+#pragma unroll
+    for (int c = 0; c < kCh; ++c) acc = fmaf(a[c], sw[t * kCh + c], acc);
+  }
+  y[i] = acc;
+}
+
+// g5[u][ci] = (sum_t W5[t][ci] gy[u - d_t]) where a5[u][ci] > 0
+__global__ void __launch_bounds__(256) k_l6_dgrad(Geo g, int batch, const float* __restrict__ gy,
+                                                  const float* __restrict__ w5, const bf16* __restrict__ a5,
+                                                  bf16* __restrict__ g5) {
+  __shared__ float sw[kTaps * kCh];
+  for (int i = threadIdx.x; i < kTaps * kCh; i += blockDim.x) sw[i] = w5[i];
+  __syncthreads();
+  const int64_t V = g.V();
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V * batch) return;
+  const int64_t b = i / V, v = i - b * V;
+  int x, y, z;
+  voxel_xyz(g, v, x, y, z);
+  float acc[kCh];
+#pragma unroll
+  for (int c = 0; c < kCh; ++c) acc[c] = 0.f;
+  for (int t = 0; t < kTaps; ++t) {
+    int64_t nb;
+    if (!nb_of(g, x, y, z, t, -1, nb)) continue;
+    const float gv = gy[b * V + nb];
+#pragma unroll
+    for (int c = 0; c < kCh; ++c) acc[c] = fmaf(sw[t * kCh + c], gv, acc[c]);
+  }
+  const uint4* m = reinterpret_cast<const uint4*>(a5 + i * kCh);
+  uint4* o = reinterpret_cast<uint4*>(g5 + i * kCh);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint4 mk = m[k];
+    const uint32_t mw[4] = {mk.x, mk.y, mk.z, mk.w};
+    uint32_t w[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      __nv_bfloat162 p = __floats2bfloat162_rn(acc[k * 8 + j * 2], acc[k * 8 + j * 2 + 1]);
+      w[j] = mask_pairs(*reinterpret_cast<uint32_t*>(&p), mw[j]);
+    }
+    o[k] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+// part[blk] = (dW5[t][ci] = sum_v a5[v + d_t][ci] gy[v],  db5 = sum_v gy[v]) over a
+// contiguous range of voxels.  Thread (w, ci) owns taps w, w + 9, w + 18.
+__global__ void __launch_bounds__(kWgThreads) k_wgrad_l6(Geo g, int batch, const bf16* __restrict__ a5,
+                                                         const float* __restrict__ gy, float* __restrict__ part) {
+  const int64_t V = g.V(), M = V * batch;
+  const int64_t per = (M + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = (int64_t)blockIdx.x * per, i1 = min(M, i0 + per);
+  const int ci = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float acc[3] = {0.f, 0.f, 0.f};
+  float db = 0.f;
+  for (int64_t i = i0; i < i1; ++i) {
+    const int64_t b = i / V, v = i - b * V;
+    int x, y, z;
+    voxel_xyz(g, v, x, y, z);
+    const float gv = gy[i];
+    db += gv;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      int64_t nb;
+      if (nb_of(g, x, y, z, w + 9 * k, 1, nb)) acc[k] = fmaf(__bfloat162float(a5[(b * V + nb) * kCh + ci]), gv, acc[k]);
+    }
+  }
+  float* P = part + (size_t)blockIdx.x * kL6Part;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) P[(w + 9 * k) * kCh + ci] = acc[k];
+  if (threadIdx.x == 0) P[kTaps * kCh] = db;
+}
+
+// part[blk] = (dW0[t][ci][co] = sum_v u[v + d_t][ci] g1[v][co],  db0[co] = sum_v g1[v][co]).
+__global__ void __launch_bounds__(kWgThreads) k_wgrad_l1(Geo g, int batch, const __nv_bfloat162* __restrict__ u,
+                                                         const bf16* __restrict__ g1, float* __restrict__ part) {
+  const int64_t V = g.V(), M = V * batch;
+  const int64_t per = (M + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = (int64_t)blockIdx.x * per, i1 = min(M, i0 + per);
+  const int co = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float acc[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+  float db = 0.f;
+  for (int64_t i = i0; i < i1; ++i) {
+    const int64_t b = i / V, v = i - b * V;
+    int x, y, z;
+    voxel_xyz(g, v, x, y, z);
+    const float gv = __bfloat162float(g1[i * kCh + co]);
+    db += gv;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      int64_t nb;
+      if (nb_of(g, x, y, z, w + 9 * k, 1, nb)) {
+        const float2 uv = __bfloat1622float2(u[b * V + nb]);
+        acc[k][0] = fmaf(uv.x, gv, acc[k][0]);
+        acc[k][1] = fmaf(uv.y, gv, acc[k][1]);
+      }
+    }
+  }
+  float* P = part + (size_t)blockIdx.x * kL1Part;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) P[((w + 9 * k) * kCin + c) * kCh + co] = acc[k][c];
+  if (w == 0) P[kTaps * kCin * kCh + co] = db;
+}
+
+// gy = (y - s t) / M and per-block sums of (y - s t)^2 (fixed grid: deterministic).
+__global__ void __launch_bounds__(256) k_loss(int64_t M, const float* __restrict__ y, const float* __restrict__ tgt,
+                                              float s, float invM, float* __restrict__ gy, double* __restrict__ part) {
+  __shared__ double red[256 / 32];
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x) {
+    const float d = y[i] - s * tgt[i];
+    gy[i] = d * invM;
+    acc += (double)d * d;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s2 = 0.0;
+    for (int w = 0; w < 256 / 32; ++w) s2 += red[w];
+    part[blockIdx.x] = s2;
+  }
+}
+__global__ void k_loss_final(const double* __restrict__ part, int n, double half_invM, double* __restrict__ loss) {
+  if (threadIdx.x != 0) return;
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += part[i];
+  *loss = s * half_invM;
+}
+
+__global__ void k_adam(int64_t n, float* __restrict__ p, const float* __restrict__ gr, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float b1, float b2, float c1, float c2, float eps) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float g = gr[i];
+  const float mi = b1 * m[i] + (1.f - b1) * g;
+  const float vi = b2 * v[i] + (1.f - b2) * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  const float mh = mi / c1, vh = vi / c2;
+  p[i] = p[i] - lr * mh / (sqrtf(vh) + eps);
+}
+
+struct PackPtrs {
+  bf16* fwd[4];
+  bf16* bwd[4];
+};
+__global__ void k_pack(const float* __restrict__ master, float* __restrict__ w0, float* __restrict__ w5, PackPtrs pp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < kTaps * kCin * kCh) w0[i] = __bfloat162float(__float2bfloat16_rn(master[layer_off(0) + i]));
+  if (i < kTaps * kCh) w5[i] = __bfloat162float(__float2bfloat16_rn(master[layer_off(5) + i]));
+  if (i < 4 * kTaps * kCh * kCh) {
+    const int l = i / (kTaps * kCh * kCh), r = i % (kTaps * kCh * kCh);
+    const int t = r / (kCh * kCh), ci = (r / kCh) % kCh, co = r % kCh;
+    const bf16 w = __float2bfloat16_rn(master[layer_off(l + 1) + r]);
+    pp.fwd[l][(t * kCh + co) * kCh + ci] = w;
+    pp.bwd[l][((kTaps - 1 - t) * kCh + ci) * kCh + co] = w;
+  }
+}
+
+// ---------------------------------------------------------------- coarse-grid transfer
+__global__ void __launch_bounds__(256) k_prep(int64_t V, const float* __restrict__ tc, const float* __restrict__ dhat,
+                                              const float* __restrict__ scal, __nv_bfloat162* __restrict__ u,
+                                              const int* gate) {
+  if (gated(gate)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  u[i] = __floats2bfloat162_rn(tc[i] * scal[0], dhat[i]);
+}
+
+__global__ void k_to_bf16(size_t n, const float* __restrict__ in, bf16* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = __float2bfloat16_rn(in[i]);
+}
+
+__global__ void k_scale_by(int64_t n, const float* __restrict__ in, const float* __restrict__ scal,
+                           float* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i] * scal[0];
+}
+
+template <class T>
+__global__ void __launch_bounds__(kRedThreads)
+    k_restrict(int nx, int ny, int nz, int c, const T* __restrict__ src, const int* __restrict__ pos,
+               float* __restrict__ tc, float* __restrict__ scal, double* __restrict__ part,
+               unsigned* __restrict__ ticket, const int* gate) {
+  if (gated(gate)) return;
+  __shared__ double red[kRedThreads / 32];
+  __shared__ bool last;
+  const int gx = nx / c, gy = ny / c, gz = nz / c;
+  const int64_t V = (int64_t)gx * gy * gz;
+  const double inv = 1.0 / ((double)c * c * c);
+  double sq = 0.0;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
+    const int cx = (int)(v % gx), cy = (int)((v / gx) % gy), cz = (int)(v / ((int64_t)gx * gy));
+    double s = 0.0;
+    for (int k = 0; k < c; ++k)
+      for (int j = 0; j < c; ++j) {
+        const int64_t rowb = ((int64_t)(cz * c + k) * ny + (cy * c + j)) * nx + (int64_t)cx * c;
+        for (int i = 0; i < c; ++i) {
+          const int64_t nat = rowb + i;
+          s += (double)src[pos ? pos[nat] : nat];
+        }
+      }
+    const float m = (float)(s * inv);
+    tc[v] = m;
+    sq += (double)m * m;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) s += red[w];
+    part[blockIdx.x] = s;
+    __threadfence();
+    last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  double s = 0.0;
+  for (unsigned b = 0; b < gridDim.x; ++b) s += __ldcg(part + b);
+  const double rms = sqrt(s / (double)V);
+  scal[0] = rms > 0.0 ? (float)(1.0 / rms) : 0.f;
+  scal[1] = (float)rms;
+  *ticket = 0u;
+}
+
+__device__ __forceinline__ void lin1(int i, int c, int G, int& lo, int& hi, float& w) {
+  const float xi = ((float)i + 0.5f) / (float)c - 0.5f;
+  const float f = floorf(xi);
+  w = xi - f;
+  const int i0 = (int)f;
+  lo = min(max(i0, 0), G - 1);
+  hi = min(max(i0 + 1, 0), G - 1);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256)
+    k_prolong(int nx, int ny, int nz, int c, int64_t np, const float* __restrict__ yc, const float* __restrict__ scal,
+              float scale, const int* __restrict__ rowAt, T* __restrict__ dst, const int* gate) {
+  if (gated(gate)) return;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int64_t nat = rowAt ? (int64_t)rowAt[p] : p;
+  if (nat < 0) return;
+  const int gx = nx / c, gy = ny / c, gz = nz / c;
+  const int x = (int)(nat % nx), y = (int)((nat / nx) % ny), z = (int)(nat / ((int64_t)nx * ny));
+  int x0, x1, y0, y1, z0, z1;
+  float wx, wy, wz;
+  lin1(x, c, gx, x0, x1, wx);
+  lin1(y, c, gy, y0, y1, wy);
+  lin1(z, c, gz, z0, z1, wz);
+  auto at = [&](int zz, int yy, int xx) { return yc[((int64_t)zz * gy + yy) * gx + xx]; };
+  const float c00 = at(z0, y0, x0) * (1.f - wz) + at(z1, y0, x0) * wz;
+  const float c01 = at(z0, y0, x1) * (1.f - wz) + at(z1, y0, x1) * wz;
+  const float c10 = at(z0, y1, x0) * (1.f - wz) + at(z1, y1, x0) * wz;
+  const float c11 = at(z0, y1, x1) * (1.f - wz) + at(z1, y1, x1) * wz;
+  const float c0 = c00 * (1.f - wy) + c10 * wy;
+  const float c1 = c01 * (1.f - wy) + c11 * wy;
+  const float val = c0 * (1.f - wx) + c1 * wx;
+  dst[p] = dst[p] + (T)(scale * scal[1] * val);
+}
+
+__global__ void __launch_bounds__(256)
+    k_coarse_logdiag(int nx, int ny, int nz, int c, const int* __restrict__ rowptr, const int* __restrict__ col,
+                     const double* __restrict__ val, int rbase, int cbase, float* __restrict__ out) {
+  const int gx = nx / c, gy = ny / c, gz = nz / c;
+  const int64_t V = (int64_t)gx * gy * gz;
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const int cx = (int)(v % gx), cy = (int)((v / gx) % gy), cz = (int)(v / ((int64_t)gx * gy));
+  double s = 0.0;
+  for (int k = 0; k < c; ++k)
+    for (int j = 0; j < c; ++j)
+      for (int i = 0; i < c; ++i) {
+        const int64_t r = ((int64_t)(cz * c + k) * ny + (cy * c + j)) * nx + (int64_t)cx * c + i;
+        double d = 0.0;
+        for (int e = rowptr[r] - rbase; e < rowptr[r + 1] - rbase; ++e)
+          if (col[e] - cbase == r) d = val[e];
+        s += log(fmax(fabs(d), 1e-300));
+      }
+  out[v] = (float)(s / ((double)c * c * c));
+}
+
+inline int blocks_for(int64_t n, int t = 256) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
+
+}  // namespace
+
+// ================================================================ host side
+void Net::init(uint64_t seed) {
+  std::vector<float> h((size_t)kNumParams, 0.f);
+  std::mt19937_64 rng(seed);
+  std::normal_distribution<double> nd(0.0, 1.0);
+  for (int l = 0; l < kLayers; ++l) {
+    const int ci = l == 0 ? kCin : kCh;
+    const double sd = std::sqrt(2.0 / (kTaps * ci));
+    float* W = h.data() + layer_off(l);
+    for (int64_t i = 0; i < layer_w(l); ++i) W[i] = (float)(nd(rng) * sd);
+  }
+  master.alloc(sizeof(float) * kNumParams);
+  grad.alloc(sizeof(float) * kNumParams);
+  adam_m.alloc(sizeof(float) * kNumParams);
+  adam_v.alloc(sizeof(float) * kNumParams);
+  h2d(master.p, h.data(), sizeof(float) * kNumParams);
+  cudaStream_t st = stream();
+  PB_CUDA(cudaMemsetAsync(adam_m.p, 0, sizeof(float) * kNumParams, st));
+  PB_CUDA(cudaMemsetAsync(adam_v.p, 0, sizeof(float) * kNumParams, st));
+  PB_CUDA(cudaMemsetAsync(grad.p, 0, sizeof(float) * kNumParams, st));
+  adam_t = 0;
+  pk.w0.alloc(sizeof(float) * kTaps * kCin * kCh);
+  pk.w5.alloc(sizeof(float) * kTaps * kCh);
+  for (int l = 0; l < 4; ++l) {
+    pk.fwd[l].alloc(sizeof(bf16) * kTaps * kCh * kCh);
+    pk.bwd[l].alloc(sizeof(bf16) * kTaps * kCh * kCh);
+  }
+  repack(st);
+}
+
+void Net::repack(cudaStream_t st) {
+  PackPtrs pp;
+  for (int l = 0; l < 4; ++l) {
+    pp.fwd[l] = dp<bf16>(pk.fwd[l]);
+    pp.bwd[l] = dp<bf16>(pk.bwd[l]);
+  }
+  k_pack<<<blocks_for(4 * kTaps * kCh * kCh), 256, 0, st>>>(dp<float>(master), dp<float>(pk.w0), dp<float>(pk.w5), pp);
+  PB_CUDA(cudaGetLastError());
+}
+
+void Acts::ensure(const Geo& gg, int b, bool training) {
+  const bool same = gg.gx == g.gx && gg.gy == g.gy && gg.gz == g.gz && b <= cap;
+  if (same && (!training || gy.p)) {
+    batch = b;
+    return;
+  }
+  g = gg;
+  batch = b;
+  cap = b;
+  const size_t M = (size_t)g.V() * b;
+  u.alloc(sizeof(__nv_bfloat162) * M);
+  for (int l = 0; l < 5; ++l) a[l].alloc(sizeof(bf16) * kCh * M);
+  y.alloc(sizeof(float) * M);
+  if (training) {
+    gA.alloc(sizeof(bf16) * kCh * M);
+    gB.alloc(sizeof(bf16) * kCh * M);
+    gy.alloc(sizeof(float) * M);
+    const Tiles T = tiles_of(g, b);
+    const int nwg = (int)std::min<int64_t>(T.total, num_sms());
+    const size_t pf = std::max<size_t>((size_t)nwg * kWgPart, (size_t)2 * num_sms() * kL1Part);
+    part.alloc(sizeof(float) * pf);
+    lossp.alloc(sizeof(double) * red_blocks());
+  }
+}
+
+static void set_smem_attrs() {
+  static bool done = false;   // attributes are per device function; one device per process
+  if (done) return;
+  PB_CUDA(cudaFuncSetAttribute(k_conv32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
+  PB_CUDA(cudaFuncSetAttribute(k_conv32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
+  PB_CUDA(cudaFuncSetAttribute(k_wgrad32, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem));
+  done = true;
+}
+
+static int conv_grid(const Geo& g, int batch) {
+  const Tiles T = tiles_of(g, batch);
+  return (int)std::min<int64_t>(T.total, 2 * (int64_t)num_sms());
+}
+
+void init_kernels() { set_smem_attrs(); }
+
+void to_bf16(size_t n, const float* in, __nv_bfloat16* out, cudaStream_t st) {
+  k_to_bf16<<<blocks_for((int64_t)n), 256, 0, st>>>(n, in, out);
+  PB_CUDA(cudaGetLastError());
+}
+
+void scale_by(int64_t n, const float* in, const float* scal, float* out, cudaStream_t st) {
+  k_scale_by<<<blocks_for(n), 256, 0, st>>>(n, in, scal, out);
+  PB_CUDA(cudaGetLastError());
+}
+
+void forward(const Net& net, Acts& A, const int* gate, cudaStream_t st) {
+  set_smem_attrs();
+  const Geo& g = A.g;
+  const int64_t M = g.V() * A.batch;
+  const float* mp = dp<float>(net.master);
+  k_l1_fwd<<<blocks_for(M), 256, 0, st>>>(g, A.batch, dp<__nv_bfloat162>(A.u), dp<float>(net.pk.w0),
+                                          mp + layer_off(0) + layer_w(0), dp<bf16>(A.a[0]), gate);
+  const int cg = conv_grid(g, A.batch);
+  for (int l = 1; l <= 4; ++l)
+    k_conv32<false><<<cg, kConvThreads, kConvSmem, st>>>(g, A.batch, dp<bf16>(A.a[l - 1]), dp<bf16>(net.pk.fwd[l - 1]),
+                                                         mp + layer_off(l) + layer_w(l), nullptr, dp<bf16>(A.a[l]), gate);
+  k_l6_fwd<<<blocks_for(M), 256, 0, st>>>(g, A.batch, dp<bf16>(A.a[4]), dp<float>(net.pk.w5),
+                                          mp + layer_off(5) + layer_w(5), dp<float>(A.y), gate);
+  PB_CUDA(cudaGetLastError());
+}
+
+void loss_grad(Net& net, Acts& A, const float* target, float target_scale, double* loss_dev, cudaStream_t st) {
+  forward(net, A, nullptr, st);   // also sets the kernels' shared-memory limits
+  const Geo& g = A.g;
+  const int64_t M = g.V() * A.batch;
+  const int rb = red_blocks();
+  k_loss<<<rb, 256, 0, st>>>(M, dp<float>(A.y), target, target_scale, (float)(1.0 / (double)M), dp<float>(A.gy),
+                             dp<double>(A.lossp));
+  k_loss_final<<<1, 32, 0, st>>>(dp<double>(A.lossp), rb, 0.5 / (double)M, loss_dev);
+  float* gr = dp<float>(net.grad);
+  float* part = dp<float>(A.part);
+  const int nsm = num_sms();
+  // output layer
+  k_wgrad_l6<<<2 * nsm, kWgThreads, 0, st>>>(g, A.batch, dp<bf16>(A.a[4]), dp<float>(A.gy), part);
+  k_reduce_parts<<<blocks_for(kL6Part), 256, 0, st>>>(part, 2 * nsm, kL6Part, kL6Part, gr + layer_off(5));
+  k_l6_dgrad<<<blocks_for(M), 256, 0, st>>>(g, A.batch, dp<float>(A.gy), dp<float>(net.pk.w5), dp<bf16>(A.a[4]),
+                                            dp<bf16>(A.gA));
+  // hidden layers, last to first
+  bf16* gcur = dp<bf16>(A.gA);
+  bf16* gnext = dp<bf16>(A.gB);
+  const Tiles T = tiles_of(g, A.batch);
+  const int nwg = (int)std::min<int64_t>(T.total, nsm);
+  const int cg = conv_grid(g, A.batch);
+  for (int l = 4; l >= 1; --l) {
+    k_wgrad32<<<nwg, kWgThreads, kWgSmem, st>>>(g, A.batch, dp<bf16>(A.a[l - 1]), gcur, part);
+    k_reduce_parts<<<blocks_for(kWgPart), 256, 0, st>>>(part, nwg, kWgPart, kWgPart, gr + layer_off(l));
+    k_conv32<true><<<cg, kConvThreads, kConvSmem, st>>>(g, A.batch, gcur, dp<bf16>(net.pk.bwd[l - 1]), nullptr,
+                                                        dp<bf16>(A.a[l - 1]), gnext, nullptr);
+    std::swap(gcur, gnext);
+  }
+  // input layer
+  k_wgrad_l1<<<2 * nsm, kWgThreads, 0, st>>>(g, A.batch, dp<__nv_bfloat162>(A.u), gcur, part);
+  k_reduce_parts<<<blocks_for(kL1Part), 256, 0, st>>>(part, 2 * nsm, kL1Part, kL1Part, gr + layer_off(0));
+  PB_CUDA(cudaGetLastError());
+}
+
+void adam(Net& net, float lr, cudaStream_t st) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  net.adam_t += 1;
+  const float c1 = (float)(1.0 - std::pow(0.9, net.adam_t));
+  const float c2 = (float)(1.0 - std::pow(0.999, net.adam_t));
+  k_adam<<<blocks_for(kNumParams), 256, 0, st>>>(kNumParams, dp<float>(net.master), dp<float>(net.grad),
+                                                 dp<float>(net.adam_m), dp<float>(net.adam_v), lr, b1, b2, c1, c2, eps);
+  PB_CUDA(cudaGetLastError());
+  net.repack(st);
+}
+
+void prep_input(const Geo& g, const float* tc, const float* dhat, const float* scal, __nv_bfloat16* u,
+                const int* gate, cudaStream_t st) {
+  k_prep<<<blocks_for(g.V()), 256, 0, st>>>(g.V(), tc, dhat, scal, reinterpret_cast<__nv_bfloat162*>(u), gate);
+  PB_CUDA(cudaGetLastError());
+}
+
+template <class T>
+void restrict_to_coarse(int nx, int ny, int nz, int c, const T* src, const int* pos, float* tc, float* scal,
+                        double* part, unsigned* ticket, const int* gate, cudaStream_t st) {
+  k_restrict<T><<<red_blocks(), kRedThreads, 0, st>>>(nx, ny, nz, c, src, pos, tc, scal, part, ticket, gate);
+  PB_CUDA(cudaGetLastError());
+}
+
+template <class T>
+void prolong_add(int nx, int ny, int nz, int c, int64_t np, const float* yc, const float* scal, float scale,
+                 const int* rowAt, T* dst, const int* gate, cudaStream_t st) {
+  k_prolong<T><<<blocks_for(np), 256, 0, st>>>(nx, ny, nz, c, np, yc, scal, scale, rowAt, dst, gate);
+  PB_CUDA(cudaGetLastError());
+}
+
+void coarse_log_diag(int nx, int ny, int nz, int c, const int* rowptr, const int* col, const double* val,
+                     int cbase, float* out, cudaStream_t st) {
+  const int64_t V = (int64_t)(nx / c) * (ny / c) * (nz / c);
+  k_coarse_logdiag<<<blocks_for(V), 256, 0, st>>>(nx, ny, nz, c, rowptr, col, val, 1, cbase, out);
+  PB_CUDA(cudaGetLastError());
+}
+
+template void restrict_to_coarse<double>(int, int, int, int, const double*, const int*, float*, float*, double*,
+                                         unsigned*, const int*, cudaStream_t);
+template void restrict_to_coarse<float>(int, int, int, int, const float*, const int*, float*, float*, double*,
+                                        unsigned*, const int*, cudaStream_t);
+template void prolong_add<double>(int, int, int, int, int64_t, const float*, const float*, float, const int*, double*,
+                                  const int*, cudaStream_t);
+template void prolong_add<float>(int, int, int, int, int64_t, const float*, const float*, float, const int*, float*,
+                                 const int*, cudaStream_t);
+
+}  // namespace cnn
+}  // namespace pb

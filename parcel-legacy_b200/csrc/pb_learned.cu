@@ -1,0 +1,441 @@
+// pb_learned.cu -- C ABI of the learned coarse-grid preconditioner stage (no counterpart in
+// the reference).
+//
+// Life cycle: parcel_b_learned_create fixes the grid and the coarsening factor;
+// parcel_b_learned_collect runs the plain solver (GMRES with the block-Jacobi ILU or Jacobi
+// preconditioner of the caller's parameters) and turns the iterate logged after every
+// restart cycle into a training pair; parcel_b_learned_train fits the network with Adam on
+// the GPU; parcel_b_solve_learned runs flexible GMRES with z = M^-1 r followed by the
+// learned coarse correction, in FP64 or in FP32 inside the FP64 refinement loop, and falls
+// back to the plain PGMRES/ILU path from the current iterate when the learned solve does
+// not reach the tolerance.
+//
+// A training pair for an iterate x_k of the plain solve with solution x*:
+//   r = b - A x_k,  z1 = M^-1 r,  t = r - A z1,  e = x* - x_k - z1  (so A e = t),
+//   input  = [bf16(R t / sigma), bf16(dhat)],  target = (R e) / sigma,  sigma = rms(R t).
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <random>
+
+#include "pb_api.cuh"
+#include "pb_cnn.cuh"
+
+namespace pb {
+
+struct Learned {
+  int nx = 0, ny = 0, nz = 0, c = 1;
+  cnn::Geo g;
+  cnn::Net net;
+  cnn::Acts train;           // training batches
+  cnn::Acts kern;            // kernel-level forward / gradient calls
+  DBuf tgt, loss;
+  double scale = 0.0;        // target scale s: 1 / rms of the collected targets
+  std::vector<DBuf> pu, pt;  // training pairs: inputs bf16 [V][2], targets float [V]
+};
+
+namespace {
+
+void check_grid(const Learned& L, const parcel_b_crs* A) {
+  PB_CHECK((int64_t)L.nx * L.ny * L.nz == (int64_t)A->n, PARCEL_B_E_ARG,
+           "matrix has %d rows, the learned stage's grid %d x %d x %d", A->n, L.nx, L.ny, L.nz);
+}
+
+// Normalised coarse mean of log|diag A|: zero mean and unit variance over the coarse grid.
+void make_dhat(const Learned& L, const DevMat<double>& A, DBuf& out) {
+  const int64_t V = L.g.V();
+  out.alloc(sizeof(float) * V);
+  cnn::coarse_log_diag(L.nx, L.ny, L.nz, L.c, A.rowptr, A.col, A.val, A.cbase, dp<float>(out), stream());
+  std::vector<float> h((size_t)V);
+  d2h(h.data(), out.p, sizeof(float) * V);
+  double m = 0.0, q = 0.0;
+  for (float v : h) m += v;
+  m /= (double)V;
+  for (float v : h) q += (v - m) * (v - m);
+  const double sd = std::sqrt(q / (double)V);
+  for (float& v : h) v = sd > 1e-12 ? (float)((v - m) / sd) : 0.f;
+  h2d(out.p, h.data(), sizeof(float) * V);
+}
+
+// z += (sigma / s) P Net([R (r - A z) / sigma, dhat])
+template <class T>
+struct LearnedStage final : ExtraStage<T> {
+  const Learned* L;
+  DBuf dhat, t, tc, scal, part, ticket;
+  cnn::Acts acts;
+  const int* pos = nullptr;
+  const int* rowAt = nullptr;
+  int64_t np = 0;
+  LearnedStage(const Learned* l, const System<T>& S) : L(l) {
+    cudaStream_t st = stream();
+    make_dhat(*L, S.Anat, dhat);
+    np = S.np;
+    if (S.permuted) {
+      pos = dp<int>(S.pos);
+      rowAt = dp<int>(S.rowAt);
+    }
+    t.alloc(sizeof(T) * np);
+    PB_CUDA(cudaMemsetAsync(t.p, 0, sizeof(T) * np, st));
+    tc.alloc(sizeof(float) * L->g.V());
+    scal.alloc(sizeof(float) * 2);
+    part.alloc(sizeof(double) * red_blocks());
+    ticket.alloc(sizeof(unsigned));
+    PB_CUDA(cudaMemsetAsync(ticket.p, 0, sizeof(unsigned), st));
+    acts.ensure(L->g, 1, false);
+    cnn::init_kernels();
+  }
+  void apply(const System<T>& S, const T* r, T* z, const int* gate, cudaStream_t st) override {
+    spmv<T, T>(S.A, z, dp<T>(t), SPMV_RES, r, gate, st);
+    cnn::restrict_to_coarse<T>(L->nx, L->ny, L->nz, L->c, dp<T>(t), pos, dp<float>(tc), dp<float>(scal),
+                               dp<double>(part), dp<unsigned>(ticket), gate, st);
+    cnn::prep_input(L->g, dp<float>(tc), dp<float>(dhat), dp<float>(scal), dp<__nv_bfloat16>(acts.u), gate, st);
+    cnn::forward(L->net, acts, gate, st);
+    const float inv_s = L->scale > 0.0 ? (float)(1.0 / L->scale) : 1.f;
+    cnn::prolong_add<T>(L->nx, L->ny, L->nz, L->c, np, dp<float>(acts.y), dp<float>(scal), inv_s, rowAt, z, gate, st);
+  }
+  int launches() const override { return 4 + 6; }
+};
+
+// A host or device float array of n entries as a device pointer (uploaded if needed).
+struct FVec {
+  DBuf own;
+  const float* p = nullptr;
+  FVec(const float* src, size_t n) {
+    if (is_device_ptr(src)) { p = src; return; }
+    own.alloc(sizeof(float) * n);
+    h2d(own.p, src, sizeof(float) * n);
+    p = dp<float>(own);
+  }
+};
+
+void copy_out(float* dst, const void* src, size_t bytes) {
+  if (is_device_ptr(dst)) { d2d(dst, src, bytes); sync(); }
+  else d2h(dst, src, bytes);
+}
+
+}  // namespace
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" {
+
+int64_t parcel_b_learned_num_params(void) { return cnn::kNumParams; }
+
+int parcel_b_learned_create(int nx, int ny, int nz, int coarsen, uint64_t seed, parcel_b_learned* out) {
+  return guarded([&]() -> int {
+    ensure_init();
+    PB_CHECK(out, PARCEL_B_E_ARG, "NULL handle pointer");
+    PB_CHECK(nx > 0 && ny > 0 && nz > 0 && coarsen >= 1, PARCEL_B_E_ARG, "bad grid %d x %d x %d / %d", nx, ny,
+             nz, coarsen);
+    PB_CHECK(nx % coarsen == 0 && ny % coarsen == 0 && nz % coarsen == 0, PARCEL_B_E_ARG,
+             "grid %d x %d x %d is not divisible by the coarsening factor %d", nx, ny, nz, coarsen);
+    auto L = std::make_unique<Learned>();
+    L->nx = nx; L->ny = ny; L->nz = nz; L->c = coarsen;
+    L->g.gx = nx / coarsen; L->g.gy = ny / coarsen; L->g.gz = nz / coarsen;
+    L->net.init(seed);
+    L->loss.alloc(sizeof(double));
+    sync();
+    *out = reinterpret_cast<parcel_b_learned>(L.release());
+    return 0;
+  });
+}
+
+int parcel_b_learned_destroy(parcel_b_learned h) {
+  return guarded([&]() -> int {
+    if (h) {
+      sync();
+      delete reinterpret_cast<Learned*>(h);
+    }
+    return 0;
+  });
+}
+
+int parcel_b_learned_get_params(parcel_b_learned h, float* params, double* target_scale) {
+  return guarded([&]() -> int {
+    PB_CHECK(h, PARCEL_B_E_ARG, "NULL handle");
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    if (params) copy_out(params, L.net.master.p, sizeof(float) * cnn::kNumParams);
+    if (target_scale) *target_scale = L.scale;
+    return 0;
+  });
+}
+
+int parcel_b_learned_set_params(parcel_b_learned h, const float* params, double target_scale) {
+  return guarded([&]() -> int {
+    PB_CHECK(h, PARCEL_B_E_ARG, "NULL handle");
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    if (params) {
+      FVec p(params, cnn::kNumParams);
+      d2d(L.net.master.p, p.p, sizeof(float) * cnn::kNumParams);
+      L.net.repack(stream());
+    }
+    if (target_scale > 0.0) L.scale = target_scale;
+    sync();
+    return 0;
+  });
+}
+
+int parcel_b_learned_forward(parcel_b_learned h, int batch, const float* u, float* y) {
+  return guarded([&]() -> int {
+    PB_CHECK(h && u && y && batch >= 1, PARCEL_B_E_ARG, "bad arguments");
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    const size_t M = (size_t)L.g.V() * batch;
+    L.kern.ensure(L.g, batch, false);
+    FVec uv(u, 2 * M);
+    cnn::to_bf16(2 * M, uv.p, dp<__nv_bfloat16>(L.kern.u), stream());
+    cnn::forward(L.net, L.kern, nullptr, stream());
+    copy_out(y, L.kern.y.p, sizeof(float) * M);
+    return 0;
+  });
+}
+
+int parcel_b_learned_grad(parcel_b_learned h, int batch, const float* u, const float* target, double* loss,
+                          float* grad) {
+  return guarded([&]() -> int {
+    PB_CHECK(h && u && target && batch >= 1, PARCEL_B_E_ARG, "bad arguments");
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    const size_t M = (size_t)L.g.V() * batch;
+    L.kern.ensure(L.g, batch, true);
+    FVec uv(u, 2 * M), tv(target, M);
+    cnn::to_bf16(2 * M, uv.p, dp<__nv_bfloat16>(L.kern.u), stream());
+    cnn::loss_grad(L.net, L.kern, tv.p, 1.f, dp<double>(L.loss), stream());
+    if (loss) d2h(loss, L.loss.p, sizeof(double));
+    if (grad) copy_out(grad, L.net.grad.p, sizeof(float) * cnn::kNumParams);
+    sync();
+    return 0;
+  });
+}
+
+int parcel_b_learned_adam(parcel_b_learned h, double lr) {
+  return guarded([&]() -> int {
+    PB_CHECK(h, PARCEL_B_E_ARG, "NULL handle");
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    cnn::adam(L.net, (float)lr, stream());
+    sync();
+    return 0;
+  });
+}
+
+int parcel_b_learned_collect(parcel_b_learned h, const parcel_b_input* prm, const parcel_b_crs* A, const double* b,
+                             int max_pairs, int* npairs) {
+  return guarded([&]() -> int {
+    ensure_init();
+    PB_CHECK(h && b, PARCEL_B_E_ARG, "bad arguments");
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    validate(A);
+    check_grid(L, A);
+    Options o = resolve_options(prm);
+    PB_CHECK(o.solver == PARCEL_B_SOLVER_GMRES, PARCEL_B_E_UNSUPPORTED,
+             "training pairs come from the plain GMRES solve (solver %d given)", o.solver);
+    o.flexible = false;
+    cudaStream_t st = stream();
+    System<double> S;
+    build_system<double>(o, *A, is_device_ptr(A->val), S);
+    DBuf dhat;
+    make_dhat(L, S.Anat, dhat);
+    const int n = A->n, np = S.np;
+    const int64_t V = L.g.V();
+    NatVec bv(b, n, is_device_ptr(b));
+    DBuf bi(sizeof(double) * np), xi(sizeof(double) * np);
+    PB_CUDA(cudaMemsetAsync(bi.p, 0, sizeof(double) * np, st));
+    PB_CUDA(cudaMemsetAsync(xi.p, 0, sizeof(double) * np, st));
+    if (S.permuted) scatter_perm<double>(n, dp<double>(bi), bv.p, dp<int>(S.pos), st);
+    else d2d(bi.p, bv.p, sizeof(double) * n);
+    const int cap = std::max(1, max_pairs);
+    std::vector<DBuf> xs;
+    xs.emplace_back(sizeof(double) * np);   // x_0 = 0
+    PB_CUDA(cudaMemsetAsync(xs.back().p, 0, sizeof(double) * np, st));
+    std::function<void(int)> hook = [&](int) {
+      if ((int)xs.size() < cap + 1) {
+        xs.emplace_back(sizeof(double) * np);
+        d2d(xs.back().p, xi.p, sizeof(double) * np);
+      }
+    };
+    o.on_cycle = &hook;
+    DBuf hist(sizeof(double) * (o.itrmax + 2));
+    SolveOut so = run_krylov<double>(o, S, dp<double>(bi), dp<double>(xi), dp<double>(hist));
+    PB_CHECK(so.iret == 0, PARCEL_B_E_BREAKDOWN, "the plain solve did not converge (iret %d): no training pairs",
+             so.iret);
+    const double bnorm = std::sqrt(dev_dot<double>(np, dp<double>(bi), dp<double>(bi)));
+    DBuf r(sizeof(double) * np), z1(sizeof(double) * np), t(sizeof(double) * np), e(sizeof(double) * np);
+    DBuf tc(sizeof(float) * V), ec(sizeof(float) * V), scal_t(sizeof(float) * 2), scal_e(sizeof(float) * 2);
+    DBuf part(sizeof(double) * red_blocks()), ticket(sizeof(unsigned));
+    PB_CUDA(cudaMemsetAsync(ticket.p, 0, sizeof(unsigned), st));
+    PB_CUDA(cudaMemsetAsync(r.p, 0, sizeof(double) * np, st));
+    PB_CUDA(cudaMemsetAsync(t.p, 0, sizeof(double) * np, st));
+    const int* pos = S.permuted ? dp<int>(S.pos) : nullptr;
+    int added = 0;
+    for (const DBuf& xk : xs) {
+      if (added >= cap) break;
+      spmv<double, double>(S.A, dp<double>(xk), dp<double>(r), SPMV_RES, dp<double>(bi), nullptr, st);
+      const double rel = std::sqrt(dev_dot<double>(np, dp<double>(r), dp<double>(r))) / bnorm;
+      if (!(rel > 1e-8)) continue;   // converged iterates carry no error to learn
+      S.M.apply(np, dp<double>(r), dp<double>(z1), nullptr, st);
+      spmv<double, double>(S.A, dp<double>(z1), dp<double>(t), SPMV_RES, dp<double>(r), nullptr, st);
+      lincomb<double>(np, dp<double>(e), dp<double>(xi), cimm(1.0), dp<double>(xk), cimm(-1.0), dp<double>(z1),
+                      cimm(-1.0), nullptr, st);
+      cnn::restrict_to_coarse<double>(L.nx, L.ny, L.nz, L.c, dp<double>(t), pos, dp<float>(tc), dp<float>(scal_t),
+                                      dp<double>(part), dp<unsigned>(ticket), nullptr, st);
+      cnn::restrict_to_coarse<double>(L.nx, L.ny, L.nz, L.c, dp<double>(e), pos, dp<float>(ec), dp<float>(scal_e),
+                                      dp<double>(part), dp<unsigned>(ticket), nullptr, st);
+      L.pu.emplace_back(sizeof(__nv_bfloat16) * 2 * V);
+      L.pt.emplace_back(sizeof(float) * V);
+      cnn::prep_input(L.g, dp<float>(tc), dp<float>(dhat), dp<float>(scal_t), dp<__nv_bfloat16>(L.pu.back()),
+                      nullptr, st);
+      cnn::scale_by(V, dp<float>(ec), dp<float>(scal_t), dp<float>(L.pt.back()), st);
+      ++added;
+    }
+    sync();
+    if (npairs) *npairs = added;
+    return 0;
+  });
+}
+
+int parcel_b_learned_num_pairs(parcel_b_learned h) {
+  return h ? (int)reinterpret_cast<Learned*>(h)->pu.size() : 0;
+}
+
+int parcel_b_learned_train(parcel_b_learned h, int steps, int batch, double lr, uint64_t seed, double* first_loss,
+                           double* last_loss) {
+  return guarded([&]() -> int {
+    PB_CHECK(h && steps >= 1 && batch >= 1 && lr > 0.0, PARCEL_B_E_ARG, "bad arguments");
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    const int np = (int)L.pu.size();
+    PB_CHECK(np > 0, PARCEL_B_E_ARG, "no training pairs: call parcel_b_learned_collect first");
+    cudaStream_t st = stream();
+    const int64_t V = L.g.V();
+    if (L.scale <= 0.0) {
+      double q = 0.0;
+      std::vector<float> hv((size_t)V);
+      for (const DBuf& p : L.pt) {
+        d2h(hv.data(), p.p, sizeof(float) * V);
+        for (float v : hv) q += (double)v * v;
+      }
+      const double rms = std::sqrt(q / ((double)V * np));
+      L.scale = rms > 0.0 ? 1.0 / rms : 1.0;
+    }
+    L.train.ensure(L.g, batch, true);
+    L.tgt.alloc(sizeof(float) * V * batch);
+    std::mt19937_64 rng(seed);
+    for (int s = 0; s < steps; ++s) {
+      for (int b = 0; b < batch; ++b) {
+        const int k = (int)(rng() % (uint64_t)np);
+        d2d(dp<char>(L.train.u) + sizeof(__nv_bfloat16) * 2 * V * b, L.pu[k].p, sizeof(__nv_bfloat16) * 2 * V);
+        d2d(dp<float>(L.tgt) + V * b, L.pt[k].p, sizeof(float) * V);
+      }
+      cnn::loss_grad(L.net, L.train, dp<float>(L.tgt), (float)L.scale, dp<double>(L.loss), st);
+      if (s == 0 && first_loss) d2h(first_loss, L.loss.p, sizeof(double));
+      cnn::adam(L.net, (float)lr, st);
+    }
+    if (last_loss) {
+      cnn::loss_grad(L.net, L.train, dp<float>(L.tgt), (float)L.scale, dp<double>(L.loss), st);
+      d2h(last_loss, L.loss.p, sizeof(double));
+    }
+    sync();
+    return 0;
+  });
+}
+
+int parcel_b_solve_learned(const parcel_b_input* prm, const parcel_b_crs* A, parcel_b_learned h, const double* b,
+                           double* x, double* reshistory, int* niter, int* iret) {
+  int rc = guarded([&]() -> int {
+    ensure_init();
+    validate(A);
+    PB_CHECK(b && x, PARCEL_B_E_ARG, "b and x must not be NULL");
+    Learned* L = reinterpret_cast<Learned*>(h);
+    if (L) check_grid(*L, A);
+    Options o = resolve_options(prm);
+    PB_CHECK(o.solver == PARCEL_B_SOLVER_GMRES, PARCEL_B_E_UNSUPPORTED,
+             "the learned stage runs inside flexible GMRES (solver %d given)", o.solver);
+    PB_CHECK(o.precon >= 0 && o.precon <= 2, PARCEL_B_E_UNSUPPORTED, "ipreflag=%d is not provided", o.precon);
+    o.flexible = true;
+    const double t0 = now_s();
+    const bool dev = is_device_ptr(A->val);
+    const bool xdev = is_device_ptr(x);
+    parcel_b_stats stt;
+    memset(&stt, 0, sizeof(stt));
+    NatVec bv(b, A->n, is_device_ptr(b)), xv(x, A->n, xdev);
+    std::vector<double> hist;
+    SolveOut so;
+    double t1 = t0;
+    if (o.inner == PARCEL_B_INNER_FP32_REFINE) {
+      std::unique_ptr<LearnedStage<float>> stage;
+      std::function<void(System<float>&)> attach = [&](System<float>& S) {
+        if (L) {
+          stage = std::make_unique<LearnedStage<float>>(L, S);
+          S.extra = stage.get();
+        }
+      };
+      MixedResult mr = solve_mixed(o, *A, dev, bv.p, xv.p, hist, &t1, &attach);
+      so.niter = mr.niter;
+      so.iret = mr.iret;
+      so.launches = mr.launches;
+      stt.refine_steps = mr.refine_steps;
+      stt.true_relres_dd = mr.true_relres_dd;
+      stt.ilu_levels_max = mr.ilu_levels_max;
+      stt.ilu_nblocks = mr.ilu_nblocks;
+    } else {
+      System<double> S;
+      build_system<double>(o, *A, dev, S);
+      std::unique_ptr<LearnedStage<double>> stage;
+      if (L) {
+        stage = std::make_unique<LearnedStage<double>>(L, S);
+        S.extra = stage.get();
+      }
+      so = solve_on_system(o, S, bv.p, xv.p, hist, &t1);
+      stt.ilu_levels_max = S.ilu_levels_max;
+      stt.ilu_nblocks = S.ilu_nblocks;
+    }
+    // The true FP64 residual decides; the plain PGMRES/ILU path finishes what the
+    // learned solve left.
+    DevMat<double> An;
+    An.n = A->n; An.nnz = A->nnz; An.rbase = 1; An.cbase = A->istart;
+    DBuf up_rp, up_ci, up_va;
+    if (dev) {
+      An.rowptr = A->rowptr; An.col = A->col; An.val = A->val;
+    } else {
+      up_rp.alloc(sizeof(int) * (A->n + 1)); h2d(up_rp.p, A->rowptr, sizeof(int) * (A->n + 1));
+      up_ci.alloc(sizeof(int) * A->nnz); h2d(up_ci.p, A->col, sizeof(int) * A->nnz);
+      up_va.alloc(sizeof(double) * A->nnz); h2d(up_va.p, A->val, sizeof(double) * A->nnz);
+      An.rowptr = dp<int>(up_rp); An.col = dp<int>(up_ci); An.val = dp<double>(up_va);
+    }
+    double rel = true_relres(An, bv.p, xv.p);
+    if (!(rel < o.rtol) && so.iret >= 0 && so.niter < o.itrmax) {
+      Options op = resolve_options(prm);
+      op.itrmax = o.itrmax - so.niter;
+      System<double> S2;
+      build_system<double>(op, *A, dev, S2);
+      std::vector<double> h2;
+      SolveOut s2 = solve_on_system(op, S2, bv.p, xv.p, h2, nullptr);
+      for (double v : h2) hist.push_back(v);
+      so.niter += s2.niter;
+      so.iret = s2.iret;
+      so.launches += s2.launches;
+      stt.fallback = 1;
+      rel = true_relres(An, bv.p, xv.p);
+    }
+    stt.true_relres = rel;
+    const double t2 = now_s();
+    if (!xdev) d2h(x, xv.p, sizeof(double) * A->n);
+    if (reshistory && !hist.empty()) {
+      size_t cnt = std::min<size_t>(hist.size(), (size_t)std::max(o.itrmax, 0));
+      if (is_device_ptr(reshistory)) { h2d(reshistory, hist.data(), sizeof(double) * cnt); sync(); }
+      else memcpy(reshistory, hist.data(), sizeof(double) * cnt);
+    }
+    if (niter) *niter = so.niter;
+    if (iret) *iret = so.iret;
+    stt.setup_s = t1 - t0;
+    stt.solve_s = t2 - t1;
+    stt.total_s = now_s() - t0;
+    stt.niter = so.niter;
+    stt.iret = so.iret;
+    stt.kernel_launches = so.launches;
+    set_stats(stt);
+    return so.iret < 0 ? so.iret : 0;
+  });
+  if (rc < 0 && iret) *iret = rc;
+  return rc;
+}
+
+}  // extern "C"

@@ -45,10 +45,12 @@ void residual_dd(const DevMat<double>& A, const double* val_lo, const double* x_
 }
 
 MixedResult solve_mixed(const Options& o, const parcel_b_crs& A, bool dev, const double* b,
-                        double* x, std::vector<double>& hist, double* setup_t) {
+                        double* x, std::vector<double>& hist, double* setup_t,
+                        const std::function<void(System<float>&)>* attach) {
   cudaStream_t st = stream();
   System<float> S;
   build_system<float>(o, A, dev, S);
+  if (attach) (*attach)(S);
   MixedResult res;
   res.ilu_levels_max = S.ilu_levels_max;
   res.ilu_nblocks = S.ilu_nblocks;

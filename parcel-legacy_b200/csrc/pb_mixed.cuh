@@ -25,8 +25,11 @@ struct MixedResult {
 // FP32 Krylov solves (PCG / BiCGStab / GMRES with an FP32 block-Jacobi ILU or Jacobi
 // preconditioner) inside an FP64 iterative-refinement loop whose residual is computed in
 // FP64 or double-double.  b, x: natural-layout device arrays; x in/out.
+// `attach`, if given, is called once on the FP32 system after it is built (it may set
+// S.extra, which turns the inner GMRES into flexible GMRES).
 MixedResult solve_mixed(const Options& o, const parcel_b_crs& A, bool dev, const double* b,
-                        double* x, std::vector<double>& hist, double* setup_t);
+                        double* x, std::vector<double>& hist, double* setup_t,
+                        const std::function<void(System<float>&)>* attach = nullptr);
 
 // CA-GMRES(s, t) (KSP_pCAGMRES, src/pcagmres.f90:1557-2518) in FP64.
 SolveOut solve_cagmres(const Options& o, System<double>& S, const double* b, double* x,

@@ -379,6 +379,17 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
   const int64_t ldv = (np + 31) & ~int64_t(31);
   const size_t vb = sizeof(T) * np;
   DBuf r(vb), Vb(sizeof(T) * ldv * (m + 1)), pv(vb), w(vb), v0(vb), x0(vb);
+  // Flexible GMRES keeps z_j = M_j^-1 v_j (the preconditioner may change between
+  // columns) and updates x with Z y instead of M^-1 V y.
+  const bool flex = o.flexible || S.extra != nullptr;
+  DBuf Zb;
+  if (flex) Zb.alloc(sizeof(T) * ldv * m);
+  T* Z = dp<T>(Zb);
+  auto precon = [&](const T* in, T* out, const int* gate) {
+    S.M.apply(np, in, out, gate, st);
+    if (S.extra) S.extra->apply(S, in, out, gate, st);
+  };
+  const int precon_launches = 1 + (S.extra ? S.extra->launches() : 0);
   DBuf hb(sizeof(double) * (m + 1) * m), eb(sizeof(double) * (m + 1)), csb(sizeof(double) * (m + 1)),
       snb(sizeof(double) * (m + 1)), yb(sizeof(double) * (m + 1));
   T *R = dp<T>(r), *V = dp<T>(Vb), *PV = dp<T>(pv), *Wv = dp<T>(w), *V0 = dp<T>(v0),
@@ -426,16 +437,17 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
         lincomb<T>(np, Vj, R, cdev(&K->tmp[0]), nullptr, cimm(0), nullptr, cimm(0), gskip, st);
         ++per_cycle;
       }
-      S.M.apply(np, Vj, PV, gskip, st);
-      ++per_cycle;
+      T* Pj = flex ? Z + (size_t)(j - 1) * ldv : PV;
+      precon(Vj, Pj, gskip);
+      per_cycle += precon_launches;
       if (o.gs == PARCEL_B_GS_CGS) {
-        spmv<T, T>(S.A, PV, Wv, SPMV_Y, nullptr, gskip, st);
+        spmv<T, T>(S.A, Pj, Wv, SPMV_Y, nullptr, gskip, st);
         multidot<T>(np, j, Wv, V, ldv, red(EPI_GM_HCGS, 0, j), gskip, st);
         cgs_update<T>(np, j, Wv, V, ldv, dp<double>(hb) + (size_t)(j - 1) * (m + 1), red(EPI_GM_NORM, 0, j),
                       gskip, st);
         per_cycle += 3;
       } else if (fused_mgs) {
-        spmv<T, T>(S.A, PV, Wv, SPMV_Y, nullptr, gskip, st);
+        spmv<T, T>(S.A, Pj, Wv, SPMV_Y, nullptr, gskip, st);
         MgsArgs<T> ma;
         ma.np = np; ma.j = j; ma.w = Wv; ma.V = V; ma.ldv = ldv;
         ma.vnext = (j < m) ? V + (size_t)j * ldv : nullptr;
@@ -448,7 +460,7 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
         per_cycle += 2;
       } else {
         int sa1[2] = {0, 0}, sb1[2] = {2, 0};   // <w, v_1>
-        spmv_dot<T, T>(S.A, PV, Wv, SPMV_Y, nullptr, V, 1, sa1, sb1, red(EPI_GM_H, 1, j), gskip, st);
+        spmv_dot<T, T>(S.A, Pj, Wv, SPMV_Y, nullptr, V, 1, sa1, sb1, red(EPI_GM_H, 1, j), gskip, st);
         ++per_cycle;
         for (int k = 1; k <= j; ++k) {
           const T* Vk = V + (size_t)(k - 1) * ldv;
@@ -468,11 +480,16 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
     }
     // update_xVec: y = H^-1 e; v0 = V y; x0 = M^-1 v0; x = x0 + x
     gm_backsolve(dp<double>(hb), dp<double>(eb), dp<double>(yb), m, K, gdone, st);
-    sum_vec<T>(np, V0, V, ldv, dp<double>(yb), K, gdone, st);
-    S.M.apply(np, V0, X0, gdone, st);
+    if (flex) {
+      sum_vec<T>(np, X0, Z, ldv, dp<double>(yb), K, gdone, st);
+    } else {
+      sum_vec<T>(np, V0, V, ldv, dp<double>(yb), K, gdone, st);
+      S.M.apply(np, V0, X0, gdone, st);
+      ++per_cycle;
+    }
     lincomb<T>(np, x, X0, cimm(1.0), x, cimm(1.0), nullptr, cimm(0), gdone, st);
     gm_post(K, m, o.itrmax, st);
-    per_cycle += 5;
+    per_cycle += 4;
   };
   GraphRunner G;
   const int max_cycles = o.itrmax / m + 2;
@@ -480,6 +497,7 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
     if (read_done(K, st)) break;
     G.launch(cycle, o.use_graphs, st);
     launches += per_cycle;
+    if (o.on_cycle) (*o.on_cycle)(c);
   }
   KState h = read_state(K);
   int merr_h = 0;

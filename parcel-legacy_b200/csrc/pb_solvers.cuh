@@ -2,6 +2,7 @@
 #pragma once
 
 #include <chrono>
+#include <functional>
 #include <memory>
 
 #include "pb_blas.cuh"
@@ -29,6 +30,8 @@ struct Options {
   int independ_nvec = 1;
   bool use_graphs = true;
   bool fused_mgs = true;
+  bool flexible = false;                               // GMRES: flexible variant (keeps M^-1 v_j)
+  const std::function<void(int)>* on_cycle = nullptr;  // GMRES: called after each restart cycle
 };
 
 Options resolve_options(const parcel_b_input* p);
@@ -41,6 +44,17 @@ struct Precon {
   IluDev<T> ilu;
   int launches_per_apply() const { return 1; }
   void apply(int64_t np, const T* r, T* s, const int* gate, cudaStream_t st) const;
+};
+
+template <class T>
+struct System;
+
+// An extra preconditioner stage after M (flexible GMRES only): z <- z + stage(r, z).
+template <class T>
+struct ExtraStage {
+  virtual ~ExtraStage() = default;
+  virtual void apply(const System<T>& S, const T* r, T* z, const int* gate, cudaStream_t st) = 0;
+  virtual int launches() const = 0;
 };
 
 // Everything a solve needs on the device, in the iteration layout.
@@ -58,6 +72,7 @@ struct System {
   DBuf Aval_T;          // natural values cast to T (FP32 path, no permutation)
   DBuf pos, rowAt, lev; // layout maps (block Jacobi)
   Precon<T> M;
+  ExtraStage<T>* extra = nullptr;   // not owned
   int ilu_levels_max = 0;
   int ilu_nblocks = 0;
 };

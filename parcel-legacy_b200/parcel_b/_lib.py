@@ -51,7 +51,7 @@ class Stats(C.Structure):
                 ("true_relres", C.c_double), ("true_relres_dd", C.c_double),
                 ("niter", C.c_int), ("iret", C.c_int), ("refine_steps", C.c_int),
                 ("kernel_launches", C.c_int), ("ilu_levels_max", C.c_int),
-                ("ilu_nblocks", C.c_int), ("reserved", C.c_int * 6)]
+                ("ilu_nblocks", C.c_int), ("fallback", C.c_int), ("reserved", C.c_int * 5)]
 
 
 P = C.c_void_p
@@ -96,6 +96,18 @@ SIGNATURES = {
     "parcel_b_dot_noalloc": (C.c_int, [C.c_int64, P, P, P, P]),
     "parcel_b_residual_dd": (C.c_int, [C.POINTER(Crs), P, P, P, P, P, P]),
     "parcel_b_bench_kernels": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, DP, DP]),
+    "parcel_b_learned_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(P)]),
+    "parcel_b_learned_destroy": (C.c_int, [P]),
+    "parcel_b_learned_num_params": (C.c_int64, []),
+    "parcel_b_learned_get_params": (C.c_int, [P, P, DP]),
+    "parcel_b_learned_set_params": (C.c_int, [P, P, C.c_double]),
+    "parcel_b_learned_forward": (C.c_int, [P, C.c_int, P, P]),
+    "parcel_b_learned_grad": (C.c_int, [P, C.c_int, P, P, DP, P]),
+    "parcel_b_learned_adam": (C.c_int, [P, C.c_double]),
+    "parcel_b_learned_collect": (C.c_int, [P, C.POINTER(Input), C.POINTER(Crs), P, C.c_int, IP]),
+    "parcel_b_learned_num_pairs": (C.c_int, [P]),
+    "parcel_b_learned_train": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_uint64, DP, DP]),
+    "parcel_b_solve_learned": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), P, P, P, P, IP, IP]),
 }
 
 _lib = None

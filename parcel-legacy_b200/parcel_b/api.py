@@ -168,3 +168,73 @@ def solve(A, b, x0=None, *, rowptr=None, col=None, val=None, **options):
         raise RuntimeError(f"parcel_b_solve failed: {_lib.last_error()}")
     return {"x": x, "reshistory": hist[: niter.value].copy(), "niter": niter.value, "iret": iret.value,
             "stats": _lib.last_stats()}
+
+
+class Learned:
+    """The learned coarse-grid preconditioner stage (no counterpart in the reference): a
+    handle on the network for an nx x ny x nz grid coarsened by ``coarsen``."""
+
+    def __init__(self, nx, ny, nz, coarsen, seed=0):
+        self._L = load()
+        h = C.c_void_p()
+        if self._L.parcel_b_learned_create(int(nx), int(ny), int(nz), int(coarsen), int(seed), C.byref(h)) != 0:
+            raise RuntimeError(f"parcel_b_learned_create failed: {_lib.last_error()}")
+        self.handle = h
+
+    def collect(self, A, b, max_pairs=16, **options):
+        """Appends training pairs from the plain GMRES solve of A x = b (options as in solve)."""
+        p = new_input(**options)
+        S = crs_struct(A)
+        n = C.c_int(0)
+        if self._L.parcel_b_learned_collect(self.handle, C.byref(p), C.byref(S), _ptr(b), int(max_pairs),
+                                            C.byref(n)) != 0:
+            raise RuntimeError(f"parcel_b_learned_collect failed: {_lib.last_error()}")
+        return n.value
+
+    def num_pairs(self):
+        return self._L.parcel_b_learned_num_pairs(self.handle)
+
+    def train(self, steps, batch=4, lr=1e-3, seed=0):
+        """Adam on the collected pairs; returns (first loss, last loss)."""
+        f, l = C.c_double(), C.c_double()
+        if self._L.parcel_b_learned_train(self.handle, int(steps), int(batch), float(lr), int(seed), C.byref(f),
+                                          C.byref(l)) != 0:
+            raise RuntimeError(f"parcel_b_learned_train failed: {_lib.last_error()}")
+        return f.value, l.value
+
+    def params(self):
+        flat = np.zeros(self._L.parcel_b_learned_num_params(), np.float32)
+        s = C.c_double()
+        self._L.parcel_b_learned_get_params(self.handle, flat.ctypes.data, C.byref(s))
+        return flat, s.value
+
+    def set_params(self, flat, scale=0.0):
+        flat = np.ascontiguousarray(flat, np.float32)
+        if self._L.parcel_b_learned_set_params(self.handle, flat.ctypes.data, float(scale)) != 0:
+            raise RuntimeError(_lib.last_error())
+
+    def __del__(self):
+        try:
+            self._L.parcel_b_learned_destroy(self.handle)
+        except Exception:
+            pass
+
+
+def solve_learned(A, b, learned, x0=None, **options):
+    """Flexible GMRES with the block-Jacobi ILU / Jacobi preconditioner of ``options`` and
+    the learned stage ``learned`` (None: the preconditioner alone).  Returns the dict of
+    ``solve``; ``stats["fallback"]`` is 1 when the plain PGMRES path finished the solve."""
+    L = load()
+    p = new_input(**options)
+    S = crs_struct(A)
+    x = np.zeros(A.n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+    itrmax = p.itrmax if p.itrmax > 0 else 100
+    hist = np.zeros(itrmax)
+    niter, iret = C.c_int(0), C.c_int(0)
+    h = learned.handle if learned is not None else None
+    rc = L.parcel_b_solve_learned(C.byref(p), C.byref(S), h, _ptr(b), _ptr(x), _ptr(hist), C.byref(niter),
+                                  C.byref(iret))
+    if rc < 0:
+        raise RuntimeError(f"parcel_b_solve_learned failed: {_lib.last_error()}")
+    return {"x": x, "reshistory": hist[: niter.value].copy(), "niter": niter.value, "iret": iret.value,
+            "stats": _lib.last_stats()}
