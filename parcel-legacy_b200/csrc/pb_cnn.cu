@@ -649,7 +649,7 @@ __device__ __forceinline__ void lin1(int i, int c, int G, int& lo, int& hi, floa
 template <class T>
 __global__ void __launch_bounds__(256)
     k_prolong(int nx, int ny, int nz, int c, int64_t np, const float* __restrict__ yc, const float* __restrict__ scal,
-              float scale, const int* __restrict__ rowAt, T* __restrict__ dst, const int* gate) {
+              float scale, const int* __restrict__ rowAt, T* __restrict__ dst, bool add, const int* gate) {
   if (gated(gate)) return;
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= np) return;
@@ -670,7 +670,53 @@ __global__ void __launch_bounds__(256)
   const float c0 = c00 * (1.f - wy) + c10 * wy;
   const float c1 = c01 * (1.f - wy) + c11 * wy;
   const float val = c0 * (1.f - wx) + c1 * wx;
-  dst[p] = dst[p] + (T)(scale * scal[1] * val);
+  const T v = (T)(scale * scal[1] * val);
+  dst[p] = add ? dst[p] + v : v;
+}
+
+// alpha = <t, q> / <q, q> (0 when q = 0): the step length that minimises ||t - alpha q||.
+// Per-block partials, the last block to finish sums them in block order.
+template <class T>
+__global__ void __launch_bounds__(kRedThreads)
+    k_alpha(int64_t n, const T* __restrict__ t, const T* __restrict__ q, double* __restrict__ part,
+            unsigned* __restrict__ ticket, double* __restrict__ alpha, const int* gate) {
+  if (gated(gate)) return;
+  __shared__ double red[2][kRedThreads / 32];
+  __shared__ bool last;
+  double tq = 0.0, qq = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double a = (double)t[i], b = (double)q[i];
+    tq += a * b;
+    qq += b * b;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    tq += __shfl_xor_sync(kFull, tq, o);
+    qq += __shfl_xor_sync(kFull, qq, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = tq;
+    red[1][threadIdx.x >> 5] = qq;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) { s0 += red[0][w]; s1 += red[1][w]; }
+    part[2 * blockIdx.x] = s0;
+    part[2 * blockIdx.x + 1] = s1;
+    __threadfence();
+    last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  double s0 = 0.0, s1 = 0.0;
+  for (unsigned b = 0; b < gridDim.x; ++b) {
+    s0 += __ldcg(part + 2 * b);
+    s1 += __ldcg(part + 2 * b + 1);
+  }
+  *alpha = s1 > 0.0 ? s0 / s1 : 0.0;
+  *ticket = 0u;
 }
 
 __global__ void __launch_bounds__(256)
@@ -865,9 +911,16 @@ void restrict_to_coarse(int nx, int ny, int nz, int c, const T* src, const int* 
 }
 
 template <class T>
-void prolong_add(int nx, int ny, int nz, int c, int64_t np, const float* yc, const float* scal, float scale,
-                 const int* rowAt, T* dst, const int* gate, cudaStream_t st) {
-  k_prolong<T><<<blocks_for(np), 256, 0, st>>>(nx, ny, nz, c, np, yc, scal, scale, rowAt, dst, gate);
+void prolong(int nx, int ny, int nz, int c, int64_t np, const float* yc, const float* scal, float scale,
+             const int* rowAt, T* dst, bool add, const int* gate, cudaStream_t st) {
+  k_prolong<T><<<blocks_for(np), 256, 0, st>>>(nx, ny, nz, c, np, yc, scal, scale, rowAt, dst, add, gate);
+  PB_CUDA(cudaGetLastError());
+}
+
+template <class T>
+void step_length(int64_t n, const T* t, const T* q, double* part, unsigned* ticket, double* alpha, const int* gate,
+                 cudaStream_t st) {
+  k_alpha<T><<<red_blocks(), kRedThreads, 0, st>>>(n, t, q, part, ticket, alpha, gate);
   PB_CUDA(cudaGetLastError());
 }
 
@@ -882,10 +935,14 @@ template void restrict_to_coarse<double>(int, int, int, int, const double*, cons
                                          unsigned*, const int*, cudaStream_t);
 template void restrict_to_coarse<float>(int, int, int, int, const float*, const int*, float*, float*, double*,
                                         unsigned*, const int*, cudaStream_t);
-template void prolong_add<double>(int, int, int, int, int64_t, const float*, const float*, float, const int*, double*,
-                                  const int*, cudaStream_t);
-template void prolong_add<float>(int, int, int, int, int64_t, const float*, const float*, float, const int*, float*,
-                                 const int*, cudaStream_t);
+template void prolong<double>(int, int, int, int, int64_t, const float*, const float*, float, const int*, double*,
+                              bool, const int*, cudaStream_t);
+template void prolong<float>(int, int, int, int, int64_t, const float*, const float*, float, const int*, float*,
+                             bool, const int*, cudaStream_t);
+template void step_length<double>(int64_t, const double*, const double*, double*, unsigned*, double*, const int*,
+                                  cudaStream_t);
+template void step_length<float>(int64_t, const float*, const float*, double*, unsigned*, double*, const int*,
+                                 cudaStream_t);
 
 }  // namespace cnn
 }  // namespace pb

@@ -7,7 +7,10 @@
 //     t  = r - A z                          (SpMV, iteration layout)
 //     tc = R t   (mean over c^3 blocks, coarse grid),  sigma = rms(tc)
 //     y  = Net([tc / sigma, dhat])          (6 conv layers, 3^3 taps, BF16, FP32 sums)
-//     z += (sigma / s) P y                  (P: cell-centred trilinear interpolation)
+//     c  = (sigma / s) P y                  (P: cell-centred trilinear interpolation)
+//     z += alpha c,  alpha = <t, A c> / <A c, A c>   (the step that minimises ||t - alpha A c||,
+//                                                     so the stage never raises the residual
+//                                                     left by the ILU step)
 //
 // dhat is the normalised coarse mean of log(diag A): the network sees the operator's
 // local coefficient through the matrix itself.  s is the target scale fixed from the
@@ -103,13 +106,19 @@ void prep_input(const Geo& g, const float* tc, const float* dhat, const float* s
 //   restrict: tc = box mean of src over c^3 blocks; scal[0] = 1/rms(tc) (0 if tc == 0),
 //             scal[1] = rms(tc).  pos maps natural rows to iteration positions (NULL:
 //             identity).  Uses `part` (>= red_blocks() doubles) and `ticket` (zero).
-//   prolong:  dst[p] += scale * scal[1] * trilinear(yc)(natural row rowAt[p]).
+//   prolong:  dst[p] (+)= scale * scal[1] * trilinear(yc)(natural row rowAt[p]); positions
+//             with rowAt[p] < 0 (layout padding) are left untouched.
 template <class T>
 void restrict_to_coarse(int nx, int ny, int nz, int c, const T* src, const int* pos, float* tc,
                         float* scal, double* part, unsigned* ticket, const int* gate, cudaStream_t st);
 template <class T>
-void prolong_add(int nx, int ny, int nz, int c, int64_t np, const float* yc, const float* scal, float scale,
-                 const int* rowAt, T* dst, const int* gate, cudaStream_t st);
+void prolong(int nx, int ny, int nz, int c, int64_t np, const float* yc, const float* scal, float scale,
+             const int* rowAt, T* dst, bool add, const int* gate, cudaStream_t st);
+// *alpha = <t, q> / <q, q> (0 if q = 0), deterministic; part >= 2 red_blocks() doubles,
+// ticket zero on entry and on exit.
+template <class T>
+void step_length(int64_t n, const T* t, const T* q, double* part, unsigned* ticket, double* alpha, const int* gate,
+                 cudaStream_t st);
 
 // Coarse mean of log|diag A| over c^3 blocks (natural CRS on the device, 1-based row
 // pointers, column base cbase).  Host normalisation follows.

@@ -57,11 +57,13 @@ void make_dhat(const Learned& L, const DevMat<double>& A, DBuf& out) {
   h2d(out.p, h.data(), sizeof(float) * V);
 }
 
-// z += (sigma / s) P Net([R (r - A z) / sigma, dhat])
+// c = (sigma / s) P Net([R t / sigma, dhat]) with t = r - A z;  z += alpha c with the
+// step alpha that minimises ||t - alpha A c||: a correction the network gets wrong (an input
+// unlike its training pairs) is scaled down instead of spoiling the Krylov basis.
 template <class T>
 struct LearnedStage final : ExtraStage<T> {
   const Learned* L;
-  DBuf dhat, t, tc, scal, part, ticket;
+  DBuf dhat, t, cf, q, alpha, tc, scal, part, ticket;
   cnn::Acts acts;
   const int* pos = nullptr;
   const int* rowAt = nullptr;
@@ -74,11 +76,14 @@ struct LearnedStage final : ExtraStage<T> {
       pos = dp<int>(S.pos);
       rowAt = dp<int>(S.rowAt);
     }
-    t.alloc(sizeof(T) * np);
-    PB_CUDA(cudaMemsetAsync(t.p, 0, sizeof(T) * np, st));
+    for (DBuf* b : {&t, &cf, &q}) {
+      b->alloc(sizeof(T) * np);
+      PB_CUDA(cudaMemsetAsync(b->p, 0, sizeof(T) * np, st));   // padding positions stay zero
+    }
+    alpha.alloc(sizeof(double));
     tc.alloc(sizeof(float) * L->g.V());
     scal.alloc(sizeof(float) * 2);
-    part.alloc(sizeof(double) * red_blocks());
+    part.alloc(sizeof(double) * 2 * red_blocks());
     ticket.alloc(sizeof(unsigned));
     PB_CUDA(cudaMemsetAsync(ticket.p, 0, sizeof(unsigned), st));
     acts.ensure(L->g, 1, false);
@@ -91,9 +96,13 @@ struct LearnedStage final : ExtraStage<T> {
     cnn::prep_input(L->g, dp<float>(tc), dp<float>(dhat), dp<float>(scal), dp<__nv_bfloat16>(acts.u), gate, st);
     cnn::forward(L->net, acts, gate, st);
     const float inv_s = L->scale > 0.0 ? (float)(1.0 / L->scale) : 1.f;
-    cnn::prolong_add<T>(L->nx, L->ny, L->nz, L->c, np, dp<float>(acts.y), dp<float>(scal), inv_s, rowAt, z, gate, st);
+    cnn::prolong<T>(L->nx, L->ny, L->nz, L->c, np, dp<float>(acts.y), dp<float>(scal), inv_s, rowAt, dp<T>(cf), false,
+                    gate, st);
+    spmv<T, T>(S.A, dp<T>(cf), dp<T>(q), SPMV_Y, nullptr, gate, st);
+    cnn::step_length<T>(np, dp<T>(t), dp<T>(q), dp<double>(part), dp<unsigned>(ticket), dp<double>(alpha), gate, st);
+    lincomb<T>(np, z, z, cimm(1.0), dp<T>(cf), cdev(dp<double>(alpha)), nullptr, cimm(0), gate, st);
   }
-  int launches() const override { return 4 + 6; }
+  int launches() const override { return 13; }
 };
 
 // A host or device float array of n entries as a device pointer (uploaded if needed).
