@@ -200,7 +200,10 @@ def run_ours(args):
     hbm, peak_kind = peaks()
     spmv_bytes = 12 * A.nnz + 4 * (A.n + 1) + 16 * A.n
     achieved = spmv_bytes / (ms_spmv.value * 1e-3) / 1e9
-    ilu_bytes = None
+    # DRAM bytes (read + write) of one k_spmv_sell launch on this workload, from one
+    # `ncu --set full -k regex:k_spmv_sell -s 1 -c 1` capture of `bench.py --kernels-only`:
+    # dram__bytes_read.sum 196.24 MB + dram__bytes_write.sum 5.30 MB (cold cache).
+    spmv_traffic = 196.237568e6 + 5.297664e6
 
     out = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -216,7 +219,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "kernel": "k_spmv_sell<double,double> (sliced-ELLPACK SpMV, level-major layout)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes": int(spmv_bytes),
+                     "peak_kind": peak_kind, "traffic": int(spmv_traffic), "algorithmic_bytes": int(spmv_bytes),
                      "us_per_launch": ms_spmv.value * 1e3},
         "kernels_us": {"spmv": ms_spmv.value * 1e3, "bj_ilu0_apply": ms_pre.value * 1e3},
         "clocks": clocks,
@@ -295,6 +298,109 @@ def run_kernels_only(args):
                       "spmv_gbs": spmv_bytes / (ms_spmv.value * 1e-3) / 1e9, "reps": args.steps}))
 
 
+VD_METRIC = "time-to-1e-10 true rel. residual (s), learned + mixed-precision FGMRES vs plain FP64 PGMRES/BJ-ILU"
+
+
+def run_vardiff(args):
+    """The learned-preconditioner workload: 3D 7-point variable-coefficient diffusion on an
+    N^3 grid (N = 256 by default), coefficient exp(g) with g a Gaussian random field
+    (correlation length 8 cells, variance 2, seed 5), harmonic-mean faces; right-hand
+    sides N(0,1).  Compares, per right-hand side and with every array already on the GPU:
+      plain   FP64 PGMRES(m) + block-Jacobi ILU(0), 64 blocks      (parcel_b_solve)
+      mixed   FP32 FGMRES(m) + FP32 BJ-ILU(0) in FP64 refinement    (parcel_b_solve_learned, no stage)
+      learned the same + the learned coarse-grid stage              (parcel_b_solve_learned)
+    The network is trained beforehand on pairs from plain solves with other right-hand
+    sides (training time reported separately).  Time: CUDA events on the library stream
+    around each synchronous solve call (set-up included)."""
+    import torch
+    from parcel_b import _lib, api, problems
+    L = _lib.load()
+    N, c, m = args.grid, args.coarsen, args.restart
+    g = problems.gaussian_random_field(N, corr_len=8.0, variance=2.0, seed=5)
+    A = problems.vardiff3d(N, np.exp(g))
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    rp, ci, va = t(A.rowptr), t(A.col), t(A.val)
+    S = api.crs_struct(A, rp, ci, va)
+    stream = torch.cuda.ExternalStream(L.parcel_b_get_stream(), device=dev)
+    common = dict(solver=3, ipreflag=2, ILU_method=0, precon_thblock=NBLOCKS, GMRES_m=m, GMRES_GSflag=1,
+                  itrmax=20000, rtolmax=RTOL)
+    hist = np.zeros(20000)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, out
+
+    def plain(bd, x):
+        p = _lib.new_input(**common)
+        n_, i_ = C.c_int(0), C.c_int(0)
+        rc = L.parcel_b_solve(C.byref(p), C.byref(S), bd.data_ptr(), x.data_ptr(), hist.ctypes.data, C.byref(n_),
+                              C.byref(i_))
+        assert rc == 0, _lib.last_error()
+        return n_.value, _lib.last_stats()
+
+    def fgmres(bd, x, h, inner):
+        p = _lib.new_input(inner_precision=inner, inner_rtol=1e-4, max_refine=80, **common)
+        n_, i_ = C.c_int(0), C.c_int(0)
+        rc = L.parcel_b_solve_learned(C.byref(p), C.byref(S), h, bd.data_ptr(), x.data_ptr(), hist.ctypes.data,
+                                      C.byref(n_), C.byref(i_))
+        assert rc == 0, _lib.last_error()
+        return n_.value, _lib.last_stats()
+
+    # training on other right-hand sides
+    t0 = time.perf_counter()
+    net = api.Learned(N, N, N, c, seed=1)
+    for sd in range(100, 100 + args.train_rhs):
+        net.collect(A, problems.rhs_normal(A.n, sd), max_pairs=32, **common)
+    t_collect = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    f_loss, l_loss = net.train(steps=args.train_steps, batch=4, lr=2e-3, seed=3)
+    t_train = time.perf_counter() - t0
+
+    rhs = [t(problems.rhs_normal(A.n, 1000 + k)) for k in range(args.rhs)]
+    x = torch.zeros(A.n, dtype=torch.float64, device=dev)
+    # warm-up (graph capture, allocations)
+    for fn in (lambda: plain(rhs[0], x.zero_()), lambda: fgmres(rhs[0], x.zero_(), None, 1),
+               lambda: fgmres(rhs[0], x.zero_(), net.handle, 1)):
+        fn()
+    clk = Clocks(0)
+    res = {"plain": [], "mixed": [], "learned": []}
+    for k, bd in enumerate(rhs):
+        if k < args.plain_rhs:
+            res["plain"].append(timed(lambda: plain(bd, x.zero_())))
+            res["mixed"].append(timed(lambda: fgmres(bd, x.zero_(), None, 1)))
+        res["learned"].append(timed(lambda: fgmres(bd, x.zero_(), net.handle, 1)))
+    clocks = clk.stop()
+
+    def summ(v):
+        ts = [a for a, _ in v]
+        return {"s_per_rhs": sum(ts) / len(ts), "rhs": len(ts), "iterations": [o[0] for _, o in v],
+                "true_relres_max": max(o[1]["true_relres"] for _, o in v),
+                "fallbacks": sum(o[1]["fallback"] for _, o in v)}
+
+    sp, sm, sl = summ(res["plain"]), summ(res["mixed"]), summ(res["learned"])
+    out = {"metric": VD_METRIC, "value": sl["s_per_rhs"] * args.rhs, "unit": "s", "n_gpus": 1,
+           "steps": args.rhs, "warmup": 1, "ms_per_step": sl["s_per_rhs"] * 1e3, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement, bf16 network",
+           "data": "synthetic",
+           "config": {"workload": f"variable-coefficient 7-pt diffusion {N}^3, k=exp(GRF(corr 8, var 2)), "
+                                  f"{args.rhs} RHS N(0,1), FGMRES({m}) + BJ-ILU(0) {NBLOCKS} blocks, "
+                                  f"learned stage on the {N // c}^3 coarse grid, tol {RTOL}",
+                      "n": A.n, "nnz": A.nnz, "coarsen": c, "l2": "inputs larger than L2"},
+           "plain_fp64": sp, "mixed_no_stage": sm, "learned": sl,
+           "speedup_vs_plain_fp64": sp["s_per_rhs"] / sl["s_per_rhs"],
+           "speedup_mixed_vs_plain_fp64": sp["s_per_rhs"] / sm["s_per_rhs"],
+           "training": {"pairs": net.num_pairs(), "collect_s": t_collect, "train_s": t_train,
+                        "steps": args.train_steps, "loss_first": f_loss, "loss_last": l_loss},
+           "clocks": clocks}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -304,8 +410,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels-only", action="store_true")
     ap.add_argument("--ilu-method", type=int, default=0)
+    ap.add_argument("--workload", default="convdiff128", choices=["convdiff128", "vardiff"],
+                    help="vardiff: the learned-preconditioner comparison (not the default line)")
+    ap.add_argument("--grid", type=int, default=256)
+    ap.add_argument("--coarsen", type=int, default=8)
+    ap.add_argument("--restart", type=int, default=40)
+    ap.add_argument("--rhs", type=int, default=16)
+    ap.add_argument("--plain-rhs", type=int, default=2)
+    ap.add_argument("--train-rhs", type=int, default=4)
+    ap.add_argument("--train-steps", type=int, default=400)
     args = ap.parse_args()
-    if args.kernels_only:
+    if args.workload == "vardiff":
+        run_vardiff(args)
+    elif args.kernels_only:
         run_kernels_only(args)
     elif args.impl == "reference":
         run_reference(args)
