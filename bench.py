@@ -336,22 +336,6 @@ def run_vardiff(args):
         e1.synchronize()
         return e0.elapsed_time(e1) / 1e3, out
 
-    def plain(bd, x):
-        p = _lib.new_input(**common)
-        n_, i_ = C.c_int(0), C.c_int(0)
-        rc = L.parcel_b_solve(C.byref(p), C.byref(S), bd.data_ptr(), x.data_ptr(), hist.ctypes.data, C.byref(n_),
-                              C.byref(i_))
-        assert rc == 0, _lib.last_error()
-        return n_.value, _lib.last_stats()
-
-    def fgmres(bd, x, h, inner):
-        p = _lib.new_input(inner_precision=inner, inner_rtol=1e-4, max_refine=80, **common)
-        n_, i_ = C.c_int(0), C.c_int(0)
-        rc = L.parcel_b_solve_learned(C.byref(p), C.byref(S), h, bd.data_ptr(), x.data_ptr(), hist.ctypes.data,
-                                      C.byref(n_), C.byref(i_))
-        assert rc == 0, _lib.last_error()
-        return n_.value, _lib.last_stats()
-
     # training on other right-hand sides
     t0 = time.perf_counter()
     net = api.Learned(N, N, N, c, seed=1)
@@ -362,39 +346,69 @@ def run_vardiff(args):
     f_loss, l_loss = net.train(steps=args.train_steps, batch=4, lr=2e-3, seed=3)
     t_train = time.perf_counter() - t0
 
-    rhs = [t(problems.rhs_normal(A.n, 1000 + k)) for k in range(args.rhs)]
-    x = torch.zeros(A.n, dtype=torch.float64, device=dev)
-    # warm-up (graph capture, allocations)
-    for fn in (lambda: plain(rhs[0], x.zero_()), lambda: fgmres(rhs[0], x.zero_(), None, 1),
-               lambda: fgmres(rhs[0], x.zero_(), net.handle, 1)):
-        fn()
+    nr = args.rhs
+    B = t(np.stack([problems.rhs_normal(A.n, 1000 + k) for k in range(nr)]))
+    X = torch.zeros_like(B)
+    it = np.zeros(nr, np.int32)
+    ir = np.zeros(nr, np.int32)
+
+    def plain_all(k_rhs):
+        """plain FP64 PGMRES: one set-up (parcel_b_setup), then parcel_b_start per RHS"""
+        p = _lib.new_input(**common)
+        h = C.c_void_p()
+        ts, its, rels = [], [], []
+        Asp = torch.sparse_csr_tensor((rp - 1).long(), (ci - 1).long(), va, size=(A.n, A.n))
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s0.record(stream)
+        assert L.parcel_b_setup(C.byref(p), C.byref(S), C.byref(h)) == 0, _lib.last_error()
+        s1.record(stream)
+        s1.synchronize()
+        setup = s0.elapsed_time(s1) / 1e3
+        for k in range(k_rhs):
+            X[k].zero_()
+            n_, i_ = C.c_int(0), C.c_int(0)
+            dt, rc = timed(lambda: L.parcel_b_start(h, B[k].data_ptr(), X[k].data_ptr(), hist.ctypes.data,
+                                                    C.byref(n_), C.byref(i_)))
+            assert rc == 0, _lib.last_error()
+            ts.append(dt)
+            its.append(n_.value)
+            rels.append(float(torch.linalg.norm(B[k] - Asp @ X[k]) / torch.linalg.norm(B[k])))
+        L.parcel_b_release(h)
+        return {"setup_s": setup, "solve_s_per_rhs": sum(ts) / len(ts), "rhs": len(ts), "iterations": its,
+                "true_relres_max": max(rels), "fallbacks": 0,
+                "s_per_rhs_amortised": setup / nr + sum(ts) / len(ts)}
+
+    def fgmres_all(h, inner):
+        """flexible GMRES (mixed precision when inner = 1), all RHS in one call, one set-up"""
+        p = _lib.new_input(inner_precision=inner, inner_rtol=1e-4, max_refine=80, **common)
+        X.zero_()
+        dt, rc = timed(lambda: L.parcel_b_solve_learned_many(C.byref(p), C.byref(S), h, nr, B.data_ptr(),
+                                                             X.data_ptr(), it.ctypes.data, ir.ctypes.data))
+        assert rc == 0, _lib.last_error()
+        st = _lib.last_stats()
+        return {"setup_s": st["setup_s"], "solve_s_per_rhs": st["solve_s"] / nr, "rhs": nr,
+                "iterations": it.tolist(), "true_relres_max": st["true_relres"], "fallbacks": st["fallback"],
+                "s_per_rhs_amortised": dt / nr, "call_s": dt}
+
+    # warm-up (graph capture, allocations) on a small call of each path
+    fgmres_all(None, 1)
     clk = Clocks(0)
-    res = {"plain": [], "mixed": [], "learned": []}
-    for k, bd in enumerate(rhs):
-        if k < args.plain_rhs:
-            res["plain"].append(timed(lambda: plain(bd, x.zero_())))
-            res["mixed"].append(timed(lambda: fgmres(bd, x.zero_(), None, 1)))
-        res["learned"].append(timed(lambda: fgmres(bd, x.zero_(), net.handle, 1)))
+    sp = plain_all(min(args.plain_rhs, nr))
+    sm = fgmres_all(None, 1)
+    sl = fgmres_all(net.handle, 1)
     clocks = clk.stop()
-
-    def summ(v):
-        ts = [a for a, _ in v]
-        return {"s_per_rhs": sum(ts) / len(ts), "rhs": len(ts), "iterations": [o[0] for _, o in v],
-                "true_relres_max": max(o[1]["true_relres"] for _, o in v),
-                "fallbacks": sum(o[1]["fallback"] for _, o in v)}
-
-    sp, sm, sl = summ(res["plain"]), summ(res["mixed"]), summ(res["learned"])
-    out = {"metric": VD_METRIC, "value": sl["s_per_rhs"] * args.rhs, "unit": "s", "n_gpus": 1,
-           "steps": args.rhs, "warmup": 1, "ms_per_step": sl["s_per_rhs"] * 1e3, "higher_is_better": False,
+    out = {"metric": VD_METRIC, "value": sl["call_s"], "unit": "s", "n_gpus": 1,
+           "steps": nr, "warmup": 1, "ms_per_step": sl["s_per_rhs_amortised"] * 1e3, "higher_is_better": False,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement, bf16 network",
            "data": "synthetic",
            "config": {"workload": f"variable-coefficient 7-pt diffusion {N}^3, k=exp(GRF(corr 8, var 2)), "
-                                  f"{args.rhs} RHS N(0,1), FGMRES({m}) + BJ-ILU(0) {NBLOCKS} blocks, "
+                                  f"{nr} RHS N(0,1), FGMRES({m}) + BJ-ILU(0) {NBLOCKS} blocks, "
                                   f"learned stage on the {N // c}^3 coarse grid, tol {RTOL}",
                       "n": A.n, "nnz": A.nnz, "coarsen": c, "l2": "inputs larger than L2"},
            "plain_fp64": sp, "mixed_no_stage": sm, "learned": sl,
-           "speedup_vs_plain_fp64": sp["s_per_rhs"] / sl["s_per_rhs"],
-           "speedup_mixed_vs_plain_fp64": sp["s_per_rhs"] / sm["s_per_rhs"],
+           "speedup_vs_plain_fp64": sp["s_per_rhs_amortised"] / sl["s_per_rhs_amortised"],
+           "speedup_mixed_vs_plain_fp64": sp["s_per_rhs_amortised"] / sm["s_per_rhs_amortised"],
            "training": {"pairs": net.num_pairs(), "collect_s": t_collect, "train_s": t_train,
                         "steps": args.train_steps, "loss_first": f_loss, "loss_last": l_loss},
            "clocks": clocks}
@@ -416,7 +430,7 @@ def main():
     ap.add_argument("--coarsen", type=int, default=8)
     ap.add_argument("--restart", type=int, default=40)
     ap.add_argument("--rhs", type=int, default=16)
-    ap.add_argument("--plain-rhs", type=int, default=2)
+    ap.add_argument("--plain-rhs", type=int, default=16)
     ap.add_argument("--train-rhs", type=int, default=4)
     ap.add_argument("--train-steps", type=int, default=400)
     args = ap.parse_args()

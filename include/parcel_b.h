@@ -142,7 +142,7 @@ typedef struct parcel_b_stats {
   int kernel_launches;      /* kernels this library launched for the solve           */
   int ilu_levels_max;       /* longest wavefront (levels) of any block-Jacobi block  */
   int ilu_nblocks;
-  int fallback;             /* learned solve: 1 if the plain PGMRES/ILU path finished it */
+  int fallback;             /* learned solve: right-hand sides the plain PGMRES finished */
   int reserved[5];
 } parcel_b_stats;
 
@@ -316,6 +316,11 @@ int parcel_b_learned_train(parcel_b_learned h, int steps, int batch, double lr, 
  * residual misses rtolmax, plain PGMRES with M continues from x (stats.fallback = 1). */
 int parcel_b_solve_learned(const parcel_b_input* prm, const parcel_b_crs* A, parcel_b_learned h,
                            const double* b, double* x, double* reshistory, int* niter, int* iret);
+/* nrhs systems A x_k = b_k with one set-up (layout, ILU factors, learned stage), solved one
+ * after the other on the device: b and x hold nrhs vectors of n entries each, niter and
+ * iret nrhs entries.  Statistics: setup_s once, solve_s for all, true_relres the worst. */
+int parcel_b_solve_learned_many(const parcel_b_input* prm, const parcel_b_crs* A, parcel_b_learned h,
+                                int nrhs, const double* b, double* x, int* niter, int* iret);
 
 #ifdef __cplusplus
 }

@@ -346,102 +346,142 @@ int parcel_b_learned_train(parcel_b_learned h, int steps, int batch, double lr, 
   });
 }
 
-int parcel_b_solve_learned(const parcel_b_input* prm, const parcel_b_crs* A, parcel_b_learned h, const double* b,
-                           double* x, double* reshistory, int* niter, int* iret) {
-  int rc = guarded([&]() -> int {
-    ensure_init();
-    validate(A);
-    PB_CHECK(b && x, PARCEL_B_E_ARG, "b and x must not be NULL");
-    Learned* L = reinterpret_cast<Learned*>(h);
-    if (L) check_grid(*L, A);
-    Options o = resolve_options(prm);
-    PB_CHECK(o.solver == PARCEL_B_SOLVER_GMRES, PARCEL_B_E_UNSUPPORTED,
-             "the learned stage runs inside flexible GMRES (solver %d given)", o.solver);
-    PB_CHECK(o.precon >= 0 && o.precon <= 2, PARCEL_B_E_UNSUPPORTED, "ipreflag=%d is not provided", o.precon);
-    o.flexible = true;
-    const double t0 = now_s();
-    const bool dev = is_device_ptr(A->val);
-    const bool xdev = is_device_ptr(x);
-    parcel_b_stats stt;
-    memset(&stt, 0, sizeof(stt));
-    NatVec bv(b, A->n, is_device_ptr(b)), xv(x, A->n, xdev);
-    std::vector<double> hist;
+}  // extern "C"
+
+namespace pb {
+namespace {
+
+// nrhs solves of A x_k = b_k with one set-up (layout, ILU factors, learned stage).  B and X
+// hold the right-hand sides and solutions one after the other (natural layout).
+int solve_learned_impl(const parcel_b_input* prm, const parcel_b_crs* A, Learned* L, int nrhs, const double* B,
+                       double* X, double* reshistory, int* niter, int* iret) {
+  ensure_init();
+  validate(A);
+  PB_CHECK(B && X && nrhs >= 1, PARCEL_B_E_ARG, "b and x must not be NULL, nrhs >= 1");
+  if (L) check_grid(*L, A);
+  Options o = resolve_options(prm);
+  PB_CHECK(o.solver == PARCEL_B_SOLVER_GMRES, PARCEL_B_E_UNSUPPORTED,
+           "the learned stage runs inside flexible GMRES (solver %d given)", o.solver);
+  PB_CHECK(o.precon >= 0 && o.precon <= 2, PARCEL_B_E_UNSUPPORTED, "ipreflag=%d is not provided", o.precon);
+  o.flexible = true;
+  const double t0 = now_s();
+  const int n = A->n;
+  const bool dev = is_device_ptr(A->val);
+  const bool bdev = is_device_ptr(B), xdev = is_device_ptr(X);
+  parcel_b_stats stt;
+  memset(&stt, 0, sizeof(stt));
+  const bool mixed = o.inner == PARCEL_B_INNER_FP32_REFINE;
+  std::unique_ptr<System<float>> S32;
+  std::unique_ptr<System<double>> S64;
+  std::unique_ptr<LearnedStage<float>> st32;
+  std::unique_ptr<LearnedStage<double>> st64;
+  if (mixed) {
+    S32 = std::make_unique<System<float>>();
+    build_system<float>(o, *A, dev, *S32);
+    if (L) { st32 = std::make_unique<LearnedStage<float>>(L, *S32); S32->extra = st32.get(); }
+    stt.ilu_levels_max = S32->ilu_levels_max;
+    stt.ilu_nblocks = S32->ilu_nblocks;
+  } else {
+    S64 = std::make_unique<System<double>>();
+    build_system<double>(o, *A, dev, *S64);
+    if (L) { st64 = std::make_unique<LearnedStage<double>>(L, *S64); S64->extra = st64.get(); }
+    stt.ilu_levels_max = S64->ilu_levels_max;
+    stt.ilu_nblocks = S64->ilu_nblocks;
+  }
+  // natural matrix on the device for the true residual (the FP64 system keeps one)
+  DevMat<double> An;
+  An.n = n; An.nnz = A->nnz; An.rbase = 1; An.cbase = A->istart;
+  DBuf up_rp, up_ci, up_va;
+  if (S64) {
+    An = S64->Anat;
+  } else if (dev) {
+    An.rowptr = A->rowptr; An.col = A->col; An.val = A->val;
+  } else {
+    up_rp.alloc(sizeof(int) * (n + 1)); h2d(up_rp.p, A->rowptr, sizeof(int) * (n + 1));
+    up_ci.alloc(sizeof(int) * A->nnz); h2d(up_ci.p, A->col, sizeof(int) * A->nnz);
+    up_va.alloc(sizeof(double) * A->nnz); h2d(up_va.p, A->val, sizeof(double) * A->nnz);
+    An.rowptr = dp<int>(up_rp); An.col = dp<int>(up_ci); An.val = dp<double>(up_va);
+  }
+  sync();
+  const double t1 = now_s();
+  std::unique_ptr<System<double>> Sfb;   // plain system, built only if a fallback is needed
+  int total = 0, worst = 0;
+  double worst_rel = 0.0;
+  std::vector<double> hist;
+  for (int k = 0; k < nrhs; ++k) {
+    NatVec bv(B + (size_t)k * n, n, bdev), xv(X + (size_t)k * n, n, xdev);
+    hist.clear();
     SolveOut so;
-    double t1 = t0;
-    if (o.inner == PARCEL_B_INNER_FP32_REFINE) {
-      std::unique_ptr<LearnedStage<float>> stage;
-      std::function<void(System<float>&)> attach = [&](System<float>& S) {
-        if (L) {
-          stage = std::make_unique<LearnedStage<float>>(L, S);
-          S.extra = stage.get();
-        }
-      };
-      MixedResult mr = solve_mixed(o, *A, dev, bv.p, xv.p, hist, &t1, &attach);
-      so.niter = mr.niter;
-      so.iret = mr.iret;
-      so.launches = mr.launches;
-      stt.refine_steps = mr.refine_steps;
-      stt.true_relres_dd = mr.true_relres_dd;
-      stt.ilu_levels_max = mr.ilu_levels_max;
-      stt.ilu_nblocks = mr.ilu_nblocks;
+    if (mixed) {
+      MixedResult mr = solve_mixed_on(o, *S32, bv.p, xv.p, hist, nullptr);
+      so.niter = mr.niter; so.iret = mr.iret; so.launches = mr.launches;
+      stt.refine_steps += mr.refine_steps;
+      stt.true_relres_dd = std::max(stt.true_relres_dd, mr.true_relres_dd);
     } else {
-      System<double> S;
-      build_system<double>(o, *A, dev, S);
-      std::unique_ptr<LearnedStage<double>> stage;
-      if (L) {
-        stage = std::make_unique<LearnedStage<double>>(L, S);
-        S.extra = stage.get();
-      }
-      so = solve_on_system(o, S, bv.p, xv.p, hist, &t1);
-      stt.ilu_levels_max = S.ilu_levels_max;
-      stt.ilu_nblocks = S.ilu_nblocks;
+      so = solve_on_system(o, *S64, bv.p, xv.p, hist, nullptr);
     }
     // The true FP64 residual decides; the plain PGMRES/ILU path finishes what the
     // learned solve left.
-    DevMat<double> An;
-    An.n = A->n; An.nnz = A->nnz; An.rbase = 1; An.cbase = A->istart;
-    DBuf up_rp, up_ci, up_va;
-    if (dev) {
-      An.rowptr = A->rowptr; An.col = A->col; An.val = A->val;
-    } else {
-      up_rp.alloc(sizeof(int) * (A->n + 1)); h2d(up_rp.p, A->rowptr, sizeof(int) * (A->n + 1));
-      up_ci.alloc(sizeof(int) * A->nnz); h2d(up_ci.p, A->col, sizeof(int) * A->nnz);
-      up_va.alloc(sizeof(double) * A->nnz); h2d(up_va.p, A->val, sizeof(double) * A->nnz);
-      An.rowptr = dp<int>(up_rp); An.col = dp<int>(up_ci); An.val = dp<double>(up_va);
-    }
     double rel = true_relres(An, bv.p, xv.p);
     if (!(rel < o.rtol) && so.iret >= 0 && so.niter < o.itrmax) {
       Options op = resolve_options(prm);
       op.itrmax = o.itrmax - so.niter;
-      System<double> S2;
-      build_system<double>(op, *A, dev, S2);
+      if (!Sfb) {
+        Sfb = std::make_unique<System<double>>();
+        build_system<double>(op, *A, dev, *Sfb);
+      }
       std::vector<double> h2;
-      SolveOut s2 = solve_on_system(op, S2, bv.p, xv.p, h2, nullptr);
+      SolveOut s2 = solve_on_system(op, *Sfb, bv.p, xv.p, h2, nullptr);
       for (double v : h2) hist.push_back(v);
       so.niter += s2.niter;
       so.iret = s2.iret;
       so.launches += s2.launches;
-      stt.fallback = 1;
+      stt.fallback += 1;
       rel = true_relres(An, bv.p, xv.p);
     }
-    stt.true_relres = rel;
-    const double t2 = now_s();
-    if (!xdev) d2h(x, xv.p, sizeof(double) * A->n);
-    if (reshistory && !hist.empty()) {
-      size_t cnt = std::min<size_t>(hist.size(), (size_t)std::max(o.itrmax, 0));
-      if (is_device_ptr(reshistory)) { h2d(reshistory, hist.data(), sizeof(double) * cnt); sync(); }
-      else memcpy(reshistory, hist.data(), sizeof(double) * cnt);
-    }
-    if (niter) *niter = so.niter;
-    if (iret) *iret = so.iret;
-    stt.setup_s = t1 - t0;
-    stt.solve_s = t2 - t1;
-    stt.total_s = now_s() - t0;
-    stt.niter = so.niter;
-    stt.iret = so.iret;
-    stt.kernel_launches = so.launches;
-    set_stats(stt);
-    return so.iret < 0 ? so.iret : 0;
+    if (!xdev) d2h(X + (size_t)k * n, xv.p, sizeof(double) * n);
+    if (niter) niter[k] = so.niter;
+    if (iret) iret[k] = so.iret;
+    if (so.iret < 0) { worst = so.iret; break; }
+    if (so.iret > worst) worst = so.iret;
+    total += so.niter;
+    stt.kernel_launches += so.launches;
+    worst_rel = std::max(worst_rel, rel);
+  }
+  if (nrhs == 1 && reshistory && !hist.empty()) {
+    size_t cnt = std::min<size_t>(hist.size(), (size_t)std::max(o.itrmax, 0));
+    if (is_device_ptr(reshistory)) { h2d(reshistory, hist.data(), sizeof(double) * cnt); sync(); }
+    else memcpy(reshistory, hist.data(), sizeof(double) * cnt);
+  }
+  const double t2 = now_s();
+  stt.true_relres = worst_rel;
+  stt.setup_s = t1 - t0;
+  stt.solve_s = t2 - t1;
+  stt.total_s = t2 - t0;
+  stt.niter = total;
+  stt.iret = worst;
+  set_stats(stt);
+  return worst < 0 ? worst : 0;
+}
+
+}  // namespace
+}  // namespace pb
+
+extern "C" {
+
+int parcel_b_solve_learned(const parcel_b_input* prm, const parcel_b_crs* A, parcel_b_learned h, const double* b,
+                           double* x, double* reshistory, int* niter, int* iret) {
+  int rc = guarded([&]() -> int {
+    return solve_learned_impl(prm, A, reinterpret_cast<Learned*>(h), 1, b, x, reshistory, niter, iret);
+  });
+  if (rc < 0 && iret) *iret = rc;
+  return rc;
+}
+
+int parcel_b_solve_learned_many(const parcel_b_input* prm, const parcel_b_crs* A, parcel_b_learned h, int nrhs,
+                                const double* b, double* x, int* niter, int* iret) {
+  int rc = guarded([&]() -> int {
+    return solve_learned_impl(prm, A, reinterpret_cast<Learned*>(h), nrhs, b, x, nullptr, niter, iret);
   });
   if (rc < 0 && iret) *iret = rc;
   return rc;

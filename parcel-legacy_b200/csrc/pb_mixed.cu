@@ -47,14 +47,19 @@ void residual_dd(const DevMat<double>& A, const double* val_lo, const double* x_
 MixedResult solve_mixed(const Options& o, const parcel_b_crs& A, bool dev, const double* b,
                         double* x, std::vector<double>& hist, double* setup_t,
                         const std::function<void(System<float>&)>* attach) {
-  cudaStream_t st = stream();
   System<float> S;
   build_system<float>(o, A, dev, S);
   if (attach) (*attach)(S);
+  return solve_mixed_on(o, S, b, x, hist, setup_t);
+}
+
+MixedResult solve_mixed_on(const Options& o, System<float>& S, const double* b, double* x,
+                           std::vector<double>& hist, double* setup_t) {
+  cudaStream_t st = stream();
   MixedResult res;
   res.ilu_levels_max = S.ilu_levels_max;
   res.ilu_nblocks = S.ilu_nblocks;
-  const int n = A.n, np = S.np;
+  const int n = S.n, np = S.np;
   DBuf r(sizeof(double) * n), rlo(sizeof(double) * n), d64(sizeof(double) * n);
   DBuf r32(sizeof(float) * np), d32(sizeof(float) * np);
   DBuf hist_dev(sizeof(double) * (o.itrmax + 2));

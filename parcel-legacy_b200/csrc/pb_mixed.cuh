@@ -31,6 +31,11 @@ MixedResult solve_mixed(const Options& o, const parcel_b_crs& A, bool dev, const
                         double* x, std::vector<double>& hist, double* setup_t,
                         const std::function<void(System<float>&)>* attach = nullptr);
 
+// The same refinement loop on an FP32 system that is already built (several right-hand
+// sides share one set-up).
+MixedResult solve_mixed_on(const Options& o, System<float>& S, const double* b, double* x,
+                           std::vector<double>& hist, double* setup_t);
+
 // CA-GMRES(s, t) (KSP_pCAGMRES, src/pcagmres.f90:1557-2518) in FP64.
 SolveOut solve_cagmres(const Options& o, System<double>& S, const double* b, double* x,
                        std::vector<double>& hist, double* setup_t);

@@ -108,6 +108,7 @@ SIGNATURES = {
     "parcel_b_learned_num_pairs": (C.c_int, [P]),
     "parcel_b_learned_train": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_uint64, DP, DP]),
     "parcel_b_solve_learned": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), P, P, P, P, IP, IP]),
+    "parcel_b_solve_learned_many": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), P, C.c_int, P, P, P, P]),
 }
 
 _lib = None
