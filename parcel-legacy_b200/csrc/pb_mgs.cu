@@ -123,6 +123,96 @@ __global__ void __launch_bounds__(kMgsThreads, 2) k_gm_mgs(MgsArgs<T> a) {
   }
 }
 
+// Streaming variant for vectors too long to stay in registers (more than 32 elements per
+// thread of the co-resident grid, e.g. 256^3 unknowns): w lives in global memory and is
+// updated in place, pass p reading w, v_{p-1} and v_p and writing w, with the same
+// operations in the same order as the register version.  Successive passes walk the rows
+// in opposite directions, so a pass starts on the rows the previous one touched last,
+// which are still in L2.  A final pass writes v_{j+1} = w / ||w||.
+template <class T>
+__global__ void __launch_bounds__(kMgsThreads, 2) k_gm_mgs_stream(MgsArgs<T> a) {
+  if (gated(a.gate)) return;
+  __shared__ double wsum[kMgsThreads / 32];
+  __shared__ double total;
+  constexpr int EB = 8;
+  const unsigned G = gridDim.x;
+  const int64_t nthr = (int64_t)G * blockDim.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nb = (a.np + nthr * EB - 1) / (nthr * EB);   // batches of EB elements per thread
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j = a.j;
+  T* __restrict__ w = a.w;
+  double hprev = 0.0, S = 0.0;
+  for (int p = 1; p <= j + 1; ++p) {
+    const T* vprev = a.V + (size_t)(p - 2) * a.ldv;
+    const T* vcur = a.V + (size_t)(p - 1) * a.ldv;
+    const T mh = (T)(-hprev);
+    const bool upd = p > 1, dotv = p <= j;
+    double part = 0.0;
+    for (int64_t bb = 0; bb < nb; ++bb) {
+      const int64_t b = (p & 1) ? bb : nb - 1 - bb;
+      T wv[EB], vp[EB], vc[EB];
+#pragma unroll
+      for (int u = 0; u < EB; ++u) {
+        const int64_t i = (b * EB + u) * nthr + tid;
+        const bool ok = i < a.np;
+        wv[u] = ok ? w[i] : T(0);
+        vp[u] = (upd && ok) ? __ldcg(vprev + i) : T(0);
+        vc[u] = (dotv && ok) ? __ldcg(vcur + i) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < EB; ++u) {
+        const int64_t i = (b * EB + u) * nthr + tid;
+        T we = wv[u];
+        if (upd) we = mh * vp[u] + we;                          // w = -h v + 1*w
+        part += dotv ? (double)(we * vc[u]) : (double)(we * we);
+        if (upd && i < a.np) w[i] = we;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+    if (lane == 0) wsum[warp] = part;
+    __syncthreads();
+    double* parts = a.parts + (size_t)(p & 1) * G;
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += wsum[i];
+      parts[blockIdx.x] = s;
+    }
+    grid_barrier(a.ctr + (p - 1), G, a.err);
+    if (warp == 0) {
+      double s = 0.0;
+      for (unsigned b = lane; b < G; b += 32) s += __ldcg(parts + b);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+      if (lane == 0) total = s;
+    }
+    __syncthreads();
+    S = total;
+    if (p <= j) {
+      hprev = S;
+      if (blockIdx.x == 0 && threadIdx.x == 0) a.red.ea.h[(size_t)(j - 1) * (a.red.ea.m + 1) + (p - 1)] = S;
+    } else if (blockIdx.x == 0) {
+      __shared__ double Sv[1];
+      if (threadIdx.x == 0) Sv[0] = S;
+      __syncthreads();
+      epilogue(Sv, 1, a.red);   // EPI_GM_NORM: h(j+1,j), Givens, history, stop test
+    }
+    __syncthreads();
+  }
+  if (a.vnext) {   // v_{j+1} = (1/||w||) w; each thread rereads only what it wrote itself
+    const T inv = (T)(1.0 / sqrt(S));
+    for (int64_t bb = 0; bb < nb; ++bb) {
+      const int64_t b = ((j + 2) & 1) ? bb : nb - 1 - bb;
+#pragma unroll
+      for (int u = 0; u < EB; ++u) {
+        const int64_t i = (b * EB + u) * nthr + tid;
+        if (i < a.np) a.vnext[i] = inv * w[i];
+      }
+    }
+  }
+}
+
 template <class T>
 int mgs_elems_needed(int64_t np, int grid) {
   int64_t nthr = (int64_t)grid * kMgsThreads;
@@ -130,6 +220,21 @@ int mgs_elems_needed(int64_t np, int grid) {
   for (int c : {1, 2, 4, 8, 16, 32})
     if (e <= c) return c;
   return -1;
+}
+
+template <class T>
+static void launch_stream(const MgsArgs<T>& a, int grid, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kMgsThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  PB_CUDA(cudaLaunchKernelEx(&cfg, k_gm_mgs_stream<T>, a));
 }
 
 template <class T, int E>
@@ -161,7 +266,7 @@ int mgs_grid() {
 
 template <class T>
 bool mgs_supported(int64_t np) {
-  return mgs_elems_needed<T>(np, mgs_grid<T>()) > 0;
+  return np > 0;   // register-resident up to 32 elements per thread, streaming beyond
 }
 
 template <class T>
@@ -174,7 +279,7 @@ void mgs_column(const MgsArgs<T>& a, cudaStream_t st) {
     case 8: launch_e<T, 8>(a, grid, st); break;
     case 16: launch_e<T, 16>(a, grid, st); break;
     case 32: launch_e<T, 32>(a, grid, st); break;
-    default: PB_CHECK(false, PARCEL_B_E_UNSUPPORTED, "vector too long for the fused MGS kernel");
+    default: launch_stream<T>(a, grid, st); break;
   }
 }
 

@@ -11,7 +11,7 @@ template <class T>
 struct MgsArgs {
   int64_t np = 0;         // vector length
   int j = 0;              // column (1-based)
-  const T* w = nullptr;   // A M^-1 v_j
+  T* w = nullptr;         // A M^-1 v_j (the streaming variant updates it in place)
   const T* V = nullptr;   // basis, column stride ldv
   int64_t ldv = 0;
   T* vnext = nullptr;     // v_{j+1} destination (null for the last column of a cycle)

@@ -189,7 +189,7 @@ def gaussian_random_field(N: int, corr_len: float = 8.0, variance: float = 2.0,
     kz, ky, kx = np.meshgrid(f, f, np.fft.rfftfreq(N), indexing="ij")
     k2 = kx ** 2 + ky ** 2 + kz ** 2
     filt = np.exp(-2.0 * (np.pi * corr_len) ** 2 * k2 / 2.0)
-    g = np.fft.irfftn(np.fft.rfftn(w) * filt, s=(N, N, N))
+    g = np.fft.irfftn(np.fft.rfftn(w) * filt, s=(N, N, N), axes=(0, 1, 2))
     g -= g.mean()
     g *= np.sqrt(variance) / g.std()
     return g

@@ -196,3 +196,19 @@ def test_multiprocess_layout_is_rejected():
     rc = _lib.load().parcel_b_solve(C.byref(p), C.byref(S), b.ctypes.data, x.ctypes.data, None,
                                     C.byref(niter), C.byref(iret))
     assert rc == _lib.E_UNSUPPORTED and iret.value == _lib.E_UNSUPPORTED
+
+
+def test_streaming_mgs_matches_oracle():
+    """140^3 rows exceed what the register-resident fused MGS holds (32 elements per
+    thread of the co-resident grid), so the streaming fused MGS runs; two restart cycles
+    of its GMRES history must match the oracle's MGS GMRES."""
+    A = problems.convdiff3d_upwind(140)
+    b = problems.rhs_normal(A.n, 5)
+    kw = dict(solver=3, ipreflag=2, ILU_method=0, precon_thblock=64, GMRES_m=30, GMRES_GSflag=1, itrmax=60,
+              rtolmax=1e-12)
+    res = api.solve(A, b, **kw)
+    xo, ho, no, io = oracle.solve(A, b, **kw)
+    assert res["niter"] == no == 60
+    h = res["reshistory"]
+    assert np.max(np.abs(h - ho) / ho) < 1e-6
+    assert _rel(res["x"], xo) < 1e-6
