@@ -588,6 +588,8 @@ __global__ void k_scale_by(int64_t n, const float* __restrict__ in, const float*
   if (i < n) out[i] = in[i] * scal[0];
 }
 
+// One warp per coarse cell: the lanes split the cell's c^3 fine rows (32-bit index
+// arithmetic: n < 2^31), sum in FP64 and lane 0 stores the mean.
 template <class T>
 __global__ void __launch_bounds__(kRedThreads)
     k_restrict(int nx, int ny, int nz, int c, const T* __restrict__ src, const int* __restrict__ pos,
@@ -596,28 +598,29 @@ __global__ void __launch_bounds__(kRedThreads)
   if (gated(gate)) return;
   __shared__ double red[kRedThreads / 32];
   __shared__ bool last;
-  const int gx = nx / c, gy = ny / c, gz = nz / c;
-  const int64_t V = (int64_t)gx * gy * gz;
-  const double inv = 1.0 / ((double)c * c * c);
+  const unsigned gx = nx / c, gy = ny / c, gz = nz / c;
+  const unsigned V = gx * gy * gz, c3 = (unsigned)(c * c * c), cc = (unsigned)(c * c);
+  const double inv = 1.0 / (double)c3;
+  const int lane = threadIdx.x & 31;
+  const unsigned wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   double sq = 0.0;
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
-    const int cx = (int)(v % gx), cy = (int)((v / gx) % gy), cz = (int)(v / ((int64_t)gx * gy));
+  for (unsigned v = wid; v < V; v += nw) {
+    const unsigned cx = v % gx, r1 = v / gx, cy = r1 % gy, cz = r1 / gy;
     double s = 0.0;
-    for (int k = 0; k < c; ++k)
-      for (int j = 0; j < c; ++j) {
-        const int64_t rowb = ((int64_t)(cz * c + k) * ny + (cy * c + j)) * nx + (int64_t)cx * c;
-        for (int i = 0; i < c; ++i) {
-          const int64_t nat = rowb + i;
-          s += (double)src[pos ? pos[nat] : nat];
-        }
-      }
-    const float m = (float)(s * inv);
-    tc[v] = m;
-    sq += (double)m * m;
-  }
+    for (unsigned e = lane; e < c3; e += 32) {
+      const unsigned i = e % c, j = (e / c) % c, k = e / cc;
+      const unsigned nat = ((cz * c + k) * ny + (cy * c + j)) * nx + cx * c + i;
+      s += (double)src[pos ? pos[nat] : nat];
+    }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    if (lane == 0) {
+      const float m = (float)(s * inv);
+      tc[v] = m;
+      sq += (double)m * m;
+    }
+  }
+  if (lane == 0) red[threadIdx.x >> 5] = sq;
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = 0.0;
@@ -653,10 +656,11 @@ __global__ void __launch_bounds__(256)
   if (gated(gate)) return;
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= np) return;
-  const int64_t nat = rowAt ? (int64_t)rowAt[p] : p;
+  const int nat = rowAt ? rowAt[p] : (int)p;
   if (nat < 0) return;
   const int gx = nx / c, gy = ny / c, gz = nz / c;
-  const int x = (int)(nat % nx), y = (int)((nat / nx) % ny), z = (int)(nat / ((int64_t)nx * ny));
+  const unsigned un = (unsigned)nat, r1 = un / (unsigned)nx;
+  const int x = (int)(un - r1 * (unsigned)nx), y = (int)(r1 % (unsigned)ny), z = (int)(r1 / (unsigned)ny);
   int x0, x1, y0, y1, z0, z1;
   float wx, wy, wz;
   lin1(x, c, gx, x0, x1, wx);

@@ -418,19 +418,22 @@ struct IluSolveArgs {
   int* err;
 };
 
-// Operands of one row of one chunk, staged from shared memory into registers.  Every
-// chunk of a sweep carries exactly KM coupled entries per row (shorter rows are padded
-// with the ring's zero slot), so the loops below have compile-time trip counts.
-template <class T, int KM>
+// Operands of the R rows (p, p + 256, ...) a consumer thread owns in one chunk, staged from
+// shared memory into registers.  Every chunk of a sweep carries exactly KM coupled entries
+// per row (shorter rows are padded with the ring's zero slot), so the loops below have
+// compile-time trip counts.  R > 1 serves levels wider than the 256 consumer threads
+// (up to 1,024 rows: 256^3 grids split into 64 blocks); the rows of a chunk belong to one
+// level and are independent, so one barrier per chunk still suffices.
+template <class T, int KM, int R>
 struct RowOps {
-  T xin, dg;
-  T val[KM];
-  int slot[KM];
+  T xin[R], dg[R];
+  T val[R][KM];
+  int slot[R][KM];
   int start, w, rbase;
 };
 
-template <class T, int KM>
-__device__ __forceinline__ void load_ops(RowOps<T, KM>& o, const unsigned char* sp, int p) {
+template <class T, int KM, int R>
+__device__ __forceinline__ void load_ops(RowOps<T, KM, R>& o, const unsigned char* sp, int p) {
   const int4 h0 = *reinterpret_cast<const int4*>(sp);
   const int rb = *reinterpret_cast<const int*>(sp + 24);
   o.start = h0.x;
@@ -441,56 +444,68 @@ __device__ __forceinline__ void load_ops(RowOps<T, KM>& o, const unsigned char* 
   const T* val = dg + wpad;
   const int* slot = reinterpret_cast<const int*>(val + KM * wpad);
   const T* xin = reinterpret_cast<const T*>(slot + KM * wpad);
-  if (p < o.w) {
-    o.xin = xin[p];
-    o.dg = dg[p];
 #pragma unroll
-    for (int k = 0; k < KM; ++k) { o.val[k] = val[k * wpad + p]; o.slot[k] = slot[k * wpad + p]; }
+  for (int r = 0; r < R; ++r) {
+    const int q = p + r * kIluConsumerThreads;
+    if (q < o.w) {
+      o.xin[r] = xin[q];
+      o.dg[r] = dg[q];
+#pragma unroll
+      for (int k = 0; k < KM; ++k) { o.val[r][k] = val[k * wpad + q]; o.slot[r][k] = slot[k * wpad + q]; }
+    }
   }
 }
 
-template <class T, bool DILU, bool FWD, int KM>
-__device__ __forceinline__ void solve_rows(const RowOps<T, KM>& c, const T* ring, T* ringw, T* vout,
+template <class T, bool DILU, bool FWD, int KM, int R>
+__device__ __forceinline__ void solve_rows(const RowOps<T, KM, R>& c, const T* ring, T* ringw, T* vout,
                                            T* accum, int p) {
-  if (p >= c.w) return;
-  T dv[KM];
+  T dv[R][KM];
 #pragma unroll
-  for (int k = 0; k < KM; ++k) dv[k] = ring[c.slot[k]];
-  T acc = (FWD || !DILU) ? c.xin : T(0);
+  for (int r = 0; r < R; ++r)
+    if (p + r * kIluConsumerThreads < c.w) {
 #pragma unroll
-  for (int k = 0; k < KM; ++k) {
-    if (FWD) acc = acc - c.val[k] * dv[k];
-    else if (DILU) acc = acc + dv[k] * c.val[k];
-    else acc = acc - dv[k] * c.val[k];
+      for (int k = 0; k < KM; ++k) dv[r][k] = ring[c.slot[r][k]];
+    }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int q = p + r * kIluConsumerThreads;
+    if (q >= c.w) continue;
+    T acc = (FWD || !DILU) ? c.xin[r] : T(0);
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+      if (FWD) acc = acc - c.val[r][k] * dv[r][k];
+      else if (DILU) acc = acc + dv[r][k] * c.val[r][k];
+      else acc = acc - dv[r][k] * c.val[r][k];
+    }
+    T out;
+    if (FWD) out = DILU ? c.dg[r] * acc : acc;
+    else if (DILU) out = c.xin[r] - c.dg[r] * acc;
+    else out = acc * c.dg[r];
+    ringw[c.rbase + q] = out;
+    vout[c.start + q] = out;
+    if (!FWD && accum) accum[c.start + q] += out;
   }
-  T out;
-  if (FWD) out = DILU ? c.dg * acc : acc;
-  else if (DILU) out = c.xin - c.dg * acc;
-  else out = acc * c.dg;
-  ringw[c.rbase + p] = out;
-  vout[c.start + p] = out;
-  if (!FWD && accum) accum[c.start + p] += out;
 }
 
 // Ring-mode consumer loop: chunk i+1's operands are loaded from its stage while chunk i
 // is solved, so after each level barrier only the ring gathers, the multiply-add chain
 // and the stores remain on the critical path.  Two register sets alternate.
-template <class T, bool DILU, bool FWD, int KM>
+template <class T, bool DILU, bool FWD, int KM, int R>
 __device__ __forceinline__ void consume_pipelined(const IluSolveArgs<T>& a, uint64_t* full,
                                                   uint64_t* empty, volatile int* sflags,
                                                   unsigned char* stages, T* ring, int nc, int gbase,
                                                   int ctid, T* vout) {
   const int NST = a.nstages;
-  RowOps<T, KM> A, B;
+  RowOps<T, KM, R> A, B;
   int done = 0;
-  auto wait_load = [&](RowOps<T, KM>& o, int g) -> bool {
+  auto wait_load = [&](RowOps<T, KM, R>& o, int g) -> bool {
     const int st = g % NST;
     if (!mbar_wait(&full[st], (g / NST) & 1, kWaitLimit)) {
       atomicExch(a.err, 3);
       sflags[0] = 1;
       return false;
     }
-    load_ops<T, KM>(o, stages + (size_t)st * a.stage_bytes, ctid);
+    load_ops<T, KM, R>(o, stages + (size_t)st * a.stage_bytes, ctid);
     return true;
   };
   auto release = [&](bool ok, int g) {
@@ -505,14 +520,14 @@ __device__ __forceinline__ void consume_pipelined(const IluSolveArgs<T>& a, uint
       // chunk i in A, prefetch i+1 into B
       bool okB = true;
       if (i + 1 < nc) okB = wait_load(B, gbase + i + 1);
-      solve_rows<T, DILU, FWD, KM>(A, ring, ring, vout, a.accum, ctid);
+      solve_rows<T, DILU, FWD, KM, R>(A, ring, ring, vout, a.accum, ctid);
       named_bar_sync(1, kIluConsumerThreads);
       if (i + 1 >= nc || sflags[0]) { done = i + 1; break; }
       release(okB, gbase + i + 1);
       // chunk i+1 in B, prefetch i+2 into A
       bool okA = true;
       if (i + 2 < nc) okA = wait_load(A, gbase + i + 2);
-      solve_rows<T, DILU, FWD, KM>(B, ring, ring, vout, a.accum, ctid);
+      solve_rows<T, DILU, FWD, KM, R>(B, ring, ring, vout, a.accum, ctid);
       named_bar_sync(1, kIluConsumerThreads);
       if (i + 2 >= nc || sflags[0]) { done = i + 2; break; }
       release(okA, gbase + i + 2);
@@ -521,7 +536,76 @@ __device__ __forceinline__ void consume_pipelined(const IluSolveArgs<T>& a, uint
   if (ctid == 0) sflags[1] = gbase + done;
 }
 
-template <class T, bool DILU, int KM>
+// Solves the R rows (p, p + 256, ...) of the staged chunk at sp, reading the operands
+// straight from shared memory: ring slots first, then the coupled values, then the
+// coefficients, so the loads of all R rows are in flight together and few stay live.
+template <class T, bool DILU, bool FWD, int KM, int R>
+__device__ __forceinline__ void solve_rows_direct(const unsigned char* sp, T* ring, T* vout, T* accum, int p) {
+  const int4 h0 = *reinterpret_cast<const int4*>(sp);
+  const int start = h0.x, w = h0.y, wpad = h0.z;
+  const int rbase = *reinterpret_cast<const int*>(sp + 24);
+  const T* dg = reinterpret_cast<const T*>(sp + kIluHeader);
+  const T* val = dg + wpad;
+  const int* slot = reinterpret_cast<const int*>(val + KM * wpad);
+  const T* xin = reinterpret_cast<const T*>(slot + KM * wpad);
+  T dv[R][KM];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int q = p + r * kIluConsumerThreads;
+    if (q < w) {
+#pragma unroll
+      for (int k = 0; k < KM; ++k) dv[r][k] = ring[slot[k * wpad + q]];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int q = p + r * kIluConsumerThreads;
+    if (q >= w) continue;
+    T acc = (FWD || !DILU) ? xin[q] : T(0);
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+      const T v = val[k * wpad + q];
+      if (FWD) acc = acc - v * dv[r][k];
+      else if (DILU) acc = acc + dv[r][k] * v;
+      else acc = acc - dv[r][k] * v;
+    }
+    T out;
+    if (FWD) out = DILU ? dg[q] * acc : acc;
+    else if (DILU) out = xin[q] - dg[q] * acc;
+    else out = acc * dg[q];
+    ring[rbase + q] = out;
+    vout[start + q] = out;
+    if (!FWD && accum) accum[start + q] += out;
+  }
+}
+
+// Consumer loop for R > 1: the chunk is solved straight from its stage (no operand copy
+// in registers); the R independent rows of each thread overlap their loads instead.
+template <class T, bool DILU, bool FWD, int KM, int R>
+__device__ __forceinline__ void consume_simple(const IluSolveArgs<T>& a, uint64_t* full, uint64_t* empty,
+                                               volatile int* sflags, unsigned char* stages, T* ring, int nc,
+                                               int gbase, int ctid, T* vout) {
+  const int NST = a.nstages;
+  int done = 0;
+  int st = gbase % NST, ph = (gbase / NST) & 1;
+  for (int i = 0; i < nc; ++i) {
+    const bool ok = mbar_wait(&full[st], ph, kWaitLimit);
+    if (!ok) {
+      atomicExch(a.err, 3);
+      sflags[0] = 1;
+    }
+    named_bar_sync(1, kIluConsumerThreads);
+    if (sflags[0]) { done = i; break; }
+    solve_rows_direct<T, DILU, FWD, KM, R>(stages + (size_t)st * a.stage_bytes, ring, vout, a.accum, ctid);
+    named_bar_sync(1, kIluConsumerThreads);   // the level is in the ring; the stage is free
+    if (ctid == 0) mbar_arrive(&empty[st]);
+    done = i + 1;
+    if (++st == NST) { st = 0; ph ^= 1; }
+  }
+  if (ctid == 0) sflags[1] = gbase + done;
+}
+
+template <class T, bool DILU, int KM, int R>
 __global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve_fast(IluSolveArgs<T> a) {
   if (gated(a.gate)) return;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -594,8 +678,13 @@ __global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve_fast(IluSolveArgs<
         cur = nxt;
       }
     } else if (nc > 0) {
-      if (fwd) consume_pipelined<T, DILU, true, KM>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.y);
-      else consume_pipelined<T, DILU, false, KM>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.s);
+      if (R == 1) {
+        if (fwd) consume_pipelined<T, DILU, true, KM, R>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.y);
+        else consume_pipelined<T, DILU, false, KM, R>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.s);
+      } else {
+        if (fwd) consume_simple<T, DILU, true, KM, R>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.y);
+        else consume_simple<T, DILU, false, KM, R>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.s);
+      }
       if (fwd) fence_proxy_async_global();
     }
     __syncthreads();
@@ -804,7 +893,9 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   {
     int maxw = 0;
     for (const auto& c : ch) maxw = std::max(maxw, c.w);
-    D.fast_km = (D.ring && maxw <= kIluConsumerThreads && kuni <= 8) ? kuni : 0;
+    D.fast_rows = maxw <= kIluConsumerThreads ? 1 : maxw <= 2 * kIluConsumerThreads ? 2
+                : maxw <= 4 * kIluConsumerThreads ? 4 : 0;
+    D.fast_km = (D.ring && D.fast_rows > 0 && kuni <= 8) ? kuni : 0;
   }
 
   D.chunks.alloc(sizeof(IluChunk) * std::max<size_t>(ch.size(), 1));
@@ -886,9 +977,9 @@ static void launch_ilu(const IluDev<T>& D, const IluSolveArgs<T>& a, cudaStream_
   kern<<<D.nb, kIluThreads, D.smem_bytes, st>>>(a);
 }
 
-template <class T, bool DILU, int KM>
+template <class T, bool DILU, int KM, int R>
 static void launch_fast(const IluDev<T>& D, const IluSolveArgs<T>& a, cudaStream_t st) {
-  auto kern = k_ilu_solve_fast<T, DILU, KM>;
+  auto kern = k_ilu_solve_fast<T, DILU, KM, R>;
   static bool configured = false;
   if (!configured) {
     PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
@@ -916,9 +1007,12 @@ void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, 
   a.ring_elems = D.ring ? D.W * D.maxWp + 1 : 0;
   a.gate = gate;
   a.err = dp<int>(D.err);
-#define FAST(KM_)                                                                 \
-  case KM_:                                                                       \
-    if (D.dilu) launch_fast<T, true, KM_>(D, a, st); else launch_fast<T, false, KM_>(D, a, st); \
+#define FAST_R(KM_, R_)                                                                            \
+  if (D.dilu) launch_fast<T, true, KM_, R_>(D, a, st); else launch_fast<T, false, KM_, R_>(D, a, st);
+#define FAST(KM_)                                                                                  \
+  case KM_:                                                                                        \
+    if (D.fast_rows == 1) { FAST_R(KM_, 1) } else if (D.fast_rows == 2) { FAST_R(KM_, 2) }         \
+    else { FAST_R(KM_, 4) }                                                                        \
     break;
   if (D.fast_km > 0) {
     switch (D.fast_km) {

@@ -79,6 +79,7 @@ struct IluDev {
   int W = 1, maxWp = 0;
   bool ring = true;
   bool dilu = false;
+  int fast_rows = 1;  // rows per consumer thread of the pipelined sweep (1, 2 or 4)
   int fast_km = 0;  // >0: pipelined ring-mode sweep with at most fast_km couplings per row
   int stage_bytes = 0, nstages = 0, smem_bytes = 0;
   DBuf chunks;      // IluChunk[]

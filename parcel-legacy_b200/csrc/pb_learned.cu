@@ -89,7 +89,7 @@ struct LearnedStage final : ExtraStage<T> {
     acts.ensure(L->g, 1, false);
     cnn::init_kernels();
   }
-  void apply(const System<T>& S, const T* r, T* z, const int* gate, cudaStream_t st) override {
+  void apply(const System<T>& S, const T* r, T* z, T* az, const int* gate, cudaStream_t st) override {
     spmv<T, T>(S.A, z, dp<T>(t), SPMV_RES, r, gate, st);
     cnn::restrict_to_coarse<T>(L->nx, L->ny, L->nz, L->c, dp<T>(t), pos, dp<float>(tc), dp<float>(scal),
                                dp<double>(part), dp<unsigned>(ticket), gate, st);
@@ -101,8 +101,10 @@ struct LearnedStage final : ExtraStage<T> {
     spmv<T, T>(S.A, dp<T>(cf), dp<T>(q), SPMV_Y, nullptr, gate, st);
     cnn::step_length<T>(np, dp<T>(t), dp<T>(q), dp<double>(part), dp<unsigned>(ticket), dp<double>(alpha), gate, st);
     lincomb<T>(np, z, z, cimm(1.0), dp<T>(cf), cdev(dp<double>(alpha)), nullptr, cimm(0), gate, st);
+    // A z = A z1 + alpha A c = (r - t) + alpha q: no SpMV of z needed
+    if (az) lincomb<T>(np, az, r, cimm(1.0), dp<T>(t), cimm(-1.0), dp<T>(q), cdev(dp<double>(alpha)), gate, st);
   }
-  int launches() const override { return 13; }
+  int launches() const override { return 14; }
 };
 
 // A host or device float array of n entries as a device pointer (uploaded if needed).

@@ -385,9 +385,11 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
   DBuf Zb;
   if (flex) Zb.alloc(sizeof(T) * ldv * m);
   T* Z = dp<T>(Zb);
-  auto precon = [&](const T* in, T* out, const int* gate) {
+  // precon(in, out, az): out = M^-1 in (+ the extra stage); with the extra stage and az
+  // given, az = A out comes from the stage and the caller's SpMV is skipped.
+  auto precon = [&](const T* in, T* out, T* az, const int* gate) {
     S.M.apply(np, in, out, gate, st);
-    if (S.extra) S.extra->apply(S, in, out, gate, st);
+    if (S.extra) S.extra->apply(S, in, out, az, gate, st);
   };
   const int precon_launches = 1 + (S.extra ? S.extra->launches() : 0);
   DBuf hb(sizeof(double) * (m + 1) * m), eb(sizeof(double) * (m + 1)), csb(sizeof(double) * (m + 1)),
@@ -438,7 +440,8 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
         ++per_cycle;
       }
       T* Pj = flex ? Z + (size_t)(j - 1) * ldv : PV;
-      precon(Vj, Pj, gskip);
+      const bool az_from_stage = S.extra && fused_mgs && o.gs != PARCEL_B_GS_CGS;
+      precon(Vj, Pj, az_from_stage ? Wv : nullptr, gskip);
       per_cycle += precon_launches;
       if (o.gs == PARCEL_B_GS_CGS) {
         spmv<T, T>(S.A, Pj, Wv, SPMV_Y, nullptr, gskip, st);
@@ -447,7 +450,7 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
                       gskip, st);
         per_cycle += 3;
       } else if (fused_mgs) {
-        spmv<T, T>(S.A, Pj, Wv, SPMV_Y, nullptr, gskip, st);
+        if (!az_from_stage) spmv<T, T>(S.A, Pj, Wv, SPMV_Y, nullptr, gskip, st);
         MgsArgs<T> ma;
         ma.np = np; ma.j = j; ma.w = Wv; ma.V = V; ma.ldv = ldv;
         ma.vnext = (j < m) ? V + (size_t)j * ldv : nullptr;
@@ -457,7 +460,7 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
         ma.gate = gskip;
         ma.red = red(EPI_GM_NORM, 0, j);
         mgs_column<T>(ma, st);
-        per_cycle += 2;
+        per_cycle += az_from_stage ? 1 : 2;
       } else {
         int sa1[2] = {0, 0}, sb1[2] = {2, 0};   // <w, v_1>
         spmv_dot<T, T>(S.A, Pj, Wv, SPMV_Y, nullptr, V, 1, sa1, sb1, red(EPI_GM_H, 1, j), gskip, st);

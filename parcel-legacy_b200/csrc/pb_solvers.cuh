@@ -50,10 +50,12 @@ template <class T>
 struct System;
 
 // An extra preconditioner stage after M (flexible GMRES only): z <- z + stage(r, z).
+// If az is not null the stage also writes A z there (when it can do so without an SpMV
+// of its own), and the caller skips its SpMV of z.
 template <class T>
 struct ExtraStage {
   virtual ~ExtraStage() = default;
-  virtual void apply(const System<T>& S, const T* r, T* z, const int* gate, cudaStream_t st) = 0;
+  virtual void apply(const System<T>& S, const T* r, T* z, T* az, const int* gate, cudaStream_t st) = 0;
   virtual int launches() const = 0;
 };
 
