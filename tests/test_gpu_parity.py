@@ -212,3 +212,19 @@ def test_streaming_mgs_matches_oracle():
     h = res["reshistory"]
     assert np.max(np.abs(h - ho) / ho) < 1e-6
     assert _rel(res["x"], xo) < 1e-6
+
+
+@pytest.mark.parametrize("blocks", [1, 2])
+@pytest.mark.parametrize("ilu", [0, 1])
+def test_wide_levels_precon_matches_oracle(blocks, ilu):
+    """Wavefronts wider than one row per consumer thread (up to 700 rows per level: 2, 4
+    rows per thread) take the multi-row fast sweep."""
+    A = problems.poisson2d_5pt(700, 700)
+    pre = dict(ipreflag=2, ILU_method=ilu, precon_thblock=blocks)
+    r = np.random.default_rng(3).standard_normal(A.n)
+    s_ref = oracle.precon_apply(A, r, **pre)
+    s = np.zeros(A.n)
+    p = _lib.new_input(**pre)
+    rc = _lib.load().parcel_b_precon_apply(C.byref(p), C.byref(api.crs_struct(A)), r.ctypes.data, s.ctypes.data)
+    assert rc == 0, _lib.last_error()
+    assert _rel(s, s_ref) < 1e-11
