@@ -58,9 +58,13 @@ struct DBuf {
     return *this;
   }
   ~DBuf() { release(); }
-  void alloc(size_t b);
-  void release();
+  void alloc(size_t b);    // zero-filled on the library stream; bytes may be rounded up
+  void zero_fill();
+  void release();          // returns the buffer to the library's cache
 };
+
+// Frees every cached buffer (after draining the library stream).
+void release_buffer_cache();
 
 template <class T> inline T* dp(const DBuf& b) { return reinterpret_cast<T*>(b.p); }
 

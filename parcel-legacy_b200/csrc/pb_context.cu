@@ -5,6 +5,7 @@
 // library needs no vendor handles: it selects the device, owns one stream and reports
 // errors as status codes instead of exiting (cu_common.h:119-124 exits on malloc failure).
 #include <cstdarg>
+#include <map>
 #include <mutex>
 
 #include "pb_common.cuh"
@@ -58,22 +59,98 @@ int num_sms() { ensure_init(); return g_sms; }
 
 int red_blocks() { return 4 * num_sms(); }
 
+// ------------------------------------------------------------------ buffer cache
+// Released buffers are kept, keyed by their rounded size, and handed to the next request
+// of that size: a solve repeated on the same problem allocates nothing after the first,
+// and no cudaFree (which waits for the whole device) sits inside a solve.  Reuse is safe
+// because every kernel, copy and memset of the library runs on the one library stream,
+// in order (parcel_b_set_stream drains the old stream before switching).  The cache holds
+// at most kCacheMax bytes, is emptied when cudaMalloc fails (then retried) and by
+// parcel_free_c_.
+namespace {
+std::mutex g_cache_mu;
+std::multimap<size_t, void*> g_cache;
+size_t g_cache_bytes = 0;
+constexpr size_t kCacheMax = size_t(16) << 30;
+
+size_t round_size(size_t b) {
+  const size_t g = b < (size_t(1) << 20) ? 512 : (size_t(2) << 20);
+  return (b + g - 1) / g * g;
+}
+
+void cache_trim_locked() {
+  for (auto& kv : g_cache) cudaFree(kv.second);
+  g_cache.clear();
+  g_cache_bytes = 0;
+}
+}  // namespace
+
+void release_buffer_cache() {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  if (g_ctx.stream) cudaStreamSynchronize(g_ctx.stream);
+  cache_trim_locked();
+}
+
 void DBuf::alloc(size_t b) {
   release();
   if (b == 0) return;
   ensure_init();
-  cudaError_t e = cudaMalloc(&p, b);
+  const size_t rb = round_size(b);
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto it = g_cache.find(rb);
+    if (it != g_cache.end()) {
+      p = it->second;
+      g_cache.erase(it);
+      g_cache_bytes -= rb;
+    }
+  }
+  if (p) {
+    bytes = rb;
+    zero_fill();
+    return;
+  }
+  cudaError_t e = cudaMalloc(&p, rb);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    {
+      std::lock_guard<std::mutex> lk(g_cache_mu);
+      if (g_ctx.stream) cudaStreamSynchronize(g_ctx.stream);
+      cache_trim_locked();
+    }
+    e = cudaMalloc(&p, rb);
+  }
   if (e != cudaSuccess) {
     p = nullptr;
     (void)cudaGetLastError();
-    set_last_error(PARCEL_B_E_NOMEM, "cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
+    set_last_error(PARCEL_B_E_NOMEM, "cudaMalloc(%zu) failed: %s", rb, cudaGetErrorString(e));
     throw Error{PARCEL_B_E_NOMEM, "cudaMalloc failed"};
   }
-  bytes = b;
+  bytes = rb;
+  zero_fill();
+}
+
+// Every buffer starts zeroed (stream-ordered): layout padding positions that no kernel
+// writes (rows of the iteration layout that belong to no matrix row) must hold zeros, not
+// a previous solve's values.
+void DBuf::zero_fill() {
+  cudaError_t e = cudaMemsetAsync(p, 0, bytes, g_ctx.stream);
+  if (e != cudaSuccess) {
+    set_last_error(PARCEL_B_E_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+    throw Error{PARCEL_B_E_CUDA, "cudaMemsetAsync failed"};
+  }
 }
 
 void DBuf::release() {
-  if (p) cudaFree(p);
+  if (p) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    if (g_cache_bytes + bytes <= kCacheMax) {
+      g_cache.emplace(bytes, p);
+      g_cache_bytes += bytes;
+    } else {
+      cudaFree(p);
+    }
+  }
   p = nullptr;
   bytes = 0;
 }
@@ -108,6 +185,7 @@ void parcel_init_c_(int* myrank) {
 }
 
 void parcel_free_c_(void) {
+  pb::release_buffer_cache();
   std::lock_guard<std::mutex> lk(pb::g_mu);
   if (pb::g_ctx.initialised && pb::g_ctx.own_stream && pb::g_ctx.stream) {
     cudaStreamSynchronize(pb::g_ctx.stream);
@@ -120,8 +198,9 @@ int parcel_b_set_stream(void* s) {
   try {
     pb::ensure_init();
     std::lock_guard<std::mutex> lk(pb::g_mu);
+    // drain the old stream: cached buffers may still be read by work queued on it
+    if (pb::g_ctx.stream) cudaStreamSynchronize(pb::g_ctx.stream);
     if (pb::g_ctx.own_stream && pb::g_ctx.stream && s) {
-      cudaStreamSynchronize(pb::g_ctx.stream);
       cudaStreamDestroy(pb::g_ctx.stream);
       pb::g_ctx.own_stream = false;
     }

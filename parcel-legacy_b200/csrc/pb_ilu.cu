@@ -498,39 +498,46 @@ __device__ __forceinline__ void consume_pipelined(const IluSolveArgs<T>& a, uint
   const int NST = a.nstages;
   RowOps<T, KM, R> A, B;
   int done = 0;
-  auto wait_load = [&](RowOps<T, KM, R>& o, int g) -> bool {
-    const int st = g % NST;
-    if (!mbar_wait(&full[st], (g / NST) & 1, kWaitLimit)) {
+  // Stage index and parity of the next chunk to load, advanced by one per chunk (no
+  // division on the per-level path); a stage is released once every consumer holds its
+  // operands in registers.
+  int ls = gbase % NST, lp = (gbase / NST) & 1;
+  auto wait_load = [&](RowOps<T, KM, R>& o, int& rel) -> bool {
+    rel = ls;
+    const bool ok = mbar_wait(&full[ls], lp, kWaitLimit);
+    if (ok) {
+      load_ops<T, KM, R>(o, stages + (size_t)ls * a.stage_bytes, ctid);
+    } else {
       atomicExch(a.err, 3);
       sflags[0] = 1;
-      return false;
     }
-    load_ops<T, KM, R>(o, stages + (size_t)st * a.stage_bytes, ctid);
-    return true;
+    if (++ls == NST) { ls = 0; lp ^= 1; }
+    return ok;
   };
-  auto release = [&](bool ok, int g) {
-    if (ctid == 0 && ok) mbar_arrive(&empty[g % NST]);
+  auto release = [&](bool ok, int st) {
+    if (ctid == 0 && ok) mbar_arrive(&empty[st]);
   };
-  bool ok = wait_load(A, gbase);
+  int relA = 0, relB = 0;
+  bool ok = wait_load(A, relA);
   named_bar_sync(1, kIluConsumerThreads);
-  release(ok, gbase);
+  release(ok, relA);
   done = 1;
   if (!sflags[0]) {
     for (int i = 0; i < nc; i += 2) {
       // chunk i in A, prefetch i+1 into B
       bool okB = true;
-      if (i + 1 < nc) okB = wait_load(B, gbase + i + 1);
+      if (i + 1 < nc) okB = wait_load(B, relB);
       solve_rows<T, DILU, FWD, KM, R>(A, ring, ring, vout, a.accum, ctid);
       named_bar_sync(1, kIluConsumerThreads);
       if (i + 1 >= nc || sflags[0]) { done = i + 1; break; }
-      release(okB, gbase + i + 1);
+      release(okB, relB);
       // chunk i+1 in B, prefetch i+2 into A
       bool okA = true;
-      if (i + 2 < nc) okA = wait_load(A, gbase + i + 2);
+      if (i + 2 < nc) okA = wait_load(A, relA);
       solve_rows<T, DILU, FWD, KM, R>(B, ring, ring, vout, a.accum, ctid);
       named_bar_sync(1, kIluConsumerThreads);
       if (i + 2 >= nc || sflags[0]) { done = i + 2; break; }
-      release(okA, gbase + i + 2);
+      release(okA, relA);
     }
   }
   if (ctid == 0) sflags[1] = gbase + done;
@@ -643,6 +650,7 @@ __global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve_fast(IluSolveArgs<
         return tab[fwd ? c0 + i : c1 - 1 - i];
       };
       ProdDesc cur = fetch(lane);
+      int pst = gbase % NST, puse = gbase / NST;   // stage and reuse count of chunk gbase
       for (int i0 = 0; i0 < nc; i0 += 32) {
         ProdDesc nxt = fetch(i0 + 32 + lane);
         const int kmax = min(32, nc - i0);
@@ -654,9 +662,8 @@ __global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve_fast(IluSolveArgs<
           d.cbytes = __shfl_sync(kFull, cur.cbytes, k);
           d.vbytes = __shfl_sync(kFull, cur.vbytes, k);
           if (lane == 0) {
-            const int g = gbase + i0 + k;
-            const int st = g % NST;
-            const int use = g / NST;
+            const int st = pst, use = puse;
+            if (++pst == NST) { pst = 0; ++puse; }
             if (sflags[0]) {
               stop = true;
             } else if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1, kWaitLimit)) {
@@ -741,6 +748,7 @@ __global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve(IluSolveArgs<T> a)
         return tab[fwd ? c0 + i : c1 - 1 - i];
       };
       ProdDesc cur = fetch(lane);
+      int pst = gbase % NST, puse = gbase / NST;   // stage and reuse count of chunk gbase
       for (int i0 = 0; i0 < nc; i0 += 32) {
         ProdDesc nxt = fetch(i0 + 32 + lane);
         const int kmax = min(32, nc - i0);
@@ -752,9 +760,8 @@ __global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve(IluSolveArgs<T> a)
           d.cbytes = __shfl_sync(kFull, cur.cbytes, k);
           d.vbytes = __shfl_sync(kFull, cur.vbytes, k);
           if (lane == 0) {
-            const int g = gbase + i0 + k;
-            const int st = g % NST;
-            const int use = g / NST;
+            const int st = pst, use = puse;
+            if (++pst == NST) { pst = 0; ++puse; }
             if (sflags[0]) {
               stop = true;
             } else if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1, kWaitLimit)) {
