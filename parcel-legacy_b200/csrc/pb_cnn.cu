@@ -1,15 +1,15 @@
 // pb_cnn.cu -- kernels of the learned coarse-grid preconditioner stage.
 //
-// The four 32 -> 32 convolutions (and their transposes in the backward pass) are implicit
-// GEMMs on the tensor cores: a CTA stages a halo brick of BF16 activations (34 x 6 x 4
-// voxels x 64 B) and all 27 taps of packed weights in shared memory with cp.async, and
-// each warp issues m16n8k16 BF16 MMAs with FP32 accumulation for one line of 32 output
-// voxels x 32 channels.  The weight gradient is the same product with the voxel axis as
-// the reduction axis (ldmatrix.trans on both operands); every CTA writes a partial and a
-// second kernel sums the partials in CTA order, so gradients are deterministic.  The
-// 2 -> 32 input layer and the 32 -> 1 output layer have too few MACs per voxel for the
-// tensor cores and run on the CUDA cores.
+// The four 32 -> 32 convolutions and their transposes (backward pass) run on the
+// 5th-generation tensor cores (tcgen05.mma, BF16 operands in shared memory, FP32
+// accumulators in TMEM; k_conv32_tc).  The weight gradient is the voxel-axis contraction
+// on warp-level MMAs (ldmatrix.trans operands, m16n8k16 BF16 -> FP32); every CTA writes a
+// partial and a second kernel sums the partials in CTA order, so gradients are
+// deterministic.  The 2 -> 32 input layer and the 32 -> 1 output layer have too few MACs
+// per voxel for the tensor cores and run on the CUDA cores.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -31,10 +31,7 @@ constexpr int BX = TX + 2, BY = TY + 2, BZ = TZ + 2;   // halo brick
 constexpr int kBrickRows = BX * BY * BZ;               // 816 voxels
 constexpr int kTileVox = TX * TY * TZ;                 // 256 voxels
 constexpr int kBrickBytes = kBrickRows * 64;           // 52,224 B
-constexpr int kWBytes = kTaps * kCh * 64;              // 55,296 B
-constexpr int kConvSmem = kBrickBytes + kWBytes + kCh * 4;
 constexpr int kWgSmem = kBrickBytes + kTileVox * 64;
-constexpr int kConvThreads = 256;                      // 8 warps: 4 (y) x 2 (z) lines
 constexpr int kWgThreads = 288;                        // 9 warps: 3 taps each
 constexpr int kWgPart = kTaps * kCh * kCh + kCh;       // W then b of one 32 -> 32 layer
 constexpr int kL1Part = kTaps * kCin * kCh + kCh;      // 1,760
@@ -52,6 +49,14 @@ __host__ __device__ inline Tiles tiles_of(const Geo& g, int batch) {
   t.per_sample = (int64_t)t.ntx * t.nty * t.ntz;
   t.total = t.per_sample * batch;
   return t;
+}
+
+// Hidden activations and their gradients are stored chunk-planar: channel group c / 8 of
+// sample b is a plane [gz][gy][gx][8 channels], planes ordered (b, c / 8).  A line of
+// voxels is then 16 contiguous bytes per voxel within a plane, so the tensor copies of the
+// tensor-core convolution move 512-byte rows.
+__host__ __device__ __forceinline__ int64_t aoff(int64_t b, int64_t v, int c, int64_t V) {
+  return ((b * 4 + (c >> 3)) * V + v) * 8 + (c & 7);
 }
 
 // 64-byte rows (32 BF16 channels) of four 16-byte chunks; the chunk index is XORed with
@@ -99,14 +104,14 @@ __device__ __forceinline__ void tile_origin(const Tiles& T, int64_t tile, int64_
 }
 
 // Halo brick of 32-channel BF16 voxels (zero outside the grid) into shared memory.
-__device__ __forceinline__ void load_brick(uint32_t sb, const bf16* in, const Geo& g, int64_t vbase, int x0,
+__device__ __forceinline__ void load_brick(uint32_t sb, const bf16* in, const Geo& g, int64_t b, int x0,
                                            int y0, int z0) {
   for (int idx = threadIdx.x; idx < kBrickRows * 4; idx += blockDim.x) {
     const int row = idx >> 2, ch = idx & 3;
     const int bx = row % BX, r2 = row / BX, by = r2 % BY, bz = r2 / BY;
     const int x = x0 + bx - 1, y = y0 + by - 1, z = z0 + bz - 1;
     const bool ok = (unsigned)x < (unsigned)g.gx && (unsigned)y < (unsigned)g.gy && (unsigned)z < (unsigned)g.gz;
-    const bf16* src = ok ? in + ((vbase + ((int64_t)z * g.gy + y) * g.gx + x) * kCh + ch * 8) : in;
+    const bf16* src = ok ? in + aoff(b, ((int64_t)z * g.gy + y) * g.gx + x, ch * 8, g.V()) : in;
     cp_async16(sb + swz(row, ch), src, ok);
   }
 }
@@ -114,98 +119,249 @@ __device__ __forceinline__ void load_brick(uint32_t sb, const bf16* in, const Ge
 // ---------------------------------------------------------------- 32 -> 32 convolution
 // out = relu(conv3(in, W) + b)                          (forward)
 // out = conv3(in, W') where mask > 0, else 0            (transposed convolution, W' mirrored)
+// ---------------------------------------------------------------- tcgen05 32 -> 32 convolution
+// The same convolution on the 5th-generation tensor cores.  A CTA of 4 warps owns an output
+// tile of 32 (x) x 4 (y) x 2 (z) voxels.  Shared memory holds three copies of the halo brick
+// shifted by dx = -1, 0, +1 (zero outside the grid), each in the canonical K-major
+// no-swizzle layout: for every 8-channel K chunk, the brick's rows (voxels) of 16 bytes one
+// after another.  Lines are 32 rows apart, so for any tap (dz, dy, dx) the 128 A rows of
+// 4 consecutive output lines form 16 core matrices 128 bytes apart (SBO = 128) and the two
+// K chunks of one MMA lie one chunk plane apart (LBO).  The packed weights of all 27 taps
+// use the same layout with N = 32 rows.  One thread issues M=128 N=32 K=16 BF16 MMAs into
+// FP32 accumulators in TMEM: per z plane the taps are dealt round-robin to 4 accumulators
+// (32 columns each), so 8 independent MMA chains are in flight; tcgen05.commit arrives on
+// an mbarrier; each warp then reads its 32 TMEM lanes (one voxel per thread, all 32
+// channels), sums the 4 partial accumulators and applies the bias + ReLU (or ReLU-mask)
+// epilogue with 64-byte stores.  The bricks arrive by tensor copies (TMA).
+constexpr int kTcLinesY = TY + 2, kTcLinesZ = TZ + 2;               // 6 x 4 brick lines
+constexpr int kTcRows = kTcLinesY * kTcLinesZ * TX;                  // 768 rows per copy
+constexpr int kTcPlane = kTcRows * 16;                              // 12,288 B per K chunk
+constexpr int kTcCopy = 4 * kTcPlane;                               // 49,152 B per shifted copy
+constexpr int kTcWTap = 4 * kCh * 16;                               // 2,048 B per tap
+constexpr int kTcWBytes = kTaps * kTcWTap;                          // 55,296 B
+constexpr int kTcSmem = 3 * kTcCopy + kTcWBytes + 256;              // + barrier, TMEM address, bias
+constexpr int kTcThreads = 160;                                     // issuer warp + 4 epilogue warps
+constexpr int kTcSplit = 2;                                         // accumulators per z plane
+constexpr int kTcCols = 2 * TZ * kTcSplit * kCh;                    // two buffers: 256 TMEM columns
+constexpr unsigned kTcWaitLimit = 1u << 24;
+// kind::f16 instruction descriptor: D FP32 (bits 4-5 = 1), A BF16 (7-9 = 1), B BF16
+// (10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kCh >> 3) << 17) | ((128u >> 4) << 24);
+
+// Shared-memory matrix descriptor, no swizzle: start >> 4 (bits 0-13), LBO >> 4 (16-29),
+// SBO >> 4 (32-45), descriptor version 1 (bits 46-47), layout type 0 (bits 61-63).
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+      ::"r"(dtmem), "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate) : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Tensor copy of one box {8 channels, 32 x, 6 y, 4 z, 1 sample} (12,288 bytes) into shared
+// memory; coordinates outside the tensor read zeros.  The innermost coordinate (channel)
+// is a multiple of 8 elements = 16 bytes.
+__device__ __forceinline__ void tma_box5(uint32_t dst, const CUtensorMap* map, int c, int x, int y, int z, int b,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+      ::"r"(dst), "l"(map), "r"(c), "r"(x), "r"(y), "r"(z), "r"(b), "r"(smem_u32(bar)) : "memory");
+}
+
 template <bool DGRAD>
-__global__ void __launch_bounds__(kConvThreads, 2)
-    k_conv32(Geo g, int batch, const bf16* __restrict__ in, const bf16* __restrict__ wpk,
-             const float* __restrict__ bias, const bf16* __restrict__ mask, bf16* __restrict__ out,
-             const int* gate) {
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_conv32_tc(const __grid_constant__ CUtensorMap tmap, Geo g, int batch, const bf16* __restrict__ wpk,
+                const float* __restrict__ bias, const bf16* __restrict__ mask, bf16* __restrict__ out,
+                int* err, const int* gate) {
   if (gated(gate)) return;
   extern __shared__ __align__(128) unsigned char smem[];
-  const uint32_t sb = smem_u32(smem), sw = sb + kBrickBytes;
-  float* sbias = reinterpret_cast<float*>(smem + kBrickBytes + kWBytes);
-  for (int idx = threadIdx.x; idx < kTaps * kCh * 4; idx += kConvThreads) {
-    const int row = idx >> 2, ch = idx & 3;
-    cp_async16(sw + swz(row, ch), wpk + row * kCh + ch * 8, true);
+  const uint32_t sbase = smem_u32(smem);
+  const uint32_t wsm = sbase + 3 * kTcCopy;
+  unsigned char* ctl = smem + 3 * kTcCopy + kTcWBytes;
+  uint64_t* lbar = reinterpret_cast<uint64_t*>(ctl);        // [2] brick halves landed (K chunks 0-1, 2-3)
+  uint64_t* abar = lbar + 2;                                 // MMAs on chunks 0-1 done
+  uint64_t* mbar = lbar + 3;                                 // [2] all MMAs of a tile done, per TMEM buffer
+  uint64_t* ebar = lbar + 5;                                 // [2] TMEM buffer read by the epilogue
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(ctl + 64);
+  float* sbias = reinterpret_cast<float*>(ctl + 128);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // weights of all taps, canonical layout: tap t, K chunk c, row n at t*2048 + c*512 + n*16
+  for (int idx = threadIdx.x; idx < kTaps * kCh * 4; idx += kTcThreads) {
+    const int c = idx & 3, n = (idx >> 2) & 31, t = idx >> 7;
+    cp_async16(wsm + t * kTcWTap + c * (kCh * 16) + n * 16, wpk + (t * kCh + n) * kCh + c * 8, true);
   }
   if (threadIdx.x < kCh) sbias[threadIdx.x] = DGRAD ? 0.f : bias[threadIdx.x];
-  const Tiles T = tiles_of(g, batch);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wy = warp & 3, wz = warp >> 2;
-  const int q = lane >> 3, rr = lane & 7, gq = lane >> 2, tq = lane & 3;
-  const int64_t V = g.V();
-  for (int64_t tile = blockIdx.x; tile < T.total; tile += gridDim.x) {
-    int64_t b;
-    int x0, y0, z0;
-    tile_origin(T, tile, b, x0, y0, z0);
-    load_brick(sb, in, g, b * V, x0, y0, z0);
-    cp_async_wait_all();
-    __syncthreads();
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.f;
-#pragma unroll 1
-    for (int t = 0; t < kTaps; ++t) {
-      const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-      const int rbase = ((wz + 1 + dz) * BY + (wy + 1 + dy)) * BX + 1 + dx;
-#pragma unroll
-      for (int ks = 0; ks < 2; ++ks) {
-        uint32_t a[2][4], bq[4][2];
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt) ldsm_x4(a[mt], sb + swz(rbase + mt * 16 + (q & 1) * 8 + rr, ks * 2 + (q >> 1)));
-#pragma unroll
-        for (int np = 0; np < 2; ++np) {
-          uint32_t r[4];
-          ldsm_x4(r, sw + swz(t * kCh + (np * 2 + (q >> 1)) * 8 + rr, ks * 2 + (q & 1)));
-          bq[np * 2][0] = r[0];
-          bq[np * 2][1] = r[1];
-          bq[np * 2 + 1][0] = r[2];
-          bq[np * 2 + 1][1] = r[3];
-        }
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-          for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[mt][nt], a[mt], bq[nt][0], bq[nt][1]);
-      }
-    }
-    __syncthreads();   // the brick is free: stage the BF16 results there
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-      for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int tv = (wz * TY + wy) * TX + mt * 16 + gq + h * 8;
-          const int co = nt * 8 + tq * 2;
-          float v0 = acc[mt][nt][h * 2], v1 = acc[mt][nt][h * 2 + 1];
-          if (!DGRAD) {
-            v0 = fmaxf(v0 + sbias[co], 0.f);
-            v1 = fmaxf(v1 + sbias[co + 1], 0.f);
-          }
-          *reinterpret_cast<__nv_bfloat162*>(smem + swz(tv, nt) + tq * 4) = __floats2bfloat162_rn(v0, v1);
-        }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < kTileVox * 4; idx += kConvThreads) {
-      const int tv = idx >> 2, ch = idx & 3;
-      const int x = x0 + tv % TX, y = y0 + (tv / TX) % TY, z = z0 + tv / (TX * TY);
-      if (x < g.gx && y < g.gy && z < g.gz) {
-        const int64_t o = (b * V + ((int64_t)z * g.gy + y) * g.gx + x) * kCh + ch * 8;
-        uint4 v = *reinterpret_cast<const uint4*>(smem + swz(tv, ch));
-        if (DGRAD) {
-          const uint4 m = *reinterpret_cast<const uint4*>(mask + o);
-          v.x = mask_pairs(v.x, m.x);
-          v.y = mask_pairs(v.y, m.y);
-          v.z = mask_pairs(v.z, m.z);
-          v.w = mask_pairs(v.w, m.w);
-        }
-        *reinterpret_cast<uint4*>(out + o) = v;
-      }
-    }
-    __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 5; ++i) mbar_init(lbar + i, 1);
+    mbar_init(ebar, 4);
+    mbar_init(ebar + 1, 4);
+    mbar_fence_init();
   }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(kTcCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  cp_async_wait_all();
+  fence_async_shared();   // the weights came through the generic proxy; the MMAs read async
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const Tiles T = tiles_of(g, batch);
+  const int64_t V = g.V();
+
+  if (warp == 0) {
+    // ---------------- issuer: tensor copies and MMAs (one elected lane)
+    if (lane == 0) {
+      auto load_half = [&](int64_t tile, int h) {   // K chunks 2h, 2h+1 of all three copies
+        int64_t b;
+        int x0, y0, z0;
+        tile_origin(T, tile, b, x0, y0, z0);
+        mbar_arrive_expect_tx(lbar + h, 6u * (unsigned)kTcPlane);
+        for (int sh = 0; sh < 3; ++sh)
+          for (int c = 2 * h; c < 2 * h + 2; ++c)
+            tma_box5(sbase + sh * kTcCopy + c * kTcPlane, &tmap, 0, x0 + sh - 1, y0 - 1, z0 - 1, (int)(b * 4 + c),
+                     lbar + h);
+      };
+      // Descriptors of the brick copies and of the weights at offset 0; every operand of the
+      // unrolled loop is that base plus a compile-time offset (>> 4 in the start field).
+      const uint64_t a_base = tc_desc(sbase, kTcPlane, 128);
+      const uint64_t b_base = tc_desc(wsm, kCh * 16, 128);
+      auto mmas = [&](int buf, int ks) {
+        const uint32_t tbuf = tmem + (uint32_t)(buf * TZ * kTcSplit * kCh);
+#pragma unroll
+        for (int t = 0; t < kTaps; ++t) {
+          const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+          const uint64_t bd = b_base + (uint64_t)((t * kTcWTap + 2 * ks * (kCh * 16)) >> 4);
+#pragma unroll
+          for (int zz = 0; zz < TZ; ++zz) {
+            const int row0 = ((zz + 1 + dz) * kTcLinesY + (1 + dy)) * TX;
+            const uint64_t ad = a_base + (uint64_t)(((dx + 1) * kTcCopy + 2 * ks * kTcPlane + row0 * 16) >> 4);
+            // tap t accumulates into chain t % kTcSplit of its z plane
+            tc_mma(tbuf + (uint32_t)((zz * kTcSplit + t % kTcSplit) * kCh), ad, bd, (ks > 0 || t >= kTcSplit) ? 1u : 0u);
+          }
+        }
+      };
+      bool ok = true;
+      int i = 0;
+      int64_t tile = blockIdx.x;
+      if (tile < T.total) { load_half(tile, 0); load_half(tile, 1); }
+      for (; tile < T.total && ok; tile += gridDim.x, ++i) {
+        const int buf = i & 1;
+        const unsigned par = (unsigned)i & 1u, bpar = (unsigned)(i >> 1) & 1u;
+        ok = mbar_wait(lbar, par, kTcWaitLimit);
+        if (ok && i >= 2) ok = mbar_wait(ebar + buf, bpar ^ 1u, kTcWaitLimit);
+        if (!ok) break;
+        tc_fence_after();
+        mmas(buf, 0);
+        tc_commit(abar);
+        ok = mbar_wait(lbar + 1, par, kTcWaitLimit);
+        if (!ok) break;
+        mmas(buf, 1);
+        tc_commit(mbar + buf);
+        const int64_t next = tile + gridDim.x;
+        ok = mbar_wait(abar, par, kTcWaitLimit);             // chunks 0-1 no longer read
+        if (ok && next < T.total) load_half(next, 0);
+        if (ok) ok = mbar_wait(mbar + buf, bpar, kTcWaitLimit);   // chunks 2-3 no longer read
+        if (ok && next < T.total) load_half(next, 1);
+      }
+      if (!ok) atomicExch(err, 4);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue warps 1-4: TMEM lanes 32 (warp % 4) .. + 31 = output line
+    const int q = warp & 3;
+    int i = 0;
+    for (int64_t tile = blockIdx.x; tile < T.total; tile += gridDim.x, ++i) {
+      const int buf = i & 1;
+      const unsigned bpar = (unsigned)(i >> 1) & 1u;
+      if (!mbar_wait(mbar + buf, bpar, kTcWaitLimit)) {
+        atomicExch(err, 6);
+        break;
+      }
+      tc_fence_after();
+      int64_t b;
+      int x0, y0, z0;
+      tile_origin(T, tile, b, x0, y0, z0);
+      float acc[TZ][32];
+#pragma unroll
+      for (int zz = 0; zz < TZ; ++zz) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[zz][j] = 0.f;
+#pragma unroll 1
+        for (int k = 0; k < kTcSplit; ++k) {
+          uint32_t r[32];
+          tc_ld32(tmem + ((uint32_t)(32 * q) << 16) + ((buf * TZ + zz) * kTcSplit + k) * kCh, r);
+#pragma unroll
+          for (int j = 0; j < 32; ++j) acc[zz][j] += __uint_as_float(r[j]);
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(ebar + buf);   // this warp's lanes of the buffer are free
+      const int y = y0 + q, x = x0 + lane;
+#pragma unroll
+      for (int zz = 0; zz < TZ; ++zz) {
+        const int z = z0 + zz;
+        if (x < g.gx && y < g.gy && z < g.gz) {
+          const int64_t vox = ((int64_t)z * g.gy + y) * g.gx + x;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            uint32_t w4[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int co = k * 8 + j * 2;
+              float v0 = acc[zz][co], v1 = acc[zz][co + 1];
+              if (!DGRAD) {
+                v0 = fmaxf(v0 + sbias[co], 0.f);
+                v1 = fmaxf(v1 + sbias[co + 1], 0.f);
+              }
+              __nv_bfloat162 pk = __floats2bfloat162_rn(v0, v1);
+              w4[j] = *reinterpret_cast<uint32_t*>(&pk);
+            }
+            const int64_t o = aoff(b, vox, k * 8, V);
+            if (DGRAD) {
+              const uint4 m = *reinterpret_cast<const uint4*>(mask + o);
+              w4[0] = mask_pairs(w4[0], m.x);
+              w4[1] = mask_pairs(w4[1], m.y);
+              w4[2] = mask_pairs(w4[2], m.z);
+              w4[3] = mask_pairs(w4[3], m.w);
+            }
+            *reinterpret_cast<uint4*>(out + o) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+          }
+        }
+      }
+    }
+  }
+  // every copy and MMA the issuer started has completed or been waited for (bounded) above
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
 }
 
 // ---------------------------------------------------------------- 32 -> 32 weight gradient
@@ -234,12 +390,12 @@ __global__ void __launch_bounds__(kWgThreads, 1)
     int64_t b;
     int x0, y0, z0;
     tile_origin(T, tile, b, x0, y0, z0);
-    load_brick(sb, a_in, g, b * V, x0, y0, z0);
+    load_brick(sb, a_in, g, b, x0, y0, z0);
     for (int idx = threadIdx.x; idx < kTileVox * 4; idx += kWgThreads) {
       const int tv = idx >> 2, ch = idx & 3;
       const int x = x0 + tv % TX, y = y0 + (tv / TX) % TY, z = z0 + tv / (TX * TY);
       const bool ok = x < g.gx && y < g.gy && z < g.gz;
-      const bf16* src = ok ? gout + ((b * V + ((int64_t)z * g.gy + y) * g.gx + x) * kCh + ch * 8) : gout;
+      const bf16* src = ok ? gout + aoff(b, ((int64_t)z * g.gy + y) * g.gx + x, ch * 8, V) : gout;
       cp_async16(sg + swz(tv, ch), src, ok);
     }
     cp_async_wait_all();
@@ -356,7 +512,6 @@ __global__ void __launch_bounds__(256) k_l1_fwd(Geo g, int batch, const __nv_bfl
       acc[c] = fmaf(uv.y, sw[(t * kCin + 1) * kCh + c], acc[c]);
     }
   }
-  uint4* o = reinterpret_cast<uint4*>(out + i * kCh);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     uint32_t w[4];
@@ -365,15 +520,15 @@ __global__ void __launch_bounds__(256) k_l1_fwd(Geo g, int batch, const __nv_bfl
       __nv_bfloat162 p = __floats2bfloat162_rn(fmaxf(acc[k * 8 + j * 2], 0.f), fmaxf(acc[k * 8 + j * 2 + 1], 0.f));
       w[j] = *reinterpret_cast<uint32_t*>(&p);
     }
-    o[k] = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(out + aoff(b, v, k * 8, V)) = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
-__device__ __forceinline__ void unpack32(const bf16* row, float (&a)[kCh]) {
-  const uint4* p = reinterpret_cast<const uint4*>(row);
+// The 32 channels of voxel v of sample b (chunk-planar layout).
+__device__ __forceinline__ void unpack32(const bf16* act, int64_t b, int64_t v, int64_t V, float (&a)[kCh]) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const uint4 q = p[k];
+    const uint4 q = *reinterpret_cast<const uint4*>(act + aoff(b, v, k * 8, V));
     const uint32_t w[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -403,7 +558,7 @@ __global__ void __launch_bounds__(256) k_l6_fwd(Geo g, int batch, const bf16* __
     int64_t nb;
     if (!nb_of(g, x, yy, z, t, 1, nb)) continue;
     float a[kCh];
-    unpack32(a5 + (b * V + nb) * kCh, a);
+    unpack32(a5, b, nb, V, a);
 #pragma unroll
     for (int c = 0; c < kCh; ++c) acc = fmaf(a[c], sw[t * kCh + c], acc);
   }
@@ -433,11 +588,10 @@ __global__ void __launch_bounds__(256) k_l6_dgrad(Geo g, int batch, const float*
 #pragma unroll
     for (int c = 0; c < kCh; ++c) acc[c] = fmaf(sw[t * kCh + c], gv, acc[c]);
   }
-  const uint4* m = reinterpret_cast<const uint4*>(a5 + i * kCh);
-  uint4* o = reinterpret_cast<uint4*>(g5 + i * kCh);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const uint4 mk = m[k];
+    const int64_t off = aoff(b, v, k * 8, V);
+    const uint4 mk = *reinterpret_cast<const uint4*>(a5 + off);
     const uint32_t mw[4] = {mk.x, mk.y, mk.z, mk.w};
     uint32_t w[4];
 #pragma unroll
@@ -445,7 +599,7 @@ __global__ void __launch_bounds__(256) k_l6_dgrad(Geo g, int batch, const float*
       __nv_bfloat162 p = __floats2bfloat162_rn(acc[k * 8 + j * 2], acc[k * 8 + j * 2 + 1]);
       w[j] = mask_pairs(*reinterpret_cast<uint32_t*>(&p), mw[j]);
     }
-    o[k] = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(g5 + off) = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
@@ -468,7 +622,7 @@ __global__ void __launch_bounds__(kWgThreads) k_wgrad_l6(Geo g, int batch, const
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       int64_t nb;
-      if (nb_of(g, x, y, z, w + 9 * k, 1, nb)) acc[k] = fmaf(__bfloat162float(a5[(b * V + nb) * kCh + ci]), gv, acc[k]);
+      if (nb_of(g, x, y, z, w + 9 * k, 1, nb)) acc[k] = fmaf(__bfloat162float(a5[aoff(b, nb, ci, V)]), gv, acc[k]);
     }
   }
   float* P = part + (size_t)blockIdx.x * kL6Part;
@@ -490,7 +644,7 @@ __global__ void __launch_bounds__(kWgThreads) k_wgrad_l1(Geo g, int batch, const
     const int64_t b = i / V, v = i - b * V;
     int x, y, z;
     voxel_xyz(g, v, x, y, z);
-    const float gv = __bfloat162float(g1[i * kCh + co]);
+    const float gv = __bfloat162float(g1[aoff(b, v, co, V)]);
     db += gv;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -759,6 +913,7 @@ void Net::init(uint64_t seed) {
     float* W = h.data() + layer_off(l);
     for (int64_t i = 0; i < layer_w(l); ++i) W[i] = (float)(nd(rng) * sd);
   }
+  err.alloc(sizeof(int));
   master.alloc(sizeof(float) * kNumParams);
   grad.alloc(sizeof(float) * kNumParams);
   adam_m.alloc(sizeof(float) * kNumParams);
@@ -816,15 +971,38 @@ void Acts::ensure(const Geo& gg, int b, bool training) {
 static void set_smem_attrs() {
   static bool done = false;   // attributes are per device function; one device per process
   if (done) return;
-  PB_CUDA(cudaFuncSetAttribute(k_conv32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
-  PB_CUDA(cudaFuncSetAttribute(k_conv32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
   PB_CUDA(cudaFuncSetAttribute(k_wgrad32, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem));
+  PB_CUDA(cudaFuncSetAttribute(k_conv32_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+  PB_CUDA(cudaFuncSetAttribute(k_conv32_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
   done = true;
 }
 
-static int conv_grid(const Geo& g, int batch) {
+// Tensor map over the chunk-planar BF16 activations, dims {8 channels, gx, gy, gz,
+// 4 B planes}, with the brick box {8, 32, 6, 4, 1}: each box row is 16 bytes of one voxel
+// and the 32 voxels of a line are contiguous (512 bytes).  Base and strides are multiples
+// of 16 bytes.
+static CUtensorMap act_map(const bf16* base, const Geo& g, int batch) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    PB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", reinterpret_cast<void**>(&encode), cudaEnableDefault, &q));
+    PB_CHECK(q == cudaDriverEntryPointSuccess && encode, PARCEL_B_E_CUDA, "cuTensorMapEncodeTiled not available");
+  }
+  CUtensorMap m;
+  const cuuint64_t dims[5] = {8, (cuuint64_t)g.gx, (cuuint64_t)g.gy, (cuuint64_t)g.gz, (cuuint64_t)batch * 4};
+  const cuuint64_t strides[4] = {16, (cuuint64_t)g.gx * 16, (cuuint64_t)g.gx * g.gy * 16, (cuuint64_t)g.V() * 16};
+  const cuuint32_t box[5] = {8, (cuuint32_t)TX, (cuuint32_t)kTcLinesY, (cuuint32_t)kTcLinesZ, 1};
+  const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(base), dims, strides, box, es,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  PB_CHECK(r == CUDA_SUCCESS, PARCEL_B_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return m;
+}
+
+static int tc_grid(const Geo& g, int batch) {   // one CTA per SM (203 KB of shared memory)
   const Tiles T = tiles_of(g, batch);
-  return (int)std::min<int64_t>(T.total, 2 * (int64_t)num_sms());
+  return (int)std::min<int64_t>(T.total, (int64_t)num_sms());
 }
 
 void init_kernels() { set_smem_attrs(); }
@@ -846,10 +1024,12 @@ void forward(const Net& net, Acts& A, const int* gate, cudaStream_t st) {
   const float* mp = dp<float>(net.master);
   k_l1_fwd<<<blocks_for(M), 256, 0, st>>>(g, A.batch, dp<__nv_bfloat162>(A.u), dp<float>(net.pk.w0),
                                           mp + layer_off(0) + layer_w(0), dp<bf16>(A.a[0]), gate);
-  const int cg = conv_grid(g, A.batch);
+  const int tg = tc_grid(g, A.batch);
   for (int l = 1; l <= 4; ++l)
-    k_conv32<false><<<cg, kConvThreads, kConvSmem, st>>>(g, A.batch, dp<bf16>(A.a[l - 1]), dp<bf16>(net.pk.fwd[l - 1]),
-                                                         mp + layer_off(l) + layer_w(l), nullptr, dp<bf16>(A.a[l]), gate);
+    k_conv32_tc<false><<<tg, kTcThreads, kTcSmem, st>>>(act_map(dp<bf16>(A.a[l - 1]), g, A.batch), g, A.batch,
+                                                        dp<bf16>(net.pk.fwd[l - 1]),
+                                                        mp + layer_off(l) + layer_w(l), nullptr, dp<bf16>(A.a[l]),
+                                                        dp<int>(net.err), gate);
   k_l6_fwd<<<blocks_for(M), 256, 0, st>>>(g, A.batch, dp<bf16>(A.a[4]), dp<float>(net.pk.w5),
                                           mp + layer_off(5) + layer_w(5), dp<float>(A.y), gate);
   PB_CUDA(cudaGetLastError());
@@ -876,12 +1056,13 @@ void loss_grad(Net& net, Acts& A, const float* target, float target_scale, doubl
   bf16* gnext = dp<bf16>(A.gB);
   const Tiles T = tiles_of(g, A.batch);
   const int nwg = (int)std::min<int64_t>(T.total, nsm);
-  const int cg = conv_grid(g, A.batch);
+  const int tg = tc_grid(g, A.batch);
   for (int l = 4; l >= 1; --l) {
     k_wgrad32<<<nwg, kWgThreads, kWgSmem, st>>>(g, A.batch, dp<bf16>(A.a[l - 1]), gcur, part);
     k_reduce_parts<<<blocks_for(kWgPart), 256, 0, st>>>(part, nwg, kWgPart, kWgPart, gr + layer_off(l));
-    k_conv32<true><<<cg, kConvThreads, kConvSmem, st>>>(g, A.batch, gcur, dp<bf16>(net.pk.bwd[l - 1]), nullptr,
-                                                        dp<bf16>(A.a[l - 1]), gnext, nullptr);
+    k_conv32_tc<true><<<tg, kTcThreads, kTcSmem, st>>>(act_map(gcur, g, A.batch), g, A.batch, dp<bf16>(net.pk.bwd[l - 1]),
+                                                       nullptr,
+                                                       dp<bf16>(A.a[l - 1]), gnext, dp<int>(net.err), nullptr);
     std::swap(gcur, gnext);
   }
   // input layer

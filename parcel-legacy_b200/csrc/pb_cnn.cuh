@@ -61,6 +61,7 @@ struct Packed {
 // Network: parameters, optimiser state and kernel-side packed weights.
 struct Net {
   DBuf master, grad, adam_m, adam_v;
+  DBuf err;                                 // nonzero: a tensor-core wait timed out
   Packed pk;
   int adam_t = 0;
   void init(uint64_t seed);                 // He-normal weights, zero biases

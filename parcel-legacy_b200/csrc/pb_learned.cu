@@ -119,6 +119,13 @@ struct FVec {
   }
 };
 
+// A tensor-core kernel that gave up waiting for its MMAs leaves a code in net.err.
+void check_net(const Learned& L) {
+  int e = 0;
+  d2h(&e, L.net.err.p, sizeof(int));
+  PB_CHECK(e == 0, PARCEL_B_E_CUDA, "network kernel: tensor-core completion wait timed out (code %d)", e);
+}
+
 void copy_out(float* dst, const void* src, size_t bytes) {
   if (is_device_ptr(dst)) { d2d(dst, src, bytes); sync(); }
   else d2h(dst, src, bytes);
@@ -196,6 +203,7 @@ int parcel_b_learned_forward(parcel_b_learned h, int batch, const float* u, floa
     FVec uv(u, 2 * M);
     cnn::to_bf16(2 * M, uv.p, dp<__nv_bfloat16>(L.kern.u), stream());
     cnn::forward(L.net, L.kern, nullptr, stream());
+    check_net(L);
     copy_out(y, L.kern.y.p, sizeof(float) * M);
     return 0;
   });
@@ -211,6 +219,7 @@ int parcel_b_learned_grad(parcel_b_learned h, int batch, const float* u, const f
     FVec uv(u, 2 * M), tv(target, M);
     cnn::to_bf16(2 * M, uv.p, dp<__nv_bfloat16>(L.kern.u), stream());
     cnn::loss_grad(L.net, L.kern, tv.p, 1.f, dp<double>(L.loss), stream());
+    check_net(L);
     if (loss) d2h(loss, L.loss.p, sizeof(double));
     if (grad) copy_out(grad, L.net.grad.p, sizeof(float) * cnn::kNumParams);
     sync();
@@ -343,7 +352,7 @@ int parcel_b_learned_train(parcel_b_learned h, int steps, int batch, double lr, 
       cnn::loss_grad(L.net, L.train, dp<float>(L.tgt), (float)L.scale, dp<double>(L.loss), st);
       d2h(last_loss, L.loss.p, sizeof(double));
     }
-    sync();
+    check_net(L);
     return 0;
   });
 }
