@@ -157,8 +157,10 @@ __global__ void __launch_bounds__(kMgsThreads, 2) k_gm_mgs_stream(MgsArgs<T> a) 
         const int64_t i = (b * EB + u) * nthr + tid;
         const bool ok = i < a.np;
         wv[u] = ok ? w[i] : T(0);
-        vp[u] = (upd && ok) ? __ldcg(vprev + i) : T(0);
-        vc[u] = (dotv && ok) ? __ldcg(vcur + i) : T(0);
+        // basis vectors stream with evict-first loads, so w (read and written every pass)
+        // stays in L2 whenever it fits (an FP32 vector of 16.8M rows is 67 MB)
+        vp[u] = (upd && ok) ? __ldcs(vprev + i) : T(0);
+        vc[u] = (dotv && ok) ? __ldcs(vcur + i) : T(0);
       }
 #pragma unroll
       for (int u = 0; u < EB; ++u) {
