@@ -65,6 +65,15 @@ struct DBuf {
 
 // Frees every cached buffer (after draining the library stream).
 void release_buffer_cache();
+// Page-locked host staging area of at least `bytes`, kept between calls (one user at a
+// time: the set-up of one system).
+void* pinned_staging(size_t bytes);
+
+// Set-up tracing: with PARCEL_B_TRACE=1 in the environment, trace_mark(label) drains the
+// library stream and prints the wall time since the previous mark to stderr.  Off by
+// default (no synchronisation is added then).
+bool trace_on();
+void trace_mark(const char* label);
 
 template <class T> inline T* dp(const DBuf& b) { return reinterpret_cast<T*>(b.p); }
 

@@ -4,7 +4,9 @@
 // GPU (`set_GPU`, cu_common.cu:489-520) and create global cuBLAS/cuSPARSE handles.  This
 // library needs no vendor handles: it selects the device, owns one stream and reports
 // errors as status codes instead of exiting (cu_common.h:119-124 exits on malloc failure).
+#include <chrono>
 #include <cstdarg>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 
@@ -55,6 +57,23 @@ void ensure_init() {
 
 cudaStream_t stream() { ensure_init(); return g_ctx.stream; }
 
+bool trace_on() {
+  static const int on = [] {
+    const char* e = getenv("PARCEL_B_TRACE");
+    return (e && e[0] == '1') ? 1 : 0;
+  }();
+  return on != 0;
+}
+
+void trace_mark(const char* label) {
+  if (!trace_on()) return;
+  static double last = 0.0;
+  cudaStreamSynchronize(g_ctx.stream);
+  const double t = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  if (last > 0.0 && label) fprintf(stderr, "[parcel_b] %-28s %9.3f ms\n", label, (t - last) * 1e3);
+  last = t;
+}
+
 int num_sms() { ensure_init(); return g_sms; }
 
 int red_blocks() { return 4 * num_sms(); }
@@ -85,10 +104,29 @@ void cache_trim_locked() {
 }
 }  // namespace
 
+namespace {
+void* g_pin = nullptr;
+size_t g_pin_bytes = 0;
+}  // namespace
+
+void* pinned_staging(size_t bytes) {
+  if (bytes > g_pin_bytes) {
+    if (g_pin) cudaFreeHost(g_pin);
+    g_pin = nullptr;
+    g_pin_bytes = 0;
+    PB_CUDA(cudaMallocHost(&g_pin, bytes));
+    g_pin_bytes = bytes;
+  }
+  return g_pin;
+}
+
 void release_buffer_cache() {
   std::lock_guard<std::mutex> lk(g_cache_mu);
   if (g_ctx.stream) cudaStreamSynchronize(g_ctx.stream);
   cache_trim_locked();
+  if (g_pin) cudaFreeHost(g_pin);
+  g_pin = nullptr;
+  g_pin_bytes = 0;
 }
 
 void DBuf::alloc(size_t b) {

@@ -109,7 +109,8 @@ void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P) {
   for (int b = 0; b < nb; ++b) P.blk_lvl[b + 1] = P.blk_lvl[b] + nlev[b];
   const int totlev = P.blk_lvl[nb];
   std::vector<int> width(totlev, 0);
-  for (int b = 0; b < nb; ++b)
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int b = 0; b < nb; ++b)   // blocks own disjoint level ranges
     for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) width[P.blk_lvl[b] + P.lev[i]]++;
   P.lvl_start.assign(totlev, 0);
   int cursor = 0, maxw = 0;
@@ -128,6 +129,7 @@ void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P) {
   // positions, stable by natural index within a level
   std::vector<int> fill(totlev, 0);
   P.rowAt.assign(P.np, -1);
+#pragma omp parallel for schedule(dynamic, 1)
   for (int b = 0; b < nb; ++b)
     for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) {
       int gl = P.blk_lvl[b] + P.lev[i];
@@ -135,12 +137,10 @@ void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P) {
       P.pos[i] = q;
       P.rowAt[q] = i;
     }
-  // chunks
-  P.chunks.clear();
-  P.blk_chunk.assign(nb + 1, 0);
-  int64_t offF = 0, offB = 0;
+  // chunks: per block in parallel, then concatenated in block order
+  std::vector<std::vector<IluChunk>> bch(nb);
+#pragma omp parallel for schedule(dynamic, 1)
   for (int b = 0; b < nb; ++b) {
-    P.blk_chunk[b] = (int)P.chunks.size();
     for (int l = 0; l < nlev[b]; ++l) {
       int gl = P.blk_lvl[b] + l;
       for (int o = 0; o < width[gl]; o += kIluChunk) {
@@ -157,62 +157,21 @@ void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P) {
         c.lvl = l;
         c.off_in_level = o;
         c.blk = b;
-        c.offF = offF;
-        c.offB = offB;
-        P.chunks.push_back(c);
+        c.offF = 0;
+        c.offB = 0;
+        bch[b].push_back(c);
       }
     }
   }
+  P.chunks.clear();
+  P.blk_chunk.assign(nb + 1, 0);
+  for (int b = 0; b < nb; ++b) {
+    P.blk_chunk[b] = (int)P.chunks.size();
+    P.chunks.insert(P.chunks.end(), bch[b].begin(), bch[b].end());
+  }
   P.blk_chunk[nb] = (int)P.chunks.size();
-  // permuted row pointer (0-based)
-  P.rowptrP.assign(P.np + 1, 0);
-  for (int q = 0; q < P.np; ++q) {
-    int i = P.rowAt[q];
-    P.rowptrP[q + 1] = P.rowptrP[q] + (i >= 0 ? rp[i + 1] - rp[i] : 0);
-  }
 }
 
-// ------------------------------------------------------------------ permuted matrix
-template <class VT>
-__global__ void k_permute_matrix(int np, const int* __restrict__ rowAt, const int* __restrict__ pos,
-                                 const int* __restrict__ rp, const int* __restrict__ ci,
-                                 const double* __restrict__ va, int rbase, int cbase,
-                                 const int* __restrict__ rpP, int* __restrict__ ciP,
-                                 VT* __restrict__ vaP) {
-  const int lanes = 8;
-  int g = (blockIdx.x * blockDim.x + threadIdx.x) / lanes;
-  int l = threadIdx.x % lanes;
-  int ng = gridDim.x * blockDim.x / lanes;
-  for (int q = g; q < np; q += ng) {
-    int i = rowAt[q];
-    if (i < 0) continue;
-    int a = rp[i] - rbase, z = rp[i + 1] - rbase;
-    int o = rpP[q];
-    for (int j = a + l; j < z; j += lanes) {
-      ciP[o + (j - a)] = pos[ci[j] - cbase];
-      vaP[o + (j - a)] = (VT)va[j];
-    }
-  }
-}
-
-template <class VT>
-void ilu_permute_matrix(const IluPlan& P, const DevMat<double>& A, const int* d_pos,
-                        const int* d_rowAt, PermMat<VT>& out, int64_t nnz) {
-  out.rowptr.alloc(sizeof(int) * (P.np + 1));
-  h2d(out.rowptr.p, P.rowptrP.data(), sizeof(int) * (P.np + 1));
-  out.col.alloc(sizeof(int) * std::max<int64_t>(nnz, 1));
-  out.val.alloc(sizeof(VT) * std::max<int64_t>(nnz, 1));
-  int blocks = 8 * num_sms();
-  k_permute_matrix<VT><<<blocks, 256, 0, stream()>>>(P.np, d_rowAt, d_pos, A.rowptr, A.col, A.val,
-                                                     A.rbase, A.cbase, dp<int>(out.rowptr),
-                                                     dp<int>(out.col), dp<VT>(out.val));
-  PB_CUDA(cudaGetLastError());
-}
-
-template void ilu_permute_matrix<double>(const IluPlan&, const DevMat<double>&, const int*,
-                                         const int*, PermMat<double>&, int64_t);
-template void ilu_permute_matrix<float>(const IluPlan&, const DevMat<double>&, const int*,
-                                        const int*, PermMat<float>&, int64_t);
 
 // ------------------------------------------------------------------ factorisation
 // In-block column range of natural row i (columns sorted): [first, last) positions.
@@ -932,6 +891,7 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   h2d(blvl.p, P.blk_lvl.data(), sizeof(int) * (P.nb + 1));
   h2d(lst.p, P.lvl_start.data(), sizeof(int) * P.lvl_start.size());
 
+  trace_mark("ilu: tables to device");
   // factorisation in natural CSR order
   const int64_t nnz = A.nnz;
   DBuf lu, Dd, Di;
@@ -954,6 +914,7 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
                                       ilu_method == 2 ? 1 : 0, dp<double>(Dd), dp<double>(Di));
     PB_CUDA(cudaGetLastError());
   }
+  trace_mark("ilu: factor");
   D.packF.alloc(D.packF_bytes);
   D.packB.alloc(D.packB_bytes);
   k_ilu_pack<T><<<std::min<int>((int)ch.size(), 65535) > 0 ? std::min<int>((int)ch.size(), 65535) : 1,

@@ -64,7 +64,6 @@ struct IluPlan {
   std::vector<int> pos;         // natural row -> permuted position
   std::vector<int> lev;         // natural row -> level within its block
   std::vector<int> rowAt;       // permuted position -> natural row, -1 = padding
-  std::vector<int> rowptrP;     // permuted 0-based row pointer (np + 1)
   std::vector<IluChunk> chunks;
   std::vector<int> blk_chunk;   // nb + 1
   std::vector<int> blk_lo, blk_hi;   // natural row ranges [lo, hi)
@@ -91,18 +90,7 @@ struct IluDev {
   DBuf err;         // int error flag
 };
 
-// Permuted matrix (0-based) in the layout of the plan.
-template <class VT>
-struct PermMat {
-  DBuf rowptr, col, val;
-  DevMat<VT> view(int np, int64_t nnz) const {
-    DevMat<VT> m;
-    m.n = np; m.nnz = nnz;
-    m.rowptr = dp<int>(rowptr); m.col = dp<int>(col); m.val = dp<VT>(val);
-    return m;
-  }
-};
-
+// Sparsity structure of the natural matrix on the host (for the wavefront plan).
 struct HostCSR {
   int n = 0;
   int64_t nnz = 0;
@@ -112,11 +100,6 @@ struct HostCSR {
 };
 
 void ilu_build_plan(const HostCSR& A, int nblocks, IluPlan& P);
-
-// Builds the permuted copy of A (values cast to VT) on the device.
-template <class VT>
-void ilu_permute_matrix(const IluPlan& P, const DevMat<double>& A, const int* d_pos,
-                        const int* d_rowAt, PermMat<VT>& out, int64_t nnz);
 
 // Factorises (ILU(0)) or computes the D-ILU diagonal on the device and packs the sweep
 // data.  ilu_method: 0 ILU(0), 1 ILUD, 2 MLUD (define.f90:40-42).  Returns a status.

@@ -103,6 +103,7 @@ void Precon<T>::apply(int64_t np, const T* r, T* s, const int* gate, cudaStream_
 template <class T>
 void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& S) {
   cudaStream_t st = stream();
+  trace_mark(nullptr);
   S.n = A.n;
   S.nnz = A.nnz;
   const int* rp = A.rowptr;
@@ -130,21 +131,21 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
 
   if (o.precon == PARCEL_B_PRECON_BLOCKJACOBI) {
     // The wavefront analysis needs the sparsity structure on the host.
-    std::vector<int> hrp, hci;
     const int* hrpp = A.rowptr;
     const int* hcip = A.col;
-    if (dev) {
-      hrp.resize(A.n + 1);
-      hci.resize(A.nnz);
-      d2h(hrp.data(), A.rowptr, sizeof(int) * (A.n + 1));
-      d2h(hci.data(), A.col, sizeof(int) * A.nnz);
-      hrpp = hrp.data();
-      hcip = hci.data();
+    if (dev) {   // through page-locked staging: twice the bandwidth of pageable copies
+      int* pin = static_cast<int*>(pinned_staging(sizeof(int) * ((size_t)A.n + 1 + (size_t)A.nnz)));
+      d2h(pin, A.rowptr, sizeof(int) * (A.n + 1));
+      d2h(pin + A.n + 1, A.col, sizeof(int) * A.nnz);
+      hrpp = pin;
+      hcip = pin + A.n + 1;
     }
+    trace_mark("setup: structure to host");
     HostCSR H;
     H.n = A.n; H.nnz = A.nnz; H.istart = A.istart; H.rowptr = hrpp; H.col = hcip;
     IluPlan P;
     ilu_build_plan(H, std::max(1, std::min(o.nblocks, A.n)), P);
+    trace_mark("setup: wavefront plan (host)");
     S.np = P.np;
     S.permuted = true;
     S.ilu_levels_max = P.max_levels;
@@ -155,6 +156,7 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
     h2d(S.pos.p, P.pos.data(), sizeof(int) * A.n);
     h2d(S.lev.p, P.lev.data(), sizeof(int) * A.n);
     h2d(S.rowAt.p, P.rowAt.data(), sizeof(int) * P.np);
+    trace_mark("setup: layout maps to device");
     {
       std::vector<int> len(A.n);
       for (int i = 0; i < A.n; ++i) len[i] = hrpp[i + 1] - hrpp[i];
@@ -162,8 +164,10 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
       S.A.nnz = A.nnz;
       build_sell<T>(S.Anat, P.np, P.rowAt, dp<int>(S.rowAt), dp<int>(S.pos), len, S.Asell, S.A);
     }
+    trace_mark("setup: sliced ELLPACK");
     ilu_setup_device<T>(P, S.Anat, o.ilu_method, dp<int>(S.pos), dp<int>(S.rowAt),
                         dp<int>(S.lev), S.M.ilu);
+    trace_mark("setup: ILU factor + pack");
   } else {
     S.np = A.n;
     S.permuted = false;

@@ -68,7 +68,6 @@ struct System {
   bool permuted = false;
   DevMat<double> Anat;  // natural matrix (reference layout)
   DBuf up_rowptr, up_col, up_val;   // uploaded copies of host inputs
-  PermMat<T> Ap;        // permuted matrix (block Jacobi)
   SellBuf<T> Asell;     // sliced-ELLPACK copy used by the SpMV
   DevMat<T> A;          // matrix of the iteration
   DBuf Aval_T;          // natural values cast to T (FP32 path, no permutation)
