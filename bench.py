@@ -107,6 +107,17 @@ class Clocks:
                 "samples": len(rows)}
 
 
+def reduce_max(values, dist=None, device=None):
+    """Element-wise maximum of a list of floats over all ranks (the slowest rank's times);
+    the values themselves on a single process."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def dist_setup(ngpus):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -122,7 +133,7 @@ def run_ours(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from parcel_b import _lib, api
     L = _lib.load()
     A, b = problem()
@@ -170,13 +181,7 @@ def run_ours(args):
         stats.append(_lib.last_stats())
     torch.cuda.synchronize()
     clocks = clk.stop()
-    step_s = max(times)
-    if dist:
-        tt = torch.tensor([step_s, sum(times)], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        step_s, tot = float(tt[0]), float(tt[1])
-    else:
-        tot = sum(times)
+    step_s, tot = reduce_max([max(times), sum(times)], dist, dev)
     value = tot / args.steps
     relres = stats[-1]["true_relres"]
 
