@@ -215,6 +215,217 @@ __global__ void __launch_bounds__(kMgsThreads, 2) k_gm_mgs_stream(MgsArgs<T> a) 
   }
 }
 
+
+// Shared-memory-staged variant, for vectors of which the grid's shared memory holds two
+// copies (about 2.1M FP64 or 4.2M FP32 rows on 148 SMs).  One CTA per SM owns a contiguous
+// range of R rows: w stays in the registers of 16 consumer warps, and the CTA's slices of
+// two basis vectors sit in shared memory -- v_{p-1} (for the update) and v_p (for the dot
+// product), v_k in buffer k & 1.  A producer warp moves the slices with bulk copies (TMA)
+// in chunks of kMgsChunk elements per consumer thread: chunk c of buffer q completes on
+// full[q][c], and the consumers release it on empty[q][c] once pass p has read v_{p-1}
+// from it, whereupon the producer refills it with v_{p+1}.  Copy issue blocks under memory
+// back-pressure, so it lives in its own warp: the consumers' sweep never waits for an
+// issue, and the copy queue stays full while the grid reduction runs.  Every basis byte is
+// read from HBM once per column.
+//
+// Grid reduction without a counter: CTA b stores its partial sum of pass p in slot
+// (p, b); warp 0 of CTA 0 waits until the pass's G slots are all written, sums them in a
+// fixed order and stores the total in total(p); every CTA waits for total(p).  All slots
+// hold the all-ones bit pattern (a NaN no arithmetic produces) before the launch and are
+// written once per launch; a partial or total that is itself a NaN is stored as the
+// canonical quiet NaN, so that it cannot read as empty.  Two L2 round trips per pass;
+// an all-to-all read of the slots costs more because 148 CTAs contend for the same lines.
+// Waits are bounded: a wait that runs out sets *err, and the CTA stops waiting and
+// issuing, then waits (bounded) for the copies it has in flight before it exits.
+constexpr int kMgsConsumers = 512;                    // consumer threads (16 warps)
+constexpr int kMgsTmaThreads = kMgsConsumers + 32;    // + one producer warp
+constexpr int kMgsChunk = 4;                          // elements per consumer per chunk
+constexpr unsigned long long kMgsEmpty = ~0ull;       // empty slot
+constexpr unsigned kSlotLimit = 1u << 21;
+constexpr unsigned kCopyLimit = 1u << 20;
+constexpr int kMgsSlotsPerLane = 8;                   // grids of up to 256 CTAs
+
+__device__ __forceinline__ unsigned long long ld_slot(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_slot(double* p, double v) {
+  if (v != v) v = __longlong_as_double(0x7ff8000000000000ll);
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(__double_as_longlong(v)) : "memory");
+}
+
+template <class T, int ELEMS>
+__global__ void __launch_bounds__(kMgsTmaThreads, 1) k_gm_mgs_tma(MgsArgs<T> a, int R) {
+  if (gated(a.gate)) return;
+  constexpr int NT = kMgsConsumers, CH = NT * kMgsChunk, NC = (ELEMS + kMgsChunk - 1) / kMgsChunk;
+  extern __shared__ __align__(128) unsigned char mgs_smem[];
+  __shared__ __align__(8) uint64_t full[2][NC], empty[2][NC];
+  __shared__ double wsum[NT / 32];
+  __shared__ double total;
+  __shared__ int sbad;
+  T* const b0 = reinterpret_cast<T*>(mgs_smem);
+  T* const b1 = b0 + R;
+  const int G = gridDim.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int j = a.j;
+  const int64_t row0 = (int64_t)blockIdx.x * R;
+  const int rows = (int)max((int64_t)0, min((int64_t)R, a.np - row0));   // rows owned
+  const int crows = (rows + 31) & ~31;   // rows copied (within ldv: ldv is a multiple of 32)
+  const int nch = (crows + CH - 1) / CH;
+  if (t == 0) {
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 2; ++q) {
+        mbar_init(&full[q][c], 1);
+        mbar_init(&empty[q][c], NT / 32);
+      }
+    sbad = 0;
+    mbar_fence_init();
+  }
+  __syncthreads();
+  double S = 0.0;
+  int last0 = 0, last1 = 0, cnt0 = 0, cnt1 = 0;   // (producer) last copy per buffer, chunks
+  if (warp == NT / 32) {
+    // ---------------------------------------------------------------- producer warp
+    if (lane == 0) {
+      auto issue = [&](int k, int c) {                 // chunk c of v_k into buffer k & 1
+        const int r0 = c * CH, nr = min(CH, crows - r0);
+        const unsigned bytes = (unsigned)(nr * sizeof(T));
+        uint64_t* bar = &full[k & 1][c];
+        mbar_arrive_expect_tx(bar, bytes);
+        bulk_g2s(((k & 1) ? b1 : b0) + r0, a.V + (size_t)(k - 1) * a.ldv + row0 + r0, bytes, bar);
+        if (k & 1) { cnt1 = last1 == k ? c + 1 : 1; last1 = k; }
+        else { cnt0 = last0 == k ? c + 1 : 1; last0 = k; }
+      };
+      for (int k = 1; k <= min(j, 2); ++k)
+        for (int c = 0; c < nch; ++c) issue(k, c);
+      // v_k (k >= 3) replaces v_{k-2}, released in pass k-1: the ((k-3)/2)-th release
+      for (int k = 3; k <= j && !sbad; ++k)
+        for (int c = 0; c < nch; ++c) {
+          if (!mbar_wait(&empty[k & 1][c], ((k - 3) >> 1) & 1, kCopyLimit)) {
+            sbad = 1;
+            atomicExch(a.err, 1);
+            break;
+          }
+          issue(k, c);
+        }
+    }
+  } else {
+    // ---------------------------------------------------------------- consumer warps
+    T w[ELEMS];
+#pragma unroll
+    for (int e = 0; e < ELEMS; ++e) {
+      const int lr = t + e * NT;
+      w[e] = lr < rows ? a.w[row0 + lr] : T(0);
+    }
+    double hprev = 0.0;
+    for (int p = 1; p <= j + 1; ++p) {
+      const bool upd = p > 1, dotv = p <= j, release = upd && p + 1 <= j;
+      const T mh = (T)(-hprev);
+      const T* bu = (p & 1) ? b0 : b1;   // v_{p-1}
+      const T* bd = (p & 1) ? b1 : b0;   // v_p
+      const unsigned par = ((p - 1) >> 1) & 1;   // v_p is the ((p-1)/2)-th copy into its buffer
+      double part = 0.0;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        if (c < nch) {
+          if (dotv && !sbad && !mbar_wait(&full[p & 1][c], par, kCopyLimit)) {
+            sbad = 1;
+            atomicExch(a.err, 1);
+          }
+#pragma unroll
+          for (int u = 0; u < kMgsChunk; ++u) {
+            const int e = c * kMgsChunk + u, lr = t + e * NT;
+            if (e < ELEMS && lr < rows) {
+              T& we = w[e];
+              if (upd) we = mh * bu[lr] + we;                          // w = -h v + 1*w
+              part += dotv ? (double)(we * bd[lr]) : (double)(we * we);
+            }
+          }
+          if (release) {   // this warp is done with chunk c of v_{p-1}
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[(p - 1) & 1][c]);
+          }
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+      if (lane == 0) wsum[warp] = part;
+      named_bar_sync(1, NT);
+      if (warp == 0) {
+        double* sl = a.slots + (size_t)(p - 1) * G;
+        if (lane == 0) {
+          double s = 0.0;
+          for (int i = 0; i < NT / 32; ++i) s += wsum[i];
+          st_slot(sl + blockIdx.x, s);
+        }
+        bool bad = sbad != 0;
+        if (blockIdx.x == 0) {   // aggregator: all partial loads in flight at once
+          unsigned long long v[kMgsSlotsPerLane];
+#pragma unroll
+          for (int i = 0; i < kMgsSlotsPerLane; ++i)
+            v[i] = lane + 32 * i < G ? ld_slot(sl + lane + 32 * i) : 0ull;
+          for (unsigned it = 0;; ++it) {
+            bool pending = false;
+#pragma unroll
+            for (int i = 0; i < kMgsSlotsPerLane; ++i) pending |= v[i] == kMgsEmpty;
+            if (!pending || bad) break;
+            if (it >= kSlotLimit) {
+              bad = true;
+              break;
+            }
+#pragma unroll
+            for (int i = 0; i < kMgsSlotsPerLane; ++i)
+              if (v[i] == kMgsEmpty) v[i] = ld_slot(sl + lane + 32 * i);
+          }
+          double s = 0.0;
+#pragma unroll
+          for (int i = 0; i < kMgsSlotsPerLane; ++i) s += __longlong_as_double(v[i]);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+          if (lane == 0) st_slot(a.totals + (p - 1), s);
+        }
+        if (lane == 0) {
+          unsigned long long v = ld_slot(a.totals + (p - 1));
+          for (unsigned it = 0; v == kMgsEmpty && !bad; v = ld_slot(a.totals + (p - 1)))
+            if (++it > kSlotLimit) bad = true;
+          total = __longlong_as_double(v);
+        }
+        if (__any_sync(kFull, bad) && lane == 0) {
+          sbad = 1;
+          atomicExch(a.err, 1);
+        }
+      }
+      named_bar_sync(1, NT);
+      S = total;
+      if (p <= j) {
+        hprev = S;
+        if (blockIdx.x == 0 && t == 0) a.red.ea.h[(size_t)(j - 1) * (a.red.ea.m + 1) + (p - 1)] = S;
+      } else if (a.vnext) {   // v_{j+1} = (1/||w||) w
+        const T inv = (T)(1.0 / sqrt(S));
+#pragma unroll
+        for (int e = 0; e < ELEMS; ++e) {
+          const int lr = t + e * NT;
+          if (lr < rows) a.vnext[row0 + lr] = inv * w[e];
+        }
+      }
+    }
+  }
+  __syncthreads();   // producer and consumers
+  if (blockIdx.x == 0 && t == 0) epilogue(&S, 1, a.red);   // EPI_GM_NORM: h(j+1,j), Givens, stop test
+  if (sbad && t == NT) {
+    // After a failed wait the consumers may not have waited for every copy: wait (bounded)
+    // for the last copy into every chunk -- chunks [0, cnt) of a buffer last received
+    // v_k, the others v_{k-2}.
+    for (int q = 0; q < 2; ++q) {
+      const int k = q ? last1 : last0, cnt = q ? cnt1 : cnt0;
+      for (int c = 0; c < nch; ++c) {
+        const int kc = c < cnt ? k : k - 2;
+        if (kc > 0) mbar_wait(&full[q][c], ((kc - 1) >> 1) & 1, kCopyLimit);
+      }
+    }
+  }
+}
+
 template <class T>
 int mgs_elems_needed(int64_t np, int grid) {
   int64_t nthr = (int64_t)grid * kMgsThreads;
@@ -266,6 +477,49 @@ int mgs_grid() {
   return g;
 }
 
+// Rows per CTA of the staged variant (a multiple of 32), or 0 when two slices of that
+// length do not fit one CTA's shared memory or 32 elements per thread.
+template <class T>
+static int mgs_tma_rows(int64_t np) {
+  static int cap = -1;
+  if (cap < 0) {
+    int optin = 0, dev = 0;
+    PB_CUDA(cudaGetDevice(&dev));
+    PB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa;
+    PB_CUDA(cudaFuncGetAttributes(&fa, k_gm_mgs_tma<T, 32>));
+    cap = std::max(0, optin - (int)fa.sharedSizeBytes);
+    for (auto f : {k_gm_mgs_tma<T, 4>, k_gm_mgs_tma<T, 8>, k_gm_mgs_tma<T, 16>, k_gm_mgs_tma<T, 24>,
+                   k_gm_mgs_tma<T, 30>, k_gm_mgs_tma<T, 32>})
+      PB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+  }
+  const int G = num_sms();
+  if (np <= 0 || G <= 0 || G > 32 * kMgsSlotsPerLane) return 0;
+  const int64_t R = (((np + G - 1) / G) + 31) & ~int64_t(31);
+  if (R > 32 * kMgsConsumers || 2 * R * (int64_t)sizeof(T) > cap) return 0;
+  return (int)R;
+}
+
+template <class T>
+bool mgs_staged(int64_t np) {
+  return mgs_tma_rows<T>(np) > 0;
+}
+
+template <class T, int E>
+static void launch_tma(const MgsArgs<T>& a, int R, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(num_sms());
+  cfg.blockDim = dim3(kMgsTmaThreads);
+  cfg.dynamicSmemBytes = 2 * (size_t)R * sizeof(T);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  PB_CUDA(cudaLaunchKernelEx(&cfg, k_gm_mgs_tma<T, E>, a, R));
+}
+
 template <class T>
 bool mgs_supported(int64_t np) {
   return np > 0;   // register-resident up to 32 elements per thread, streaming beyond
@@ -273,6 +527,16 @@ bool mgs_supported(int64_t np) {
 
 template <class T>
 void mgs_column(const MgsArgs<T>& a, cudaStream_t st) {
+  if (const int R = mgs_tma_rows<T>(a.np)) {
+    PB_CHECK(a.slots != nullptr && a.totals != nullptr, PARCEL_B_E_ARG, "staged MGS launched without slots");
+    if (R <= 4 * kMgsConsumers) launch_tma<T, 4>(a, R, st);
+    else if (R <= 8 * kMgsConsumers) launch_tma<T, 8>(a, R, st);
+    else if (R <= 16 * kMgsConsumers) launch_tma<T, 16>(a, R, st);
+    else if (R <= 24 * kMgsConsumers) launch_tma<T, 24>(a, R, st);
+    else if (R <= 30 * kMgsConsumers) launch_tma<T, 30>(a, R, st);
+    else launch_tma<T, 32>(a, R, st);
+    return;
+  }
   const int grid = mgs_grid<T>();
   switch (mgs_elems_needed<T>(a.np, grid)) {
     case 1: launch_e<T, 1>(a, grid, st); break;
@@ -291,5 +555,7 @@ template void mgs_column<double>(const MgsArgs<double>&, cudaStream_t);
 template void mgs_column<float>(const MgsArgs<float>&, cudaStream_t);
 template int mgs_grid<double>();
 template int mgs_grid<float>();
+template bool mgs_staged<double>(int64_t);
+template bool mgs_staged<float>(int64_t);
 
 }  // namespace pb

@@ -17,6 +17,8 @@ struct MgsArgs {
   T* vnext = nullptr;     // v_{j+1} destination (null for the last column of a cycle)
   double* parts = nullptr;   // 2 * grid partial sums
   unsigned* ctr = nullptr;   // j+1 zeroed barrier counters
+  double* slots = nullptr;   // staged variant: (j+1) x num_sms() partial-sum slots and
+  double* totals = nullptr;  // j+1 total slots, all preset to all-ones bytes (mgs_staged)
   int* err = nullptr;
   const int* gate = nullptr;
   Red red;                // EPI_GM_NORM epilogue arguments
@@ -25,5 +27,9 @@ struct MgsArgs {
 template <class T> bool mgs_supported(int64_t np);
 template <class T> void mgs_column(const MgsArgs<T>& a, cudaStream_t st);
 template <class T> int mgs_grid();
+// True when mgs_column runs the shared-memory-staged variant for this length; it then
+// uses MgsArgs::slots (j+1 rows of num_sms() doubles) and MgsArgs::totals (j+1 doubles),
+// every byte 0xFF before the launch, instead of ctr / parts.
+template <class T> bool mgs_staged(int64_t np);
 
 }  // namespace pb

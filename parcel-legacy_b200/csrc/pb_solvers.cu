@@ -424,13 +424,21 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
   }
   // Fused one-launch MGS (pb_mgs.cu) when the vector fits its register tiling.
   const bool fused_mgs = o.gs != PARCEL_B_GS_CGS && o.fused_mgs && mgs_supported<T>(np);
+  // The staged variant reduces through per-(column, pass, CTA) slots that start every
+  // cycle as all-ones bytes; the others through per-(column, pass) counters that start at 0.
+  const bool staged_mgs = fused_mgs && mgs_staged<T>(np);
+  const size_t nslots = (size_t)m * (m + 2) * (size_t)(num_sms() + 1);   // partials, then totals
   DBuf mparts(sizeof(double) * 2 * (size_t)std::max(1, mgs_grid<T>())),
-      mctr(sizeof(unsigned) * (size_t)m * (m + 2)), merr(sizeof(int));
+      mctr(sizeof(unsigned) * (size_t)m * (m + 2)), merr(sizeof(int)),
+      mslots(staged_mgs ? sizeof(double) * nslots : 0);
   PB_CUDA(cudaMemsetAsync(merr.p, 0, sizeof(int), st));
   int per_cycle = 0;
   auto cycle = [&] {
     per_cycle = 0;
-    if (fused_mgs) {
+    if (staged_mgs) {
+      PB_CUDA(cudaMemsetAsync(mslots.p, 0xFF, sizeof(double) * nslots, st));
+      ++per_cycle;
+    } else if (fused_mgs) {
       PB_CUDA(cudaMemsetAsync(mctr.p, 0, sizeof(unsigned) * (size_t)m * (m + 2), st));
       ++per_cycle;
     }
@@ -460,6 +468,10 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
         ma.vnext = (j < m) ? V + (size_t)j * ldv : nullptr;
         ma.parts = dp<double>(mparts);
         ma.ctr = dp<unsigned>(mctr) + (size_t)(j - 1) * (m + 2);
+        if (staged_mgs) {
+          ma.slots = dp<double>(mslots) + (size_t)(j - 1) * (m + 2) * num_sms();
+          ma.totals = dp<double>(mslots) + (size_t)m * (m + 2) * num_sms() + (size_t)(j - 1) * (m + 2);
+        }
         ma.err = dp<int>(merr);
         ma.gate = gskip;
         ma.red = red(EPI_GM_NORM, 0, j);
