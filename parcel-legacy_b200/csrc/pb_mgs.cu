@@ -218,15 +218,17 @@ __global__ void __launch_bounds__(kMgsThreads, 2) k_gm_mgs_stream(MgsArgs<T> a) 
 
 // Shared-memory-staged variant, for vectors of which the grid's shared memory holds two
 // copies (about 2.1M FP64 or 4.2M FP32 rows on 148 SMs).  One CTA per SM owns a contiguous
-// range of R rows: w stays in the registers of 16 consumer warps, and the CTA's slices of
+// range of R rows: w stays in the registers of 15 consumer warps, and the CTA's slices of
 // two basis vectors sit in shared memory -- v_{p-1} (for the update) and v_p (for the dot
 // product), v_k in buffer k & 1.  A producer warp moves the slices with bulk copies (TMA)
-// in chunks of kMgsChunk elements per consumer thread: chunk c of buffer q completes on
-// full[q][c], and the consumers release it on empty[q][c] once pass p has read v_{p-1}
-// from it, whereupon the producer refills it with v_{p+1}.  Copy issue blocks under memory
-// back-pressure, so it lives in its own warp: the consumers' sweep never waits for an
-// issue, and the copy queue stays full while the grid reduction runs.  Every basis byte is
-// read from HBM once per column.
+// in chunks of kMgsChunk elements per consumer thread; all chunks of one copy of a vector
+// complete on full[q] (one wait per pass: the copy of v_p is issued a whole pass before it
+// is needed, and 15 warps polling one mbarrier word per chunk cost more than the chunks'
+// arrival times could save).  The consumers release chunk c of v_{p-1} on empty[q][c] as
+// soon as pass p has read it, whereupon the producer refills it with v_{p+1}.  Copy issue
+// blocks under memory back-pressure, so it lives in its own warp: the consumers' sweep
+// never waits for an issue, and the copy queue stays full while the grid reduction runs.
+// Every basis byte is read from HBM once per column.
 //
 // Grid reduction without a counter: CTA b stores its partial sum of pass p in slot
 // (p, b); warp 0 of CTA 0 waits until the pass's G slots are all written, sums them in a
@@ -237,8 +239,10 @@ __global__ void __launch_bounds__(kMgsThreads, 2) k_gm_mgs_stream(MgsArgs<T> a) 
 // an all-to-all read of the slots costs more because 148 CTAs contend for the same lines.
 // Waits are bounded: a wait that runs out sets *err, and the CTA stops waiting and
 // issuing, then waits (bounded) for the copies it has in flight before it exits.
-constexpr int kMgsConsumers = 512;                    // consumer threads (16 warps)
-constexpr int kMgsTmaThreads = kMgsConsumers + 32;    // + one producer warp
+// 15 consumer warps and one producer warp: 4 warps per SM sub-partition, so that each
+// thread can hold 128 registers (a 17th warp would cap them at 96)
+constexpr int kMgsConsumers = 480;
+constexpr int kMgsTmaThreads = kMgsConsumers + 32;
 constexpr int kMgsChunk = 4;                          // elements per consumer per chunk
 constexpr unsigned long long kMgsEmpty = ~0ull;       // empty slot
 constexpr unsigned kSlotLimit = 1u << 21;
@@ -260,7 +264,7 @@ __global__ void __launch_bounds__(kMgsTmaThreads, 1) k_gm_mgs_tma(MgsArgs<T> a, 
   if (gated(a.gate)) return;
   constexpr int NT = kMgsConsumers, CH = NT * kMgsChunk, NC = (ELEMS + kMgsChunk - 1) / kMgsChunk;
   extern __shared__ __align__(128) unsigned char mgs_smem[];
-  __shared__ __align__(8) uint64_t full[2][NC], empty[2][NC];
+  __shared__ __align__(8) uint64_t full[2], empty[2][NC];
   __shared__ double wsum[NT / 32];
   __shared__ double total;
   __shared__ int sbad;
@@ -273,41 +277,58 @@ __global__ void __launch_bounds__(kMgsTmaThreads, 1) k_gm_mgs_tma(MgsArgs<T> a, 
   const int crows = (rows + 31) & ~31;   // rows copied (within ldv: ldv is a multiple of 32)
   const int nch = (crows + CH - 1) / CH;
   if (t == 0) {
-    for (int c = 0; c < NC; ++c)
-      for (int q = 0; q < 2; ++q) {
-        mbar_init(&full[q][c], 1);
-        mbar_init(&empty[q][c], NT / 32);
-      }
+    for (int q = 0; q < 2; ++q) {
+      mbar_init(&full[q], 1);
+      for (int c = 0; c < NC; ++c) mbar_init(&empty[q][c], NT / 32);
+    }
     sbad = 0;
     mbar_fence_init();
   }
   __syncthreads();
   double S = 0.0;
-  int last0 = 0, last1 = 0, cnt0 = 0, cnt1 = 0;   // (producer) last copy per buffer, chunks
+  int last0 = 0, last1 = 0;   // (producer) last vector whose copy into buffer 0 / 1 is complete
   if (warp == NT / 32) {
     // ---------------------------------------------------------------- producer warp
-    if (lane == 0) {
-      auto issue = [&](int k, int c) {                 // chunk c of v_k into buffer k & 1
+    if (lane == 0 && nch > 0) {   // a CTA without rows copies and waits for nothing
+      // chunk c of v_k into buffer k & 1; the arrival after the last chunk closes the copy
+      auto issue = [&](int k, int c) {
         const int r0 = c * CH, nr = min(CH, crows - r0);
         const unsigned bytes = (unsigned)(nr * sizeof(T));
-        uint64_t* bar = &full[k & 1][c];
-        mbar_arrive_expect_tx(bar, bytes);
-        bulk_g2s(((k & 1) ? b1 : b0) + r0, a.V + (size_t)(k - 1) * a.ldv + row0 + r0, bytes, bar);
-        if (k & 1) { cnt1 = last1 == k ? c + 1 : 1; last1 = k; }
-        else { cnt0 = last0 == k ? c + 1 : 1; last0 = k; }
+        mbar_expect_tx(&full[k & 1], bytes);
+        bulk_g2s(((k & 1) ? b1 : b0) + r0, a.V + (size_t)(k - 1) * a.ldv + row0 + r0, bytes, &full[k & 1]);
       };
-      for (int k = 1; k <= min(j, 2); ++k)
-        for (int c = 0; c < nch; ++c) issue(k, c);
-      // v_k (k >= 3) replaces v_{k-2}, released in pass k-1: the ((k-3)/2)-th release
-      for (int k = 3; k <= j && !sbad; ++k)
+      auto close = [&](int k) {
+        mbar_arrive(&full[k & 1]);
+        if (k & 1) last1 = k; else last0 = k;
+      };
+      auto fail = [&] {
+        sbad = 1;
+        atomicExch(a.err, 1);
+      };
+      for (int c = 0; c < nch; ++c) issue(1, c);
+      close(1);
+      // v_2 streams while pass 1 runs: w and v_1 get the bandwidth first
+      if (j >= 2) {
+        if (mbar_wait(&full[1], 0, kCopyLimit)) {
+          for (int c = 0; c < nch; ++c) issue(2, c);
+          close(2);
+        } else {
+          fail();
+        }
+      }
+      // v_k (k >= 3) replaces v_{k-2}, released in pass k-1: the ((k-3)/2)-th release.
+      // A failed wait still closes the copy, so that its phase completes once the chunks
+      // already issued have landed.
+      for (int k = 3; k <= j && !sbad; ++k) {
         for (int c = 0; c < nch; ++c) {
           if (!mbar_wait(&empty[k & 1][c], ((k - 3) >> 1) & 1, kCopyLimit)) {
-            sbad = 1;
-            atomicExch(a.err, 1);
+            fail();
             break;
           }
           issue(k, c);
         }
+        close(k);
+      }
     }
   } else {
     // ---------------------------------------------------------------- consumer warps
@@ -325,13 +346,13 @@ __global__ void __launch_bounds__(kMgsTmaThreads, 1) k_gm_mgs_tma(MgsArgs<T> a, 
       const T* bd = (p & 1) ? b1 : b0;   // v_p
       const unsigned par = ((p - 1) >> 1) & 1;   // v_p is the ((p-1)/2)-th copy into its buffer
       double part = 0.0;
+      if (dotv && nch > 0 && !sbad && !mbar_wait(&full[p & 1], par, kCopyLimit)) {
+        sbad = 1;
+        atomicExch(a.err, 1);
+      }
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         if (c < nch) {
-          if (dotv && !sbad && !mbar_wait(&full[p & 1][c], par, kCopyLimit)) {
-            sbad = 1;
-            atomicExch(a.err, 1);
-          }
 #pragma unroll
           for (int u = 0; u < kMgsChunk; ++u) {
             const int e = c * kMgsChunk + u, lr = t + e * NT;
@@ -414,17 +435,13 @@ __global__ void __launch_bounds__(kMgsTmaThreads, 1) k_gm_mgs_tma(MgsArgs<T> a, 
   if (blockIdx.x == 0 && t == 0) epilogue(&S, 1, a.red);   // EPI_GM_NORM: h(j+1,j), Givens, stop test
   if (sbad && t == NT) {
     // After a failed wait the consumers may not have waited for every copy: wait (bounded)
-    // for the last copy into every chunk -- chunks [0, cnt) of a buffer last received
-    // v_k, the others v_{k-2}.
+    // for the last copy into each buffer (every copy is closed, so its phase completes
+    // once its bytes have landed; the copies before it into the same buffer had completed).
     for (int q = 0; q < 2; ++q) {
-      const int k = q ? last1 : last0, cnt = q ? cnt1 : cnt0;
-      for (int c = 0; c < nch; ++c) {
-        const int kc = c < cnt ? k : k - 2;
-        if (kc > 0) mbar_wait(&full[q][c], ((kc - 1) >> 1) & 1, kCopyLimit);
-      }
+      const int k = q ? last1 : last0;
+      if (k > 0) mbar_wait(&full[q], ((k - 1) >> 1) & 1, kCopyLimit);
     }
-  }
-}
+  }}
 
 template <class T>
 int mgs_elems_needed(int64_t np, int grid) {
@@ -478,7 +495,7 @@ int mgs_grid() {
 }
 
 // Rows per CTA of the staged variant (a multiple of 32), or 0 when two slices of that
-// length do not fit one CTA's shared memory or 32 elements per thread.
+// length do not fit one CTA's shared memory or 35 elements per consumer thread.
 template <class T>
 static int mgs_tma_rows(int64_t np) {
   static int cap = -1;
@@ -487,16 +504,16 @@ static int mgs_tma_rows(int64_t np) {
     PB_CUDA(cudaGetDevice(&dev));
     PB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     cudaFuncAttributes fa;
-    PB_CUDA(cudaFuncGetAttributes(&fa, k_gm_mgs_tma<T, 32>));
+    PB_CUDA(cudaFuncGetAttributes(&fa, k_gm_mgs_tma<T, 35>));   // the most static shared memory
     cap = std::max(0, optin - (int)fa.sharedSizeBytes);
     for (auto f : {k_gm_mgs_tma<T, 4>, k_gm_mgs_tma<T, 8>, k_gm_mgs_tma<T, 16>, k_gm_mgs_tma<T, 24>,
-                   k_gm_mgs_tma<T, 30>, k_gm_mgs_tma<T, 32>})
+                   k_gm_mgs_tma<T, 31>, k_gm_mgs_tma<T, 35>})
       PB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
   }
   const int G = num_sms();
   if (np <= 0 || G <= 0 || G > 32 * kMgsSlotsPerLane) return 0;
   const int64_t R = (((np + G - 1) / G) + 31) & ~int64_t(31);
-  if (R > 32 * kMgsConsumers || 2 * R * (int64_t)sizeof(T) > cap) return 0;
+  if (R > 35 * kMgsConsumers || 2 * R * (int64_t)sizeof(T) > cap) return 0;
   return (int)R;
 }
 
@@ -533,8 +550,8 @@ void mgs_column(const MgsArgs<T>& a, cudaStream_t st) {
     else if (R <= 8 * kMgsConsumers) launch_tma<T, 8>(a, R, st);
     else if (R <= 16 * kMgsConsumers) launch_tma<T, 16>(a, R, st);
     else if (R <= 24 * kMgsConsumers) launch_tma<T, 24>(a, R, st);
-    else if (R <= 30 * kMgsConsumers) launch_tma<T, 30>(a, R, st);
-    else launch_tma<T, 32>(a, R, st);
+    else if (R <= 31 * kMgsConsumers) launch_tma<T, 31>(a, R, st);
+    else launch_tma<T, 35>(a, R, st);
     return;
   }
   const int grid = mgs_grid<T>();
