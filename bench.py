@@ -80,6 +80,15 @@ class Clocks:
         except Exception:
             self.p = None
 
+    def started(self, timeout: float = 5.0):
+        """Waits for the first sample, so that nvidia-smi's own start-up (which competes
+        for the host cores the set-up uses) lies before the timed region."""
+        t0 = time.perf_counter()
+        while self.p is not None and time.perf_counter() - t0 < timeout:
+            if os.path.getsize(self.f.name) > 0:
+                return
+            time.sleep(0.02)
+
     def stop(self):
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -166,6 +175,7 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize()
     clk = Clocks(local)
+    clk.started()
     times, stats = [], []
     for _ in range(args.steps):
         x.zero_()
@@ -399,6 +409,7 @@ def run_vardiff(args):
     # warm-up (graph capture, allocations) on a small call of each path
     fgmres_all(None, 1)
     clk = Clocks(0)
+    clk.started()
     sp = plain_all(min(args.plain_rhs, nr))
     sm = fgmres_all(None, 1)
     sl = fgmres_all(net.handle, 1)

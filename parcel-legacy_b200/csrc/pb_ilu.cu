@@ -21,6 +21,7 @@
 // a shared-memory ring, so a level step costs shared-memory latency and one named
 // barrier.  The arithmetic of every row is the reference's: same operands, same order.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <numeric>
 
@@ -43,58 +44,85 @@ void divide_region(int r, int np, long idown, long iup, long* lo, long* hi) {
 
 }  // namespace
 
+void ilu_block_rows(int b, int nb, int n, int* lo, int* hi) {
+  long l, h;
+  divide_region(b, nb, 1, n, &l, &h);
+  *lo = (int)(l - 1);
+  *hi = (int)h;
+}
+
+__global__ void k_scatter_rowat(int n, const int* __restrict__ pos, int* __restrict__ rowAt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) rowAt[pos[i]] = i;
+}
+
+void scatter_positions(int n, const int* pos, int* rowAt, cudaStream_t st) {
+  if (n <= 0) return;
+  const int grid = (int)std::min<int64_t>(((int64_t)n + 255) / 256, 8LL * num_sms());
+  k_scatter_rowat<<<grid, 256, 0, st>>>(n, pos, rowAt);
+  PB_CUDA(cudaGetLastError());
+}
+
 // ------------------------------------------------------------------ host plan
-void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P) {
+// Levels: row x waits for every in-block row y < x coupled to it in either direction
+// (a lower entry of x, or an upper entry (y, x) of y), so one level order serves the
+// forward and the backward sweep.  The dependency window W is the largest level gap of
+// any coupling + 1; it is found in the same pass: lower couplings compare with rows whose
+// level is final, upper couplings (y, x) through the lowest level among x's upper-entry
+// sources, known once x is reached.
+void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P, int* pos_out, int* lev_out,
+                    const std::function<void(int)>& block_ready) {
   const int n = A.n;
   P.n = n;
   P.nb = nb;
-  P.lev.assign(n, 0);
-  P.pos.assign(n, 0);
+  P.lev = lev_out;
+  P.pos = pos_out;
   P.blk_lo.resize(nb);
   P.blk_hi.resize(nb);
-  for (int b = 0; b < nb; ++b) {
-    long lo, hi;
-    divide_region(b, nb, 1, n, &lo, &hi);
-    P.blk_lo[b] = (int)(lo - 1);
-    P.blk_hi[b] = (int)hi;
-  }
+  for (int b = 0; b < nb; ++b) ilu_block_rows(b, nb, n, &P.blk_lo[b], &P.blk_hi[b]);
   std::vector<int> nlev(nb, 0), gap(nb, 0), missing_diag(nb, 0);
   std::vector<int> cL(n, 0), cU(n, 0);
   const int* rp = A.rowptr;
   const int* ci = A.col;
   const int cb = A.istart;
+  int* lev = lev_out;
 #pragma omp parallel for schedule(dynamic, 1)
   for (int b = 0; b < nb; ++b) {
+    if (block_ready) block_ready(b);
     const int lo = P.blk_lo[b], hi = P.blk_hi[b];
-    std::vector<int> lb(hi - lo, 0);
+    std::vector<int> lb(hi - lo, 0), lsrc(hi - lo, INT_MAX);
     int maxlev = 0, g = 0;
     for (int i = lo; i < hi; ++i) {
       int L = lb[i - lo];
-      int nl = 0, nu = 0;
+      int nl = 0, nu = 0, lmin = INT_MAX;
       bool diag = false;
       for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
-        int c = ci[j] - cb;
+        const int c = ci[j] - cb;
         if (c < lo || c >= hi) continue;
-        if (c < i) { L = std::max(L, P.lev[c] + 1); ++nl; }
-        else if (c > i) ++nu;
-        else diag = true;
+        if (c < i) {
+          L = std::max(L, lev[c] + 1);
+          lmin = std::min(lmin, lev[c]);
+          ++nl;
+        } else if (c > i) {
+          ++nu;
+        } else {
+          diag = true;
+        }
       }
       if (!diag) missing_diag[b] = 1;
-      P.lev[i] = L;
+      lev[i] = L;
       cL[i] = nl; cU[i] = nu;
       maxlev = std::max(maxlev, L);
+      lmin = std::min(lmin, lsrc[i - lo]);
+      if (lmin != INT_MAX) g = std::max(g, L - lmin);
       // an upper entry (i, c) makes c wait for i in the backward sweep order as well
       for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
-        int c = ci[j] - cb;
-        if (c > i && c < hi) lb[c - lo] = std::max(lb[c - lo], L + 1);
+        const int c = ci[j] - cb;
+        if (c > i && c < hi) {
+          lb[c - lo] = std::max(lb[c - lo], L + 1);
+          lsrc[c - lo] = std::min(lsrc[c - lo], L);
+        }
       }
     }
-    for (int i = lo; i < hi; ++i)
-      for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
-        int c = ci[j] - cb;
-        if (c < lo || c >= hi || c == i) continue;
-        g = std::max(g, std::abs(P.lev[i] - P.lev[c]));
-      }
     nlev[b] = maxlev + 1;
     gap[b] = g;
   }
@@ -104,14 +132,19 @@ void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P) {
                      "block-Jacobi block %d has a row without an in-block diagonal entry", b);
       throw Error{PARCEL_B_E_ZERO_PIVOT, "missing diagonal"};
     }
-  // level widths and starts; permuted layout, block by block, level by level
+  // level widths and coupling counts; permuted layout, block by block, level by level
   P.blk_lvl.assign(nb + 1, 0);
   for (int b = 0; b < nb; ++b) P.blk_lvl[b + 1] = P.blk_lvl[b] + nlev[b];
   const int totlev = P.blk_lvl[nb];
-  std::vector<int> width(totlev, 0);
+  std::vector<int> width(totlev, 0), kl(totlev, 0), ku(totlev, 0);
 #pragma omp parallel for schedule(dynamic, 1)
   for (int b = 0; b < nb; ++b)   // blocks own disjoint level ranges
-    for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) width[P.blk_lvl[b] + P.lev[i]]++;
+    for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) {
+      const int gl = P.blk_lvl[b] + lev[i];
+      width[gl]++;
+      kl[gl] = std::max(kl[gl], cL[i]);
+      ku[gl] = std::max(ku[gl], cU[i]);
+    }
   P.lvl_start.assign(totlev, 0);
   int cursor = 0, maxw = 0;
   for (int b = 0; b < nb; ++b)
@@ -128,46 +161,35 @@ void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P) {
   P.W = *std::max_element(gap.begin(), gap.end()) + 1;
   // positions, stable by natural index within a level
   std::vector<int> fill(totlev, 0);
-  P.rowAt.assign(P.np, -1);
 #pragma omp parallel for schedule(dynamic, 1)
   for (int b = 0; b < nb; ++b)
     for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) {
-      int gl = P.blk_lvl[b] + P.lev[i];
-      int q = P.lvl_start[gl] + fill[gl]++;
-      P.pos[i] = q;
-      P.rowAt[q] = i;
+      const int gl = P.blk_lvl[b] + lev[i];
+      pos_out[i] = P.lvl_start[gl] + fill[gl]++;
     }
-  // chunks: per block in parallel, then concatenated in block order
-  std::vector<std::vector<IluChunk>> bch(nb);
-#pragma omp parallel for schedule(dynamic, 1)
+  // chunks (a level split at kIluChunk rows carries its level's coupling maxima), in
+  // block order
+  P.chunks.clear();
+  P.blk_chunk.assign(nb + 1, 0);
   for (int b = 0; b < nb; ++b) {
+    P.blk_chunk[b] = (int)P.chunks.size();
     for (int l = 0; l < nlev[b]; ++l) {
-      int gl = P.blk_lvl[b] + l;
+      const int gl = P.blk_lvl[b] + l;
       for (int o = 0; o < width[gl]; o += kIluChunk) {
         IluChunk c;
         c.start = P.lvl_start[gl] + o;
         c.w = std::min(kIluChunk, width[gl] - o);
         c.wpad = align4(c.w);
-        c.KL = 0; c.KU = 0;
-        for (int p = 0; p < c.w; ++p) {
-          int i = P.rowAt[c.start + p];
-          c.KL = std::max(c.KL, cL[i]);
-          c.KU = std::max(c.KU, cU[i]);
-        }
+        c.KL = kl[gl];
+        c.KU = ku[gl];
         c.lvl = l;
         c.off_in_level = o;
         c.blk = b;
         c.offF = 0;
         c.offB = 0;
-        bch[b].push_back(c);
+        P.chunks.push_back(c);
       }
     }
-  }
-  P.chunks.clear();
-  P.blk_chunk.assign(nb + 1, 0);
-  for (int b = 0; b < nb; ++b) {
-    P.blk_chunk[b] = (int)P.chunks.size();
-    P.chunks.insert(P.chunks.end(), bch[b].begin(), bch[b].end());
   }
   P.blk_chunk[nb] = (int)P.chunks.size();
 }

@@ -1,6 +1,8 @@
 // pb_ilu.cuh -- block-Jacobi ILU(0) / D-ILU preconditioner on the level-major layout.
 #pragma once
 
+#include <functional>
+
 #include "pb_common.cuh"
 
 namespace pb {
@@ -31,13 +33,12 @@ struct SellBuf {
 };
 
 // Builds the sliced-ELLPACK copy of the natural CRS matrix A in the row order
-// rowAt (permuted position -> natural row, -1 = empty row; null = identity) with columns
-// mapped through pos (natural -> permuted; null = identity).  row_len holds the host-side
-// length of every natural row.  Fills M's SELL fields.
+// rowAt (device: permuted position -> natural row, -1 = empty row; null = identity) with
+// columns mapped through pos (device: natural -> permuted; null = identity).  Slice widths
+// and offsets are computed on the device.  Fills M's SELL fields.
 template <class VT>
-void build_sell(const DevMat<double>& A, int np, const std::vector<int>& rowAt_h,
-                const int* rowAt_d, const int* pos_d, const std::vector<int>& row_len,
-                SellBuf<VT>& buf, DevMat<VT>& M);
+void build_sell(const DevMat<double>& A, int np, const int* rowAt_d, const int* pos_d, SellBuf<VT>& buf,
+                DevMat<VT>& M);
 
 // One chunk = up to kIluChunk rows of one wavefront level of one block.
 struct IluChunk {
@@ -61,9 +62,8 @@ struct IluPlan {
   int W = 1;            // ring depth in levels
   int maxWp = 0;        // widest chunk (padded)
   int max_levels = 0;
-  std::vector<int> pos;         // natural row -> permuted position
-  std::vector<int> lev;         // natural row -> level within its block
-  std::vector<int> rowAt;       // permuted position -> natural row, -1 = padding
+  int* pos = nullptr;           // natural row -> permuted position (caller's storage, n)
+  int* lev = nullptr;           // natural row -> level within its block (caller's storage, n)
   std::vector<IluChunk> chunks;
   std::vector<int> blk_chunk;   // nb + 1
   std::vector<int> blk_lo, blk_hi;   // natural row ranges [lo, hi)
@@ -99,7 +99,16 @@ struct HostCSR {
   const int* col = nullptr;      // 1-based global
 };
 
-void ilu_build_plan(const HostCSR& A, int nblocks, IluPlan& P);
+// Natural rows [lo, hi) of block-Jacobi block b of nb (0-based).
+void ilu_block_rows(int b, int nb, int n, int* lo, int* hi);
+// rowAt[pos[i]] = i for i < n (entries not hit keep their value).
+void scatter_positions(int n, const int* pos, int* rowAt, cudaStream_t st);
+
+// Wavefront plan of the block-Jacobi blocks.  pos_out and lev_out (n entries each) receive
+// the permutation and the levels.  block_ready(b), when given, is called before block b's
+// rows are read (the structure may still be arriving from the device).
+void ilu_build_plan(const HostCSR& A, int nblocks, IluPlan& P, int* pos_out, int* lev_out,
+                    const std::function<void(int)>& block_ready = {});
 
 // Factorises (ILU(0)) or computes the D-ILU diagonal on the device and packs the sweep
 // data.  ilu_method: 0 ILU(0), 1 ILUD, 2 MLUD (define.f90:40-42).  Returns a status.

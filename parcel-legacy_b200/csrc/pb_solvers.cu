@@ -17,6 +17,9 @@
 #include <type_traits>
 
 #include "pb_mgs.cuh"
+
+#include <atomic>
+#include <functional>
 #include "pb_solvers.cuh"
 
 namespace pb {
@@ -130,21 +133,65 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
   S.M.kind = o.precon;
 
   if (o.precon == PARCEL_B_PRECON_BLOCKJACOBI) {
-    // The wavefront analysis needs the sparsity structure on the host.
+    // The wavefront analysis runs on the host.  A device-resident structure comes back
+    // through page-locked staging: the row pointers first, then the column indices in
+    // block-aligned pieces, each with an event, so that the plan of the first blocks
+    // overlaps the copy of the others.  The plan writes the permutation and the levels
+    // into the same staging area, from where they go back to the device.
+    const int nb = std::max(1, std::min(o.nblocks, A.n));
+    const size_t n1 = (size_t)A.n + 1, nz = (size_t)A.nnz;
+    int* pin = static_cast<int*>(pinned_staging(sizeof(int) * ((dev ? n1 + nz : 0) + 2 * (size_t)A.n)));
+    int* hpos = pin + (dev ? n1 + nz : 0);
+    int* hlev = hpos + A.n;
     const int* hrpp = A.rowptr;
     const int* hcip = A.col;
-    if (dev) {   // through page-locked staging: twice the bandwidth of pageable copies
-      int* pin = static_cast<int*>(pinned_staging(sizeof(int) * ((size_t)A.n + 1 + (size_t)A.nnz)));
-      d2h(pin, A.rowptr, sizeof(int) * (A.n + 1));
-      d2h(pin + A.n + 1, A.col, sizeof(int) * A.nnz);
+    constexpr int kPieces = 4;
+    cudaEvent_t ev[kPieces] = {};
+    std::vector<int> piece_of(nb, 0);
+    std::atomic<int> copy_failed{0};
+    std::function<void(int)> ready;
+    auto destroy_events = [&] {
+      for (auto& e : ev)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+    };
+    if (dev) {
+      d2h(pin, A.rowptr, sizeof(int) * n1);   // synchronous: the row pointers size the pieces
       hrpp = pin;
-      hcip = pin + A.n + 1;
+      hcip = pin + n1;
+      for (int k = 0; k < kPieces; ++k) {
+        const int b0 = (int)((int64_t)nb * k / kPieces), b1 = (int)((int64_t)nb * (k + 1) / kPieces);
+        for (int b = b0; b < b1; ++b) piece_of[b] = k;
+        cudaError_t e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+        if (e == cudaSuccess && b1 > b0) {
+          int lo0, hi0, lo1, hi1;
+          ilu_block_rows(b0, nb, A.n, &lo0, &hi0);
+          ilu_block_rows(b1 - 1, nb, A.n, &lo1, &hi1);
+          const size_t j0 = (size_t)(hrpp[lo0] - 1), j1 = (size_t)(hrpp[hi1] - 1);   // 1-based
+          if (j1 > j0) e = cudaMemcpyAsync(pin + n1 + j0, A.col + j0, sizeof(int) * (j1 - j0), cudaMemcpyDeviceToHost, st);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(ev[k], st);
+        if (e != cudaSuccess) {
+          destroy_events();
+          PB_CUDA(e);
+        }
+      }
+      // called from the plan's parallel loop: no exception may leave it
+      ready = [&](int b) {
+        if (cudaEventSynchronize(ev[piece_of[b]]) != cudaSuccess) copy_failed = 1;
+      };
     }
-    trace_mark("setup: structure to host");
     HostCSR H;
     H.n = A.n; H.nnz = A.nnz; H.istart = A.istart; H.rowptr = hrpp; H.col = hcip;
     IluPlan P;
-    ilu_build_plan(H, std::max(1, std::min(o.nblocks, A.n)), P);
+    trace_mark("setup: row pointers to host");
+    try {
+      ilu_build_plan(H, nb, P, hpos, hlev, ready);
+    } catch (...) {
+      destroy_events();
+      throw;
+    }
+    destroy_events();
+    PB_CHECK(!copy_failed, PARCEL_B_E_CUDA, "copy of the sparsity structure to the host failed");
     trace_mark("setup: wavefront plan (host)");
     S.np = P.np;
     S.permuted = true;
@@ -153,17 +200,14 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
     S.pos.alloc(sizeof(int) * A.n);
     S.lev.alloc(sizeof(int) * A.n);
     S.rowAt.alloc(sizeof(int) * P.np);
-    h2d(S.pos.p, P.pos.data(), sizeof(int) * A.n);
-    h2d(S.lev.p, P.lev.data(), sizeof(int) * A.n);
-    h2d(S.rowAt.p, P.rowAt.data(), sizeof(int) * P.np);
+    h2d(S.pos.p, hpos, sizeof(int) * A.n);
+    h2d(S.lev.p, hlev, sizeof(int) * A.n);
+    PB_CUDA(cudaMemsetAsync(S.rowAt.p, 0xFF, sizeof(int) * P.np, st));   // padding: -1
+    scatter_positions(A.n, dp<int>(S.pos), dp<int>(S.rowAt), st);
     trace_mark("setup: layout maps to device");
-    {
-      std::vector<int> len(A.n);
-      for (int i = 0; i < A.n; ++i) len[i] = hrpp[i + 1] - hrpp[i];
-      S.A = DevMat<T>{};
-      S.A.nnz = A.nnz;
-      build_sell<T>(S.Anat, P.np, P.rowAt, dp<int>(S.rowAt), dp<int>(S.pos), len, S.Asell, S.A);
-    }
+    S.A = DevMat<T>{};
+    S.A.nnz = A.nnz;
+    build_sell<T>(S.Anat, P.np, dp<int>(S.rowAt), dp<int>(S.pos), S.Asell, S.A);
     trace_mark("setup: sliced ELLPACK");
     ilu_setup_device<T>(P, S.Anat, o.ilu_method, dp<int>(S.pos), dp<int>(S.rowAt),
                         dp<int>(S.lev), S.M.ilu);
@@ -180,12 +224,8 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
       S.A.val = dp<T>(S.Aval_T); S.A.rbase = 1; S.A.cbase = A.istart;
     }
     {
-      std::vector<int> hrp(A.n + 1), len(A.n);
-      if (dev) d2h(hrp.data(), A.rowptr, sizeof(int) * (A.n + 1));
-      else memcpy(hrp.data(), A.rowptr, sizeof(int) * (A.n + 1));
-      for (int i = 0; i < A.n; ++i) len[i] = hrp[i + 1] - hrp[i];
       DevMat<T> M = S.A;
-      build_sell<T>(S.Anat, A.n, std::vector<int>(), nullptr, nullptr, len, S.Asell, M);
+      build_sell<T>(S.Anat, A.n, nullptr, nullptr, S.Asell, M);
       S.A = M;
     }
     if (o.precon == PARCEL_B_PRECON_POINTJACOBI) {

@@ -237,33 +237,74 @@ __global__ void k_fill_sell(int np, const int* __restrict__ rowAt, const int* __
   }
 }
 
-template <class VT>
-void build_sell(const DevMat<double>& A, int np, const std::vector<int>& rowAt_h, const int* rowAt_d,
-                const int* pos_d, const std::vector<int>& row_len, SellBuf<VT>& buf, DevMat<VT>& M) {
-  const int ns = (np + 31) / 32;
-  std::vector<int> off(ns + 1, 0), w(ns, 0);
-  for (int s = 0; s < ns; ++s) {
-    int mx = 0;
-    for (int l = 0; l < 32; ++l) {
-      const int q = s * 32 + l;
-      if (q >= np) break;
-      const int i = rowAt_h.empty() ? q : rowAt_h[q];
-      if (i >= 0) mx = std::max(mx, row_len[i]);
+// Slice widths: the longest of the 32 rows of each slice (warp per slice).
+__global__ void k_sell_width(int np, const int* __restrict__ rowAt, const int* __restrict__ rp,
+                             int* __restrict__ sw) {
+  const int ns = (np + 31) >> 5;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < (ns << 5); q += gridDim.x * blockDim.x) {
+    int len = 0;
+    if (q < np) {
+      const int i = rowAt ? rowAt[q] : q;
+      if (i >= 0) len = rp[i + 1] - rp[i];
     }
-    w[s] = mx;
-    PB_CHECK((int64_t)off[s] + 32LL * mx < INT32_MAX, PARCEL_B_E_UNSUPPORTED, "matrix too large for int32 SELL");
-    off[s + 1] = off[s] + 32 * mx;
+    len = __reduce_max_sync(kFull, len);
+    if ((q & 31) == 0) sw[q >> 5] = len;
   }
-  const int64_t total = std::max(off[ns], 1);
+}
+
+// Slice offsets off[s] = 32 * (w[0] + ... + w[s-1]) for s = 0..ns, one block; the 64-bit
+// total goes to *total so that the host can check it against the int32 range.
+constexpr int kSellScanThreads = 1024;
+__global__ void __launch_bounds__(kSellScanThreads) k_sell_offsets(int ns, const int* __restrict__ sw,
+                                                                   int* __restrict__ off,
+                                                                   long long* __restrict__ total) {
+  __shared__ long long part[kSellScanThreads];
+  const int t = threadIdx.x;
+  const int per = (ns + kSellScanThreads - 1) / kSellScanThreads;
+  const int a = min(ns, t * per), z = min(ns, a + per);
+  long long loc = 0;
+  for (int s = a; s < z; ++s) loc += 32LL * sw[s];
+  part[t] = loc;
+  __syncthreads();
+  for (int d = 1; d < kSellScanThreads; d <<= 1) {   // inclusive scan of the per-thread sums
+    const long long v = t >= d ? part[t - d] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  long long run = part[t] - loc;
+  for (int s = a; s < z; ++s) {
+    off[s] = (int)min(run, (long long)INT32_MAX);
+    run += 32LL * sw[s];
+  }
+  if (t == kSellScanThreads - 1) {
+    off[ns] = (int)min(part[t], (long long)INT32_MAX);
+    *total = part[t];
+  }
+}
+
+template <class VT>
+void build_sell(const DevMat<double>& A, int np, const int* rowAt_d, const int* pos_d, SellBuf<VT>& buf,
+                DevMat<VT>& M) {
+  cudaStream_t st = stream();
+  const int ns = (np + 31) / 32;
   buf.off.alloc(sizeof(int) * (ns + 1));
   buf.w.alloc(sizeof(int) * std::max(ns, 1));
+  DBuf tot(sizeof(long long));
+  const int grid = (int)std::min<int64_t>(((int64_t)ns * 32 + 255) / 256, 8LL * num_sms());
+  k_sell_width<<<std::max(grid, 1), 256, 0, st>>>(np, rowAt_d, A.rowptr, dp<int>(buf.w));
+  PB_CUDA(cudaGetLastError());
+  k_sell_offsets<<<1, kSellScanThreads, 0, st>>>(ns, dp<int>(buf.w), dp<int>(buf.off), dp<long long>(tot));
+  PB_CUDA(cudaGetLastError());
+  long long total = 0;
+  d2h(&total, tot.p, sizeof(long long));
+  PB_CHECK(total < INT32_MAX, PARCEL_B_E_UNSUPPORTED, "matrix too large for int32 SELL");
+  total = std::max(total, 1LL);
   buf.col.alloc(sizeof(int) * total);
   buf.val.alloc(sizeof(VT) * total);
-  h2d(buf.off.p, off.data(), sizeof(int) * (ns + 1));
-  h2d(buf.w.p, w.data(), sizeof(int) * ns);
-  k_fill_sell<VT><<<8 * num_sms(), 256, 0, stream()>>>(np, rowAt_d, pos_d, A.rowptr, A.col, A.val, A.rbase,
-                                                       A.cbase, dp<int>(buf.off), dp<int>(buf.w),
-                                                       dp<int>(buf.col), dp<VT>(buf.val));
+  k_fill_sell<VT><<<8 * num_sms(), 256, 0, st>>>(np, rowAt_d, pos_d, A.rowptr, A.col, A.val, A.rbase,
+                                                 A.cbase, dp<int>(buf.off), dp<int>(buf.w),
+                                                 dp<int>(buf.col), dp<VT>(buf.val));
   PB_CUDA(cudaGetLastError());
   M.nslices = ns;
   M.s_off = dp<int>(buf.off);
@@ -273,10 +314,10 @@ void build_sell(const DevMat<double>& A, int np, const std::vector<int>& rowAt_h
   M.n = np;
 }
 
-template void build_sell<double>(const DevMat<double>&, int, const std::vector<int>&, const int*, const int*,
-                                 const std::vector<int>&, SellBuf<double>&, DevMat<double>&);
-template void build_sell<float>(const DevMat<double>&, int, const std::vector<int>&, const int*, const int*,
-                                const std::vector<int>&, SellBuf<float>&, DevMat<float>&);
+template void build_sell<double>(const DevMat<double>&, int, const int*, const int*, SellBuf<double>&,
+                                 DevMat<double>&);
+template void build_sell<float>(const DevMat<double>&, int, const int*, const int*, SellBuf<float>&,
+                                DevMat<float>&);
 
 template void spmv<double, double>(const DevMat<double>&, const double*, double*, int,
                                    const double*, const int*, cudaStream_t);
