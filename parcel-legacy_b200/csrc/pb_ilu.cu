@@ -214,6 +214,35 @@ __device__ __forceinline__ void inblock_range(const int* rp, const int* ci, int 
 // ILU(0) IKJ factorisation of every block, level by level; one CTA per block.
 // ILU_LU_crs (matrix.f90:7970-8072).  Explicit roundings keep the reference's
 // two-rounding a - b*c.
+//
+// A row of at most kFacCap entries is staged in registers: its columns and values in one
+// batch of loads, then for each lower in-block entry (increasing column) the pivot row in
+// one batch; the eliminations run on the registers in the reference's order and the row
+// is written back once.  Longer rows (or pivot rows) take the entry-by-entry path.
+constexpr int kFacCap = 8;
+
+__device__ __forceinline__ void ilu0_row_generic(const int* rp, const int* ci, int rbase, int cbase, int i, int lo, int hi,
+                                 double* lu) {
+  int ia, iz, idg;
+  inblock_range(rp, ci, rbase, cbase, i, lo, hi, &ia, &iz, &idg);
+  for (int kc = ia; kc < iz; ++kc) {
+    int k = ci[kc] - cbase;
+    if (k > i - 1) break;
+    int ka, kz, kk;
+    inblock_range(rp, ci, rbase, cbase, k, lo, hi, &ka, &kz, &kk);
+    double lik = __ddiv_rn(lu[kc], lu[kk]);
+    lu[kc] = lik;
+    for (int jc = kc + 1; jc < iz; ++jc) {
+      int j = ci[jc] - cbase;
+      for (int kj = kk; kj < kz; ++kj) {
+        int cj = ci[kj] - cbase;
+        if (cj == j) { lu[jc] = __dsub_rn(lu[jc], __dmul_rn(lik, lu[kj])); break; }
+        if (cj > j) break;
+      }
+    }
+  }
+}
+
 __global__ void k_ilu0_factor(const IluChunk* __restrict__ ch, const int* __restrict__ blk_chunk,
                               const int* __restrict__ blk_lo, const int* __restrict__ blk_hi,
                               const int* __restrict__ rowAt, const int* __restrict__ rp,
@@ -223,31 +252,70 @@ __global__ void k_ilu0_factor(const IluChunk* __restrict__ ch, const int* __rest
   for (int c = blk_chunk[b]; c < blk_chunk[b + 1]; ++c) {
     const IluChunk C = ch[c];
     for (int p = threadIdx.x; p < C.w; p += blockDim.x) {
-      int i = rowAt[C.start + p];
-      int ia, iz, idg;
-      inblock_range(rp, ci, rbase, cbase, i, lo, hi, &ia, &iz, &idg);
-      for (int kc = ia; kc < iz; ++kc) {
-        int k = ci[kc] - cbase;
-        if (k > i - 1) break;
-        int ka, kz, kk;
-        inblock_range(rp, ci, rbase, cbase, k, lo, hi, &ka, &kz, &kk);
-        double lik = __ddiv_rn(lu[kc], lu[kk]);
-        lu[kc] = lik;
-        for (int jc = kc + 1; jc < iz; ++jc) {
-          int j = ci[jc] - cbase;
-          for (int kj = kk; kj < kz; ++kj) {
-            int cj = ci[kj] - cbase;
-            if (cj == j) { lu[jc] = __dsub_rn(lu[jc], __dmul_rn(lik, lu[kj])); break; }
-            if (cj > j) break;
-          }
+      const int i = rowAt[C.start + p];
+      const int a = rp[i] - rbase, z = rp[i + 1] - rbase;
+      if (z - a > kFacCap) {
+        ilu0_row_generic(rp, ci, rbase, cbase, i, lo, hi, lu);
+        continue;
+      }
+      int col[kFacCap];
+      double val[kFacCap];
+#pragma unroll
+      for (int e = 0; e < kFacCap; ++e) {
+        col[e] = e < z - a ? ci[a + e] - cbase : INT_MAX;
+        val[e] = e < z - a ? lu[a + e] : 0.0;
+      }
+      // pivot rows must fit as well; otherwise the whole row goes the generic way
+      bool fits = true;
+#pragma unroll
+      for (int e = 0; e < kFacCap; ++e) {
+        const int k = col[e];
+        if (k >= lo && k < i && rp[k + 1] - rp[k] > kFacCap) fits = false;
+      }
+      if (!fits) {
+        ilu0_row_generic(rp, ci, rbase, cbase, i, lo, hi, lu);
+        continue;
+      }
+      // e walks the row; the register arrays are only ever indexed by unrolled loops
+      for (int e = 0; e < z - a; ++e) {
+        int k = INT_MAX;
+        double ve = 0.0;
+#pragma unroll
+        for (int q = 0; q < kFacCap; ++q)
+          if (q == e) { k = col[q]; ve = val[q]; }
+        if (k < lo || k >= i) continue;   // lower in-block entries only, increasing column
+        const int ka = rp[k] - rbase, kz = rp[k + 1] - rbase;
+        int kcol[kFacCap];
+        double kval[kFacCap];
+#pragma unroll
+        for (int f = 0; f < kFacCap; ++f) {
+          kcol[f] = f < kz - ka ? ci[ka + f] - cbase : INT_MAX;
+          kval[f] = f < kz - ka ? lu[ka + f] : 0.0;
+        }
+        double ukk = 0.0;
+#pragma unroll
+        for (int f = 0; f < kFacCap; ++f)
+          if (kcol[f] == k) ukk = kval[f];
+        const double lik = __ddiv_rn(ve, ukk);
+        // l_ik replaces a_ik; the in-block entries after it lose l_ik u_kj where row k
+        // has column j (> k)
+#pragma unroll
+        for (int g = 0; g < kFacCap; ++g) {
+          if (g == e) val[g] = lik;
+          const int j = col[g];
+#pragma unroll
+          for (int f = 0; f < kFacCap; ++f)
+            if (g > e && kcol[f] == j && j > k && j < hi) val[g] = __dsub_rn(val[g], __dmul_rn(lik, kval[f]));
         }
       }
+#pragma unroll
+      for (int e = 0; e < kFacCap; ++e)
+        if (e < z - a) lu[a + e] = val[e];
     }
     __syncthreads();
   }
 }
 
-// D-ILU diagonal, level by level; DILU_DInv_crs (matrix.f90:3482-3648).
 __global__ void k_dilu_diag(const IluChunk* __restrict__ ch, const int* __restrict__ blk_chunk,
                             const int* __restrict__ blk_lo, const int* __restrict__ blk_hi,
                             const int* __restrict__ rowAt, const int* __restrict__ rp,
