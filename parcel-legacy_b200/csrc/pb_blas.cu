@@ -222,12 +222,35 @@ __global__ void k_sum_vec(int64_t n, T* __restrict__ v0, const T* __restrict__ V
 }
 
 // y = H^-1 e by back substitution over the mm used columns (update_xVec,
-// pcagmres.f90:1136-1236), one thread.
+// pcagmres.f90:1136-1236).  The warp stages the used part of H and e in shared memory
+// (coalesced); one thread then substitutes in the reference's order.  Restarts up to
+// kBackSmemM use the staged copy, longer ones read H from global memory.
+constexpr int kBackSmemM = 64;
 __global__ void k_gm_backsolve(const double* h, const double* e, double* y, int m0, KState* st,
                                const int* gate) {
   if (gated(gate)) return;
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  __shared__ double sh[kBackSmemM * kBackSmemM], se[kBackSmemM], sy[kBackSmemM];
   const int m = st->mm;
+  const bool staged = m <= kBackSmemM;
+  if (staged) {
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+      const int r = t % m, c = t / m;   // H(r, c), column-major
+      sh[r + c * kBackSmemM] = h[(size_t)r + (size_t)c * (m0 + 1)];
+    }
+    for (int t = threadIdx.x; t < m; t += blockDim.x) se[t] = e[t];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  if (staged) {
+    for (int i = m; i >= 1; --i) {
+      double v = se[i - 1];
+      for (int j = m; j >= i + 1; --j) v = v - sh[(i - 1) + (j - 1) * kBackSmemM] * sy[j - 1];
+      const double d = sh[(i - 1) + (i - 1) * kBackSmemM];
+      sy[i - 1] = (d == 0.0) ? v / 1.0e-300 : v / d;
+    }
+    for (int i = 0; i < m; ++i) y[i] = sy[i];
+    return;
+  }
   for (int i = m; i >= 1; --i) {
     double v = e[i - 1];
     for (int j = m; j >= i + 1; --j) v = v - h[(size_t)(i - 1) + (size_t)(j - 1) * (m0 + 1)] * y[j - 1];
@@ -340,7 +363,7 @@ void sum_vec(int64_t n, T* v0, const T* V, int64_t ldv, const double* y, const K
 
 void gm_backsolve(const double* h, const double* e, double* y, int m0, KState* st, const int* gate,
                   cudaStream_t s_) {
-  k_gm_backsolve<<<1, 32, 0, s_>>>(h, e, y, m0, st, gate);
+  k_gm_backsolve<<<1, 256, 0, s_>>>(h, e, y, m0, st, gate);
   PB_CUDA(cudaGetLastError());
 }
 

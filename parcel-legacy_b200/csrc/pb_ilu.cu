@@ -21,6 +21,7 @@
 // a shared-memory ring, so a level step costs shared-memory latency and one named
 // barrier.  The arithmetic of every row is the reference's: same operands, same order.
 #include <algorithm>
+#include <omp.h>
 #include <climits>
 #include <cmath>
 #include <numeric>
@@ -85,43 +86,52 @@ void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P, int* pos_out, int* lev
   const int* ci = A.col;
   const int cb = A.istart;
   int* lev = lev_out;
-#pragma omp parallel for schedule(dynamic, 1)
+  // one core is left to the caller's other threads: a plan thread that the scheduler
+  // pre-empts for a time slice would hold up the whole loop
+  const int nthr = std::max(1, omp_get_num_procs() - 1);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthr)
   for (int b = 0; b < nb; ++b) {
     if (block_ready) block_ready(b);
     const int lo = P.blk_lo[b], hi = P.blk_hi[b];
     std::vector<int> lb(hi - lo, 0), lsrc(hi - lo, INT_MAX);
     int maxlev = 0, g = 0;
     for (int i = lo; i < hi; ++i) {
+      // columns are sorted: the lower entries come first, so the row's level is final at
+      // its first upper entry and one walk over the row suffices
       int L = lb[i - lo];
-      int nl = 0, nu = 0, lmin = INT_MAX;
-      bool diag = false;
+      int nl = 0, nu = 0, lmin = lsrc[i - lo];
+      bool diag = false, fixed = false, unsorted = false;
       for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
         const int c = ci[j] - cb;
         if (c < lo || c >= hi) continue;
         if (c < i) {
+          unsorted |= fixed;
           L = std::max(L, lev[c] + 1);
           lmin = std::min(lmin, lev[c]);
           ++nl;
-        } else if (c > i) {
-          ++nu;
-        } else {
+        } else if (c == i) {
           diag = true;
+        } else {
+          fixed = true;
+          // an upper entry (i, c) makes c wait for i in the backward sweep order as well
+          lb[c - lo] = std::max(lb[c - lo], L + 1);
+          lsrc[c - lo] = std::min(lsrc[c - lo], L);
+          ++nu;
         }
       }
+      if (unsorted)   // a lower entry after an upper one: redo the upper entries with the final level
+        for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
+          const int c = ci[j] - cb;
+          if (c > i && c < hi) {
+            lb[c - lo] = std::max(lb[c - lo], L + 1);
+            lsrc[c - lo] = std::min(lsrc[c - lo], L);   // an earlier, smaller L only widens W
+          }
+        }
       if (!diag) missing_diag[b] = 1;
       lev[i] = L;
       cL[i] = nl; cU[i] = nu;
       maxlev = std::max(maxlev, L);
-      lmin = std::min(lmin, lsrc[i - lo]);
       if (lmin != INT_MAX) g = std::max(g, L - lmin);
-      // an upper entry (i, c) makes c wait for i in the backward sweep order as well
-      for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
-        const int c = ci[j] - cb;
-        if (c > i && c < hi) {
-          lb[c - lo] = std::max(lb[c - lo], L + 1);
-          lsrc[c - lo] = std::min(lsrc[c - lo], L);
-        }
-      }
     }
     nlev[b] = maxlev + 1;
     gap[b] = g;
@@ -137,7 +147,7 @@ void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P, int* pos_out, int* lev
   for (int b = 0; b < nb; ++b) P.blk_lvl[b + 1] = P.blk_lvl[b] + nlev[b];
   const int totlev = P.blk_lvl[nb];
   std::vector<int> width(totlev, 0), kl(totlev, 0), ku(totlev, 0);
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthr)
   for (int b = 0; b < nb; ++b)   // blocks own disjoint level ranges
     for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) {
       const int gl = P.blk_lvl[b] + lev[i];
@@ -161,7 +171,7 @@ void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P, int* pos_out, int* lev
   P.W = *std::max_element(gap.begin(), gap.end()) + 1;
   // positions, stable by natural index within a level
   std::vector<int> fill(totlev, 0);
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthr)
   for (int b = 0; b < nb; ++b)
     for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) {
       const int gl = P.blk_lvl[b] + lev[i];
@@ -265,12 +275,20 @@ __global__ void k_ilu0_factor(const IluChunk* __restrict__ ch, const int* __rest
         col[e] = e < z - a ? ci[a + e] - cbase : INT_MAX;
         val[e] = e < z - a ? lu[a + e] : 0.0;
       }
-      // pivot rows must fit as well; otherwise the whole row goes the generic way
+      // pivot rows must fit as well; otherwise the whole row goes the generic way.  Their
+      // bounds are kept for the eliminations.
       bool fits = true;
+      int pa[kFacCap], pz[kFacCap];
 #pragma unroll
       for (int e = 0; e < kFacCap; ++e) {
         const int k = col[e];
-        if (k >= lo && k < i && rp[k + 1] - rp[k] > kFacCap) fits = false;
+        pa[e] = 0;
+        pz[e] = 0;
+        if (k >= lo && k < i) {
+          pa[e] = rp[k] - rbase;
+          pz[e] = rp[k + 1] - rbase;
+          if (pz[e] - pa[e] > kFacCap) fits = false;
+        }
       }
       if (!fits) {
         ilu0_row_generic(rp, ci, rbase, cbase, i, lo, hi, lu);
@@ -278,13 +296,12 @@ __global__ void k_ilu0_factor(const IluChunk* __restrict__ ch, const int* __rest
       }
       // e walks the row; the register arrays are only ever indexed by unrolled loops
       for (int e = 0; e < z - a; ++e) {
-        int k = INT_MAX;
+        int k = INT_MAX, ka = 0, kz = 0;
         double ve = 0.0;
 #pragma unroll
         for (int q = 0; q < kFacCap; ++q)
-          if (q == e) { k = col[q]; ve = val[q]; }
+          if (q == e) { k = col[q]; ve = val[q]; ka = pa[q]; kz = pz[q]; }
         if (k < lo || k >= i) continue;   // lower in-block entries only, increasing column
-        const int ka = rp[k] - rbase, kz = rp[k + 1] - rbase;
         int kcol[kFacCap];
         double kval[kFacCap];
 #pragma unroll
