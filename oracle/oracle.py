@@ -62,6 +62,10 @@ def lib():
         L.orc_precon_apply_h.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_precon_destroy.argtypes = [C.c_void_p]
         L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_ddcg.argtypes = [C.POINTER(OrcMat), C.c_void_p, C.POINTER(OrcParams), C.c_int, C.c_int,
+                               C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.orc_ddcg.restype = C.c_int
         _lib = L
     return _lib
 
@@ -101,6 +105,25 @@ def solve(A, b, x0=None, **kw):
     if rc != 0:
         return x, hist[:0], 0, rc
     return x, hist[:niter.value].copy(), niter.value, iret.value
+
+
+def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, a_lo=None, prec_A=2, prec_b=2, prec_x=2, prec_M=2,
+         **kw):
+    """Double-double PCG (ddKSP_pCG); returns (x_hi, x_lo, reshistory[:niter], niter, iret)."""
+    M = A if isinstance(A, Matrix) else Matrix(A)
+    p = params(solver=1, **kw)
+    f = lambda v: None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+    bh, bl, alo = f(b_hi), f(b_lo), f(a_lo)
+    xh = np.zeros(M.n) if x0_hi is None else np.array(x0_hi, dtype=np.float64, copy=True)
+    xl = np.zeros(M.n) if x0_lo is None else np.array(x0_lo, dtype=np.float64, copy=True)
+    hist = np.zeros(max(p.itrmax, 1) + 1)
+    niter, iret = C.c_int(0), C.c_int(0)
+    ptr = lambda v: None if v is None else _ptr(v)
+    rc = lib().orc_ddcg(C.byref(M.s), ptr(alo), C.byref(p), prec_A, prec_b, prec_x, prec_M, _ptr(bh), ptr(bl),
+                        _ptr(xh), _ptr(xl), _ptr(hist), C.byref(niter), C.byref(iret))
+    if rc != 0:
+        return xh, xl, hist[:0], 0, rc
+    return xh, xl, hist[:niter.value].copy(), niter.value, iret.value
 
 
 def spmv(A, x):

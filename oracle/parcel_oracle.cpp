@@ -584,6 +584,305 @@ void pgmres(const OrcMat& A, const Precon& P, const OrcParams& prm, const double
 }  // namespace
 
 // ---------------------------------------------------------------------------------
+// Double-double CG (ddKSP_pCG, ddpcg.f90:247-563) and its building blocks.
+//
+// dd arithmetic (dd_func.f90:5-239): "sloppy" add/sub (two-sum of the high parts, low
+// parts added, renormalised), Dekker product with the split constant 134217729 = 2^27+1,
+// division by one Newton correction, square root from 1/sqrt(hi).  Built with
+// -ffp-contract=off, so every operation rounds once, as the reference's Fortran does.
+struct DD { double hi, lo; };
+
+DD dd_add(DD a, DD b) {
+  double p1 = a.hi + b.hi;
+  double p2 = p1 - a.hi;
+  double t1l = (a.hi - (p1 - p2)) + (b.hi - p2);
+  double t1h = p1;
+  t1l = t1l + a.lo + b.lo;
+  double s1 = t1h + t1l;
+  t1l = t1l - (s1 - t1h);
+  return DD{s1, t1l};
+}
+DD dd_sub(DD a, DD b) {
+  double p1 = a.hi - b.hi;
+  double p2 = p1 - a.hi;
+  double t1l = (a.hi - (p1 - p2)) - (b.hi + p2);
+  double t1h = p1;
+  t1l = t1l + a.lo - b.lo;
+  double s1 = t1h + t1l;
+  t1l = t1l - (s1 - t1h);
+  return DD{s1, t1l};
+}
+DD dd_mul(DD a, DD b) {
+  double t1h = a.hi * b.hi;
+  double u1 = 134217729.0 * a.hi;
+  double p1 = u1 - (u1 - a.hi);
+  double p2 = a.hi - p1;
+  u1 = 134217729.0 * b.hi;
+  double r1 = u1 - (u1 - b.hi);
+  double r2 = b.hi - r1;
+  double t1l = ((p1 * r1 - t1h) + p1 * r2 + p2 * r1) + p2 * r2;
+  t1l = t1l + (a.hi * b.lo + a.lo * b.hi);
+  double s1 = t1h + t1l;
+  t1l = t1l - (s1 - t1h);
+  return DD{s1, t1l};
+}
+DD dd_div(DD a, DD b) {
+  double q1 = a.hi / b.hi;
+  double t1h = b.hi * q1;
+  double u1 = 134217729.0 * b.hi;
+  double p1 = u1 - (u1 - b.hi);
+  double p2 = b.hi - p1;
+  u1 = 134217729.0 * q1;
+  double r1 = u1 - (u1 - q1);
+  double r2 = q1 - r1;
+  double t1l = ((p1 * r1 - t1h) + p1 * r2 + p2 * r1) + p2 * r2;
+  t1l = t1l + (b.lo * q1);
+  double s1 = t1h + t1l;
+  t1l = t1l - (s1 - t1h);
+  t1h = s1;
+  s1 = a.hi - t1h;
+  r1 = s1 - a.hi;
+  double s2 = (a.hi - (s1 - r1)) - (t1h + r1);
+  s2 = s2 - t1l;
+  s2 = s2 + a.lo;
+  double q2 = (s1 + s2) / b.hi;
+  double h = q1 + q2;
+  return DD{h, q2 - (h - q1)};
+}
+// A zero argument falls through to the general formula (the reference sets 0 and then
+// overwrites it); a negative one gives 0.
+DD dd_sqrt(DD a) {
+  if (a.hi < 0.0 || (a.hi == 0.0 && a.lo < 0.0)) return DD{0.0, 0.0};
+  double x = 1.0 / std::sqrt(a.hi);
+  double ax = a.hi * x;
+  DD y = dd_mul(DD{x, 0.0}, DD{0.5, 0.0});
+  DD z = dd_mul(DD{ax, 0.0}, DD{ax, 0.0});
+  DD t2 = dd_sub(a, z);
+  DD t1 = dd_mul(t2, y);
+  return dd_add(t1, DD{ax, 0.0});
+}
+
+// dd dot: DD_NCHUNK contiguous chunks, each summed in index order, then the chunk sums
+// in chunk order (fixed, independent of the thread count; the reference's blocked
+// accumulators, ddvec.f90:111-240, follow its OpenMP split instead).
+constexpr int DD_NCHUNK = 1024;
+DD dd_dot(long n, const double* xh, const double* xl, const double* yh, const double* yl) {
+  DD part[DD_NCHUNK];
+  long nch = std::min<long>(DD_NCHUNK, std::max<long>(1, n));
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < nch; ++c) {
+    long lo = n * c / nch, hi = n * (c + 1) / nch;
+    DD s{0.0, 0.0};
+    for (long i = lo; i < hi; ++i) s = dd_add(s, dd_mul(DD{xh[i], xl[i]}, DD{yh[i], yl[i]}));
+    part[c] = s;
+  }
+  DD s{0.0, 0.0};
+  for (long c = 0; c < nch; ++c) s = dd_add(s, part[c]);
+  return s;
+}
+
+// ddMatVec_crs (ddmatrix.f90:1785-2355), single process: per row, c = a_ij x_j and
+// t = c + t over the row in CRS order.  A's low parts are used when alo is given.
+void dd_spmv(const OrcMat& A, const double* alo, const double* xh, const double* xl, double* yh, double* yl) {
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < A.n; ++i) {
+    DD t{0.0, 0.0};
+    for (long j = A.rowptr[i] - 1; j < A.rowptr[i + 1] - 1; ++j) {
+      const long c = A.col[j] - A.istart;
+      t = dd_add(dd_mul(DD{A.val[j], alo ? alo[j] : 0.0}, DD{xh[c], xl[c]}), t);
+    }
+    yh[i] = t.hi;
+    yl[i] = t.lo;
+  }
+}
+
+// ddaxpy (ddvec.f90:14-54): y = alpha x + beta y
+void dd_axpy(long n, DD alpha, DD beta, const double* xh, const double* xl, double* yh, double* yl) {
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; ++i) {
+    DD c = dd_mul(beta, DD{yh[i], yl[i]});
+    DD b = dd_mul(alpha, DD{xh[i], xl[i]});
+    DD y = dd_add(b, c);
+    yh[i] = y.hi;
+    yl[i] = y.lo;
+  }
+}
+
+struct DdPrecon {
+  int kind = ORC_PRECON_NONE;
+  int method = ORC_ILUD;
+  int prec = 2;                          // PRECISION_PRECONDITION
+  std::vector<double> dh, dl;            // D^-1 (point Jacobi or D-ILU), double-double
+  std::vector<DiluBlock> blocks;         // D-ILU L / U ranges
+};
+
+// ddget_DInv_crs (ddmatrix.f90:283-349): D^-1 = 1 / a_ii, a zero pivot replaced by 1e-100.
+void dd_setup_pj(const OrcMat& A, const double* alo, DdPrecon& P) {
+  P.dh.assign(A.n, 0.0);
+  P.dl.assign(A.n, 0.0);
+  for (long k = 0; k < A.n; ++k)
+    for (long j = A.rowptr[k] - 1; j < A.rowptr[k + 1] - 1; ++j)
+      if (A.col[j] - A.istart == k) {
+        DD a{A.val[j], alo ? alo[j] : 0.0};
+        DD d = (a.hi == 0.0 && a.lo == 0.0) ? dd_div(DD{1.0, 0.0}, DD{1.0e-100, 0.0})
+                                            : dd_div(DD{1.0, 0.0}, a);
+        P.dh[k] = d.hi;
+        P.dl[k] = d.lo;
+      }
+}
+
+// ddDILU_DInv_crs (ddmatrix.f90:1451-1640) with independ_nvec = 1: the D-ILU diagonal in
+// dd arithmetic, then D^-1 = 1 / D (a zero D replaced by 1e-100).  The L / U ranges of the
+// sweeps are the double setup's.
+int dd_setup_dilu(const OrcMat& A, const double* alo, int nb, int method, DdPrecon& P) {
+  Precon tmp;
+  int err = setup_dilu(A, nb, method, tmp);
+  if (err) return err;
+  P.blocks = tmp.dilu;
+  P.dh.assign(A.n, 0.0);
+  P.dl.assign(A.n, 0.0);
+  auto av = [&](long j) { return DD{A.val[j], alo ? alo[j] : 0.0}; };
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int b = 0; b < nb; ++b) {
+    const DiluBlock& B = P.blocks[b];
+    long gs = A.istart + B.r0, ge = A.istart + B.r1 - 1;
+    long m = B.r1 - B.r0;
+    std::vector<DD> D(m, DD{0.0, 0.0});
+    for (long k = 0; k < m; ++k) {
+      long gk = B.r0 + k;
+      long jstart = -1;
+      for (long j = A.rowptr[gk] - 1; j < A.rowptr[gk + 1] - 1; ++j) {
+        if (A.col[j] < gs || A.col[j] > ge) continue;
+        if (jstart == -1) jstart = j;
+        long colk = A.col[j] - A.istart;
+        if (colk < gk) continue;
+        D[k] = colk == gk ? av(j) : DD{0.0, 0.0};
+        for (long jr = jstart; jr < j; ++jr) {
+          long kr = A.col[jr] - A.istart;              // local row of the L entry
+          for (long i = A.rowptr[kr] - 1; i < A.rowptr[kr + 1] - 1; ++i) {
+            if (A.col[i] < gs) continue;
+            if (A.col[i] > ge) break;
+            long rc = A.col[i] - A.istart;
+            bool take = method == ORC_ILUD ? rc == gk : kr < rc;
+            if (!take) continue;
+            DD c = dd_mul(av(jr), av(i));
+            DD dk = D[kr - B.r0];
+            c = (dk.hi == 0.0 && dk.lo == 0.0) ? dd_div(c, DD{1.0e-100, 0.0}) : dd_div(c, dk);
+            D[k] = dd_sub(D[k], c);
+            if (method == ORC_ILUD) break;
+          }
+        }
+        break;
+      }
+    }
+    for (long k = 0; k < m; ++k) {
+      DD d = (D[k].hi == 0.0 && D[k].lo == 0.0) ? dd_div(DD{1.0, 0.0}, DD{1.0e-100, 0.0})
+                                                : dd_div(DD{1.0, 0.0}, D[k]);
+      P.dh[B.r0 + k] = d.hi;
+      P.dl[B.r0 + k] = d.lo;
+    }
+  }
+  return 0;
+}
+
+// ddsolve_ILU_crs (ddmatrix.f90:4310-4680), independ_nvec = 1: forward
+// z = r - sum L s, s = z D^-1; backward z = sum U s (Ustart down to Uend), s = s - D^-1 z.
+// PRECISION_PRECONDITION 1 drops the low parts of A and of D^-1.
+void dd_solve_dilu_block(const OrcMat& A, const double* alo, const DiluBlock& B, const double* dh,
+                         const double* dl, int prec, const double* rh, const double* rl, double* sh,
+                         double* sl) {
+  long m = B.r1 - B.r0;
+  long off = A.istart + B.r0;
+  auto av = [&](long j) { return DD{A.val[j], (prec == 2 && alo) ? alo[j] : 0.0}; };
+  for (long k = 0; k < m; ++k) {
+    DD zz{rh[k], rl[k]};
+    for (long j = B.Ls[k]; j <= B.Le[k]; ++j) {
+      long c = A.col[j] - off;
+      zz = dd_sub(zz, dd_mul(DD{sh[c], sl[c]}, av(j)));
+    }
+    DD s = dd_mul(zz, DD{dh[k], prec == 2 ? dl[k] : 0.0});
+    sh[k] = s.hi;
+    sl[k] = s.lo;
+  }
+  for (long k = m - 1; k >= 0; --k) {
+    DD zz{0.0, 0.0};
+    for (long j = B.Us[k]; j >= B.Ue[k]; --j) {
+      long c = A.col[j] - off;
+      zz = dd_add(zz, dd_mul(DD{sh[c], sl[c]}, av(j)));
+    }
+    DD c = dd_mul(DD{dh[k], prec == 2 ? dl[k] : 0.0}, zz);
+    DD s = dd_sub(DD{sh[k], sl[k]}, c);
+    sh[k] = s.hi;
+    sl[k] = s.lo;
+  }
+}
+
+void dd_apply_precon(const OrcMat& A, const double* alo, const DdPrecon& P, const double* rh,
+                     const double* rl, double* sh, double* sl) {
+  switch (P.kind) {
+    case ORC_PRECON_NONE:
+#pragma omp parallel for schedule(static)
+      for (long i = 0; i < A.n; ++i) { sh[i] = rh[i]; sl[i] = rl[i]; }
+      break;
+    case ORC_PRECON_PJ:
+#pragma omp parallel for schedule(static)
+      for (long i = 0; i < A.n; ++i) {   // ddpointJacobi (ddmatrix.f90:3523-3567): z = D^-1 r
+        DD z = dd_mul(DD{P.dh[i], P.prec == 2 ? P.dl[i] : 0.0}, DD{rh[i], rl[i]});
+        sh[i] = z.hi;
+        sl[i] = z.lo;
+      }
+      break;
+    default:
+#pragma omp parallel for schedule(dynamic, 1)
+      for (size_t b = 0; b < P.blocks.size(); ++b) {
+        const long r0 = P.blocks[b].r0;
+        dd_solve_dilu_block(A, alo, P.blocks[b], P.dh.data() + r0, P.dl.data() + r0, P.prec, rh + r0,
+                            rl + r0, sh + r0, sl + r0);
+      }
+      break;
+  }
+}
+
+// ddKSP_pCG (ddpcg.f90:247-563): lagged x update, stop on the recursive residual.
+void ddpcg(const OrcMat& A, const double* alo, const DdPrecon& P, const OrcParams& prm, const double* bh,
+           const double* bl, double* xh, double* xl, double* hist, int* niter, int* iret) {
+  long n = A.n;
+  std::vector<double> rh(n), rl(n), ph(n, 0.0), pl(n, 0.0), qh(n), ql(n), sh(n), sl(n);
+  dd_spmv(A, alo, xh, xl, rh.data(), rl.data());                 // ddcalc_res: r = A x,
+  dd_axpy(n, DD{1.0, 0.0}, DD{-1.0, 0.0}, bh, bl, rh.data(), rl.data());   // r = 1 b - 1 r
+  DD bnorm = dd_sqrt(dd_dot(n, bh, bl, bh, bl));
+  DD rnorm = dd_sqrt(dd_dot(n, rh.data(), rl.data(), rh.data(), rl.data()));
+  DD alpha{0.0, 0.0}, beta{0.0, 0.0};
+  dd_apply_precon(A, alo, P, rh.data(), rl.data(), sh.data(), sl.data());
+  DD rho0 = dd_dot(n, sh.data(), sl.data(), rh.data(), rl.data());
+  int itr;
+  for (itr = 1; itr <= prm.itrmax; ++itr) {
+    hist[itr - 1] = rnorm.hi / bnorm.hi;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {                 // ddCG_axpy2 (ddpcg.f90:9-59)
+      DD x = dd_add(DD{xh[i], xl[i]}, dd_mul(alpha, DD{ph[i], pl[i]}));
+      DD p = dd_add(DD{sh[i], sl[i]}, dd_mul(beta, DD{ph[i], pl[i]}));
+      xh[i] = x.hi; xl[i] = x.lo;
+      ph[i] = p.hi; pl[i] = p.lo;
+    }
+    dd_spmv(A, alo, ph.data(), pl.data(), qh.data(), ql.data());
+    DD gamma = dd_dot(n, ph.data(), pl.data(), qh.data(), ql.data());
+    alpha = dd_div(rho0, gamma);
+    DD t1 = dd_mul(DD{-1.0, 0.0}, alpha);
+    dd_axpy(n, t1, DD{1.0, 0.0}, qh.data(), ql.data(), rh.data(), rl.data());
+    dd_apply_precon(A, alo, P, rh.data(), rl.data(), sh.data(), sl.data());
+    DD rho1 = dd_dot(n, sh.data(), sl.data(), rh.data(), rl.data());   // ddCG_calc_dot2
+    rnorm = dd_sqrt(dd_dot(n, rh.data(), rl.data(), rh.data(), rl.data()));
+    if (rnorm.hi / bnorm.hi < prm.rtolmax) break;
+    beta = dd_div(rho1, rho0);
+    rho0 = rho1;
+  }
+  dd_axpy(n, alpha, DD{1.0, 0.0}, ph.data(), pl.data(), xh, xl);
+  *niter = std::min(prm.itrmax, itr);
+  *iret = (prm.itrmax <= itr) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------------
 // C entry points used by the tests and the CPU-baseline leg of bench.py.
 extern "C" {
 
@@ -663,5 +962,35 @@ void orc_precon_apply_h(void* h, const double* r, double* s) {
 }
 
 void orc_precon_destroy(void* h) { delete static_cast<Precon*>(h); }
+
+// ddKSP_pCG through PARCEL_ddKSP_CRS's precision flags (ddwrapper.f90:184-280):
+// prec_A/b/x/M = 1 (double) or 2 (double-double).  A low parts (alo), b low parts and the
+// initial x low parts may be null.  ipreflag 0 / 1 / 2-3 (D-ILU, ILU_method 1 or 2).
+int orc_ddcg(const OrcMat* A, const double* alo, const OrcParams* prm, int prec_A, int prec_b, int prec_x,
+             int prec_M, const double* bh, const double* bl, double* xh, double* xl, double* hist, int* niter,
+             int* iret) {
+  const long n = A->n;
+  std::vector<double> bl0(n, 0.0), xl0(n, 0.0);
+  if (prec_b == 2 && bl) std::copy(bl, bl + n, bl0.begin());
+  if (prec_x == 2 && xl) std::copy(xl, xl + n, xl0.begin());
+  const double* a_lo = (prec_A == 2) ? alo : nullptr;
+  DdPrecon P;
+  P.prec = prec_M;
+  int kind = prm->ipreflag == ORC_PRECON_AS ? ORC_PRECON_BJ : prm->ipreflag;
+  P.kind = kind;
+  P.method = prm->ILU_method < 0 ? ORC_ILUD : prm->ILU_method;
+  if (kind == ORC_PRECON_PJ) {
+    dd_setup_pj(*A, a_lo, P);
+  } else if (kind == ORC_PRECON_BJ) {
+    if (P.method == ORC_ILU0) return ORC_E_UNSUPPORTED;
+    int err = dd_setup_dilu(*A, a_lo, nblocks_for(*A, prm->precon_thblock), P.method, P);
+    if (err) return err;
+  } else if (kind != ORC_PRECON_NONE) {
+    return ORC_E_UNSUPPORTED;
+  }
+  ddpcg(*A, a_lo, P, *prm, bh, bl0.data(), xh, xl0.data(), hist, niter, iret);
+  if (prec_x == 2 && xl) std::copy(xl0.begin(), xl0.end(), xl);
+  return 0;
+}
 
 }  // extern "C"

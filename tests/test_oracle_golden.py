@@ -3,7 +3,9 @@
 Known answers (src/example/template_cpu/STDOUT_run and template_gpu/STDOUT_run): CG on the
 160^3 Poisson problem of src/example/problem.f90, rtolmax 1e-9, x0 = 0.
   * block-Jacobi D-ILU (ILU_method=1), 80 blocks: 291 iterations, rel. error 5.1459e-9;
-  * block-Jacobi ILU(0), 4 blocks (cuSPARSE on GPU, one block per rank): 227 iterations.
+  * block-Jacobi ILU(0), 4 blocks (cuSPARSE on GPU, one block per rank): 227 iterations;
+  * double-double CG (template_cpu/STDOUT_run_dd, every PRECISION_* = 2), block-Jacobi
+    D-ILU, 80 blocks: 291 iterations, max|x - x_exact| = 4.957113223374998e-9.
 Match criteria: iteration count within +-2 and per-iteration relative history difference
 <= 1e-6 (the reference's OpenMP/MPI reductions sum in a different order).
 """
@@ -73,3 +75,18 @@ def test_oracle_ilu0_is_exact_for_tridiagonal():
     r = rng.standard_normal(n)
     s = oracle.precon_apply(A, r, ipreflag=2, ILU_method=0, precon_thblock=1)
     assert np.allclose(M @ s, r, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.slow
+def test_ddcg_dilu80_matches_template_cpu_dd():
+    """The oracle's double-double CG (ddKSP_pCG) against STDOUT_run_dd's dd history."""
+    fx = golden()["cpu_cg_dilu80_dd"]
+    A, b, xe = poisson_reference(160)
+    xh, xl, h, niter, iret = oracle.ddcg(A, b, ipreflag=2, ILU_method=1, precon_thblock=80, itrmax=2000,
+                                         rtolmax=1e-9)
+    g = np.array(fx["history_dd"])
+    assert iret == 0 and abs(niter - len(g)) <= 2
+    k = min(len(g), len(h))
+    assert (np.abs(h[:k] - g[:k]) / g[:k]).max() <= 1e-6
+    err = np.abs(xh + xl - xe).max()
+    assert abs(err - fx["abs_err"]) / fx["abs_err"] < 1e-3
