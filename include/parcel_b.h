@@ -201,6 +201,15 @@ void parcel_dcagmres_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int3
 /* ---- drop-in shims, GPU-build ABI: vecx, vecb, crsa, crsrow_ptr and crscol are passed
  * as `devicemem*` (src/CUDA/src/cu_common.h:37-42), whose first member is the device
  * pointer; a `void**` pointing at the device pointer is the same thing. ------------- */
+/* parcel_ddcg_c (src/example/c2fortran_kernel.f90:620-708): the double-double CG with the
+ * reference's argument order; host arrays; niter in = itrmax, out = iterations. */
+void parcel_ddcg_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo, int32_t* n,
+                    int32_t* gn, int32_t* nnz, int32_t* istart, double* crsa, double* crsa_lo,
+                    int32_t* crsrow_ptr, int32_t* crscol, int* ipreflag, int* ilu_method, int* addl,
+                    int* iflagas, int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                    int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock,
+                    int* precision_a, int* precision_b, int* precision_x, int* precision_precondition,
+                    int* iret);
 void parcel_dcg_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn,
                        int32_t* nnz, int32_t* istart, void** crsa, void** crsrow_ptr,
                        void** crscol, int* ipreflag, int* ilu_method, int* addl,
@@ -269,6 +278,19 @@ int parcel_b_dot_noalloc(int64_t n, const double* x, const double* y, double* re
  * arrays; returns r as (r_hi, r_lo). */
 int parcel_b_residual_dd(const parcel_b_crs* A, const double* x_hi, const double* x_lo,
                          const double* b_hi, const double* b_lo, double* r_hi, double* r_lo);
+
+/* Double-double preconditioned CG (ddKSP_pCG, src/ddpcg.f90:247-563, called through
+ * PARCEL_ddKSP_CRS's precision flags, src/ddwrapper.f90:184-280).  Each of A, b, x and
+ * the preconditioner is in double (1) or double-double (2): a low-part array (val_lo,
+ * b_lo, x_lo) is used when its flag is 2 and may be NULL otherwise (or to mean zero).
+ * prm->solver is ignored (CG); ipreflag 0 (none), 1 (point Jacobi) or 2/3 (block-Jacobi
+ * D-ILU, ILU_method 1 or 2; ILU(0) returns PARCEL_B_E_UNSUPPORTED).  x_hi (and x_lo when
+ * precision_x is 2) in/out.  Host or device arrays.  The reference runs this solver on
+ * the CPU only; here it runs on the GPU with the reference's dd operation order
+ * (dd_func.f90) and a fixed dot-product split, bit-for-bit reproducible. */
+int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo, int precision_A,
+                  int precision_b, int precision_x, int precision_precondition, const double* b_hi,
+                  const double* b_lo, double* x_hi, double* x_lo, double* reshistory, int* niter, int* iret);
 
 /* Kernel timing for benchmarks: builds the solver layout and preconditioner described by
  * prm (setup excluded from the timing), then launches `reps` back-to-back SpMVs and `reps`

@@ -1,0 +1,581 @@
+// pb_ddcg.cu -- double-double preconditioned CG on the GPU (PARCEL_ddKSP_CRS, solver 1).
+//
+// Reference: ddKSP_pCG (src/ddpcg.f90:247-563) with the precision flags of
+// PARCEL_ddKSP_CRS (src/ddwrapper.f90:184-280): A, b, x and the preconditioner each in
+// double (1) or double-double (2).  The reference runs its dd solvers on the CPU only
+// (src/ddkrylov.f90:81,207); this is a GPU implementation of the same arithmetic.
+//
+// Every dd operation is the reference's sequence of explicitly rounded double operations
+// (pb_device.cuh), every per-row loop runs in the reference's order (the CRS order for the
+// SpMV, L start..end and U start down to end for the D-ILU sweeps, the D-ILU diagonal
+// recurrence of ddDILU_DInv_crs), and the dot products sum a fixed split of the index
+// range (1,024 contiguous chunks, each in index order, then the chunk sums in order), so
+// the solve is bit-for-bit reproducible and identical to the CPU oracle's restatement.
+// The D-ILU rows run level by level on the wavefront plan of the FP64 block-Jacobi path;
+// the level order changes no row's arithmetic.
+#include <cstring>
+#include <vector>
+
+#include "pb_api.cuh"
+#include "pb_device.cuh"
+#include "pb_ilu.cuh"
+
+namespace pb {
+
+namespace {
+
+constexpr int kDdChunks = 1024;   // dot-product split (shared with the oracle)
+constexpr int kDdThreads = 256;
+
+#define GRID_LOOP(i, n) \
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+inline int grid_for(int64_t n) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + kDdThreads - 1) / kDdThreads, 8LL * num_sms()));
+}
+
+// Scalars of the iteration, on the device.
+struct DdScal {
+  dd bnorm, rnorm, rho0, rho1, gamma, alpha, beta, t1;
+};
+
+// ------------------------------------------------------------------ vector kernels
+// y = A x: per row, c = a_ij x_j and t = c + t in CRS order (ddMatVec_crs, single process).
+__global__ void k_dd_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                          const double* __restrict__ ah, const double* __restrict__ al, int cbase,
+                          const double* __restrict__ xh, const double* __restrict__ xl, double* __restrict__ yh,
+                          double* __restrict__ yl) {
+  GRID_LOOP(i, n) {
+    dd t{0.0, 0.0};
+    for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
+      const int c = ci[j] - cbase;
+      t = dd_add(dd_mul(dd{ah[j], al ? al[j] : 0.0}, dd{xh[c], xl[c]}), t);
+    }
+    yh[i] = t.hi;
+    yl[i] = t.lo;
+  }
+}
+
+// ddaxpy (ddvec.f90:14-54): y = alpha x + beta y, the scalars read from the device.
+__global__ void k_dd_axpy(int n, const dd* alpha, const dd* beta, const double* __restrict__ xh,
+                          const double* __restrict__ xl, double* __restrict__ yh, double* __restrict__ yl) {
+  const dd a = *alpha, b = *beta;
+  GRID_LOOP(i, n) {
+    const dd c = dd_mul(b, dd{yh[i], yl[i]});
+    const dd t = dd_mul(a, dd{xh[i], xl[i]});
+    const dd y = dd_add(t, c);
+    yh[i] = y.hi;
+    yl[i] = y.lo;
+  }
+}
+
+// ddCG_axpy2 (ddpcg.f90:9-59): x = x + alpha p, p = s + beta p.
+__global__ void k_dd_cg_axpy2(int n, const DdScal* sc, double* __restrict__ xh, double* __restrict__ xl,
+                              double* __restrict__ ph, double* __restrict__ pl, const double* __restrict__ sh,
+                              const double* __restrict__ sl) {
+  const dd a = sc->alpha, b = sc->beta;
+  GRID_LOOP(i, n) {
+    const dd p = dd{ph[i], pl[i]};
+    const dd x = dd_add(dd{xh[i], xl[i]}, dd_mul(a, p));
+    const dd q = dd_add(dd{sh[i], sl[i]}, dd_mul(b, p));
+    xh[i] = x.hi;
+    xl[i] = x.lo;
+    ph[i] = q.hi;
+    pl[i] = q.lo;
+  }
+}
+
+// Dot product, first stage: chunk c of kDdChunks (contiguous, index order).
+__global__ void k_dd_dot_chunks(int64_t n, int nch, const double* __restrict__ xh, const double* __restrict__ xl,
+                                const double* __restrict__ yh, const double* __restrict__ yl, dd* part) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nch) return;
+  const int64_t lo = n * c / nch, hi = n * (c + 1) / nch;
+  dd s{0.0, 0.0};
+  for (int64_t i = lo; i < hi; ++i) s = dd_add(s, dd_mul(dd{xh[i], xl[i]}, dd{yh[i], yl[i]}));
+  part[c] = s;
+}
+
+// Second stage: the chunk sums in chunk order, into *out.
+__global__ void k_dd_dot_final(int nch, const dd* part, dd* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  dd s{0.0, 0.0};
+  for (int c = 0; c < nch; ++c) s = dd_add(s, part[c]);
+  *out = s;
+}
+
+enum DdStep { DD_INIT_NORMS = 0, DD_INIT_RHO, DD_ALPHA, DD_RNORM, DD_BETA };
+
+// Scalar updates of ddKSP_pCG, one thread.
+__global__ void k_dd_scal(DdScal* sc, int step, const dd* bdot, const dd* rdot) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  switch (step) {
+    case DD_INIT_NORMS:
+      sc->bnorm = dd_sqrt(*bdot);
+      sc->rnorm = dd_sqrt(*rdot);
+      sc->alpha = dd{0.0, 0.0};
+      sc->beta = dd{0.0, 0.0};
+      break;
+    case DD_INIT_RHO:
+      sc->rho0 = *bdot;
+      break;
+    case DD_ALPHA:
+      sc->gamma = *bdot;
+      sc->alpha = dd_div(sc->rho0, sc->gamma);
+      sc->t1 = dd_mul(dd{-1.0, 0.0}, sc->alpha);
+      break;
+    case DD_RNORM:
+      sc->rho1 = *bdot;
+      sc->rnorm = dd_sqrt(*rdot);
+      break;
+    case DD_BETA:
+      sc->beta = dd_div(sc->rho1, sc->rho0);
+      sc->rho0 = sc->rho1;
+      break;
+  }
+}
+
+// ------------------------------------------------------------------ preconditioners
+// ddget_DInv_crs (ddmatrix.f90:283-349): 1 / a_ii, a zero pivot replaced by 1e-100.
+__global__ void k_dd_pj_dinv(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                             const double* __restrict__ ah, const double* __restrict__ al, int cbase,
+                             double* __restrict__ dh, double* __restrict__ dl) {
+  GRID_LOOP(k, n) {
+    for (int j = rp[k] - 1; j < rp[k + 1] - 1; ++j)
+      if (ci[j] - cbase == k) {
+        const dd a{ah[j], al ? al[j] : 0.0};
+        const dd d = (a.hi == 0.0 && a.lo == 0.0) ? dd_div(dd{1.0, 0.0}, dd{1.0e-100, 0.0})
+                                                  : dd_div(dd{1.0, 0.0}, a);
+        dh[k] = d.hi;
+        dl[k] = d.lo;
+      }
+  }
+}
+
+// ddpointJacobi (ddmatrix.f90:3523-3567): s = D^-1 r; precision 1 drops D^-1's low part.
+__global__ void k_dd_pj_apply(int n, const double* __restrict__ dh, const double* __restrict__ dl, int prec,
+                              const double* __restrict__ rh, const double* __restrict__ rl, double* __restrict__ sh,
+                              double* __restrict__ sl) {
+  GRID_LOOP(i, n) {
+    const dd z = dd_mul(dd{dh[i], prec == 2 ? dl[i] : 0.0}, dd{rh[i], rl[i]});
+    sh[i] = z.hi;
+    sl[i] = z.lo;
+  }
+}
+
+__global__ void k_dd_copy(int n, const double* __restrict__ rh, const double* __restrict__ rl,
+                          double* __restrict__ sh, double* __restrict__ sl) {
+  GRID_LOOP(i, n) {
+    sh[i] = rh[i];
+    sl[i] = rl[i];
+  }
+}
+
+// In-block L / U ranges of every row (the sweeps of ddsolve_ILU_crs): forward j = Ls..Le,
+// backward j = Us down to Ue (0-based positions).
+__global__ void k_dd_ranges(int n, int nb, const int* __restrict__ blk_lo, const int* __restrict__ blk_hi,
+                            const int* __restrict__ blk_of, const int* __restrict__ rp, const int* __restrict__ ci,
+                            int cbase, int4* __restrict__ rng) {
+  GRID_LOOP(k, n) {
+    const int b = blk_of[k];
+    const int lo = blk_lo[b], hi = blk_hi[b];
+    const int a = rp[k] - 1, z = rp[k + 1] - 1;
+    int Ls = z - 1, Le = a, Us = a, Ue = z - 1;
+    for (int j = a; j < z; ++j)
+      if (ci[j] - cbase >= lo) { Ls = j; break; }
+    for (int j = a; j < z; ++j) {
+      const int c = ci[j] - cbase;
+      if (c < lo) continue;
+      if (c >= k) { Le = j - 1; break; }
+    }
+    for (int j = z - 1; j >= a; --j)
+      if (ci[j] - cbase <= hi - 1) { Us = j; break; }
+    for (int j = z - 1; j >= a; --j)
+      if (ci[j] - cbase <= k) { Ue = j + 1; break; }
+    rng[k] = make_int4(Ls, Le, Us, Ue);
+  }
+}
+
+// ddDILU_DInv_crs (ddmatrix.f90:1451-1640), independ_nvec = 1, one CTA per block, level by
+// level: D_k = a_kk - sum over the lower in-block entries a_kr (kr < k) of a_kr a_rk / D_r
+// (ILUD: the entry of row r in column k only; MLUD: every entry of row r right of r), then
+// D^-1 = 1 / D (a zero D replaced by 1e-100).
+__global__ void k_dd_dilu_diag(const IluChunk* __restrict__ ch, const int* __restrict__ blk_chunk,
+                               const int* __restrict__ blk_lo, const int* __restrict__ blk_hi,
+                               const int* __restrict__ rowAt, const int* __restrict__ rp,
+                               const int* __restrict__ ci, const double* __restrict__ ah,
+                               const double* __restrict__ al, int cbase, int mlud, double* Dh, double* Dl,
+                               double* __restrict__ dih, double* __restrict__ dil) {
+  const int b = blockIdx.x;
+  const int lo = blk_lo[b], hi = blk_hi[b];
+  auto av = [&](int j) { return dd{ah[j], al ? al[j] : 0.0}; };
+  for (int c = blk_chunk[b]; c < blk_chunk[b + 1]; ++c) {
+    const IluChunk C = ch[c];
+    for (int p = threadIdx.x; p < C.w; p += blockDim.x) {
+      const int k = rowAt[C.start + p];
+      dd D{0.0, 0.0};
+      int jstart = -1;
+      for (int j = rp[k] - 1; j < rp[k + 1] - 1; ++j) {
+        const int col = ci[j] - cbase;
+        if (col < lo || col >= hi) continue;
+        if (jstart == -1) jstart = j;
+        if (col < k) continue;
+        D = col == k ? av(j) : dd{0.0, 0.0};
+        for (int jr = jstart; jr < j; ++jr) {
+          const int kr = ci[jr] - cbase;
+          const dd Dr{Dh[kr], Dl[kr]};
+          for (int i = rp[kr] - 1; i < rp[kr + 1] - 1; ++i) {
+            const int rc = ci[i] - cbase;
+            if (rc < lo) continue;
+            if (rc >= hi) break;
+            const bool take = mlud ? kr < rc : rc == k;
+            if (!take) continue;
+            dd t = dd_mul(av(jr), av(i));
+            t = (Dr.hi == 0.0 && Dr.lo == 0.0) ? dd_div(t, dd{1.0e-100, 0.0}) : dd_div(t, Dr);
+            D = dd_sub(D, t);
+            if (!mlud) break;
+          }
+        }
+        break;
+      }
+      Dh[k] = D.hi;
+      Dl[k] = D.lo;
+      const dd di = (D.hi == 0.0 && D.lo == 0.0) ? dd_div(dd{1.0, 0.0}, dd{1.0e-100, 0.0})
+                                                 : dd_div(dd{1.0, 0.0}, D);
+      dih[k] = di.hi;
+      dil[k] = di.lo;
+    }
+    __syncthreads();
+  }
+}
+
+// ddsolve_ILU_crs (ddmatrix.f90:4310-4680), independ_nvec = 1, one CTA per block, the
+// forward levels in order then the backward levels in reverse:
+//   forward  z = r_k - sum_{j=Ls..Le} s_c a_j,  s_k = z D^-1
+//   backward z = sum_{j=Us..Ue, descending} s_c a_j,  s_k = s_k - D^-1 z
+// Precision 1 drops the low parts of A and of D^-1.
+__global__ void k_dd_dilu_sweep(const IluChunk* __restrict__ ch, const int* __restrict__ blk_chunk,
+                                const int* __restrict__ rowAt, const int4* __restrict__ rng,
+                                const int* __restrict__ ci, const double* __restrict__ ah,
+                                const double* __restrict__ al, int cbase, const double* __restrict__ dih,
+                                const double* __restrict__ dil, int prec, const double* __restrict__ rh,
+                                const double* __restrict__ rl, double* sh, double* sl) {
+  const int b = blockIdx.x;
+  const int c0 = blk_chunk[b], c1 = blk_chunk[b + 1];
+  auto av = [&](int j) { return dd{ah[j], (prec == 2 && al) ? al[j] : 0.0}; };
+  for (int c = c0; c < c1; ++c) {
+    const IluChunk C = ch[c];
+    for (int p = threadIdx.x; p < C.w; p += blockDim.x) {
+      const int k = rowAt[C.start + p];
+      const int4 r = rng[k];
+      dd z{rh[k], rl[k]};
+      for (int j = r.x; j <= r.y; ++j) {
+        const int col = ci[j] - cbase;
+        z = dd_sub(z, dd_mul(dd{sh[col], sl[col]}, av(j)));
+      }
+      const dd s = dd_mul(z, dd{dih[k], prec == 2 ? dil[k] : 0.0});
+      sh[k] = s.hi;
+      sl[k] = s.lo;
+    }
+    __syncthreads();
+  }
+  for (int c = c1 - 1; c >= c0; --c) {
+    const IluChunk C = ch[c];
+    for (int p = threadIdx.x; p < C.w; p += blockDim.x) {
+      const int k = rowAt[C.start + p];
+      const int4 r = rng[k];
+      dd z{0.0, 0.0};
+      for (int j = r.z; j >= r.w; --j) {
+        const int col = ci[j] - cbase;
+        z = dd_add(z, dd_mul(dd{sh[col], sl[col]}, av(j)));
+      }
+      const dd t = dd_mul(dd{dih[k], prec == 2 ? dil[k] : 0.0}, z);
+      const dd s = dd_sub(dd{sh[k], sl[k]}, t);
+      sh[k] = s.hi;
+      sl[k] = s.lo;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_block_of(int nb, const int* __restrict__ blk_lo, const int* __restrict__ blk_hi, int* blk_of) {
+  const int b = blockIdx.x;
+  if (b >= nb) return;
+  for (int k = blk_lo[b] + threadIdx.x; k < blk_hi[b]; k += blockDim.x) blk_of[k] = b;
+}
+
+// ------------------------------------------------------------------ host side
+struct DdVec {
+  DBuf h, l;
+  explicit DdVec(int n) : h(sizeof(double) * std::max(n, 1)), l(sizeof(double) * std::max(n, 1)) {}
+  double* hi() const { return dp<double>(h); }
+  double* lo() const { return dp<double>(l); }
+};
+
+struct DdPrecon {
+  int kind = PARCEL_B_PRECON_NONE;
+  int prec = 2;
+  DBuf dih, dil;                        // D^-1 (point Jacobi, D-ILU)
+  DBuf chunks, blk_chunk, rowAt, rng;   // D-ILU level plan and row ranges
+  int nb = 0;
+};
+
+// Device copy of a natural-layout array given by host or device pointer (null stays null).
+struct Arr {
+  DBuf own;
+  const void* p = nullptr;
+  Arr(const void* src, size_t bytes) {
+    if (!src) return;
+    if (is_device_ptr(src)) { p = src; return; }
+    own.alloc(bytes);
+    h2d(own.p, src, bytes);
+    p = own.p;
+  }
+};
+
+struct DdSystem {
+  int n = 0, cbase = 1;
+  const int* rp = nullptr;
+  const int* ci = nullptr;
+  const double* ah = nullptr;
+  const double* al = nullptr;   // null: A's low parts are zero
+};
+
+void dd_dot(const DdSystem& S, const double* xh, const double* xl, const double* yh, const double* yl, dd* part,
+            dd* out, cudaStream_t st) {
+  const int nch = (int)std::min<int64_t>(kDdChunks, std::max(1, S.n));
+  k_dd_dot_chunks<<<(nch + 255) / 256, 256, 0, st>>>(S.n, nch, xh, xl, yh, yl, part);
+  k_dd_dot_final<<<1, 32, 0, st>>>(nch, part, out);
+}
+
+void dd_setup_precon(const Options& o, const parcel_b_crs& A, const DdSystem& S, int prec_M, DdPrecon& P) {
+  cudaStream_t st = stream();
+  P.kind = o.precon == PARCEL_B_PRECON_ADDITIVESCHWARZ ? PARCEL_B_PRECON_BLOCKJACOBI : o.precon;
+  P.prec = prec_M;
+  if (P.kind == PARCEL_B_PRECON_NONE) return;
+  P.dih.alloc(sizeof(double) * S.n);
+  P.dil.alloc(sizeof(double) * S.n);
+  if (P.kind == PARCEL_B_PRECON_POINTJACOBI) {
+    k_dd_pj_dinv<<<grid_for(S.n), kDdThreads, 0, st>>>(S.n, S.rp, S.ci, S.ah, S.al, S.cbase, dp<double>(P.dih),
+                                                        dp<double>(P.dil));
+    PB_CUDA(cudaGetLastError());
+    return;
+  }
+  PB_CHECK(P.kind == PARCEL_B_PRECON_BLOCKJACOBI, PARCEL_B_E_UNSUPPORTED,
+           "ipreflag=%d: the dd CG provides none, point Jacobi and block Jacobi", o.precon);
+  PB_CHECK(o.ilu_method == 1 || o.ilu_method == 2, PARCEL_B_E_UNSUPPORTED,
+           "ILU_method=%d: the dd CG's block-Jacobi preconditioner is D-ILU (1 or 2)", o.ilu_method);
+  // wavefront plan on the host (the structure comes back from the device if it lives there)
+  std::vector<int> hrp, hci;
+  const int* hrpp = A.rowptr;
+  const int* hcip = A.col;
+  if (is_device_ptr(A.rowptr)) {
+    hrp.resize((size_t)A.n + 1);
+    hci.resize((size_t)A.nnz);
+    d2h(hrp.data(), A.rowptr, sizeof(int) * hrp.size());
+    d2h(hci.data(), A.col, sizeof(int) * hci.size());
+    hrpp = hrp.data();
+    hcip = hci.data();
+  }
+  HostCSR H;
+  H.n = A.n; H.nnz = A.nnz; H.istart = A.istart; H.rowptr = hrpp; H.col = hcip;
+  std::vector<int> pos(A.n), lev(A.n);
+  IluPlan plan;
+  ilu_build_plan(H, std::max(1, std::min(o.nblocks, A.n)), plan, pos.data(), lev.data());
+  P.nb = plan.nb;
+  P.chunks.alloc(sizeof(IluChunk) * std::max<size_t>(plan.chunks.size(), 1));
+  h2d(P.chunks.p, plan.chunks.data(), sizeof(IluChunk) * plan.chunks.size());
+  P.blk_chunk.alloc(sizeof(int) * (plan.nb + 1));
+  h2d(P.blk_chunk.p, plan.blk_chunk.data(), sizeof(int) * (plan.nb + 1));
+  DBuf dpos(sizeof(int) * A.n), blo(sizeof(int) * plan.nb), bhi(sizeof(int) * plan.nb), bof(sizeof(int) * A.n);
+  h2d(dpos.p, pos.data(), sizeof(int) * A.n);
+  h2d(blo.p, plan.blk_lo.data(), sizeof(int) * plan.nb);
+  h2d(bhi.p, plan.blk_hi.data(), sizeof(int) * plan.nb);
+  P.rowAt.alloc(sizeof(int) * plan.np);
+  PB_CUDA(cudaMemsetAsync(P.rowAt.p, 0xFF, sizeof(int) * plan.np, st));
+  scatter_positions(A.n, dp<int>(dpos), dp<int>(P.rowAt), st);
+  k_block_of<<<plan.nb, 256, 0, st>>>(plan.nb, dp<int>(blo), dp<int>(bhi), dp<int>(bof));
+  P.rng.alloc(sizeof(int4) * A.n);
+  k_dd_ranges<<<grid_for(A.n), kDdThreads, 0, st>>>(A.n, plan.nb, dp<int>(blo), dp<int>(bhi), dp<int>(bof), S.rp,
+                                                     S.ci, S.cbase, dp<int4>(P.rng));
+  DBuf Dh(sizeof(double) * A.n), Dl(sizeof(double) * A.n);
+  k_dd_dilu_diag<<<plan.nb, kDdThreads, 0, st>>>(dp<IluChunk>(P.chunks), dp<int>(P.blk_chunk), dp<int>(blo),
+                                                 dp<int>(bhi), dp<int>(P.rowAt), S.rp, S.ci, S.ah, S.al, S.cbase,
+                                                 o.ilu_method == 2 ? 1 : 0, dp<double>(Dh), dp<double>(Dl),
+                                                 dp<double>(P.dih), dp<double>(P.dil));
+  PB_CUDA(cudaGetLastError());
+  sync();   // the temporaries above are released on return
+}
+
+void dd_apply_precon(const DdSystem& S, const DdPrecon& P, const double* rh, const double* rl, double* sh,
+                     double* sl, cudaStream_t st) {
+  switch (P.kind) {
+    case PARCEL_B_PRECON_NONE:
+      k_dd_copy<<<grid_for(S.n), kDdThreads, 0, st>>>(S.n, rh, rl, sh, sl);
+      break;
+    case PARCEL_B_PRECON_POINTJACOBI:
+      k_dd_pj_apply<<<grid_for(S.n), kDdThreads, 0, st>>>(S.n, dp<double>(P.dih), dp<double>(P.dil), P.prec, rh,
+                                                          rl, sh, sl);
+      break;
+    default:
+      k_dd_dilu_sweep<<<P.nb, kDdThreads, 0, st>>>(dp<IluChunk>(P.chunks), dp<int>(P.blk_chunk), dp<int>(P.rowAt),
+                                                   dp<int4>(P.rng), S.ci, S.ah, S.al, S.cbase, dp<double>(P.dih),
+                                                   dp<double>(P.dil), P.prec, rh, rl, sh, sl);
+      break;
+  }
+}
+
+}  // namespace
+
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo,
+                             int precision_A, int precision_b, int precision_x, int precision_precondition,
+                             const double* b_hi, const double* b_lo, double* x_hi, double* x_lo,
+                             double* reshistory, int* niter, int* iret) {
+  int used = 0, ir = 0;
+  const int rc = guarded([&]() -> int {
+    ensure_init();
+    validate(A);
+    PB_CHECK(b_hi && x_hi, PARCEL_B_E_ARG, "b_hi and x_hi must not be NULL");
+    for (int f : {precision_A, precision_b, precision_x, precision_precondition})
+      PB_CHECK(f == 1 || f == 2, PARCEL_B_E_ARG, "precision flags are 1 (double) or 2 (double-double)");
+    Options o = resolve_options(prm);
+    PB_CHECK(o.independ_nvec == 1, PARCEL_B_E_UNSUPPORTED,
+             "independ_nvec=%d: only 1 (the reference default) is provided", o.independ_nvec);
+    cudaStream_t st = stream();
+    const int n = A->n;
+    const double t0 = now_s();
+    DdSystem S;
+    S.n = n;
+    S.cbase = A->istart;
+    Arr arp(A->rowptr, sizeof(int) * ((size_t)n + 1)), aci(A->col, sizeof(int) * (size_t)A->nnz),
+        aah(A->val, sizeof(double) * (size_t)A->nnz),
+        aal(precision_A == 2 ? val_lo : nullptr, sizeof(double) * (size_t)A->nnz);
+    S.rp = static_cast<const int*>(arp.p);
+    S.ci = static_cast<const int*>(aci.p);
+    S.ah = static_cast<const double*>(aah.p);
+    S.al = static_cast<const double*>(aal.p);
+    DdPrecon P;
+    dd_setup_precon(o, *A, S, precision_precondition, P);
+    // vectors: x and b in dd, the low parts zero unless their precision is 2
+    DdVec x(n), b(n), r(n), p(n), q(n), s(n);
+    auto load = [&](DdVec& v, const double* hi, const double* lo, bool use_lo) {
+      if (is_device_ptr(hi)) PB_CUDA(cudaMemcpyAsync(v.hi(), hi, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      else h2d(v.hi(), hi, sizeof(double) * n);
+      if (use_lo && lo) {
+        if (is_device_ptr(lo)) PB_CUDA(cudaMemcpyAsync(v.lo(), lo, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        else h2d(v.lo(), lo, sizeof(double) * n);
+      }
+    };
+    load(x, x_hi, x_lo, precision_x == 2);
+    load(b, b_hi, b_lo, precision_b == 2);
+    DBuf scal(sizeof(DdScal)), part(sizeof(dd) * kDdChunks), d1(sizeof(dd)), d2(sizeof(dd)), cst(sizeof(dd) * 4);
+    DdScal* sc = dp<DdScal>(scal);
+    dd* dcst = dp<dd>(cst);   // 1, -1, 0, (unused)
+    {
+      const dd h[4] = {dd{1.0, 0.0}, dd{-1.0, 0.0}, dd{0.0, 0.0}, dd{0.0, 0.0}};
+      h2d(dcst, h, sizeof(h));
+    }
+    const int g = grid_for(n);
+    auto spmv = [&](const DdVec& in, DdVec& out) {
+      k_dd_spmv<<<g, kDdThreads, 0, st>>>(n, S.rp, S.ci, S.ah, S.al, S.cbase, in.hi(), in.lo(), out.hi(), out.lo());
+    };
+    auto dot = [&](const DdVec& u, const DdVec& v, DBuf& out) {
+      dd_dot(S, u.hi(), u.lo(), v.hi(), v.lo(), dp<dd>(part), dp<dd>(out), st);
+    };
+    // r = b - A x (ddcalc_res: r = A x, then r = 1 b + (-1) r)
+    spmv(x, r);
+    k_dd_axpy<<<g, kDdThreads, 0, st>>>(n, dcst + 0, dcst + 1, b.hi(), b.lo(), r.hi(), r.lo());
+    dot(b, b, d1);
+    dot(r, r, d2);
+    k_dd_scal<<<1, 32, 0, st>>>(sc, DD_INIT_NORMS, dp<dd>(d1), dp<dd>(d2));
+    dd_apply_precon(S, P, r.hi(), r.lo(), s.hi(), s.lo(), st);
+    dot(s, r, d1);
+    k_dd_scal<<<1, 32, 0, st>>>(sc, DD_INIT_RHO, dp<dd>(d1), nullptr);
+    PB_CUDA(cudaGetLastError());
+    const double setup_end = now_s();
+    DdScal h;
+    PB_CUDA(cudaMemcpyAsync(&h, sc, sizeof(DdScal), cudaMemcpyDeviceToHost, st));
+    sync();
+    const double bnorm = h.bnorm.hi;
+    double rnorm = h.rnorm.hi;
+    int itr;
+    for (itr = 1; itr <= o.itrmax; ++itr) {
+      if (reshistory) reshistory[itr - 1] = rnorm / bnorm;
+      k_dd_cg_axpy2<<<g, kDdThreads, 0, st>>>(n, sc, x.hi(), x.lo(), p.hi(), p.lo(), s.hi(), s.lo());
+      spmv(p, q);
+      dot(p, q, d1);
+      k_dd_scal<<<1, 32, 0, st>>>(sc, DD_ALPHA, dp<dd>(d1), nullptr);
+      k_dd_axpy<<<g, kDdThreads, 0, st>>>(n, &sc->t1, dcst + 0, q.hi(), q.lo(), r.hi(), r.lo());
+      dd_apply_precon(S, P, r.hi(), r.lo(), s.hi(), s.lo(), st);
+      dot(s, r, d1);
+      dot(r, r, d2);
+      k_dd_scal<<<1, 32, 0, st>>>(sc, DD_RNORM, dp<dd>(d1), dp<dd>(d2));
+      PB_CUDA(cudaGetLastError());
+      double rn;
+      PB_CUDA(cudaMemcpyAsync(&rn, &sc->rnorm.hi, sizeof(double), cudaMemcpyDeviceToHost, st));
+      sync();
+      rnorm = rn;
+      if (rnorm / bnorm < o.rtol) break;
+      k_dd_scal<<<1, 32, 0, st>>>(sc, DD_BETA, nullptr, nullptr);
+    }
+    // x = alpha p + 1 x
+    k_dd_axpy<<<g, kDdThreads, 0, st>>>(n, &sc->alpha, dcst + 0, p.hi(), p.lo(), x.hi(), x.lo());
+    PB_CUDA(cudaGetLastError());
+    used = std::min(o.itrmax, itr);
+    ir = (o.itrmax <= itr) ? 1 : 0;
+    auto store = [&](double* dst, const double* src) {
+      if (is_device_ptr(dst)) PB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      else PB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    };
+    store(x_hi, x.hi());
+    if (precision_x == 2 && x_lo) store(x_lo, x.lo());
+    sync();
+    parcel_b_stats stt;
+    memset(&stt, 0, sizeof(stt));
+    stt.setup_s = setup_end - t0;
+    stt.solve_s = now_s() - setup_end;
+    stt.ilu_nblocks = P.nb;
+    set_stats(stt);
+    return 0;
+  });
+  if (niter) *niter = rc == 0 ? used : 0;
+  if (iret) *iret = rc == 0 ? ir : rc;
+  return rc;
+}
+
+extern "C" void parcel_ddcg_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo,
+                               int32_t* n, int32_t* gn, int32_t* nnz, int32_t* istart, double* crsa,
+                               double* crsa_lo, int32_t* crsrow_ptr, int32_t* crscol, int* ipreflag,
+                               int* ilu_method, int* addl, int* iflagas, int* niter, double* rtolmax,
+                               double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                               int* independ_nvec, int* nblock, int* precision_a, int* precision_b,
+                               int* precision_x, int* precision_precondition, int* iret) {
+  (void)icomm;
+  parcel_b_input p;
+  parcel_b_input_init(&p);
+  p.solver = PARCEL_B_SOLVER_CG;
+  p.ipreflag = *ipreflag;
+  p.ILU_method = *ilu_method;
+  p.addL = *addl;
+  p.iflagAS = *iflagas;
+  p.itrmax = *niter;
+  p.rtolmax = *rtolmax;
+  p.abstolmax = 0.0;
+  p.iovlflag = *iovlflag;
+  p.precon_thblock = *precon_thblock;
+  p.Neuman_itr = *neuman_itr;
+  p.independ_nvec = *independ_nvec;
+  p.nBlock = *nblock;
+  parcel_b_crs A;
+  A.n = *n; A.gn = *gn; A.nnz = *nnz; A.istart = *istart;
+  A.rowptr = crsrow_ptr; A.col = crscol; A.val = crsa;
+  int used = 0, ir = 0;
+  parcel_b_ddcg(&p, &A, crsa_lo, *precision_a, *precision_b, *precision_x, *precision_precondition, vecb,
+                vecb_lo, vecx, vecx_lo, reshistory, &used, &ir);
+  *niter = used;
+  *iret = ir;
+}

@@ -152,4 +152,45 @@ __device__ __forceinline__ dd dd_mul(dd a, dd b) {
   return dd{s1, t1l};
 }
 
+// dd_div (dd_func.f90:99-142): q1 = a.hi / b.hi, the product b * q1 formed exactly with
+// the Dekker split, one correction q2 = (a - b q1) / b.hi, renormalised.
+__device__ __forceinline__ dd dd_div(dd a, dd b) {
+  const double q1 = __ddiv_rn(a.hi, b.hi);
+  double t1h = __dmul_rn(b.hi, q1);
+  double u1 = __dmul_rn(134217729.0, b.hi);
+  const double p1 = __dsub_rn(u1, __dsub_rn(u1, b.hi));
+  const double p2 = __dsub_rn(b.hi, p1);
+  u1 = __dmul_rn(134217729.0, q1);
+  double r1 = __dsub_rn(u1, __dsub_rn(u1, q1));
+  const double r2 = __dsub_rn(q1, r1);
+  double t1l = __dadd_rn(__dadd_rn(__dadd_rn(__dsub_rn(__dmul_rn(p1, r1), t1h), __dmul_rn(p1, r2)),
+                                   __dmul_rn(p2, r1)),
+                         __dmul_rn(p2, r2));
+  t1l = __dadd_rn(t1l, __dmul_rn(b.lo, q1));
+  double s1 = __dadd_rn(t1h, t1l);
+  t1l = __dsub_rn(t1l, __dsub_rn(s1, t1h));
+  t1h = s1;
+  s1 = __dsub_rn(a.hi, t1h);
+  r1 = __dsub_rn(s1, a.hi);
+  double s2 = __dsub_rn(__dsub_rn(a.hi, __dsub_rn(s1, r1)), __dadd_rn(t1h, r1));
+  s2 = __dsub_rn(s2, t1l);
+  s2 = __dadd_rn(s2, a.lo);
+  const double q2 = __ddiv_rn(__dadd_rn(s1, s2), b.hi);
+  const double h = __dadd_rn(q1, q2);
+  return dd{h, __dsub_rn(q2, __dsub_rn(h, q1))};
+}
+
+// dd_sqrt (dd_func.f90:143-239): x = 1 / sqrt(a.hi), then one correction in dd.  A zero
+// argument falls through to the general formula as in the reference; a negative one gives 0.
+__device__ __forceinline__ dd dd_sqrt(dd a) {
+  if (a.hi < 0.0 || (a.hi == 0.0 && a.lo < 0.0)) return dd{0.0, 0.0};
+  const double x = __ddiv_rn(1.0, __dsqrt_rn(a.hi));
+  const double ax = __dmul_rn(a.hi, x);
+  const dd y = dd_mul(dd{x, 0.0}, dd{0.5, 0.0});
+  const dd z = dd_mul(dd{ax, 0.0}, dd{ax, 0.0});
+  const dd t2 = dd_sub(a, z);
+  const dd t1 = dd_mul(t2, y);
+  return dd_add(t1, dd{ax, 0.0});
+}
+
 }  // namespace pb

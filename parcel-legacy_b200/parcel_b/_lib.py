@@ -95,6 +95,10 @@ SIGNATURES = {
     "parcel_b_dot": (C.c_int, [C.c_int64, P, P, DP]),
     "parcel_b_dot_noalloc": (C.c_int, [C.c_int64, P, P, P, P]),
     "parcel_b_residual_dd": (C.c_int, [C.POINTER(Crs), P, P, P, P, P, P]),
+    "parcel_b_ddcg": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), P, C.c_int, C.c_int, C.c_int, C.c_int, P, P,
+                                P, P, P, IP, IP]),
+    "parcel_ddcg_c_": (None, [IP, P, P, P, P, I32P, I32P, I32P, I32P, P, P, P, P, IP, IP, IP, IP, IP, DP, P, IP,
+                              IP, IP, IP, IP, IP, IP, IP, IP, IP]),
     "parcel_b_bench_kernels": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, DP, DP]),
     "parcel_b_learned_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(P)]),
     "parcel_b_learned_destroy": (C.c_int, [P]),

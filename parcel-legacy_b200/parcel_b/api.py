@@ -170,6 +170,38 @@ def solve(A, b, x0=None, *, rowptr=None, col=None, val=None, **options):
             "stats": _lib.last_stats()}
 
 
+def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=None, rowptr=None, col=None, val=None,
+         precision_A=2, precision_b=2, precision_x=2, precision_precondition=2, **options):
+    """PARCEL_ddKSP_CRS with the CG solver: the double-double PCG on the GPU.  Vectors and the
+    matrix's low parts as numpy arrays (host) or CUDA tensors (device).  Returns a dict with
+    x_hi, x_lo, reshistory, niter, iret and the library's statistics."""
+    L = load()
+    p = new_input(**options)
+    S = crs_struct(A, rowptr, col, val)
+    on_dev = hasattr(b_hi, "is_cuda") and b_hi.is_cuda
+
+    def fresh(v):
+        if v is not None:
+            return v.clone() if on_dev else np.array(v, dtype=np.float64, copy=True)
+        if on_dev:
+            import torch
+            return torch.zeros_like(b_hi)
+        return np.zeros(A.n)
+
+    xh, xl = fresh(x0_hi), fresh(x0_lo)
+    itrmax = p.itrmax if p.itrmax > 0 else 100
+    hist = np.zeros(itrmax)
+    niter, iret = C.c_int(0), C.c_int(0)
+    opt = lambda v: None if v is None else _ptr(v)
+    rc = L.parcel_b_ddcg(C.byref(p), C.byref(S), opt(val_lo), precision_A, precision_b, precision_x,
+                         precision_precondition, _ptr(b_hi), opt(b_lo), _ptr(xh), _ptr(xl), _ptr(hist),
+                         C.byref(niter), C.byref(iret))
+    if rc < 0:
+        raise RuntimeError(f"parcel_b_ddcg failed: {_lib.last_error()}")
+    return {"x_hi": xh, "x_lo": xl, "reshistory": hist[: niter.value].copy(), "niter": niter.value,
+            "iret": iret.value, "stats": _lib.last_stats()}
+
+
 class Learned:
     """The learned coarse-grid preconditioner stage (no counterpart in the reference): a
     handle on the network for an nx x ny x nz grid coarsened by ``coarsen``."""
