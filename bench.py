@@ -431,6 +431,93 @@ def run_vardiff(args):
     print(json.dumps(out))
 
 
+DD_METRIC = "time to 1e-9 recursive rel. residual (s), double-double PCG + block-Jacobi D-ILU"
+
+
+def run_ddcg(args):
+    """The reference's double-double CG configuration (template_cpu/STDOUT_run_dd): 160^3
+    Poisson of src/example/problem.f90, CG with block-Jacobi D-ILU (ILUD), 80 blocks, every
+    PRECISION_* = 2, rtol 1e-9, x0 = 0.  value: the whole parcel_b_ddcg call with the
+    arrays in HBM (CUDA events on the library stream); e2e: parcel_ddcg_c_ with host arrays
+    (copies in and out inside the timed region); cpu_baseline: the oracle's C++/OpenMP
+    restatement of ddKSP_pCG, one full solve.  The reference's own CPU run printed a CRS
+    solve time of 3.79 s with 4 MPI ranks x 20 OpenMP threads on its authors' machine."""
+    import torch
+    from parcel_b import _lib, api, problems
+    L = _lib.load()
+    A, b, xe = problems.poisson3d_reference(160, 160, 160)
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    rp, ci, va, bd = t(A.rowptr), t(A.col), t(A.val), t(b)
+    stream = torch.cuda.ExternalStream(L.parcel_b_get_stream(), device=dev)
+    kw = dict(itrmax=2000, rtolmax=1e-9, ipreflag=2, ILU_method=1, precon_thblock=80)
+
+    def solve_dev():
+        return api.ddcg(A, bd, rowptr=rp, col=ci, val=va, **kw)
+
+    for _ in range(args.warmup):
+        res = solve_dev()
+    torch.cuda.synchronize()
+    clk = Clocks(0)
+    clk.started()
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = solve_dev()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    clocks = clk.stop()
+    x = res["x_hi"].cpu().numpy() + res["x_lo"].cpu().numpy()
+    err = float(np.abs(x - xe).max())
+    # end to end through the reference-ordered C shim with pinned host arrays
+    hp = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    h_rp, h_ci, h_va, h_b = hp(A.rowptr), hp(A.col), hp(A.val), hp(b)
+    zeros = lambda m: torch.zeros(m, dtype=torch.float64).pin_memory().numpy()
+    h_x, h_xl, h_bl, h_al = zeros(A.n), zeros(A.n), zeros(A.n), zeros(A.nnz)
+    hist = np.zeros(2000)
+    I = lambda v: C.byref(C.c_int(v))
+    i32 = lambda v: C.byref(C.c_int32(v))
+    ptr = lambda a: a.ctypes.data
+
+    def solve_host():
+        h_x[:] = 0.0
+        h_xl[:] = 0.0
+        niter, iret = C.c_int(2000), C.c_int(0)
+        L.parcel_ddcg_c_(I(0), ptr(h_x), ptr(h_xl), ptr(h_b), ptr(h_bl), i32(A.n), i32(A.n), i32(A.nnz), i32(1),
+                         ptr(h_va), ptr(h_al), ptr(h_rp), ptr(h_ci), I(2), I(1), I(0), I(1), C.byref(niter),
+                         C.byref(C.c_double(1e-9)), ptr(hist), I(0), I(80), I(1), I(1), I(2000), I(2), I(2), I(2),
+                         I(2), C.byref(iret))
+        return niter.value, iret.value
+
+    solve_host()
+    e2e = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        solve_host()
+        e2e.append(time.perf_counter() - t0)
+    out = {"metric": DD_METRIC, "value": sum(times) / len(times), "unit": "s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "double-double (pairs of f64)", "data": "synthetic",
+           "config": {"workload": "CG + block-Jacobi D-ILU (ILUD), 80 blocks, 160^3 Poisson (problem.f90), "
+                                  "PRECISION_A/b/x/PRECONDITION = 2, rtol 1e-9",
+                      "n": A.n, "nnz": A.nnz, "l2": "inputs larger than L2 (dd vectors 65 MB each + matrix)"},
+           "iterations": res["niter"], "iret": res["iret"], "max_abs_err": err,
+           "step_times_s": [round(v, 6) for v in times],
+           "e2e": {"value": sum(e2e) / len(e2e), "unit": "s",
+                   "h2d_bytes_per_step": int(A.rowptr.nbytes + A.col.nbytes + 2 * A.val.nbytes + 4 * A.n * 8),
+                   "d2h_bytes_per_step": int(2 * A.n * 8 + res["niter"] * 8)},
+           "reference_printed_solve_s": 3.79280038102297, "clocks": clocks}
+    if not args.no_cpu_baseline:
+        import oracle
+        t0 = time.perf_counter()
+        _, _, h, niter, iret = oracle.ddcg(A, b, **kw)
+        out["cpu_baseline"] = {"value": time.perf_counter() - t0, "unit": "s", "cores": oracle.num_threads(),
+                               "kind": "port", "sample": f"one full oracle solve ({niter} iterations, iret {iret})"}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -440,8 +527,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels-only", action="store_true")
     ap.add_argument("--ilu-method", type=int, default=0)
-    ap.add_argument("--workload", default="convdiff128", choices=["convdiff128", "vardiff"],
-                    help="vardiff: the learned-preconditioner comparison (not the default line)")
+    ap.add_argument("--workload", default="convdiff128", choices=["convdiff128", "vardiff", "ddcg160"],
+                    help="vardiff: the learned-preconditioner comparison; ddcg160: the double-double CG "
+                         "configuration of the reference's dd example (neither is the default line)")
     ap.add_argument("--grid", type=int, default=256)
     ap.add_argument("--coarsen", type=int, default=8)
     ap.add_argument("--restart", type=int, default=40)
@@ -452,6 +540,8 @@ def main():
     args = ap.parse_args()
     if args.workload == "vardiff":
         run_vardiff(args)
+    elif args.workload == "ddcg160":
+        run_ddcg(args)
     elif args.kernels_only:
         run_kernels_only(args)
     elif args.impl == "reference":

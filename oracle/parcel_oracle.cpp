@@ -662,22 +662,31 @@ DD dd_sqrt(DD a) {
   return dd_add(t1, DD{ax, 0.0});
 }
 
-// dd dot: DD_NCHUNK contiguous chunks, each summed in index order, then the chunk sums
-// in chunk order (fixed, independent of the thread count; the reference's blocked
-// accumulators, ddvec.f90:111-240, follow its OpenMP split instead).
-constexpr int DD_NCHUNK = 1024;
+// dd dot in a fixed order, independent of the thread count (the reference's blocked
+// accumulators, ddvec.f90:111-240, follow its OpenMP split instead): nc = min(32768, n)
+// contiguous chunks, each summed in index order; the chunk sums in ng = min(256, nc)
+// contiguous groups, each summed in chunk order; the group sums in order.  Each sum
+// starts from 0 and adds with dd_add(sum, term).
+constexpr long DD_NCHUNK = 32768, DD_NGROUP = 256;
 DD dd_dot(long n, const double* xh, const double* xl, const double* yh, const double* yl) {
-  DD part[DD_NCHUNK];
-  long nch = std::min<long>(DD_NCHUNK, std::max<long>(1, n));
+  const long nc = std::min<long>(DD_NCHUNK, std::max<long>(1, n));
+  const long ng = std::min<long>(DD_NGROUP, nc);
+  std::vector<DD> part(nc), grp(ng);
 #pragma omp parallel for schedule(static)
-  for (long c = 0; c < nch; ++c) {
-    long lo = n * c / nch, hi = n * (c + 1) / nch;
+  for (long c = 0; c < nc; ++c) {
+    const long lo = n * c / nc, hi = n * (c + 1) / nc;
     DD s{0.0, 0.0};
     for (long i = lo; i < hi; ++i) s = dd_add(s, dd_mul(DD{xh[i], xl[i]}, DD{yh[i], yl[i]}));
     part[c] = s;
   }
+  for (long g = 0; g < ng; ++g) {
+    const long lo = nc * g / ng, hi = nc * (g + 1) / ng;
+    DD s{0.0, 0.0};
+    for (long c = lo; c < hi; ++c) s = dd_add(s, part[c]);
+    grp[g] = s;
+  }
   DD s{0.0, 0.0};
-  for (long c = 0; c < nch; ++c) s = dd_add(s, part[c]);
+  for (long g = 0; g < ng; ++g) s = dd_add(s, grp[g]);
   return s;
 }
 

@@ -8,8 +8,8 @@
 // Every dd operation is the reference's sequence of explicitly rounded double operations
 // (pb_device.cuh), every per-row loop runs in the reference's order (the CRS order for the
 // SpMV, L start..end and U start down to end for the D-ILU sweeps, the D-ILU diagonal
-// recurrence of ddDILU_DInv_crs), and the dot products sum a fixed split of the index
-// range (1,024 contiguous chunks, each in index order, then the chunk sums in order), so
+// recurrence of ddDILU_DInv_crs), and the dot products sum in a fixed order (32,768
+// contiguous chunks in index order, their sums in 256 groups, the group sums in order), so
 // the solve is bit-for-bit reproducible and identical to the CPU oracle's restatement.
 // The D-ILU rows run level by level on the wavefront plan of the FP64 block-Jacobi path;
 // the level order changes no row's arithmetic.
@@ -24,7 +24,8 @@ namespace pb {
 
 namespace {
 
-constexpr int kDdChunks = 1024;   // dot-product split (shared with the oracle)
+constexpr int kDdChunks = 32768;   // dot-product split (the oracle uses the same order)
+constexpr int kDdGroups = 256;
 constexpr int kDdThreads = 256;
 
 #define GRID_LOOP(i, n) \
@@ -85,7 +86,8 @@ __global__ void k_dd_cg_axpy2(int n, const DdScal* sc, double* __restrict__ xh, 
   }
 }
 
-// Dot product, first stage: chunk c of kDdChunks (contiguous, index order).
+// Dot product in a fixed order: nc = min(32768, n) contiguous chunks in index order, their
+// sums in ng = min(256, nc) contiguous groups in chunk order, the group sums in order.
 __global__ void k_dd_dot_chunks(int64_t n, int nch, const double* __restrict__ xh, const double* __restrict__ xl,
                                 const double* __restrict__ yh, const double* __restrict__ yl, dd* part) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -96,11 +98,19 @@ __global__ void k_dd_dot_chunks(int64_t n, int nch, const double* __restrict__ x
   part[c] = s;
 }
 
-// Second stage: the chunk sums in chunk order, into *out.
-__global__ void k_dd_dot_final(int nch, const dd* part, dd* out) {
+__global__ void k_dd_dot_groups(int nch, int ngr, const dd* part, dd* grp) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngr) return;
+  const int lo = (int)((int64_t)nch * g / ngr), hi = (int)((int64_t)nch * (g + 1) / ngr);
+  dd s{0.0, 0.0};
+  for (int c = lo; c < hi; ++c) s = dd_add(s, part[c]);
+  grp[g] = s;
+}
+
+__global__ void k_dd_dot_final(int ngr, const dd* grp, dd* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   dd s{0.0, 0.0};
-  for (int c = 0; c < nch; ++c) s = dd_add(s, part[c]);
+  for (int g = 0; g < ngr; ++g) s = dd_add(s, grp[g]);
   *out = s;
 }
 
@@ -344,8 +354,10 @@ struct DdSystem {
 void dd_dot(const DdSystem& S, const double* xh, const double* xl, const double* yh, const double* yl, dd* part,
             dd* out, cudaStream_t st) {
   const int nch = (int)std::min<int64_t>(kDdChunks, std::max(1, S.n));
+  const int ngr = std::min(kDdGroups, nch);
   k_dd_dot_chunks<<<(nch + 255) / 256, 256, 0, st>>>(S.n, nch, xh, xl, yh, yl, part);
-  k_dd_dot_final<<<1, 32, 0, st>>>(nch, part, out);
+  k_dd_dot_groups<<<(ngr + 255) / 256, 256, 0, st>>>(nch, ngr, part, part + kDdChunks);
+  k_dd_dot_final<<<1, 32, 0, st>>>(ngr, part + kDdChunks, out);
 }
 
 void dd_setup_precon(const Options& o, const parcel_b_crs& A, const DdSystem& S, int prec_M, DdPrecon& P) {
@@ -472,7 +484,8 @@ extern "C" int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, c
     };
     load(x, x_hi, x_lo, precision_x == 2);
     load(b, b_hi, b_lo, precision_b == 2);
-    DBuf scal(sizeof(DdScal)), part(sizeof(dd) * kDdChunks), d1(sizeof(dd)), d2(sizeof(dd)), cst(sizeof(dd) * 4);
+    DBuf scal(sizeof(DdScal)), part(sizeof(dd) * (kDdChunks + kDdGroups)), d1(sizeof(dd)), d2(sizeof(dd)),
+        cst(sizeof(dd) * 4);
     DdScal* sc = dp<DdScal>(scal);
     dd* dcst = dp<dd>(cst);   // 1, -1, 0, (unused)
     {
