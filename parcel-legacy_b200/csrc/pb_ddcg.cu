@@ -263,48 +263,203 @@ __global__ void k_dd_dilu_diag(const IluChunk* __restrict__ ch, const int* __res
 // forward levels in order then the backward levels in reverse:
 //   forward  z = r_k - sum_{j=Ls..Le} s_c a_j,  s_k = z D^-1
 //   backward z = sum_{j=Us..Ue, descending} s_c a_j,  s_k = s_k - D^-1 z
-// Precision 1 drops the low parts of A and of D^-1.
-__global__ void k_dd_dilu_sweep(const IluChunk* __restrict__ ch, const int* __restrict__ blk_chunk,
-                                const int* __restrict__ rowAt, const int4* __restrict__ rng,
-                                const int* __restrict__ ci, const double* __restrict__ ah,
-                                const double* __restrict__ al, int cbase, const double* __restrict__ dih,
-                                const double* __restrict__ dil, int prec, const double* __restrict__ rh,
-                                const double* __restrict__ rl, double* sh, double* sl) {
+// Precision 1 drops the low parts of A and of D^-1 (baked into the row records).
+//
+// Each row's data sits in level order (position q of the wavefront layout): its natural
+// index, its first kPre couplings (column and value) in the loop order above, its
+// coupling count and first position (for couplings past kPre, read from the CRS), its
+// D^-1, and its input (r for the forward sweep; the forward result, written in level order
+// as well, for the backward sweep).  So everything a level needs except the values s_c of
+// the rows it depends on is read by position, independent of earlier levels, and the next
+// level's part is loaded before the current level's barrier: after the barrier only the
+// gathers of s_c, the dd chain and the stores remain.
+constexpr int kPre = 3;       // couplings per row held in the records
+constexpr int kRowsPer = 2;   // rows per thread staged ahead (levels of up to 512 rows)
+
+struct DdRecords {
+  int np = 0;
+  const int* k;             // natural row at position q, -1 = padding
+  const int2* nj[2];        // [fwd, bwd]: (coupling count, first position)
+  const int* col[2];        // [dir][t * np + q]
+  const double* ah[2];
+  const double* al[2];
+  const double* dh;         // D^-1 at q (low part 0 under precision 1)
+  const double* dl;
+};
+
+__global__ void k_dd_records(int np, const int* __restrict__ rowAt, const int4* __restrict__ rng,
+                             const int* __restrict__ ci, const double* __restrict__ ah, const double* __restrict__ al,
+                             int cbase, const double* __restrict__ dih, const double* __restrict__ dil, int prec,
+                             int* rk, int2* nj0, int2* nj1, int* c0, int* c1, double* a0h, double* a0l, double* a1h,
+                             double* a1l, double* rdh, double* rdl) {
+  GRID_LOOP(q, np) {
+    const int k = rowAt[q];
+    rk[q] = k;
+    if (k < 0) {
+      nj0[q] = make_int2(0, 0);
+      nj1[q] = make_int2(0, 0);
+      rdh[q] = 0.0;
+      rdl[q] = 0.0;
+      continue;
+    }
+    const int4 r = rng[k];
+    const int nf = max(0, r.y - r.x + 1), nb = max(0, r.z - r.w + 1);
+    nj0[q] = make_int2(nf, r.x);
+    nj1[q] = make_int2(nb, r.z);
+    for (int t = 0; t < kPre; ++t) {
+      const int64_t o = (int64_t)t * np + q;
+      if (t < nf) {
+        const int j = r.x + t;
+        c0[o] = ci[j] - cbase;
+        a0h[o] = ah[j];
+        a0l[o] = (prec == 2 && al) ? al[j] : 0.0;
+      }
+      if (t < nb) {
+        const int j = r.z - t;
+        c1[o] = ci[j] - cbase;
+        a1h[o] = ah[j];
+        a1l[o] = (prec == 2 && al) ? al[j] : 0.0;
+      }
+    }
+    rdh[q] = dih[k];
+    rdl[q] = prec == 2 ? dil[k] : 0.0;
+  }
+}
+
+// r in level order (padding positions 0).
+__global__ void k_dd_gather(int np, const int* __restrict__ rk, const double* __restrict__ xh,
+                            const double* __restrict__ xl, double* __restrict__ qh, double* __restrict__ ql) {
+  GRID_LOOP(q, np) {
+    const int k = rk[q];
+    qh[q] = k >= 0 ? xh[k] : 0.0;
+    ql[q] = k >= 0 ? xl[k] : 0.0;
+  }
+}
+
+struct DdStage {
+  int k[kRowsPer], n[kRowsPer], j0[kRowsPer], q[kRowsPer];
+  int col[kRowsPer][kPre];
+  dd a[kRowsPer][kPre];
+  dd x[kRowsPer], di[kRowsPer];
+};
+
+template <int DIR>
+__device__ __forceinline__ void dd_stage(DdStage& S, const IluChunk& C, const DdRecords& R, const double* xh,
+                                         const double* xl) {
+#pragma unroll
+  for (int u = 0; u < kRowsPer; ++u) {
+    const int p = threadIdx.x + u * blockDim.x;
+    S.k[u] = -1;
+    if (p < C.w) {
+      const int q = C.start + p;
+      S.q[u] = q;
+      S.k[u] = R.k[q];
+      const int2 nj = R.nj[DIR][q];
+      S.n[u] = nj.x;
+      S.j0[u] = nj.y;
+#pragma unroll
+      for (int t = 0; t < kPre; ++t)
+        if (t < nj.x) {
+          const int64_t o = (int64_t)t * R.np + q;
+          S.col[u][t] = R.col[DIR][o];
+          S.a[u][t] = dd{R.ah[DIR][o], R.al[DIR][o]};
+        }
+      S.x[u] = dd{xh[q], xl[q]};
+      S.di[u] = dd{R.dh[q], R.dl[q]};
+    }
+  }
+}
+
+template <int DIR>
+__device__ __forceinline__ dd dd_row(int k, int n, int j0, const int* col, const dd* a, dd x, dd di,
+                                     const int* __restrict__ ci, const double* __restrict__ ah,
+                                     const double* __restrict__ al, int cbase, int prec, const double* sh,
+                                     const double* sl) {
+  dd z = DIR == 0 ? x : dd{0.0, 0.0};
+#pragma unroll
+  for (int t = 0; t < kPre; ++t)
+    if (t < n) {
+      const dd v = dd_mul(dd{sh[col[t]], sl[col[t]]}, a[t]);
+      z = DIR == 0 ? dd_sub(z, v) : dd_add(z, v);
+    }
+  for (int t = kPre; t < n; ++t) {   // couplings past the records, straight from the CRS
+    const int j = DIR == 0 ? j0 + t : j0 - t;
+    const int c = ci[j] - cbase;
+    const dd v = dd_mul(dd{sh[c], sl[c]}, dd{ah[j], (prec == 2 && al) ? al[j] : 0.0});
+    z = DIR == 0 ? dd_sub(z, v) : dd_add(z, v);
+  }
+  (void)k;
+  return DIR == 0 ? dd_mul(z, di) : dd_sub(x, dd_mul(di, z));
+}
+
+// The rows of one level: the staged ones, then any past kRowsPer per thread.
+template <int DIR>
+__device__ __forceinline__ void dd_level(const DdStage& S, const IluChunk& C, const DdRecords& R, const double* xh,
+                                         const double* xl, const int* __restrict__ ci, const double* __restrict__ ah,
+                                         const double* __restrict__ al, int cbase, int prec, double* sh, double* sl,
+                                         double* fqh, double* fql) {
+#pragma unroll
+  for (int u = 0; u < kRowsPer; ++u) {
+    const int k = S.k[u];
+    if (k < 0) continue;
+    const dd s = dd_row<DIR>(k, S.n[u], S.j0[u], S.col[u], S.a[u], S.x[u], S.di[u], ci, ah, al, cbase, prec, sh, sl);
+    sh[k] = s.hi;
+    sl[k] = s.lo;
+    if (DIR == 0) {
+      fqh[S.q[u]] = s.hi;
+      fql[S.q[u]] = s.lo;
+    }
+  }
+  for (int p = threadIdx.x + kRowsPer * blockDim.x; p < C.w; p += blockDim.x) {
+    const int q = C.start + p;
+    const int k = R.k[q];
+    const int2 nj = R.nj[DIR][q];
+    int col[kPre];
+    dd a[kPre];
+#pragma unroll
+    for (int t = 0; t < kPre; ++t)
+      if (t < nj.x) {
+        const int64_t o = (int64_t)t * R.np + q;
+        col[t] = R.col[DIR][o];
+        a[t] = dd{R.ah[DIR][o], R.al[DIR][o]};
+      }
+    const dd s = dd_row<DIR>(k, nj.x, nj.y, col, a, dd{xh[q], xl[q]}, dd{R.dh[q], R.dl[q]}, ci, ah, al, cbase, prec,
+                             sh, sl);
+    sh[k] = s.hi;
+    sl[k] = s.lo;
+    if (DIR == 0) {
+      fqh[q] = s.hi;
+      fql[q] = s.lo;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256, 1)
+    k_dd_dilu_sweep(const IluChunk* __restrict__ ch, const int* __restrict__ blk_chunk, DdRecords R,
+                    const int* __restrict__ ci, const double* __restrict__ ah, const double* __restrict__ al, int cbase,
+                    int prec, const double* __restrict__ rqh, const double* __restrict__ rql, double* fqh, double* fql,
+                    double* sh, double* sl) {
   const int b = blockIdx.x;
   const int c0 = blk_chunk[b], c1 = blk_chunk[b + 1];
-  auto av = [&](int j) { return dd{ah[j], (prec == 2 && al) ? al[j] : 0.0}; };
+  if (c1 <= c0) return;
+  DdStage A, B;
+  // forward: input r in level order; the results also go to level order for the backward
+  dd_stage<0>(A, ch[c0], R, rqh, rql);
   for (int c = c0; c < c1; ++c) {
     const IluChunk C = ch[c];
-    for (int p = threadIdx.x; p < C.w; p += blockDim.x) {
-      const int k = rowAt[C.start + p];
-      const int4 r = rng[k];
-      dd z{rh[k], rl[k]};
-      for (int j = r.x; j <= r.y; ++j) {
-        const int col = ci[j] - cbase;
-        z = dd_sub(z, dd_mul(dd{sh[col], sl[col]}, av(j)));
-      }
-      const dd s = dd_mul(z, dd{dih[k], prec == 2 ? dil[k] : 0.0});
-      sh[k] = s.hi;
-      sl[k] = s.lo;
-    }
+    if (c + 1 < c1) dd_stage<0>(B, ch[c + 1], R, rqh, rql);
+    dd_level<0>(A, C, R, rqh, rql, ci, ah, al, cbase, prec, sh, sl, fqh, fql);
     __syncthreads();
+    A = B;
   }
+  // backward: input the forward result (complete after the barrier above)
+  dd_stage<1>(A, ch[c1 - 1], R, fqh, fql);
   for (int c = c1 - 1; c >= c0; --c) {
     const IluChunk C = ch[c];
-    for (int p = threadIdx.x; p < C.w; p += blockDim.x) {
-      const int k = rowAt[C.start + p];
-      const int4 r = rng[k];
-      dd z{0.0, 0.0};
-      for (int j = r.z; j >= r.w; --j) {
-        const int col = ci[j] - cbase;
-        z = dd_add(z, dd_mul(dd{sh[col], sl[col]}, av(j)));
-      }
-      const dd t = dd_mul(dd{dih[k], prec == 2 ? dil[k] : 0.0}, z);
-      const dd s = dd_sub(dd{sh[k], sl[k]}, t);
-      sh[k] = s.hi;
-      sl[k] = s.lo;
-    }
+    if (c - 1 >= c0) dd_stage<1>(B, ch[c - 1], R, fqh, fql);
+    dd_level<1>(A, C, R, fqh, fql, ci, ah, al, cbase, prec, sh, sl, nullptr, nullptr);
     __syncthreads();
+    A = B;
   }
 }
 
@@ -327,7 +482,25 @@ struct DdPrecon {
   int prec = 2;
   DBuf dih, dil;                        // D^-1 (point Jacobi, D-ILU)
   DBuf chunks, blk_chunk, rowAt, rng;   // D-ILU level plan and row ranges
-  int nb = 0;
+  int nb = 0, np = 0;
+  DBuf rk, nj0, nj1, c0, c1, a0h, a0l, a1h, a1l, rdh, rdl;   // level-ordered row records
+  DBuf rqh, rql, fqh, fql;                                     // r and the forward result in level order
+  DdRecords rec() const {
+    DdRecords R;
+    R.np = np;
+    R.k = dp<int>(rk);
+    R.nj[0] = dp<int2>(nj0);
+    R.nj[1] = dp<int2>(nj1);
+    R.col[0] = dp<int>(c0);
+    R.col[1] = dp<int>(c1);
+    R.ah[0] = dp<double>(a0h);
+    R.al[0] = dp<double>(a0l);
+    R.ah[1] = dp<double>(a1h);
+    R.al[1] = dp<double>(a1l);
+    R.dh = dp<double>(rdh);
+    R.dl = dp<double>(rdl);
+    return R;
+  }
 };
 
 // Device copy of a natural-layout array given by host or device pointer (null stays null).
@@ -416,6 +589,22 @@ void dd_setup_precon(const Options& o, const parcel_b_crs& A, const DdSystem& S,
                                                  o.ilu_method == 2 ? 1 : 0, dp<double>(Dh), dp<double>(Dl),
                                                  dp<double>(P.dih), dp<double>(P.dil));
   PB_CUDA(cudaGetLastError());
+  const int np = plan.np;
+  P.np = np;
+  const size_t nq = (size_t)np, nt = (size_t)kPre * np;
+  P.rk.alloc(sizeof(int) * nq);
+  P.nj0.alloc(sizeof(int2) * nq);
+  P.nj1.alloc(sizeof(int2) * nq);
+  P.c0.alloc(sizeof(int) * nt);
+  P.c1.alloc(sizeof(int) * nt);
+  for (DBuf* d : {&P.a0h, &P.a0l, &P.a1h, &P.a1l}) d->alloc(sizeof(double) * nt);
+  for (DBuf* d : {&P.rdh, &P.rdl, &P.rqh, &P.rql, &P.fqh, &P.fql}) d->alloc(sizeof(double) * nq);
+  k_dd_records<<<grid_for(np), kDdThreads, 0, st>>>(np, dp<int>(P.rowAt), dp<int4>(P.rng), S.ci, S.ah, S.al, S.cbase,
+                                                     dp<double>(P.dih), dp<double>(P.dil), prec_M, dp<int>(P.rk),
+                                                     dp<int2>(P.nj0), dp<int2>(P.nj1), dp<int>(P.c0), dp<int>(P.c1),
+                                                     dp<double>(P.a0h), dp<double>(P.a0l), dp<double>(P.a1h),
+                                                     dp<double>(P.a1l), dp<double>(P.rdh), dp<double>(P.rdl));
+  PB_CUDA(cudaGetLastError());
   sync();   // the temporaries above are released on return
 }
 
@@ -430,9 +619,11 @@ void dd_apply_precon(const DdSystem& S, const DdPrecon& P, const double* rh, con
                                                           rl, sh, sl);
       break;
     default:
-      k_dd_dilu_sweep<<<P.nb, kDdThreads, 0, st>>>(dp<IluChunk>(P.chunks), dp<int>(P.blk_chunk), dp<int>(P.rowAt),
-                                                   dp<int4>(P.rng), S.ci, S.ah, S.al, S.cbase, dp<double>(P.dih),
-                                                   dp<double>(P.dil), P.prec, rh, rl, sh, sl);
+      k_dd_gather<<<grid_for(P.np), kDdThreads, 0, st>>>(P.np, dp<int>(P.rk), rh, rl, dp<double>(P.rqh),
+                                                          dp<double>(P.rql));
+      k_dd_dilu_sweep<<<P.nb, kDdThreads, 0, st>>>(dp<IluChunk>(P.chunks), dp<int>(P.blk_chunk), P.rec(), S.ci, S.ah,
+                                                   S.al, S.cbase, P.prec, dp<double>(P.rqh), dp<double>(P.rql),
+                                                   dp<double>(P.fqh), dp<double>(P.fql), sh, sl);
       break;
   }
 }
