@@ -210,6 +210,14 @@ void parcel_ddcg_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, dou
                     int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock,
                     int* precision_a, int* precision_b, int* precision_x, int* precision_precondition,
                     int* iret);
+/* parcel_ddbicgstab_c (src/example/c2fortran_kernel.f90:710-799): same argument list. */
+void parcel_ddbicgstab_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo, int32_t* n,
+                          int32_t* gn, int32_t* nnz, int32_t* istart, double* crsa, double* crsa_lo,
+                          int32_t* crsrow_ptr, int32_t* crscol, int* ipreflag, int* ilu_method, int* addl,
+                          int* iflagas, int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                          int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock,
+                          int* precision_a, int* precision_b, int* precision_x, int* precision_precondition,
+                          int* iret);
 void parcel_dcg_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn,
                        int32_t* nnz, int32_t* istart, void** crsa, void** crsrow_ptr,
                        void** crscol, int* ipreflag, int* ilu_method, int* addl,
@@ -291,6 +299,12 @@ int parcel_b_residual_dd(const parcel_b_crs* A, const double* x_hi, const double
 int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo, int precision_A,
                   int precision_b, int precision_x, int precision_precondition, const double* b_hi,
                   const double* b_lo, double* x_hi, double* x_lo, double* reshistory, int* niter, int* iret);
+/* Double-double BiCGStab (ddKSP_pBiCG, src/ddpbicg.f90:496-875), right-preconditioned,
+ * with the same arguments and preconditioners as parcel_b_ddcg; the history entry is the
+ * high part of the dd quotient rnorm / bnorm, as in the reference. */
+int parcel_b_ddbicgstab(const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo, int precision_A,
+                        int precision_b, int precision_x, int precision_precondition, const double* b_hi,
+                        const double* b_lo, double* x_hi, double* x_lo, double* reshistory, int* niter, int* iret);
 
 /* Kernel timing for benchmarks: builds the solver layout and preconditioner described by
  * prm (setup excluded from the timing), then launches `reps` back-to-back SpMVs and `reps`

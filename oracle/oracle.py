@@ -108,10 +108,11 @@ def solve(A, b, x0=None, **kw):
 
 
 def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, a_lo=None, prec_A=2, prec_b=2, prec_x=2, prec_M=2,
-         **kw):
-    """Double-double PCG (ddKSP_pCG); returns (x_hi, x_lo, reshistory[:niter], niter, iret)."""
+         solver=1, **kw):
+    """Double-double PCG (ddKSP_pCG, solver=1) or BiCGStab (ddKSP_pBiCG, solver=2); returns
+    (x_hi, x_lo, reshistory[:niter], niter, iret)."""
     M = A if isinstance(A, Matrix) else Matrix(A)
-    p = params(solver=1, **kw)
+    p = params(solver=solver, **kw)
     f = lambda v: None if v is None else np.ascontiguousarray(v, dtype=np.float64)
     bh, bl, alo = f(b_hi), f(b_lo), f(a_lo)
     xh = np.zeros(M.n) if x0_hi is None else np.array(x0_hi, dtype=np.float64, copy=True)

@@ -891,6 +891,70 @@ void ddpcg(const OrcMat& A, const double* alo, const DdPrecon& P, const OrcParam
   *iret = (prm.itrmax <= itr) ? 1 : 0;
 }
 
+// ddKSP_pBiCG (ddpbicg.f90:496-875): right-preconditioned BiCGStab in dd, with the vector
+// updates of ddBiCG_axpy3 / axpy4 / axpy3_dot / axpy4_ (ddpbicg.f90:8-326).  The history
+// entry is the high part of dd_div(rnorm, bnorm).
+void ddbicg(const OrcMat& A, const double* alo, const DdPrecon& P, const OrcParams& prm, const double* bh,
+            const double* bl, double* xh, double* xl, double* hist, int* niter, int* iret) {
+  const long n = A.n;
+  std::vector<double> rh(n), rl(n), r0h(n), r0l(n), ph(n), pl(n), pph(n), ppl(n), qh(n), ql(n), eh(n), el(n),
+      peh(n), pel(n), vh(n), vl(n);
+  dd_spmv(A, alo, xh, xl, rh.data(), rl.data());
+  dd_axpy(n, DD{1.0, 0.0}, DD{-1.0, 0.0}, bh, bl, rh.data(), rl.data());
+  r0h = rh; r0l = rl; ph = rh; pl = rl;
+  DD bnorm = dd_dot(n, bh, bl, bh, bl);
+  DD c1 = dd_dot(n, r0h.data(), r0l.data(), r0h.data(), r0l.data());
+  DD rnorm = c1;
+  bnorm = dd_sqrt(bnorm);
+  rnorm = dd_sqrt(rnorm);
+  DD c2{0.0, 0.0}, c3{0.0, 0.0};
+  int itr;
+  for (itr = 1; itr <= prm.itrmax; ++itr) {
+    hist[itr - 1] = dd_div(rnorm, bnorm).hi;
+    dd_apply_precon(A, alo, P, ph.data(), pl.data(), pph.data(), ppl.data());
+    dd_spmv(A, alo, pph.data(), ppl.data(), qh.data(), ql.data());
+    c2 = dd_dot(n, r0h.data(), r0l.data(), qh.data(), ql.data());
+    const DD alpha = dd_div(c1, c2);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {   // ddBiCG_axpy3: e = r - alpha q
+      DD e = dd_sub(DD{rh[i], rl[i]}, dd_mul(alpha, DD{qh[i], ql[i]}));
+      eh[i] = e.hi; el[i] = e.lo;
+    }
+    dd_apply_precon(A, alo, P, eh.data(), el.data(), peh.data(), pel.data());
+    dd_spmv(A, alo, peh.data(), pel.data(), vh.data(), vl.data());
+    const DD t1 = dd_dot(n, eh.data(), el.data(), vh.data(), vl.data());   // ddBiCG_calc_dot2
+    const DD t2 = dd_dot(n, vh.data(), vl.data(), vh.data(), vl.data());
+    c3 = dd_div(t1, t2);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {   // ddBiCG_axpy4: x = x + (alpha pp + c3 pe)
+      DD c = dd_mul(c3, DD{peh[i], pel[i]});
+      DD b = dd_mul(alpha, DD{pph[i], ppl[i]});
+      c = dd_add(b, c);
+      DD x = dd_add(DD{xh[i], xl[i]}, c);
+      xh[i] = x.hi; xl[i] = x.lo;
+    }
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {   // ddBiCG_axpy3_dot: r = e - c3 v
+      DD r = dd_sub(DD{eh[i], el[i]}, dd_mul(c3, DD{vh[i], vl[i]}));
+      rh[i] = r.hi; rl[i] = r.lo;
+    }
+    c1 = dd_dot(n, rh.data(), rl.data(), r0h.data(), r0l.data());
+    rnorm = dd_sqrt(dd_dot(n, rh.data(), rl.data(), rh.data(), rl.data()));
+    if (rnorm.hi / bnorm.hi < prm.rtolmax) break;
+    const DD beta = dd_div(c1, dd_mul(c3, c2));
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {   // ddBiCG_axpy4_: p = r + beta (p - c3 q)
+      DD c = dd_mul(c3, DD{qh[i], ql[i]});
+      c = dd_sub(DD{ph[i], pl[i]}, c);
+      c = dd_mul(beta, c);
+      DD pn = dd_add(DD{rh[i], rl[i]}, c);
+      ph[i] = pn.hi; pl[i] = pn.lo;
+    }
+  }
+  *niter = std::min(prm.itrmax, itr);
+  *iret = (prm.itrmax <= itr) ? 1 : 0;
+}
+
 // ---------------------------------------------------------------------------------
 // C entry points used by the tests and the CPU-baseline leg of bench.py.
 extern "C" {
@@ -972,7 +1036,8 @@ void orc_precon_apply_h(void* h, const double* r, double* s) {
 
 void orc_precon_destroy(void* h) { delete static_cast<Precon*>(h); }
 
-// ddKSP_pCG through PARCEL_ddKSP_CRS's precision flags (ddwrapper.f90:184-280):
+// ddKSP_pCG (prm->solver 1) or ddKSP_pBiCG (2) through PARCEL_ddKSP_CRS's precision flags
+// (ddwrapper.f90:184-280):
 // prec_A/b/x/M = 1 (double) or 2 (double-double).  A low parts (alo), b low parts and the
 // initial x low parts may be null.  ipreflag 0 / 1 / 2-3 (D-ILU, ILU_method 1 or 2).
 int orc_ddcg(const OrcMat* A, const double* alo, const OrcParams* prm, int prec_A, int prec_b, int prec_x,
@@ -997,7 +1062,10 @@ int orc_ddcg(const OrcMat* A, const double* alo, const OrcParams* prm, int prec_
   } else if (kind != ORC_PRECON_NONE) {
     return ORC_E_UNSUPPORTED;
   }
-  ddpcg(*A, a_lo, P, *prm, bh, bl0.data(), xh, xl0.data(), hist, niter, iret);
+  if (prm->solver == ORC_SOLVER_BICG)
+    ddbicg(*A, a_lo, P, *prm, bh, bl0.data(), xh, xl0.data(), hist, niter, iret);
+  else
+    ddpcg(*A, a_lo, P, *prm, bh, bl0.data(), xh, xl0.data(), hist, niter, iret);
   if (prec_x == 2 && xl) std::copy(xl0.begin(), xl0.end(), xl);
   return 0;
 }

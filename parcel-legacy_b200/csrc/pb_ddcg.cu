@@ -1,6 +1,8 @@
-// pb_ddcg.cu -- double-double preconditioned CG on the GPU (PARCEL_ddKSP_CRS, solver 1).
+// pb_ddcg.cu -- double-double preconditioned CG and BiCGStab on the GPU (PARCEL_ddKSP_CRS,
+// solvers 1 and 2).
 //
-// Reference: ddKSP_pCG (src/ddpcg.f90:247-563) with the precision flags of
+// Reference: ddKSP_pCG (src/ddpcg.f90:247-563) and ddKSP_pBiCG (src/ddpbicg.f90:496-875)
+// with the precision flags of
 // PARCEL_ddKSP_CRS (src/ddwrapper.f90:184-280): A, b, x and the preconditioner each in
 // double (1) or double-double (2).  The reference runs its dd solvers on the CPU only
 // (src/ddkrylov.f90:81,207); this is a GPU implementation of the same arithmetic.
@@ -142,6 +144,99 @@ __global__ void k_dd_scal(DdScal* sc, int step, const dd* bdot, const dd* rdot) 
       sc->beta = dd_div(sc->rho1, sc->rho0);
       sc->rho0 = sc->rho1;
       break;
+  }
+}
+
+// ------------------------------------------------------------------ BiCGStab (ddKSP_pBiCG)
+// Scalars of ddKSP_pBiCG (ddpbicg.f90:496-875); hist = high part of dd_div(rnorm, bnorm).
+struct DdScalB {
+  dd bnorm, rnorm, c1, c2, c3, alpha, beta;
+  double hist;
+};
+
+enum DdStepB { DDB_INIT = 0, DDB_ALPHA, DDB_C3, DDB_RNORM, DDB_BETA };
+
+__global__ void k_dd_scal_b(DdScalB* sc, int step, const dd* d1, const dd* d2) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  switch (step) {
+    case DDB_INIT:   // d1 = <b, b>, d2 = <r0, r0>
+      sc->bnorm = dd_sqrt(*d1);
+      sc->c1 = *d2;
+      sc->rnorm = dd_sqrt(sc->c1);
+      sc->hist = dd_div(sc->rnorm, sc->bnorm).hi;
+      sc->c2 = dd{0.0, 0.0};
+      sc->c3 = dd{0.0, 0.0};
+      break;
+    case DDB_ALPHA:   // d1 = <r0, q>
+      sc->c2 = *d1;
+      sc->alpha = dd_div(sc->c1, sc->c2);
+      break;
+    case DDB_C3:   // d1 = <e, v>, d2 = <v, v>
+      sc->c3 = dd_div(*d1, *d2);
+      break;
+    case DDB_RNORM:   // d1 = <r, r0>, d2 = <r, r>
+      sc->c1 = *d1;
+      sc->rnorm = dd_sqrt(*d2);
+      sc->hist = dd_div(sc->rnorm, sc->bnorm).hi;
+      break;
+    case DDB_BETA:
+      sc->beta = dd_div(sc->c1, dd_mul(sc->c3, sc->c2));
+      break;
+  }
+}
+
+// ddBiCG_axpy3 (ddpbicg.f90:8-43): e = r - alpha q
+__global__ void k_dd_bicg_axpy3(int n, const DdScalB* sc, const double* __restrict__ rh, const double* __restrict__ rl,
+                                const double* __restrict__ qh, const double* __restrict__ ql, double* __restrict__ eh,
+                                double* __restrict__ el) {
+  const dd a = sc->alpha;
+  GRID_LOOP(i, n) {
+    const dd e = dd_sub(dd{rh[i], rl[i]}, dd_mul(a, dd{qh[i], ql[i]}));
+    eh[i] = e.hi;
+    el[i] = e.lo;
+  }
+}
+
+// ddBiCG_axpy4 (ddpbicg.f90:282-326): x = x + (alpha pp + c3 pe)
+__global__ void k_dd_bicg_axpy4(int n, const DdScalB* sc, double* __restrict__ xh, double* __restrict__ xl,
+                                const double* __restrict__ pph, const double* __restrict__ ppl,
+                                const double* __restrict__ peh, const double* __restrict__ pel) {
+  const dd a = sc->alpha, c3 = sc->c3;
+  GRID_LOOP(i, n) {
+    dd c = dd_mul(c3, dd{peh[i], pel[i]});
+    const dd b = dd_mul(a, dd{pph[i], ppl[i]});
+    c = dd_add(b, c);
+    const dd x = dd_add(dd{xh[i], xl[i]}, c);
+    xh[i] = x.hi;
+    xl[i] = x.lo;
+  }
+}
+
+// ddBiCG_axpy3_dot's update (ddpbicg.f90:95-279): r = e - c3 v (its two dot products
+// follow as separate fixed-order dots)
+__global__ void k_dd_bicg_axpy3r(int n, const DdScalB* sc, const double* __restrict__ eh, const double* __restrict__ el,
+                                 const double* __restrict__ vh, const double* __restrict__ vl, double* __restrict__ rh,
+                                 double* __restrict__ rl) {
+  const dd c3 = sc->c3;
+  GRID_LOOP(i, n) {
+    const dd r = dd_sub(dd{eh[i], el[i]}, dd_mul(c3, dd{vh[i], vl[i]}));
+    rh[i] = r.hi;
+    rl[i] = r.lo;
+  }
+}
+
+// ddBiCG_axpy4_ (ddpbicg.f90:46-90): p = r + beta (p - c3 q)
+__global__ void k_dd_bicg_axpy4p(int n, const DdScalB* sc, double* __restrict__ ph, double* __restrict__ pl,
+                                 const double* __restrict__ rh, const double* __restrict__ rl,
+                                 const double* __restrict__ qh, const double* __restrict__ ql) {
+  const dd c3 = sc->c3, beta = sc->beta;
+  GRID_LOOP(i, n) {
+    dd c = dd_mul(c3, dd{qh[i], ql[i]});
+    c = dd_sub(dd{ph[i], pl[i]}, c);
+    c = dd_mul(beta, c);
+    const dd p = dd_add(dd{rh[i], rl[i]}, c);
+    ph[i] = p.hi;
+    pl[i] = p.lo;
   }
 }
 
@@ -634,10 +729,12 @@ void dd_apply_precon(const DdSystem& S, const DdPrecon& P, const double* rh, con
 
 using namespace pb;
 
-extern "C" int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo,
-                             int precision_A, int precision_b, int precision_x, int precision_precondition,
-                             const double* b_hi, const double* b_lo, double* x_hi, double* x_lo,
-                             double* reshistory, int* niter, int* iret) {
+namespace {
+
+// The dd Krylov solves of PARCEL_ddKSP_CRS: CG (ddKSP_pCG) or BiCGStab (ddKSP_pBiCG).
+int dd_krylov(int solver, const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo, int precision_A,
+              int precision_b, int precision_x, int precision_precondition, const double* b_hi, const double* b_lo,
+              double* x_hi, double* x_lo, double* reshistory, int* niter, int* iret) {
   int used = 0, ir = 0;
   const int rc = guarded([&]() -> int {
     ensure_init();
@@ -665,6 +762,7 @@ extern "C" int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, c
     dd_setup_precon(o, *A, S, precision_precondition, P);
     // vectors: x and b in dd, the low parts zero unless their precision is 2
     DdVec x(n), b(n), r(n), p(n), q(n), s(n);
+    const bool bicg = solver == PARCEL_B_SOLVER_BICG;
     auto load = [&](DdVec& v, const double* hi, const double* lo, bool use_lo) {
       if (is_device_ptr(hi)) PB_CUDA(cudaMemcpyAsync(v.hi(), hi, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
       else h2d(v.hi(), hi, sizeof(double) * n);
@@ -693,6 +791,9 @@ extern "C" int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, c
     // r = b - A x (ddcalc_res: r = A x, then r = 1 b + (-1) r)
     spmv(x, r);
     k_dd_axpy<<<g, kDdThreads, 0, st>>>(n, dcst + 0, dcst + 1, b.hi(), b.lo(), r.hi(), r.lo());
+    double setup_end = 0.0;
+    int itr = 1;
+    if (!bicg) {
     dot(b, b, d1);
     dot(r, r, d2);
     k_dd_scal<<<1, 32, 0, st>>>(sc, DD_INIT_NORMS, dp<dd>(d1), dp<dd>(d2));
@@ -700,13 +801,12 @@ extern "C" int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, c
     dot(s, r, d1);
     k_dd_scal<<<1, 32, 0, st>>>(sc, DD_INIT_RHO, dp<dd>(d1), nullptr);
     PB_CUDA(cudaGetLastError());
-    const double setup_end = now_s();
+    setup_end = now_s();
     DdScal h;
     PB_CUDA(cudaMemcpyAsync(&h, sc, sizeof(DdScal), cudaMemcpyDeviceToHost, st));
     sync();
     const double bnorm = h.bnorm.hi;
     double rnorm = h.rnorm.hi;
-    int itr;
     for (itr = 1; itr <= o.itrmax; ++itr) {
       if (reshistory) reshistory[itr - 1] = rnorm / bnorm;
       k_dd_cg_axpy2<<<g, kDdThreads, 0, st>>>(n, sc, x.hi(), x.lo(), p.hi(), p.lo(), s.hi(), s.lo());
@@ -729,6 +829,52 @@ extern "C" int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, c
     // x = alpha p + 1 x
     k_dd_axpy<<<g, kDdThreads, 0, st>>>(n, &sc->alpha, dcst + 0, p.hi(), p.lo(), x.hi(), x.lo());
     PB_CUDA(cudaGetLastError());
+    } else {
+    // ddKSP_pBiCG: r0 = p = r; c1 = <r0, r0>
+    DdVec r0(n), pp(n), e(n), pe(n), v(n);
+    DBuf scb(sizeof(DdScalB));
+    DdScalB* sb = dp<DdScalB>(scb);
+    k_dd_copy<<<g, kDdThreads, 0, st>>>(n, r.hi(), r.lo(), r0.hi(), r0.lo());
+    k_dd_copy<<<g, kDdThreads, 0, st>>>(n, r.hi(), r.lo(), p.hi(), p.lo());
+    dot(b, b, d1);
+    dot(r0, r0, d2);
+    k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_INIT, dp<dd>(d1), dp<dd>(d2));
+    PB_CUDA(cudaGetLastError());
+    setup_end = now_s();
+    DdScalB h;
+    PB_CUDA(cudaMemcpyAsync(&h, sb, sizeof(DdScalB), cudaMemcpyDeviceToHost, st));
+    sync();
+    const double bnorm = h.bnorm.hi;
+    double hist = h.hist;
+    for (itr = 1; itr <= o.itrmax; ++itr) {
+      if (reshistory) reshistory[itr - 1] = hist;
+      dd_apply_precon(S, P, p.hi(), p.lo(), pp.hi(), pp.lo(), st);
+      spmv(pp, q);
+      dot(r0, q, d1);
+      k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_ALPHA, dp<dd>(d1), nullptr);
+      k_dd_bicg_axpy3<<<g, kDdThreads, 0, st>>>(n, sb, r.hi(), r.lo(), q.hi(), q.lo(), e.hi(), e.lo());
+      dd_apply_precon(S, P, e.hi(), e.lo(), pe.hi(), pe.lo(), st);
+      spmv(pe, v);
+      dot(e, v, d1);
+      dot(v, v, d2);
+      k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_C3, dp<dd>(d1), dp<dd>(d2));
+      k_dd_bicg_axpy4<<<g, kDdThreads, 0, st>>>(n, sb, x.hi(), x.lo(), pp.hi(), pp.lo(), pe.hi(), pe.lo());
+      k_dd_bicg_axpy3r<<<g, kDdThreads, 0, st>>>(n, sb, e.hi(), e.lo(), v.hi(), v.lo(), r.hi(), r.lo());
+      dot(r, r0, d1);
+      dot(r, r, d2);
+      k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_RNORM, dp<dd>(d1), dp<dd>(d2));
+      PB_CUDA(cudaGetLastError());
+      double rn[2];
+      PB_CUDA(cudaMemcpyAsync(&rn[0], &sb->rnorm.hi, sizeof(double), cudaMemcpyDeviceToHost, st));
+      PB_CUDA(cudaMemcpyAsync(&rn[1], &sb->hist, sizeof(double), cudaMemcpyDeviceToHost, st));
+      sync();
+      hist = rn[1];
+      if (rn[0] / bnorm < o.rtol) break;
+      k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_BETA, nullptr, nullptr);
+      k_dd_bicg_axpy4p<<<g, kDdThreads, 0, st>>>(n, sb, p.hi(), p.lo(), r.hi(), r.lo(), q.hi(), q.lo());
+    }
+    PB_CUDA(cudaGetLastError());
+    }
     used = std::min(o.itrmax, itr);
     ir = (o.itrmax <= itr) ? 1 : 0;
     auto store = [&](double* dst, const double* src) {
@@ -751,17 +897,37 @@ extern "C" int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, c
   return rc;
 }
 
-extern "C" void parcel_ddcg_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo,
-                               int32_t* n, int32_t* gn, int32_t* nnz, int32_t* istart, double* crsa,
-                               double* crsa_lo, int32_t* crsrow_ptr, int32_t* crscol, int* ipreflag,
-                               int* ilu_method, int* addl, int* iflagas, int* niter, double* rtolmax,
-                               double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
-                               int* independ_nvec, int* nblock, int* precision_a, int* precision_b,
-                               int* precision_x, int* precision_precondition, int* iret) {
-  (void)icomm;
+}  // namespace
+
+extern "C" int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo,
+                             int precision_A, int precision_b, int precision_x, int precision_precondition,
+                             const double* b_hi, const double* b_lo, double* x_hi, double* x_lo,
+                             double* reshistory, int* niter, int* iret) {
+  return dd_krylov(PARCEL_B_SOLVER_CG, prm, A, val_lo, precision_A, precision_b, precision_x, precision_precondition,
+                   b_hi, b_lo, x_hi, x_lo, reshistory, niter, iret);
+}
+
+extern "C" int parcel_b_ddbicgstab(const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo,
+                                   int precision_A, int precision_b, int precision_x, int precision_precondition,
+                                   const double* b_hi, const double* b_lo, double* x_hi, double* x_lo,
+                                   double* reshistory, int* niter, int* iret) {
+  return dd_krylov(PARCEL_B_SOLVER_BICG, prm, A, val_lo, precision_A, precision_b, precision_x,
+                   precision_precondition, b_hi, b_lo, x_hi, x_lo, reshistory, niter, iret);
+}
+
+namespace {
+
+// parcel_dd*_c (src/example/c2fortran_kernel.f90:620-799): every argument by reference,
+// host arrays, niter in = itrmax and out = iterations.
+void dd_shim(int solver, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo, int32_t* n, int32_t* gn,
+             int32_t* nnz, int32_t* istart, double* crsa, double* crsa_lo, int32_t* crsrow_ptr, int32_t* crscol,
+             int* ipreflag, int* ilu_method, int* addl, int* iflagas, int* niter, double* rtolmax,
+             double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr, int* independ_nvec,
+             int* nblock, int* precision_a, int* precision_b, int* precision_x, int* precision_precondition,
+             int* iret) {
   parcel_b_input p;
   parcel_b_input_init(&p);
-  p.solver = PARCEL_B_SOLVER_CG;
+  p.solver = solver;
   p.ipreflag = *ipreflag;
   p.ILU_method = *ilu_method;
   p.addL = *addl;
@@ -778,8 +944,36 @@ extern "C" void parcel_ddcg_c_(int* icomm, double* vecx, double* vecx_lo, double
   A.n = *n; A.gn = *gn; A.nnz = *nnz; A.istart = *istart;
   A.rowptr = crsrow_ptr; A.col = crscol; A.val = crsa;
   int used = 0, ir = 0;
-  parcel_b_ddcg(&p, &A, crsa_lo, *precision_a, *precision_b, *precision_x, *precision_precondition, vecb,
-                vecb_lo, vecx, vecx_lo, reshistory, &used, &ir);
+  dd_krylov(solver, &p, &A, crsa_lo, *precision_a, *precision_b, *precision_x, *precision_precondition, vecb,
+            vecb_lo, vecx, vecx_lo, reshistory, &used, &ir);
   *niter = used;
   *iret = ir;
+}
+
+}  // namespace
+
+extern "C" void parcel_ddcg_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo,
+                               int32_t* n, int32_t* gn, int32_t* nnz, int32_t* istart, double* crsa,
+                               double* crsa_lo, int32_t* crsrow_ptr, int32_t* crscol, int* ipreflag,
+                               int* ilu_method, int* addl, int* iflagas, int* niter, double* rtolmax,
+                               double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                               int* independ_nvec, int* nblock, int* precision_a, int* precision_b,
+                               int* precision_x, int* precision_precondition, int* iret) {
+  (void)icomm;
+  dd_shim(PARCEL_B_SOLVER_CG, vecx, vecx_lo, vecb, vecb_lo, n, gn, nnz, istart, crsa, crsa_lo, crsrow_ptr, crscol,
+          ipreflag, ilu_method, addl, iflagas, niter, rtolmax, reshistory, iovlflag, precon_thblock, neuman_itr,
+          independ_nvec, nblock, precision_a, precision_b, precision_x, precision_precondition, iret);
+}
+
+extern "C" void parcel_ddbicgstab_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo,
+                                     int32_t* n, int32_t* gn, int32_t* nnz, int32_t* istart, double* crsa,
+                                     double* crsa_lo, int32_t* crsrow_ptr, int32_t* crscol, int* ipreflag,
+                                     int* ilu_method, int* addl, int* iflagas, int* niter, double* rtolmax,
+                                     double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                                     int* independ_nvec, int* nblock, int* precision_a, int* precision_b,
+                                     int* precision_x, int* precision_precondition, int* iret) {
+  (void)icomm;
+  dd_shim(PARCEL_B_SOLVER_BICG, vecx, vecx_lo, vecb, vecb_lo, n, gn, nnz, istart, crsa, crsa_lo, crsrow_ptr,
+          crscol, ipreflag, ilu_method, addl, iflagas, niter, rtolmax, reshistory, iovlflag, precon_thblock,
+          neuman_itr, independ_nvec, nblock, precision_a, precision_b, precision_x, precision_precondition, iret);
 }

@@ -170,12 +170,18 @@ def solve(A, b, x0=None, *, rowptr=None, col=None, val=None, **options):
             "stats": _lib.last_stats()}
 
 
+def ddbicgstab(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, **kw):
+    """The double-double BiCGStab (ddKSP_pBiCG); arguments and result as ddcg."""
+    return ddcg(A, b_hi, b_lo, x0_hi, x0_lo, solver=2, **kw)
+
+
 def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=None, rowptr=None, col=None, val=None,
-         precision_A=2, precision_b=2, precision_x=2, precision_precondition=2, **options):
-    """PARCEL_ddKSP_CRS with the CG solver: the double-double PCG on the GPU.  Vectors and the
-    matrix's low parts as numpy arrays (host) or CUDA tensors (device).  Returns a dict with
-    x_hi, x_lo, reshistory, niter, iret and the library's statistics."""
+         precision_A=2, precision_b=2, precision_x=2, precision_precondition=2, solver=1, **options):
+    """PARCEL_ddKSP_CRS: the double-double PCG (solver=1) or BiCGStab (solver=2) on the GPU.
+    Vectors and the matrix's low parts as numpy arrays (host) or CUDA tensors (device).
+    Returns a dict with x_hi, x_lo, reshistory, niter, iret and the library's statistics."""
     L = load()
+    fn = L.parcel_b_ddbicgstab if solver == 2 else L.parcel_b_ddcg
     p = new_input(**options)
     S = crs_struct(A, rowptr, col, val)
     on_dev = hasattr(b_hi, "is_cuda") and b_hi.is_cuda
@@ -193,11 +199,10 @@ def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=None, rowptr=None
     hist = np.zeros(itrmax)
     niter, iret = C.c_int(0), C.c_int(0)
     opt = lambda v: None if v is None else _ptr(v)
-    rc = L.parcel_b_ddcg(C.byref(p), C.byref(S), opt(val_lo), precision_A, precision_b, precision_x,
-                         precision_precondition, _ptr(b_hi), opt(b_lo), _ptr(xh), _ptr(xl), _ptr(hist),
-                         C.byref(niter), C.byref(iret))
+    rc = fn(C.byref(p), C.byref(S), opt(val_lo), precision_A, precision_b, precision_x, precision_precondition,
+            _ptr(b_hi), opt(b_lo), _ptr(xh), _ptr(xl), _ptr(hist), C.byref(niter), C.byref(iret))
     if rc < 0:
-        raise RuntimeError(f"parcel_b_ddcg failed: {_lib.last_error()}")
+        raise RuntimeError(f"dd solve failed: {_lib.last_error()}")
     return {"x_hi": xh, "x_lo": xl, "reshistory": hist[: niter.value].copy(), "niter": niter.value,
             "iret": iret.value, "stats": _lib.last_stats()}
 

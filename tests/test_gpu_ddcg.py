@@ -100,3 +100,49 @@ def test_ddcg_reproduces_reference_dd_output():
     assert (np.abs(g["reshistory"][:k] - ref[:k]) / ref[:k]).max() <= 1e-6
     err = np.abs(g["x_hi"] + g["x_lo"] - xe).max()
     assert abs(err - fx["abs_err"]) / fx["abs_err"] < 1e-3
+
+
+def _convdiff(g, seed):
+    from parcel_b import problems
+    A = problems.convdiff3d_upwind(g)
+    return A, problems.rhs_normal(A.n, seed)
+
+
+@pytest.mark.parametrize("case", CASES, ids=["dilu-ilud-8", "dilu-mlud-5", "point-jacobi", "none"])
+def test_ddbicgstab_matches_oracle_bit_for_bit(case):
+    """ddKSP_pBiCG on a nonsymmetric 3D convection-diffusion matrix."""
+    from parcel_b import api
+    A, b = _convdiff(20, 4)
+    kw = dict(itrmax=400, rtolmax=1e-12, **case)
+    g = api.ddbicgstab(A, b, **kw)
+    xh, xl, h, niter, iret = oracle.ddcg(A, b, solver=2, **kw)
+    assert g["iret"] == iret == 0
+    assert g["niter"] == niter
+    assert np.array_equal(g["reshistory"], h)
+    assert np.array_equal(g["x_hi"], xh) and np.array_equal(g["x_lo"], xl)
+
+
+def test_ddbicgstab_precision_flags_and_shim():
+    """Mixed precision flags, and parcel_ddbicgstab_c_ against the native entry."""
+    from parcel_b import _lib, api
+    A, b = _convdiff(16, 5)
+    alo, blo = _lo(A.val, 6), _lo(b, 7)
+    kw = dict(itrmax=300, rtolmax=1e-11, ipreflag=2, ILU_method=1, precon_thblock=4)
+    g = api.ddbicgstab(A, b, b_lo=blo, val_lo=alo, precision_A=2, precision_b=2, precision_x=2,
+                       precision_precondition=1, **kw)
+    xh, xl, h, niter, iret = oracle.ddcg(A, b, solver=2, b_lo=blo, a_lo=alo, prec_M=1, **kw)
+    assert g["niter"] == niter and np.array_equal(g["reshistory"], h)
+    assert np.array_equal(g["x_hi"], xh) and np.array_equal(g["x_lo"], xl)
+    n = A.n
+    x, xl2 = np.zeros(n), np.zeros(n)
+    hist = np.zeros(300)
+    I = lambda v: C.byref(C.c_int(v))
+    i32 = lambda v: C.byref(C.c_int32(v))
+    it, ir = C.c_int(300), C.c_int(0)
+    ptr = lambda a: a.ctypes.data
+    _lib.load().parcel_ddbicgstab_c_(I(0), ptr(x), ptr(xl2), ptr(b), ptr(blo), i32(n), i32(n), i32(A.nnz), i32(1),
+                                     ptr(A.val), ptr(alo), ptr(A.rowptr), ptr(A.col), I(2), I(1), I(0), I(1),
+                                     C.byref(it), C.byref(C.c_double(1e-11)), ptr(hist), I(0), I(4), I(1), I(1),
+                                     I(2000), I(2), I(2), I(2), I(1), C.byref(ir))
+    assert ir.value == 0 and it.value == niter
+    assert np.array_equal(x, xh) and np.array_equal(xl2, xl)
