@@ -218,6 +218,15 @@ void parcel_ddbicgstab_c_(int* icomm, double* vecx, double* vecx_lo, double* vec
                           int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock,
                           int* precision_a, int* precision_b, int* precision_x, int* precision_precondition,
                           int* iret);
+/* parcel_ddgmres_c (src/example/c2fortran_kernel.f90:801-898): the same list with the
+ * restart length and the Gram-Schmidt flag after nblock. */
+void parcel_ddgmres_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo, int32_t* n,
+                       int32_t* gn, int32_t* nnz, int32_t* istart, double* crsa, double* crsa_lo,
+                       int32_t* crsrow_ptr, int32_t* crscol, int* ipreflag, int* ilu_method, int* addl,
+                       int* iflagas, int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                       int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock, int* restart,
+                       int* gmres_gsflag, int* precision_a, int* precision_b, int* precision_x,
+                       int* precision_precondition, int* iret);
 void parcel_dcg_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn,
                        int32_t* nnz, int32_t* istart, void** crsa, void** crsrow_ptr,
                        void** crscol, int* ipreflag, int* ilu_method, int* addl,
@@ -305,6 +314,14 @@ int parcel_b_ddcg(const parcel_b_input* prm, const parcel_b_crs* A, const double
 int parcel_b_ddbicgstab(const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo, int precision_A,
                         int precision_b, int precision_x, int precision_precondition, const double* b_hi,
                         const double* b_lo, double* x_hi, double* x_lo, double* reshistory, int* niter, int* iret);
+/* Double-double GMRES(m) (ddKSP_pGMRES, src/ddpgmres.f90:254-713), right-preconditioned,
+ * with the same arguments and preconditioners as parcel_b_ddcg; the restart length is
+ * prm->GMRES_m and the orthogonalisation prm->GMRES_GSflag (MGS or CGS, as in
+ * ddQRDecomposition.f90:4-121).  niter and the history follow the reference: entry 1 is
+ * the starting residual and entry k + 1 the residual after iteration k. */
+int parcel_b_ddgmres(const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo, int precision_A,
+                     int precision_b, int precision_x, int precision_precondition, const double* b_hi,
+                     const double* b_lo, double* x_hi, double* x_lo, double* reshistory, int* niter, int* iret);
 
 /* Kernel timing for benchmarks: builds the solver layout and preconditioner described by
  * prm (setup excluded from the timing), then launches `reps` back-to-back SpMVs and `reps`

@@ -109,7 +109,8 @@ def solve(A, b, x0=None, **kw):
 
 def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, a_lo=None, prec_A=2, prec_b=2, prec_x=2, prec_M=2,
          solver=1, **kw):
-    """Double-double PCG (ddKSP_pCG, solver=1) or BiCGStab (ddKSP_pBiCG, solver=2); returns
+    """Double-double PCG (ddKSP_pCG, solver=1), BiCGStab (ddKSP_pBiCG, solver=2) or GMRES(m)
+    (ddKSP_pGMRES, solver=3, GMRES_m / GMRES_GSflag as for gmres); returns
     (x_hi, x_lo, reshistory[:niter], niter, iret)."""
     M = A if isinstance(A, Matrix) else Matrix(A)
     p = params(solver=solver, **kw)

@@ -566,7 +566,7 @@ void pgmres(const OrcMat& A, const Precon& P, const OrcParams& prm, const double
       givens(m, h.data(), inner, c.data(), s.data(), e.data());
       rnorm = std::fabs(e[inner]);
       mm = inner;
-      hist[itr + inner - 1] = rnorm / bnorm;
+      if (itr + inner <= prm.itrmax) hist[itr + inner - 1] = rnorm / bnorm;
       if (rnorm / bnorm < prm.rtolmax) { exit_inner = true; break; }
       if (itr + inner == prm.itrmax) { exit_inner = true; break; }
     }
@@ -955,6 +955,123 @@ void ddbicg(const OrcMat& A, const double* alo, const DdPrecon& P, const OrcPara
   *iret = (prm.itrmax <= itr) ? 1 : 0;
 }
 
+// ddGivensRotations (ddpgmres.f90:147-250) on column i (1-based) of the (m+1) x m
+// Hessenberg matrix h, with the reference's operand orders and its zero-diagonal guard
+// (divide by 1e-100).
+void dd_givens(int m, DD* h, int i, DD* c, DD* s, DD* e) {
+  DD* col = h + (long)(i - 1) * (m + 1);
+  for (int k = 1; k <= i - 1; ++k) {
+    const DD t1 = dd_sub(dd_mul(col[k - 1], c[k - 1]), dd_mul(col[k], s[k - 1]));
+    const DD t2 = dd_add(dd_mul(col[k - 1], s[k - 1]), dd_mul(col[k], c[k - 1]));
+    col[k - 1] = t1;
+    col[k] = t2;
+  }
+  const DD d = col[i - 1];
+  const DD t = (d.hi == 0.0 && d.lo == 0.0) ? dd_div(col[i], DD{1.0e-100, 0.0}) : dd_div(col[i], d);
+  const DD q = dd_sqrt(dd_add(DD{1.0, 0.0}, dd_mul(t, t)));
+  c[i - 1] = dd_div(DD{1.0, 0.0}, q);
+  s[i - 1] = dd_mul(DD{-1.0, 0.0}, dd_mul(c[i - 1], t));
+  const DD e1 = dd_sub(dd_mul(c[i - 1], e[i - 1]), dd_mul(s[i - 1], e[i]));
+  const DD e2 = dd_add(dd_mul(s[i - 1], e[i - 1]), dd_mul(c[i - 1], e[i]));
+  e[i - 1] = e1;
+  e[i] = e2;
+  col[i - 1] = dd_sub(dd_mul(c[i - 1], col[i - 1]), dd_mul(s[i - 1], col[i]));
+  col[i] = DD{0.0, 0.0};
+}
+
+// ddKSP_pGMRES (ddpgmres.f90:254-713): right-preconditioned GMRES(m) in dd.  MGS
+// (ddMGS_Orthonormalization, ddQRDecomposition.f90:4-47) projects w on v_1..v_{i-1} one
+// at a time with <w, v_k>; CGS (ddCGS_Orthonormalization, :49-121) takes <v_k, w> for all
+// k < i from the same w and then subtracts.  Both finish with <w, v_i>, w -= h_ii v_i and
+// h_{i+1,i} = sqrt(<w, w>).  The restart residual is tested only against abstolmax, which
+// parcel_ddgmres fixes at 0 (ddwrapper.f90:438), so that test never fires.  History
+// entries are rnorm.hi / bnorm.hi; the first cycle also stores its starting residual.
+// With itrmax = 1 the first cycle runs all m steps (the itr + inner == itrmax exit cannot
+// fire) and the reference writes their history past entry itrmax; here those entries are
+// dropped.  For itrmax > 1 an unconverged solve stops at itr + inner == itrmax with iret 0,
+// as in the reference.
+void ddgmres(const OrcMat& A, const double* alo, const DdPrecon& P, const OrcParams& prm, const double* bh,
+             const double* bl, double* xh, double* xl, double* hist, int* niter, int* iret) {
+  const long n = A.n;
+  const int m = prm.GMRES_m > 0 ? prm.GMRES_m : 4;
+  const int gs = prm.GMRES_GSflag > 0 ? prm.GMRES_GSflag : ORC_GS_MGS;
+  std::vector<double> rh(n), rl(n), Vh((long)(m + 1) * n, 0.0), Vl((long)(m + 1) * n, 0.0), pvh(n), pvl(n),
+      wh(n), wl(n), x0h(n), x0l(n), v0h(n), v0l(n);
+  std::vector<DD> h((long)(m + 1) * m), c(m + 1), s(m + 1), e(m + 1), y(m + 1);
+  const DD one{1.0, 0.0}, mone{-1.0, 0.0}, zero{0.0, 0.0};
+  const DD bnorm = dd_sqrt(dd_dot(n, bh, bl, bh, bl));
+  double rnorm = 0.0;
+  int itr = 1, inner = 1, mm = 0;
+  for (itr = 1; itr <= prm.itrmax; itr += m) {
+    std::fill(e.begin(), e.end(), zero); std::fill(c.begin(), c.end(), zero);
+    std::fill(s.begin(), s.end(), zero); std::fill(y.begin(), y.end(), zero);
+    std::fill(h.begin(), h.end(), zero);
+    dd_spmv(A, alo, xh, xl, rh.data(), rl.data());                        // ddcalc_res
+    dd_axpy(n, one, mone, bh, bl, rh.data(), rl.data());
+    const DD rn = dd_sqrt(dd_dot(n, rh.data(), rl.data(), rh.data(), rl.data()));
+    dd_axpy(n, dd_div(mone, rn), zero, rh.data(), rl.data(), Vh.data(), Vl.data());   // v_1 = -r / |r|
+    e[0] = dd_mul(mone, rn);
+    rnorm = rn.hi;
+    if (itr == 1) hist[itr - 1] = rnorm / bnorm.hi;
+    bool exit_inner = false;
+    for (inner = 1; inner <= m; ++inner) {
+      const long off = (long)(inner - 1) * n;
+      dd_apply_precon(A, alo, P, Vh.data() + off, Vl.data() + off, pvh.data(), pvl.data());
+      dd_spmv(A, alo, pvh.data(), pvl.data(), wh.data(), wl.data());
+      DD* col = h.data() + (long)(inner - 1) * (m + 1);
+      if (gs == ORC_GS_MGS) {
+        for (int k = 1; k < inner; ++k) {
+          const long ok = (long)(k - 1) * n;
+          col[k - 1] = dd_dot(n, wh.data(), wl.data(), Vh.data() + ok, Vl.data() + ok);
+          dd_axpy(n, dd_mul(mone, col[k - 1]), one, Vh.data() + ok, Vl.data() + ok, wh.data(), wl.data());
+        }
+      } else {
+        for (int k = 1; k < inner; ++k) {
+          const long ok = (long)(k - 1) * n;
+          col[k - 1] = dd_dot(n, Vh.data() + ok, Vl.data() + ok, wh.data(), wl.data());
+        }
+        for (int k = 1; k < inner; ++k) {
+          const long ok = (long)(k - 1) * n;
+          dd_axpy(n, dd_mul(mone, col[k - 1]), one, Vh.data() + ok, Vl.data() + ok, wh.data(), wl.data());
+        }
+      }
+      col[inner - 1] = dd_dot(n, wh.data(), wl.data(), Vh.data() + off, Vl.data() + off);
+      dd_axpy(n, dd_mul(mone, col[inner - 1]), one, Vh.data() + off, Vl.data() + off, wh.data(), wl.data());
+      col[inner] = dd_sqrt(dd_dot(n, wh.data(), wl.data(), wh.data(), wl.data()));
+      const long on = (long)inner * n;
+      dd_axpy(n, dd_div(one, col[inner]), zero, wh.data(), wl.data(), Vh.data() + on, Vl.data() + on);
+      dd_givens(m, h.data(), inner, c.data(), s.data(), e.data());
+      rnorm = std::fabs(e[inner].hi);
+      mm = inner;
+      if (itr + inner <= prm.itrmax) hist[itr + inner - 1] = rnorm / bnorm.hi;
+      if (rnorm / bnorm.hi < prm.rtolmax || itr + inner == prm.itrmax) { exit_inner = true; break; }
+    }
+    if (!exit_inner) inner = m + 1;             // Fortran DO variable after completion
+    if (m < mm) mm = m;
+    // ddupdate_xVec (ddpgmres.f90:52-145): y = H^-1 e, v0 = V y, x = M^-1 v0 + x
+    for (int i = mm; i >= 1; --i) {
+      y[i - 1] = e[i - 1];
+      for (int j = mm; j >= i + 1; --j)
+        y[i - 1] = dd_sub(y[i - 1], dd_mul(h[(i - 1) + (long)(j - 1) * (m + 1)], y[j - 1]));
+      const DD d = h[(i - 1) + (long)(i - 1) * (m + 1)];
+      y[i - 1] = (d.hi == 0.0 && d.lo == 0.0) ? dd_div(y[i - 1], DD{1.0e-100, 0.0}) : dd_div(y[i - 1], d);
+    }
+#pragma omp parallel for schedule(static)
+    for (long j = 0; j < n; ++j) {               // ddsum_vec (ddpgmres.f90:7-50)
+      DD t{0.0, 0.0};
+      for (int i = 0; i < mm; ++i) t = dd_add(t, dd_mul(y[i], DD{Vh[(long)i * n + j], Vl[(long)i * n + j]}));
+      v0h[j] = t.hi;
+      v0l[j] = t.lo;
+    }
+    dd_apply_precon(A, alo, P, v0h.data(), v0l.data(), x0h.data(), x0l.data());
+    dd_axpy(n, one, one, x0h.data(), x0l.data(), xh, xl);
+    if (rnorm / bnorm.hi < prm.rtolmax) break;
+    if (itr + inner == prm.itrmax) break;
+  }
+  *niter = std::min(prm.itrmax, itr + inner);
+  *iret = (prm.itrmax <= itr) ? 1 : 0;
+}
+
 // ---------------------------------------------------------------------------------
 // C entry points used by the tests and the CPU-baseline leg of bench.py.
 extern "C" {
@@ -1064,6 +1181,8 @@ int orc_ddcg(const OrcMat* A, const double* alo, const OrcParams* prm, int prec_
   }
   if (prm->solver == ORC_SOLVER_BICG)
     ddbicg(*A, a_lo, P, *prm, bh, bl0.data(), xh, xl0.data(), hist, niter, iret);
+  else if (prm->solver == ORC_SOLVER_GMRES)
+    ddgmres(*A, a_lo, P, *prm, bh, bl0.data(), xh, xl0.data(), hist, niter, iret);
   else
     ddpcg(*A, a_lo, P, *prm, bh, bl0.data(), xh, xl0.data(), hist, niter, iret);
   if (prec_x == 2 && xl) std::copy(xl0.begin(), xl0.end(), xl);

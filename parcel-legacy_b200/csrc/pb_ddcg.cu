@@ -1,8 +1,8 @@
-// pb_ddcg.cu -- double-double preconditioned CG and BiCGStab on the GPU (PARCEL_ddKSP_CRS,
-// solvers 1 and 2).
+// pb_ddcg.cu -- double-double preconditioned CG, BiCGStab and GMRES(m) on the GPU
+// (PARCEL_ddKSP_CRS, solvers 1, 2 and 3).
 //
-// Reference: ddKSP_pCG (src/ddpcg.f90:247-563) and ddKSP_pBiCG (src/ddpbicg.f90:496-875)
-// with the precision flags of
+// Reference: ddKSP_pCG (src/ddpcg.f90:247-563), ddKSP_pBiCG (src/ddpbicg.f90:496-875) and
+// ddKSP_pGMRES (src/ddpgmres.f90:254-713) with the precision flags of
 // PARCEL_ddKSP_CRS (src/ddwrapper.f90:184-280): A, b, x and the preconditioner each in
 // double (1) or double-double (2).  The reference runs its dd solvers on the CPU only
 // (src/ddkrylov.f90:81,207); this is a GPU implementation of the same arithmetic.
@@ -237,6 +237,132 @@ __global__ void k_dd_bicg_axpy4p(int n, const DdScalB* sc, double* __restrict__ 
     const dd p = dd_add(dd{rh[i], rl[i]}, c);
     ph[i] = p.hi;
     pl[i] = p.lo;
+  }
+}
+
+// ------------------------------------------------------------------ GMRES (ddKSP_pGMRES)
+// Small state of ddKSP_pGMRES (ddpgmres.f90:254-713), on the device: the (m+1) x m
+// Hessenberg matrix (column-major), the rotations c and s, the rotated right-hand side e
+// and the update coefficients y.
+struct DdGm {
+  int m = 0;
+  dd* h = nullptr;
+  dd* c = nullptr;
+  dd* s = nullptr;
+  dd* e = nullptr;
+  dd* y = nullptr;
+  dd* bnorm = nullptr;
+  dd* t1 = nullptr;       // the scale of the next basis vector
+  double* rn = nullptr;   // the residual norm's high part, read by the host
+};
+
+enum DdStepG { DDG_BNORM = 0, DDG_START, DDG_NORM, DDG_SOLVE };
+
+// ddGivensRotations (ddpgmres.f90:147-250) on column i (1-based).
+__device__ void dd_givens(const DdGm& g, int i) {
+  dd* col = g.h + (int64_t)(i - 1) * (g.m + 1);
+  dd* c = g.c;
+  dd* s = g.s;
+  dd* e = g.e;
+  for (int k = 1; k <= i - 1; ++k) {
+    const dd t1 = dd_sub(dd_mul(col[k - 1], c[k - 1]), dd_mul(col[k], s[k - 1]));
+    const dd t2 = dd_add(dd_mul(col[k - 1], s[k - 1]), dd_mul(col[k], c[k - 1]));
+    col[k - 1] = t1;
+    col[k] = t2;
+  }
+  const dd d = col[i - 1];
+  const dd t = (d.hi == 0.0 && d.lo == 0.0) ? dd_div(col[i], dd{1.0e-100, 0.0}) : dd_div(col[i], d);
+  const dd q = dd_sqrt(dd_add(dd{1.0, 0.0}, dd_mul(t, t)));
+  c[i - 1] = dd_div(dd{1.0, 0.0}, q);
+  s[i - 1] = dd_mul(dd{-1.0, 0.0}, dd_mul(c[i - 1], t));
+  const dd e1 = dd_sub(dd_mul(c[i - 1], e[i - 1]), dd_mul(s[i - 1], e[i]));
+  const dd e2 = dd_add(dd_mul(s[i - 1], e[i - 1]), dd_mul(c[i - 1], e[i]));
+  e[i - 1] = e1;
+  e[i] = e2;
+  col[i - 1] = dd_sub(dd_mul(c[i - 1], col[i - 1]), dd_mul(s[i - 1], col[i]));
+  col[i] = dd{0.0, 0.0};
+}
+
+// Scalar steps of ddKSP_pGMRES, one thread.  DDG_START: d = <r, r> of the restart
+// residual; DDG_NORM: d = <w, w> for column i, then the rotation of that column;
+// DDG_SOLVE: y = H^-1 e over the first i columns (ddupdate_xVec, ddpgmres.f90:98-118).
+__global__ void k_dd_gm_scal(DdGm g, int step, int i, const dd* d) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int ld = g.m + 1;
+  switch (step) {
+    case DDG_BNORM:
+      *g.bnorm = dd_sqrt(*d);
+      break;
+    case DDG_START: {
+      for (int k = 0; k < ld * g.m; ++k) g.h[k] = dd{0.0, 0.0};
+      for (int k = 0; k < ld; ++k) g.c[k] = g.s[k] = g.e[k] = g.y[k] = dd{0.0, 0.0};
+      const dd rn = dd_sqrt(*d);
+      *g.t1 = dd_div(dd{-1.0, 0.0}, rn);
+      g.e[0] = dd_mul(dd{-1.0, 0.0}, rn);
+      *g.rn = rn.hi;
+      break;
+    }
+    case DDG_NORM: {
+      dd* col = g.h + (int64_t)(i - 1) * ld;
+      col[i] = dd_sqrt(*d);
+      *g.t1 = dd_div(dd{1.0, 0.0}, col[i]);
+      dd_givens(g, i);
+      *g.rn = fabs(g.e[i].hi);
+      break;
+    }
+    case DDG_SOLVE:
+      for (int r = i; r >= 1; --r) {
+        dd y = g.e[r - 1];
+        for (int j = i; j >= r + 1; --j) y = dd_sub(y, dd_mul(g.h[(r - 1) + (int64_t)(j - 1) * ld], g.y[j - 1]));
+        const dd dg = g.h[(r - 1) + (int64_t)(r - 1) * ld];
+        g.y[r - 1] = (dg.hi == 0.0 && dg.lo == 0.0) ? dd_div(y, dd{1.0e-100, 0.0}) : dd_div(y, dg);
+      }
+      break;
+  }
+}
+
+// w = (-h) v + 1 w with h read from the device (the projection step of
+// ddMGS_Orthonormalization, ddQRDecomposition.f90:27-44).
+__global__ void k_dd_axpy_nh(int n, const dd* hk, const double* __restrict__ vh, const double* __restrict__ vl,
+                             double* __restrict__ wh, double* __restrict__ wl) {
+  const dd a = dd_mul(dd{-1.0, 0.0}, *hk), b = dd{1.0, 0.0};
+  GRID_LOOP(i, n) {
+    const dd c = dd_mul(b, dd{wh[i], wl[i]});
+    const dd t = dd_mul(a, dd{vh[i], vl[i]});
+    const dd w = dd_add(t, c);
+    wh[i] = w.hi;
+    wl[i] = w.lo;
+  }
+}
+
+// The subtractions of ddCGS_Orthonormalization (ddQRDecomposition.f90:73-86),
+// w = (-h_k) v_k + 1 w for k = 1..cnt in that order, in one pass over w and the basis.
+__global__ void k_dd_cgs_sub(int n, int cnt, const dd* hcol, const double* __restrict__ Vh,
+                             const double* __restrict__ Vl, int64_t ldv, double* __restrict__ wh,
+                             double* __restrict__ wl) {
+  const dd b = dd{1.0, 0.0};
+  GRID_LOOP(i, n) {
+    dd w = dd{wh[i], wl[i]};
+    for (int k = 0; k < cnt; ++k) {
+      const dd a = dd_mul(dd{-1.0, 0.0}, hcol[k]);
+      const dd c = dd_mul(b, w);
+      const dd t = dd_mul(a, dd{Vh[k * ldv + i], Vl[k * ldv + i]});
+      w = dd_add(t, c);
+    }
+    wh[i] = w.hi;
+    wl[i] = w.lo;
+  }
+}
+
+// ddsum_vec (ddpgmres.f90:7-50): v0 = sum_k y_k v_k, k in order, from 0.
+__global__ void k_dd_sum_vec(int n, int mm, const dd* y, const double* __restrict__ Vh,
+                             const double* __restrict__ Vl, int64_t ldv, double* __restrict__ v0h,
+                             double* __restrict__ v0l) {
+  GRID_LOOP(i, n) {
+    dd t{0.0, 0.0};
+    for (int k = 0; k < mm; ++k) t = dd_add(t, dd_mul(y[k], dd{Vh[k * ldv + i], Vl[k * ldv + i]}));
+    v0h[i] = t.hi;
+    v0l[i] = t.lo;
   }
 }
 
@@ -731,7 +857,248 @@ using namespace pb;
 
 namespace {
 
-// The dd Krylov solves of PARCEL_ddKSP_CRS: CG (ddKSP_pCG) or BiCGStab (ddKSP_pBiCG).
+// What the dd solver loops share: the system, the preconditioner, the stream, the dot
+// scratch and the constants 1, -1 and 0 on the device.
+struct DdRun {
+  const DdSystem& S;
+  const DdPrecon& P;
+  cudaStream_t st;
+  int n, g;
+  dd* part;
+  dd* one;
+  dd* mone;
+  dd* zero;
+  void spmv(const double* xh, const double* xl, double* yh, double* yl) const {
+    k_dd_spmv<<<g, kDdThreads, 0, st>>>(n, S.rp, S.ci, S.ah, S.al, S.cbase, xh, xl, yh, yl);
+  }
+  void spmv(const DdVec& x, DdVec& y) const { spmv(x.hi(), x.lo(), y.hi(), y.lo()); }
+  void dot(const double* xh, const double* xl, const double* yh, const double* yl, dd* out) const {
+    dd_dot(S, xh, xl, yh, yl, part, out, st);
+  }
+  void dot(const DdVec& u, const DdVec& v, DBuf& out) const { dot(u.hi(), u.lo(), v.hi(), v.lo(), dp<dd>(out)); }
+  // y = alpha x + beta y (ddaxpy)
+  void axpy(const dd* alpha, const dd* beta, const double* xh, const double* xl, double* yh, double* yl) const {
+    k_dd_axpy<<<g, kDdThreads, 0, st>>>(n, alpha, beta, xh, xl, yh, yl);
+  }
+  void precon(const double* rh, const double* rl, double* sh, double* sl) const {
+    dd_apply_precon(S, P, rh, rl, sh, sl, st);
+  }
+  // r = b - A x (ddcalc_res: r = A x, then r = 1 b + (-1) r)
+  void residual(const DdVec& x, const DdVec& b, DdVec& r) const {
+    spmv(x, r);
+    axpy(one, mone, b.hi(), b.lo(), r.hi(), r.lo());
+  }
+};
+
+struct DdLoop {
+  int used = 0, iret = 0;
+  double setup_end = 0.0;
+};
+
+double read_double(const double* dev, cudaStream_t st) {
+  double v;
+  PB_CUDA(cudaMemcpyAsync(&v, dev, sizeof(double), cudaMemcpyDeviceToHost, st));
+  PB_CUDA(cudaStreamSynchronize(st));
+  return v;
+}
+
+// ddKSP_pCG (ddpcg.f90:247-563).
+DdLoop dd_cg_loop(const DdRun& R, const Options& o, DdVec& x, const DdVec& b, double* reshistory) {
+  const int n = R.n, g = R.g;
+  cudaStream_t st = R.st;
+  DdLoop L;
+  DdVec r(n), p(n), q(n), s(n);
+  DBuf scal(sizeof(DdScal)), d1(sizeof(dd)), d2(sizeof(dd));
+  DdScal* sc = dp<DdScal>(scal);
+  R.residual(x, b, r);
+  R.dot(b, b, d1);
+  R.dot(r, r, d2);
+  k_dd_scal<<<1, 32, 0, st>>>(sc, DD_INIT_NORMS, dp<dd>(d1), dp<dd>(d2));
+  R.precon(r.hi(), r.lo(), s.hi(), s.lo());
+  R.dot(s, r, d1);
+  k_dd_scal<<<1, 32, 0, st>>>(sc, DD_INIT_RHO, dp<dd>(d1), nullptr);
+  PB_CUDA(cudaGetLastError());
+  L.setup_end = now_s();
+  DdScal h;
+  PB_CUDA(cudaMemcpyAsync(&h, sc, sizeof(DdScal), cudaMemcpyDeviceToHost, st));
+  sync();
+  const double bnorm = h.bnorm.hi;
+  double rnorm = h.rnorm.hi;
+  int itr;
+  for (itr = 1; itr <= o.itrmax; ++itr) {
+    if (reshistory) reshistory[itr - 1] = rnorm / bnorm;
+    k_dd_cg_axpy2<<<g, kDdThreads, 0, st>>>(n, sc, x.hi(), x.lo(), p.hi(), p.lo(), s.hi(), s.lo());
+    R.spmv(p, q);
+    R.dot(p, q, d1);
+    k_dd_scal<<<1, 32, 0, st>>>(sc, DD_ALPHA, dp<dd>(d1), nullptr);
+    R.axpy(&sc->t1, R.one, q.hi(), q.lo(), r.hi(), r.lo());
+    R.precon(r.hi(), r.lo(), s.hi(), s.lo());
+    R.dot(s, r, d1);
+    R.dot(r, r, d2);
+    k_dd_scal<<<1, 32, 0, st>>>(sc, DD_RNORM, dp<dd>(d1), dp<dd>(d2));
+    PB_CUDA(cudaGetLastError());
+    rnorm = read_double(&sc->rnorm.hi, st);
+    if (rnorm / bnorm < o.rtol) break;
+    k_dd_scal<<<1, 32, 0, st>>>(sc, DD_BETA, nullptr, nullptr);
+  }
+  // x = alpha p + 1 x
+  R.axpy(&sc->alpha, R.one, p.hi(), p.lo(), x.hi(), x.lo());
+  PB_CUDA(cudaGetLastError());
+  L.used = std::min(o.itrmax, itr);
+  L.iret = (o.itrmax <= itr) ? 1 : 0;
+  return L;
+}
+
+// ddKSP_pBiCG (ddpbicg.f90:496-875): r0 = p = r, c1 = <r0, r0>.
+DdLoop dd_bicg_loop(const DdRun& R, const Options& o, DdVec& x, const DdVec& b, double* reshistory) {
+  const int n = R.n, g = R.g;
+  cudaStream_t st = R.st;
+  DdLoop L;
+  DdVec r(n), p(n), q(n), r0(n), pp(n), e(n), pe(n), v(n);
+  DBuf scb(sizeof(DdScalB)), d1(sizeof(dd)), d2(sizeof(dd));
+  DdScalB* sb = dp<DdScalB>(scb);
+  R.residual(x, b, r);
+  k_dd_copy<<<g, kDdThreads, 0, st>>>(n, r.hi(), r.lo(), r0.hi(), r0.lo());
+  k_dd_copy<<<g, kDdThreads, 0, st>>>(n, r.hi(), r.lo(), p.hi(), p.lo());
+  R.dot(b, b, d1);
+  R.dot(r0, r0, d2);
+  k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_INIT, dp<dd>(d1), dp<dd>(d2));
+  PB_CUDA(cudaGetLastError());
+  L.setup_end = now_s();
+  DdScalB h;
+  PB_CUDA(cudaMemcpyAsync(&h, sb, sizeof(DdScalB), cudaMemcpyDeviceToHost, st));
+  sync();
+  const double bnorm = h.bnorm.hi;
+  double hist = h.hist;
+  int itr;
+  for (itr = 1; itr <= o.itrmax; ++itr) {
+    if (reshistory) reshistory[itr - 1] = hist;
+    R.precon(p.hi(), p.lo(), pp.hi(), pp.lo());
+    R.spmv(pp, q);
+    R.dot(r0, q, d1);
+    k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_ALPHA, dp<dd>(d1), nullptr);
+    k_dd_bicg_axpy3<<<g, kDdThreads, 0, st>>>(n, sb, r.hi(), r.lo(), q.hi(), q.lo(), e.hi(), e.lo());
+    R.precon(e.hi(), e.lo(), pe.hi(), pe.lo());
+    R.spmv(pe, v);
+    R.dot(e, v, d1);
+    R.dot(v, v, d2);
+    k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_C3, dp<dd>(d1), dp<dd>(d2));
+    k_dd_bicg_axpy4<<<g, kDdThreads, 0, st>>>(n, sb, x.hi(), x.lo(), pp.hi(), pp.lo(), pe.hi(), pe.lo());
+    k_dd_bicg_axpy3r<<<g, kDdThreads, 0, st>>>(n, sb, e.hi(), e.lo(), v.hi(), v.lo(), r.hi(), r.lo());
+    R.dot(r, r0, d1);
+    R.dot(r, r, d2);
+    k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_RNORM, dp<dd>(d1), dp<dd>(d2));
+    PB_CUDA(cudaGetLastError());
+    double rn[2];
+    PB_CUDA(cudaMemcpyAsync(&rn[0], &sb->rnorm.hi, sizeof(double), cudaMemcpyDeviceToHost, st));
+    PB_CUDA(cudaMemcpyAsync(&rn[1], &sb->hist, sizeof(double), cudaMemcpyDeviceToHost, st));
+    sync();
+    hist = rn[1];
+    if (rn[0] / bnorm < o.rtol) break;
+    k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_BETA, nullptr, nullptr);
+    k_dd_bicg_axpy4p<<<g, kDdThreads, 0, st>>>(n, sb, p.hi(), p.lo(), r.hi(), r.lo(), q.hi(), q.lo());
+  }
+  PB_CUDA(cudaGetLastError());
+  L.used = std::min(o.itrmax, itr);
+  L.iret = (o.itrmax <= itr) ? 1 : 0;
+  return L;
+}
+
+// ddKSP_pGMRES (ddpgmres.f90:254-713): right-preconditioned GMRES(m), MGS or CGS.  The
+// restart residual is tested only against abstolmax, which parcel_ddgmres fixes at 0
+// (ddwrapper.f90:438), so that test is left out.  History entries are rnorm.hi / bnorm.hi;
+// the first cycle also stores its starting residual.  Entries past itrmax (the reference
+// writes m of them when itrmax is 1) are not stored.
+DdLoop dd_gmres_loop(const DdRun& R, const Options& o, DdVec& x, const DdVec& b, double* reshistory) {
+  const int n = R.n, g = R.g;
+  cudaStream_t st = R.st;
+  DdLoop L;
+  const int m = std::max(1, o.m);
+  const bool mgs = o.gs != PARCEL_B_GS_CGS;
+  const int64_t ldv = n;
+  DdVec r(n), pv(n), w(n), x0(n), v0(n);
+  DBuf Vh(sizeof(double) * (size_t)(m + 1) * ldv), Vl(sizeof(double) * (size_t)(m + 1) * ldv);   // zero-filled
+  auto vh = [&](int k) { return dp<double>(Vh) + (int64_t)k * ldv; };   // v_{k+1}
+  auto vl = [&](int k) { return dp<double>(Vl) + (int64_t)k * ldv; };
+  const int ld = m + 1;
+  DBuf hbuf(sizeof(dd) * (size_t)ld * m), cbuf(sizeof(dd) * ld), sbuf(sizeof(dd) * ld), ebuf(sizeof(dd) * ld),
+      ybuf(sizeof(dd) * ld), sc(sizeof(dd) * 2 + sizeof(double)), d1(sizeof(dd));
+  DdGm G;
+  G.m = m;
+  G.h = dp<dd>(hbuf);
+  G.c = dp<dd>(cbuf);
+  G.s = dp<dd>(sbuf);
+  G.e = dp<dd>(ebuf);
+  G.y = dp<dd>(ybuf);
+  G.bnorm = dp<dd>(sc);
+  G.t1 = G.bnorm + 1;
+  G.rn = reinterpret_cast<double*>(G.bnorm + 2);
+  R.dot(b, b, d1);
+  k_dd_gm_scal<<<1, 32, 0, st>>>(G, DDG_BNORM, 0, dp<dd>(d1));
+  PB_CUDA(cudaGetLastError());
+  dd bn;
+  PB_CUDA(cudaMemcpyAsync(&bn, G.bnorm, sizeof(dd), cudaMemcpyDeviceToHost, st));
+  sync();
+  L.setup_end = now_s();
+  const double bnorm = bn.hi;
+  auto hist_at = [&](int k, double v) {   // 1-based entry k
+    if (reshistory && k >= 1 && k <= o.itrmax) reshistory[k - 1] = v;
+  };
+  double rnorm = 0.0;
+  int itr = 1, inner = 1, mm = 0;
+  for (itr = 1; itr <= o.itrmax; itr += m) {
+    R.residual(x, b, r);
+    R.dot(r, r, d1);
+    k_dd_gm_scal<<<1, 32, 0, st>>>(G, DDG_START, 0, dp<dd>(d1));
+    R.axpy(G.t1, R.zero, r.hi(), r.lo(), vh(0), vl(0));   // v_1 = -r / |r|
+    PB_CUDA(cudaGetLastError());
+    rnorm = read_double(G.rn, st);
+    if (itr == 1) hist_at(itr, rnorm / bnorm);
+    bool exit_inner = false;
+    for (inner = 1; inner <= m; ++inner) {
+      R.precon(vh(inner - 1), vl(inner - 1), pv.hi(), pv.lo());
+      R.spmv(pv, w);
+      dd* col = G.h + (int64_t)(inner - 1) * ld;
+      if (mgs) {
+        for (int k = 1; k < inner; ++k) {
+          R.dot(w.hi(), w.lo(), vh(k - 1), vl(k - 1), col + (k - 1));
+          k_dd_axpy_nh<<<g, kDdThreads, 0, st>>>(n, col + (k - 1), vh(k - 1), vl(k - 1), w.hi(), w.lo());
+        }
+      } else if (inner > 1) {
+        for (int k = 1; k < inner; ++k) R.dot(vh(k - 1), vl(k - 1), w.hi(), w.lo(), col + (k - 1));
+        k_dd_cgs_sub<<<g, kDdThreads, 0, st>>>(n, inner - 1, col, dp<double>(Vh), dp<double>(Vl), ldv, w.hi(),
+                                               w.lo());
+      }
+      R.dot(w.hi(), w.lo(), vh(inner - 1), vl(inner - 1), col + (inner - 1));
+      k_dd_axpy_nh<<<g, kDdThreads, 0, st>>>(n, col + (inner - 1), vh(inner - 1), vl(inner - 1), w.hi(), w.lo());
+      R.dot(w, w, d1);
+      k_dd_gm_scal<<<1, 32, 0, st>>>(G, DDG_NORM, inner, dp<dd>(d1));
+      R.axpy(G.t1, R.zero, w.hi(), w.lo(), vh(inner), vl(inner));   // v_{i+1} = w / |w|
+      PB_CUDA(cudaGetLastError());
+      rnorm = read_double(G.rn, st);
+      mm = inner;
+      hist_at(itr + inner, rnorm / bnorm);
+      if (rnorm / bnorm < o.rtol || itr + inner == o.itrmax) { exit_inner = true; break; }
+    }
+    if (!exit_inner) inner = m + 1;   // the Fortran DO variable after a completed loop
+    if (m < mm) mm = m;
+    // ddupdate_xVec (ddpgmres.f90:52-145): y = H^-1 e, v0 = V y, x = M^-1 v0 + x
+    k_dd_gm_scal<<<1, 32, 0, st>>>(G, DDG_SOLVE, mm, nullptr);
+    k_dd_sum_vec<<<g, kDdThreads, 0, st>>>(n, mm, G.y, dp<double>(Vh), dp<double>(Vl), ldv, v0.hi(), v0.lo());
+    R.precon(v0.hi(), v0.lo(), x0.hi(), x0.lo());
+    R.axpy(R.one, R.one, x0.hi(), x0.lo(), x.hi(), x.lo());
+    PB_CUDA(cudaGetLastError());
+    if (rnorm / bnorm < o.rtol) break;
+    if (itr + inner == o.itrmax) break;
+  }
+  sync();
+  L.used = std::min(o.itrmax, itr + inner);
+  L.iret = (o.itrmax <= itr) ? 1 : 0;
+  return L;
+}
+
+// The dd Krylov solves of PARCEL_ddKSP_CRS: CG (ddKSP_pCG), BiCGStab (ddKSP_pBiCG) or
+// GMRES(m) (ddKSP_pGMRES).
 int dd_krylov(int solver, const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo, int precision_A,
               int precision_b, int precision_x, int precision_precondition, const double* b_hi, const double* b_lo,
               double* x_hi, double* x_lo, double* reshistory, int* niter, int* iret) {
@@ -760,9 +1127,8 @@ int dd_krylov(int solver, const parcel_b_input* prm, const parcel_b_crs* A, cons
     S.al = static_cast<const double*>(aal.p);
     DdPrecon P;
     dd_setup_precon(o, *A, S, precision_precondition, P);
-    // vectors: x and b in dd, the low parts zero unless their precision is 2
-    DdVec x(n), b(n), r(n), p(n), q(n), s(n);
-    const bool bicg = solver == PARCEL_B_SOLVER_BICG;
+    // x and b in dd, the low parts zero unless their precision is 2
+    DdVec x(n), b(n);
     auto load = [&](DdVec& v, const double* hi, const double* lo, bool use_lo) {
       if (is_device_ptr(hi)) PB_CUDA(cudaMemcpyAsync(v.hi(), hi, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
       else h2d(v.hi(), hi, sizeof(double) * n);
@@ -773,110 +1139,19 @@ int dd_krylov(int solver, const parcel_b_input* prm, const parcel_b_crs* A, cons
     };
     load(x, x_hi, x_lo, precision_x == 2);
     load(b, b_hi, b_lo, precision_b == 2);
-    DBuf scal(sizeof(DdScal)), part(sizeof(dd) * (kDdChunks + kDdGroups)), d1(sizeof(dd)), d2(sizeof(dd)),
-        cst(sizeof(dd) * 4);
-    DdScal* sc = dp<DdScal>(scal);
-    dd* dcst = dp<dd>(cst);   // 1, -1, 0, (unused)
+    DBuf part(sizeof(dd) * (kDdChunks + kDdGroups)), cst(sizeof(dd) * 3);
+    dd* dcst = dp<dd>(cst);
     {
-      const dd h[4] = {dd{1.0, 0.0}, dd{-1.0, 0.0}, dd{0.0, 0.0}, dd{0.0, 0.0}};
+      const dd h[3] = {dd{1.0, 0.0}, dd{-1.0, 0.0}, dd{0.0, 0.0}};
       h2d(dcst, h, sizeof(h));
     }
-    const int g = grid_for(n);
-    auto spmv = [&](const DdVec& in, DdVec& out) {
-      k_dd_spmv<<<g, kDdThreads, 0, st>>>(n, S.rp, S.ci, S.ah, S.al, S.cbase, in.hi(), in.lo(), out.hi(), out.lo());
-    };
-    auto dot = [&](const DdVec& u, const DdVec& v, DBuf& out) {
-      dd_dot(S, u.hi(), u.lo(), v.hi(), v.lo(), dp<dd>(part), dp<dd>(out), st);
-    };
-    // r = b - A x (ddcalc_res: r = A x, then r = 1 b + (-1) r)
-    spmv(x, r);
-    k_dd_axpy<<<g, kDdThreads, 0, st>>>(n, dcst + 0, dcst + 1, b.hi(), b.lo(), r.hi(), r.lo());
-    double setup_end = 0.0;
-    int itr = 1;
-    if (!bicg) {
-    dot(b, b, d1);
-    dot(r, r, d2);
-    k_dd_scal<<<1, 32, 0, st>>>(sc, DD_INIT_NORMS, dp<dd>(d1), dp<dd>(d2));
-    dd_apply_precon(S, P, r.hi(), r.lo(), s.hi(), s.lo(), st);
-    dot(s, r, d1);
-    k_dd_scal<<<1, 32, 0, st>>>(sc, DD_INIT_RHO, dp<dd>(d1), nullptr);
-    PB_CUDA(cudaGetLastError());
-    setup_end = now_s();
-    DdScal h;
-    PB_CUDA(cudaMemcpyAsync(&h, sc, sizeof(DdScal), cudaMemcpyDeviceToHost, st));
-    sync();
-    const double bnorm = h.bnorm.hi;
-    double rnorm = h.rnorm.hi;
-    for (itr = 1; itr <= o.itrmax; ++itr) {
-      if (reshistory) reshistory[itr - 1] = rnorm / bnorm;
-      k_dd_cg_axpy2<<<g, kDdThreads, 0, st>>>(n, sc, x.hi(), x.lo(), p.hi(), p.lo(), s.hi(), s.lo());
-      spmv(p, q);
-      dot(p, q, d1);
-      k_dd_scal<<<1, 32, 0, st>>>(sc, DD_ALPHA, dp<dd>(d1), nullptr);
-      k_dd_axpy<<<g, kDdThreads, 0, st>>>(n, &sc->t1, dcst + 0, q.hi(), q.lo(), r.hi(), r.lo());
-      dd_apply_precon(S, P, r.hi(), r.lo(), s.hi(), s.lo(), st);
-      dot(s, r, d1);
-      dot(r, r, d2);
-      k_dd_scal<<<1, 32, 0, st>>>(sc, DD_RNORM, dp<dd>(d1), dp<dd>(d2));
-      PB_CUDA(cudaGetLastError());
-      double rn;
-      PB_CUDA(cudaMemcpyAsync(&rn, &sc->rnorm.hi, sizeof(double), cudaMemcpyDeviceToHost, st));
-      sync();
-      rnorm = rn;
-      if (rnorm / bnorm < o.rtol) break;
-      k_dd_scal<<<1, 32, 0, st>>>(sc, DD_BETA, nullptr, nullptr);
-    }
-    // x = alpha p + 1 x
-    k_dd_axpy<<<g, kDdThreads, 0, st>>>(n, &sc->alpha, dcst + 0, p.hi(), p.lo(), x.hi(), x.lo());
-    PB_CUDA(cudaGetLastError());
-    } else {
-    // ddKSP_pBiCG: r0 = p = r; c1 = <r0, r0>
-    DdVec r0(n), pp(n), e(n), pe(n), v(n);
-    DBuf scb(sizeof(DdScalB));
-    DdScalB* sb = dp<DdScalB>(scb);
-    k_dd_copy<<<g, kDdThreads, 0, st>>>(n, r.hi(), r.lo(), r0.hi(), r0.lo());
-    k_dd_copy<<<g, kDdThreads, 0, st>>>(n, r.hi(), r.lo(), p.hi(), p.lo());
-    dot(b, b, d1);
-    dot(r0, r0, d2);
-    k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_INIT, dp<dd>(d1), dp<dd>(d2));
-    PB_CUDA(cudaGetLastError());
-    setup_end = now_s();
-    DdScalB h;
-    PB_CUDA(cudaMemcpyAsync(&h, sb, sizeof(DdScalB), cudaMemcpyDeviceToHost, st));
-    sync();
-    const double bnorm = h.bnorm.hi;
-    double hist = h.hist;
-    for (itr = 1; itr <= o.itrmax; ++itr) {
-      if (reshistory) reshistory[itr - 1] = hist;
-      dd_apply_precon(S, P, p.hi(), p.lo(), pp.hi(), pp.lo(), st);
-      spmv(pp, q);
-      dot(r0, q, d1);
-      k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_ALPHA, dp<dd>(d1), nullptr);
-      k_dd_bicg_axpy3<<<g, kDdThreads, 0, st>>>(n, sb, r.hi(), r.lo(), q.hi(), q.lo(), e.hi(), e.lo());
-      dd_apply_precon(S, P, e.hi(), e.lo(), pe.hi(), pe.lo(), st);
-      spmv(pe, v);
-      dot(e, v, d1);
-      dot(v, v, d2);
-      k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_C3, dp<dd>(d1), dp<dd>(d2));
-      k_dd_bicg_axpy4<<<g, kDdThreads, 0, st>>>(n, sb, x.hi(), x.lo(), pp.hi(), pp.lo(), pe.hi(), pe.lo());
-      k_dd_bicg_axpy3r<<<g, kDdThreads, 0, st>>>(n, sb, e.hi(), e.lo(), v.hi(), v.lo(), r.hi(), r.lo());
-      dot(r, r0, d1);
-      dot(r, r, d2);
-      k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_RNORM, dp<dd>(d1), dp<dd>(d2));
-      PB_CUDA(cudaGetLastError());
-      double rn[2];
-      PB_CUDA(cudaMemcpyAsync(&rn[0], &sb->rnorm.hi, sizeof(double), cudaMemcpyDeviceToHost, st));
-      PB_CUDA(cudaMemcpyAsync(&rn[1], &sb->hist, sizeof(double), cudaMemcpyDeviceToHost, st));
-      sync();
-      hist = rn[1];
-      if (rn[0] / bnorm < o.rtol) break;
-      k_dd_scal_b<<<1, 32, 0, st>>>(sb, DDB_BETA, nullptr, nullptr);
-      k_dd_bicg_axpy4p<<<g, kDdThreads, 0, st>>>(n, sb, p.hi(), p.lo(), r.hi(), r.lo(), q.hi(), q.lo());
-    }
-    PB_CUDA(cudaGetLastError());
-    }
-    used = std::min(o.itrmax, itr);
-    ir = (o.itrmax <= itr) ? 1 : 0;
+    const DdRun R{S, P, st, n, grid_for(n), dp<dd>(part), dcst, dcst + 1, dcst + 2};
+    DdLoop L;
+    if (solver == PARCEL_B_SOLVER_BICG) L = dd_bicg_loop(R, o, x, b, reshistory);
+    else if (solver == PARCEL_B_SOLVER_GMRES) L = dd_gmres_loop(R, o, x, b, reshistory);
+    else L = dd_cg_loop(R, o, x, b, reshistory);
+    used = L.used;
+    ir = L.iret;
     auto store = [&](double* dst, const double* src) {
       if (is_device_ptr(dst)) PB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
       else PB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
@@ -886,8 +1161,8 @@ int dd_krylov(int solver, const parcel_b_input* prm, const parcel_b_crs* A, cons
     sync();
     parcel_b_stats stt;
     memset(&stt, 0, sizeof(stt));
-    stt.setup_s = setup_end - t0;
-    stt.solve_s = now_s() - setup_end;
+    stt.setup_s = L.setup_end - t0;
+    stt.solve_s = now_s() - L.setup_end;
     stt.ilu_nblocks = P.nb;
     set_stats(stt);
     return 0;
@@ -915,19 +1190,29 @@ extern "C" int parcel_b_ddbicgstab(const parcel_b_input* prm, const parcel_b_crs
                    precision_precondition, b_hi, b_lo, x_hi, x_lo, reshistory, niter, iret);
 }
 
+extern "C" int parcel_b_ddgmres(const parcel_b_input* prm, const parcel_b_crs* A, const double* val_lo,
+                                int precision_A, int precision_b, int precision_x, int precision_precondition,
+                                const double* b_hi, const double* b_lo, double* x_hi, double* x_lo,
+                                double* reshistory, int* niter, int* iret) {
+  return dd_krylov(PARCEL_B_SOLVER_GMRES, prm, A, val_lo, precision_A, precision_b, precision_x,
+                   precision_precondition, b_hi, b_lo, x_hi, x_lo, reshistory, niter, iret);
+}
+
 namespace {
 
-// parcel_dd*_c (src/example/c2fortran_kernel.f90:620-799): every argument by reference,
+// parcel_dd*_c (src/example/c2fortran_kernel.f90:620-898): every argument by reference,
 // host arrays, niter in = itrmax and out = iterations.
 void dd_shim(int solver, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo, int32_t* n, int32_t* gn,
              int32_t* nnz, int32_t* istart, double* crsa, double* crsa_lo, int32_t* crsrow_ptr, int32_t* crscol,
              int* ipreflag, int* ilu_method, int* addl, int* iflagas, int* niter, double* rtolmax,
              double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr, int* independ_nvec,
              int* nblock, int* precision_a, int* precision_b, int* precision_x, int* precision_precondition,
-             int* iret) {
+             int* iret, int* restart = nullptr, int* gmres_gsflag = nullptr) {
   parcel_b_input p;
   parcel_b_input_init(&p);
   p.solver = solver;
+  if (restart) p.GMRES_m = *restart;
+  if (gmres_gsflag) p.GMRES_GSflag = *gmres_gsflag;
   p.ipreflag = *ipreflag;
   p.ILU_method = *ilu_method;
   p.addL = *addl;
@@ -976,4 +1261,19 @@ extern "C" void parcel_ddbicgstab_c_(int* icomm, double* vecx, double* vecx_lo, 
   dd_shim(PARCEL_B_SOLVER_BICG, vecx, vecx_lo, vecb, vecb_lo, n, gn, nnz, istart, crsa, crsa_lo, crsrow_ptr,
           crscol, ipreflag, ilu_method, addl, iflagas, niter, rtolmax, reshistory, iovlflag, precon_thblock,
           neuman_itr, independ_nvec, nblock, precision_a, precision_b, precision_x, precision_precondition, iret);
+}
+
+extern "C" void parcel_ddgmres_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo,
+                                  int32_t* n, int32_t* gn, int32_t* nnz, int32_t* istart, double* crsa,
+                                  double* crsa_lo, int32_t* crsrow_ptr, int32_t* crscol, int* ipreflag,
+                                  int* ilu_method, int* addl, int* iflagas, int* niter, double* rtolmax,
+                                  double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                                  int* independ_nvec, int* nblock, int* restart, int* gmres_gsflag,
+                                  int* precision_a, int* precision_b, int* precision_x, int* precision_precondition,
+                                  int* iret) {
+  (void)icomm;
+  dd_shim(PARCEL_B_SOLVER_GMRES, vecx, vecx_lo, vecb, vecb_lo, n, gn, nnz, istart, crsa, crsa_lo, crsrow_ptr,
+          crscol, ipreflag, ilu_method, addl, iflagas, niter, rtolmax, reshistory, iovlflag, precon_thblock,
+          neuman_itr, independ_nvec, nblock, precision_a, precision_b, precision_x, precision_precondition, iret,
+          restart, gmres_gsflag);
 }

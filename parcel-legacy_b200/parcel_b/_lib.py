@@ -103,6 +103,10 @@ SIGNATURES = {
                                       P, P, P, P, IP, IP]),
     "parcel_ddbicgstab_c_": (None, [IP, P, P, P, P, I32P, I32P, I32P, I32P, P, P, P, P, IP, IP, IP, IP, IP, DP, P,
                                     IP, IP, IP, IP, IP, IP, IP, IP, IP, IP]),
+    "parcel_b_ddgmres": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), P, C.c_int, C.c_int, C.c_int, C.c_int, P,
+                                   P, P, P, P, IP, IP]),
+    "parcel_ddgmres_c_": (None, [IP, P, P, P, P, I32P, I32P, I32P, I32P, P, P, P, P, IP, IP, IP, IP, IP, DP, P,
+                                 IP, IP, IP, IP, IP, IP, IP, IP, IP, IP, IP, IP]),
     "parcel_b_bench_kernels": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, DP, DP]),
     "parcel_b_learned_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(P)]),
     "parcel_b_learned_destroy": (C.c_int, [P]),

@@ -175,13 +175,20 @@ def ddbicgstab(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, **kw):
     return ddcg(A, b_hi, b_lo, x0_hi, x0_lo, solver=2, **kw)
 
 
+def ddgmres(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, **kw):
+    """The double-double GMRES(m) (ddKSP_pGMRES; GMRES_m and GMRES_GSflag as for solve);
+    arguments and result as ddcg."""
+    return ddcg(A, b_hi, b_lo, x0_hi, x0_lo, solver=3, **kw)
+
+
 def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=None, rowptr=None, col=None, val=None,
          precision_A=2, precision_b=2, precision_x=2, precision_precondition=2, solver=1, **options):
-    """PARCEL_ddKSP_CRS: the double-double PCG (solver=1) or BiCGStab (solver=2) on the GPU.
+    """PARCEL_ddKSP_CRS: the double-double PCG (solver=1), BiCGStab (solver=2) or GMRES(m)
+    (solver=3) on the GPU.
     Vectors and the matrix's low parts as numpy arrays (host) or CUDA tensors (device).
     Returns a dict with x_hi, x_lo, reshistory, niter, iret and the library's statistics."""
     L = load()
-    fn = L.parcel_b_ddbicgstab if solver == 2 else L.parcel_b_ddcg
+    fn = {2: L.parcel_b_ddbicgstab, 3: L.parcel_b_ddgmres}.get(solver, L.parcel_b_ddcg)
     p = new_input(**options)
     S = crs_struct(A, rowptr, col, val)
     on_dev = hasattr(b_hi, "is_cuda") and b_hi.is_cuda

@@ -146,3 +146,67 @@ def test_ddbicgstab_precision_flags_and_shim():
                                      I(2000), I(2), I(2), I(2), I(1), C.byref(ir))
     assert ir.value == 0 and it.value == niter
     assert np.array_equal(x, xh) and np.array_equal(xl2, xl)
+
+
+GM_CASES = [
+    dict(GMRES_GSflag=1, ipreflag=2, ILU_method=1, precon_thblock=8),
+    dict(GMRES_GSflag=2, ipreflag=2, ILU_method=2, precon_thblock=5),
+    dict(GMRES_GSflag=1, ipreflag=1),
+    dict(GMRES_GSflag=2, ipreflag=0),
+]
+
+
+@pytest.mark.parametrize("case", GM_CASES, ids=["mgs-dilu-ilud-8", "cgs-dilu-mlud-5", "mgs-point-jacobi",
+                                                "cgs-none"])
+def test_ddgmres_matches_oracle_bit_for_bit(case):
+    """ddKSP_pGMRES(10) on a nonsymmetric 3D convection-diffusion matrix, several restarts."""
+    from parcel_b import api
+    A, b = _convdiff(18, 8)
+    kw = dict(itrmax=400, rtolmax=1e-12, GMRES_m=10, **case)
+    g = api.ddgmres(A, b, **kw)
+    xh, xl, h, niter, iret = oracle.ddcg(A, b, solver=3, **kw)
+    assert g["iret"] == iret == 0
+    assert g["niter"] == niter
+    assert np.array_equal(g["reshistory"], h)
+    assert np.array_equal(g["x_hi"], xh) and np.array_equal(g["x_lo"], xl)
+
+
+@pytest.mark.parametrize("itrmax,want_iret", [(23, 0), (1, 1)], ids=["inside-a-cycle", "itrmax-1"])
+def test_ddgmres_iteration_limit_and_precision_flags(itrmax, want_iret):
+    """The reference's itrmax handling: the stop at itr + inner == itrmax keeps iret 0; with
+    itrmax = 1 that stop cannot fire, the first cycle runs all m steps and iret is 1.  A and
+    M in double, b and x in double-double."""
+    from parcel_b import api
+    A, b = _convdiff(14, 9)
+    alo, blo = _lo(A.val, 10), _lo(b, 11)
+    kw = dict(itrmax=itrmax, rtolmax=1e-14, GMRES_m=8, GMRES_GSflag=1, ipreflag=2, ILU_method=1,
+              precon_thblock=4)
+    g = api.ddgmres(A, b, b_lo=blo, val_lo=alo, precision_A=1, precision_b=2, precision_x=2,
+                    precision_precondition=1, **kw)
+    xh, xl, h, niter, iret = oracle.ddcg(A, b, solver=3, b_lo=blo, a_lo=alo, prec_A=1, prec_M=1, **kw)
+    assert g["iret"] == iret == want_iret and g["niter"] == niter == itrmax
+    assert np.array_equal(g["reshistory"], h)
+    assert np.array_equal(g["x_hi"], xh) and np.array_equal(g["x_lo"], xl)
+
+
+def test_ddgmres_c_shim_matches_native_entry():
+    """parcel_ddgmres_c_ (restart and Gram-Schmidt flag after nblock) equals parcel_b_ddgmres."""
+    from parcel_b import _lib, api
+    A, b = _convdiff(12, 12)
+    n = A.n
+    ref = api.ddgmres(A, b, itrmax=300, rtolmax=1e-11, GMRES_m=12, GMRES_GSflag=2, ipreflag=2, ILU_method=1,
+                      precon_thblock=4)
+    x, xl, blo = np.zeros(n), np.zeros(n), np.zeros(n)
+    alo = np.zeros(A.nnz)
+    hist = np.zeros(300)
+    I = lambda v: C.byref(C.c_int(v))
+    i32 = lambda v: C.byref(C.c_int32(v))
+    it, ir = C.c_int(300), C.c_int(0)
+    ptr = lambda a: a.ctypes.data
+    _lib.load().parcel_ddgmres_c_(I(0), ptr(x), ptr(xl), ptr(b), ptr(blo), i32(n), i32(n), i32(A.nnz), i32(1),
+                                  ptr(A.val), ptr(alo), ptr(A.rowptr), ptr(A.col), I(2), I(1), I(0), I(1),
+                                  C.byref(it), C.byref(C.c_double(1e-11)), ptr(hist), I(0), I(4), I(1), I(1),
+                                  I(2000), I(12), I(2), I(2), I(2), I(2), I(2), C.byref(ir))
+    assert ir.value == 0 and it.value == ref["niter"]
+    assert np.array_equal(x, ref["x_hi"]) and np.array_equal(xl, ref["x_lo"])
+    assert np.array_equal(hist[: it.value], ref["reshistory"])
