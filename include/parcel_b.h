@@ -129,6 +129,19 @@ typedef struct parcel_b_crs {
   const double* val;
 } parcel_b_crs;
 
+/* Matrix in DIA format (PARCEL_KSP_DIA, src/wrapper.f90:224-357): val[j*n + k] is the entry
+ * of row k (0-based) on diagonal j, whose 1-based global column is k + istart + offset[j];
+ * nnd distinct offsets.  Entries equal to zero, and entries whose column falls outside rows
+ * 1..n, are not part of the matrix. */
+typedef struct parcel_b_dia {
+  int32_t n;
+  int32_t gn;
+  int32_t istart;
+  int32_t nnd;
+  const double* val;
+  const int32_t* offset;
+} parcel_b_dia;
+
 /* Per-solve statistics (extension). */
 typedef struct parcel_b_stats {
   double setup_s;           /* preconditioner + layout setup, wall seconds           */
@@ -163,6 +176,20 @@ int parcel_b_last_stats(parcel_b_stats* out);
  * niter returns the iterations used; iret as described above. */
 int parcel_b_solve(const parcel_b_input* prm, const parcel_b_crs* A, const double* b,
                    double* x, double* reshistory, int* niter, int* iret);
+
+/* PARCEL_KSP_DIA: as parcel_b_solve for a DIA matrix (host or device arrays).  The DIA
+ * arrays become CRS once, on the GPU (each row's nonzero entries in ascending column
+ * order, as dia2crs, src/matrix.f90:7536-7576, gives them for ascending offsets), and the
+ * CRS solve runs on that; the conversion time is part of the setup statistics. */
+int parcel_b_solve_dia(const parcel_b_input* prm, const parcel_b_dia* A, const double* b,
+                       double* x, double* reshistory, int* niter, int* iret);
+/* PARCEL_ddKSP_DIA: the double-double CG / BiCGStab / GMRES (prm->solver 1, 2 or 3) on a
+ * DIA matrix, with the arguments of parcel_b_ddcg (val_lo: the low parts, laid out as
+ * A->val). */
+int parcel_b_ddsolve_dia(const parcel_b_input* prm, const parcel_b_dia* A, const double* val_lo,
+                         int precision_A, int precision_b, int precision_x, int precision_precondition,
+                         const double* b_hi, const double* b_lo, double* x_hi, double* x_lo,
+                         double* reshistory, int* niter, int* iret);
 
 /* ---- drop-in shims, CPU-build ABI (host arrays; src/example/c2fortran_kernel.f90) ----
  * parcel_dcg_c       : c2fortran_kernel.f90:334-432  -> parcel_dcg (wrapper.f90:1995)
@@ -227,6 +254,46 @@ void parcel_ddgmres_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, 
                        int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock, int* restart,
                        int* gmres_gsflag, int* precision_a, int* precision_b, int* precision_x,
                        int* precision_precondition, int* iret);
+/* DIA shims (src/example/c2fortran_kernel.f90:1228-1872): the CRS lists with n, gn, istart,
+ * diaA, offset, nnd in place of n, gn, nnz, istart, crsa, crsrow_ptr, crscol. */
+void parcel_dcg_dia_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int32_t* gn, int32_t* istart,
+                       double* diaA, int32_t* offset, int32_t* nnd, int* ipreflag, int* ilu_method, int* addl,
+                       int* iflagas, int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                       int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock, int* iret);
+void parcel_dbicgstab_dia_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int32_t* gn, int32_t* istart,
+                             double* diaA, int32_t* offset, int32_t* nnd, int* ipreflag, int* ilu_method, int* addl,
+                             int* iflagas, int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                             int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock, int* iret);
+void parcel_dgmres_dia_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int32_t* gn, int32_t* istart,
+                          double* diaA, int32_t* offset, int32_t* nnd, int* ipreflag, int* ilu_method, int* addl,
+                          int* iflagas, int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                          int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock, int* restart,
+                          int* gmres_gsflag, int* iret);
+void parcel_dcagmres_dia_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int32_t* gn, int32_t* istart,
+                            double* diaA, int32_t* offset, int32_t* nnd, int* ipreflag, int* ilu_method, int* addl,
+                            int* iflagas, int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                            int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock,
+                            int* cagmres_sstep, int* cagmres_tstep, int* cagmres_basis, int* cagmres_qrflag,
+                            int* iret);
+void parcel_ddcg_dia_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo, int32_t* n,
+                        int32_t* gn, int32_t* istart, double* diaA, double* diaA_lo, int32_t* offset, int32_t* nnd,
+                        int* ipreflag, int* ilu_method, int* addl, int* iflagas, int* niter, double* rtolmax,
+                        double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                        int* independ_nvec, int* nblock, int* precision_a, int* precision_b, int* precision_x,
+                        int* precision_precondition, int* iret);
+void parcel_ddbicgstab_dia_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo, int32_t* n,
+                              int32_t* gn, int32_t* istart, double* diaA, double* diaA_lo, int32_t* offset,
+                              int32_t* nnd, int* ipreflag, int* ilu_method, int* addl, int* iflagas, int* niter,
+                              double* rtolmax, double* reshistory, int* iovlflag, int* precon_thblock,
+                              int* neuman_itr, int* independ_nvec, int* nblock, int* precision_a, int* precision_b,
+                              int* precision_x, int* precision_precondition, int* iret);
+/* parcel_ddgmres_dia_c has no Neuman_itr argument (c2fortran_kernel.f90:1681-1773). */
+void parcel_ddgmres_dia_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo, int32_t* n,
+                           int32_t* gn, int32_t* istart, double* diaA, double* diaA_lo, int32_t* offset,
+                           int32_t* nnd, int* ipreflag, int* ilu_method, int* addl, int* iflagas, int* niter,
+                           double* rtolmax, double* reshistory, int* iovlflag, int* precon_thblock,
+                           int* independ_nvec, int* nblock, int* restart, int* gmres_gsflag, int* precision_a,
+                           int* precision_b, int* precision_x, int* precision_precondition, int* iret);
 void parcel_dcg_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn,
                        int32_t* nnz, int32_t* istart, void** crsa, void** crsrow_ptr,
                        void** crscol, int* ipreflag, int* ilu_method, int* addl,
@@ -254,6 +321,28 @@ void parcel_dcagmres_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, in
                             int* independ_nvec, int* nblock, int* cagmres_sstep,
                             int* cagmres_tstep, int* cagmres_basis, int* cagmres_qrflag,
                             int* iret);
+/* DIA shims of the CUDA build: vecx, vecb, diaA and offset as device pointers passed by
+ * reference (type(c_ptr) arguments). */
+void parcel_dcg_dia_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn, int32_t* istart,
+                           void** diaA, void** offset, int32_t* nnd, int* ipreflag, int* ilu_method, int* addl,
+                           int* iflagas, int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                           int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock, int* iret);
+void parcel_dbicgstab_dia_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn, int32_t* istart,
+                                 void** diaA, void** offset, int32_t* nnd, int* ipreflag, int* ilu_method,
+                                 int* addl, int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                                 int* iovlflag, int* precon_thblock, int* neuman_itr, int* independ_nvec,
+                                 int* nblock, int* iret);
+void parcel_dgmres_dia_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn, int32_t* istart,
+                              void** diaA, void** offset, int32_t* nnd, int* ipreflag, int* ilu_method, int* addl,
+                              int* iflagas, int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                              int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock, int* restart,
+                              int* gmres_gsflag, int* iret);
+void parcel_dcagmres_dia_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int32_t* gn, int32_t* istart,
+                                void** diaA, void** offset, int32_t* nnd, int* ipreflag, int* ilu_method,
+                                int* addl, int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                                int* iovlflag, int* precon_thblock, int* neuman_itr, int* independ_nvec,
+                                int* nblock, int* cagmres_sstep, int* cagmres_tstep, int* cagmres_basis,
+                                int* cagmres_qrflag, int* iret);
 
 /* ---- split setup / solve (set_ksp_crs_c, start_ksp_solver_crs_c, get_vecx_ksp_crs_c,
  *      get_reshistory_ksp_crs_c: src/example/c2fortran_kernel.f90:2855-2961) ----------

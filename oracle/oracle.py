@@ -183,3 +183,64 @@ class Precon:
         if getattr(self, "h", None):
             lib().orc_precon_destroy(self.h)
             self.h = None
+
+
+# ---------------------------------------------------------------------------------------
+# DIA format (one process, istart = 1).
+
+class _Crs:
+    """Minimal CRS container (1-based rowptr / col) for the oracle's entry points."""
+
+    def __init__(self, n, rowptr, col, val):
+        self.n, self.rowptr, self.col, self.val, self.istart = n, rowptr, col, val, 1
+
+    @property
+    def nnz(self):
+        return int(self.col.shape[0])
+
+
+def crs_to_dia(A, val=None):
+    """get_nnd_crs_without_sort + crs2dia_without_sort (src/matrix.f90:7147-7211, 7494-7534):
+    the distinct offsets col - row in ascending order and dia[j*n + k] = A(k, k + offset[j]),
+    zero where A has no entry.  val replaces A.val (e.g. the low parts of a dd matrix)."""
+    n = int(A.n)
+    rp = np.asarray(A.rowptr, dtype=np.int64) - 1
+    col = np.asarray(A.col, dtype=np.int64) - 1
+    v = np.asarray(A.val if val is None else val, dtype=np.float64)
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(rp))
+    d = col - rows
+    offsets = np.unique(d)
+    j = np.searchsorted(offsets, d)
+    dia = np.zeros(len(offsets) * n)
+    dia[j * n + rows] = v
+    return dia, offsets.astype(np.int32)
+
+
+def dia_to_crs(dia, offset, n, dia_lo=None):
+    """dia2crs (src/matrix.f90:7536-7576) on one process: row k keeps the entries with
+    |a| > minReal8 = 0 (src/type.f90:445), here with the diagonals in ascending offset order
+    so that the columns are sorted; an entry whose column falls outside rows 1..n (a halo
+    column in the reference, zero on one process) is left out.  Returns (CRS, low parts or
+    None)."""
+    dia = np.asarray(dia, dtype=np.float64).reshape(len(offset), n)
+    lo = None if dia_lo is None else np.asarray(dia_lo, dtype=np.float64).reshape(len(offset), n)
+    order = np.argsort(np.asarray(offset), kind="stable")
+    cols, vals, los, rows = [], [], [], []
+    k = np.arange(n, dtype=np.int64)
+    for j in order:
+        c = k + int(offset[j])
+        keep = (c >= 0) & (c < n) & ((np.abs(dia[j]) > 0.0) | ((np.abs(lo[j]) > 0.0) if lo is not None else False))
+        rows.append(k[keep]); cols.append(c[keep]); vals.append(dia[j][keep])
+        if lo is not None:
+            los.append(lo[j][keep])
+    rows, cols, vals = np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
+    perm = np.lexsort((cols, rows))
+    rowptr = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.int32) + 1
+    A = _Crs(n, rowptr, (cols[perm] + 1).astype(np.int32), vals[perm])
+    return A, (np.concatenate(los)[perm] if lo is not None else None)
+
+
+def solve_dia(dia, offset, b, x0=None, **kw):
+    """PARCEL_KSP_DIA: the DIA matrix as dia2crs defines it, solved by the CRS oracle."""
+    A, _ = dia_to_crs(dia, offset, len(b))
+    return solve(A, b, x0, **kw)

@@ -46,6 +46,11 @@ class Crs(C.Structure):
                 ("rowptr", C.c_void_p), ("col", C.c_void_p), ("val", C.c_void_p)]
 
 
+class Dia(C.Structure):
+    _fields_ = [("n", C.c_int32), ("gn", C.c_int32), ("istart", C.c_int32), ("nnd", C.c_int32),
+                ("val", C.c_void_p), ("offset", C.c_void_p)]
+
+
 class Stats(C.Structure):
     _fields_ = [("setup_s", C.c_double), ("solve_s", C.c_double), ("total_s", C.c_double),
                 ("true_relres", C.c_double), ("true_relres_dd", C.c_double),
@@ -107,6 +112,26 @@ SIGNATURES = {
                                    P, P, P, P, IP, IP]),
     "parcel_ddgmres_c_": (None, [IP, P, P, P, P, I32P, I32P, I32P, I32P, P, P, P, P, IP, IP, IP, IP, IP, DP, P,
                                  IP, IP, IP, IP, IP, IP, IP, IP, IP, IP, IP, IP]),
+    "parcel_b_solve_dia": (C.c_int, [C.POINTER(Input), C.POINTER(Dia), P, P, P, IP, IP]),
+    "parcel_b_ddsolve_dia": (C.c_int, [C.POINTER(Input), C.POINTER(Dia), P, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       P, P, P, P, P, IP, IP]),
+    # DIA shims: n, gn, istart, diaA, offset, nnd in place of the CRS arguments
+    "parcel_dcg_dia_c_": (None, [IP, P, P, I32P, I32P, I32P, P, P, I32P] + [IP] * 5 + [DP, P] + [IP] * 6),
+    "parcel_dbicgstab_dia_c_": (None, [IP, P, P, I32P, I32P, I32P, P, P, I32P] + [IP] * 5 + [DP, P] + [IP] * 6),
+    "parcel_dgmres_dia_c_": (None, [IP, P, P, I32P, I32P, I32P, P, P, I32P] + [IP] * 5 + [DP, P] + [IP] * 8),
+    "parcel_dcagmres_dia_c_": (None, [IP, P, P, I32P, I32P, I32P, P, P, I32P] + [IP] * 5 + [DP, P] + [IP] * 10),
+    "parcel_dcg_dia_gpu_c_": (None, [IP, P, P, I32P, I32P, I32P, P, P, I32P] + [IP] * 5 + [DP, P] + [IP] * 6),
+    "parcel_dbicgstab_dia_gpu_c_": (None, [IP, P, P, I32P, I32P, I32P, P, P, I32P] + [IP] * 5 + [DP, P] +
+                                    [IP] * 6),
+    "parcel_dgmres_dia_gpu_c_": (None, [IP, P, P, I32P, I32P, I32P, P, P, I32P] + [IP] * 5 + [DP, P] + [IP] * 8),
+    "parcel_dcagmres_dia_gpu_c_": (None, [IP, P, P, I32P, I32P, I32P, P, P, I32P] + [IP] * 5 + [DP, P] +
+                                   [IP] * 10),
+    "parcel_ddcg_dia_c_": (None, [IP, P, P, P, P, I32P, I32P, I32P, P, P, P, I32P] + [IP] * 5 + [DP, P] +
+                           [IP] * 10),
+    "parcel_ddbicgstab_dia_c_": (None, [IP, P, P, P, P, I32P, I32P, I32P, P, P, P, I32P] + [IP] * 5 + [DP, P] +
+                                 [IP] * 10),
+    "parcel_ddgmres_dia_c_": (None, [IP, P, P, P, P, I32P, I32P, I32P, P, P, P, I32P] + [IP] * 5 + [DP, P] +
+                              [IP] * 11),
     "parcel_b_bench_kernels": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, DP, DP]),
     "parcel_b_learned_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(P)]),
     "parcel_b_learned_destroy": (C.c_int, [P]),

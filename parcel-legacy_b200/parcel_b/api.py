@@ -214,6 +214,61 @@ def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=None, rowptr=None
             "iret": iret.value, "stats": _lib.last_stats()}
 
 
+def dia_struct(val, offset, n):
+    """parcel_b_dia over DIA arrays (numpy or CUDA tensors): val[j*n + k] is row k's entry on
+    the diagonal with column offset offset[j]."""
+    return _lib.Dia(int(n), int(n), 1, int(len(offset)), _ptr(val), _ptr(offset))
+
+
+def solve_dia(val, offset, b, x0=None, **options):
+    """PARCEL_KSP_DIA: as solve, for a matrix in DIA format (val: nnd*n doubles, diagonal
+    after diagonal; offset: nnd int32 column offsets)."""
+    L = load()
+    p = new_input(**options)
+    n = int(b.shape[0])
+    D = dia_struct(val, offset, n)
+    on_dev = hasattr(b, "is_cuda") and b.is_cuda
+    if x0 is None:
+        if on_dev:
+            import torch
+            x = torch.zeros_like(b)
+        else:
+            x = np.zeros(n)
+    else:
+        x = x0.clone() if on_dev else np.array(x0, dtype=np.float64, copy=True)
+    itrmax = p.itrmax if p.itrmax > 0 else 100
+    hist = np.zeros(itrmax)
+    niter, iret = C.c_int(0), C.c_int(0)
+    rc = L.parcel_b_solve_dia(C.byref(p), C.byref(D), _ptr(b), _ptr(x), _ptr(hist), C.byref(niter), C.byref(iret))
+    if rc < 0:
+        raise RuntimeError(f"parcel_b_solve_dia failed: {_lib.last_error()}")
+    return {"x": x, "reshistory": hist[: niter.value].copy(), "niter": niter.value, "iret": iret.value,
+            "stats": _lib.last_stats()}
+
+
+def ddsolve_dia(val, offset, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=None, precision_A=2,
+                precision_b=2, precision_x=2, precision_precondition=2, solver=1, **options):
+    """PARCEL_ddKSP_DIA: the double-double CG (solver=1), BiCGStab (2) or GMRES (3) for a
+    matrix in DIA format; arguments and result as ddcg."""
+    L = load()
+    p = new_input(solver=solver, **options)
+    n = int(b_hi.shape[0])
+    D = dia_struct(val, offset, n)
+    xh = np.zeros(n) if x0_hi is None else np.array(x0_hi, dtype=np.float64, copy=True)
+    xl = np.zeros(n) if x0_lo is None else np.array(x0_lo, dtype=np.float64, copy=True)
+    itrmax = p.itrmax if p.itrmax > 0 else 100
+    hist = np.zeros(itrmax)
+    niter, iret = C.c_int(0), C.c_int(0)
+    opt = lambda v: None if v is None else _ptr(v)
+    rc = L.parcel_b_ddsolve_dia(C.byref(p), C.byref(D), opt(val_lo), precision_A, precision_b, precision_x,
+                                precision_precondition, _ptr(b_hi), opt(b_lo), _ptr(xh), _ptr(xl), _ptr(hist),
+                                C.byref(niter), C.byref(iret))
+    if rc < 0:
+        raise RuntimeError(f"dd DIA solve failed: {_lib.last_error()}")
+    return {"x_hi": xh, "x_lo": xl, "reshistory": hist[: niter.value].copy(), "niter": niter.value,
+            "iret": iret.value, "stats": _lib.last_stats()}
+
+
 class Learned:
     """The learned coarse-grid preconditioner stage (no counterpart in the reference): a
     handle on the network for an nx x ny x nz grid coarsened by ``coarsen``."""

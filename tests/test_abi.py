@@ -23,7 +23,9 @@ def declared_functions():
 def test_header_declares_the_reference_entry_points():
     names = declared_functions()
     for n in ("parcel_dcg_c_", "parcel_dbicgstab_c_", "parcel_dgmres_c_", "parcel_dcagmres_c_",
-              "parcel_init_c_", "parcel_free_c_", "parcel_b_solve"):
+              "parcel_init_c_", "parcel_free_c_", "parcel_b_solve", "parcel_ddcg_c_", "parcel_ddbicgstab_c_",
+              "parcel_ddgmres_c_", "parcel_dcg_dia_c_", "parcel_dbicgstab_dia_c_", "parcel_dgmres_dia_c_",
+              "parcel_dcagmres_dia_c_", "parcel_ddcg_dia_c_", "parcel_ddbicgstab_dia_c_", "parcel_ddgmres_dia_c_"):
         assert n in names
 
 
@@ -40,14 +42,15 @@ def test_ctypes_signatures_cover_the_header():
 def test_struct_layouts_match_c(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "parcel_b.h"\n'
-                   'int main(){printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(parcel_b_input), '
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(parcel_b_input), '
                    'sizeof(parcel_b_stats), sizeof(parcel_b_crs), offsetof(parcel_b_input, rtolmax), '
-                   'offsetof(parcel_b_input, inner_rtol), offsetof(parcel_b_crs, rowptr));return 0;}\n')
+                   'offsetof(parcel_b_input, inner_rtol), offsetof(parcel_b_crs, rowptr), '
+                   'sizeof(parcel_b_dia), offsetof(parcel_b_dia, offset));return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
     want = [C.sizeof(_lib.Input), C.sizeof(_lib.Stats), C.sizeof(_lib.Crs), _lib.Input.rtolmax.offset,
-            _lib.Input.inner_rtol.offset, _lib.Crs.rowptr.offset]
+            _lib.Input.inner_rtol.offset, _lib.Crs.rowptr.offset, C.sizeof(_lib.Dia), _lib.Dia.offset.offset]
     assert [int(v) for v in out] == want
 
 
