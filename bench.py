@@ -518,6 +518,99 @@ def run_ddcg(args):
     print(json.dumps(out))
 
 
+DDG_METRIC = "time to 1e-10 rel. residual (s), double-double GMRES(30) + block-Jacobi D-ILU"
+
+
+def run_ddgmres(args):
+    """Double-double GMRES(30), MGS, block-Jacobi D-ILU (ILUD) with 64 blocks, every
+    PRECISION_* = 2, on the FP64 line's matrix (3D 7-point upwind convection-diffusion
+    128^3, b ~ N(0,1)), rtol 1e-10.  value: the whole parcel_b_ddgmres call with the arrays
+    in HBM (CUDA events on the library stream); e2e: parcel_ddgmres_c_ with pinned host
+    arrays; cpu_baseline: the oracle's restatement of ddKSP_pGMRES on two restart cycles
+    (60 iterations), scaled to the GPU's iteration count.  The reference publishes no time
+    for its dd GMRES."""
+    import torch
+    from parcel_b import _lib, api
+    L = _lib.load()
+    A, b = problem()
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    rp, ci, va, bd = t(A.rowptr), t(A.col), t(A.val), t(b)
+    stream = torch.cuda.ExternalStream(L.parcel_b_get_stream(), device=dev)
+    itrmax = 3000
+    kw = dict(itrmax=itrmax, rtolmax=1e-10, ipreflag=2, ILU_method=1, precon_thblock=NBLOCKS, GMRES_m=GMRES_M,
+              GMRES_GSflag=1)
+
+    def solve_dev():
+        return api.ddgmres(A, bd, rowptr=rp, col=ci, val=va, **kw)
+
+    for _ in range(args.warmup):
+        res = solve_dev()
+    torch.cuda.synchronize()
+    clk = Clocks(0)
+    clk.started()
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = solve_dev()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    clocks = clk.stop()
+    import oracle
+    x = res["x_hi"].cpu().numpy() + res["x_lo"].cpu().numpy()
+    relres = oracle.true_relres(A, b, x)
+    hp = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    h_rp, h_ci, h_va, h_b = hp(A.rowptr), hp(A.col), hp(A.val), hp(b)
+    zeros = lambda m: torch.zeros(m, dtype=torch.float64).pin_memory().numpy()
+    h_x, h_xl, h_bl, h_al = zeros(A.n), zeros(A.n), zeros(A.n), zeros(A.nnz)
+    hist = np.zeros(itrmax)
+    I = lambda v: C.byref(C.c_int(v))
+    i32 = lambda v: C.byref(C.c_int32(v))
+    ptr = lambda a: a.ctypes.data
+
+    def solve_host():
+        h_x[:] = 0.0
+        h_xl[:] = 0.0
+        niter, iret = C.c_int(itrmax), C.c_int(0)
+        L.parcel_ddgmres_c_(I(0), ptr(h_x), ptr(h_xl), ptr(h_b), ptr(h_bl), i32(A.n), i32(A.n), i32(A.nnz), i32(1),
+                            ptr(h_va), ptr(h_al), ptr(h_rp), ptr(h_ci), I(2), I(1), I(0), I(1), C.byref(niter),
+                            C.byref(C.c_double(1e-10)), ptr(hist), I(0), I(NBLOCKS), I(1), I(1), I(2000),
+                            I(GMRES_M), I(1), I(2), I(2), I(2), I(2), C.byref(iret))
+        return niter.value, iret.value
+
+    solve_host()
+    e2e = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        solve_host()
+        e2e.append(time.perf_counter() - t0)
+    out = {"metric": DDG_METRIC, "value": sum(times) / len(times), "unit": "s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "double-double (pairs of f64)", "data": "synthetic",
+           "config": {"workload": f"dd GMRES({GMRES_M}) MGS + block-Jacobi D-ILU (ILUD), {NBLOCKS} blocks, "
+                                  f"3D 7-pt upwind convection-diffusion {N_GRID}^3, b~N(0,1), "
+                                  "PRECISION_A/b/x/PRECONDITION = 2, rtol 1e-10",
+                      "n": A.n, "nnz": A.nnz, "l2": "inputs larger than L2 (dd vectors 34 MB each, basis 1 GB)"},
+           "iterations": res["niter"], "iret": res["iret"], "true_relres": relres,
+           "step_times_s": [round(v, 6) for v in times],
+           "e2e": {"value": sum(e2e) / len(e2e), "unit": "s",
+                   "h2d_bytes_per_step": int(A.rowptr.nbytes + A.col.nbytes + 2 * A.val.nbytes + 4 * A.n * 8),
+                   "d2h_bytes_per_step": int(2 * A.n * 8 + res["niter"] * 8)},
+           "clocks": clocks}
+    if not args.no_cpu_baseline:
+        sample = 2 * GMRES_M
+        t0 = time.perf_counter()
+        _, _, h, niter, iret = oracle.ddcg(A, b, solver=3, **dict(kw, itrmax=sample))
+        el = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": el * res["niter"] / max(niter, 1), "unit": "s", "cores": oracle.num_threads(),
+                               "kind": "port",
+                               "sample": f"the oracle's dd GMRES on the same workload for {niter} iterations "
+                                         f"({el:.1f} s, set-up included), scaled to {res['niter']} iterations"}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -527,9 +620,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels-only", action="store_true")
     ap.add_argument("--ilu-method", type=int, default=0)
-    ap.add_argument("--workload", default="convdiff128", choices=["convdiff128", "vardiff", "ddcg160"],
+    ap.add_argument("--workload", default="convdiff128", choices=["convdiff128", "vardiff", "ddcg160", "ddgmres128"],
                     help="vardiff: the learned-preconditioner comparison; ddcg160: the double-double CG "
-                         "configuration of the reference's dd example (neither is the default line)")
+                         "configuration of the reference's dd example; ddgmres128: the double-double GMRES "
+                         "on the default line's matrix (none of them is the default line)")
     ap.add_argument("--grid", type=int, default=256)
     ap.add_argument("--coarsen", type=int, default=8)
     ap.add_argument("--restart", type=int, default=40)
@@ -542,6 +636,8 @@ def main():
         run_vardiff(args)
     elif args.workload == "ddcg160":
         run_ddcg(args)
+    elif args.workload == "ddgmres128":
+        run_ddgmres(args)
     elif args.kernels_only:
         run_kernels_only(args)
     elif args.impl == "reference":
