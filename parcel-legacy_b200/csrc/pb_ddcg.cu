@@ -89,31 +89,48 @@ __global__ void k_dd_cg_axpy2(int n, const DdScal* sc, double* __restrict__ xh, 
 }
 
 // Dot product in a fixed order: nc = min(32768, n) contiguous chunks in index order, their
-// sums in ng = min(256, nc) contiguous groups in chunk order, the group sums in order.
-__global__ void k_dd_dot_chunks(int64_t n, int nch, const double* __restrict__ xh, const double* __restrict__ xl,
-                                const double* __restrict__ yh, const double* __restrict__ yl, dd* part) {
+// sums in ng = min(256, nc) contiguous groups in chunk order, the group sums in order.  One
+// launch: thread c of the grid sums chunk c; the last CTA to finish (an atomic ticket, no
+// waiting) sums the groups, one thread per group, and thread 0 adds the group sums.  The
+// ticket counter is reset by that CTA for the next dot on the stream.
+__global__ void __launch_bounds__(256) k_dd_dot(int64_t n, int nch, int ngr, const double* __restrict__ xh,
+                                                const double* __restrict__ xl, const double* __restrict__ yh,
+                                                const double* __restrict__ yl, dd* part, unsigned* ticket,
+                                                dd* out) {
+  __shared__ dd grp[kDdGroups];
+  __shared__ bool last;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nch) return;
-  const int64_t lo = n * c / nch, hi = n * (c + 1) / nch;
-  dd s{0.0, 0.0};
-  for (int64_t i = lo; i < hi; ++i) s = dd_add(s, dd_mul(dd{xh[i], xl[i]}, dd{yh[i], yl[i]}));
-  part[c] = s;
-}
-
-__global__ void k_dd_dot_groups(int nch, int ngr, const dd* part, dd* grp) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ngr) return;
-  const int lo = (int)((int64_t)nch * g / ngr), hi = (int)((int64_t)nch * (g + 1) / ngr);
-  dd s{0.0, 0.0};
-  for (int c = lo; c < hi; ++c) s = dd_add(s, part[c]);
-  grp[g] = s;
-}
-
-__global__ void k_dd_dot_final(int ngr, const dd* grp, dd* out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  dd s{0.0, 0.0};
-  for (int g = 0; g < ngr; ++g) s = dd_add(s, grp[g]);
-  *out = s;
+  if (c < nch) {
+    const int64_t lo = n * c / nch, hi = n * (c + 1) / nch;
+    dd s{0.0, 0.0};
+#pragma unroll 4
+    for (int64_t i = lo; i < hi; ++i) s = dd_add(s, dd_mul(dd{xh[i], xl[i]}, dd{yh[i], yl[i]}));
+    part[c] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int g = threadIdx.x;
+  if (g < ngr) {
+    const int lo = (int)((int64_t)nch * g / ngr), hi = (int)((int64_t)nch * (g + 1) / ngr);
+    dd s{0.0, 0.0};
+#pragma unroll 8
+    for (int k = lo; k < hi; ++k) {
+      const double2 v = __ldcg(reinterpret_cast<const double2*>(part + k));
+      s = dd_add(s, dd{v.x, v.y});
+    }
+    grp[g] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    dd s{0.0, 0.0};
+    for (int k = 0; k < ngr; ++k) s = dd_add(s, grp[k]);
+    *out = s;
+    *ticket = 0u;
+  }
 }
 
 enum DdStep { DD_INIT_NORMS = 0, DD_INIT_RHO, DD_ALPHA, DD_RNORM, DD_BETA };
@@ -745,13 +762,13 @@ struct DdSystem {
   const double* al = nullptr;   // null: A's low parts are zero
 };
 
+// part: kDdChunks chunk sums followed by the ticket counter (zero between dots).
 void dd_dot(const DdSystem& S, const double* xh, const double* xl, const double* yh, const double* yl, dd* part,
             dd* out, cudaStream_t st) {
   const int nch = (int)std::min<int64_t>(kDdChunks, std::max(1, S.n));
   const int ngr = std::min(kDdGroups, nch);
-  k_dd_dot_chunks<<<(nch + 255) / 256, 256, 0, st>>>(S.n, nch, xh, xl, yh, yl, part);
-  k_dd_dot_groups<<<(ngr + 255) / 256, 256, 0, st>>>(nch, ngr, part, part + kDdChunks);
-  k_dd_dot_final<<<1, 32, 0, st>>>(ngr, part + kDdChunks, out);
+  k_dd_dot<<<(nch + 255) / 256, 256, 0, st>>>(S.n, nch, ngr, xh, xl, yh, yl, part,
+                                              reinterpret_cast<unsigned*>(part + kDdChunks), out);
 }
 
 void dd_setup_precon(const Options& o, const parcel_b_crs& A, const DdSystem& S, int prec_M, DdPrecon& P) {
