@@ -293,6 +293,49 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def run_reference_dd(args):
+    """Reference arm of the dd workloads: the oracle's restatement of ddKSP_pCG (ddcg160) or
+    ddKSP_pGMRES (ddgmres128) on all host cores, one full solve per step (the reference's
+    Fortran cannot be built here)."""
+    rank, world, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import oracle
+    from parcel_b import problems
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    if args.workload == "ddcg160":
+        A, b, _ = problems.poisson3d_reference(160, 160, 160)
+        kw = dict(solver=1, itrmax=2000, rtolmax=1e-9, ipreflag=2, ILU_method=1, precon_thblock=80)
+        metric, workload = DD_METRIC, ("CG + block-Jacobi D-ILU (ILUD), 80 blocks, 160^3 Poisson (problem.f90), "
+                                       "PRECISION_A/b/x/PRECONDITION = 2, rtol 1e-9")
+    else:
+        A, b = problem()
+        kw = dict(solver=3, itrmax=3000, rtolmax=1e-10, ipreflag=2, ILU_method=1, precon_thblock=NBLOCKS,
+                  GMRES_m=GMRES_M, GMRES_GSflag=1)
+        metric, workload = DDG_METRIC, (f"dd GMRES({GMRES_M}) MGS + block-Jacobi D-ILU (ILUD), {NBLOCKS} blocks, "
+                                        f"3D 7-pt upwind convection-diffusion {N_GRID}^3, b~N(0,1), "
+                                        "PRECISION_A/b/x/PRECONDITION = 2, rtol 1e-10")
+    times, niter, iret = [], 0, 0
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        _, _, _, niter, iret = oracle.ddcg(A, b, **kw)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    value = sum(times) / len(times)
+    out = {"impl": "reference", "metric": metric, "value": value, "unit": "s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "double-double (pairs of f64)", "data": "synthetic",
+           "config": {"workload": workload, "n": A.n, "nnz": A.nnz},
+           "iterations": niter, "iret": iret,
+           "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port",
+                            "sample": "full solves of the same workload by the C++/OpenMP restatement of the "
+                                      "reference's dd solver (its Fortran cannot be built here)"},
+           "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
 def run_kernels_only(args):
     """Times the SpMV and the block-Jacobi ILU(0) application of the benchmark workload
     (CUDA events on the library stream), without solving; used for kernel profiles."""
@@ -632,7 +675,13 @@ def main():
     ap.add_argument("--train-rhs", type=int, default=4)
     ap.add_argument("--train-steps", type=int, default=400)
     args = ap.parse_args()
-    if args.workload == "vardiff":
+    if args.impl == "reference" and args.workload in ("ddcg160", "ddgmres128"):
+        run_reference_dd(args)
+    elif args.impl == "reference" and args.workload == "vardiff":
+        print(json.dumps({"impl": "reference", "unavailable": "the learned preconditioner has no counterpart in "
+                                                              "the reference; its plain-preconditioner arm is part "
+                                                              "of the vardiff line"}))
+    elif args.workload == "vardiff":
         run_vardiff(args)
     elif args.workload == "ddcg160":
         run_ddcg(args)

@@ -51,3 +51,23 @@ def test_reduce_max_single_process_is_identity():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.reduce_max([0.3, 4.0]) == [0.3, 4.0]
+
+
+def test_reference_arm_of_a_workload_without_a_reference_counterpart():
+    """--impl reference prints an 'unavailable' line for the learned-preconditioner workload."""
+    import json
+    import subprocess
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                          "vardiff"], capture_output=True, text=True, timeout=120, check=True).stdout
+    line = json.loads(out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_reference_arm_on_other_ranks_does_no_work():
+    """Under torchrun only rank 0 runs the reference arm; the others exit 0 at once."""
+    import subprocess
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    for wl in ("convdiff128", "ddcg160", "ddgmres128"):
+        r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", wl],
+                           capture_output=True, text=True, timeout=120, env=env)
+        assert r.returncode == 0 and r.stdout.strip() == "", (wl, r.stdout, r.stderr[-500:])
