@@ -59,3 +59,31 @@ def test_input_defaults_are_minus_one():
     for f in ("ipreflag", "ILU_method", "solver", "GMRES_m", "itrmax", "precon_thblock", "independ_nvec"):
         assert getattr(p, f) == -1
     assert p.rtolmax == -1.0
+
+
+def test_fortran_interfaces_match_the_header():
+    """parcel_b_iso.f90 is shipped uncompiled (no Fortran compiler in this image): check that
+    each bind(c) interface has the C declaration's arguments, in order, with matching kinds."""
+    hdr = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    decls = {m.group(1): [a.strip() for a in m.group(2).split(",") if a.strip() and a.strip() != "void"]
+             for m in re.finditer(r"void\s+(parcel_\w+_c_)\s*\(([^)]*)\)", hdr)}
+    src = open(os.path.join(ROOT, "parcel-legacy_b200", "fortran", "parcel_b_iso.f90")).read()
+    src = re.sub(r"&\s*\n\s*", " ", src)
+    stmts = re.findall(r"subroutine\s+(c_\w+)\s*\(([^)]*)\)\s*bind\(c,\s*name=\"(\w+)\"\)", src)
+    stmts += [(n, "", s) for n, s in re.findall(r"subroutine\s+(c_\w+)\s*\(\)\s*bind\(c,\s*name=\"(\w+)\"\)", src)]
+    assert len(stmts) >= 16
+    for name, args, sym in stmts:
+        fargs = [a.strip() for a in args.split(",") if a.strip()]
+        body = re.search(r"subroutine\s+%s\s*\(.*?end subroutine %s" % (name, name), src, flags=re.S).group(0)
+        kinds = {}
+        for kind, names in re.findall(r"(integer\(c_int\)|integer\(c_int32_t\)|real\(c_double\))\s*::\s*([^\n]*)",
+                                      body):
+            for nm in names.split(","):
+                kinds[re.sub(r"\(\*\)", "", nm.strip()).lower()] = kind
+        assert sym in decls, sym
+        assert len(decls[sym]) == len(fargs), sym
+        for ca, fa in zip(decls[sym], fargs):
+            ct = ca.replace(" ", "")
+            want = ("real(c_double)" if ct.startswith("double*") else
+                    "integer(c_int32_t)" if ct.startswith("int32_t*") else "integer(c_int)")
+            assert kinds.get(fa.lower()) == want, (sym, ca, fa, kinds.get(fa.lower()))
