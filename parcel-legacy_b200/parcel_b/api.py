@@ -187,6 +187,12 @@ def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=None, rowptr=None
     (solver=3) on the GPU.
     Vectors and the matrix's low parts as numpy arrays (host) or CUDA tensors (device).
     Returns a dict with x_hi, x_lo, reshistory, niter, iret and the library's statistics."""
+    nnz = int((col if col is not None else A.col).shape[0])
+    _check("b_hi", b_hi, "float64", A.n)
+    _check("b_lo", b_lo, "float64", A.n)
+    _check("x0_hi", x0_hi, "float64", A.n)
+    _check("x0_lo", x0_lo, "float64", A.n)
+    _check("val_lo", val_lo, "float64", nnz)
     L = load()
     fn = {2: L.parcel_b_ddbicgstab, 3: L.parcel_b_ddgmres}.get(solver, L.parcel_b_ddcg)
     p = new_input(**options)
@@ -214,6 +220,18 @@ def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=None, rowptr=None
             "iret": iret.value, "stats": _lib.last_stats()}
 
 
+def _check(name, a, dtype, length=None):
+    """Raises before the library is called when an array has the wrong element type or
+    length (a wrong type would be read as another type by the C side)."""
+    if a is None:
+        return
+    got = str(a.dtype).replace("torch.", "")
+    if got != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {got}")
+    if length is not None and int(a.shape[0]) != int(length):
+        raise ValueError(f"{name} has {int(a.shape[0])} entries, expected {int(length)}")
+
+
 def dia_struct(val, offset, n):
     """parcel_b_dia over DIA arrays (numpy or CUDA tensors): val[j*n + k] is row k's entry on
     the diagonal with column offset offset[j]."""
@@ -223,9 +241,13 @@ def dia_struct(val, offset, n):
 def solve_dia(val, offset, b, x0=None, **options):
     """PARCEL_KSP_DIA: as solve, for a matrix in DIA format (val: nnd*n doubles, diagonal
     after diagonal; offset: nnd int32 column offsets)."""
+    n = int(b.shape[0])
+    _check("offset", offset, "int32")
+    _check("val", val, "float64", len(offset) * n)
+    _check("b", b, "float64")
+    _check("x0", x0, "float64", n)
     L = load()
     p = new_input(**options)
-    n = int(b.shape[0])
     D = dia_struct(val, offset, n)
     on_dev = hasattr(b, "is_cuda") and b.is_cuda
     if x0 is None:
@@ -250,9 +272,14 @@ def ddsolve_dia(val, offset, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=
                 precision_b=2, precision_x=2, precision_precondition=2, solver=1, **options):
     """PARCEL_ddKSP_DIA: the double-double CG (solver=1), BiCGStab (2) or GMRES (3) for a
     matrix in DIA format; arguments and result as ddcg."""
+    n = int(b_hi.shape[0])
+    _check("offset", offset, "int32")
+    _check("val", val, "float64", len(offset) * n)
+    _check("val_lo", val_lo, "float64", len(offset) * n)
+    _check("b_hi", b_hi, "float64")
+    _check("b_lo", b_lo, "float64", n)
     L = load()
     p = new_input(solver=solver, **options)
-    n = int(b_hi.shape[0])
     D = dia_struct(val, offset, n)
     xh = np.zeros(n) if x0_hi is None else np.array(x0_hi, dtype=np.float64, copy=True)
     xl = np.zeros(n) if x0_lo is None else np.array(x0_lo, dtype=np.float64, copy=True)

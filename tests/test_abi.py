@@ -87,3 +87,25 @@ def test_fortran_interfaces_match_the_header():
             want = ("real(c_double)" if ct.startswith("double*") else
                     "integer(c_int32_t)" if ct.startswith("int32_t*") else "integer(c_int)")
             assert kinds.get(fa.lower()) == want, (sym, ca, fa, kinds.get(fa.lower()))
+
+
+def test_python_api_rejects_mistyped_arrays_before_calling_the_library():
+    """Wrong element types or lengths raise in Python; nothing reaches the C side."""
+    import numpy as np
+    from parcel_b import api, problems
+    A = problems.convdiff3d_upwind(4)
+    b = np.ones(A.n)
+    val = np.zeros(7 * A.n)
+    off = np.array([-16, -4, -1, 0, 1, 4, 16], dtype=np.int32)
+    with pytest.raises(TypeError, match="offset must be int32"):
+        api.solve_dia(val, off.astype(np.int64), b)
+    with pytest.raises(ValueError, match="val has"):
+        api.solve_dia(val[:-1], off, b)
+    with pytest.raises(TypeError, match="b must be float64"):
+        api.solve_dia(val, off, b.astype(np.float32))
+    with pytest.raises(ValueError, match="val_lo has"):
+        api.ddsolve_dia(val, off, b, val_lo=np.zeros(3))
+    with pytest.raises(ValueError, match="val_lo has"):
+        api.ddcg(A, b, val_lo=np.zeros(A.nnz + 1))
+    with pytest.raises(TypeError, match="b_lo must be float64"):
+        api.ddgmres(A, b, b_lo=np.zeros(A.n, dtype=np.float32))
