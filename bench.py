@@ -216,7 +216,8 @@ def run_ours(args):
     spmv_bytes = 12 * A.nnz + 4 * (A.n + 1) + 16 * A.n
     achieved = spmv_bytes / (ms_spmv.value * 1e-3) / 1e9
     # DRAM bytes (read + write) of one k_spmv_sell launch on this workload, from one
-    # `ncu --set full -k regex:k_spmv_sell -s 1 -c 1` capture of `bench.py --kernels-only`:
+    # `ncu --set full --clock-control none -k regex:k_spmv_sell -s 1 -c 1` capture of
+    # `bench.py --kernels-only`:
     # dram__bytes_read.sum 196.24 MB + dram__bytes_write.sum 5.30 MB (cold cache).
     spmv_traffic = 196.237568e6 + 5.297664e6
 

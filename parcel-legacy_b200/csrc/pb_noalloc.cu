@@ -4,8 +4,10 @@
 // host application that has already carved up the GPU with its own memory pool, code
 // running where cudaMalloc is forbidden or would synchronise the device at a bad moment
 // (inside a larger asynchronous pipeline), or a caller that must not fail on a full GPU.
-// parcel_b_dot_noalloc computes the same deterministic dot product as parcel_b_dot, but
-// its scratch (one partial sum per block and the block-completion ticket) lives in a
+// parcel_b_dot_noalloc sums the same FP64 products as parcel_b_dot, in a different fixed
+// order (16,384 elements per block instead of parcel_b_dot's grid), so its result is
+// deterministic for a given n but may differ from parcel_b_dot's in the last bits.  Its
+// scratch (one partial sum per block and the block-completion ticket) lives in a
 // file-scope device array that exists for as long as the library is loaded.  It calls
 // neither cudaMalloc nor cudaFree nor any allocating library routine, and it does not
 // create a stream: it launches on the stream the caller passes.
@@ -105,9 +107,15 @@ extern "C" int parcel_b_dot_noalloc(int64_t n, const double* x, const double* y,
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (e != cudaSuccess) {
     set_last_error(PARCEL_B_E_CUDA, "parcel_b_dot_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
     return PARCEL_B_E_CUDA;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_last_error(PARCEL_B_E_UNSUPPORTED,
+                   "parcel_b_dot_noalloc: device %d exceeds the %d devices its scratch table covers",
+                   dev, kMaxDevices);
+    return PARCEL_B_E_UNSUPPORTED;
   }
   double* scratch = nullptr;
   {

@@ -230,6 +230,9 @@ def _check(name, a, dtype, length=None):
         raise TypeError(f"{name} must be {dtype}, got {got}")
     if length is not None and int(a.shape[0]) != int(length):
         raise ValueError(f"{name} has {int(a.shape[0])} entries, expected {int(length)}")
+    dense = a.is_contiguous() if hasattr(a, "is_contiguous") else bool(a.flags.c_contiguous)
+    if not dense:
+        raise ValueError(f"{name} must be contiguous (the library reads it as a dense array)")
 
 
 def dia_struct(val, offset, n):
@@ -278,6 +281,8 @@ def ddsolve_dia(val, offset, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=
     _check("val_lo", val_lo, "float64", len(offset) * n)
     _check("b_hi", b_hi, "float64")
     _check("b_lo", b_lo, "float64", n)
+    _check("x0_hi", x0_hi, "float64", n)
+    _check("x0_lo", x0_lo, "float64", n)
     L = load()
     p = new_input(solver=solver, **options)
     D = dia_struct(val, offset, n)

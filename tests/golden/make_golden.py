@@ -3,7 +3,7 @@
 Run once in a checkout that has the reference mounted (it reads the reference's text
 output files; nothing here executes reference code):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference checkout>
 
 Writes tests/golden/reference_templates.json.  The fixtures are the reference's only
 known-answer outputs for this path (src/example/template_cpu/STDOUT_run,
@@ -79,4 +79,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the reference checkout>")
+    main(sys.argv[1])

@@ -64,6 +64,26 @@ def test_noalloc_dot_matches_dot_twice(torch_cuda, n):
     assert abs(got2 - ref2) <= RTOL * ref2
 
 
+def test_noalloc_dot_leaves_device_memory_unchanged(torch_cuda):
+    """After one warm call (the per-device set-up), further calls change neither the
+    device's free memory nor torch's reserved pool: nothing is allocated."""
+    torch = torch_cuda
+    L = _lib.load()
+    n = 3_000_017
+    x = torch.randn(n, dtype=torch.float64, device="cuda")
+    res = torch.zeros(1, dtype=torch.float64, device="cuda")
+    _dot_noalloc(L, torch, x, x, res)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    reserved0 = torch.cuda.memory_reserved()
+    for _ in range(5):
+        _dot_noalloc(L, torch, x, x, res)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert torch.cuda.memory_reserved() == reserved0
+
+
 def test_noalloc_dot_exact_on_integers(torch_cuda):
     torch = torch_cuda
     L = _lib.load()
