@@ -457,6 +457,133 @@ __global__ void k_ilu_pack(const IluChunk* __restrict__ ch, int nchunks,
   }
 }
 
+// ------------------------------------------------------------------ grouped sweep
+// The fast sweep streams GROUPS of consecutive chunks (levels, or 512-row pieces of a
+// level) of one block: one bulk copy of the group's packed record plus one of its slice of
+// the input vector fills one shared-memory stage, so the consumers wait on a stage
+// barrier once per group and, between levels, pass only the level barrier.  The rows of a
+// group are contiguous in the permuted layout ([sstart, sstart + sspan)).  Group record:
+//   int4 hdr              {nchunks, sstart, sspan, 0}
+//   int4 cd[kGrpMax][2]   per chunk in sweep order: {rec, w, ring, gs}, {xin, 0, 0, 0}:
+//                         stage byte offsets of the first row's row record and input
+//                         value, rows, ring byte offset of the first row, permuted
+//                         position of the first row
+//   row records           one per position of the span, `stride` bytes apart:
+//                           T dg        1/U_kk or D^-1 (backward sweep, forward D-ILU only)
+//                           T val[K]    coupled coefficients in the reference's order
+//                           u16 slot[K] ring byte offsets of the coupled rows (the ring's
+//                                       zero slot for padding)
+//                         padded to an odd number of T-sized words, so that the 32 lanes
+//                         of a warp reading consecutive records hit distinct banks.
+// The stage holds T xin[sspan] (the input slice) after the records, 16-byte aligned.
+// Positions without a row (level padding) have zero records.
+constexpr int kGrpMax = 15;
+constexpr int kGrpHdr = 512;   // 16 + kGrpMax * 32, rounded up
+
+__host__ __device__ constexpr int rec_words(int tsize, bool has_dg, int K) {
+  return ((has_dg ? 1 : 0) + K + (2 * K + tsize - 1) / tsize) | 1;
+}
+__host__ __device__ constexpr int rec_stride(int tsize, bool has_dg, int K) {
+  return rec_words(tsize, has_dg, K) * tsize;
+}
+
+// Packs the group records of the grouped sweep (layout above): one CTA per group;
+// gi[g] = {first chunk, end chunk, sstart, sspan}, goff[g] = byte offsets of the forward
+// and backward records.
+template <class T>
+__global__ void k_ilu_pack_grp(const int4* __restrict__ gi, const int64_t* __restrict__ goff, int ngroups,
+                               const IluChunk* __restrict__ ch, const int* __restrict__ blk_lo,
+                               const int* __restrict__ blk_hi, const int* __restrict__ blk_lvl,
+                               const int* __restrict__ lvl_start, const int* __restrict__ rowAt,
+                               const int* __restrict__ pos, const int* __restrict__ lev,
+                               const int* __restrict__ rp, const int* __restrict__ ci, int rbase, int cbase,
+                               const double* __restrict__ vL, const double* __restrict__ vU,
+                               const double* __restrict__ Dinv, int dilu, int W, int maxWp, int K,
+                               unsigned char* packF, unsigned char* packB) {
+  const int sz = (int)sizeof(T);
+  const int zslot = W * maxWp * sz;   // byte offset of the ring's zero slot
+  const int strF = rec_stride(sz, dilu != 0, K), strB = rec_stride(sz, true, K);
+  for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+    const int4 G = gi[g];
+    const int c0 = G.x, c1 = G.y, sstart = G.z, sspan = G.w;
+    const int nch = c1 - c0;
+    const int blk = ch[c0].blk;
+    const int lo = blk_lo[blk], hi = blk_hi[blk];
+    unsigned char* f = packF + goff[2 * g];
+    unsigned char* bk = packB + goff[2 * g + 1];
+    const int xF = kGrpHdr + (int)(((int64_t)sspan * strF + 15) & ~int64_t(15));
+    const int xB = kGrpHdr + (int)(((int64_t)sspan * strB + 15) & ~int64_t(15));
+    for (int t = threadIdx.x; t < kGrpHdr / 16; t += blockDim.x) {
+      int4 hf = make_int4(0, 0, 0, 0), hb = make_int4(0, 0, 0, 0);
+      const int j = (t - 1) >> 1, half = (t - 1) & 1;
+      if (t == 0) {
+        hf = make_int4(nch, sstart, sspan, 0);
+        hb = hf;
+      } else if (j < nch) {
+        const IluChunk& cf = ch[c0 + j];       // forward: increasing level
+        const IluChunk& cb = ch[c1 - 1 - j];   // backward: decreasing level
+        if (half == 0) {
+          hf = make_int4(kGrpHdr + (cf.start - sstart) * strF, cf.w,
+                         ((cf.lvl % W) * maxWp + cf.off_in_level) * sz, cf.start);
+          hb = make_int4(kGrpHdr + (cb.start - sstart) * strB, cb.w,
+                         ((cb.lvl % W) * maxWp + cb.off_in_level) * sz, cb.start);
+        } else {
+          hf = make_int4(xF + (cf.start - sstart) * sz, 0, 0, 0);
+          hb = make_int4(xB + (cb.start - sstart) * sz, 0, 0, 0);
+        }
+      }
+      reinterpret_cast<int4*>(f)[t] = hf;
+      reinterpret_cast<int4*>(bk)[t] = hb;
+    }
+    for (int i = threadIdx.x; i < sspan; i += blockDim.x) {
+      unsigned char* rf = f + kGrpHdr + (size_t)i * strF;
+      unsigned char* rb = bk + kGrpHdr + (size_t)i * strB;
+      for (int o = 0; o < strF; o += 4) *reinterpret_cast<int*>(rf + o) = 0;
+      for (int o = 0; o < strB; o += 4) *reinterpret_cast<int*>(rb + o) = 0;
+      T* valF = reinterpret_cast<T*>(rf + (dilu ? sz : 0));
+      unsigned short* slF = reinterpret_cast<unsigned short*>(rf + (dilu ? sz : 0) + K * sz);
+      T* valB = reinterpret_cast<T*>(rb + sz);
+      unsigned short* slB = reinterpret_cast<unsigned short*>(rb + sz + K * sz);
+      const int nat = rowAt[sstart + i];
+      if (nat < 0) {
+        for (int k = 0; k < K; ++k) { slF[k] = (unsigned short)zslot; slB[k] = (unsigned short)zslot; }
+        continue;
+      }
+      int ia, iz, idg;
+      inblock_range(rp, ci, rbase, cbase, nat, lo, hi, &ia, &iz, &idg);
+      auto slot_of = [&](int cnat) -> int {
+        const int l = lev[cnat];
+        return ((l % W) * maxWp + (pos[cnat] - lvl_start[blk_lvl[blk] + l])) * sz;
+      };
+      // forward: strictly lower in-block entries, increasing column
+      int k = 0;
+      for (int j = ia; j < idg; ++j, ++k) {
+        valF[k] = (T)vL[j];
+        slF[k] = (unsigned short)slot_of(ci[j] - cbase);
+      }
+      for (; k < K; ++k) slF[k] = (unsigned short)zslot;
+      if (dilu) *reinterpret_cast<T*>(rf) = (T)Dinv[nat];
+      // backward: strictly upper in-block entries; ILU(0) increasing column
+      // (solve_LU_crs), D-ILU decreasing column (solve_ILU_crs runs Ustart down to Uend)
+      k = 0;
+      if (!dilu) {
+        for (int j = idg + 1; j < iz; ++j, ++k) {
+          valB[k] = (T)vU[j];
+          slB[k] = (unsigned short)slot_of(ci[j] - cbase);
+        }
+        *reinterpret_cast<T*>(rb) = (T)(1.0 / vU[idg]);   // reciprocal of U_kk: the sweep multiplies
+      } else {
+        for (int j = iz - 1; j > idg; --j, ++k) {
+          valB[k] = (T)vU[j];
+          slB[k] = (unsigned short)slot_of(ci[j] - cbase);
+        }
+        *reinterpret_cast<T*>(rb) = (T)Dinv[nat];
+      }
+      for (; k < K; ++k) slB[k] = (unsigned short)zslot;
+    }
+  }
+}
+
 // ------------------------------------------------------------------ the sweep kernel
 constexpr int kIluProducerWarps = 1;
 constexpr int kIluConsumerThreads = 256;
@@ -484,58 +611,132 @@ struct IluSolveArgs {
   int* err;
 };
 
-// Operands of the R rows (p, p + 256, ...) a consumer thread owns in one chunk, staged from
-// shared memory into registers.  Every chunk of a sweep carries exactly KM coupled entries
-// per row (shorter rows are padded with the ring's zero slot), so the loops below have
-// compile-time trip counts.  R > 1 serves levels wider than the 256 consumer threads
-// (up to 1,024 rows: 256^3 grids split into 64 blocks); the rows of a chunk belong to one
-// level and are independent, so one barrier per chunk still suffices.
-template <class T, int KM, int R>
-struct RowOps {
-  T xin[R], dg[R];
-  T val[R][KM];
-  int slot[R][KM];
-  int start, w, rbase;
+constexpr int kBarLevel = 1;                      // consumers, once per chunk
+constexpr int kBarTurn = 2;                       // consumers -> producer: forward sweep written
+constexpr int kBarStage0 = 3;                     // consumers -> producer: stage s free (id 3 + s)
+constexpr int kGrpMaxStages = 12;                 // named barrier ids 3..14
+
+// Producer descriptor of one group: {packed offset / 16, record bytes, first permuted
+// position, vector-slice bytes}.
+struct GrpDesc { int off16, cbytes, start, vbytes; };
+
+template <class T>
+struct GrpArgs {
+  const GrpDesc* tabF;   // per group, forward order
+  const GrpDesc* tabB;   // per group, forward order (the backward sweep walks it backwards)
+  const int* blk_grp;    // nb + 1
+  const unsigned char* packF;
+  const unsigned char* packB;
+  const T* r;
+  T* y;
+  T* s;
+  int stage_bytes, nstages, ring_elems;
+  const int* gate;
+  int* err;
 };
 
+// Operands of the R rows (p, p + NC, ...) a consumer thread owns in one chunk, staged in
+// registers one chunk ahead: coefficients, the input values, the shared-memory addresses
+// of the coupled ring values and of the row's own ring slot, and the output address.
+// Every chunk carries exactly KM coupled entries per row (shorter rows point at the ring's
+// zero slot), so the loops have compile-time trip counts.
 template <class T, int KM, int R>
-__device__ __forceinline__ void load_ops(RowOps<T, KM, R>& o, const unsigned char* sp, int p) {
-  const int4 h0 = *reinterpret_cast<const int4*>(sp);
-  const int rb = *reinterpret_cast<const int*>(sp + 24);
-  o.start = h0.x;
-  o.w = h0.y;
-  o.rbase = rb;
-  const int wpad = h0.z;
-  const T* dg = reinterpret_cast<const T*>(sp + kIluHeader);
-  const T* val = dg + wpad;
-  const int* slot = reinterpret_cast<const int*>(val + KM * wpad);
-  const T* xin = reinterpret_cast<const T*>(slot + KM * wpad);
+struct GOps {
+  T xin[R], dg[R];
+  T val[R][KM];
+  uint32_t gaddr[R][KM];
+  uint32_t waddr;
+  T* gout;
+  int w;
+};
+
+__device__ __forceinline__ void named_bar_arrive(int id, int nthreads) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Shared-memory accesses that the compiler keeps in program order ("memory" clobber): the
+// ring gathers of a level are issued before the next chunk's operand loads, so they do not
+// queue behind them.
+__device__ __forceinline__ double lds_ord(uint32_t a, double) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ float lds_ord(uint32_t a, float) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ void sts(uint32_t a, double v) {
+  asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ void sts(uint32_t a, float v) {
+  asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+
+
+// The K ring byte offsets of a row record, read as whole T-sized words.
+template <class T, int KM>
+__device__ __forceinline__ void load_slots(const unsigned char* sp, uint32_t ring_s, uint32_t (&ga)[KM]) {
+  if constexpr (sizeof(T) == 8) {
+    const unsigned long long* w = reinterpret_cast<const unsigned long long*>(sp);
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int q = p + r * kIluConsumerThreads;
-    if (q < o.w) {
-      o.xin[r] = xin[q];
-      o.dg[r] = dg[q];
+    for (int k0 = 0; k0 < KM; k0 += 4) {
+      const unsigned long long v = w[k0 / 4];
 #pragma unroll
-      for (int k = 0; k < KM; ++k) { o.val[r][k] = val[k * wpad + q]; o.slot[r][k] = slot[k * wpad + q]; }
+      for (int k = k0; k < KM && k < k0 + 4; ++k) ga[k] = ring_s + (uint32_t)((v >> (16 * (k - k0))) & 0xffffu);
+    }
+  } else {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(sp);
+#pragma unroll
+    for (int k0 = 0; k0 < KM; k0 += 2) {
+      const uint32_t v = w[k0 / 2];
+      ga[k0] = ring_s + (v & 0xffffu);
+      if (k0 + 1 < KM) ga[k0 + 1] = ring_s + (v >> 16);
     }
   }
 }
 
-template <class T, bool DILU, bool FWD, int KM, int R>
-__device__ __forceinline__ void solve_rows(const RowOps<T, KM, R>& c, const T* ring, T* ringw, T* vout,
-                                           T* accum, int p) {
-  T dv[R][KM];
-#pragma unroll
-  for (int r = 0; r < R; ++r)
-    if (p + r * kIluConsumerThreads < c.w) {
-#pragma unroll
-      for (int k = 0; k < KM; ++k) dv[r][k] = ring[c.slot[r][k]];
-    }
+template <class T, bool HAS_DG, int KM, int R, int NC>
+__device__ __forceinline__ void gload(GOps<T, KM, R>& o, const unsigned char* sp, int j, int p, uint32_t ring_s,
+                                      T* vout) {
+  constexpr int STR = rec_stride((int)sizeof(T), HAS_DG, KM);
+  constexpr int VOFF = HAS_DG ? (int)sizeof(T) : 0;
+  constexpr int SOFF = VOFF + KM * (int)sizeof(T);
+  const int4 c0 = reinterpret_cast<const int4*>(sp)[1 + 2 * j];
+  const int xoff = reinterpret_cast<const int*>(sp)[4 * (2 + 2 * j)];
+  o.w = c0.y;
+  o.waddr = ring_s + (uint32_t)c0.z + (uint32_t)(p * (int)sizeof(T));
+  o.gout = vout + c0.w + p;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    const int q = p + r * kIluConsumerThreads;
-    if (q >= c.w) continue;
+    const int q = p + r * NC;
+    if (q < o.w) {
+      const unsigned char* rec = sp + c0.x + q * STR;
+      o.xin[r] = *reinterpret_cast<const T*>(sp + xoff + q * (int)sizeof(T));
+      o.dg[r] = HAS_DG ? *reinterpret_cast<const T*>(rec) : T(1);
+#pragma unroll
+      for (int k = 0; k < KM; ++k) o.val[r][k] = reinterpret_cast<const T*>(rec + VOFF)[k];
+      load_slots<T, KM>(rec + SOFF, ring_s, o.gaddr[r]);
+    }
+  }
+}
+
+template <class T, int KM, int R, int NC>
+__device__ __forceinline__ void ggather(const GOps<T, KM, R>& c, int p, T (&dv)[R][KM]) {
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    if (p + r * NC < c.w) {
+#pragma unroll
+      for (int k = 0; k < KM; ++k) dv[r][k] = lds_ord(c.gaddr[r][k], T(0));
+    }
+}
+
+template <class T, bool DILU, bool FWD, int KM, int R, int NC>
+__device__ __forceinline__ void gsolve(const GOps<T, KM, R>& c, const T (&dv)[R][KM], int p) {
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    if (p + r * NC >= c.w) continue;
     T acc = (FWD || !DILU) ? c.xin[r] : T(0);
 #pragma unroll
     for (int k = 0; k < KM; ++k) {
@@ -547,225 +748,158 @@ __device__ __forceinline__ void solve_rows(const RowOps<T, KM, R>& c, const T* r
     if (FWD) out = DILU ? c.dg[r] * acc : acc;
     else if (DILU) out = c.xin[r] - c.dg[r] * acc;
     else out = acc * c.dg[r];
-    ringw[c.rbase + q] = out;
-    vout[c.start + q] = out;
-    if (!FWD && accum) accum[c.start + q] += out;
+    sts(c.waddr + (uint32_t)(r * NC * (int)sizeof(T)), out);
+    c.gout[r * NC] = out;
   }
 }
 
-// Ring-mode consumer loop: chunk i+1's operands are loaded from its stage while chunk i
-// is solved, so after each level barrier only the ring gathers, the multiply-add chain
-// and the stores remain on the critical path.  Two register sets alternate.
-template <class T, bool DILU, bool FWD, int KM, int R>
-__device__ __forceinline__ void consume_pipelined(const IluSolveArgs<T>& a, uint64_t* full,
-                                                  uint64_t* empty, volatile int* sflags,
-                                                  unsigned char* stages, T* ring, int nc, int gbase,
-                                                  int ctid, T* vout) {
+// Consumer side of one sweep over groups [g0, g0 + ng) of the sequence (NG groups over both
+// sweeps).  Per chunk: gather the coupled values from the ring, load the next chunk's
+// operands, finish the rows, and pass the level barrier.  A stage that never landed sets
+// the abort flag; every consumer reads it after the barrier that follows a stage wait, so
+// all return together (`arrived` tells how far each released stages).
+template <class T, bool DILU, bool FWD, int KM, int R, int NC>
+__device__ __forceinline__ void gsweep(const GrpArgs<T>& a, uint64_t* full, volatile int* sflags,
+                                       unsigned char* stages, uint32_t ring_s, int g0, int ng, int NG, int p,
+                                       T* vout, int* arrived) {
+  constexpr bool HAS_DG = DILU || !FWD;
+  constexpr int NT = NC + 32;
   const int NST = a.nstages;
-  RowOps<T, KM, R> A, B;
-  int done = 0;
-  // Stage index and parity of the next chunk to load, advanced by one per chunk (no
-  // division on the per-level path); a stage is released once every consumer holds its
-  // operands in registers.
-  int ls = gbase % NST, lp = (gbase / NST) & 1;
-  auto wait_load = [&](RowOps<T, KM, R>& o, int& rel) -> bool {
-    rel = ls;
-    const bool ok = mbar_wait(&full[ls], lp, kWaitLimit);
-    if (ok) {
-      load_ops<T, KM, R>(o, stages + (size_t)ls * a.stage_bytes, ctid);
-    } else {
-      atomicExch(a.err, 3);
-      sflags[0] = 1;
+  if (ng <= 0) return;
+  int g = g0, st = g0 % NST, ph = (g0 / NST) & 1, j = 0, nch = 0;
+  // Loads the chunk at the cursor into o (waiting for its group's stage when the cursor
+  // has just entered the group), then advances the cursor.  Returns 1 when loaded, 0 at
+  // the end of the sweep (the same for every thread), -1 when the stage did not land.
+  bool entered = false;   // the last next() waited for a stage (the same for every thread)
+  auto next = [&](GOps<T, KM, R>& o) -> int {
+    entered = false;
+    if (g >= g0 + ng) return 0;
+    const unsigned char* sp = stages + (size_t)st * a.stage_bytes;
+    if (j == 0) {
+      entered = true;
+      // warp-uniform outcome, so the aligned barrier instructions below never diverge
+      if (!__all_sync(kFull, mbar_wait(&full[st], ph, kWaitLimit))) {
+        atomicExch(a.err, 3);
+        sflags[0] = 1;
+        return -1;
+      }
+      nch = reinterpret_cast<const int*>(sp)[0];
     }
-    if (++ls == NST) { ls = 0; lp ^= 1; }
-    return ok;
-  };
-  auto release = [&](bool ok, int st) {
-    if (ctid == 0 && ok) mbar_arrive(&empty[st]);
-  };
-  int relA = 0, relB = 0;
-  bool ok = wait_load(A, relA);
-  named_bar_sync(1, kIluConsumerThreads);
-  release(ok, relA);
-  done = 1;
-  if (!sflags[0]) {
-    for (int i = 0; i < nc; i += 2) {
-      // chunk i in A, prefetch i+1 into B
-      bool okB = true;
-      if (i + 1 < nc) okB = wait_load(B, relB);
-      solve_rows<T, DILU, FWD, KM, R>(A, ring, ring, vout, a.accum, ctid);
-      named_bar_sync(1, kIluConsumerThreads);
-      if (i + 1 >= nc || sflags[0]) { done = i + 1; break; }
-      release(okB, relB);
-      // chunk i+1 in B, prefetch i+2 into A
-      bool okA = true;
-      if (i + 2 < nc) okA = wait_load(A, relA);
-      solve_rows<T, DILU, FWD, KM, R>(B, ring, ring, vout, a.accum, ctid);
-      named_bar_sync(1, kIluConsumerThreads);
-      if (i + 2 >= nc || sflags[0]) { done = i + 2; break; }
-      release(okA, relA);
+    gload<T, HAS_DG, KM, R, NC>(o, sp, j, p, ring_s, vout);
+    if (++j == nch) {
+      // every operand of the group is in this thread's registers: release the stage
+      if (g + NST < NG) named_bar_arrive(kBarStage0 + st, NT);
+      *arrived = g + 1;
+      j = 0;
+      ++g;
+      if (++st == NST) { st = 0; ph ^= 1; }
     }
-  }
-  if (ctid == 0) sflags[1] = gbase + done;
-}
-
-// Solves the R rows (p, p + 256, ...) of the staged chunk at sp, reading the operands
-// straight from shared memory: ring slots first, then the coupled values, then the
-// coefficients, so the loads of all R rows are in flight together and few stay live.
-template <class T, bool DILU, bool FWD, int KM, int R>
-__device__ __forceinline__ void solve_rows_direct(const unsigned char* sp, T* ring, T* vout, T* accum, int p) {
-  const int4 h0 = *reinterpret_cast<const int4*>(sp);
-  const int start = h0.x, w = h0.y, wpad = h0.z;
-  const int rbase = *reinterpret_cast<const int*>(sp + 24);
-  const T* dg = reinterpret_cast<const T*>(sp + kIluHeader);
-  const T* val = dg + wpad;
-  const int* slot = reinterpret_cast<const int*>(val + KM * wpad);
-  const T* xin = reinterpret_cast<const T*>(slot + KM * wpad);
+    return 1;
+  };
+  // level barrier; after a stage wait every consumer also reads the abort flag, which a
+  // consumer whose wait failed has set before the barrier
+  auto level_barrier = [&]() -> bool {
+    named_bar_sync(kBarLevel, NC);
+    return !(entered && sflags[0]);
+  };
+  GOps<T, KM, R> A, B;
   T dv[R][KM];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int q = p + r * kIluConsumerThreads;
-    if (q < w) {
-#pragma unroll
-      for (int k = 0; k < KM; ++k) dv[r][k] = ring[slot[k * wpad + q]];
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int q = p + r * kIluConsumerThreads;
-    if (q >= w) continue;
-    T acc = (FWD || !DILU) ? xin[q] : T(0);
-#pragma unroll
-    for (int k = 0; k < KM; ++k) {
-      const T v = val[k * wpad + q];
-      if (FWD) acc = acc - v * dv[r][k];
-      else if (DILU) acc = acc + dv[r][k] * v;
-      else acc = acc - dv[r][k] * v;
-    }
-    T out;
-    if (FWD) out = DILU ? dg[q] * acc : acc;
-    else if (DILU) out = xin[q] - dg[q] * acc;
-    else out = acc * dg[q];
-    ring[rbase + q] = out;
-    vout[start + q] = out;
-    if (!FWD && accum) accum[start + q] += out;
+  int sA = next(A), sB = 0;
+  if (!level_barrier()) return;
+  while (sA > 0) {
+    ggather<T, KM, R, NC>(A, p, dv);
+    sB = next(B);
+    gsolve<T, DILU, FWD, KM, R, NC>(A, dv, p);
+    if (!level_barrier() || sB == 0) return;
+    ggather<T, KM, R, NC>(B, p, dv);
+    sA = next(A);
+    gsolve<T, DILU, FWD, KM, R, NC>(B, dv, p);
+    if (!level_barrier()) return;
   }
 }
 
-// Consumer loop for R > 1: the chunk is solved straight from its stage (no operand copy
-// in registers); the R independent rows of each thread overlap their loads instead.
-template <class T, bool DILU, bool FWD, int KM, int R>
-__device__ __forceinline__ void consume_simple(const IluSolveArgs<T>& a, uint64_t* full, uint64_t* empty,
-                                               volatile int* sflags, unsigned char* stages, T* ring, int nc,
-                                               int gbase, int ctid, T* vout) {
-  const int NST = a.nstages;
-  int done = 0;
-  int st = gbase % NST, ph = (gbase / NST) & 1;
-  for (int i = 0; i < nc; ++i) {
-    const bool ok = mbar_wait(&full[st], ph, kWaitLimit);
-    if (!ok) {
-      atomicExch(a.err, 3);
-      sflags[0] = 1;
-    }
-    named_bar_sync(1, kIluConsumerThreads);
-    if (sflags[0]) { done = i; break; }
-    solve_rows_direct<T, DILU, FWD, KM, R>(stages + (size_t)st * a.stage_bytes, ring, vout, a.accum, ctid);
-    named_bar_sync(1, kIluConsumerThreads);   // the level is in the ring; the stage is free
-    if (ctid == 0) mbar_arrive(&empty[st]);
-    done = i + 1;
-    if (++st == NST) { st = 0; ph ^= 1; }
-  }
-  if (ctid == 0) sflags[1] = gbase + done;
-}
-
-template <class T, bool DILU, int KM, int R>
-__global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve_fast(IluSolveArgs<T> a) {
+template <class T, bool DILU, int KM, int R, int NC>
+__global__ void __launch_bounds__(NC + 32, 1) k_ilu_sweep_grp(GrpArgs<T> a) {
   if (gated(a.gate)) return;
+  constexpr int NT = NC + 32;
   extern __shared__ __align__(128) unsigned char smem[];
   const int NST = a.nstages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-  uint64_t* empty = full + NST;
-  volatile int* sflags = reinterpret_cast<volatile int*>(empty + NST);
-  T* ring = reinterpret_cast<T*>(smem + ((16 * NST + 16 + 127) & ~127));
+  volatile int* sflags = reinterpret_cast<volatile int*>(full + kGrpMaxStages);
+  T* ring = reinterpret_cast<T*>(smem + 128);
   unsigned char* stages =
       reinterpret_cast<unsigned char*>(ring) + (((size_t)a.ring_elems * sizeof(T) + 127) & ~size_t(127));
   const int b = blockIdx.x;
-  const int c0 = a.blk_chunk[b], c1 = a.blk_chunk[b + 1];
-  const int nc = c1 - c0;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const bool producer = warp < kIluProducerWarps;
-  const int ctid = threadIdx.x - 32 * kIluProducerWarps;
-  int issued = 0;
+  const int c0 = a.blk_grp[b], c1 = a.blk_grp[b + 1];
+  const int nGF = c1 - c0, NG = 2 * nGF;
   if (threadIdx.x == 0) {
-    for (int i = 0; i < NST; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
+    for (int i = 0; i < NST; ++i) mbar_init(&full[i], 1);
     sflags[0] = 0;
-    sflags[1] = 0;
     mbar_fence_init();
   }
   for (int i = threadIdx.x; i < a.ring_elems; i += blockDim.x) ring[i] = T(0);
   __syncthreads();
-  for (int phase = 0; phase < 2; ++phase) {
-    const bool fwd = phase == 0;
-    const int gbase = phase * nc;
-    if (producer) {
-      const unsigned char* pack = fwd ? a.packF : a.packB;
-      const T* vin = fwd ? a.r : a.y;
-      const ProdDesc* tab = fwd ? a.tabF : a.tabB;
-      auto fetch = [&](int i) -> ProdDesc {
-        if (i >= nc) return ProdDesc{0, 0, 0, 0};
-        return tab[fwd ? c0 + i : c1 - 1 - i];
-      };
-      ProdDesc cur = fetch(lane);
-      int pst = gbase % NST, puse = gbase / NST;   // stage and reuse count of chunk gbase
-      for (int i0 = 0; i0 < nc; i0 += 32) {
-        ProdDesc nxt = fetch(i0 + 32 + lane);
-        const int kmax = min(32, nc - i0);
-        bool stop = false;
-        for (int k = 0; k < kmax; ++k) {
-          ProdDesc d;
-          d.off16 = __shfl_sync(kFull, cur.off16, k);
-          d.start = __shfl_sync(kFull, cur.start, k);
-          d.cbytes = __shfl_sync(kFull, cur.cbytes, k);
-          d.vbytes = __shfl_sync(kFull, cur.vbytes, k);
-          if (lane == 0) {
-            const int st = pst, use = puse;
-            if (++pst == NST) { pst = 0; ++puse; }
-            if (sflags[0]) {
-              stop = true;
-            } else if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1, kWaitLimit)) {
-              atomicExch(a.err, 2);
-              sflags[0] = 1;
-              stop = true;
-            } else {
-              unsigned char* dst = stages + (size_t)st * a.stage_bytes;
-              mbar_arrive_expect_tx(&full[st], (unsigned)(d.cbytes + d.vbytes));
-              bulk_g2s(dst, pack + (size_t)d.off16 * 16, (unsigned)d.cbytes, &full[st]);
-              bulk_g2s(dst + d.cbytes, vin + d.start, (unsigned)d.vbytes, &full[st]);
-              ++issued;
-            }
-          }
-          stop = __shfl_sync(kFull, stop, 0);
-          if (stop) break;
+  if (threadIdx.x >= NC) {
+    // Producer warp: lane 0 fills stage g % NST with group g once the consumers have
+    // released the stage (named barrier kBarStage0 + stage: a hardware wait, no polling).
+    // A backward group's slice of y can only be copied once the forward sweep has
+    // written it (barrier kBarTurn), so before that only its record is copied.
+    const bool lead = threadIdx.x == NC;
+    int issued = 0;     // groups whose copies were issued
+    bool turned = false;
+    auto desc = [&](int g) -> GrpDesc { return g < nGF ? a.tabF[c0 + g] : a.tabB[c1 - 1 - (g - nGF)]; };
+    auto turn = [&]() {
+      named_bar_sync(kBarTurn, NT);
+      turned = true;
+      if (lead)
+        for (int g = nGF; g < issued; ++g) {
+          const GrpDesc d = desc(g);
+          bulk_g2s(stages + (size_t)(g % NST) * a.stage_bytes + d.cbytes, a.y + d.start, (unsigned)d.vbytes,
+                   &full[g % NST]);
         }
-        if (stop) break;
-        cur = nxt;
+    };
+    for (int g = 0; g < NG; ++g) {
+      if (g == nGF + NST && !turned) turn();
+      if (g >= NST) named_bar_sync(kBarStage0 + g % NST, NT);
+      if (sflags[0]) continue;   // aborted: keep the barrier sequence, issue nothing
+      if (lead) {
+        const GrpDesc d = desc(g);
+        const int st = g % NST;
+        unsigned char* dst = stages + (size_t)st * a.stage_bytes;
+        const bool fwd = g < nGF;
+        mbar_arrive_expect_tx(&full[st], (unsigned)(d.cbytes + d.vbytes));
+        bulk_g2s(dst, (fwd ? a.packF : a.packB) + (size_t)d.off16 * 16, (unsigned)d.cbytes, &full[st]);
+        if (fwd) bulk_g2s(dst + d.cbytes, a.r + d.start, (unsigned)d.vbytes, &full[st]);
+        else if (turned) bulk_g2s(dst + d.cbytes, a.y + d.start, (unsigned)d.vbytes, &full[st]);
       }
-    } else if (nc > 0) {
-      if (R == 1) {
-        if (fwd) consume_pipelined<T, DILU, true, KM, R>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.y);
-        else consume_pipelined<T, DILU, false, KM, R>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.s);
-      } else {
-        if (fwd) consume_simple<T, DILU, true, KM, R>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.y);
-        else consume_simple<T, DILU, false, KM, R>(a, full, empty, sflags, stages, ring, nc, gbase, ctid, a.s);
-      }
-      if (fwd) fence_proxy_async_global();
+      issued = g + 1;
     }
-    __syncthreads();
-    if (sflags[0]) break;
+    if (!turned) turn();
+    // wait (bounded) for the last copy into every stage, so that no bulk copy is still
+    // writing into this CTA's shared memory when it exits
+    if (lead)
+      for (int g = max(0, issued - NST); g < issued; ++g) mbar_wait(&full[g % NST], (g / NST) & 1, kWaitLimit);
+    return;
   }
-  if (sflags[0] && threadIdx.x == 0) {
-    for (int g = sflags[1]; g < issued; ++g) mbar_wait(&full[g % NST], (g / NST) & 1, kWaitLimit);
+  const int p = threadIdx.x;
+  const uint32_t ring_s = smem_u32(ring);
+  int arrived = 0;   // groups (sequence index) whose stage this thread has released
+  gsweep<T, DILU, true, KM, R, NC>(a, full, sflags, stages, ring_s, 0, nGF, NG, p, a.y, &arrived);
+  // forward result written: make it visible to the producer's bulk copies
+  fence_proxy_async_global();
+  if (sflags[0]) {
+    // aborted: complete the producer's barrier sequence (blocking syncs, in its order)
+    for (int g = arrived; g < nGF; ++g)
+      if (g + NST < NG) named_bar_sync(kBarStage0 + g % NST, NT);
+    arrived = max(arrived, nGF);
+    named_bar_sync(kBarTurn, NT);
+  } else {
+    named_bar_arrive(kBarTurn, NT);
+    gsweep<T, DILU, false, KM, R, NC>(a, full, sflags, stages, ring_s, nGF, nGF, NG, p, a.s, &arrived);
   }
+  if (sflags[0])
+    for (int g = arrived; g < NG; ++g)
+      if (g + NST < NG) named_bar_sync(kBarStage0 + g % NST, NT);
 }
 
 template <class T, bool DILU, bool RING>
@@ -929,26 +1063,16 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   D.dilu = ilu_method != 0;
   D.W = P.W;
   D.maxWp = std::max(4, P.maxWp);
-  // chunk byte offsets for this value type; every chunk carries the same number of
-  // coupled entries per row (the matrix-wide maximum, rounded up to a supported count)
+  // every chunk carries the same number of coupled entries per row (the matrix-wide
+  // maximum, rounded up to a supported count)
   std::vector<IluChunk> ch = P.chunks;
-  int kmax = 0;
-  for (const auto& c : ch) kmax = std::max(kmax, std::max(c.KL, c.KU));
+  int kmax = 0, maxw = 0;
+  for (const auto& c : ch) { kmax = std::max(kmax, std::max(c.KL, c.KU)); maxw = std::max(maxw, c.w); }
   int kuni = kmax;
   for (int c : {1, 2, 3, 4, 6, 8})
     if (kmax <= c) { kuni = c; break; }
   for (auto& c : ch) { c.KL = kuni; c.KU = kuni; }
-  int64_t oF = 0, oB = 0;
-  int64_t max_stage = 0;
-  for (auto& c : ch) {
-    c.offF = oF; c.offB = oB;
-    int64_t bf = chunk_bytes<T>(c.wpad, c.KL), bb = chunk_bytes<T>(c.wpad, c.KU);
-    oF += align16(bf); oB += align16(bb);
-    max_stage = std::max(max_stage, std::max(bf, bb) + (int64_t)c.wpad * (int64_t)sizeof(T));
-  }
-  D.packF_bytes = std::max<int64_t>(oF, 16);
-  D.packB_bytes = std::max<int64_t>(oB, 16);
-  D.stage_bytes = (int)((max_stage + 127) & ~int64_t(127));
+  D.K = kuni;
   // shared memory budget: barriers + ring + stages
   int dev_smem = 0;
   PB_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx().device));
@@ -956,24 +1080,94 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   int64_t ring_bytes = ((int64_t)D.W * D.maxWp + 1) * sizeof(T);
   D.ring = ring_bytes <= 64 * 1024;
   int64_t ring_alloc = D.ring ? ((ring_bytes + 127) & ~int64_t(127)) : 0;
-  int nst = 16;
-  auto need = [&](int k) { return (int64_t)((16 * k + 16 + 127) & ~127) + ring_alloc + (int64_t)k * D.stage_bytes; };
-  while (nst > 2 && need(nst) > budget) --nst;
-  PB_CHECK(need(nst) <= budget, PARCEL_B_E_UNSUPPORTED,
-           "block-Jacobi level too wide for shared memory (stage %d bytes)", D.stage_bytes);
-  D.nstages = nst;
-  D.smem_bytes = (int)need(nst);
-  {
-    int maxw = 0;
-    for (const auto& c : ch) maxw = std::max(maxw, c.w);
-    D.fast_rows = maxw <= kIluConsumerThreads ? 1 : maxw <= 2 * kIluConsumerThreads ? 2
-                : maxw <= 4 * kIluConsumerThreads ? 4 : 0;
-    D.fast_km = (D.ring && D.fast_rows > 0 && kuni <= 8) ? kuni : 0;
-  }
-
-  D.chunks.alloc(sizeof(IluChunk) * std::max<size_t>(ch.size(), 1));
-  h2d(D.chunks.p, ch.data(), sizeof(IluChunk) * ch.size());
-  {
+  // consumer threads and rows per thread of the grouped sweep
+  if (maxw <= 128) { D.nc = 128; D.rows = 1; }
+  else if (maxw <= 256) { D.nc = 256; D.rows = 1; }
+  else { D.nc = 256; D.rows = 2; }   // chunks have at most kIluChunk = 512 rows
+  D.grp = D.ring && D.rows > 0 && kuni <= 8;
+  if (D.grp) {
+    // Groups of consecutive chunks of one block, each at most kGrpMax chunks and about a
+    // quarter of the stage budget (a chunk larger than that forms a group of its own).
+    const int64_t sz = sizeof(T);
+    const int64_t strF = rec_stride((int)sz, D.dilu, kuni), strB = rec_stride((int)sz, true, kuni);
+    auto grp_bytes = [&](int64_t span) {   // backward record (the larger) + vector slice
+      return kGrpHdr + ((span * strB + 15) & ~int64_t(15)) + span * sz;
+    };
+        const int64_t target = (budget - 128 - ring_alloc) / 4;
+    std::vector<int4> gi;
+    std::vector<int> blk_grp(P.nb + 1, 0);
+    int64_t max_stage = 0;
+    for (int b = 0; b < P.nb; ++b) {
+      blk_grp[b] = (int)gi.size();
+      int c = P.blk_chunk[b];
+      while (c < P.blk_chunk[b + 1]) {
+        const int sstart = ch[c].start;
+        int e = c + 1;
+        auto span_to = [&](int ce) { return (int64_t)align4(ch[ce - 1].start + ch[ce - 1].w) - sstart; };
+        while (e < P.blk_chunk[b + 1] && e - c < kGrpMax && grp_bytes(span_to(e + 1)) <= target) ++e;
+        const int64_t span = span_to(e);
+        gi.push_back(make_int4(c, e, sstart, (int)span));
+        max_stage = std::max(max_stage, grp_bytes(span));
+        c = e;
+      }
+    }
+    blk_grp[P.nb] = (int)gi.size();
+    const int ng = (int)gi.size();
+    std::vector<int64_t> goff(2 * (size_t)std::max(ng, 1), 0);
+    std::vector<GrpDesc> tf(ng), tb(ng);
+    int64_t oF = 0, oB = 0;
+    for (int g = 0; g < ng; ++g) {
+      const int64_t span = gi[g].w;
+      const int64_t cbF = kGrpHdr + ((span * strF + 15) & ~int64_t(15));
+      const int64_t cbB = kGrpHdr + ((span * strB + 15) & ~int64_t(15));
+      goff[2 * g] = oF;
+      goff[2 * g + 1] = oB;
+      PB_CHECK(oF / 16 < INT32_MAX && oB / 16 < INT32_MAX, PARCEL_B_E_UNSUPPORTED,
+               "packed preconditioner larger than 32 GiB");
+      tf[g] = GrpDesc{(int)(oF / 16), (int)cbF, gi[g].z, (int)(span * sz)};
+      tb[g] = GrpDesc{(int)(oB / 16), (int)cbB, gi[g].z, (int)(span * sz)};
+      oF += align16(cbF);
+      oB += align16(cbB);
+    }
+    D.packF_bytes = std::max<int64_t>(oF, 16);
+    D.packB_bytes = std::max<int64_t>(oB, 16);
+    D.stage_bytes = (int)((max_stage + 127) & ~int64_t(127));
+    const int64_t room = budget - 128 - ring_alloc;
+    D.nstages = (int)std::min<int64_t>(kGrpMaxStages, room / D.stage_bytes);
+    PB_CHECK(D.nstages >= 2, PARCEL_B_E_UNSUPPORTED,
+             "block-Jacobi level too wide for shared memory (stage %d bytes)", D.stage_bytes);
+    D.smem_bytes = (int)(128 + ring_alloc + (int64_t)D.nstages * D.stage_bytes);
+    D.ngroups = ng;
+    D.tabF.alloc(sizeof(GrpDesc) * std::max(ng, 1));
+    D.tabB.alloc(sizeof(GrpDesc) * std::max(ng, 1));
+    h2d(D.tabF.p, tf.data(), sizeof(GrpDesc) * ng);
+    h2d(D.tabB.p, tb.data(), sizeof(GrpDesc) * ng);
+    D.blk_grp.alloc(sizeof(int) * (P.nb + 1));
+    h2d(D.blk_grp.p, blk_grp.data(), sizeof(int) * (P.nb + 1));
+    D.ginfo.alloc(sizeof(int4) * std::max(ng, 1));
+    h2d(D.ginfo.p, gi.data(), sizeof(int4) * ng);
+    D.goff.alloc(sizeof(int64_t) * goff.size());
+    h2d(D.goff.p, goff.data(), sizeof(int64_t) * goff.size());
+  } else {
+    // per-chunk records for the general sweep
+    int64_t oF = 0, oB = 0;
+    int64_t max_stage = 0;
+    for (auto& c : ch) {
+      c.offF = oF; c.offB = oB;
+      int64_t bf = chunk_bytes<T>(c.wpad, c.KL), bb = chunk_bytes<T>(c.wpad, c.KU);
+      oF += align16(bf); oB += align16(bb);
+      max_stage = std::max(max_stage, std::max(bf, bb) + (int64_t)c.wpad * (int64_t)sizeof(T));
+    }
+    D.packF_bytes = std::max<int64_t>(oF, 16);
+    D.packB_bytes = std::max<int64_t>(oB, 16);
+    D.stage_bytes = (int)((max_stage + 127) & ~int64_t(127));
+    int nst = 16;
+    auto need = [&](int k) { return (int64_t)((16 * k + 16 + 127) & ~127) + ring_alloc + (int64_t)k * D.stage_bytes; };
+    while (nst > 2 && need(nst) > budget) --nst;
+    PB_CHECK(need(nst) <= budget, PARCEL_B_E_UNSUPPORTED,
+             "block-Jacobi level too wide for shared memory (stage %d bytes)", D.stage_bytes);
+    D.nstages = nst;
+    D.smem_bytes = (int)need(nst);
     std::vector<ProdDesc> tf(ch.size()), tb(ch.size());
     for (size_t i = 0; i < ch.size(); ++i) {
       const IluChunk& c = ch[i];
@@ -989,6 +1183,8 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
     h2d(D.tabF.p, tf.data(), sizeof(ProdDesc) * ch.size());
     h2d(D.tabB.p, tb.data(), sizeof(ProdDesc) * ch.size());
   }
+  D.chunks.alloc(sizeof(IluChunk) * std::max<size_t>(ch.size(), 1));
+  h2d(D.chunks.p, ch.data(), sizeof(IluChunk) * ch.size());
   D.blk_chunk.alloc(sizeof(int) * (P.nb + 1));
   h2d(D.blk_chunk.p, P.blk_chunk.data(), sizeof(int) * (P.nb + 1));
   DBuf blo(sizeof(int) * P.nb), bhi(sizeof(int) * P.nb);
@@ -1024,12 +1220,20 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   trace_mark("ilu: factor");
   D.packF.alloc(D.packF_bytes);
   D.packB.alloc(D.packB_bytes);
-  k_ilu_pack<T><<<std::min<int>((int)ch.size(), 65535) > 0 ? std::min<int>((int)ch.size(), 65535) : 1,
-                  128, 0, st>>>(
-      dp<IluChunk>(D.chunks), (int)ch.size(), dp<int>(blo), dp<int>(bhi), dp<int>(blvl),
-      dp<int>(lst), d_rowAt, d_pos, d_lev, A.rowptr, A.col, A.rbase, A.cbase, vL, vU,
-      D.dilu ? dp<double>(Di) : nullptr, D.dilu ? 1 : 0, D.ring ? 1 : 0, D.W, D.maxWp,
-      dp<unsigned char>(D.packF), dp<unsigned char>(D.packB));
+  if (D.grp) {
+    k_ilu_pack_grp<T><<<std::max(1, std::min(D.ngroups, 65535)), 256, 0, st>>>(
+        dp<int4>(D.ginfo), dp<int64_t>(D.goff), D.ngroups, dp<IluChunk>(D.chunks), dp<int>(blo), dp<int>(bhi),
+        dp<int>(blvl), dp<int>(lst), d_rowAt, d_pos, d_lev, A.rowptr, A.col, A.rbase, A.cbase, vL, vU,
+        D.dilu ? dp<double>(Di) : nullptr, D.dilu ? 1 : 0, D.W, D.maxWp, D.K, dp<unsigned char>(D.packF),
+        dp<unsigned char>(D.packB));
+  } else {
+    k_ilu_pack<T><<<std::min<int>((int)ch.size(), 65535) > 0 ? std::min<int>((int)ch.size(), 65535) : 1,
+                    128, 0, st>>>(
+        dp<IluChunk>(D.chunks), (int)ch.size(), dp<int>(blo), dp<int>(bhi), dp<int>(blvl),
+        dp<int>(lst), d_rowAt, d_pos, d_lev, A.rowptr, A.col, A.rbase, A.cbase, vL, vU,
+        D.dilu ? dp<double>(Di) : nullptr, D.dilu ? 1 : 0, D.ring ? 1 : 0, D.W, D.maxWp,
+        dp<unsigned char>(D.packF), dp<unsigned char>(D.packB));
+  }
   PB_CUDA(cudaGetLastError());
   D.ytmp.alloc(sizeof(T) * (P.np + 4));
   PB_CUDA(cudaMemsetAsync(D.ytmp.p, 0, sizeof(T) * (P.np + 4), st));
@@ -1052,19 +1256,51 @@ static void launch_ilu(const IluDev<T>& D, const IluSolveArgs<T>& a, cudaStream_
   kern<<<D.nb, kIluThreads, D.smem_bytes, st>>>(a);
 }
 
-template <class T, bool DILU, int KM, int R>
-static void launch_fast(const IluDev<T>& D, const IluSolveArgs<T>& a, cudaStream_t st) {
-  auto kern = k_ilu_solve_fast<T, DILU, KM, R>;
+template <class T, bool DILU, int KM, int R, int NC>
+static void launch_grp(const IluDev<T>& D, const GrpArgs<T>& a, cudaStream_t st) {
+  auto kern = k_ilu_sweep_grp<T, DILU, KM, R, NC>;
   static bool configured = false;
   if (!configured) {
     PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     configured = true;
   }
-  kern<<<D.nb, kIluThreads, D.smem_bytes, st>>>(a);
+  kern<<<D.nb, NC + 32, D.smem_bytes, st>>>(a);
 }
 
 template <class T>
 void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, cudaStream_t st) {
+  if (D.grp && !accum) {
+    GrpArgs<T> g;
+    g.tabF = dp<GrpDesc>(D.tabF);
+    g.tabB = dp<GrpDesc>(D.tabB);
+    g.blk_grp = dp<int>(D.blk_grp);
+    g.packF = dp<unsigned char>(D.packF);
+    g.packB = dp<unsigned char>(D.packB);
+    g.r = r;
+    g.y = dp<T>(D.ytmp);
+    g.s = s;
+    g.stage_bytes = D.stage_bytes;
+    g.nstages = D.nstages;
+    g.ring_elems = D.W * D.maxWp + 1;
+    g.gate = gate;
+    g.err = dp<int>(D.err);
+#define GRP_R(KM_, R_, NC_)                                                                        \
+  if (D.dilu) launch_grp<T, true, KM_, R_, NC_>(D, g, st); else launch_grp<T, false, KM_, R_, NC_>(D, g, st);
+#define GRP(KM_)                                                                                   \
+  case KM_:                                                                                        \
+    if (D.nc == 128) { GRP_R(KM_, 1, 128) }                                                        \
+    else if (D.rows == 1) { GRP_R(KM_, 1, 256) } else { GRP_R(KM_, 2, 256) }                       \
+    break;
+    switch (D.K) {
+      GRP(1) GRP(2) GRP(3) GRP(4) GRP(6) GRP(8)
+      default: PB_CHECK(false, PARCEL_B_E_ARG, "unsupported coupling count %d", D.K);
+    }
+#undef GRP
+#undef GRP_R
+    PB_CUDA(cudaGetLastError());
+    return;
+  }
+  PB_CHECK(!D.grp, PARCEL_B_E_UNSUPPORTED, "accumulating block-Jacobi apply needs the general sweep");
   IluSolveArgs<T> a;
   a.tabF = dp<ProdDesc>(D.tabF);
   a.tabB = dp<ProdDesc>(D.tabB);
@@ -1082,19 +1318,7 @@ void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, 
   a.ring_elems = D.ring ? D.W * D.maxWp + 1 : 0;
   a.gate = gate;
   a.err = dp<int>(D.err);
-#define FAST_R(KM_, R_)                                                                            \
-  if (D.dilu) launch_fast<T, true, KM_, R_>(D, a, st); else launch_fast<T, false, KM_, R_>(D, a, st);
-#define FAST(KM_)                                                                                  \
-  case KM_:                                                                                        \
-    if (D.fast_rows == 1) { FAST_R(KM_, 1) } else if (D.fast_rows == 2) { FAST_R(KM_, 2) }         \
-    else { FAST_R(KM_, 4) }                                                                        \
-    break;
-  if (D.fast_km > 0) {
-    switch (D.fast_km) {
-      FAST(1) FAST(2) FAST(3) FAST(4) FAST(6) FAST(8)
-      default: PB_CHECK(false, PARCEL_B_E_ARG, "unsupported coupling count %d", D.fast_km);
-    }
-  } else if (D.dilu) {
+  if (D.dilu) {
     if (D.ring) launch_ilu<T, true, true>(D, a, st); else launch_ilu<T, true, false>(D, a, st);
   } else {
     if (D.ring) launch_ilu<T, false, true>(D, a, st); else launch_ilu<T, false, false>(D, a, st);

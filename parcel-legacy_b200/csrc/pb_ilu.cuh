@@ -40,7 +40,8 @@ template <class VT>
 void build_sell(const DevMat<double>& A, int np, const int* rowAt_d, const int* pos_d, SellBuf<VT>& buf,
                 DevMat<VT>& M);
 
-// One chunk = up to kIluChunk rows of one wavefront level of one block.
+// One chunk = up to kIluChunk rows of one wavefront level of one block.  Wider levels are
+// split into several chunks (their rows are independent; each chunk is one sweep step).
 struct IluChunk {
   int start;         // permuted position of the first row (multiple of 4)
   int w;             // rows
@@ -51,7 +52,7 @@ struct IluChunk {
   int blk;           // block-Jacobi block
   int64_t offF, offB;   // byte offsets of the packed forward / backward data
 };
-constexpr int kIluChunk = 1024;     // rows per chunk (multiple of 4)
+constexpr int kIluChunk = 512;      // rows per chunk (multiple of 4)
 constexpr int kIluHeader = 32;      // bytes of the per-chunk header in the packed data
 
 // Host-side plan: wavefront levels of every block and the permuted, padded layout.
@@ -78,11 +79,16 @@ struct IluDev {
   int W = 1, maxWp = 0;
   bool ring = true;
   bool dilu = false;
-  int fast_rows = 1;  // rows per consumer thread of the pipelined sweep (1, 2 or 4)
-  int fast_km = 0;  // >0: pipelined ring-mode sweep with at most fast_km couplings per row
+  bool grp = false;  // grouped sweep (ring mode, K <= 8, two stages fit); else the general one
+  int nc = 256;      // consumer threads of the grouped sweep (128 or 256)
+  int rows = 1;      // rows per consumer thread of the grouped sweep (1 or 2)
+  int K = 0;         // coupled entries per row in every record
+  int ngroups = 0;
   int stage_bytes = 0, nstages = 0, smem_bytes = 0;
   DBuf chunks;      // IluChunk[]
-  DBuf tabF, tabB;  // per-chunk producer descriptors
+  DBuf tabF, tabB;  // producer descriptors: per group (grouped sweep) or per chunk
+  DBuf blk_grp;     // int[nb+1]: first group of each block
+  DBuf ginfo, goff; // per group {first chunk, end chunk, sstart, sspan} and record offsets
   DBuf blk_chunk;   // int[nb+1]
   DBuf packF, packB;
   int64_t packF_bytes = 0, packB_bytes = 0;
