@@ -58,6 +58,13 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def config(world):
+    """The workload description both arms print (the reference arm runs the same problem)."""
+    return {"workload": WORKLOAD, "n": 2097152, "nnz": 14581760, "blocks": NBLOCKS, "restart": GMRES_M,
+            "orthogonalization": "MGS", "l2": "inputs larger than L2 (217 MB matrix, 126 MB L2)",
+            "parallelism": f"replicas x{world}"}
+
+
 def problem():
     from parcel_b import problems
     A = problems.convdiff3d_upwind(N_GRID)
@@ -220,14 +227,20 @@ def run_ours(args):
     # `bench.py --kernels-only`:
     # dram__bytes_read.sum 196.24 MB + dram__bytes_write.sum 5.30 MB (cold cache).
     spmv_traffic = 196.237568e6 + 5.297664e6
+    # the step's dominant kernel: the block-Jacobi ILU(0) application (forward + backward
+    # sweep), algorithmic bytes 12 nnz + 8 (n + 1) + 32 n (L and U values and columns, row
+    # pointers, r read, z written twice); DRAM bytes of one k_ilu_sweep_grp launch from one
+    # `ncu --set full --clock-control none -k regex:k_ilu_sweep_grp -s 3 -c 1` capture of
+    # `bench.py --kernels-only --steps 5`: read 199.03 MB + write 23.18 MB.
+    ilu_bytes = 12 * A.nnz + 8 * (A.n + 1) + 32 * A.n
+    ilu_achieved = ilu_bytes / (ms_pre.value * 1e-3) / 1e9
+    ilu_traffic = 199.030784e6 + 23.179264e6
 
     out = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": A.n, "nnz": A.nnz, "blocks": NBLOCKS, "restart": GMRES_M,
-                   "orthogonalization": "MGS", "l2": "inputs larger than L2 (217 MB matrix, 126 MB L2)",
-                   "parallelism": f"replicas x{world}"},
+        "config": config(world),
         "iterations": niter, "iret": iret, "true_relres": relres,
         "step_times_s": [round(t_, 6) for t_ in times],
         "setup_s": stats[-1]["setup_s"], "solve_s": stats[-1]["solve_s"],
@@ -237,17 +250,44 @@ def run_ours(args):
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": int(spmv_traffic), "algorithmic_bytes": int(spmv_bytes),
                      "us_per_launch": ms_spmv.value * 1e3},
+        "roofline_dominant": {"bound": "hbm (the sweep is level-latency bound: 2 x 256 dependent levels per block)",
+                              "kernel": "k_ilu_sweep_grp<double> (block-Jacobi ILU(0) apply, 64 CTAs)",
+                              "achieved": ilu_achieved, "peak": hbm, "unit": "GB/s", "frac": ilu_achieved / hbm,
+                              "peak_kind": peak_kind, "traffic": int(ilu_traffic),
+                              "algorithmic_bytes": int(ilu_bytes), "us_per_launch": ms_pre.value * 1e3,
+                              "launches_per_step": niter - (-niter // GMRES_M)},
         "kernels_us": {"spmv": ms_spmv.value * 1e3, "bj_ilu0_apply": ms_pre.value * 1e3},
         "clocks": clocks,
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
     }
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(A, b)
+    if world == 1 and args.target_rhs > 0:   # one process only: the other ranks would wait on a barrier
+        out["target"] = target_summary(args)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def target_summary(args):
+    """The learned + mixed-precision target on its own workload (256^3 variable-coefficient
+    diffusion), with a reduced number of right-hand sides: seconds per right-hand side of
+    the plain FP64 path, the mixed-precision path without the stage and the learned path."""
+    v = vardiff_compare(args.grid, args.coarsen, args.restart, args.target_rhs, args.target_rhs,
+                        args.target_train_rhs, args.target_train_steps)
+    return {"workload": v["config"]["workload"], "rhs": args.target_rhs,
+            "plain_fp64_s_per_rhs": v["plain_fp64"]["s_per_rhs_amortised"],
+            "mixed_s_per_rhs": v["mixed_no_stage"]["s_per_rhs_amortised"],
+            "learned_s_per_rhs": v["learned"]["s_per_rhs_amortised"],
+            "speedup": v["speedup_vs_plain_fp64"],
+            "iterations": {"plain_fp64": v["plain_fp64"]["iterations"], "mixed": v["mixed_no_stage"]["iterations"],
+                           "learned": v["learned"]["iterations"]},
+            "true_relres_max": {"plain_fp64": v["plain_fp64"]["true_relres_max"],
+                                "mixed": v["mixed_no_stage"]["true_relres_max"],
+                                "learned": v["learned"]["true_relres_max"]},
+            "training": v["training"]}
 
 
 def cpu_baseline(A, b):
@@ -284,7 +324,7 @@ def run_reference(args):
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "n": A.n, "nnz": A.nnz, "blocks": NBLOCKS, "restart": GMRES_M},
+           "config": config(world),
            "iterations": niter,
            "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port",
                             "sample": "full solves of the same workload by the C++/OpenMP restatement of "
@@ -360,7 +400,7 @@ def run_kernels_only(args):
 VD_METRIC = "time-to-1e-10 true rel. residual (s), learned + mixed-precision FGMRES vs plain FP64 PGMRES/BJ-ILU"
 
 
-def run_vardiff(args):
+def vardiff_compare(N, c, m, nr, plain_rhs, train_rhs, train_steps):
     """The learned-preconditioner workload: 3D 7-point variable-coefficient diffusion on an
     N^3 grid (N = 256 by default), coefficient exp(g) with g a Gaussian random field
     (correlation length 8 cells, variance 2, seed 5), harmonic-mean faces; right-hand
@@ -374,7 +414,6 @@ def run_vardiff(args):
     import torch
     from parcel_b import _lib, api, problems
     L = _lib.load()
-    N, c, m = args.grid, args.coarsen, args.restart
     g = problems.gaussian_random_field(N, corr_len=8.0, variance=2.0, seed=5)
     A = problems.vardiff3d(N, np.exp(g))
     dev = torch.device("cuda", 0)
@@ -398,14 +437,13 @@ def run_vardiff(args):
     # training on other right-hand sides
     t0 = time.perf_counter()
     net = api.Learned(N, N, N, c, seed=1)
-    for sd in range(100, 100 + args.train_rhs):
+    for sd in range(100, 100 + train_rhs):
         net.collect(A, problems.rhs_normal(A.n, sd), max_pairs=32, **common)
     t_collect = time.perf_counter() - t0
     t0 = time.perf_counter()
-    f_loss, l_loss = net.train(steps=args.train_steps, batch=4, lr=2e-3, seed=3)
+    f_loss, l_loss = net.train(steps=train_steps, batch=4, lr=2e-3, seed=3)
     t_train = time.perf_counter() - t0
 
-    nr = args.rhs
     B = t(np.stack([problems.rhs_normal(A.n, 1000 + k) for k in range(nr)]))
     X = torch.zeros_like(B)
     it = np.zeros(nr, np.int32)
@@ -454,7 +492,7 @@ def run_vardiff(args):
     fgmres_all(None, 1)
     clk = Clocks(0)
     clk.started()
-    sp = plain_all(min(args.plain_rhs, nr))
+    sp = plain_all(min(plain_rhs, nr))
     sm = fgmres_all(None, 1)
     sl = fgmres_all(net.handle, 1)
     clocks = clk.stop()
@@ -470,9 +508,14 @@ def run_vardiff(args):
            "speedup_vs_plain_fp64": sp["s_per_rhs_amortised"] / sl["s_per_rhs_amortised"],
            "speedup_mixed_vs_plain_fp64": sp["s_per_rhs_amortised"] / sm["s_per_rhs_amortised"],
            "training": {"pairs": net.num_pairs(), "collect_s": t_collect, "train_s": t_train,
-                        "steps": args.train_steps, "loss_first": f_loss, "loss_last": l_loss},
+                        "steps": train_steps, "loss_first": f_loss, "loss_last": l_loss},
            "clocks": clocks}
-    print(json.dumps(out))
+    return out
+
+
+def run_vardiff(args):
+    print(json.dumps(vardiff_compare(args.grid, args.coarsen, args.restart, args.rhs, args.plain_rhs,
+                                     args.train_rhs, args.train_steps)))
 
 
 DD_METRIC = "time to 1e-9 recursive rel. residual (s), double-double PCG + block-Jacobi D-ILU"
@@ -655,6 +698,247 @@ def run_ddgmres(args):
     print(json.dumps(out))
 
 
+
+# ---------------------------------------------------------------- configurations C1, C3, C4
+CFG_METRIC = "time to the configuration's tolerance (s): true rel. residual for GMRES-type solves, recursive for CG"
+
+
+def _cfg(name):
+    """The three further configurations of the hot path, each with its solver options, the
+    reference-facing entry used for the end-to-end time, the kernels that bound it and the
+    oracle solve that times the reference's algorithm on the host."""
+    from parcel_b import problems
+    if name == "poisson2d256":
+        A = problems.poisson2d_5pt(256, 256)
+        b = problems.rhs_uniform(A.n, 1)
+        return dict(A=A, b=b, shim="parcel_dcg", dtype="f64",
+                    workload="PCG FP64 + point Jacobi, 2D 5-pt Poisson 256^2 (4 / -1, Dirichlet), b~U[-1,1), "
+                             "x0=0, rtol 1e-8 (recursive residual)",
+                    opts=dict(solver=1, ipreflag=1, itrmax=5000, rtolmax=1e-8),
+                    shim_args=dict(ipreflag=1, ILU_method=0), kern=dict(ipreflag=1), dominant="spmv",
+                    l2="5.2 MB per SpMV: L2-resident, launch-bound (not scored against HBM)")
+    if name == "aniso192":
+        A = problems.aniso3d(192, k=(1.0, 1e-2, 1e-4))
+        b = problems.rhs_uniform(A.n, 3)
+        opts = dict(solver=1, ipreflag=2, ILU_method=0, precon_thblock=64, itrmax=20000, rtolmax=1e-12,
+                    inner_precision=1, residual_dd=1, inner_rtol=1e-4, max_refine=80)
+        return dict(A=A, b=b, shim=None, dtype="f32 inner / f64 + dd refinement",
+                    workload="mixed precision: FP32 PCG + FP32 block-Jacobi ILU(0) 64 blocks inside FP64 / "
+                             "double-double refinement, anisotropic 7-pt (1, 1e-2, 1e-4) 192^3, b~U[-1,1), "
+                             "stop at FP64 true rel. residual 1e-12",
+                    opts=opts, kern=dict(ipreflag=2, ILU_method=0, precon_thblock=64, inner_precision=1),
+                    dominant="precon", l2="inputs larger than L2 (FP32 matrix 394 MB)")
+    if name == "banded4m":
+        A = problems.banded_random(4_000_000, bandwidth=64, nnz_row=9, seed=4)
+        b = problems.rhs_normal(A.n, 4)
+        return dict(A=A, b=b, shim="parcel_dcagmres", dtype="f64",
+                    workload="CA-GMRES(s=8, t=8: restart 64) FP64, Newton basis with Leja-ordered Ritz shifts, "
+                             "TSQR, point Jacobi, random banded nonsymmetric n=4,000,000 (9 nnz/row in |i-j|<=64, "
+                             "diagonal 1.2 x row abs sum), b~N(0,1), tol 1e-10",
+                    opts=dict(solver=4, CAGMRES_sstep=8, CAGMRES_tstep=8, CAGMRES_basis=1, CAGMRES_QRflag=3,
+                              ipreflag=1, itrmax=3000, rtolmax=1e-10),
+                    shim_args=dict(ipreflag=1, ILU_method=0, CAGMRES_sstep=8, CAGMRES_tstep=8, CAGMRES_basis=1,
+                                   CAGMRES_QRflag=3),
+                    kern=dict(ipreflag=1), dominant="spmv", l2="inputs larger than L2 (512 MB per SpMV)")
+    raise ValueError(name)
+
+
+def _cfg_oracle(name, c, max_s=None):
+    """The reference's algorithm on the host: the C++/OpenMP oracle (PCG, block-Jacobi ILU,
+    point Jacobi) or the numpy CA-GMRES restatement.  Returns (seconds, niter, iret, x,
+    cores, sample)."""
+    import oracle
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    A, b = c["A"], c["b"]
+    if name == "banded4m":
+        import cagmres
+        t0 = time.perf_counter()
+        x, h, niter, iret = cagmres.pcagmres(A, b, s=8, t=8, basis=1, qrflag=3, itrmax=3000, rtolmax=1e-10,
+                                             ipreflag=1)
+        return (time.perf_counter() - t0, niter, iret, x, 1,
+                "one full solve by the numpy restatement of KSP_pCAGMRES (scipy SpMV, one core)")
+    kw = dict(c["opts"])
+    for k in ("inner_precision", "residual_dd", "inner_rtol", "max_refine"):
+        kw.pop(k, None)
+    reps = 20 if name == "poisson2d256" else 1
+    M = oracle.Matrix(A)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        x, h, niter, iret = oracle.solve(M, b, **kw)
+    dt = (time.perf_counter() - t0) / reps
+    what = "FP64 PCG + block-Jacobi ILU(0) to 1e-12" if name == "aniso192" else "PCG + point Jacobi"
+    return (dt, niter, iret, x, cores,
+            f"{reps} full solve(s) by the C++/OpenMP restatement ({what}), mean time per solve")
+
+
+def run_config(args):
+    import torch
+    from parcel_b import _lib, api
+    name = args.workload
+    L = _lib.load()
+    c = _cfg(name)
+    A, b = c["A"], c["b"]
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    rp, ci, va, bd = t(A.rowptr), t(A.col), t(A.val), t(b)
+    stream = torch.cuda.ExternalStream(L.parcel_b_get_stream(), device=dev)
+    itrmax = c["opts"]["itrmax"]
+    hist = np.zeros(itrmax)
+    x = torch.zeros(A.n, dtype=torch.float64, device=dev)
+    S_dev = api.crs_struct(A, rp, ci, va)
+
+    def solve_dev():
+        x.zero_()
+        if c["shim"]:
+            fn = getattr(api, c["shim"])
+            n_, i_ = fn(x, bd, A.n, A.n, A.nnz, 1, va, rp, ci, addL=0, iflagAS=1, itrmax=itrmax,
+                        rtolmax=c["opts"]["rtolmax"], reshistory=hist, **c["shim_args"])
+            return n_, i_, _lib.last_stats()
+        p_ = _lib.new_input(**c["opts"])
+        n_, i_ = C.c_int(0), C.c_int(0)
+        rc_ = L.parcel_b_solve(C.byref(p_), C.byref(S_dev), bd.data_ptr(), x.data_ptr(), hist.ctypes.data,
+                               C.byref(n_), C.byref(i_))
+        assert rc_ == 0, _lib.last_error()
+        return n_.value, i_.value, _lib.last_stats()
+
+    for _ in range(args.warmup):
+        solve_dev()
+    torch.cuda.synchronize()
+    clk = Clocks(0)
+    clk.started()
+    times, stats = [], None
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        niter, iret, stats = solve_dev()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    clocks = clk.stop()
+    xg = x.cpu().numpy()
+    import oracle
+    relres = oracle.true_relres(A, b, xg)
+
+    # end to end: pinned host arrays through the reference-facing entry (the C shim, or
+    # parcel_b_solve for the mixed-precision extension), copies inside the timed region
+    hp = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    h_rp, h_ci, h_va, h_b = hp(A.rowptr), hp(A.col), hp(A.val), hp(b)
+    h_x = torch.zeros(A.n, dtype=torch.float64).pin_memory().numpy()
+
+    def solve_host():
+        h_x[:] = 0.0
+        if c["shim"]:
+            fn = getattr(api, c["shim"])
+            return fn(h_x, h_b, A.n, A.n, A.nnz, 1, h_va, h_rp, h_ci, addL=0, iflagAS=1, itrmax=itrmax,
+                      rtolmax=c["opts"]["rtolmax"], reshistory=hist, **c["shim_args"])
+        Ah = type(A)(n=A.n, rowptr=h_rp, col=h_ci, val=h_va)
+        p_ = _lib.new_input(**c["opts"])
+        n_, i_ = C.c_int(0), C.c_int(0)
+        rc_ = L.parcel_b_solve(C.byref(p_), C.byref(api.crs_struct(Ah)), h_b.ctypes.data, h_x.ctypes.data,
+                               hist.ctypes.data, C.byref(n_), C.byref(i_))
+        assert rc_ == 0, _lib.last_error()
+        return n_.value, i_.value
+
+    solve_host()
+    e2e = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        solve_host()
+        e2e.append(time.perf_counter() - t0)
+
+    # the kernels that bound the iteration (CUDA events on the library stream)
+    ms_spmv, ms_pre = C.c_double(0), C.c_double(0)
+    p = _lib.new_input(**c["kern"])
+    rc = L.parcel_b_bench_kernels(C.byref(p), C.byref(api.crs_struct(A, rp, ci, va)), 50, C.byref(ms_spmv),
+                                  C.byref(ms_pre))
+    assert rc == 0, _lib.last_error()
+    hbm, peak_kind = peaks()
+    f32 = c["kern"].get("inner_precision", 0) == 1
+    vb = 4 if f32 else 8
+    spmv_bytes = (vb + 4) * A.nnz + 4 * (A.n + 1) + 2 * vb * A.n
+    # block-Jacobi ILU: L and U values and columns, row pointers, r read, z written twice
+    pre_bytes = (vb + 4) * A.nnz + 8 * (A.n + 1) + 4 * vb * A.n if c["dominant"] == "precon" else 3 * 8 * A.n
+    if c["dominant"] == "spmv":
+        rk, rb, rt = ("k_spmv_sell<double,double> (sliced-ELLPACK SpMV)", spmv_bytes, ms_spmv.value)
+    else:
+        rk, rb, rt = ("k_ilu_sweep_grp<float> (block-Jacobi ILU(0) forward + backward sweep, FP32)", pre_bytes,
+                      ms_pre.value)
+    ach = rb / (rt * 1e-3) / 1e9
+    value = sum(times) / len(times)
+    out = {"metric": CFG_METRIC, "value": value, "unit": "s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": c["dtype"], "data": "synthetic",
+           "config": {"workload": c["workload"], "n": A.n, "nnz": A.nnz, "l2": c["l2"]},
+           "iterations": niter, "iret": iret, "true_relres": relres,
+           "step_times_s": [round(v, 6) for v in times],
+           "setup_s": stats["setup_s"], "solve_s": stats["solve_s"],
+           "e2e": {"value": sum(e2e) / len(e2e), "unit": "s",
+                   "h2d_bytes_per_step": int(A.rowptr.nbytes + A.col.nbytes + A.val.nbytes + 2 * A.n * 8),
+                   "d2h_bytes_per_step": int(A.n * 8 + itrmax * 8)},
+           "roofline": {"bound": "hbm", "kernel": rk, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                        "frac": ach / hbm, "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes": int(rb),
+                        "us_per_launch": rt * 1e3},
+           "kernels_us": {"spmv": ms_spmv.value * 1e3, "precon_apply": ms_pre.value * 1e3},
+           "clocks": clocks, "gpu_launches": int(stats["kernel_launches"])}
+    if name == "aniso192":
+        out["refine_steps"] = stats["refine_steps"]
+        out["true_relres_dd"] = stats["true_relres_dd"]
+        # the plain FP64 GPU path on the same system, for the mixed-precision gain
+        kw = {k: v for k, v in c["opts"].items() if k not in ("inner_precision", "residual_dd", "inner_rtol",
+                                                                "max_refine")}
+        api.solve(A, bd, rowptr=rp, col=ci, val=va, **kw)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r64 = api.solve(A, bd, rowptr=rp, col=ci, val=va, **kw)
+        e1.record(stream)
+        e1.synchronize()
+        out["plain_fp64_gpu"] = {"s": e0.elapsed_time(e1) / 1e3, "iterations": r64["niter"],
+                                 "true_relres": oracle.true_relres(A, b, r64["x"].cpu().numpy())}
+        # double-double reference solution: the library's dd CG with D-ILU (bit-identical to the
+        # oracle's dd CG in the tests), run to a dd recursive residual of 1e-24
+        rdd = api.ddcg(A, bd, rowptr=rp, col=ci, val=va, itrmax=20000, rtolmax=1e-24, ipreflag=2, ILU_method=1,
+                       precon_thblock=64)
+        xdd_hi, xdd_lo = rdd["x_hi"].cpu().numpy(), rdd["x_lo"].cpu().numpy()
+        scale = np.abs(xdd_hi).max()
+        out["error_vs_dd_reference"] = {
+            "max_abs_rel": float(np.abs((xg - xdd_hi) - xdd_lo).max() / scale),
+            "dd_solve": f"dd CG + D-ILU 64 blocks, {rdd['niter']} iterations, dd recursive residual 1e-24"}
+    if not args.no_cpu_baseline:
+        dt, no, io, xo, cores, sample = _cfg_oracle(name, c)
+        out["cpu_baseline"] = {"value": dt, "unit": "s", "cores": cores,
+                               "kind": "port", "sample": sample + f" ({no} iterations, iret {io})"}
+        out["oracle_iterations"] = no
+        if name == "aniso192":
+            out["error_vs_fp64_oracle"] = {"max_abs_rel": float(np.abs(xg - xo).max() / np.abs(xo).max()),
+                                           "oracle_true_relres": oracle.true_relres(A, b, xo)}
+    print(json.dumps(out))
+
+
+def run_reference_config(args):
+    rank, world, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    name = args.workload
+    c = _cfg(name)
+    times, niter, iret, cores, sample = [], 0, 0, 1, ""
+    for i in range(args.warmup + args.steps):
+        dt, niter, iret, _, cores, sample = _cfg_oracle(name, c)
+        if i >= args.warmup:
+            times.append(dt)
+    value = sum(times) / len(times)
+    out = {"impl": "reference", "metric": CFG_METRIC, "value": value, "unit": "s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": c["workload"], "n": c["A"].n, "nnz": c["A"].nnz, "l2": c["l2"]},
+           "iterations": niter, "iret": iret,
+           "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -664,7 +948,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels-only", action="store_true")
     ap.add_argument("--ilu-method", type=int, default=0)
-    ap.add_argument("--workload", default="convdiff128", choices=["convdiff128", "vardiff", "ddcg160", "ddgmres128"],
+    ap.add_argument("--workload", default="convdiff128",
+                    choices=["convdiff128", "vardiff", "ddcg160", "ddgmres128", "poisson2d256", "aniso192",
+                             "banded4m"],
                     help="vardiff: the learned-preconditioner comparison; ddcg160: the double-double CG "
                          "configuration of the reference's dd example; ddgmres128: the double-double GMRES "
                          "on the default line's matrix (none of them is the default line)")
@@ -675,6 +961,10 @@ def main():
     ap.add_argument("--plain-rhs", type=int, default=16)
     ap.add_argument("--train-rhs", type=int, default=4)
     ap.add_argument("--train-steps", type=int, default=400)
+    ap.add_argument("--target-rhs", type=int, default=2,
+                    help="right-hand sides of the learned-preconditioner target on the default line (0: skip)")
+    ap.add_argument("--target-train-rhs", type=int, default=2)
+    ap.add_argument("--target-train-steps", type=int, default=300)
     args = ap.parse_args()
     if args.impl == "reference" and args.workload in ("ddcg160", "ddgmres128"):
         run_reference_dd(args)
@@ -682,6 +972,11 @@ def main():
         print(json.dumps({"impl": "reference", "unavailable": "the learned preconditioner has no counterpart in "
                                                               "the reference; its plain-preconditioner arm is part "
                                                               "of the vardiff line"}))
+    elif args.workload in ("poisson2d256", "aniso192", "banded4m"):
+        if args.impl == "reference":
+            run_reference_config(args)
+        else:
+            run_config(args)
     elif args.workload == "vardiff":
         run_vardiff(args)
     elif args.workload == "ddcg160":

@@ -415,7 +415,8 @@ int parcel_b_ddgmres(const parcel_b_input* prm, const parcel_b_crs* A, const dou
 /* Kernel timing for benchmarks: builds the solver layout and preconditioner described by
  * prm (setup excluded from the timing), then launches `reps` back-to-back SpMVs and `reps`
  * preconditioner applications on the library stream and returns the mean milliseconds per
- * launch of each, measured with CUDA events on that stream.  Host or device matrix. */
+ * launch of each, measured with CUDA events on that stream.  Host or device matrix.  With
+ * prm->inner_precision = 1 it times the FP32 system of the mixed-precision path. */
 int parcel_b_bench_kernels(const parcel_b_input* prm, const parcel_b_crs* A, int reps,
                            double* ms_spmv, double* ms_precon);
 

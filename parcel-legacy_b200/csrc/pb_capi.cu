@@ -507,34 +507,44 @@ int parcel_b_bench_kernels(const parcel_b_input* prm, const parcel_b_crs* A, int
     validate(A);
     PB_CHECK(reps > 0 && ms_spmv && ms_precon, PARCEL_B_E_ARG, "bad arguments");
     Options o = resolve_options(prm);
-    System<double> S;
-    build_system<double>(o, *A, is_device_ptr(A->val), S);
-    cudaStream_t st = stream();
-    const int np = S.np;
-    DBuf x(sizeof(double) * np), y(sizeof(double) * np);
-    fill(np, dp<double>(x), 1.0, st);
-    PB_CUDA(cudaMemsetAsync(y.p, 0, sizeof(double) * np, st));
-    cudaEvent_t e0, e1;
-    PB_CUDA(cudaEventCreate(&e0));
-    PB_CUDA(cudaEventCreate(&e1));
-    for (int i = 0; i < 3; ++i) spmv<double, double>(S.A, dp<double>(x), dp<double>(y), SPMV_Y, nullptr, nullptr, st);
-    PB_CUDA(cudaEventRecord(e0, st));
-    for (int i = 0; i < reps; ++i)
-      spmv<double, double>(S.A, dp<double>(x), dp<double>(y), SPMV_Y, nullptr, nullptr, st);
-    PB_CUDA(cudaEventRecord(e1, st));
-    PB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    PB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    *ms_spmv = ms / reps;
-    for (int i = 0; i < 3; ++i) S.M.apply(np, dp<double>(y), dp<double>(x), nullptr, st);
-    PB_CUDA(cudaEventRecord(e0, st));
-    for (int i = 0; i < reps; ++i) S.M.apply(np, dp<double>(y), dp<double>(x), nullptr, st);
-    PB_CUDA(cudaEventRecord(e1, st));
-    PB_CUDA(cudaEventSynchronize(e1));
-    PB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    *ms_precon = ms / reps;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    auto run = [&](auto tag) {
+      using T = decltype(tag);
+      System<T> S;
+      build_system<T>(o, *A, is_device_ptr(A->val), S);
+      cudaStream_t st = stream();
+      const int np = S.np;
+      DBuf x(sizeof(T) * np), y(sizeof(T) * np);
+      if constexpr (sizeof(T) == sizeof(double)) {
+        fill(np, dp<double>(x), 1.0, st);
+      } else {
+        DBuf one(sizeof(double) * np);
+        fill(np, dp<double>(one), 1.0, st);
+        convert<T, double>(np, dp<T>(x), dp<double>(one), st);
+      }
+      PB_CUDA(cudaMemsetAsync(y.p, 0, sizeof(T) * np, st));
+      cudaEvent_t e0, e1;
+      PB_CUDA(cudaEventCreate(&e0));
+      PB_CUDA(cudaEventCreate(&e1));
+      for (int i = 0; i < 3; ++i) spmv<T, T>(S.A, dp<T>(x), dp<T>(y), SPMV_Y, nullptr, nullptr, st);
+      PB_CUDA(cudaEventRecord(e0, st));
+      for (int i = 0; i < reps; ++i) spmv<T, T>(S.A, dp<T>(x), dp<T>(y), SPMV_Y, nullptr, nullptr, st);
+      PB_CUDA(cudaEventRecord(e1, st));
+      PB_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      PB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      *ms_spmv = ms / reps;
+      for (int i = 0; i < 3; ++i) S.M.apply(np, dp<T>(y), dp<T>(x), nullptr, st);
+      PB_CUDA(cudaEventRecord(e0, st));
+      for (int i = 0; i < reps; ++i) S.M.apply(np, dp<T>(y), dp<T>(x), nullptr, st);
+      PB_CUDA(cudaEventRecord(e1, st));
+      PB_CUDA(cudaEventSynchronize(e1));
+      PB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      *ms_precon = ms / reps;
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    };
+    // inner_precision = 1 times the FP32 system of the mixed-precision path
+    if (o.inner == PARCEL_B_INNER_FP32_REFINE) run(float(0)); else run(double(0));
     return 0;
   });
 }

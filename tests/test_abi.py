@@ -61,32 +61,125 @@ def test_input_defaults_are_minus_one():
     assert p.rtolmax == -1.0
 
 
+FORTRAN = os.path.join(ROOT, "parcel-legacy_b200", "fortran", "parcel_b_iso.f90")
+
+
+def _fortran_source():
+    src = re.sub(r"!.*", "", open(FORTRAN).read())
+    return re.sub(r"&\s*\n\s*", " ", src)
+
+
+def _c_declarations():
+    hdr = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(void|int)\s+(parcel_\w+)\s*\(([^)]*)\)", hdr):
+        args = [a.strip() for a in m.group(3).split(",") if a.strip() and a.strip() != "void"]
+        out[m.group(2)] = (m.group(1), args)
+    return out
+
+
+def _fortran_kind(c_arg):
+    """The Fortran declaration a C parameter must have in a bind(c) interface (the name is
+    dropped, so only the type and the pointer level remain)."""
+    t = re.sub(r"\bconst\b", "", c_arg)
+    t = re.sub(r"\w+$", "", t.strip()).replace(" ", "")
+    return {"double*": {"real(c_double)", "type(c_ptr),value"}, "int32_t*": {"integer(c_int32_t)"},
+            "int*": {"integer(c_int)"}, "int": {"integer(c_int),value"}, "void**": {"type(c_ptr)"},
+            "parcel_b_input*": {"type(KSP_INPUT_PARAM)"}, "parcel_b_crs*": {"type(parcel_b_crs_t)"}}[t]
+
+
 def test_fortran_interfaces_match_the_header():
     """parcel_b_iso.f90 is shipped uncompiled (no Fortran compiler in this image): check that
-    each bind(c) interface has the C declaration's arguments, in order, with matching kinds."""
-    hdr = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
-    decls = {m.group(1): [a.strip() for a in m.group(2).split(",") if a.strip() and a.strip() != "void"]
-             for m in re.finditer(r"void\s+(parcel_\w+_c_)\s*\(([^)]*)\)", hdr)}
-    src = open(os.path.join(ROOT, "parcel-legacy_b200", "fortran", "parcel_b_iso.f90")).read()
-    src = re.sub(r"&\s*\n\s*", " ", src)
-    stmts = re.findall(r"subroutine\s+(c_\w+)\s*\(([^)]*)\)\s*bind\(c,\s*name=\"(\w+)\"\)", src)
-    stmts += [(n, "", s) for n, s in re.findall(r"subroutine\s+(c_\w+)\s*\(\)\s*bind\(c,\s*name=\"(\w+)\"\)", src)]
-    assert len(stmts) >= 16
-    for name, args, sym in stmts:
-        fargs = [a.strip() for a in args.split(",") if a.strip()]
-        body = re.search(r"subroutine\s+%s\s*\(.*?end subroutine %s" % (name, name), src, flags=re.S).group(0)
+    each bind(c) interface (subroutine or integer function) has the C declaration's
+    arguments, in order, with matching kinds and passing (by value or by reference)."""
+    decls = _c_declarations()
+    src = _fortran_source()
+    stmts = re.findall(r"(subroutine|integer\(c_int\) function)\s+(c_\w+)\s*\(([^)]*)\)\s*bind\(c,\s*name=\"(\w+)\"\)",
+                       src)
+    stmts += [("subroutine", n, "", s) for n, s in
+              re.findall(r"subroutine\s+(c_\w+)\s*\(\)\s*bind\(c,\s*name=\"(\w+)\"\)", src)]
+    assert len(stmts) >= 26
+    for kind, name, args, sym in stmts:
+        fargs = [a.strip().lower() for a in args.split(",") if a.strip()]
+        end = "end subroutine" if kind == "subroutine" else "end function"
+        body = re.search(r"%s\s*\(.*?%s %s" % (name, end, name), src, flags=re.S).group(0)
         kinds = {}
-        for kind, names in re.findall(r"(integer\(c_int\)|integer\(c_int32_t\)|real\(c_double\))\s*::\s*([^\n]*)",
-                                      body):
+        for decl, names in re.findall(r"(integer\(c_int\)(?:,\s*value)?|integer\(c_int32_t\)|real\(c_double\)|"
+                                      r"type\(c_ptr\)(?:,\s*value)?|type\(KSP_INPUT_PARAM\)|type\(parcel_b_crs_t\))"
+                                      r"\s*::\s*([^\n]*)", body):
             for nm in names.split(","):
-                kinds[re.sub(r"\(\*\)", "", nm.strip()).lower()] = kind
+                kinds[re.sub(r"\(\*\)", "", nm.strip()).lower()] = decl.replace(" ", "")
         assert sym in decls, sym
-        assert len(decls[sym]) == len(fargs), sym
-        for ca, fa in zip(decls[sym], fargs):
-            ct = ca.replace(" ", "")
-            want = ("real(c_double)" if ct.startswith("double*") else
-                    "integer(c_int32_t)" if ct.startswith("int32_t*") else "integer(c_int)")
-            assert kinds.get(fa.lower()) == want, (sym, ca, fa, kinds.get(fa.lower()))
+        ret, cargs = decls[sym]
+        assert (ret == "void") == (kind == "subroutine"), sym
+        assert len(cargs) == len(fargs), sym
+        for ca, fa in zip(cargs, fargs):
+            assert kinds.get(fa) in _fortran_kind(ca), (sym, ca, fa, kinds.get(fa))
+
+
+def _c_struct_fields(name):
+    hdr = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), hdr, flags=re.S).group(1)
+    out = []
+    for decl in body.split(";"):
+        decl = decl.replace("const", " ").strip()
+        if not decl:
+            continue
+        m = re.match(r"(\w+\s*\**)\s*(.+)$", decl)
+        t, names = m.group(1).replace(" ", ""), m.group(2)
+        for nm in names.split(","):
+            nm = nm.strip()
+            n_ = int(re.search(r"\[(\d+)\]", nm).group(1)) if "[" in nm else 1
+            out.append((re.sub(r"\[.*", "", nm), t.replace("const", "").strip(), n_))
+    return out
+
+
+def _f_type_fields(name):
+    src = _fortran_source()
+    body = re.search(r"type,\s*bind\(c\)\s*::\s*%s(.*?)end type %s" % (name, name), src, flags=re.S).group(1)
+    out = []
+    for t, names in re.findall(r"(integer\(c_int\)|integer\(c_int32_t\)|integer\(c_int64_t\)|real\(c_double\)|"
+                               r"type\(c_ptr\))\s*::\s*([^\n]*)", body):
+        for nm in names.split(","):
+            nm = nm.strip()
+            n_ = int(re.search(r"\((\d+)\)", nm).group(1)) if "(" in nm else 1
+            out.append((re.sub(r"\(.*", "", nm), t, n_))
+    return out
+
+
+def test_fortran_types_match_the_c_structs():
+    """type(KSP_INPUT_PARAM) of module krylov is parcel_b_input member for member (names,
+    order, kinds, array lengths), and parcel_b_crs_t is parcel_b_crs, so C's and Fortran's
+    layout rules give both the same offsets."""
+    ckind = {"int": "integer(c_int)", "int32_t": "integer(c_int32_t)", "int64_t": "integer(c_int64_t)",
+             "double": "real(c_double)", "int32_t*": "type(c_ptr)", "double*": "type(c_ptr)"}
+    for cname, fname in (("parcel_b_input", "KSP_INPUT_PARAM"), ("parcel_b_crs", "parcel_b_crs_t")):
+        c = [(n.lower(), ckind[t.replace(" ", "")], k) for n, t, k in _c_struct_fields(cname)]
+        f = [(n.lower(), t, k) for n, t, k in _f_type_fields(fname)]
+        assert c == f, (cname, c, f)
+    # the reference's KSP_INPUT_PARAM fields come first, in the reference's order
+    # (src/type.f90:907-946)
+    ref = ["ipreflag", "ilu_method", "addl", "iflagas", "solver", "iovlflag", "gmres_m", "gmres_gsflag",
+           "cagmres_sstep", "cagmres_tstep", "cagmres_basis", "cagmres_qrflag", "cbcg_kstep", "cbcg_eigenflag",
+           "power_method_itrmax", "caarnoldi_sstep", "caarnoldi_tstep", "caarnoldi_basis", "caarnoldi_qrflag",
+           "machineflag", "dataflag", "calcflag", "neuman_itr", "neuman_local", "itrmax", "rtolmax", "abstolmax",
+           "independ_nvec", "precon_thblock", "nblock", "precision_a", "precision_b", "precision_x",
+           "precision_precondition"]
+    assert [n.lower() for n, _, _ in _f_type_fields("KSP_INPUT_PARAM")][:len(ref)] == ref
+
+
+def test_fortran_wrapper_provides_the_reference_entry_points():
+    """Module PARCEL_wrapper offers the reference's generic entries and both builds' forms of
+    the solver wrappers (host arrays, or device addresses as type(c_ptr))."""
+    src = _fortran_source().lower()
+    for name in ("init_parcel_input", "parcel_ddksp_crs", "parcel_dcg_host", "parcel_dcg_dev", "parcel_dgmres_dev",
+                 "parcel_dbicgstab_dev", "parcel_dcagmres_dev", "parcel_ksp_crs_host", "parcel_ksp_crs_dev"):
+        assert re.search(r"subroutine %s\s*\(" % name, src), name
+    for generic in ("parcel_ksp_crs", "parcel_dcg", "parcel_dbicgstab", "parcel_dgmres", "parcel_dcagmres"):
+        m = re.search(r"interface %s\s+module procedure ([\w, ]+)" % generic, src)
+        assert m and {generic + "_host", generic + "_dev"} == {p.strip() for p in m.group(1).split(",")}, generic
+    for mod in ("parcel_integer", "parcel_define", "krylov", "parcel_wrapper"):
+        assert re.search(r"^module %s\b" % mod, src, flags=re.M), mod
 
 
 def test_python_api_rejects_mistyped_arrays_before_calling_the_library():
