@@ -274,19 +274,17 @@ def run_ours(args):
 def target_summary(args):
     """The learned + mixed-precision target on its own workload (256^3 variable-coefficient
     diffusion), with a reduced number of right-hand sides: seconds per right-hand side of
-    the plain FP64 path, the mixed-precision path without the stage and the learned path."""
+    the plain FP64 path, the mixed-precision path without the stage, the coarse stage
+    without and with the network, and the coarse stage at 8 steps without the network."""
     v = vardiff_compare(args.grid, args.coarsen, args.restart, args.target_rhs, args.target_rhs,
-                        args.target_train_rhs, args.target_train_steps)
+                        args.target_train_rhs, args.target_train_steps, k=args.coarse_steps)
+    arms = ("plain_fp64", "mixed_no_stage", "mixed_coarse", "learned", "mixed_coarse_k8")
     return {"workload": v["config"]["workload"], "rhs": args.target_rhs,
-            "plain_fp64_s_per_rhs": v["plain_fp64"]["s_per_rhs_amortised"],
-            "mixed_s_per_rhs": v["mixed_no_stage"]["s_per_rhs_amortised"],
-            "learned_s_per_rhs": v["learned"]["s_per_rhs_amortised"],
+            "s_per_rhs": {a: v[a]["s_per_rhs_amortised"] for a in arms},
             "speedup": v["speedup_vs_plain_fp64"],
-            "iterations": {"plain_fp64": v["plain_fp64"]["iterations"], "mixed": v["mixed_no_stage"]["iterations"],
-                           "learned": v["learned"]["iterations"]},
-            "true_relres_max": {"plain_fp64": v["plain_fp64"]["true_relres_max"],
-                                "mixed": v["mixed_no_stage"]["true_relres_max"],
-                                "learned": v["learned"]["true_relres_max"]},
+            "network_gain": v["network_gain"],
+            "iterations": {a: v[a]["iterations"] for a in arms},
+            "true_relres_max": {a: v[a]["true_relres_max"] for a in arms},
             "training": v["training"]}
 
 
@@ -400,17 +398,22 @@ def run_kernels_only(args):
 VD_METRIC = "time-to-1e-10 true rel. residual (s), learned + mixed-precision FGMRES vs plain FP64 PGMRES/BJ-ILU"
 
 
-def vardiff_compare(N, c, m, nr, plain_rhs, train_rhs, train_steps):
+def vardiff_compare(N, c, m, nr, plain_rhs, train_rhs, train_steps, k=2, reps=3):
     """The learned-preconditioner workload: 3D 7-point variable-coefficient diffusion on an
     N^3 grid (N = 256 by default), coefficient exp(g) with g a Gaussian random field
     (correlation length 8 cells, variance 2, seed 5), harmonic-mean faces; right-hand
-    sides N(0,1).  Compares, per right-hand side and with every array already on the GPU:
-      plain   FP64 PGMRES(m) + block-Jacobi ILU(0), 64 blocks      (parcel_b_solve)
-      mixed   FP32 FGMRES(m) + FP32 BJ-ILU(0) in FP64 refinement    (parcel_b_solve_learned, no stage)
-      learned the same + the learned coarse-grid stage              (parcel_b_solve_learned)
+    sides N(0,1).  Arms, per right-hand side, every array already on the GPU, set-up
+    included and amortised over the right-hand sides of one call:
+      plain_fp64        FP64 PGMRES(m) + block-Jacobi ILU(0), 64 blocks (parcel_b_setup / _start)
+      mixed_no_stage    FP32 FGMRES(m) + FP32 BJ-ILU(0) in FP64 refinement (parcel_b_solve_learned_many)
+      mixed_coarse      the same + the Galerkin coarse stage, k coarse PCG steps from zero
+      learned           the same + the coarse stage started from the trained network's guess
+      mixed_coarse_k8   the coarse stage without the network at 8 coarse PCG steps
     The network is trained beforehand on pairs from plain solves with other right-hand
     sides (training time reported separately).  Time: CUDA events on the library stream
-    around each synchronous solve call (set-up included)."""
+    around each synchronous call; the FGMRES arms report the median of `reps` calls (host
+    hiccups such as a slow graph instantiation land in single calls), the plain arm one
+    call."""
     import torch
     from parcel_b import _lib, api, problems
     L = _lib.load()
@@ -438,23 +441,23 @@ def vardiff_compare(N, c, m, nr, plain_rhs, train_rhs, train_steps):
     t0 = time.perf_counter()
     net = api.Learned(N, N, N, c, seed=1)
     for sd in range(100, 100 + train_rhs):
-        net.collect(A, problems.rhs_normal(A.n, sd), max_pairs=32, **common)
+        net.collect(A, problems.rhs_normal(A.n, sd), max_pairs=64, **common)
     t_collect = time.perf_counter() - t0
     t0 = time.perf_counter()
     f_loss, l_loss = net.train(steps=train_steps, batch=4, lr=2e-3, seed=3)
     t_train = time.perf_counter() - t0
 
-    B = t(np.stack([problems.rhs_normal(A.n, 1000 + k) for k in range(nr)]))
+    B = t(np.stack([problems.rhs_normal(A.n, 1000 + j) for j in range(nr)]))
     X = torch.zeros_like(B)
     it = np.zeros(nr, np.int32)
     ir = np.zeros(nr, np.int32)
+    Asp = torch.sparse_csr_tensor((rp - 1).long(), (ci - 1).long(), va, size=(A.n, A.n))
 
     def plain_all(k_rhs):
         """plain FP64 PGMRES: one set-up (parcel_b_setup), then parcel_b_start per RHS"""
         p = _lib.new_input(**common)
         h = C.c_void_p()
         ts, its, rels = [], [], []
-        Asp = torch.sparse_csr_tensor((rp - 1).long(), (ci - 1).long(), va, size=(A.n, A.n))
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         s0.record(stream)
@@ -462,51 +465,69 @@ def vardiff_compare(N, c, m, nr, plain_rhs, train_rhs, train_steps):
         s1.record(stream)
         s1.synchronize()
         setup = s0.elapsed_time(s1) / 1e3
-        for k in range(k_rhs):
-            X[k].zero_()
+        for j in range(k_rhs):
+            X[j].zero_()
             n_, i_ = C.c_int(0), C.c_int(0)
-            dt, rc = timed(lambda: L.parcel_b_start(h, B[k].data_ptr(), X[k].data_ptr(), hist.ctypes.data,
+            dt, rc = timed(lambda: L.parcel_b_start(h, B[j].data_ptr(), X[j].data_ptr(), hist.ctypes.data,
                                                     C.byref(n_), C.byref(i_)))
             assert rc == 0, _lib.last_error()
             ts.append(dt)
             its.append(n_.value)
-            rels.append(float(torch.linalg.norm(B[k] - Asp @ X[k]) / torch.linalg.norm(B[k])))
+            rels.append(float(torch.linalg.norm(B[j] - Asp @ X[j]) / torch.linalg.norm(B[j])))
         L.parcel_b_release(h)
         return {"setup_s": setup, "solve_s_per_rhs": sum(ts) / len(ts), "rhs": len(ts), "iterations": its,
                 "true_relres_max": max(rels), "fallbacks": 0,
                 "s_per_rhs_amortised": setup / nr + sum(ts) / len(ts)}
 
-    def fgmres_all(h, inner):
-        """flexible GMRES (mixed precision when inner = 1), all RHS in one call, one set-up"""
+    def fgmres_all(h, inner=1, n_rep=reps):
+        """flexible GMRES (mixed precision when inner = 1), all RHS in one call, one set-up;
+        the median of n_rep calls"""
         p = _lib.new_input(inner_precision=inner, inner_rtol=1e-4, max_refine=80, **common)
-        X.zero_()
-        dt, rc = timed(lambda: L.parcel_b_solve_learned_many(C.byref(p), C.byref(S), h, nr, B.data_ptr(),
-                                                             X.data_ptr(), it.ctypes.data, ir.ctypes.data))
-        assert rc == 0, _lib.last_error()
-        st = _lib.last_stats()
+        calls = []
+        for _ in range(n_rep):
+            X.zero_()
+            dt, rc = timed(lambda: L.parcel_b_solve_learned_many(C.byref(p), C.byref(S), h, nr, B.data_ptr(),
+                                                                 X.data_ptr(), it.ctypes.data, ir.ctypes.data))
+            assert rc == 0, _lib.last_error()
+            calls.append((dt, _lib.last_stats()))
+        rel = max(float(torch.linalg.norm(B[j] - Asp @ X[j]) / torch.linalg.norm(B[j])) for j in range(nr))
+        dt, st = sorted(calls, key=lambda q: q[0])[len(calls) // 2]
         return {"setup_s": st["setup_s"], "solve_s_per_rhs": st["solve_s"] / nr, "rhs": nr,
-                "iterations": it.tolist(), "true_relres_max": st["true_relres"], "fallbacks": st["fallback"],
-                "s_per_rhs_amortised": dt / nr, "call_s": dt}
+                "iterations": it.tolist(), "true_relres_max": rel, "fallbacks": st["fallback"],
+                "refine_steps": st["refine_steps"], "s_per_rhs_amortised": dt / nr, "call_s": dt,
+                "calls_s": [round(q[0], 4) for q in calls]}
 
-    # warm-up (graph capture, allocations) on a small call of each path
-    fgmres_all(None, 1)
+    # warm-up (graph capture, allocations) on a call of each FGMRES path
+    fgmres_all(None, n_rep=1)
+    net.set_stage(k, 1)
+    fgmres_all(net.handle, n_rep=1)
     clk = Clocks(0)
     clk.started()
     sp = plain_all(min(plain_rhs, nr))
-    sm = fgmres_all(None, 1)
-    sl = fgmres_all(net.handle, 1)
+    sm = fgmres_all(None)
+    net.set_stage(k, 0)
+    sc = fgmres_all(net.handle)
+    net.set_stage(k, 1)
+    sl = fgmres_all(net.handle)
+    net.set_stage(8, 0)
+    s8 = fgmres_all(net.handle)
     clocks = clk.stop()
+    mean = lambda r: float(np.mean(r["iterations"]))
     out = {"metric": VD_METRIC, "value": sl["call_s"], "unit": "s", "n_gpus": 1,
            "steps": nr, "warmup": 1, "ms_per_step": sl["s_per_rhs_amortised"] * 1e3, "higher_is_better": False,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement, bf16 network",
            "data": "synthetic",
            "config": {"workload": f"variable-coefficient 7-pt diffusion {N}^3, k=exp(GRF(corr 8, var 2)), "
-                                  f"{nr} RHS N(0,1), FGMRES({m}) + BJ-ILU(0) {NBLOCKS} blocks, "
-                                  f"learned stage on the {N // c}^3 coarse grid, tol {RTOL}",
-                      "n": A.n, "nnz": A.nnz, "coarsen": c, "l2": "inputs larger than L2"},
-           "plain_fp64": sp, "mixed_no_stage": sm, "learned": sl,
+                                  f"{nr} RHS N(0,1), FGMRES({m}) + BJ-ILU(0) {NBLOCKS} blocks + Galerkin coarse "
+                                  f"stage on the {N // c}^3 grid ({k} coarse PCG steps, network guess), "
+                                  f"tol {RTOL}",
+                      "n": A.n, "nnz": A.nnz, "coarsen": c, "coarse_steps": k, "l2": "inputs larger than L2"},
+           "plain_fp64": sp, "mixed_no_stage": sm, "mixed_coarse": sc, "learned": sl, "mixed_coarse_k8": s8,
            "speedup_vs_plain_fp64": sp["s_per_rhs_amortised"] / sl["s_per_rhs_amortised"],
            "speedup_mixed_vs_plain_fp64": sp["s_per_rhs_amortised"] / sm["s_per_rhs_amortised"],
+           "network_gain": {"iterations_without": mean(sc), "iterations_with": mean(sl),
+                            "time_ratio": sc["s_per_rhs_amortised"] / sl["s_per_rhs_amortised"],
+                            "vs_coarse_k8_time_ratio": s8["s_per_rhs_amortised"] / sl["s_per_rhs_amortised"]},
            "training": {"pairs": net.num_pairs(), "collect_s": t_collect, "train_s": t_train,
                         "steps": train_steps, "loss_first": f_loss, "loss_last": l_loss},
            "clocks": clocks}
@@ -515,7 +536,7 @@ def vardiff_compare(N, c, m, nr, plain_rhs, train_rhs, train_steps):
 
 def run_vardiff(args):
     print(json.dumps(vardiff_compare(args.grid, args.coarsen, args.restart, args.rhs, args.plain_rhs,
-                                     args.train_rhs, args.train_steps)))
+                                     args.train_rhs, args.train_steps, k=args.coarse_steps)))
 
 
 DD_METRIC = "time to 1e-9 recursive rel. residual (s), double-double PCG + block-Jacobi D-ILU"
@@ -960,11 +981,13 @@ def main():
     ap.add_argument("--rhs", type=int, default=16)
     ap.add_argument("--plain-rhs", type=int, default=16)
     ap.add_argument("--train-rhs", type=int, default=4)
+    ap.add_argument("--coarse-steps", type=int, default=2,
+                    help="coarse PCG steps of the learned stage (the mixed_coarse arm uses the same)")
     ap.add_argument("--train-steps", type=int, default=400)
     ap.add_argument("--target-rhs", type=int, default=2,
                     help="right-hand sides of the learned-preconditioner target on the default line (0: skip)")
     ap.add_argument("--target-train-rhs", type=int, default=2)
-    ap.add_argument("--target-train-steps", type=int, default=300)
+    ap.add_argument("--target-train-steps", type=int, default=400)
     args = ap.parse_args()
     if args.impl == "reference" and args.workload in ("ddcg160", "ddgmres128"):
         run_reference_dd(args)

@@ -420,15 +420,17 @@ int parcel_b_ddgmres(const parcel_b_input* prm, const parcel_b_crs* A, const dou
 int parcel_b_bench_kernels(const parcel_b_input* prm, const parcel_b_crs* A, int reps,
                            double* ms_spmv, double* ms_precon);
 
-/* ---- learned coarse-grid preconditioner stage (no counterpart in the reference) -----
- * Flexible GMRES with z = M^-1 r followed by a learned coarse correction:
- *   t = r - A z,  z += (sigma / s) P Net([R t / sigma, dhat]),  sigma = rms(R t),
- * R = mean over coarsen^3 blocks of the natural grid (row = (z ny + y) nx + x), P =
- * cell-centred trilinear interpolation, dhat = normalised coarse log|diag A|, s = the
- * target scale fixed from the training pairs.  Net: six BF16 3x3x3 convolutions,
- * 2 -> 32 -> 32 -> 32 -> 32 -> 32 -> 1 channels, ReLU between, zero padding, FP32 sums.
- * Parameters (FP32): for layer l = 0..5, W_l[27][C_in][C_out] (tap 9(dz+1)+3(dy+1)+(dx+1))
- * then b_l[C_out]. */
+/* ---- learned two-level preconditioner stage (no counterpart in the reference) --------
+ * Flexible GMRES with the additive two-level preconditioner
+ *   z = M^-1 v + P y,   y ~ A_c^-1 P^T v,   A_c = P^T A P  (Galerkin, 27-point),
+ * on a structured nx x ny x nz grid (natural row = (z ny + y) nx + x) coarsened by an even
+ * factor c: P = cell-centred trilinear interpolation clamped at the boundary.  y comes from
+ * coarse_steps Jacobi-preconditioned CG iterations on A_c, started from the network's
+ * prediction of the coarse error (scaled by the A_c-optimal gamma) or from zero.
+ * Net: six BF16 3x3x3 convolutions, 2 -> 32 -> 32 -> 32 -> 32 -> 32 -> 1 channels, ReLU
+ * between, zero padding, FP32 sums; inputs [P^T v / rms, dhat], dhat = normalised coarse
+ * log|diag A|.  Parameters (FP32): for layer l = 0..5, W_l[27][C_in][C_out]
+ * (tap 9(dz+1)+3(dy+1)+(dx+1)) then b_l[C_out]. */
 typedef struct parcel_b_learned_s* parcel_b_learned;
 int parcel_b_learned_create(int nx, int ny, int nz, int coarsen, uint64_t seed, parcel_b_learned* out);
 int parcel_b_learned_destroy(parcel_b_learned h);
@@ -447,13 +449,28 @@ int parcel_b_learned_grad(parcel_b_learned h, int batch, const float* u, const f
 /* One Adam step (beta 0.9 / 0.999, eps 1e-8) with the last gradient. */
 int parcel_b_learned_adam(parcel_b_learned h, double lr);
 /* Solves A x = b with the plain GMRES of prm (x0 = 0) and appends up to max_pairs
- * training pairs from the iterates after each restart cycle (x_0 = 0 included). */
+ * training pairs, one per residual r = b - A x_k after each restart cycle (x_0 = 0
+ * included): input [P^T r / sigma, dhat], target y / sigma with A_c y = P^T r (400 coarse
+ * PCG iterations), sigma = rms(P^T r).  Needs an even coarsening factor. */
 int parcel_b_learned_collect(parcel_b_learned h, const parcel_b_input* prm, const parcel_b_crs* A,
                              const double* b, int max_pairs, int* npairs);
 int parcel_b_learned_num_pairs(parcel_b_learned h);
 /* Adam over the collected pairs: `steps` steps of `batch` pairs drawn with `seed`. */
 int parcel_b_learned_train(parcel_b_learned h, int steps, int batch, double lr, uint64_t seed,
                            double* first_loss, double* last_loss);
+/* Coarse solve of the stage: coarse_steps >= 0 Jacobi-PCG iterations, started from the
+ * network's guess (use_net 1) or from zero (use_net 0).  Defaults: 8 and 1. */
+int parcel_b_learned_set_stage(parcel_b_learned h, int coarse_steps, int use_net);
+/* The stage's Galerkin operator for A on the handle's grid: ac[27][Vc] FP64, tap
+ * t = 9(dz+1)+3(dy+1)+(dx+1), zero where the neighbour lies outside the coarse grid. */
+int parcel_b_learned_galerkin(parcel_b_learned h, const parcel_b_crs* A, double* ac);
+/* The stage's coarse solve on its own: `steps` Jacobi-PCG iterations on A_c y = rc (FP32,
+ * one thread-block cluster), from zero (g0 NULL) or from gamma g0. */
+int parcel_b_learned_coarse_solve(parcel_b_learned h, const parcel_b_crs* A, const float* rc, const float* g0,
+                                  int steps, float* y);
+/* Grid transfers in the natural layout: to_coarse 1: out[Vc] = P^T in[n]; 0: out[n] = P in[Vc]
+ * (computed in FP32). */
+int parcel_b_learned_transfer(parcel_b_learned h, int to_coarse, const double* in, double* out);
 /* Flexible GMRES(GMRES_m) with M from prm and the learned stage (h NULL: M alone), FP64
  * or, with inner_precision = 1, FP32 inside the FP64 refinement loop.  If the FP64 true
  * residual misses rtolmax, plain PGMRES with M continues from x (stats.fallback = 1). */

@@ -742,141 +742,6 @@ __global__ void k_scale_by(int64_t n, const float* __restrict__ in, const float*
   if (i < n) out[i] = in[i] * scal[0];
 }
 
-// One warp per coarse cell: the lanes split the cell's c^3 fine rows (32-bit index
-// arithmetic: n < 2^31), sum in FP64 and lane 0 stores the mean.
-template <class T>
-__global__ void __launch_bounds__(kRedThreads)
-    k_restrict(int nx, int ny, int nz, int c, const T* __restrict__ src, const int* __restrict__ pos,
-               float* __restrict__ tc, float* __restrict__ scal, double* __restrict__ part,
-               unsigned* __restrict__ ticket, const int* gate) {
-  if (gated(gate)) return;
-  __shared__ double red[kRedThreads / 32];
-  __shared__ bool last;
-  const unsigned gx = nx / c, gy = ny / c, gz = nz / c;
-  const unsigned V = gx * gy * gz, c3 = (unsigned)(c * c * c), cc = (unsigned)(c * c);
-  const double inv = 1.0 / (double)c3;
-  const int lane = threadIdx.x & 31;
-  const unsigned wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  double sq = 0.0;
-  for (unsigned v = wid; v < V; v += nw) {
-    const unsigned cx = v % gx, r1 = v / gx, cy = r1 % gy, cz = r1 / gy;
-    double s = 0.0;
-    for (unsigned e = lane; e < c3; e += 32) {
-      const unsigned i = e % c, j = (e / c) % c, k = e / cc;
-      const unsigned nat = ((cz * c + k) * ny + (cy * c + j)) * nx + cx * c + i;
-      s += (double)src[pos ? pos[nat] : nat];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
-    if (lane == 0) {
-      const float m = (float)(s * inv);
-      tc[v] = m;
-      sq += (double)m * m;
-    }
-  }
-  if (lane == 0) red[threadIdx.x >> 5] = sq;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < kRedThreads / 32; ++w) s += red[w];
-    part[blockIdx.x] = s;
-    __threadfence();
-    last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last || threadIdx.x != 0) return;
-  __threadfence();
-  double s = 0.0;
-  for (unsigned b = 0; b < gridDim.x; ++b) s += __ldcg(part + b);
-  const double rms = sqrt(s / (double)V);
-  scal[0] = rms > 0.0 ? (float)(1.0 / rms) : 0.f;
-  scal[1] = (float)rms;
-  *ticket = 0u;
-}
-
-__device__ __forceinline__ void lin1(int i, int c, int G, int& lo, int& hi, float& w) {
-  const float xi = ((float)i + 0.5f) / (float)c - 0.5f;
-  const float f = floorf(xi);
-  w = xi - f;
-  const int i0 = (int)f;
-  lo = min(max(i0, 0), G - 1);
-  hi = min(max(i0 + 1, 0), G - 1);
-}
-
-template <class T>
-__global__ void __launch_bounds__(256)
-    k_prolong(int nx, int ny, int nz, int c, int64_t np, const float* __restrict__ yc, const float* __restrict__ scal,
-              float scale, const int* __restrict__ rowAt, T* __restrict__ dst, bool add, const int* gate) {
-  if (gated(gate)) return;
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= np) return;
-  const int nat = rowAt ? rowAt[p] : (int)p;
-  if (nat < 0) return;
-  const int gx = nx / c, gy = ny / c, gz = nz / c;
-  const unsigned un = (unsigned)nat, r1 = un / (unsigned)nx;
-  const int x = (int)(un - r1 * (unsigned)nx), y = (int)(r1 % (unsigned)ny), z = (int)(r1 / (unsigned)ny);
-  int x0, x1, y0, y1, z0, z1;
-  float wx, wy, wz;
-  lin1(x, c, gx, x0, x1, wx);
-  lin1(y, c, gy, y0, y1, wy);
-  lin1(z, c, gz, z0, z1, wz);
-  auto at = [&](int zz, int yy, int xx) { return yc[((int64_t)zz * gy + yy) * gx + xx]; };
-  const float c00 = at(z0, y0, x0) * (1.f - wz) + at(z1, y0, x0) * wz;
-  const float c01 = at(z0, y0, x1) * (1.f - wz) + at(z1, y0, x1) * wz;
-  const float c10 = at(z0, y1, x0) * (1.f - wz) + at(z1, y1, x0) * wz;
-  const float c11 = at(z0, y1, x1) * (1.f - wz) + at(z1, y1, x1) * wz;
-  const float c0 = c00 * (1.f - wy) + c10 * wy;
-  const float c1 = c01 * (1.f - wy) + c11 * wy;
-  const float val = c0 * (1.f - wx) + c1 * wx;
-  const T v = (T)(scale * scal[1] * val);
-  dst[p] = add ? dst[p] + v : v;
-}
-
-// alpha = <t, q> / <q, q> (0 when q = 0): the step length that minimises ||t - alpha q||.
-// Per-block partials, the last block to finish sums them in block order.
-template <class T>
-__global__ void __launch_bounds__(kRedThreads)
-    k_alpha(int64_t n, const T* __restrict__ t, const T* __restrict__ q, double* __restrict__ part,
-            unsigned* __restrict__ ticket, double* __restrict__ alpha, const int* gate) {
-  if (gated(gate)) return;
-  __shared__ double red[2][kRedThreads / 32];
-  __shared__ bool last;
-  double tq = 0.0, qq = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double a = (double)t[i], b = (double)q[i];
-    tq += a * b;
-    qq += b * b;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    tq += __shfl_xor_sync(kFull, tq, o);
-    qq += __shfl_xor_sync(kFull, qq, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    red[0][threadIdx.x >> 5] = tq;
-    red[1][threadIdx.x >> 5] = qq;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s0 = 0.0, s1 = 0.0;
-    for (int w = 0; w < kRedThreads / 32; ++w) { s0 += red[0][w]; s1 += red[1][w]; }
-    part[2 * blockIdx.x] = s0;
-    part[2 * blockIdx.x + 1] = s1;
-    __threadfence();
-    last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last || threadIdx.x != 0) return;
-  __threadfence();
-  double s0 = 0.0, s1 = 0.0;
-  for (unsigned b = 0; b < gridDim.x; ++b) {
-    s0 += __ldcg(part + 2 * b);
-    s1 += __ldcg(part + 2 * b + 1);
-  }
-  *alpha = s1 > 0.0 ? s0 / s1 : 0.0;
-  *ticket = 0u;
-}
-
 __global__ void __launch_bounds__(256)
     k_coarse_logdiag(int nx, int ny, int nz, int c, const int* __restrict__ rowptr, const int* __restrict__ col,
                      const double* __restrict__ val, int rbase, int cbase, float* __restrict__ out) {
@@ -1088,46 +953,12 @@ void prep_input(const Geo& g, const float* tc, const float* dhat, const float* s
   PB_CUDA(cudaGetLastError());
 }
 
-template <class T>
-void restrict_to_coarse(int nx, int ny, int nz, int c, const T* src, const int* pos, float* tc, float* scal,
-                        double* part, unsigned* ticket, const int* gate, cudaStream_t st) {
-  k_restrict<T><<<red_blocks(), kRedThreads, 0, st>>>(nx, ny, nz, c, src, pos, tc, scal, part, ticket, gate);
-  PB_CUDA(cudaGetLastError());
-}
-
-template <class T>
-void prolong(int nx, int ny, int nz, int c, int64_t np, const float* yc, const float* scal, float scale,
-             const int* rowAt, T* dst, bool add, const int* gate, cudaStream_t st) {
-  k_prolong<T><<<blocks_for(np), 256, 0, st>>>(nx, ny, nz, c, np, yc, scal, scale, rowAt, dst, add, gate);
-  PB_CUDA(cudaGetLastError());
-}
-
-template <class T>
-void step_length(int64_t n, const T* t, const T* q, double* part, unsigned* ticket, double* alpha, const int* gate,
-                 cudaStream_t st) {
-  k_alpha<T><<<red_blocks(), kRedThreads, 0, st>>>(n, t, q, part, ticket, alpha, gate);
-  PB_CUDA(cudaGetLastError());
-}
-
 void coarse_log_diag(int nx, int ny, int nz, int c, const int* rowptr, const int* col, const double* val,
                      int cbase, float* out, cudaStream_t st) {
   const int64_t V = (int64_t)(nx / c) * (ny / c) * (nz / c);
   k_coarse_logdiag<<<blocks_for(V), 256, 0, st>>>(nx, ny, nz, c, rowptr, col, val, 1, cbase, out);
   PB_CUDA(cudaGetLastError());
 }
-
-template void restrict_to_coarse<double>(int, int, int, int, const double*, const int*, float*, float*, double*,
-                                         unsigned*, const int*, cudaStream_t);
-template void restrict_to_coarse<float>(int, int, int, int, const float*, const int*, float*, float*, double*,
-                                        unsigned*, const int*, cudaStream_t);
-template void prolong<double>(int, int, int, int, int64_t, const float*, const float*, float, const int*, double*,
-                              bool, const int*, cudaStream_t);
-template void prolong<float>(int, int, int, int, int64_t, const float*, const float*, float, const int*, float*,
-                             bool, const int*, cudaStream_t);
-template void step_length<double>(int64_t, const double*, const double*, double*, unsigned*, double*, const int*,
-                                  cudaStream_t);
-template void step_length<float>(int64_t, const float*, const float*, double*, unsigned*, double*, const int*,
-                                 cudaStream_t);
 
 }  // namespace cnn
 }  // namespace pb

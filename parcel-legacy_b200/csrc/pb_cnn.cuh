@@ -1,20 +1,15 @@
 // pb_cnn.cuh -- the learned coarse-grid preconditioner stage (BF16 3D CNN).
 //
-// No counterpart in the reference: PARCEL has no learned component.  The stage sits after
-// the block-Jacobi ILU inside flexible GMRES:
+// No counterpart in the reference: PARCEL has no learned component.  The network works on
+// the coarse grid of the two-level preconditioner stage (pb_coarse.cuh): from the coarse
+// residual rc = P^T v and the coefficient channel it predicts the coarse error
+// A_c^-1 rc, which starts the stage's coarse Jacobi-PCG:
 //
-//     z  = M_ILU^-1 r
-//     t  = r - A z                          (SpMV, iteration layout)
-//     tc = R t   (mean over c^3 blocks, coarse grid),  sigma = rms(tc)
-//     y  = Net([tc / sigma, dhat])          (6 conv layers, 3^3 taps, BF16, FP32 sums)
-//     c  = (sigma / s) P y                  (P: cell-centred trilinear interpolation)
-//     z += alpha c,  alpha = <t, A c> / <A c, A c>   (the step that minimises ||t - alpha A c||,
-//                                                     so the stage never raises the residual
-//                                                     left by the ILU step)
+//     y0 = Net([rc / sigma, dhat])   (6 conv layers, 3^3 taps, BF16, FP32 sums), sigma = rms(rc)
 //
 // dhat is the normalised coarse mean of log(diag A): the network sees the operator's
-// local coefficient through the matrix itself.  s is the target scale fixed from the
-// training set.  Network layout: channels last, voxel v = (z gy + y) gx + x on the coarse
+// local coefficient through the matrix itself.  Training targets are scaled by s, fixed
+// from the training set (the coarse solve rescales the guess, so s needs no inverse).  Network layout: channels last, voxel v = (z gy + y) gx + x on the coarse
 // grid, samples contiguous; hidden activations BF16 [V][32].
 //
 // Parameters (FP32 master copy, Adam state alongside): layer l = 0..5 stores
@@ -102,24 +97,6 @@ void scale_by(int64_t n, const float* in, const float* scal, float* out, cudaStr
 // Input preparation: u[v] = (bf16(tc[v] * scal[0]), bf16(dhat[v])) for one sample.
 void prep_input(const Geo& g, const float* tc, const float* dhat, const float* scal, __nv_bfloat16* u,
                 const int* gate, cudaStream_t st);
-
-// Coarse-grid transfer between an iteration-layout fine vector and the coarse grid.
-//   restrict: tc = box mean of src over c^3 blocks; scal[0] = 1/rms(tc) (0 if tc == 0),
-//             scal[1] = rms(tc).  pos maps natural rows to iteration positions (NULL:
-//             identity).  Uses `part` (>= red_blocks() doubles) and `ticket` (zero).
-//   prolong:  dst[p] (+)= scale * scal[1] * trilinear(yc)(natural row rowAt[p]); positions
-//             with rowAt[p] < 0 (layout padding) are left untouched.
-template <class T>
-void restrict_to_coarse(int nx, int ny, int nz, int c, const T* src, const int* pos, float* tc,
-                        float* scal, double* part, unsigned* ticket, const int* gate, cudaStream_t st);
-template <class T>
-void prolong(int nx, int ny, int nz, int c, int64_t np, const float* yc, const float* scal, float scale,
-             const int* rowAt, T* dst, bool add, const int* gate, cudaStream_t st);
-// *alpha = <t, q> / <q, q> (0 if q = 0), deterministic; part >= 2 red_blocks() doubles,
-// ticket zero on entry and on exit.
-template <class T>
-void step_length(int64_t n, const T* t, const T* q, double* part, unsigned* ticket, double* alpha, const int* gate,
-                 cudaStream_t st);
 
 // Coarse mean of log|diag A| over c^3 blocks (natural CRS on the device, 1-based row
 // pointers, column base cbase).  Host normalisation follows.

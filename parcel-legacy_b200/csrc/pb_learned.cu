@@ -1,18 +1,19 @@
-// pb_learned.cu -- C ABI of the learned coarse-grid preconditioner stage (no counterpart in
+// pb_learned.cu -- C ABI of the learned two-level preconditioner stage (no counterpart in
 // the reference).
 //
 // Life cycle: parcel_b_learned_create fixes the grid and the coarsening factor;
 // parcel_b_learned_collect runs the plain solver (GMRES with the block-Jacobi ILU or Jacobi
-// preconditioner of the caller's parameters) and turns the iterate logged after every
-// restart cycle into a training pair; parcel_b_learned_train fits the network with Adam on
-// the GPU; parcel_b_solve_learned runs flexible GMRES with z = M^-1 r followed by the
-// learned coarse correction, in FP64 or in FP32 inside the FP64 refinement loop, and falls
-// back to the plain PGMRES/ILU path from the current iterate when the learned solve does
-// not reach the tolerance.
+// preconditioner of the caller's parameters) and turns the residual after every restart
+// cycle into a training pair; parcel_b_learned_train fits the network with Adam on the GPU;
+// parcel_b_learned_set_stage chooses the coarse solve (Jacobi-PCG steps, network guess on
+// or off); parcel_b_solve_learned runs flexible GMRES with z = M^-1 v + P y, in FP64 or in
+// FP32 inside the FP64 refinement loop, and falls back to the plain PGMRES/ILU path from
+// the current iterate when the learned solve does not reach the tolerance.
 //
-// A training pair for an iterate x_k of the plain solve with solution x*:
-//   r = b - A x_k,  z1 = M^-1 r,  t = r - A z1,  e = x* - x_k - z1  (so A e = t),
-//   input  = [bf16(R t / sigma), bf16(dhat)],  target = (R e) / sigma,  sigma = rms(R t).
+// A training pair for a residual r = b - A x_k of the plain solve: the coarse residual
+// rc = P^T r and the coarse error y* with A_c y* = rc (A_c = P^T A P, solved by many
+// coarse PCG steps):  input = [bf16(rc / sigma), bf16(dhat)],  target = y* / sigma,
+// sigma = rms(rc).  In the stage the network's output is the coarse PCG's starting guess.
 #include <algorithm>
 #include <cmath>
 #include <memory>
@@ -20,6 +21,7 @@
 
 #include "pb_api.cuh"
 #include "pb_cnn.cuh"
+#include "pb_coarse.cuh"
 
 namespace pb {
 
@@ -32,7 +34,12 @@ struct Learned {
   DBuf tgt, loss;
   double scale = 0.0;        // target scale s: 1 / rms of the collected targets
   std::vector<DBuf> pu, pt;  // training pairs: inputs bf16 [V][2], targets float [V]
+  int coarse_steps = 8;      // Jacobi-PCG iterations of the stage's coarse solve
+  bool use_net = true;       // start the coarse solve from the network's guess
 };
+
+// Coarse PCG iterations behind a training target (the coarse error A_c^-1 rc).
+constexpr int kTargetSteps = 400;
 
 namespace {
 
@@ -57,54 +64,111 @@ void make_dhat(const Learned& L, const DevMat<double>& A, DBuf& out) {
   h2d(out.p, h.data(), sizeof(float) * V);
 }
 
-// c = (sigma / s) P Net([R t / sigma, dhat]) with t = r - A z;  z += alpha c with the
-// step alpha that minimises ||t - alpha A c||: a correction the network gets wrong (an input
-// unlike its training pairs) is scaled down instead of spoiling the Krylov basis.
+// The Galerkin coarse operator of a matrix on the handle's grid, FP64 and FP32.
+struct CoarseOp {
+  coarse::Grid g;
+  DBuf ac64, ac32, dinv;
+  void build(const Learned& L, const DevMat<double>& A) {
+    g = coarse::Grid(L.nx, L.ny, L.nz, L.c);
+    coarse::check_grid(g);
+    const int64_t V = g.Vc();
+    ac64.alloc(sizeof(double) * coarse::kTaps * V);
+    ac32.alloc(sizeof(float) * coarse::kTaps * V);
+    dinv.alloc(sizeof(float) * V);
+    coarse::galerkin(g, A, dp<double>(ac64), stream());
+    coarse::to_f32(V, dp<double>(ac64), dp<float>(ac32), dp<float>(dinv), stream());
+  }
+  coarse::PcgArgs args(const float* rc, const float* g0, float* y, int steps, const int* gate) const {
+    coarse::PcgArgs a;
+    a.g = g; a.ac = dp<float>(ac32); a.dinv = dp<float>(dinv);
+    a.rc = rc; a.g0 = g0; a.y = y; a.steps = steps; a.gate = gate;
+    return a;
+  }
+};
+
+// Additive two-level stage: z = M^-1 v + P y with y from `steps` Jacobi-PCG iterations on
+// A_c y = P^T v, started from the network's guess (use_net) or from zero.  The coarse
+// branch (restriction, network, coarse solve) runs on a side stream while the ILU sweep
+// runs on the solver's stream (the sweep uses one CTA per block-Jacobi block and leaves the
+// other SMs idle); the prolongation joins the two.
 template <class T>
-struct LearnedStage final : ExtraStage<T> {
+struct TwoLevelStage final : ExtraStage<T> {
   const Learned* L;
-  DBuf dhat, t, cf, q, alpha, tc, scal, part, ticket;
+  CoarseOp op;
+  DBuf hc, rc, y, scal, dhat;
   cnn::Acts acts;
   const int* pos = nullptr;
   const int* rowAt = nullptr;
   int64_t np = 0;
-  LearnedStage(const Learned* l, const System<T>& S) : L(l) {
-    cudaStream_t st = stream();
-    make_dhat(*L, S.Anat, dhat);
+  int steps = 0;
+  bool net = false;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  TwoLevelStage(const Learned* l, const System<T>& S) : L(l) {
+    op.build(*L, S.Anat);
+    steps = L->coarse_steps;
+    net = L->use_net;
     np = S.np;
     if (S.permuted) {
       pos = dp<int>(S.pos);
       rowAt = dp<int>(S.rowAt);
     }
-    for (DBuf* b : {&t, &cf, &q}) {
-      b->alloc(sizeof(T) * np);
-      PB_CUDA(cudaMemsetAsync(b->p, 0, sizeof(T) * np, st));   // padding positions stay zero
-    }
-    alpha.alloc(sizeof(double));
-    tc.alloc(sizeof(float) * L->g.V());
+    const int64_t V = op.g.Vc();
+    hc.alloc(sizeof(float) * 8 * op.g.Vh());
+    rc.alloc(sizeof(float) * V);
+    y.alloc(sizeof(float) * V);
     scal.alloc(sizeof(float) * 2);
-    part.alloc(sizeof(double) * 2 * red_blocks());
-    ticket.alloc(sizeof(unsigned));
-    PB_CUDA(cudaMemsetAsync(ticket.p, 0, sizeof(unsigned), st));
-    acts.ensure(L->g, 1, false);
-    cnn::init_kernels();
+    if (net) {
+      make_dhat(*L, S.Anat, dhat);
+      acts.ensure(L->g, 1, false);
+      cnn::init_kernels();
+    }
+    PB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    PB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    PB_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
   }
-  void apply(const System<T>& S, const T* r, T* z, T* az, const int* gate, cudaStream_t st) override {
-    spmv<T, T>(S.A, z, dp<T>(t), SPMV_RES, r, gate, st);
-    cnn::restrict_to_coarse<T>(L->nx, L->ny, L->nz, L->c, dp<T>(t), pos, dp<float>(tc), dp<float>(scal),
-                               dp<double>(part), dp<unsigned>(ticket), gate, st);
-    cnn::prep_input(L->g, dp<float>(tc), dp<float>(dhat), dp<float>(scal), dp<__nv_bfloat16>(acts.u), gate, st);
-    cnn::forward(L->net, acts, gate, st);
-    const float inv_s = L->scale > 0.0 ? (float)(1.0 / L->scale) : 1.f;
-    cnn::prolong<T>(L->nx, L->ny, L->nz, L->c, np, dp<float>(acts.y), dp<float>(scal), inv_s, rowAt, dp<T>(cf), false,
-                    gate, st);
-    spmv<T, T>(S.A, dp<T>(cf), dp<T>(q), SPMV_Y, nullptr, gate, st);
-    cnn::step_length<T>(np, dp<T>(t), dp<T>(q), dp<double>(part), dp<unsigned>(ticket), dp<double>(alpha), gate, st);
-    lincomb<T>(np, z, z, cimm(1.0), dp<T>(cf), cdev(dp<double>(alpha)), nullptr, cimm(0), gate, st);
-    // A z = A z1 + alpha A c = (r - t) + alpha q: no SpMV of z needed
-    if (az) lincomb<T>(np, az, r, cimm(1.0), dp<T>(t), cimm(-1.0), dp<T>(q), cdev(dp<double>(alpha)), gate, st);
+  ~TwoLevelStage() override {
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
   }
-  int launches() const override { return 14; }
+  void begin(const System<T>&, const T* r, const int* gate, cudaStream_t st) override {
+    PB_CUDA(cudaEventRecord(ev_fork, st));
+    PB_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
+    coarse::restrict_fine<T>(op.g, r, pos, dp<float>(hc), dp<float>(rc), gate, side);
+    const float* g0 = nullptr;
+    if (net) {
+      coarse::rms(op.g.Vc(), dp<float>(rc), dp<float>(scal), gate, side);
+      cnn::prep_input(L->g, dp<float>(rc), dp<float>(dhat), dp<float>(scal), dp<__nv_bfloat16>(acts.u), gate, side);
+      cnn::forward(L->net, acts, gate, side);
+      g0 = dp<float>(acts.y);
+    }
+    coarse::pcg(op.args(dp<float>(rc), g0, dp<float>(y), steps, gate), side);
+    PB_CUDA(cudaEventRecord(ev_join, side));
+  }
+  void apply(const System<T>&, const T*, T* z, T*, const int* gate, cudaStream_t st) override {
+    PB_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
+    coarse::prolong_add<T>(op.g, np, dp<float>(y), rowAt, z, gate, st);
+  }
+  bool provides_az() const override { return false; }
+  int launches() const override { return net ? 12 : 4; }
+};
+
+// The caller's natural CRS matrix on the device (uploaded if its arrays live on the host).
+struct NatMat {
+  DBuf rp, ci, va;
+  DevMat<double> A;
+  explicit NatMat(const parcel_b_crs& c) {
+    A.n = c.n; A.nnz = c.nnz; A.rbase = 1; A.cbase = c.istart;
+    if (is_device_ptr(c.val)) {
+      A.rowptr = c.rowptr; A.col = c.col; A.val = c.val;
+      return;
+    }
+    rp.alloc(sizeof(int) * (c.n + 1)); h2d(rp.p, c.rowptr, sizeof(int) * (c.n + 1));
+    ci.alloc(sizeof(int) * c.nnz); h2d(ci.p, c.col, sizeof(int) * c.nnz);
+    va.alloc(sizeof(double) * c.nnz); h2d(va.p, c.val, sizeof(double) * c.nnz);
+    A.rowptr = dp<int>(rp); A.col = dp<int>(ci); A.val = dp<double>(va);
+  }
 };
 
 // A host or device float array of n entries as a device pointer (uploaded if needed).
@@ -278,12 +342,11 @@ int parcel_b_learned_collect(parcel_b_learned h, const parcel_b_input* prm, cons
     PB_CHECK(so.iret == 0, PARCEL_B_E_BREAKDOWN, "the plain solve did not converge (iret %d): no training pairs",
              so.iret);
     const double bnorm = std::sqrt(dev_dot<double>(np, dp<double>(bi), dp<double>(bi)));
-    DBuf r(sizeof(double) * np), z1(sizeof(double) * np), t(sizeof(double) * np), e(sizeof(double) * np);
-    DBuf tc(sizeof(float) * V), ec(sizeof(float) * V), scal_t(sizeof(float) * 2), scal_e(sizeof(float) * 2);
-    DBuf part(sizeof(double) * red_blocks()), ticket(sizeof(unsigned));
-    PB_CUDA(cudaMemsetAsync(ticket.p, 0, sizeof(unsigned), st));
+    CoarseOp op;
+    op.build(L, S.Anat);
+    DBuf r(sizeof(double) * np), hc(sizeof(float) * 8 * op.g.Vh()), rc(sizeof(float) * V), ys(sizeof(float) * V),
+        scal(sizeof(float) * 2);
     PB_CUDA(cudaMemsetAsync(r.p, 0, sizeof(double) * np, st));
-    PB_CUDA(cudaMemsetAsync(t.p, 0, sizeof(double) * np, st));
     const int* pos = S.permuted ? dp<int>(S.pos) : nullptr;
     int added = 0;
     for (const DBuf& xk : xs) {
@@ -291,23 +354,102 @@ int parcel_b_learned_collect(parcel_b_learned h, const parcel_b_input* prm, cons
       spmv<double, double>(S.A, dp<double>(xk), dp<double>(r), SPMV_RES, dp<double>(bi), nullptr, st);
       const double rel = std::sqrt(dev_dot<double>(np, dp<double>(r), dp<double>(r))) / bnorm;
       if (!(rel > 1e-8)) continue;   // converged iterates carry no error to learn
-      S.M.apply(np, dp<double>(r), dp<double>(z1), nullptr, st);
-      spmv<double, double>(S.A, dp<double>(z1), dp<double>(t), SPMV_RES, dp<double>(r), nullptr, st);
-      lincomb<double>(np, dp<double>(e), dp<double>(xi), cimm(1.0), dp<double>(xk), cimm(-1.0), dp<double>(z1),
-                      cimm(-1.0), nullptr, st);
-      cnn::restrict_to_coarse<double>(L.nx, L.ny, L.nz, L.c, dp<double>(t), pos, dp<float>(tc), dp<float>(scal_t),
-                                      dp<double>(part), dp<unsigned>(ticket), nullptr, st);
-      cnn::restrict_to_coarse<double>(L.nx, L.ny, L.nz, L.c, dp<double>(e), pos, dp<float>(ec), dp<float>(scal_e),
-                                      dp<double>(part), dp<unsigned>(ticket), nullptr, st);
+      coarse::restrict_fine<double>(op.g, dp<double>(r), pos, dp<float>(hc), dp<float>(rc), nullptr, st);
+      coarse::rms(V, dp<float>(rc), dp<float>(scal), nullptr, st);
+      coarse::pcg(op.args(dp<float>(rc), nullptr, dp<float>(ys), kTargetSteps, nullptr), st);
       L.pu.emplace_back(sizeof(__nv_bfloat16) * 2 * V);
       L.pt.emplace_back(sizeof(float) * V);
-      cnn::prep_input(L.g, dp<float>(tc), dp<float>(dhat), dp<float>(scal_t), dp<__nv_bfloat16>(L.pu.back()),
+      cnn::prep_input(L.g, dp<float>(rc), dp<float>(dhat), dp<float>(scal), dp<__nv_bfloat16>(L.pu.back()),
                       nullptr, st);
-      cnn::scale_by(V, dp<float>(ec), dp<float>(scal_t), dp<float>(L.pt.back()), st);
+      cnn::scale_by(V, dp<float>(ys), dp<float>(scal), dp<float>(L.pt.back()), st);
       ++added;
     }
     sync();
     if (npairs) *npairs = added;
+    return 0;
+  });
+}
+
+int parcel_b_learned_set_stage(parcel_b_learned h, int coarse_steps, int use_net) {
+  return guarded([&]() -> int {
+    PB_CHECK(h && coarse_steps >= 0 && (use_net == 0 || use_net == 1), PARCEL_B_E_ARG,
+             "bad arguments (coarse_steps %d, use_net %d)", coarse_steps, use_net);
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    L.coarse_steps = coarse_steps;
+    L.use_net = use_net != 0;
+    return 0;
+  });
+}
+
+int parcel_b_learned_galerkin(parcel_b_learned h, const parcel_b_crs* A, double* ac) {
+  return guarded([&]() -> int {
+    ensure_init();
+    PB_CHECK(h && ac, PARCEL_B_E_ARG, "bad arguments");
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    validate(A);
+    check_grid(L, A);
+    NatMat M(*A);
+    CoarseOp op;
+    op.build(L, M.A);
+    const size_t bytes = sizeof(double) * coarse::kTaps * op.g.Vc();
+    if (is_device_ptr(ac)) { d2d(ac, op.ac64.p, bytes); sync(); }
+    else d2h(ac, op.ac64.p, bytes);
+    return 0;
+  });
+}
+
+int parcel_b_learned_coarse_solve(parcel_b_learned h, const parcel_b_crs* A, const float* rc, const float* g0,
+                                  int steps, float* y) {
+  return guarded([&]() -> int {
+    ensure_init();
+    PB_CHECK(h && rc && y && steps >= 0, PARCEL_B_E_ARG, "bad arguments");
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    validate(A);
+    check_grid(L, A);
+    NatMat M(*A);
+    CoarseOp op;
+    op.build(L, M.A);
+    const int64_t V = op.g.Vc();
+    FVec r(rc, V);
+    std::unique_ptr<FVec> gv;
+    if (g0) gv = std::make_unique<FVec>(g0, V);
+    DBuf out(sizeof(float) * V);
+    coarse::pcg(op.args(r.p, gv ? gv->p : nullptr, dp<float>(out), steps, nullptr), stream());
+    copy_out(y, out.p, sizeof(float) * V);
+    return 0;
+  });
+}
+
+int parcel_b_learned_transfer(parcel_b_learned h, int to_coarse, const double* in, double* out) {
+  return guarded([&]() -> int {
+    ensure_init();
+    PB_CHECK(h && in && out && (to_coarse == 0 || to_coarse == 1), PARCEL_B_E_ARG, "bad arguments");
+    Learned& L = *reinterpret_cast<Learned*>(h);
+    const coarse::Grid g(L.nx, L.ny, L.nz, L.c);
+    coarse::check_grid(g);
+    const int64_t n = (int64_t)L.nx * L.ny * L.nz, V = g.Vc();
+    cudaStream_t st = stream();
+    if (to_coarse) {
+      NatVec v(in, (int)n, is_device_ptr(in));
+      DBuf hc(sizeof(float) * 8 * g.Vh()), rc(sizeof(float) * V);
+      coarse::restrict_fine<double>(g, v.p, nullptr, dp<float>(hc), dp<float>(rc), nullptr, st);
+      std::vector<float> hr((size_t)V);
+      d2h(hr.data(), rc.p, sizeof(float) * V);
+      std::vector<double> hd(hr.begin(), hr.end());
+      if (is_device_ptr(out)) { h2d(out, hd.data(), sizeof(double) * V); sync(); }
+      else memcpy(out, hd.data(), sizeof(double) * V);
+    } else {
+      std::vector<double> hin((size_t)V);
+      if (is_device_ptr(in)) d2h(hin.data(), in, sizeof(double) * V);
+      else memcpy(hin.data(), in, sizeof(double) * V);
+      std::vector<float> hf(hin.begin(), hin.end());
+      DBuf yc(sizeof(float) * V), z(sizeof(double) * n);
+      h2d(yc.p, hf.data(), sizeof(float) * V);
+      PB_CUDA(cudaMemsetAsync(z.p, 0, sizeof(double) * n, st));
+      coarse::prolong_add<double>(g, n, dp<float>(yc), nullptr, dp<double>(z), nullptr, st);
+      if (is_device_ptr(out)) { d2d(out, z.p, sizeof(double) * n); sync(); }
+      else d2h(out, z.p, sizeof(double) * n);
+    }
     return 0;
   });
 }
@@ -384,18 +526,18 @@ int solve_learned_impl(const parcel_b_input* prm, const parcel_b_crs* A, Learned
   const bool mixed = o.inner == PARCEL_B_INNER_FP32_REFINE;
   std::unique_ptr<System<float>> S32;
   std::unique_ptr<System<double>> S64;
-  std::unique_ptr<LearnedStage<float>> st32;
-  std::unique_ptr<LearnedStage<double>> st64;
+  std::unique_ptr<TwoLevelStage<float>> st32;
+  std::unique_ptr<TwoLevelStage<double>> st64;
   if (mixed) {
     S32 = std::make_unique<System<float>>();
     build_system<float>(o, *A, dev, *S32);
-    if (L) { st32 = std::make_unique<LearnedStage<float>>(L, *S32); S32->extra = st32.get(); }
+    if (L) { st32 = std::make_unique<TwoLevelStage<float>>(L, *S32); S32->extra = st32.get(); }
     stt.ilu_levels_max = S32->ilu_levels_max;
     stt.ilu_nblocks = S32->ilu_nblocks;
   } else {
     S64 = std::make_unique<System<double>>();
     build_system<double>(o, *A, dev, *S64);
-    if (L) { st64 = std::make_unique<LearnedStage<double>>(L, *S64); S64->extra = st64.get(); }
+    if (L) { st64 = std::make_unique<TwoLevelStage<double>>(L, *S64); S64->extra = st64.get(); }
     stt.ilu_levels_max = S64->ilu_levels_max;
     stt.ilu_nblocks = S64->ilu_nblocks;
   }

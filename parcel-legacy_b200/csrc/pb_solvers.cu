@@ -247,6 +247,7 @@ struct GraphRunner {
   void launch(F&& f, bool use_graph, cudaStream_t st) {
     if (!use_graph) { f(); return; }
     if (!exec) {
+      trace_mark(nullptr);
       cudaGraph_t g = nullptr;
       PB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       try {
@@ -260,8 +261,10 @@ struct GraphRunner {
       PB_CUDA(cudaStreamEndCapture(st, &g));
       PB_CUDA(cudaGraphInstantiate(&exec, g, 0));
       cudaGraphDestroy(g);
+      trace_mark("graph: capture + instantiate");
     }
     PB_CUDA(cudaGraphLaunch(exec, st));
+    trace_mark("graph: replay");
   }
 };
 
@@ -432,6 +435,7 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
   // precon(in, out, az): out = M^-1 in (+ the extra stage); with the extra stage and az
   // given, az = A out comes from the stage and the caller's SpMV is skipped.
   auto precon = [&](const T* in, T* out, T* az, const int* gate) {
+    if (S.extra) S.extra->begin(S, in, gate, st);
     S.M.apply(np, in, out, gate, st);
     if (S.extra) S.extra->apply(S, in, out, az, gate, st);
   };
@@ -492,7 +496,7 @@ static SolveOut run_gmres(const Options& o, const System<T>& S, const T* b, T* x
         ++per_cycle;
       }
       T* Pj = flex ? Z + (size_t)(j - 1) * ldv : PV;
-      const bool az_from_stage = S.extra && fused_mgs && o.gs != PARCEL_B_GS_CGS;
+      const bool az_from_stage = S.extra && S.extra->provides_az() && fused_mgs && o.gs != PARCEL_B_GS_CGS;
       precon(Vj, Pj, az_from_stage ? Wv : nullptr, gskip);
       per_cycle += precon_launches;
       if (o.gs == PARCEL_B_GS_CGS) {

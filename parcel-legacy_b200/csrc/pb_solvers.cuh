@@ -49,13 +49,17 @@ struct Precon {
 template <class T>
 struct System;
 
-// An extra preconditioner stage after M (flexible GMRES only): z <- z + stage(r, z).
-// If az is not null the stage also writes A z there (when it can do so without an SpMV
-// of its own), and the caller skips its SpMV of z.
+// An extra preconditioner stage around M (flexible GMRES only): begin(r) is called before
+// z = M^-1 r is launched (work that does not need z may start on a side stream there),
+// apply(r, z) after it: z <- z + stage(r, z).  If az is not null and provides_az() is
+// true, the stage also writes A z there (when it can do so without an SpMV of its own),
+// and the caller skips its SpMV of z.
 template <class T>
 struct ExtraStage {
   virtual ~ExtraStage() = default;
+  virtual void begin(const System<T>&, const T*, const int*, cudaStream_t) {}
   virtual void apply(const System<T>& S, const T* r, T* z, T* az, const int* gate, cudaStream_t st) = 0;
+  virtual bool provides_az() const { return true; }
   virtual int launches() const = 0;
 };
 

@@ -144,6 +144,10 @@ SIGNATURES = {
     "parcel_b_learned_collect": (C.c_int, [P, C.POINTER(Input), C.POINTER(Crs), P, C.c_int, IP]),
     "parcel_b_learned_num_pairs": (C.c_int, [P]),
     "parcel_b_learned_train": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_uint64, DP, DP]),
+    "parcel_b_learned_set_stage": (C.c_int, [P, C.c_int, C.c_int]),
+    "parcel_b_learned_galerkin": (C.c_int, [P, C.POINTER(Crs), P]),
+    "parcel_b_learned_coarse_solve": (C.c_int, [P, C.POINTER(Crs), P, P, C.c_int, P]),
+    "parcel_b_learned_transfer": (C.c_int, [P, C.c_int, P, P]),
     "parcel_b_solve_learned": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), P, P, P, P, IP, IP]),
     "parcel_b_solve_learned_many": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), P, C.c_int, P, P, P, P]),
 }

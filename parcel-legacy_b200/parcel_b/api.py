@@ -302,8 +302,9 @@ def ddsolve_dia(val, offset, b_hi, b_lo=None, x0_hi=None, x0_lo=None, *, val_lo=
 
 
 class Learned:
-    """The learned coarse-grid preconditioner stage (no counterpart in the reference): a
-    handle on the network for an nx x ny x nz grid coarsened by ``coarsen``."""
+    """The learned two-level preconditioner stage (no counterpart in the reference): a
+    handle on the network and the coarse solve for an nx x ny x nz grid coarsened by
+    ``coarsen`` (even for the stage)."""
 
     def __init__(self, nx, ny, nz, coarsen, seed=0):
         self._L = load()
@@ -311,6 +312,53 @@ class Learned:
         if self._L.parcel_b_learned_create(int(nx), int(ny), int(nz), int(coarsen), int(seed), C.byref(h)) != 0:
             raise RuntimeError(f"parcel_b_learned_create failed: {_lib.last_error()}")
         self.handle = h
+        self.grid = (int(nx), int(ny), int(nz), int(coarsen))
+
+    @property
+    def coarse_cells(self):
+        nx, ny, nz, c = self.grid
+        return (nx // c) * (ny // c) * (nz // c)
+
+    def set_stage(self, coarse_steps, use_net):
+        """Coarse solve of the stage: Jacobi-PCG iterations, network guess on or off."""
+        if self._L.parcel_b_learned_set_stage(self.handle, int(coarse_steps), int(bool(use_net))) != 0:
+            raise RuntimeError(f"parcel_b_learned_set_stage failed: {_lib.last_error()}")
+
+    def galerkin(self, A):
+        """The stage's 27-tap Galerkin operator for A: array [27][Vc] (float64)."""
+        ac = np.zeros((27, self.coarse_cells))
+        if self._L.parcel_b_learned_galerkin(self.handle, C.byref(crs_struct(A)), ac.ctypes.data) != 0:
+            raise RuntimeError(f"parcel_b_learned_galerkin failed: {_lib.last_error()}")
+        return ac
+
+    def coarse_solve(self, A, rc, steps, g0=None):
+        """`steps` coarse Jacobi-PCG iterations on P^T A P y = rc (float32), from zero or gamma g0."""
+        rc = np.ascontiguousarray(rc, np.float32)
+        g = None if g0 is None else np.ascontiguousarray(g0, np.float32)
+        y = np.zeros(self.coarse_cells, np.float32)
+        rcode = self._L.parcel_b_learned_coarse_solve(self.handle, C.byref(crs_struct(A)), rc.ctypes.data,
+                                                      None if g is None else g.ctypes.data, int(steps),
+                                                      y.ctypes.data)
+        if rcode != 0:
+            raise RuntimeError(f"parcel_b_learned_coarse_solve failed: {_lib.last_error()}")
+        return y
+
+    def restrict(self, v):
+        """P^T v (natural layout, computed in FP32)."""
+        v = np.ascontiguousarray(v, np.float64)
+        out = np.zeros(self.coarse_cells)
+        if self._L.parcel_b_learned_transfer(self.handle, 1, v.ctypes.data, out.ctypes.data) != 0:
+            raise RuntimeError(f"parcel_b_learned_transfer failed: {_lib.last_error()}")
+        return out
+
+    def prolong(self, y):
+        """P y (natural layout, computed in FP32)."""
+        nx, ny, nz, _ = self.grid
+        y = np.ascontiguousarray(y, np.float64)
+        out = np.zeros(nx * ny * nz)
+        if self._L.parcel_b_learned_transfer(self.handle, 0, y.ctypes.data, out.ctypes.data) != 0:
+            raise RuntimeError(f"parcel_b_learned_transfer failed: {_lib.last_error()}")
+        return out
 
     def collect(self, A, b, max_pairs=16, **options):
         """Appends training pairs from the plain GMRES solve of A x = b (options as in solve)."""
