@@ -395,6 +395,62 @@ def run_kernels_only(args):
                       "spmv_gbs": spmv_bytes / (ms_spmv.value * 1e-3) / 1e9, "reps": args.steps}))
 
 
+def run_network_only(args):
+    """The learned stage's network alone (for kernel profiles): a handle for a 256^3 grid
+    coarsened by 4 (64^3 coarse voxels), two forward passes on random inputs, CUDA-event
+    time of the second."""
+    import torch
+    from parcel_b import _lib, api
+    L = _lib.load()
+    net = api.Learned(256, 256, 256, 4, seed=1)
+    V = 64 ** 3
+    u = torch.randn(V * 2, dtype=torch.float32, device="cuda")
+    y = torch.zeros(V, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.ExternalStream(L.parcel_b_get_stream(), device=torch.device("cuda", 0))
+    ms = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        assert L.parcel_b_learned_forward(net.handle, 1, u.data_ptr(), y.data_ptr()) == 0, _lib.last_error()
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    flops = 2.0 * V * 27 * (2 * 32 + 4 * 32 * 32 + 32)
+    print(json.dumps({"network_forward_ms": ms[-1], "coarse_voxels": V, "tflops": flops / (ms[-1] * 1e-3) / 1e12}))
+
+
+def run_learned_only(args):
+    """One learned-stage solve for kernel profiles: 256^3 variable-coefficient diffusion,
+    FP32 FGMRES(40) inside FP64 refinement, BJ-ILU(0) 64 blocks, Galerkin coarse stage with
+    --coarse-steps PCG steps from an untrained network's guess (the stage's cost does not
+    depend on the weights), stopped after --itrmax inner iterations."""
+    import torch
+    from parcel_b import _lib, api, problems
+    N, c = args.grid, args.coarsen
+    g = problems.gaussian_random_field(N, corr_len=8.0, variance=2.0, seed=5)
+    A = problems.vardiff3d(N, np.exp(g))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    rp, ci, va, bd = t(A.rowptr), t(A.col), t(A.val), t(problems.rhs_normal(A.n, 1000))
+    net = api.Learned(N, N, N, c, seed=1)
+    net.set_stage(args.coarse_steps, 1)
+    L = _lib.load()
+    p = _lib.new_input(solver=3, ipreflag=2, ILU_method=0, precon_thblock=NBLOCKS, GMRES_m=args.restart,
+                       GMRES_GSflag=1, itrmax=args.itrmax, rtolmax=RTOL, inner_precision=1, inner_rtol=1e-4,
+                       max_refine=80)
+    S = api.crs_struct(A, rp, ci, va)
+    x = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    niter, iret = C.c_int(0), C.c_int(0)
+    t0 = time.perf_counter()
+    rc = L.parcel_b_solve_learned(C.byref(p), C.byref(S), net.handle, bd.data_ptr(), x.data_ptr(), None,
+                                  C.byref(niter), C.byref(iret))
+    torch.cuda.synchronize()
+    assert rc == 0, _lib.last_error()
+    st = _lib.last_stats()
+    print(json.dumps({"iterations": niter.value, "iret": iret.value, "wall_s": time.perf_counter() - t0,
+                      "setup_s": st["setup_s"], "solve_s": st["solve_s"], "kernel_launches": st["kernel_launches"]}))
+
+
 VD_METRIC = "time-to-1e-10 true rel. residual (s), learned + mixed-precision FGMRES vs plain FP64 PGMRES/BJ-ILU"
 
 
@@ -968,6 +1024,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels-only", action="store_true")
+    ap.add_argument("--network", action="store_true", help="with --kernels-only: the learned stage's network alone")
+    ap.add_argument("--learned", action="store_true",
+                    help="with --kernels-only: one learned-stage solve of --itrmax inner iterations")
+    ap.add_argument("--itrmax", type=int, default=80)
     ap.add_argument("--ilu-method", type=int, default=0)
     ap.add_argument("--workload", default="convdiff128",
                     choices=["convdiff128", "vardiff", "ddcg160", "ddgmres128", "poisson2d256", "aniso192",
@@ -1006,6 +1066,10 @@ def main():
         run_ddcg(args)
     elif args.workload == "ddgmres128":
         run_ddgmres(args)
+    elif args.kernels_only and args.network:
+        run_network_only(args)
+    elif args.kernels_only and args.learned:
+        run_learned_only(args)
     elif args.kernels_only:
         run_kernels_only(args)
     elif args.impl == "reference":

@@ -420,6 +420,22 @@ int parcel_b_ddgmres(const parcel_b_input* prm, const parcel_b_crs* A, const dou
 int parcel_b_bench_kernels(const parcel_b_input* prm, const parcel_b_crs* A, int reps,
                            double* ms_spmv, double* ms_precon);
 
+/* ---- one process's share of a row-distributed system ---------------------------------
+ * The GPU side of the multi-process solve (parcel_b/dist.py), which mirrors the reference's
+ * MPI decomposition: contiguous rows per process (src/krylov.f90:447-470), the halo of x
+ * exchanged before every product (src/comm.f90:528-597), block-Jacobi blocks inside each
+ * process (src/matrix.f90:8074-8134).  A holds this process's n rows with local column ids:
+ * 1..n for owned rows, n+1..n_ext for halo values (istart = 1; host or device arrays).  The
+ * preconditioner of prm (none, point Jacobi or block-Jacobi ILU / D-ILU over the owned rows,
+ * precon_thblock blocks) is built on the owned-owned submatrix. */
+typedef struct parcel_b_local_s* parcel_b_local;
+int parcel_b_local_create(const parcel_b_input* prm, const parcel_b_crs* A, int n_ext, parcel_b_local* out);
+/* y[n] = A x_ext[n_ext], device arrays. */
+int parcel_b_local_spmv(parcel_b_local h, const double* x_ext, double* y);
+/* z[n] = M^-1 r[n], device arrays. */
+int parcel_b_local_precon(parcel_b_local h, const double* r, double* z);
+int parcel_b_local_destroy(parcel_b_local h);
+
 /* ---- learned two-level preconditioner stage (no counterpart in the reference) --------
  * Flexible GMRES with the additive two-level preconditioner
  *   z = M^-1 v + P y,   y ~ A_c^-1 P^T v,   A_c = P^T A P  (Galerkin, 27-point),

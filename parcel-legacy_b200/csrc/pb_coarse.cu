@@ -6,12 +6,13 @@
 //                    over the fine cells f whose interpolation involves I; every thread keeps
 //                    private sums for the 27 taps in shared memory and the 27 tap owners add
 //                    the threads' sums in thread order (deterministic).
-//   k_restrict_half  one warp per half cell ((c/2)^3 fine cells that share their two coarse
-//                    parents along every axis): the 8 weighted sums of the half cell.
+//   k_restrict_half  one thread per half cell ((c/2)^3 fine cells that share their two
+//                    coarse parents along every axis): the 8 weighted sums of the half cell.
 //   k_restrict_sum   one thread per coarse cell: adds the half-cell sums that belong to it,
 //                    in a fixed order.
-//   k_prolong_add    one thread per iteration-layout position: z += trilinear(y).
-//   k_coarse_pcg     one thread-block cluster (8 CTAs x 1024 threads), see pcg().
+//   k_prolong_add    one thread per iteration-layout position: z += trilinear(y), the fine
+//                    cell's coordinates read from a packed per-position code (k_pack_coords).
+//   k_coarse_pcg     one thread-block cluster (8 CTAs x 512 threads), see pcg().
 #include <cooperative_groups.h>
 
 #include "pb_coarse.cuh"
@@ -24,10 +25,12 @@ namespace coarse {
 namespace {
 
 constexpr int kGalThreads = 128;
-constexpr int kPcgThreads = 1024;
+constexpr int kPcgThreads = 512;
 constexpr int kPcgCluster = 8;
-constexpr int kPcgMaxCpt = 8;       // coarse cells per thread
+constexpr int kPcgMaxCpt = 16;      // coarse cells per thread
+constexpr int64_t kMaxCoarseCells = 49152;   // the prolongation stages the coarse vector in shared memory
 constexpr int kRmsThreads = 1024;
+constexpr int kProlongThreads = 1024;
 
 // Interpolation along one axis: fine index i -> coarse parents lo, hi (clamped) and the
 // weight w of hi (1 - w of lo).  u = (2 i + 1 - c) / (2 c) exactly.
@@ -118,46 +121,43 @@ __global__ void k_to_f32(int64_t Vc, const double* __restrict__ ac64, float* __r
 }
 
 // Half cell H = (hx, hy, hz) covers fine cells [hx c/2, (hx + 1) c/2) along x (and so on);
-// all of them interpolate from the same two coarse cells per axis.  hc[8 H + 4 cz + 2 cy + cx]
-// = sum over the half cell of v * wz_cz * wy_cy * wx_cx (w_0 = 1 - w, w_1 = w).
+// all of them interpolate from the same two coarse cells per axis, and the weight of the
+// upper one for local offset l is (2 l + 1) / (2 c), plus 1/2 when hx is even.
+// hc[8 H + 4 cz + 2 cy + cx] = sum over the half cell of v * wz_cz * wy_cy * wx_cx
+// (w_0 = 1 - w, w_1 = w), one thread per half cell, summed in z, y, x order.
 template <class T>
 __global__ void __launch_bounds__(256)
     k_restrict_half(Grid g, const T* __restrict__ v, const int* __restrict__ pos, float* __restrict__ hc,
                     const int* gate) {
   if (gated(gate)) return;
-  const int lane = threadIdx.x & 31;
-  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= g.Vh()) return;
+  const int64_t H = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (H >= g.Vh()) return;
   const int hn = 2 * g.gx, hm = 2 * g.gy;
-  const int hx = (int)(w % hn), hy = (int)((w / hn) % hm), hz = (int)(w / ((int64_t)hn * hm));
-  const int hs = g.c / 2, n3 = hs * hs * hs;
-  double m[8];
+  const int hx = (int)(H % hn), hy = (int)((H / hn) % hm), hz = (int)(H / ((int64_t)hn * hm));
+  const int hs = g.c / 2;
+  const float inv2c = 0.5f / (float)g.c;
+  const float ox = (hx & 1) ? 0.f : 0.5f, oy = (hy & 1) ? 0.f : 0.5f, oz = (hz & 1) ? 0.f : 0.5f;
+  float m[8];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) m[k] = 0.0;
-  for (int e = lane; e < n3; e += 32) {
-    const int x = hx * hs + e % hs, y = hy * hs + (e / hs) % hs, z = hz * hs + e / (hs * hs);
-    const int64_t nat = ((int64_t)z * g.ny + y) * g.nx + x;
-    const double val = (double)v[pos ? pos[nat] : nat];
-    int l, u;
-    double wx, wy, wz;
-    lin1(x, g.c, g.gx, l, u, wx);
-    lin1(y, g.c, g.gy, l, u, wy);
-    lin1(z, g.c, g.gz, l, u, wz);
+  for (int k = 0; k < 8; ++k) m[k] = 0.f;
+  for (int lz = 0; lz < hs; ++lz) {
+    const float wz = oz + (float)(2 * lz + 1) * inv2c;
+    for (int ly = 0; ly < hs; ++ly) {
+      const float wy = oy + (float)(2 * ly + 1) * inv2c;
+      const float wyz[4] = {(1.f - wy) * (1.f - wz), wy * (1.f - wz), (1.f - wy) * wz, wy * wz};
+      const int64_t row = ((int64_t)(hz * hs + lz) * g.ny + (hy * hs + ly)) * g.nx + (int64_t)hx * hs;
+      for (int lx = 0; lx < hs; ++lx) {
+        const float wx = ox + (float)(2 * lx + 1) * inv2c;
+        const int64_t nat = row + lx;
+        const float val = (float)v[pos ? pos[nat] : nat];
+        const float a0 = val * (1.f - wx), a1 = val * wx;
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
-      m[k] += val * ((k & 4) ? wz : 1.0 - wz) * ((k & 2) ? wy : 1.0 - wy) * ((k & 1) ? wx : 1.0 - wx);
+        for (int k = 0; k < 8; ++k) m[k] = fmaf((k & 1) ? a1 : a0, wyz[k >> 1], m[k]);
+      }
+    }
   }
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    double s = m[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
-    m[k] = s;
-  }
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) hc[8 * w + k] = (float)m[k];
-  }
+  for (int k = 0; k < 8; ++k) hc[8 * H + k] = m[k];
 }
 
 // Half cells along one axis whose corner (0: lower parent, 1: upper parent) is coarse
@@ -193,30 +193,61 @@ __global__ void __launch_bounds__(256)
   rc[I] = s;
 }
 
-template <class T>
+// Interpolation along one axis in FP32 (c even: u is never an integer, so the rounding of
+// (i + 1/2) / c cannot move floor(u)).
+__device__ __forceinline__ void lin1f(int i, float inv_c, int G, int& lo, int& hi, float& w) {
+  const float u = ((float)i + 0.5f) * inv_c - 0.5f;
+  const float f = floorf(u);
+  w = u - f;
+  const int i0 = (int)f;
+  lo = min(max(i0, 0), G - 1);
+  hi = min(max(i0 + 1, 0), G - 1);
+}
+
+// code[p] = x | y << 10 | z << 20 of the natural row at iteration position p, -1 for padding.
 __global__ void __launch_bounds__(256)
-    k_prolong_add(Grid g, int64_t np, const float* __restrict__ y, const int* __restrict__ rowAt, T* __restrict__ z,
-                  const int* gate) {
-  if (gated(gate)) return;
+    k_pack_coords(Grid g, int64_t np, const int* __restrict__ rowAt, int* __restrict__ code) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= np) return;
   const int64_t nat = rowAt ? (int64_t)rowAt[p] : p;
-  if (nat < 0) return;
-  const int x = (int)(nat % g.nx), yy = (int)((nat / g.nx) % g.ny), zz = (int)(nat / ((int64_t)g.nx * g.ny));
-  int x0, x1, y0, y1, z0, z1;
-  double wx, wy, wz;
-  lin1(x, g.c, g.gx, x0, x1, wx);
-  lin1(yy, g.c, g.gy, y0, y1, wy);
-  lin1(zz, g.c, g.gz, z0, z1, wz);
-  const float fx = (float)wx, fy = (float)wy, fz = (float)wz;
-  auto at = [&](int c, int b, int a) { return __ldg(y + ((int64_t)c * g.gy + b) * g.gx + a); };
-  const float c00 = at(z0, y0, x0) * (1.f - fz) + at(z1, y0, x0) * fz;
-  const float c01 = at(z0, y0, x1) * (1.f - fz) + at(z1, y0, x1) * fz;
-  const float c10 = at(z0, y1, x0) * (1.f - fz) + at(z1, y1, x0) * fz;
-  const float c11 = at(z0, y1, x1) * (1.f - fz) + at(z1, y1, x1) * fz;
-  const float c0 = c00 * (1.f - fy) + c10 * fy;
-  const float c1 = c01 * (1.f - fy) + c11 * fy;
-  z[p] += (T)(c0 * (1.f - fx) + c1 * fx);
+  if (nat < 0) { code[p] = -1; return; }
+  const int x = (int)(nat % g.nx), y = (int)((nat / g.nx) % g.ny), z = (int)(nat / ((int64_t)g.nx * g.ny));
+  code[p] = x | (y << 10) | (z << 20);
+}
+
+// One CTA per SM over a grid-stride range of positions; the coarse vector is first copied
+// into shared memory (the trilinear gathers of neighbouring positions hit scattered coarse
+// cells, which from L1 costs a wavefront per distinct line).
+template <class T>
+__global__ void __launch_bounds__(kProlongThreads)
+    k_prolong_add(Grid g, int64_t np, const float* __restrict__ y, const int* __restrict__ code, T* __restrict__ z,
+                  const int* gate) {
+  if (gated(gate)) return;
+  extern __shared__ float ys[];
+  const int64_t V = g.Vc();
+  for (int64_t i = threadIdx.x; i < V; i += kProlongThreads) ys[i] = __ldg(y + i);
+  __syncthreads();
+  const float inv_c = 1.f / (float)g.c;
+  const int gxy = g.gx * g.gy;
+  for (int64_t p = (int64_t)blockIdx.x * kProlongThreads + threadIdx.x; p < np;
+       p += (int64_t)gridDim.x * kProlongThreads) {
+    const int cd = code[p];
+    if (cd < 0) continue;
+    int x0, x1, y0, y1, z0, z1;
+    float fx, fy, fz;
+    lin1f(cd & 1023, inv_c, g.gx, x0, x1, fx);
+    lin1f((cd >> 10) & 1023, inv_c, g.gy, y0, y1, fy);
+    lin1f(cd >> 20, inv_c, g.gz, z0, z1, fz);
+    const float* p0 = ys + z0 * gxy;
+    const float* p1 = ys + z1 * gxy;
+    const float c00 = p0[y0 * g.gx + x0] * (1.f - fz) + p1[y0 * g.gx + x0] * fz;
+    const float c01 = p0[y0 * g.gx + x1] * (1.f - fz) + p1[y0 * g.gx + x1] * fz;
+    const float c10 = p0[y1 * g.gx + x0] * (1.f - fz) + p1[y1 * g.gx + x0] * fz;
+    const float c11 = p0[y1 * g.gx + x1] * (1.f - fz) + p1[y1 * g.gx + x1] * fz;
+    const float c0 = c00 * (1.f - fy) + c10 * fy;
+    const float c1 = c01 * (1.f - fy) + c11 * fy;
+    z[p] += (T)(c0 * (1.f - fx) + c1 * fx);
+  }
 }
 
 __global__ void __launch_bounds__(kRmsThreads) k_rms(int64_t V, const float* __restrict__ v, float* __restrict__ scal,
@@ -282,23 +313,35 @@ __device__ __forceinline__ void cluster_sum(double (&v)[N], double* wred, double
   }
 }
 
+// pe holds this CTA's ppr coarse planes of the search direction between one halo plane
+// below and one above: exchange() publishes the CTA's planes, waits for the cluster and
+// copies the neighbours' boundary planes into the halos (zero at the grid's ends), so the
+// product reads shared memory only.
 template <int CPT>
 __global__ void __launch_bounds__(kPcgThreads, 1) k_coarse_pcg(PcgK K) {
-  extern __shared__ float p_s[];                   // this CTA's part of the search direction
+  extern __shared__ float pe[];                    // (ppr + 2) planes
   __shared__ double wred[2 * kPcgThreads / 32];
   __shared__ double slots[2][2 * kPcgCluster];     // alternating tables of the cluster sums
-  __shared__ float* ptab[kPcgCluster];
   const PcgArgs& a = K.a;
   if (gated(a.gate)) return;                      // every CTA reads the same flag
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank(), ncta = (int)cl.num_blocks();
-  const int gx = a.g.gx, gy = a.g.gy, gz = a.g.gz;
-  const int64_t Vc = a.g.Vc(), gxy = (int64_t)gx * gy;
-  if (threadIdx.x < ncta) ptab[threadIdx.x] = cl.map_shared_rank(p_s, (int)threadIdx.x);
+  const int gx = a.g.gx, gy = a.g.gy;
+  const int gxy = gx * gy;
+  const int64_t Vc = a.g.Vc();
   const int64_t base = (int64_t)rank * K.chunk;
   const int64_t left = Vc - base;
   const int nloc = left <= 0 ? 0 : (int)(left < K.chunk ? left : K.chunk);
+  const int64_t left_next = Vc - base - K.chunk;
+  const bool has_prev = rank > 0 && nloc > 0;
+  const bool has_next = rank + 1 < ncta && left_next > 0;
   float y[CPT], r[CPT], p[CPT], d[CPT], q[CPT];
+  int cxy[CPT];                                    // x | y << 10 | local plane << 20
+  const int halo_hi = (K.ppr + 1) * gxy;
+  for (int i = threadIdx.x; i < gxy; i += kPcgThreads) {
+    pe[i] = 0.f;
+    pe[halo_hi + i] = 0.f;
+  }
   int par = 0;
   auto sum1 = [&](double x) {
     double v[1] = {x};
@@ -306,7 +349,24 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_coarse_pcg(PcgK K) {
     par ^= 1;
     return v[0];
   };
-  // q = A_c p_s over the local cells (p_s of all CTAs complete: caller synchronised).
+  auto exchange = [&](const float (&src)[CPT]) {
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+      const int i = threadIdx.x + k * kPcgThreads;
+      if (i < nloc) pe[gxy + i] = src[k];
+    }
+    cl.sync();
+    if (has_prev) {
+      const float* rp = cl.map_shared_rank(pe, rank - 1) + (size_t)K.ppr * gxy;   // its last plane
+      for (int i = threadIdx.x; i < gxy; i += kPcgThreads) pe[i] = rp[i];
+    }
+    if (has_next) {
+      const float* rn = cl.map_shared_rank(pe, rank + 1) + gxy;                    // its first plane
+      for (int i = threadIdx.x; i < gxy; i += kPcgThreads) pe[halo_hi + i] = rn[i];
+    }
+    __syncthreads();
+  };
+  // q = A_c (the exchanged vector) over the local cells
   auto spmv = [&]() {
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
@@ -314,37 +374,32 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_coarse_pcg(PcgK K) {
       q[k] = 0.f;
       if (i >= nloc) continue;
       const int64_t I = base + i;
-      const int Ix = (int)(I % gx), Iy = (int)((I / gx) % gy), Iz = (int)(I / gxy);
+      const int x = cxy[k] & 1023, yy = (cxy[k] >> 10) & 1023, lz = cxy[k] >> 20;
+      const float* c0 = pe + (lz + 1) * gxy + yy * gx + x;
       float s = 0.f;
 #pragma unroll
       for (int t = 0; t < kTaps; ++t) {
         const int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
-        const int jx = Ix + dx, jy = Iy + dy, jz = Iz + dz;
-        if (jx < 0 || jx >= gx || jy < 0 || jy >= gy || jz < 0 || jz >= gz) continue;
-        const int owner = jz / K.ppr;
-        const int64_t loc = (int64_t)(jz - owner * K.ppr) * gxy + (int64_t)jy * gx + jx;
-        s += __ldg(a.ac + (int64_t)t * Vc + I) * ptab[owner][loc];
+        if ((dx < 0 && x == 0) || (dx > 0 && x == gx - 1) || (dy < 0 && yy == 0) || (dy > 0 && yy == gy - 1))
+          continue;
+        s += __ldg(a.ac + (int64_t)t * Vc + I) * c0[dz * gxy + dy * gx + dx];
       }
       q[k] = s;
     }
   };
-  cl.sync();   // ptab written, and every CTA of the cluster running before any remote access
 #pragma unroll
   for (int k = 0; k < CPT; ++k) {
     const int i = threadIdx.x + k * kPcgThreads;
     const bool in = i < nloc;
+    cxy[k] = in ? ((i % gx) | (((i / gx) % gy) << 10) | ((i / gxy) << 20)) : 0;
     r[k] = in ? a.rc[base + i] : 0.f;
     d[k] = in ? a.dinv[base + i] : 0.f;
     y[k] = (in && a.g0) ? a.g0[base + i] : 0.f;
   }
+  cl.sync();   // halos zeroed, and every CTA of the cluster running before any remote access
   if (a.g0) {
     // y = gamma g0 with gamma = <rc, g0> / <g0, A_c g0>; r = rc - gamma A_c g0
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-      const int i = threadIdx.x + k * kPcgThreads;
-      if (i < nloc) p_s[i] = y[k];
-    }
-    cl.sync();
+    exchange(y);
     spmv();
     double v[2] = {0.0, 0.0};
 #pragma unroll
@@ -370,12 +425,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_coarse_pcg(PcgK K) {
   rz = sum1(rz);
   for (int it = 0; it < a.steps; ++it) {
     if (!(fabs(rz) > 0.0)) break;               // converged or NaN: the same in every CTA
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-      const int i = threadIdx.x + k * kPcgThreads;
-      if (i < nloc) p_s[i] = p[k];
-    }
-    cl.sync();
+    exchange(p);
     spmv();
     double pq = 0.0;
 #pragma unroll
@@ -408,13 +458,18 @@ int pcg_ppr(const Grid& g) { return (g.gz + kPcgCluster - 1) / kPcgCluster; }
 
 }  // namespace
 
-int64_t max_coarse_cells() { return (int64_t)kPcgCluster * kPcgThreads * kPcgMaxCpt; }
+int64_t max_coarse_cells() { return kMaxCoarseCells; }
 
 void check_grid(const Grid& g) {
   PB_CHECK(g.c >= 2 && g.c % 2 == 0, PARCEL_B_E_ARG, "the coarse-grid stage needs an even coarsening factor (%d)",
            g.c);
   PB_CHECK(g.nx % g.c == 0 && g.ny % g.c == 0 && g.nz % g.c == 0 && g.gx > 0 && g.gy > 0 && g.gz > 0,
            PARCEL_B_E_ARG, "grid %d x %d x %d is not divisible by the coarsening factor %d", g.nx, g.ny, g.nz, g.c);
+  PB_CHECK(g.nx <= 1024 && g.ny <= 1024 && g.nz <= 1024, PARCEL_B_E_UNSUPPORTED,
+           "the coarse-grid stage supports at most 1024 cells per axis (grid %d x %d x %d)", g.nx, g.ny, g.nz);
+  PB_CHECK(g.Vc() <= kMaxCoarseCells, PARCEL_B_E_UNSUPPORTED,
+           "coarse grid %d x %d x %d has more than %lld cells: use a larger coarsening factor", g.gx, g.gy, g.gz,
+           (long long)kMaxCoarseCells);
   const int64_t chunk = (int64_t)pcg_ppr(g) * g.gx * g.gy;
   PB_CHECK(chunk <= (int64_t)kPcgThreads * kPcgMaxCpt, PARCEL_B_E_UNSUPPORTED,
            "coarse grid %d x %d x %d is too large for the one-cluster coarse solver (at most %d cells per CTA, "
@@ -438,16 +493,27 @@ void to_f32(int64_t Vc, const double* ac64, float* ac32, float* dinv32, cudaStre
 template <class T>
 void restrict_fine(const Grid& g, const T* v, const int* pos, float* hc, float* rc, const int* gate,
                    cudaStream_t st) {
-  const int64_t warps = g.Vh();
-  k_restrict_half<T><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(g, v, pos, hc, gate);
+  k_restrict_half<T><<<(unsigned)((g.Vh() + 255) / 256), 256, 0, st>>>(g, v, pos, hc, gate);
   k_restrict_sum<<<(unsigned)((g.Vc() + 255) / 256), 256, 0, st>>>(g, hc, rc, gate);
   PB_CUDA(cudaGetLastError());
 }
 
+void pack_coords(const Grid& g, int64_t np, const int* rowAt, int* code, cudaStream_t st) {
+  k_pack_coords<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(g, np, rowAt, code);
+  PB_CUDA(cudaGetLastError());
+}
+
 template <class T>
-void prolong_add(const Grid& g, int64_t np, const float* y, const int* rowAt, T* z, const int* gate,
+void prolong_add(const Grid& g, int64_t np, const float* y, const int* code, T* z, const int* gate,
                  cudaStream_t st) {
-  k_prolong_add<T><<<(unsigned)((np + 255) / 256), 256, 0, st>>>(g, np, y, rowAt, z, gate);
+  const size_t smem = sizeof(float) * (size_t)g.Vc();
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[sizeof(T) == 8]) {   // before any stream capture: the stage's constructor calls this first
+    PB_CUDA(cudaFuncSetAttribute(k_prolong_add<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(float) * kMaxCoarseCells)));
+    attr_set[sizeof(T) == 8] = true;
+  }
+  k_prolong_add<T><<<num_sms(), kProlongThreads, smem, st>>>(g, np, y, code, z, gate);
   PB_CUDA(cudaGetLastError());
 }
 
@@ -466,7 +532,7 @@ void pcg(const PcgArgs& a, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(kPcgCluster);
   cfg.blockDim = dim3(kPcgThreads);
-  cfg.dynamicSmemBytes = sizeof(float) * (size_t)K.chunk;
+  cfg.dynamicSmemBytes = sizeof(float) * (size_t)(K.ppr + 2) * a.g.gx * a.g.gy;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -478,7 +544,8 @@ void pcg(const PcgArgs& a, cudaStream_t st) {
   if (cpt <= 1) PB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_pcg<1>, K));
   else if (cpt <= 2) PB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_pcg<2>, K));
   else if (cpt <= 4) PB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_pcg<4>, K));
-  else PB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_pcg<8>, K));
+  else if (cpt <= 8) PB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_pcg<8>, K));
+  else PB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_pcg<16>, K));
 }
 
 template void restrict_fine<float>(const Grid&, const float*, const int*, float*, float*, const int*, cudaStream_t);

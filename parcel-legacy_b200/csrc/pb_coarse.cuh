@@ -35,8 +35,10 @@ struct Grid {
   __host__ __device__ int64_t Vh() const { return (int64_t)8 * gx * gy * gz; }   // half cells
 };
 
-// Throws unless the grid suits the transfer operators (c even, dims divisible by c) and
-// the coarse problem fits one thread-block cluster of the coarse solver.
+// Throws unless the grid suits the transfer operators (c even, dims divisible by c, at most
+// 1024 cells per axis) and the coarse problem has at most max_coarse_cells() cells (49,152:
+// the prolongation keeps the coarse vector in shared memory) and fits one thread-block
+// cluster of the coarse solver.
 void check_grid(const Grid& g);
 int64_t max_coarse_cells();
 
@@ -51,10 +53,12 @@ void to_f32(int64_t Vc, const double* ac64, float* ac32, float* dinv32, cudaStre
 template <class T>
 void restrict_fine(const Grid& g, const T* v, const int* pos, float* hc, float* rc, const int* gate,
                    cudaStream_t st);
-// z[p] += (P y)(natural row rowAt[p]) for p < np (rowAt NULL: p is the natural row;
-// rowAt[p] < 0 marks layout padding, left untouched).
+// code[p] = x | y << 10 | z << 20 of the natural row rowAt[p] (rowAt NULL: p itself), -1
+// where rowAt[p] < 0 (layout padding).
+void pack_coords(const Grid& g, int64_t np, const int* rowAt, int* code, cudaStream_t st);
+// z[p] += (P y)(fine cell code[p]) for p < np; code[p] < 0 is left untouched.
 template <class T>
-void prolong_add(const Grid& g, int64_t np, const float* y, const int* rowAt, T* z, const int* gate,
+void prolong_add(const Grid& g, int64_t np, const float* y, const int* code, T* z, const int* gate,
                  cudaStream_t st);
 // scal[0] = 1 / rms(v), scal[1] = rms(v) over Vc entries (0, 0 for v == 0); one CTA.
 void rms(int64_t Vc, const float* v, float* scal, const int* gate, cudaStream_t st);

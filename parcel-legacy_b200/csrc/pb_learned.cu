@@ -95,10 +95,9 @@ template <class T>
 struct TwoLevelStage final : ExtraStage<T> {
   const Learned* L;
   CoarseOp op;
-  DBuf hc, rc, y, scal, dhat;
+  DBuf hc, rc, y, scal, dhat, code;
   cnn::Acts acts;
   const int* pos = nullptr;
-  const int* rowAt = nullptr;
   int64_t np = 0;
   int steps = 0;
   bool net = false;
@@ -109,10 +108,9 @@ struct TwoLevelStage final : ExtraStage<T> {
     steps = L->coarse_steps;
     net = L->use_net;
     np = S.np;
-    if (S.permuted) {
-      pos = dp<int>(S.pos);
-      rowAt = dp<int>(S.rowAt);
-    }
+    if (S.permuted) pos = dp<int>(S.pos);
+    code.alloc(sizeof(int) * np);
+    coarse::pack_coords(op.g, np, S.permuted ? dp<int>(S.rowAt) : nullptr, dp<int>(code), stream());
     const int64_t V = op.g.Vc();
     hc.alloc(sizeof(float) * 8 * op.g.Vh());
     rc.alloc(sizeof(float) * V);
@@ -148,7 +146,7 @@ struct TwoLevelStage final : ExtraStage<T> {
   }
   void apply(const System<T>&, const T*, T* z, T*, const int* gate, cudaStream_t st) override {
     PB_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
-    coarse::prolong_add<T>(op.g, np, dp<float>(y), rowAt, z, gate, st);
+    coarse::prolong_add<T>(op.g, np, dp<float>(y), dp<int>(code), z, gate, st);
   }
   bool provides_az() const override { return false; }
   int launches() const override { return net ? 12 : 4; }
@@ -443,10 +441,11 @@ int parcel_b_learned_transfer(parcel_b_learned h, int to_coarse, const double* i
       if (is_device_ptr(in)) d2h(hin.data(), in, sizeof(double) * V);
       else memcpy(hin.data(), in, sizeof(double) * V);
       std::vector<float> hf(hin.begin(), hin.end());
-      DBuf yc(sizeof(float) * V), z(sizeof(double) * n);
+      DBuf yc(sizeof(float) * V), z(sizeof(double) * n), code(sizeof(int) * n);
       h2d(yc.p, hf.data(), sizeof(float) * V);
       PB_CUDA(cudaMemsetAsync(z.p, 0, sizeof(double) * n, st));
-      coarse::prolong_add<double>(g, n, dp<float>(yc), nullptr, dp<double>(z), nullptr, st);
+      coarse::pack_coords(g, n, nullptr, dp<int>(code), st);
+      coarse::prolong_add<double>(g, n, dp<float>(yc), dp<int>(code), dp<double>(z), nullptr, st);
       if (is_device_ptr(out)) { d2d(out, z.p, sizeof(double) * n); sync(); }
       else d2h(out, z.p, sizeof(double) * n);
     }

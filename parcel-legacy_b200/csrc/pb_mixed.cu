@@ -91,7 +91,9 @@ MixedResult solve_mixed_on(const Options& o, System<float>& S, const double* b, 
     else convert<float, double>(n, dp<float>(r32), dp<double>(r), st);
     PB_CUDA(cudaMemsetAsync(d32.p, 0, sizeof(float) * np, st));
     oi.itrmax = o.itrmax - total;
+    trace_mark("refine: outer residual");
     SolveOut so = run_krylov<float>(oi, S, dp<float>(r32), dp<float>(d32), dp<double>(hist_dev));
+    trace_mark("refine: inner solve");
     res.launches += so.launches + 2;
     if (so.niter > 0) {
       std::vector<double> h(so.niter);

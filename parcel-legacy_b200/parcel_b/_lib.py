@@ -133,6 +133,10 @@ SIGNATURES = {
     "parcel_ddgmres_dia_c_": (None, [IP, P, P, P, P, I32P, I32P, I32P, P, P, P, I32P] + [IP] * 5 + [DP, P] +
                               [IP] * 11),
     "parcel_b_bench_kernels": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, DP, DP]),
+    "parcel_b_local_create": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, C.POINTER(P)]),
+    "parcel_b_local_spmv": (C.c_int, [P, P, P]),
+    "parcel_b_local_precon": (C.c_int, [P, P, P]),
+    "parcel_b_local_destroy": (C.c_int, [P]),
     "parcel_b_learned_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(P)]),
     "parcel_b_learned_destroy": (C.c_int, [P]),
     "parcel_b_learned_num_params": (C.c_int64, []),

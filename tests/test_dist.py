@@ -1,0 +1,124 @@
+"""The row-distributed solve (parcel_b/dist.py) on CPU processes over gloo.
+
+Two (and three) processes split the rows of a matrix contiguously at block-Jacobi block
+boundaries; each runs the distributed recurrences with a test backend: its local product
+in numpy and its block-Jacobi ILU(0) from the oracle on its owned-owned submatrix.  The
+histories must reproduce the single-process oracle solve with the same blocks (the inner
+products sum the per-process partials in rank order, so they differ from one process's
+order by round-off only, which grows as the residual falls: 1e-8 relative while the
+residual is above 1e-8 of its start, against the 1e-6 of the solver parity tests),
+with the same iteration counts and return codes.  This covers the host logic of the
+decomposition (layout, halo plan, exchange, reductions, recurrences); the GPU backend runs
+in tests/test_gpu_dist.py."""
+import multiprocessing as mp
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+class NumpyLocal:
+    """Test backend: the process's rows as a scipy matrix over [owned | halo] and the
+    oracle's block-Jacobi ILU on the owned-owned submatrix."""
+
+    def __init__(self, lay, val, nblocks, ipreflag):
+        import scipy.sparse as sp
+        import torch
+
+        import oracle
+        from parcel_b import problems
+        rp = lay.rowptr.astype(np.int64) - 1
+        ci = lay.local_col.astype(np.int64) - 1
+        self.torch = torch
+        self.A = sp.csr_matrix((val, ci, rp), shape=(lay.n, lay.n_ext))
+        own = self.A[:, :lay.n].tocsr()
+        own.sort_indices()
+        Aoo = problems.CRS(n=lay.n, rowptr=(own.indptr + 1).astype(np.int32), col=(own.indices + 1).astype(np.int32),
+                           val=own.data.astype(np.float64))
+        self.M = oracle.Precon(oracle.Matrix(Aoo), ipreflag=ipreflag, ILU_method=0, precon_thblock=nblocks)
+
+    def spmv(self, x_ext, y):
+        y.copy_(self.torch.from_numpy(self.A @ x_ext.numpy()))
+
+    def precon(self, r, z):
+        z.copy_(self.torch.from_numpy(np.asarray(self.M(r.numpy().copy()), dtype=np.float64)))
+
+
+def _problem(kind):
+    from parcel_b import problems
+    if kind == "cg":
+        A, b, _ = problems.poisson3d_reference(12, 12, 12)
+        return A, b, dict(solver=1, itrmax=500, rtolmax=1e-9)
+    A = problems.convdiff3d_upwind(12)
+    b = problems.rhs_normal(A.n, 3)
+    return A, b, dict(solver=3, itrmax=500, rtolmax=1e-10, GMRES_m=10, GMRES_GSflag=1)
+
+
+def _worker(rank, world, port, kind, nblocks, q):
+    try:
+        sys.path[:0] = [os.path.join(ROOT, "parcel-legacy_b200"), os.path.join(ROOT, "oracle")]
+        import torch
+        import torch.distributed as dist
+
+        from parcel_b import dist as pdist
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+        A, b, kw = _problem(kind)
+        per = A.n // world                         # block boundaries: n and nblocks divide evenly
+        lo, hi = rank * per, (rank + 1) * per
+        rp = A.rowptr[lo:hi + 1] - A.rowptr[lo] + 1
+        k0, k1 = A.rowptr[lo] - 1, A.rowptr[hi] - 1
+        lay = pdist.Layout(hi - lo, A.n, lo + 1, rp, A.col[k0:k1])
+        be = NumpyLocal(lay, A.val[k0:k1], nblocks // world, 2)
+        x = torch.zeros(hi - lo, dtype=torch.float64)
+        niter, iret, hist = pdist.solve(lay, A.val[k0:k1], torch.from_numpy(b[lo:hi].copy()), x, backend=be, **kw)
+        q.put((rank, niter, iret, hist, x.numpy(), lay.n_ext - lay.n))
+        dist.destroy_process_group()
+    except Exception as e:  # pragma: no cover - reported to the parent
+        import traceback
+        q.put((rank, "error", traceback.format_exc(), None, None, None))
+
+
+def _run(kind, world, nblocks):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, kind, nblocks, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+    for o in out:
+        assert o[1] != "error", o[2]
+    return sorted(out, key=lambda o: o[0])
+
+
+@pytest.mark.parametrize("kind,world", [("cg", 2), ("gmres", 2), ("gmres", 3)])
+def test_distributed_solve_reproduces_single_process_history(kind, world):
+    import oracle
+    nblocks = 2 * world
+    A, b, kw = _problem(kind)
+    if A.n % world or (A.n // world) % (nblocks // world):
+        pytest.skip("rows do not split evenly")
+    xo, ho, no, io = oracle.solve(A, b, ipreflag=2, ILU_method=0, precon_thblock=nblocks, **kw)
+    out = _run(kind, world, nblocks)
+    for rank, niter, iret, hist, x, nhalo in out:
+        assert (niter, iret) == (no, io), (rank, niter, iret, no, io)
+        m = ho[:niter] > 1e-8 * ho[0]
+        assert np.max(np.abs(hist[m] - ho[:niter][m]) / ho[:niter][m]) < 1e-8
+        assert nhalo > 0
+    x = np.concatenate([o[4] for o in out])
+    assert np.max(np.abs(x - xo)) <= 1e-8 * np.max(np.abs(xo))
