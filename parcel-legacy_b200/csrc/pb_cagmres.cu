@@ -75,6 +75,107 @@ __global__ void __launch_bounds__(256) k_tsgemm_atb(int64_t n, const double* __r
   }
 }
 
+// Partial C = A^T B, register-blocked, for p <= 64 and q <= QM: thread (mb, g) accumulates
+// the 2 x q outputs of A columns 2 mb, 2 mb + 1 over the rows g, g + G, ... of every tile
+// (G = 512 / ceil(p / 2) row groups).  Tiles of R rows (a multiple of 32 chosen so that three
+// fill the shared memory) are staged row-major with an odd row stride (the column-wise fills
+// and the row-wise reads are both free of bank conflicts) by asynchronous 8-byte copies,
+// three deep: two tiles stream in while one is multiplied, which keeps enough bytes in
+// flight per SM for HBM speed.  At the end the row groups' sums are added in group order.
+// The reads of A and B are the only HBM traffic.
+constexpr int kTsRbMaxP = 64;
+constexpr int kTsRbStages = 3;
+constexpr int kTsRbSmem = 200 * 1024;
+constexpr int kTsRbThreads = 512;
+constexpr int kTsRbMB = 2;          // A columns per thread
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <int QM>
+__global__ void __launch_bounds__(kTsRbThreads, 1) k_tsgemm_rb(int64_t n, const double* __restrict__ A, int64_t lda,
+                                                              int p, const double* __restrict__ B, int64_t ldb, int q,
+                                                              int R, double* __restrict__ part) {
+  extern __shared__ double sh[];
+  const int npb = (p + kTsRbMB - 1) / kTsRbMB;
+  const int G = kTsRbThreads / npb;
+  const int pw = kTsRbMB * npb;
+  const int stride = (pw + QM) | 1;                   // odd
+  const int tile = R * stride;
+  double* out = sh + kTsRbStages * tile;              // [pw][QM] group sums
+  const int mb = threadIdx.x % npb, g = threadIdx.x / npb;
+  const bool active = g < G;
+  for (int i = threadIdx.x; i < kTsRbStages * tile + pw * QM; i += kTsRbThreads) sh[i] = 0.0;
+  __syncthreads();
+  double acc[kTsRbMB][QM];
+#pragma unroll
+  for (int k = 0; k < kTsRbMB; ++k)
+#pragma unroll
+    for (int j = 0; j < QM; ++j) acc[k][j] = 0.0;
+  const int64_t step = (int64_t)gridDim.x * R;
+  const int64_t first = (int64_t)blockIdx.x * R;
+  // copies tile t (rows first + t step ...) into its stage; rows past n become zeros; an
+  // empty group is committed past the end so that the group count stays uniform
+  auto fill = [&](int64_t t) {
+    const int64_t r0 = first + t * step;
+    if (r0 < n) {
+      double* tb = sh + (t % kTsRbStages) * tile;
+      const int cols = p + q;
+      for (int idx = threadIdx.x; idx < cols * R; idx += kTsRbThreads) {
+        const int c = idx / R, rr = idx - c * R;
+        const int64_t row = r0 + rr;
+        double* dst = tb + rr * stride + (c < p ? c : pw + (c - p));
+        if (row < n) cp_async8(dst, c < p ? A + (size_t)c * lda + row : B + (size_t)(c - p) * ldb + row);
+        else *dst = 0.0;   // this stage is not being read: the round that read it ended with a barrier
+      }
+    }
+    cp_async_commit();
+  };
+  fill(0);
+  fill(1);
+  for (int64_t t = 0; first + t * step < n; ++t) {
+    cp_async_wait<1>();   // tile t has landed (only tile t + 1 may still be in flight)
+    __syncthreads();
+    const double* tb = sh + (t % kTsRbStages) * tile;
+    if (active) {
+      for (int rr = g; rr < R; rr += G) {
+        const double* rowp = tb + rr * stride;
+        double a[kTsRbMB], b[QM];
+#pragma unroll
+        for (int k = 0; k < kTsRbMB; ++k) a[k] = rowp[kTsRbMB * mb + k];
+#pragma unroll
+        for (int j = 0; j < QM; ++j) b[j] = rowp[pw + j];
+#pragma unroll
+        for (int k = 0; k < kTsRbMB; ++k)
+#pragma unroll
+          for (int j = 0; j < QM; ++j) acc[k][j] += a[k] * b[j];
+      }
+    }
+    __syncthreads();      // stage t % 3 is refilled two rounds later
+    fill(t + 2);
+  }
+  cp_async_wait<0>();
+  // row groups' sums, added in group order
+  for (int gg = 0; gg < G; ++gg) {
+    if (active && g == gg) {
+#pragma unroll
+      for (int k = 0; k < kTsRbMB; ++k)
+#pragma unroll
+        for (int j = 0; j < QM; ++j) out[(kTsRbMB * mb + k) * QM + j] += acc[k][j];
+    }
+    __syncthreads();
+  }
+  const int pq = p * q;
+  for (int idx = threadIdx.x; idx < pq; idx += kTsRbThreads) {
+    const int i = idx % p, j = idx / p;
+    part[(size_t)blockIdx.x * pq + idx] = out[i * QM + j];
+  }
+}
+
 // out[idx] = sum over blocks b (in order) of part[b*pq + idx]
 __global__ void k_sum_parts(const double* __restrict__ part, int nblk, int pq, double* __restrict__ out) {
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < pq; idx += gridDim.x * blockDim.x) {
@@ -202,10 +303,34 @@ int tsgemm_blocks() { return 2 * num_sms(); }
 // C (p x q) = A^T B on the host, A/B device panels of n rows.
 Mat tsgemm(Dev& D, int64_t n, const double* A, int64_t lda, int p, const double* B, int64_t ldb, int q) {
   PB_CHECK(p * q <= kTsMaxPQ, PARCEL_B_E_UNSUPPORTED, "block product %dx%d too large", p, q);
-  const int nb = tsgemm_blocks();
+  int nb = tsgemm_blocks();
   cudaStream_t st = stream();
-  const size_t smem = sizeof(double) * (size_t)(p + q) * kTsRows;
-  k_tsgemm_atb<<<nb, 256, smem, st>>>(n, A, lda, p, B, ldb, q, dp<double>(D.part));
+  if (p <= kTsRbMaxP && q <= 16) {
+    const int pw = kTsRbMB * ((p + kTsRbMB - 1) / kTsRbMB);
+    auto launch = [&](auto kern, int QM) {
+      const int stride = (pw + QM) | 1;
+      int R = (int)((kTsRbSmem - sizeof(double) * pw * QM) / (sizeof(double) * kTsRbStages * stride));
+      R = std::max(32, std::min(512, R / 32 * 32));
+      const size_t smem = sizeof(double) * ((size_t)kTsRbStages * R * stride + (size_t)pw * QM);
+      static bool attr[17] = {};
+      if (!attr[QM]) {
+        PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kTsRbSmem));
+        attr[QM] = true;
+      }
+      kern<<<num_sms(), kTsRbThreads, smem, st>>>(n, A, lda, p, B, ldb, q, R, dp<double>(D.part));
+      return num_sms();
+    };
+    int used;
+    if (q <= 4) used = launch(k_tsgemm_rb<4>, 4);
+    else if (q <= 8) used = launch(k_tsgemm_rb<8>, 8);
+    else if (q <= 9) used = launch(k_tsgemm_rb<9>, 9);
+    else if (q <= 12) used = launch(k_tsgemm_rb<12>, 12);
+    else used = launch(k_tsgemm_rb<16>, 16);
+    nb = used;
+  } else {
+    const size_t smem = sizeof(double) * (size_t)(p + q) * kTsRows;
+    k_tsgemm_atb<<<nb, 256, smem, st>>>(n, A, lda, p, B, ldb, q, dp<double>(D.part));
+  }
   PB_CUDA(cudaGetLastError());
   k_sum_parts<<<(p * q + 127) / 128, 128, 0, st>>>(dp<double>(D.part), nb, p * q, dp<double>(D.out));
   PB_CUDA(cudaGetLastError());
