@@ -186,34 +186,48 @@ __global__ void k_sum_parts(const double* __restrict__ part, int nblk, int pq, d
 }
 
 // V(:, c) = V(:, c) - sum_j Q(:, j) R(j, c) for c < q, j < p (CAGMRES_GEMM order).
-__global__ void k_block_update(int64_t n, double* __restrict__ V, int64_t ldv, int q,
-                               const double* __restrict__ Q, int64_t ldq, int p,
-                               const double* __restrict__ R /* p x q, ld p */) {
+// V(:, 0..q-1) -= Q(:, 0..p-1) R (R p x q, ld p), one thread per row; QM >= q is a
+// compile-time bound, so the row's q values stay in registers.
+template <int QM>
+__global__ void __launch_bounds__(256) k_block_update(int64_t n, double* __restrict__ V, int64_t ldv, int q,
+                                                      const double* __restrict__ Q, int64_t ldq, int p,
+                                                      const double* __restrict__ R) {
   extern __shared__ double Rs[];
   for (int i = threadIdx.x; i < p * q; i += blockDim.x) Rs[i] = R[i];
   __syncthreads();
   for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x) {
-    double acc[16];
-    for (int c = 0; c < q; ++c) acc[c] = V[(size_t)c * ldv + row];
+    double acc[QM];
+#pragma unroll
+    for (int c = 0; c < QM; ++c) acc[c] = c < q ? V[(size_t)c * ldv + row] : 0.0;
     for (int j = 0; j < p; ++j) {
       const double qv = Q[(size_t)j * ldq + row];
-      for (int c = 0; c < q; ++c) acc[c] = acc[c] - qv * Rs[c * p + j];
+#pragma unroll
+      for (int c = 0; c < QM; ++c)
+        if (c < q) acc[c] = acc[c] - qv * Rs[c * p + j];
     }
-    for (int c = 0; c < q; ++c) V[(size_t)c * ldv + row] = acc[c];
+#pragma unroll
+    for (int c = 0; c < QM; ++c)
+      if (c < q) V[(size_t)c * ldv + row] = acc[c];
   }
 }
 
-// Q(:, k) = sum_{j<=k} V(:, j) Rinv(j, k), c columns.
-__global__ void k_apply_rinv(int64_t n, const double* __restrict__ V, int64_t ldv, int c,
-                             const double* __restrict__ Ri, double* __restrict__ Q, int64_t ldq) {
+// Q(:, k) = sum_{j <= k} V(:, j) Ri(j, k), one thread per row, the row in registers.
+template <int CM>
+__global__ void __launch_bounds__(256) k_apply_rinv(int64_t n, const double* __restrict__ V, int64_t ldv, int c,
+                                                    const double* __restrict__ Ri, double* __restrict__ Q,
+                                                    int64_t ldq) {
   __shared__ double Rs[16 * 16];
   for (int i = threadIdx.x; i < c * c; i += blockDim.x) Rs[i] = Ri[i];
   __syncthreads();
   for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x) {
-    double v[16];
-    for (int j = 0; j < c; ++j) v[j] = V[(size_t)j * ldv + row];
-    for (int k = 0; k < c; ++k) {
+    double v[CM];
+#pragma unroll
+    for (int j = 0; j < CM; ++j) v[j] = j < c ? V[(size_t)j * ldv + row] : 0.0;
+#pragma unroll
+    for (int k = 0; k < CM; ++k) {
+      if (k >= c) break;
       double s = 0.0;
+#pragma unroll
       for (int j = 0; j <= k; ++j) s += v[j] * Rs[k * c + j];
       Q[(size_t)k * ldq + row] = s;
     }
@@ -383,7 +397,8 @@ void apply_rinv(Dev& D, int64_t n, const double* V, int64_t ldv, const Mat& Ri, 
   D.small.alloc(sizeof(double) * c * c);
   h2d(D.small.p, Ri.a.data(), sizeof(double) * c * c);
   const int grid = std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 8 * num_sms()));
-  k_apply_rinv<<<grid, 256, 0, stream()>>>(n, V, ldv, c, dp<double>(D.small), Q, ldq);
+  if (c <= 8) k_apply_rinv<8><<<grid, 256, 0, stream()>>>(n, V, ldv, c, dp<double>(D.small), Q, ldq);
+  else k_apply_rinv<16><<<grid, 256, 0, stream()>>>(n, V, ldv, c, dp<double>(D.small), Q, ldq);
   PB_CUDA(cudaGetLastError());
 }
 
@@ -642,8 +657,12 @@ SolveOut solve_cagmres(const Options& o, System<double>& S, const double* b_nat,
         D.small.alloc(sizeof(double) * s1 * s);
         h2d(D.small.p, Rsub.a.data(), sizeof(double) * s1 * s);
         const int grid = std::max<int64_t>(1, std::min<int64_t>((np + 255) / 256, 8 * num_sms()));
-        k_block_update<<<grid, 256, sizeof(double) * s1 * s, st>>>(np, col(V, 1), ldv, s, Q, ldv, s1,
-                                                                     dp<double>(D.small));
+        if (s <= 8)
+          k_block_update<8><<<grid, 256, sizeof(double) * s1 * s, st>>>(np, col(V, 1), ldv, s, Q, ldv, s1,
+                                                                        dp<double>(D.small));
+        else
+          k_block_update<16><<<grid, 256, sizeof(double) * s1 * s, st>>>(np, col(V, 1), ldv, s, Q, ldv, s1,
+                                                                         dp<double>(D.small));
         PB_CUDA(cudaGetLastError());
         Rk = qr_r_only(D, np, col(V, 1), ldv, s, o.qrflag);
         apply_rinv(D, np, col(V, 1), ldv, dense::trinv_upper(Rk), col(Q, s1), ldv);
