@@ -264,6 +264,8 @@ def run_ours(args):
         out["cpu_baseline"] = cpu_baseline(A, b)
     if world == 1 and args.target_rhs > 0:   # one process only: the other ranks would wait on a barrier
         out["target"] = target_summary(args)
+    if world == 1 and not args.no_configs:
+        out["configs_gpu"] = configs_summary()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -286,6 +288,58 @@ def target_summary(args):
             "iterations": {a: v[a]["iterations"] for a in arms},
             "true_relres_max": {a: v[a]["true_relres_max"] for a in arms},
             "training": v["training"]}
+
+
+def configs_summary():
+    """GPU time, iterations and true residual of the other configurations and of the
+    double-double solvers, each one warm-up and two timed solves with the arrays in HBM (CUDA
+    events on the library stream), so that the default line carries them too; their full
+    lines (e2e, CPU baselines, rooflines) come from --workload."""
+    import torch
+    from parcel_b import _lib, api, problems
+    import oracle
+    L = _lib.load()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.ExternalStream(L.parcel_b_get_stream(), device=dev)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    def timed(fn, reps=2):
+        fn()
+        ts, out = [], None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = fn()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return min(ts), out
+
+    out = {}
+    for name in ("poisson2d256", "aniso192", "banded4m"):
+        c = _cfg(name)
+        A, b = c["A"], c["b"]
+        rp, ci, va, bd = t(A.rowptr), t(A.col), t(A.val), t(b)
+        sec, r = timed(lambda: api.solve(A, bd, rowptr=rp, col=ci, val=va, **c["opts"]))
+        out[name] = {"s": sec, "iterations": r["niter"], "iret": r["iret"],
+                     "true_relres": oracle.true_relres(A, b, r["x"].cpu().numpy())}
+        del rp, ci, va, bd
+    A, b, xe = problems.poisson3d_reference(160, 160, 160)
+    rp, ci, va, bd = t(A.rowptr), t(A.col), t(A.val), t(b)
+    sec, r = timed(lambda: api.ddcg(A, bd, rowptr=rp, col=ci, val=va, itrmax=2000, rtolmax=1e-9, ipreflag=2,
+                                    ILU_method=1, precon_thblock=80))
+    x = r["x_hi"].cpu().numpy() + r["x_lo"].cpu().numpy()
+    out["ddcg160"] = {"s": sec, "iterations": r["niter"], "iret": r["iret"],
+                      "max_abs_error": float(np.abs(x - xe).max())}
+    A, b = problem()
+    rp, ci, va, bd = t(A.rowptr), t(A.col), t(A.val), t(b)
+    sec, r = timed(lambda: api.ddgmres(A, bd, rowptr=rp, col=ci, val=va, itrmax=3000, rtolmax=1e-10, ipreflag=2,
+                                       ILU_method=1, precon_thblock=NBLOCKS, GMRES_m=GMRES_M, GMRES_GSflag=1), reps=1)
+    x = r["x_hi"].cpu().numpy() + r["x_lo"].cpu().numpy()
+    out["ddgmres128"] = {"s": sec, "iterations": r["niter"], "iret": r["iret"],
+                         "true_relres": oracle.true_relres(A, b, x)}
+    return out
 
 
 def cpu_baseline(A, b):
@@ -385,14 +439,26 @@ def run_kernels_only(args):
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     rp, ci, va = t(A.rowptr), t(A.col), t(A.val)
     ms_spmv, ms_pre = C.c_double(0), C.c_double(0)
-    p = _lib.new_input(solver=3, ipreflag=2, ILU_method=args.ilu_method, precon_thblock=NBLOCKS,
-                       GMRES_m=GMRES_M)
+    p = _lib.new_input(solver=3, ipreflag=1 if args.natural else 2, ILU_method=args.ilu_method,
+                       precon_thblock=NBLOCKS, GMRES_m=GMRES_M)
     rc = L.parcel_b_bench_kernels(C.byref(p), C.byref(api.crs_struct(A, rp, ci, va)), args.steps,
                                   C.byref(ms_spmv), C.byref(ms_pre))
     assert rc == 0, _lib.last_error()
-    spmv_bytes = 12 * A.nnz + 4 * (A.n + 1) + 16 * A.n
+    diag = 0
+    if args.natural:
+        # point Jacobi keeps the natural layout, where the 7-point stencil's product runs on
+        # its diagonal copy: 7 values + x + y per row (no column indices)
+        spmv_bytes = 8 * 7 * A.n + 16 * A.n
+        r = api.solve(A, t(b), rowptr=rp, col=ci, val=va, solver=3, ipreflag=1, GMRES_m=GMRES_M, itrmax=2,
+                      rtolmax=RTOL)
+        diag = r["stats"]["spmv_diagonals"]
+    else:
+        spmv_bytes = 12 * A.nnz + 4 * (A.n + 1) + 16 * A.n
     print(json.dumps({"spmv_us": ms_spmv.value * 1e3, "precon_us": ms_pre.value * 1e3,
-                      "spmv_gbs": spmv_bytes / (ms_spmv.value * 1e-3) / 1e9, "reps": args.steps}))
+                      "spmv_gbs": spmv_bytes / (ms_spmv.value * 1e-3) / 1e9, "spmv_bytes": spmv_bytes,
+                      "layout": "natural, diagonal copy" if args.natural else "block-Jacobi level order, SELL",
+                      "spmv_diagonals": diag,
+                      "reps": args.steps}))
 
 
 def run_network_only(args):
@@ -1023,11 +1089,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="default line without the GPU summary of the other configurations")
     ap.add_argument("--kernels-only", action="store_true")
     ap.add_argument("--network", action="store_true", help="with --kernels-only: the learned stage's network alone")
     ap.add_argument("--learned", action="store_true",
                     help="with --kernels-only: one learned-stage solve of --itrmax inner iterations")
     ap.add_argument("--itrmax", type=int, default=80)
+    ap.add_argument("--natural", action="store_true",
+                    help="with --kernels-only: point Jacobi, natural layout (the SpMV's diagonal copy)")
     ap.add_argument("--ilu-method", type=int, default=0)
     ap.add_argument("--workload", default="convdiff128",
                     choices=["convdiff128", "vardiff", "ddcg160", "ddgmres128", "poisson2d256", "aniso192",

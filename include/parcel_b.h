@@ -156,7 +156,9 @@ typedef struct parcel_b_stats {
   int ilu_levels_max;       /* longest wavefront (levels) of any block-Jacobi block  */
   int ilu_nblocks;
   int fallback;             /* learned solve: right-hand sides the plain PGMRES finished */
-  int reserved[5];
+  int spmv_diagonals;       /* > 0: the SpMV ran on a diagonal (DIA) copy with this many
+                               diagonals (natural layout: no or point-Jacobi preconditioner) */
+  int reserved[4];
 } parcel_b_stats;
 
 /* ---- lifecycle: PARCEL_Init / PARCEL_Free (src/c_krylov_wrapper.f90:6-23,

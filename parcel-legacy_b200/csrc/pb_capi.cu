@@ -164,6 +164,7 @@ int parcel_b_solve(const parcel_b_input* prm, const parcel_b_crs* A, const doubl
       so = solve_cagmres(o, S, bv.p, xv.p, hist, &t1);
       stt.ilu_levels_max = S.ilu_levels_max;
       stt.ilu_nblocks = S.ilu_nblocks;
+      stt.spmv_diagonals = S.spmv_diagonals;
       stt.true_relres = true_relres(S.Anat, bv.p, xv.p);
     } else if (o.inner == PARCEL_B_INNER_FP32_REFINE) {
       MixedResult mr = solve_mixed(o, *A, dev, bv.p, xv.p, hist, &t1);
@@ -181,6 +182,7 @@ int parcel_b_solve(const parcel_b_input* prm, const parcel_b_crs* A, const doubl
       so = solve_on_system(o, S, bv.p, xv.p, hist, &t1);
       stt.ilu_levels_max = S.ilu_levels_max;
       stt.ilu_nblocks = S.ilu_nblocks;
+      stt.spmv_diagonals = S.spmv_diagonals;
       stt.true_relres = true_relres(S.Anat, bv.p, xv.p);
     }
     const double t2 = now_s();
@@ -402,6 +404,7 @@ int parcel_b_start(parcel_b_handle h, const double* b, double* x, double* reshis
     stt.kernel_launches = so.launches;
     stt.ilu_levels_max = h->h.S->ilu_levels_max;
     stt.ilu_nblocks = h->h.S->ilu_nblocks;
+    stt.spmv_diagonals = h->h.S->spmv_diagonals;
     set_stats(stt);
     return so.iret < 0 ? so.iret : 0;
   });

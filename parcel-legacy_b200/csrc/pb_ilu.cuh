@@ -25,12 +25,22 @@ struct DevMat {
   const int* s_w = nullptr;
   const int* s_col = nullptr;
   const VT* s_val = nullptr;
+  // Diagonal (DIA) copy used by the SpMV when present (natural layout of a matrix whose
+  // entries lie on at most kDiaMaxDiag diagonals): entry of row r on diagonal k (column
+  // r + d_off[k], offsets ascending) at d_val[(r - r % 32) nd + 32 k + r % 32] (32-row
+  // slices, as the ELLPACK copy), zero where the row has no entry.
+  int ndiag = 0;
+  const int* d_off = nullptr;
+  const VT* d_val = nullptr;
 };
 
 template <class VT>
 struct SellBuf {
   DBuf off, w, col, val;
+  DBuf doff, dval;   // diagonal copy (build_dia)
 };
+
+constexpr int kDiaMaxDiag = 16;
 
 // Builds the sliced-ELLPACK copy of the natural CRS matrix A in the row order
 // rowAt (device: permuted position -> natural row, -1 = empty row; null = identity) with
@@ -39,6 +49,11 @@ struct SellBuf {
 template <class VT>
 void build_sell(const DevMat<double>& A, int np, const int* rowAt_d, const int* pos_d, SellBuf<VT>& buf,
                 DevMat<VT>& M);
+// Builds the diagonal copy of the natural CRS matrix A when every entry lies on one of at
+// most kDiaMaxDiag diagonals and the copy holds at most 1.5 nnz values; fills M's DIA fields
+// and returns the number of diagonals (0: not built).
+template <class VT>
+int build_dia(const DevMat<double>& A, SellBuf<VT>& buf, DevMat<VT>& M);
 
 // One chunk = up to kIluChunk rows of one wavefront level of one block.  Wider levels are
 // split into several chunks (their rows are independent; each chunk is one sweep step).

@@ -226,6 +226,7 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
     {
       DevMat<T> M = S.A;
       build_sell<T>(S.Anat, A.n, nullptr, nullptr, S.Asell, M);
+      S.spmv_diagonals = build_dia<T>(S.Anat, S.Asell, M);
       S.A = M;
     }
     if (o.precon == PARCEL_B_PRECON_POINTJACOBI) {

@@ -80,6 +80,7 @@ struct System {
   ExtraStage<T>* extra = nullptr;   // not owned
   int ilu_levels_max = 0;
   int ilu_nblocks = 0;
+  int spmv_diagonals = 0;           // > 0: the SpMV runs on a diagonal copy (natural layout)
 };
 
 template <class T>

@@ -15,6 +15,9 @@
 // device.
 #include "pb_device.cuh"
 #include "pb_epilogue.cuh"
+#include <algorithm>
+#include <vector>
+
 #include "pb_spmv.cuh"
 
 namespace pb {
@@ -161,6 +164,64 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_spmv_sell(int n, int nslices
   if constexpr (ND > 0) reduce_and_finish<ND>(acc, red);
 }
 
+// Position of row r's entry on diagonal k in the diagonal copy: sliced like the ELLPACK copy
+// (32-row slices, the slice's diagonals one after the other, 32 values each), so that a
+// warp reads one contiguous run of 32 nd values per slice; only the column indices are
+// gone.  (Diagonal-major storage, each diagonal a separate array, ran at half the speed.)
+__host__ __device__ __forceinline__ int64_t dia_at(int64_t r, int k, int nd) {
+  return (r & ~int64_t(31)) * nd + (int64_t)k * 32 + (r & 31);
+}
+
+// Diagonal-format SpMV (natural layout): one thread per row, the diagonals in ascending
+// offset order, so a row's products are summed in its CRS column order (an absent entry
+// contributes an exact zero).  Values stream coalesced and without column indices; the
+// x gathers of neighbouring rows are contiguous.
+template <class VT, class XT, int ND, bool RES>
+__global__ void __launch_bounds__(kRedThreads, 4) k_spmv_dia(int n, int nd, const int* __restrict__ doff,
+                                                       const VT* __restrict__ dval, const XT* __restrict__ x,
+                                                       XT* __restrict__ y, const XT* __restrict__ b,
+                                                       const XT* __restrict__ d, int sa0, int sb0, int sa1,
+                                                       int sb1, Red red, const int* gate) {
+  if (gated(gate)) return;
+  __shared__ int offs[kDiaMaxDiag];
+  if (threadIdx.x < nd) offs[threadIdx.x] = doff[threadIdx.x];
+  __syncthreads();
+  double acc[ND > 0 ? ND : 1];
+#pragma unroll
+  for (int k = 0; k < (ND > 0 ? ND : 1); ++k) acc[k] = 0.0;
+  // a warp takes whole 32-row slices, the grid's warps consecutive ones, so that all warps
+  // together sweep the copy front to back (as the sliced-ELLPACK product does)
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int nslices = (n + 31) >> 5;
+  for (int sl = warp; sl < nslices; sl += nwarps) {
+    const int row = sl * 32 + lane;
+    if (row >= n) continue;
+    VT v[kDiaMaxDiag];
+#pragma unroll
+    for (int k = 0; k < kDiaMaxDiag; ++k)
+      if (k < nd) v[k] = __ldcs(dval + dia_at(row, k, nd));
+    XT sum = XT(0);
+#pragma unroll
+    for (int k = 0; k < kDiaMaxDiag; ++k) {
+      if (k < nd) {
+        int c = row + offs[k];
+        c = c < 0 ? 0 : (c >= n ? n - 1 : c);     // out of the matrix: the stored value is zero
+        sum += (XT)v[k] * __ldg(x + c);
+      }
+    }
+    XT yv = RES ? b[row] - sum : sum;
+    y[row] = yv;
+    if constexpr (ND > 0) {
+      XT src[3] = {yv, x[row], d ? d[row] : XT(0)};
+      acc[0] += (double)(src[sa0] * src[sb0]);
+      if (ND > 1) acc[ND > 1 ? 1 : 0] += (double)(src[sa1] * src[sb1]);
+    }
+  }
+  if constexpr (ND > 0) reduce_and_finish<ND>(acc, red);
+}
+
 template <class VT, class XT, int ND, bool RES>
 static void launch_spmv(const DevMat<VT>& A, const XT* x, XT* y, const XT* b, const XT* d,
                         const int* sa, const int* sb, const Red& red, const int* gate,
@@ -168,6 +229,12 @@ static void launch_spmv(const DevMat<VT>& A, const XT* x, XT* y, const XT* b, co
   const int lpr = spmv_lanes(A.n, A.nnz);
   const int grid = red_blocks();
   int a0 = sa ? sa[0] : 0, b0 = sb ? sb[0] : 0, a1 = sa ? sa[1] : 0, b1 = sb ? sb[1] : 0;
+  if (A.d_val) {
+    k_spmv_dia<VT, XT, ND, RES><<<grid, kRedThreads, 0, st>>>(A.n, A.ndiag, A.d_off, A.d_val, x, y, b, d, a0, b0,
+                                                             a1, b1, red, gate);
+    PB_CUDA(cudaGetLastError());
+    return;
+  }
   if (A.s_val) {
     k_spmv_sell<VT, XT, ND, RES><<<grid, kRedThreads, 0, st>>>(A.n, A.nslices, A.s_off, A.s_w, A.s_col,
                                                               A.s_val, x, y, b, d, a0, b0, a1, b1, red,
@@ -313,6 +380,101 @@ void build_sell(const DevMat<double>& A, int np, const int* rowAt_d, const int* 
   M.s_val = dp<VT>(buf.val);
   M.n = np;
 }
+
+// Any entry off the candidate diagonals sets *miss.
+__global__ void k_dia_check(int n, const int* __restrict__ rp, const int* __restrict__ ci, int rbase, int cbase,
+                            int nd, const int* __restrict__ doff, int* __restrict__ miss) {
+  __shared__ int offs[kDiaMaxDiag];
+  if (threadIdx.x < nd) offs[threadIdx.x] = doff[threadIdx.x];
+  __syncthreads();
+  bool bad = false;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    for (int e = rp[r] - rbase; e < rp[r + 1] - rbase; ++e) {
+      const int o = ci[e] - cbase - r;
+      bool hit = false;
+      for (int k = 0; k < nd; ++k) hit |= offs[k] == o;
+      bad |= !hit;
+    }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(miss, 1);
+}
+
+template <class VT>
+__global__ void k_dia_fill(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const double* __restrict__ va, int rbase, int cbase, int nd, const int* __restrict__ doff,
+                           VT* __restrict__ dval) {
+  __shared__ int offs[kDiaMaxDiag];
+  if (threadIdx.x < nd) offs[threadIdx.x] = doff[threadIdx.x];
+  __syncthreads();
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    for (int e = rp[r] - rbase; e < rp[r + 1] - rbase; ++e) {
+      const int o = ci[e] - cbase - r;
+      for (int k = 0; k < nd; ++k)
+        if (offs[k] == o) dval[dia_at(r, k, nd)] = (VT)va[e];
+    }
+}
+
+// Row t of 64 sample rows scattered over the matrix (a multiplicative hash of t, so that a
+// stencil's boundary rows, which lie on regular strides, do not make up the sample):
+// out[t][0] = its entry count (more than kDiaMaxDiag: only the count), out[t][1..] = its
+// column offsets.
+__global__ void k_dia_sample(int n, const int* __restrict__ rp, const int* __restrict__ ci, int rbase, int cbase,
+                             int* __restrict__ out) {
+  const int t = threadIdx.x;
+  const int r = (int)(((uint64_t)(t + 1) * 2654435761ull) % (uint64_t)n);
+  int* o = out + t * (kDiaMaxDiag + 1);
+  const int b = rp[r] - rbase, e = rp[r + 1] - rbase;
+  o[0] = e - b;
+  if (e - b <= kDiaMaxDiag)
+    for (int k = b; k < e; ++k) o[1 + k - b] = ci[k] - cbase - r;
+}
+
+template <class VT>
+int build_dia(const DevMat<double>& A, SellBuf<VT>& buf, DevMat<VT>& M) {
+  cudaStream_t st = stream();
+  const int n = A.n;
+  if (n < 2) return 0;
+  // candidate diagonals: the offsets found in 64 rows scattered over the matrix (interior
+  // rows of a stencil carry all of them, boundary rows a subset), gathered in one launch
+  constexpr int kSamples = 64;
+  DBuf sm(sizeof(int) * kSamples * (kDiaMaxDiag + 1));
+  k_dia_sample<<<1, kSamples, 0, st>>>(n, A.rowptr, A.col, A.rbase, A.cbase, dp<int>(sm));
+  PB_CUDA(cudaGetLastError());
+  std::vector<int> hs(kSamples * (kDiaMaxDiag + 1));
+  d2h(hs.data(), sm.p, sizeof(int) * hs.size());
+  std::vector<int> offs;
+  for (int t = 0; t < kSamples; ++t) {
+    const int len = hs[t * (kDiaMaxDiag + 1)];
+    if (len > kDiaMaxDiag) return 0;
+    for (int k = 0; k < len; ++k) offs.push_back(hs[t * (kDiaMaxDiag + 1) + 1 + k]);
+  }
+  std::sort(offs.begin(), offs.end());
+  offs.erase(std::unique(offs.begin(), offs.end()), offs.end());
+  if ((int)offs.size() > kDiaMaxDiag) return 0;
+  if (offs.empty()) return 0;
+  const int nd = (int)offs.size();
+  if ((double)nd * n > 1.5 * (double)std::max<int64_t>(A.nnz, 1)) return 0;
+  buf.doff.alloc(sizeof(int) * kDiaMaxDiag);
+  h2d(buf.doff.p, offs.data(), sizeof(int) * nd);
+  DBuf miss(sizeof(int));
+  PB_CUDA(cudaMemsetAsync(miss.p, 0, sizeof(int), st));
+  const int grid = std::max(1, std::min((n + 255) / 256, 8 * num_sms()));
+  k_dia_check<<<grid, 256, 0, st>>>(n, A.rowptr, A.col, A.rbase, A.cbase, nd, dp<int>(buf.doff), dp<int>(miss));
+  PB_CUDA(cudaGetLastError());
+  int m = 0;
+  d2h(&m, miss.p, sizeof(int));
+  if (m) return 0;
+  buf.dval.alloc(sizeof(VT) * (size_t)nd * (((size_t)n + 31) & ~size_t(31)));   // zero-filled
+  k_dia_fill<VT><<<grid, 256, 0, st>>>(n, A.rowptr, A.col, A.val, A.rbase, A.cbase, nd, dp<int>(buf.doff),
+                                       dp<VT>(buf.dval));
+  PB_CUDA(cudaGetLastError());
+  M.ndiag = nd;
+  M.d_off = dp<int>(buf.doff);
+  M.d_val = dp<VT>(buf.dval);
+  return nd;
+}
+
+template int build_dia<double>(const DevMat<double>&, SellBuf<double>&, DevMat<double>&);
+template int build_dia<float>(const DevMat<double>&, SellBuf<float>&, DevMat<float>&);
 
 template void build_sell<double>(const DevMat<double>&, int, const int*, const int*, SellBuf<double>&,
                                  DevMat<double>&);

@@ -56,7 +56,8 @@ class Stats(C.Structure):
                 ("true_relres", C.c_double), ("true_relres_dd", C.c_double),
                 ("niter", C.c_int), ("iret", C.c_int), ("refine_steps", C.c_int),
                 ("kernel_launches", C.c_int), ("ilu_levels_max", C.c_int),
-                ("ilu_nblocks", C.c_int), ("fallback", C.c_int), ("reserved", C.c_int * 5)]
+                ("ilu_nblocks", C.c_int), ("fallback", C.c_int), ("spmv_diagonals", C.c_int),
+                ("reserved", C.c_int * 4)]
 
 
 P = C.c_void_p
