@@ -1081,9 +1081,12 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   D.ring = ring_bytes <= 64 * 1024;
   int64_t ring_alloc = D.ring ? ((ring_bytes + 127) & ~int64_t(127)) : 0;
   // consumer threads and rows per thread of the grouped sweep
+  // (one row per thread: a second row slot costs every level its predicated instructions,
+  // although few levels are wider than 256 rows)
   if (maxw <= 128) { D.nc = 128; D.rows = 1; }
   else if (maxw <= 256) { D.nc = 256; D.rows = 1; }
-  else { D.nc = 256; D.rows = 2; }   // chunks have at most kIluChunk = 512 rows
+  else if (maxw <= 384) { D.nc = 384; D.rows = 1; }
+  else { D.nc = 512; D.rows = 1; }   // chunks have at most kIluChunk = 512 rows
   D.grp = D.ring && D.rows > 0 && kuni <= 8;
   if (D.grp) {
     // Groups of consecutive chunks of one block, each at most kGrpMax chunks and about a
@@ -1289,7 +1292,8 @@ void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, 
 #define GRP(KM_)                                                                                   \
   case KM_:                                                                                        \
     if (D.nc == 128) { GRP_R(KM_, 1, 128) }                                                        \
-    else if (D.rows == 1) { GRP_R(KM_, 1, 256) } else { GRP_R(KM_, 2, 256) }                       \
+    else if (D.nc == 256) { GRP_R(KM_, 1, 256) }                                                   \
+    else if (D.nc == 384) { GRP_R(KM_, 1, 384) } else { GRP_R(KM_, 1, 512) }                       \
     break;
     switch (D.K) {
       GRP(1) GRP(2) GRP(3) GRP(4) GRP(6) GRP(8)
