@@ -520,7 +520,7 @@ def run_learned_only(args):
 VD_METRIC = "time-to-1e-10 true rel. residual (s), learned + mixed-precision FGMRES vs plain FP64 PGMRES/BJ-ILU"
 
 
-def vardiff_compare(N, c, m, nr, plain_rhs, train_rhs, train_steps, k=2, reps=3):
+def vardiff_compare(N, c, m, nr, plain_rhs, train_rhs, train_steps, k=2, reps=5):
     """The learned-preconditioner workload: 3D 7-point variable-coefficient diffusion on an
     N^3 grid (N = 256 by default), coefficient exp(g) with g a Gaussian random field
     (correlation length 8 cells, variance 2, seed 5), harmonic-mean faces; right-hand

@@ -663,31 +663,26 @@ DD dd_sqrt(DD a) {
 }
 
 // dd dot in a fixed order, independent of the thread count (the reference's blocked
-// accumulators, ddvec.f90:111-240, follow its OpenMP split instead): nc = min(32768, n)
-// contiguous chunks, each summed in index order; the chunk sums in ng = min(256, nc)
-// contiguous groups, each summed in chunk order; the group sums in order.  Each sum
-// starts from 0 and adds with dd_add(sum, term).
-constexpr long DD_NCHUNK = 32768, DD_NGROUP = 256;
+// accumulators, ddvec.f90:111-240, follow its OpenMP split instead): stream t (0 <= t <
+// 2^17) sums the products of the elements i = t, t + 2^17, ... in increasing i, starting
+// from 0 and adding with dd_add(sum, term); the 2^17 stream sums are combined by a complete
+// binary tree, level by level, neighbours in pairs (s'[k] = dd_add(s[2k], s[2k+1])).
+constexpr long DD_NSTREAM = 1L << 17;
 DD dd_dot(long n, const double* xh, const double* xl, const double* yh, const double* yl) {
-  const long nc = std::min<long>(DD_NCHUNK, std::max<long>(1, n));
-  const long ng = std::min<long>(DD_NGROUP, nc);
-  std::vector<DD> part(nc), grp(ng);
+  std::vector<DD> s(DD_NSTREAM);
 #pragma omp parallel for schedule(static)
-  for (long c = 0; c < nc; ++c) {
-    const long lo = n * c / nc, hi = n * (c + 1) / nc;
-    DD s{0.0, 0.0};
-    for (long i = lo; i < hi; ++i) s = dd_add(s, dd_mul(DD{xh[i], xl[i]}, DD{yh[i], yl[i]}));
-    part[c] = s;
+  for (long t = 0; t < DD_NSTREAM; ++t) {
+    DD a{0.0, 0.0};
+    for (long i = t; i < n; i += DD_NSTREAM) a = dd_add(a, dd_mul(DD{xh[i], xl[i]}, DD{yh[i], yl[i]}));
+    s[t] = a;
   }
-  for (long g = 0; g < ng; ++g) {
-    const long lo = nc * g / ng, hi = nc * (g + 1) / ng;
-    DD s{0.0, 0.0};
-    for (long c = lo; c < hi; ++c) s = dd_add(s, part[c]);
-    grp[g] = s;
+  std::vector<DD> u(DD_NSTREAM / 2);
+  for (long h = DD_NSTREAM / 2; h > 0; h /= 2) {
+#pragma omp parallel for schedule(static) if (h >= 4096)
+    for (long k = 0; k < h; ++k) u[k] = dd_add(s[2 * k], s[2 * k + 1]);
+    std::copy(u.begin(), u.begin() + h, s.begin());
   }
-  DD s{0.0, 0.0};
-  for (long g = 0; g < ng; ++g) s = dd_add(s, grp[g]);
-  return s;
+  return s[0];
 }
 
 // ddMatVec_crs (ddmatrix.f90:1785-2355), single process: per row, c = a_ij x_j and

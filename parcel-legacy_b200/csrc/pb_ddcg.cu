@@ -26,8 +26,9 @@ namespace pb {
 
 namespace {
 
-constexpr int kDdChunks = 32768;   // dot-product split (the oracle uses the same order)
-constexpr int kDdGroups = 256;
+constexpr int kDdStreams = 1 << 17;                 // dot-product streams (the oracle uses the same order)
+constexpr int kDdDotThreads = 256;
+constexpr int kDdDotCtas = kDdStreams / kDdDotThreads;   // 512
 constexpr int kDdThreads = 256;
 
 #define GRID_LOOP(i, n) \
@@ -88,47 +89,63 @@ __global__ void k_dd_cg_axpy2(int n, const DdScal* sc, double* __restrict__ xh, 
   }
 }
 
-// Dot product in a fixed order: nc = min(32768, n) contiguous chunks in index order, their
-// sums in ng = min(256, nc) contiguous groups in chunk order, the group sums in order.  One
-// launch: thread c of the grid sums chunk c; the last CTA to finish (an atomic ticket, no
-// waiting) sums the groups, one thread per group, and thread 0 adds the group sums.  The
-// ticket counter is reset by that CTA for the next dot on the stream.
-__global__ void __launch_bounds__(256) k_dd_dot(int64_t n, int nch, int ngr, const double* __restrict__ xh,
-                                                const double* __restrict__ xl, const double* __restrict__ yh,
-                                                const double* __restrict__ yl, dd* part, unsigned* ticket,
-                                                dd* out) {
-  __shared__ dd grp[kDdGroups];
-  __shared__ bool last;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < nch) {
-    const int64_t lo = n * c / nch, hi = n * (c + 1) / nch;
-    dd s{0.0, 0.0};
-#pragma unroll 4
-    for (int64_t i = lo; i < hi; ++i) s = dd_add(s, dd_mul(dd{xh[i], xl[i]}, dd{yh[i], yl[i]}));
-    part[c] = s;
+// Dot product in a fixed order: stream t (0 <= t < 2^17) sums the products of the elements
+// i = t, t + 2^17, ... in increasing i, from zero; the 2^17 stream sums are combined by a
+// complete binary tree (level by level, neighbours in pairs: s'[k] = s[2k] + s[2k+1]).
+// One launch: thread t of the grid owns stream t, so every load is coalesced; each CTA
+// folds its 256 streams (an aligned subtree) in shared memory and stores its sum; the last
+// CTA to finish (an atomic ticket, no waiting) folds the 512 CTA sums and stores the result.
+// The ticket counter is reset by that CTA for the next dot on the stream.
+__device__ __forceinline__ void dd_tree(dd* v, int count) {
+  // v[0..count) -> v[0], count a power of two, all threads of the CTA taking part
+  for (int h = count >> 1; h > 0; h >>= 1) {
+    dd r{0.0, 0.0};
+    for (int k = threadIdx.x; k < h; k += blockDim.x) r = dd_add(v[2 * k], v[2 * k + 1]);
+    __syncthreads();
+    for (int k = threadIdx.x; k < h; k += blockDim.x) v[k] = r;   // h <= blockDim.x after the first level
+    __syncthreads();
   }
-  __threadfence();
+}
+
+__global__ void __launch_bounds__(kDdDotThreads) k_dd_dot(int64_t n, const double* __restrict__ xh,
+                                                        const double* __restrict__ xl, const double* __restrict__ yh,
+                                                        const double* __restrict__ yl, dd* part, unsigned* ticket,
+                                                        dd* out) {
+  __shared__ dd tr[2 * kDdDotThreads];
+  __shared__ bool last;
+  const int64_t t = (int64_t)blockIdx.x * kDdDotThreads + threadIdx.x;
+  dd s{0.0, 0.0};
+  int64_t i = t;
+  for (; i + 3 * (int64_t)kDdStreams < n; i += 4 * (int64_t)kDdStreams) {
+    double ah[4], al[4], bh[4], bl[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int64_t q = i + u * (int64_t)kDdStreams;
+      ah[u] = xh[q]; al[u] = xl[q]; bh[u] = yh[q]; bl[u] = yl[q];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) s = dd_add(s, dd_mul(dd{ah[u], al[u]}, dd{bh[u], bl[u]}));
+  }
+  for (; i < n; i += kDdStreams) s = dd_add(s, dd_mul(dd{xh[i], xl[i]}, dd{yh[i], yl[i]}));
+  tr[threadIdx.x] = s;
   __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  dd_tree(tr, kDdDotThreads);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = tr[0];
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
   __syncthreads();
   if (!last) return;
   __threadfence();
-  const int g = threadIdx.x;
-  if (g < ngr) {
-    const int lo = (int)((int64_t)nch * g / ngr), hi = (int)((int64_t)nch * (g + 1) / ngr);
-    dd s{0.0, 0.0};
-#pragma unroll 8
-    for (int k = lo; k < hi; ++k) {
-      const double2 v = __ldcg(reinterpret_cast<const double2*>(part + k));
-      s = dd_add(s, dd{v.x, v.y});
-    }
-    grp[g] = s;
+  for (int k = threadIdx.x; k < kDdDotCtas; k += kDdDotThreads) {
+    const double2 v = __ldcg(reinterpret_cast<const double2*>(part + k));
+    tr[k] = dd{v.x, v.y};
   }
   __syncthreads();
+  dd_tree(tr, kDdDotCtas);
   if (threadIdx.x == 0) {
-    dd s{0.0, 0.0};
-    for (int k = 0; k < ngr; ++k) s = dd_add(s, grp[k]);
-    *out = s;
+    *out = tr[0];
     *ticket = 0u;
   }
 }
@@ -762,13 +779,11 @@ struct DdSystem {
   const double* al = nullptr;   // null: A's low parts are zero
 };
 
-// part: kDdChunks chunk sums followed by the ticket counter (zero between dots).
+// part: kDdDotCtas CTA sums followed by the ticket counter (zero between dots).
 void dd_dot(const DdSystem& S, const double* xh, const double* xl, const double* yh, const double* yl, dd* part,
             dd* out, cudaStream_t st) {
-  const int nch = (int)std::min<int64_t>(kDdChunks, std::max(1, S.n));
-  const int ngr = std::min(kDdGroups, nch);
-  k_dd_dot<<<(nch + 255) / 256, 256, 0, st>>>(S.n, nch, ngr, xh, xl, yh, yl, part,
-                                              reinterpret_cast<unsigned*>(part + kDdChunks), out);
+  k_dd_dot<<<kDdDotCtas, kDdDotThreads, 0, st>>>(S.n, xh, xl, yh, yl, part,
+                                                reinterpret_cast<unsigned*>(part + kDdDotCtas), out);
 }
 
 void dd_setup_precon(const Options& o, const parcel_b_crs& A, const DdSystem& S, int prec_M, DdPrecon& P) {
@@ -1156,7 +1171,7 @@ int dd_krylov(int solver, const parcel_b_input* prm, const parcel_b_crs* A, cons
     };
     load(x, x_hi, x_lo, precision_x == 2);
     load(b, b_hi, b_lo, precision_b == 2);
-    DBuf part(sizeof(dd) * (kDdChunks + kDdGroups)), cst(sizeof(dd) * 3);
+    DBuf part(sizeof(dd) * (kDdDotCtas + 1)), cst(sizeof(dd) * 3);
     dd* dcst = dp<dd>(cst);
     {
       const dd h[3] = {dd{1.0, 0.0}, dd{-1.0, 0.0}, dd{0.0, 0.0}};
