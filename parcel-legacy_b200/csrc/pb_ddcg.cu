@@ -530,12 +530,14 @@ __global__ void k_dd_dilu_diag(const IluChunk* __restrict__ ch, const int* __res
 // gathers of s_c, the dd chain and the stores remain.
 constexpr int kPre = 3;       // couplings per row held in the records
 constexpr int kRowsPer = 2;   // rows per thread staged ahead (levels of up to 512 rows)
+constexpr int kDdRingBytes = 160 * 1024;   // largest shared-memory ring of the sweep
 
 struct DdRecords {
   int np = 0;
   const int* k;             // natural row at position q, -1 = padding
+  const int* rs;            // ring slot of the row at position q (ring mode)
   const int2* nj[2];        // [fwd, bwd]: (coupling count, first position)
-  const int* col[2];        // [dir][t * np + q]
+  const int* col[2];        // [dir][t * np + q]: natural column, or its ring slot (ring mode)
   const double* ah[2];
   const double* al[2];
   const double* dh;         // D^-1 at q (low part 0 under precision 1)
@@ -545,11 +547,12 @@ struct DdRecords {
 __global__ void k_dd_records(int np, const int* __restrict__ rowAt, const int4* __restrict__ rng,
                              const int* __restrict__ ci, const double* __restrict__ ah, const double* __restrict__ al,
                              int cbase, const double* __restrict__ dih, const double* __restrict__ dil, int prec,
-                             int* rk, int2* nj0, int2* nj1, int* c0, int* c1, double* a0h, double* a0l, double* a1h,
-                             double* a1l, double* rdh, double* rdl) {
+                             const int* __restrict__ rslot, int* rk, int* rs, int2* nj0, int2* nj1, int* c0, int* c1,
+                             double* a0h, double* a0l, double* a1h, double* a1l, double* rdh, double* rdl) {
   GRID_LOOP(q, np) {
     const int k = rowAt[q];
     rk[q] = k;
+    rs[q] = (rslot && k >= 0) ? rslot[k] : 0;
     if (k < 0) {
       nj0[q] = make_int2(0, 0);
       nj1[q] = make_int2(0, 0);
@@ -565,13 +568,13 @@ __global__ void k_dd_records(int np, const int* __restrict__ rowAt, const int4* 
       const int64_t o = (int64_t)t * np + q;
       if (t < nf) {
         const int j = r.x + t;
-        c0[o] = ci[j] - cbase;
+        c0[o] = rslot ? rslot[ci[j] - cbase] : ci[j] - cbase;
         a0h[o] = ah[j];
         a0l[o] = (prec == 2 && al) ? al[j] : 0.0;
       }
       if (t < nb) {
         const int j = r.z - t;
-        c1[o] = ci[j] - cbase;
+        c1[o] = rslot ? rslot[ci[j] - cbase] : ci[j] - cbase;
         a1h[o] = ah[j];
         a1l[o] = (prec == 2 && al) ? al[j] : 0.0;
       }
@@ -592,7 +595,7 @@ __global__ void k_dd_gather(int np, const int* __restrict__ rk, const double* __
 }
 
 struct DdStage {
-  int k[kRowsPer], n[kRowsPer], j0[kRowsPer], q[kRowsPer];
+  int k[kRowsPer], n[kRowsPer], j0[kRowsPer], q[kRowsPer], rs[kRowsPer];
   int col[kRowsPer][kPre];
   dd a[kRowsPer][kPre];
   dd x[kRowsPer], di[kRowsPer];
@@ -609,6 +612,7 @@ __device__ __forceinline__ void dd_stage(DdStage& S, const IluChunk& C, const Dd
       const int q = C.start + p;
       S.q[u] = q;
       S.k[u] = R.k[q];
+      S.rs[u] = R.rs[q];
       const int2 nj = R.nj[DIR][q];
       S.n[u] = nj.x;
       S.j0[u] = nj.y;
@@ -625,16 +629,18 @@ __device__ __forceinline__ void dd_stage(DdStage& S, const IluChunk& C, const Dd
   }
 }
 
-template <int DIR>
+// ringh / ringl: the shared-memory ring of the last W levels' results (RING), indexed by the
+// records' slots; otherwise the staged couplings read the natural-order output sh / sl.
+template <int DIR, bool RING>
 __device__ __forceinline__ dd dd_row(int k, int n, int j0, const int* col, const dd* a, dd x, dd di,
                                      const int* __restrict__ ci, const double* __restrict__ ah,
                                      const double* __restrict__ al, int cbase, int prec, const double* sh,
-                                     const double* sl) {
+                                     const double* sl, const double* ringh, const double* ringl) {
   dd z = DIR == 0 ? x : dd{0.0, 0.0};
 #pragma unroll
   for (int t = 0; t < kPre; ++t)
     if (t < n) {
-      const dd v = dd_mul(dd{sh[col[t]], sl[col[t]]}, a[t]);
+      const dd v = RING ? dd_mul(dd{ringh[col[t]], ringl[col[t]]}, a[t]) : dd_mul(dd{sh[col[t]], sl[col[t]]}, a[t]);
       z = DIR == 0 ? dd_sub(z, v) : dd_add(z, v);
     }
   for (int t = kPre; t < n; ++t) {   // couplings past the records, straight from the CRS
@@ -648,16 +654,21 @@ __device__ __forceinline__ dd dd_row(int k, int n, int j0, const int* col, const
 }
 
 // The rows of one level: the staged ones, then any past kRowsPer per thread.
-template <int DIR>
+template <int DIR, bool RING>
 __device__ __forceinline__ void dd_level(const DdStage& S, const IluChunk& C, const DdRecords& R, const double* xh,
                                          const double* xl, const int* __restrict__ ci, const double* __restrict__ ah,
                                          const double* __restrict__ al, int cbase, int prec, double* sh, double* sl,
-                                         double* fqh, double* fql) {
+                                         double* fqh, double* fql, double* ringh, double* ringl) {
 #pragma unroll
   for (int u = 0; u < kRowsPer; ++u) {
     const int k = S.k[u];
     if (k < 0) continue;
-    const dd s = dd_row<DIR>(k, S.n[u], S.j0[u], S.col[u], S.a[u], S.x[u], S.di[u], ci, ah, al, cbase, prec, sh, sl);
+    const dd s = dd_row<DIR, RING>(k, S.n[u], S.j0[u], S.col[u], S.a[u], S.x[u], S.di[u], ci, ah, al, cbase, prec, sh,
+                                   sl, ringh, ringl);
+    if (RING) {
+      ringh[S.rs[u]] = s.hi;
+      ringl[S.rs[u]] = s.lo;
+    }
     sh[k] = s.hi;
     sl[k] = s.lo;
     if (DIR == 0) {
@@ -678,8 +689,12 @@ __device__ __forceinline__ void dd_level(const DdStage& S, const IluChunk& C, co
         col[t] = R.col[DIR][o];
         a[t] = dd{R.ah[DIR][o], R.al[DIR][o]};
       }
-    const dd s = dd_row<DIR>(k, nj.x, nj.y, col, a, dd{xh[q], xl[q]}, dd{R.dh[q], R.dl[q]}, ci, ah, al, cbase, prec,
-                             sh, sl);
+    const dd s = dd_row<DIR, RING>(k, nj.x, nj.y, col, a, dd{xh[q], xl[q]}, dd{R.dh[q], R.dl[q]}, ci, ah, al, cbase,
+                                   prec, sh, sl, ringh, ringl);
+    if (RING) {
+      ringh[R.rs[q]] = s.hi;
+      ringl[R.rs[q]] = s.lo;
+    }
     sh[k] = s.hi;
     sl[k] = s.lo;
     if (DIR == 0) {
@@ -689,11 +704,18 @@ __device__ __forceinline__ void dd_level(const DdStage& S, const IluChunk& C, co
   }
 }
 
+// RING: the results of the last W levels also go to a shared-memory ring (ring_rows slots),
+// from which the staged couplings are read: a level's dependency gathers are then
+// shared-memory loads instead of L2 round trips.
+template <bool RING>
 __global__ void __launch_bounds__(256, 1)
     k_dd_dilu_sweep(const IluChunk* __restrict__ ch, const int* __restrict__ blk_chunk, DdRecords R,
                     const int* __restrict__ ci, const double* __restrict__ ah, const double* __restrict__ al, int cbase,
                     int prec, const double* __restrict__ rqh, const double* __restrict__ rql, double* fqh, double* fql,
-                    double* sh, double* sl) {
+                    double* sh, double* sl, int ring_rows) {
+  extern __shared__ double ringbuf[];
+  double* ringh = ringbuf;
+  double* ringl = ringbuf + ring_rows;
   const int b = blockIdx.x;
   const int c0 = blk_chunk[b], c1 = blk_chunk[b + 1];
   if (c1 <= c0) return;
@@ -703,7 +725,7 @@ __global__ void __launch_bounds__(256, 1)
   for (int c = c0; c < c1; ++c) {
     const IluChunk C = ch[c];
     if (c + 1 < c1) dd_stage<0>(B, ch[c + 1], R, rqh, rql);
-    dd_level<0>(A, C, R, rqh, rql, ci, ah, al, cbase, prec, sh, sl, fqh, fql);
+    dd_level<0, RING>(A, C, R, rqh, rql, ci, ah, al, cbase, prec, sh, sl, fqh, fql, ringh, ringl);
     __syncthreads();
     A = B;
   }
@@ -712,7 +734,7 @@ __global__ void __launch_bounds__(256, 1)
   for (int c = c1 - 1; c >= c0; --c) {
     const IluChunk C = ch[c];
     if (c - 1 >= c0) dd_stage<1>(B, ch[c - 1], R, fqh, fql);
-    dd_level<1>(A, C, R, fqh, fql, ci, ah, al, cbase, prec, sh, sl, nullptr, nullptr);
+    dd_level<1, RING>(A, C, R, fqh, fql, ci, ah, al, cbase, prec, sh, sl, nullptr, nullptr, ringh, ringl);
     __syncthreads();
     A = B;
   }
@@ -738,12 +760,14 @@ struct DdPrecon {
   DBuf dih, dil;                        // D^-1 (point Jacobi, D-ILU)
   DBuf chunks, blk_chunk, rowAt, rng;   // D-ILU level plan and row ranges
   int nb = 0, np = 0;
-  DBuf rk, nj0, nj1, c0, c1, a0h, a0l, a1h, a1l, rdh, rdl;   // level-ordered row records
+  DBuf rk, rs, nj0, nj1, c0, c1, a0h, a0l, a1h, a1l, rdh, rdl;   // level-ordered row records
+  int ring_rows = 0;                                               // > 0: the sweep's shared-memory ring
   DBuf rqh, rql, fqh, fql;                                     // r and the forward result in level order
   DdRecords rec() const {
     DdRecords R;
     R.np = np;
     R.k = dp<int>(rk);
+    R.rs = dp<int>(rs);
     R.nj[0] = dp<int2>(nj0);
     R.nj[1] = dp<int2>(nj1);
     R.col[0] = dp<int>(c0);
@@ -844,8 +868,25 @@ void dd_setup_precon(const Options& o, const parcel_b_crs& A, const DdSystem& S,
   PB_CUDA(cudaGetLastError());
   const int np = plan.np;
   P.np = np;
+  // ring: slot of natural row c = (level % W) * LW + (position - the level's first position),
+  // LW the widest level; used when its hi and lo parts fit kDdRingBytes of shared memory
+  const int LW = plan.maxWp;   // the widest level (rows, rounded up to 4)
+  const int64_t ring_rows = (int64_t)plan.W * LW;
+  DBuf drs;
+  if (ring_rows > 0 && 2 * ring_rows * (int64_t)sizeof(double) <= kDdRingBytes) {
+    std::vector<int> rslot(A.n);
+    for (int b = 0; b < plan.nb; ++b)
+      for (int c = plan.blk_lo[b]; c < plan.blk_hi[b]; ++c) {
+        const int l = lev[c];
+        rslot[c] = (l % plan.W) * LW + (pos[c] - plan.lvl_start[plan.blk_lvl[b] + l]);
+      }
+    drs.alloc(sizeof(int) * A.n);
+    h2d(drs.p, rslot.data(), sizeof(int) * A.n);
+    P.ring_rows = (int)ring_rows;
+  }
   const size_t nq = (size_t)np, nt = (size_t)kPre * np;
   P.rk.alloc(sizeof(int) * nq);
+  P.rs.alloc(sizeof(int) * nq);
   P.nj0.alloc(sizeof(int2) * nq);
   P.nj1.alloc(sizeof(int2) * nq);
   P.c0.alloc(sizeof(int) * nt);
@@ -853,8 +894,9 @@ void dd_setup_precon(const Options& o, const parcel_b_crs& A, const DdSystem& S,
   for (DBuf* d : {&P.a0h, &P.a0l, &P.a1h, &P.a1l}) d->alloc(sizeof(double) * nt);
   for (DBuf* d : {&P.rdh, &P.rdl, &P.rqh, &P.rql, &P.fqh, &P.fql}) d->alloc(sizeof(double) * nq);
   k_dd_records<<<grid_for(np), kDdThreads, 0, st>>>(np, dp<int>(P.rowAt), dp<int4>(P.rng), S.ci, S.ah, S.al, S.cbase,
-                                                     dp<double>(P.dih), dp<double>(P.dil), prec_M, dp<int>(P.rk),
-                                                     dp<int2>(P.nj0), dp<int2>(P.nj1), dp<int>(P.c0), dp<int>(P.c1),
+                                                     dp<double>(P.dih), dp<double>(P.dil), prec_M,
+                                                     P.ring_rows ? dp<int>(drs) : nullptr, dp<int>(P.rk),
+                                                     dp<int>(P.rs), dp<int2>(P.nj0), dp<int2>(P.nj1), dp<int>(P.c0), dp<int>(P.c1),
                                                      dp<double>(P.a0h), dp<double>(P.a0l), dp<double>(P.a1h),
                                                      dp<double>(P.a1l), dp<double>(P.rdh), dp<double>(P.rdl));
   PB_CUDA(cudaGetLastError());
@@ -874,9 +916,22 @@ void dd_apply_precon(const DdSystem& S, const DdPrecon& P, const double* rh, con
     default:
       k_dd_gather<<<grid_for(P.np), kDdThreads, 0, st>>>(P.np, dp<int>(P.rk), rh, rl, dp<double>(P.rqh),
                                                           dp<double>(P.rql));
-      k_dd_dilu_sweep<<<P.nb, kDdThreads, 0, st>>>(dp<IluChunk>(P.chunks), dp<int>(P.blk_chunk), P.rec(), S.ci, S.ah,
-                                                   S.al, S.cbase, P.prec, dp<double>(P.rqh), dp<double>(P.rql),
-                                                   dp<double>(P.fqh), dp<double>(P.fql), sh, sl);
+      if (P.ring_rows) {
+        static bool attr = false;
+        if (!attr) {
+          PB_CUDA(cudaFuncSetAttribute(k_dd_dilu_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kDdRingBytes));
+          attr = true;
+        }
+        k_dd_dilu_sweep<true><<<P.nb, kDdThreads, 2 * sizeof(double) * P.ring_rows, st>>>(
+            dp<IluChunk>(P.chunks), dp<int>(P.blk_chunk), P.rec(), S.ci, S.ah, S.al, S.cbase, P.prec,
+            dp<double>(P.rqh), dp<double>(P.rql), dp<double>(P.fqh), dp<double>(P.fql), sh, sl, P.ring_rows);
+      } else {
+        k_dd_dilu_sweep<false><<<P.nb, kDdThreads, 0, st>>>(dp<IluChunk>(P.chunks), dp<int>(P.blk_chunk), P.rec(),
+                                                            S.ci, S.ah, S.al, S.cbase, P.prec, dp<double>(P.rqh),
+                                                            dp<double>(P.rql), dp<double>(P.fqh), dp<double>(P.fql),
+                                                            sh, sl, 0);
+      }
       break;
   }
 }
