@@ -142,6 +142,29 @@ typedef struct parcel_b_dia {
   const int32_t* offset;
 } parcel_b_dia;
 
+/* DDM stencil format (src/src_DDM; argument list of parcel_dcg_ddm_c,
+ * src/example/c2fortran_kernel.f90:2964-3064): one process's box of a structured grid,
+ * padded by `margin` cells on both sides of each of the ndim axes, x fastest, so the box
+ * holds m = prod(n_grids[d] + 2 margin) cells (set_grids_decompostion,
+ * src/example/ddm_setup.f90).  Stencil point k couples interior cell j with cell
+ * j + offset[k], offset[k] = sum_d offset_dim[k + nnd d] * stride_d, with the value
+ * val[k m + j] (diaA); margin cells carry no unknowns.  b and x hold m entries (the
+ * interior cells are used; x's margin is left as it is). */
+#define PARCEL_B_DDM_BOXES_THREADS 0   /* CPU build: precon_thblock slabs along div_direc_th */
+#define PARCEL_B_DDM_BOXES_CUBES   1   /* GPU build (DDM_CUDA_BJ): n_d / 4 boxes per axis    */
+typedef struct parcel_b_ddm {
+  int32_t ndim;                /* 1..3                                                      */
+  int32_t n_grids[3];          /* interior cells per axis (entries beyond ndim ignored)     */
+  int32_t margin;              /* padding cells per side, >= the largest |offset_dim|       */
+  int64_t m;                   /* padded cells (n of parcel_dcg_ddm_c)                       */
+  int32_t nnd;                 /* stencil points, at most 32                                 */
+  const int32_t* offset;       /* nnd linear offsets                                         */
+  const int32_t* offset_dim;   /* nnd x ndim per-axis offsets, column-major (offset_dim)     */
+  const double* val;           /* nnd x m values (diaA)                                      */
+  int32_t div_direc_th;        /* thread-slab axis: 1 x, 2 y, 3 z                            */
+  int32_t boxes;               /* PARCEL_B_DDM_BOXES_*                                       */
+} parcel_b_ddm;
+
 /* Per-solve statistics (extension). */
 typedef struct parcel_b_stats {
   double setup_s;           /* preconditioner + layout setup, wall seconds           */
@@ -192,6 +215,32 @@ int parcel_b_ddsolve_dia(const parcel_b_input* prm, const parcel_b_dia* A, const
                          int precision_A, int precision_b, int precision_x, int precision_precondition,
                          const double* b_hi, const double* b_lo, double* x_hi, double* x_lo,
                          double* reshistory, int* niter, int* iret);
+
+/* parcel_ddm_main (src/src_DDM/ddm_kernel.f90:463-1756) on one process: CG / BiCGStab /
+ * GMRES / CA-GMRES (prm->solver) on the interior cells of a DDM box (host or device arrays).
+ * ipreflag 0 none, 1 point Jacobi, 2 block-Jacobi D-ILU on the boxes A->boxes selects
+ * (precon_thblock slabs for PARCEL_B_DDM_BOXES_THREADS); ILU_method is not used (the DDM
+ * preconditioner is D-ILU).  Not provided: additive Schwarz (ipreflag 3), the Neumann
+ * series (4) and the x-line-independent D-ILU (independ_nvec = 1), each refused with
+ * PARCEL_B_E_UNSUPPORTED.  The cells are renumbered box by box, each box's cells in
+ * lexicographic order, and the CRS solvers run on that matrix with the boxes as the
+ * block-Jacobi blocks; the renumbering time is part of the setup statistics. */
+int parcel_b_solve_ddm(const parcel_b_input* prm, const parcel_b_ddm* A, const double* b, double* x,
+                       double* reshistory, int* niter, int* iret);
+/* parcel_ddm_main_dd (ddm_kernel.f90:1758-1899): the double-double CG / BiCGStab / GMRES
+ * (prm->solver 1, 2 or 3) on a DDM box, with the arguments of parcel_b_ddcg (val_lo: the
+ * low parts, laid out as A->val; b_lo / x_lo: m entries or NULL). */
+int parcel_b_ddsolve_ddm(const parcel_b_input* prm, const parcel_b_ddm* A, const double* val_lo,
+                         int precision_A, int precision_b, int precision_x, int precision_precondition,
+                         const double* b_hi, const double* b_lo, double* x_hi, double* x_lo,
+                         double* reshistory, int* niter, int* iret);
+/* The renumbering of a DDM box: perm[r] (0-based padded cell of row r, for the interior
+ * cells) and the rows at which the boxes start (starts[0] = 0, starts[nb] = interior
+ * cells).  *nblocks: in, the capacity of starts minus one; out, the number of boxes (the
+ * call fails with PARCEL_B_E_ARG, having set it, when the capacity is too small).  perm may
+ * be NULL. */
+int parcel_b_ddm_order(const parcel_b_ddm* A, int precon_thblock, int32_t* perm, int32_t* starts,
+                       int32_t* nblocks);
 
 /* ---- drop-in shims, CPU-build ABI (host arrays; src/example/c2fortran_kernel.f90) ----
  * parcel_dcg_c       : c2fortran_kernel.f90:334-432  -> parcel_dcg (wrapper.f90:1995)
@@ -346,6 +395,90 @@ void parcel_dcagmres_dia_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n
                                 int* nblock, int* cagmres_sstep, int* cagmres_tstep, int* cagmres_basis,
                                 int* cagmres_qrflag, int* iret);
 
+/* ---- DDM drop-in shims (src/example/c2fortran_kernel.f90:2964-3691) -----------------
+ * parcel_dcg_ddm_c 2964-3064, parcel_dbicgstab_ddm_c 3066-3164, parcel_dgmres_ddm_c
+ * 3166-3270, parcel_ddcg_ddm_c 3272-3371, parcel_ddbicgstab_ddm_c 3373-3472,
+ * parcel_ddgmres_ddm_c 3474-3578, parcel_dcagmres_ddm_c 3580-3691.  n = m padded cells;
+ * one process (npe_dim all 1, no neighbour ranks; a box split over processes runs through
+ * parcel_b.ddm on torch.distributed).  The CPU-build forms (host arrays) cut the boxes as
+ * the CPU build does (precon_thblock slabs along div_direc_th), the _gpu_ forms (device
+ * arrays behind devicemem handles, as the CUDA build passes them) as the CUDA build does
+ * (n_d / 4 boxes per axis).  niter: in = itrmax, out = iterations used. */
+void parcel_dcg_ddm_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int* nnd, int32_t* offset,
+                       double* diaA, int* num_neighbor_ranks, int* neighbor_ranks, int* margin, int* ndim,
+                       int* npe_dim, int* n_grids, int* offset_dim, int* div_direc_th, int* ipreflag,
+                       int* addl, int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                       int* iovlflag, int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock,
+                       int* iret);
+void parcel_dbicgstab_ddm_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int* nnd, int32_t* offset,
+                             double* diaA, int* num_neighbor_ranks, int* neighbor_ranks, int* margin,
+                             int* ndim, int* npe_dim, int* n_grids, int* offset_dim, int* div_direc_th,
+                             int* ipreflag, int* addl, int* iflagas, int* niter, double* rtolmax,
+                             double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                             int* independ_nvec, int* nblock, int* iret);
+void parcel_dgmres_ddm_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int* nnd, int32_t* offset,
+                          double* diaA, int* num_neighbor_ranks, int* neighbor_ranks, int* margin,
+                          int* ndim, int* npe_dim, int* n_grids, int* offset_dim, int* div_direc_th,
+                          int* ipreflag, int* addl, int* iflagas, int* niter, double* rtolmax,
+                          double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                          int* independ_nvec, int* nblock, int* restart, int* gmres_gsflag, int* iret);
+void parcel_dcagmres_ddm_c_(int* icomm, double* vecx, double* vecb, int32_t* n, int* nnd, int32_t* offset,
+                            double* diaA, int* num_neighbor_ranks, int* neighbor_ranks, int* margin,
+                            int* ndim, int* npe_dim, int* n_grids, int* offset_dim, int* div_direc_th,
+                            int* ipreflag, int* addl, int* iflagas, int* niter, double* rtolmax,
+                            double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                            int* independ_nvec, int* nblock, int* cagmres_sstep, int* cagmres_tstep,
+                            int* cagmres_basis, int* cagmres_qrflag, int* iret);
+void parcel_ddcg_ddm_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo,
+                        int32_t* n, int* nnd, int32_t* offset, double* diaA, double* diaA_lo,
+                        int* num_neighbor_ranks, int* neighbor_ranks, int* margin, int* ndim, int* npe_dim,
+                        int* n_grids, int* offset_dim, int* div_direc_th, int* ipreflag, int* addl,
+                        int* iflagas, int* niter, double* rtolmax, double* reshistory, int* iovlflag,
+                        int* precon_thblock, int* neuman_itr, int* independ_nvec, int* nblock,
+                        int* precision_A, int* precision_b, int* precision_x, int* precision_precondition,
+                        int* iret);
+void parcel_ddbicgstab_ddm_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo,
+                              int32_t* n, int* nnd, int32_t* offset, double* diaA, double* diaA_lo,
+                              int* num_neighbor_ranks, int* neighbor_ranks, int* margin, int* ndim,
+                              int* npe_dim, int* n_grids, int* offset_dim, int* div_direc_th, int* ipreflag,
+                              int* addl, int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                              int* iovlflag, int* precon_thblock, int* neuman_itr, int* independ_nvec,
+                              int* nblock, int* precision_A, int* precision_b, int* precision_x,
+                              int* precision_precondition, int* iret);
+void parcel_ddgmres_ddm_c_(int* icomm, double* vecx, double* vecx_lo, double* vecb, double* vecb_lo,
+                           int32_t* n, int* nnd, int32_t* offset, double* diaA, double* diaA_lo,
+                           int* num_neighbor_ranks, int* neighbor_ranks, int* margin, int* ndim,
+                           int* npe_dim, int* n_grids, int* offset_dim, int* div_direc_th, int* ipreflag,
+                           int* addl, int* iflagas, int* niter, double* rtolmax, double* reshistory,
+                           int* iovlflag, int* precon_thblock, int* neuman_itr, int* independ_nvec,
+                           int* nblock, int* restart, int* gmres_gsflag, int* precision_A, int* precision_b,
+                           int* precision_x, int* precision_precondition, int* iret);
+void parcel_dcg_ddm_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int* nnd, void** offset,
+                           void** diaA, int* num_neighbor_ranks, int* neighbor_ranks, int* margin,
+                           int* ndim, int* npe_dim, int* n_grids, int* offset_dim, int* div_direc_th,
+                           int* ipreflag, int* addl, int* iflagas, int* niter, double* rtolmax,
+                           double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                           int* independ_nvec, int* nblock, int* iret);
+void parcel_dbicgstab_ddm_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int* nnd, void** offset,
+                                 void** diaA, int* num_neighbor_ranks, int* neighbor_ranks, int* margin,
+                                 int* ndim, int* npe_dim, int* n_grids, int* offset_dim, int* div_direc_th,
+                                 int* ipreflag, int* addl, int* iflagas, int* niter, double* rtolmax,
+                                 double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                                 int* independ_nvec, int* nblock, int* iret);
+void parcel_dgmres_ddm_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int* nnd, void** offset,
+                              void** diaA, int* num_neighbor_ranks, int* neighbor_ranks, int* margin,
+                              int* ndim, int* npe_dim, int* n_grids, int* offset_dim, int* div_direc_th,
+                              int* ipreflag, int* addl, int* iflagas, int* niter, double* rtolmax,
+                              double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                              int* independ_nvec, int* nblock, int* restart, int* gmres_gsflag, int* iret);
+void parcel_dcagmres_ddm_gpu_c_(int* icomm, void** vecx, void** vecb, int32_t* n, int* nnd, void** offset,
+                                void** diaA, int* num_neighbor_ranks, int* neighbor_ranks, int* margin,
+                                int* ndim, int* npe_dim, int* n_grids, int* offset_dim, int* div_direc_th,
+                                int* ipreflag, int* addl, int* iflagas, int* niter, double* rtolmax,
+                                double* reshistory, int* iovlflag, int* precon_thblock, int* neuman_itr,
+                                int* independ_nvec, int* nblock, int* cagmres_sstep, int* cagmres_tstep,
+                                int* cagmres_basis, int* cagmres_qrflag, int* iret);
+
 /* ---- split setup / solve (set_ksp_crs_c, start_ksp_solver_crs_c, get_vecx_ksp_crs_c,
  *      get_reshistory_ksp_crs_c: src/example/c2fortran_kernel.f90:2855-2961) ----------
  * A handle keeps the matrix layout and preconditioner on the device between solves. */
@@ -432,6 +565,11 @@ int parcel_b_bench_kernels(const parcel_b_input* prm, const parcel_b_crs* A, int
  * precon_thblock blocks) is built on the owned-owned submatrix. */
 typedef struct parcel_b_local_s* parcel_b_local;
 int parcel_b_local_create(const parcel_b_input* prm, const parcel_b_crs* A, int n_ext, parcel_b_local* out);
+/* As parcel_b_local_create, with explicit block-Jacobi blocks: the owned rows
+ * [starts[b], starts[b+1]) for b < nblocks (starts[0] = 0, starts[nblocks] = n; the boxes of
+ * a DDM process, parcel_b_ddm_order). */
+int parcel_b_local_create_blocks(const parcel_b_input* prm, const parcel_b_crs* A, int n_ext, int nblocks,
+                                 const int32_t* starts, parcel_b_local* out);
 /* y[n] = A x_ext[n_ext], device arrays. */
 int parcel_b_local_spmv(parcel_b_local h, const double* x_ext, double* y);
 /* z[n] = M^-1 r[n], device arrays. */

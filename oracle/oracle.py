@@ -66,12 +66,35 @@ def lib():
                                C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_ddcg.restype = C.c_int
+        L.orc_set_blocks.argtypes = [C.c_int, C.c_void_p]
+        L.orc_set_blocks.restype = C.c_int
         _lib = L
     return _lib
 
 
 def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
+
+
+class _Blocks:
+    """Explicit block-Jacobi blocks for the calls inside the with-statement: `starts` are
+    the 0-based first rows of the blocks followed by n (None: the equal split of
+    precon_thblock)."""
+
+    def __init__(self, starts):
+        self.starts = None if starts is None else np.ascontiguousarray(starts, dtype=np.int64)
+
+    def __enter__(self):
+        if self.starts is not None:
+            rc = lib().orc_set_blocks(len(self.starts) - 1, _ptr(self.starts))
+            if rc != 0:
+                raise ValueError("block starts must rise from 0 to n")
+        return self
+
+    def __exit__(self, *exc):
+        if self.starts is not None:
+            lib().orc_set_blocks(0, None)
+        return False
 
 
 class Matrix:
@@ -92,23 +115,25 @@ def params(solver=1, ipreflag=0, ILU_method=1, precon_thblock=-1, itrmax=1000, r
                      GMRES_m, GMRES_GSflag, sstep, tstep, basis, qrflag)
 
 
-def solve(A, b, x0=None, **kw):
-    """Runs the oracle solve; returns (x, reshistory[:niter], niter, iret)."""
+def solve(A, b, x0=None, blocks=None, **kw):
+    """Runs the oracle solve; returns (x, reshistory[:niter], niter, iret).  blocks:
+    explicit block-Jacobi row starts (see _Blocks)."""
     M = A if isinstance(A, Matrix) else Matrix(A)
     p = params(**kw)
     b = np.ascontiguousarray(b, dtype=np.float64)
     x = np.zeros(M.n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
     hist = np.zeros(max(p.itrmax, 1) + 1)
     niter, iret = C.c_int(0), C.c_int(0)
-    rc = lib().orc_solve(C.byref(M.s), C.byref(p), _ptr(b), _ptr(x), _ptr(hist),
-                         C.byref(niter), C.byref(iret))
+    with _Blocks(blocks):
+        rc = lib().orc_solve(C.byref(M.s), C.byref(p), _ptr(b), _ptr(x), _ptr(hist),
+                             C.byref(niter), C.byref(iret))
     if rc != 0:
         return x, hist[:0], 0, rc
     return x, hist[:niter.value].copy(), niter.value, iret.value
 
 
 def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, a_lo=None, prec_A=2, prec_b=2, prec_x=2, prec_M=2,
-         solver=1, **kw):
+         solver=1, blocks=None, **kw):
     """Double-double PCG (ddKSP_pCG, solver=1), BiCGStab (ddKSP_pBiCG, solver=2) or GMRES(m)
     (ddKSP_pGMRES, solver=3, GMRES_m / GMRES_GSflag as for gmres); returns
     (x_hi, x_lo, reshistory[:niter], niter, iret)."""
@@ -121,8 +146,9 @@ def ddcg(A, b_hi, b_lo=None, x0_hi=None, x0_lo=None, a_lo=None, prec_A=2, prec_b
     hist = np.zeros(max(p.itrmax, 1) + 1)
     niter, iret = C.c_int(0), C.c_int(0)
     ptr = lambda v: None if v is None else _ptr(v)
-    rc = lib().orc_ddcg(C.byref(M.s), ptr(alo), C.byref(p), prec_A, prec_b, prec_x, prec_M, _ptr(bh), ptr(bl),
-                        _ptr(xh), _ptr(xl), _ptr(hist), C.byref(niter), C.byref(iret))
+    with _Blocks(blocks):
+        rc = lib().orc_ddcg(C.byref(M.s), ptr(alo), C.byref(p), prec_A, prec_b, prec_x, prec_M, _ptr(bh),
+                            ptr(bl), _ptr(xh), _ptr(xl), _ptr(hist), C.byref(niter), C.byref(iret))
     if rc != 0:
         return xh, xl, hist[:0], 0, rc
     return xh, xl, hist[:niter.value].copy(), niter.value, iret.value
@@ -136,12 +162,13 @@ def spmv(A, x):
     return y
 
 
-def precon_apply(A, r, **kw):
+def precon_apply(A, r, blocks=None, **kw):
     M = A if isinstance(A, Matrix) else Matrix(A)
     p = params(**kw)
     r = np.ascontiguousarray(r, dtype=np.float64)
     s = np.zeros(M.n)
-    rc = lib().orc_precon_apply(C.byref(M.s), C.byref(p), _ptr(r), _ptr(s))
+    with _Blocks(blocks):
+        rc = lib().orc_precon_apply(C.byref(M.s), C.byref(p), _ptr(r), _ptr(s))
     if rc != 0:
         raise RuntimeError(f"oracle preconditioner setup failed: {rc}")
     return s
@@ -165,11 +192,12 @@ def num_threads() -> int:
 class Precon:
     """Persistent oracle preconditioner (setup once, apply many times)."""
 
-    def __init__(self, M: "Matrix", **kw):
+    def __init__(self, M: "Matrix", blocks=None, **kw):
         self.M = M
         self.p = params(**kw)
         err = C.c_int(0)
-        self.h = lib().orc_precon_create(C.byref(M.s), C.byref(self.p), C.byref(err))
+        with _Blocks(blocks):
+            self.h = lib().orc_precon_create(C.byref(M.s), C.byref(self.p), C.byref(err))
         if not self.h:
             raise RuntimeError(f"oracle preconditioner setup failed: {err.value}")
 

@@ -148,13 +148,25 @@ struct Precon {
   const OrcMat* A = nullptr;
 };
 
+// Explicit block boundaries (0-based row starts followed by n), set by orc_set_blocks for
+// the stencil-format (DDM) solves, whose blocks are the boxes of a geometric split laid out
+// one after another; empty: divide_region's equal split.
+std::vector<long> g_blk;
+
 int nblocks_for(const OrcMat& A, int thblock) {
+  if (!g_blk.empty()) return (int)g_blk.size() - 1;
   // The reference uses one block per OpenMP thread, capped by precon_thblock
   // (common.f90:89-123).  The oracle takes the block count explicitly; <= 0 means one
   // block, which is what the reference GPU build computes per process (cusparse.cu:17-197).
   int nb = thblock > 0 ? thblock : 1;
   if (nb > A.n) nb = A.n;
   return nb;
+}
+
+// Rows of block b, 1-based inclusive like divide_region.
+void block_rows(int b, int nb, long n, long* lo, long* hi) {
+  if (!g_blk.empty()) { *lo = g_blk[b] + 1; *hi = g_blk[b + 1]; return; }
+  divide_region(b, nb, 1, n, lo, hi);
 }
 
 // get_DInv_crs (matrix.f90:3104-3144): 1/a_ii, a zero pivot replaced by 1e-300.
@@ -177,7 +189,7 @@ int setup_ilu0(const OrcMat& A, int nb, Precon& P) {
 #pragma omp parallel for schedule(dynamic, 1) reduction(min : err)
   for (int b = 0; b < nb; ++b) {
     long lo, hi;
-    divide_region(b, nb, 1, A.n, &lo, &hi);
+    block_rows(b, nb, A.n, &lo, &hi);
     IluBlock& B = P.ilu[b];
     B.r0 = lo - 1; B.r1 = hi;
     long m = B.r1 - B.r0;
@@ -256,7 +268,7 @@ int setup_dilu(const OrcMat& A, int nb, int method, Precon& P) {
 #pragma omp parallel for schedule(dynamic, 1) reduction(min : err)
   for (int b = 0; b < nb; ++b) {
     long lo, hi;
-    divide_region(b, nb, 1, A.n, &lo, &hi);
+    block_rows(b, nb, A.n, &lo, &hi);
     DiluBlock& B = P.dilu[b];
     B.r0 = lo - 1; B.r1 = hi;
     long gs = A.istart + B.r0, ge = A.istart + B.r1 - 1;   // global in-block column range
@@ -343,6 +355,7 @@ int setup_precon(const OrcMat& A, const OrcParams& prm, Precon& P) {
   if (kind == ORC_PRECON_AS) kind = ORC_PRECON_BJ;     // one process: AS reduces to BJ
   P.kind = kind;
   P.ilu_method = prm.ILU_method < 0 ? ORC_ILUD : prm.ILU_method;  // default ILUD (type.f90:1042)
+  if (!g_blk.empty() && g_blk.back() != A.n) return ORC_E_ARG;
   int nb = nblocks_for(A, prm.precon_thblock);
   switch (kind) {
     case ORC_PRECON_NONE: return 0;
@@ -1087,6 +1100,18 @@ void orc_set_threads(int t) {
 #endif
 }
 
+// Explicit block-Jacobi blocks for the following calls: starts[0..nb] (0-based, starts[0]
+// = 0, starts[nb] = n, increasing); nb = 0 returns to the equal split.
+int orc_set_blocks(int nb, const long* starts) {
+  g_blk.clear();
+  if (nb <= 0) return 0;
+  if (!starts || starts[0] != 0) return ORC_E_ARG;
+  for (int b = 0; b < nb; ++b)
+    if (starts[b + 1] <= starts[b]) return ORC_E_ARG;
+  g_blk.assign(starts, starts + nb + 1);
+  return 0;
+}
+
 void orc_spmv(const OrcMat* A, const double* x, double* y) { spmv(*A, x, y); }
 
 double orc_dot(long n, const double* x, const double* y) { return dot(n, x, y); }
@@ -1169,6 +1194,7 @@ int orc_ddcg(const OrcMat* A, const double* alo, const OrcParams* prm, int prec_
     dd_setup_pj(*A, a_lo, P);
   } else if (kind == ORC_PRECON_BJ) {
     if (P.method == ORC_ILU0) return ORC_E_UNSUPPORTED;
+    if (!g_blk.empty() && g_blk.back() != n) return ORC_E_ARG;
     int err = dd_setup_dilu(*A, a_lo, nblocks_for(*A, prm->precon_thblock), P.method, P);
     if (err) return err;
   } else if (kind != ORC_PRECON_NONE) {

@@ -843,7 +843,7 @@ void dd_setup_precon(const Options& o, const parcel_b_crs& A, const DdSystem& S,
   H.n = A.n; H.nnz = A.nnz; H.istart = A.istart; H.rowptr = hrpp; H.col = hcip;
   std::vector<int> pos(A.n), lev(A.n);
   IluPlan plan;
-  ilu_build_plan(H, std::max(1, std::min(o.nblocks, A.n)), plan, pos.data(), lev.data());
+  ilu_build_plan(H, block_split(o, A.n), plan, pos.data(), lev.data());
   P.nb = plan.nb;
   P.chunks.alloc(sizeof(IluChunk) * std::max<size_t>(plan.chunks.size(), 1));
   h2d(P.chunks.p, plan.chunks.data(), sizeof(IluChunk) * plan.chunks.size());

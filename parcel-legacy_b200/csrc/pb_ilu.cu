@@ -70,16 +70,17 @@ void scatter_positions(int n, const int* pos, int* rowAt, cudaStream_t st) {
 // any coupling + 1; it is found in the same pass: lower couplings compare with rows whose
 // level is final, upper couplings (y, x) through the lowest level among x's upper-entry
 // sources, known once x is reached.
-void ilu_build_plan(const HostCSR& A, int nb, IluPlan& P, int* pos_out, int* lev_out,
+void ilu_build_plan(const HostCSR& A, const BlockSplit& blocks, IluPlan& P, int* pos_out, int* lev_out,
                     const std::function<void(int)>& block_ready) {
   const int n = A.n;
+  const int nb = blocks.nb;
   P.n = n;
   P.nb = nb;
   P.lev = lev_out;
   P.pos = pos_out;
   P.blk_lo.resize(nb);
   P.blk_hi.resize(nb);
-  for (int b = 0; b < nb; ++b) ilu_block_rows(b, nb, n, &P.blk_lo[b], &P.blk_hi[b]);
+  for (int b = 0; b < nb; ++b) blocks.rows(b, n, &P.blk_lo[b], &P.blk_hi[b]);
   std::vector<int> nlev(nb, 0), gap(nb, 0), missing_diag(nb, 0);
   std::vector<int> cL(n, 0), cU(n, 0);
   const int* rp = A.rowptr;

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <functional>
+#include <vector>
 
 #include "pb_common.cuh"
 
@@ -122,13 +123,26 @@ struct HostCSR {
 
 // Natural rows [lo, hi) of block-Jacobi block b of nb (0-based).
 void ilu_block_rows(int b, int nb, int n, int* lo, int* hi);
+
+// Row ranges of the block-Jacobi blocks: divide_region's equal split of the n rows into nb
+// parts (common.f90:125-182), or explicit 0-based row starts, starts[nb] = n (the boxes of a
+// stencil-format matrix, laid out one after another).
+struct BlockSplit {
+  int nb = 1;
+  std::vector<int> starts;
+  void rows(int b, int n, int* lo, int* hi) const {
+    if (starts.empty()) { ilu_block_rows(b, nb, n, lo, hi); return; }
+    *lo = starts[b];
+    *hi = starts[b + 1];
+  }
+};
 // rowAt[pos[i]] = i for i < n (entries not hit keep their value).
 void scatter_positions(int n, const int* pos, int* rowAt, cudaStream_t st);
 
 // Wavefront plan of the block-Jacobi blocks.  pos_out and lev_out (n entries each) receive
 // the permutation and the levels.  block_ready(b), when given, is called before block b's
 // rows are read (the structure may still be arriving from the device).
-void ilu_build_plan(const HostCSR& A, int nblocks, IluPlan& P, int* pos_out, int* lev_out,
+void ilu_build_plan(const HostCSR& A, const BlockSplit& blocks, IluPlan& P, int* pos_out, int* lev_out,
                     const std::function<void(int)>& block_ready = {});
 
 // Factorises (ILU(0)) or computes the D-ILU diagonal on the device and packs the sweep

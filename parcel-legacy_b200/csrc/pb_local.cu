@@ -94,6 +94,20 @@ int parcel_b_local_create(const parcel_b_input* prm, const parcel_b_crs* A, int 
   });
 }
 
+int parcel_b_local_create_blocks(const parcel_b_input* prm, const parcel_b_crs* A, int n_ext, int nblocks,
+                                 const int32_t* starts, parcel_b_local* out) {
+  std::vector<int> s;
+  const int rc = guarded([&]() -> int {
+    PB_CHECK(starts != nullptr && nblocks >= 1, PARCEL_B_E_ARG, "explicit blocks: nblocks = %d, starts %s", nblocks,
+             starts ? "given" : "NULL");
+    s.assign(starts, starts + nblocks + 1);
+    return 0;
+  });
+  if (rc < 0) return rc;
+  ScopedBlockStarts blocks(&s);   // the owned-owned system's block split (block_split checks it)
+  return parcel_b_local_create(prm, A, n_ext, out);
+}
+
 int parcel_b_local_spmv(parcel_b_local h, const double* x_ext, double* y) {
   return guarded([&]() -> int {
     PB_CHECK(h && x_ext && y, PARCEL_B_E_ARG, "NULL argument");

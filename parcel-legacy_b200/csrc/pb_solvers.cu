@@ -29,8 +29,32 @@ double now_s() {
 }
 
 // ------------------------------------------------------------------ options
+namespace {
+thread_local const std::vector<int>* t_block_starts = nullptr;
+}  // namespace
+
+ScopedBlockStarts::ScopedBlockStarts(const std::vector<int>* starts) { t_block_starts = starts; }
+ScopedBlockStarts::~ScopedBlockStarts() { t_block_starts = nullptr; }
+
+BlockSplit block_split(const Options& o, int n) {
+  BlockSplit bs;
+  if (o.block_starts.empty()) {
+    bs.nb = std::max(1, std::min(o.nblocks, n));
+    return bs;
+  }
+  const auto& s = o.block_starts;
+  PB_CHECK(s.size() >= 2 && s.front() == 0 && s.back() == n, PARCEL_B_E_ARG,
+           "explicit blocks must start at row 0 and end at n = %d", n);
+  for (size_t b = 0; b + 1 < s.size(); ++b)
+    PB_CHECK(s[b + 1] > s[b], PARCEL_B_E_ARG, "explicit block %d is empty", (int)b);
+  bs.nb = (int)s.size() - 1;
+  bs.starts = s;
+  return bs;
+}
+
 Options resolve_options(const parcel_b_input* p) {
   Options o;
+  if (t_block_starts) o.block_starts = *t_block_starts;
   if (!p) return o;
   if (p->solver > 0) o.solver = p->solver;
   if (p->ipreflag >= 0) o.precon = p->ipreflag;
@@ -138,7 +162,8 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
     // block-aligned pieces, each with an event, so that the plan of the first blocks
     // overlaps the copy of the others.  The plan writes the permutation and the levels
     // into the same staging area, from where they go back to the device.
-    const int nb = std::max(1, std::min(o.nblocks, A.n));
+    const BlockSplit bs = block_split(o, A.n);
+    const int nb = bs.nb;
     const size_t n1 = (size_t)A.n + 1, nz = (size_t)A.nnz;
     int* pin = static_cast<int*>(pinned_staging(sizeof(int) * ((dev ? n1 + nz : 0) + 2 * (size_t)A.n)));
     int* hpos = pin + (dev ? n1 + nz : 0);
@@ -164,8 +189,8 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
         cudaError_t e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
         if (e == cudaSuccess && b1 > b0) {
           int lo0, hi0, lo1, hi1;
-          ilu_block_rows(b0, nb, A.n, &lo0, &hi0);
-          ilu_block_rows(b1 - 1, nb, A.n, &lo1, &hi1);
+          bs.rows(b0, A.n, &lo0, &hi0);
+          bs.rows(b1 - 1, A.n, &lo1, &hi1);
           const size_t j0 = (size_t)(hrpp[lo0] - 1), j1 = (size_t)(hrpp[hi1] - 1);   // 1-based
           if (j1 > j0) e = cudaMemcpyAsync(pin + n1 + j0, A.col + j0, sizeof(int) * (j1 - j0), cudaMemcpyDeviceToHost, st);
         }
@@ -185,7 +210,7 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
     IluPlan P;
     trace_mark("setup: row pointers to host");
     try {
-      ilu_build_plan(H, nb, P, hpos, hlev, ready);
+      ilu_build_plan(H, bs, P, hpos, hlev, ready);
     } catch (...) {
       destroy_events();
       throw;

@@ -28,6 +28,7 @@ struct Options {
   double inner_rtol = 1e-4;
   int max_refine = 50;
   int independ_nvec = 1;
+  std::vector<int> block_starts;                       // explicit block-Jacobi blocks (BlockSplit)
   bool use_graphs = true;
   bool fused_mgs = true;
   bool flexible = false;                               // GMRES: flexible variant (keeps M^-1 v_j)
@@ -35,6 +36,19 @@ struct Options {
 };
 
 Options resolve_options(const parcel_b_input* p);
+
+// The block-Jacobi blocks of an n-row solve: o.block_starts when given (checked: rising
+// from 0 to n), else divide_region's split into min(o.nblocks, n) blocks.
+BlockSplit block_split(const Options& o, int n);
+
+// Explicit block starts for every resolve_options on this thread while the guard lives
+// (a stencil-format solve hands its boxes to the CRS solvers this way).
+struct ScopedBlockStarts {
+  explicit ScopedBlockStarts(const std::vector<int>* starts);
+  ~ScopedBlockStarts();
+  ScopedBlockStarts(const ScopedBlockStarts&) = delete;
+  ScopedBlockStarts& operator=(const ScopedBlockStarts&) = delete;
+};
 
 // Preconditioner on iteration-layout vectors.
 template <class T>

@@ -51,6 +51,12 @@ class Dia(C.Structure):
                 ("val", C.c_void_p), ("offset", C.c_void_p)]
 
 
+class Ddm(C.Structure):
+    _fields_ = [("ndim", C.c_int32), ("n_grids", C.c_int32 * 3), ("margin", C.c_int32), ("m", C.c_int64),
+                ("nnd", C.c_int32), ("offset", C.c_void_p), ("offset_dim", C.c_void_p), ("val", C.c_void_p),
+                ("div_direc_th", C.c_int32), ("boxes", C.c_int32)]
+
+
 class Stats(C.Structure):
     _fields_ = [("setup_s", C.c_double), ("solve_s", C.c_double), ("total_s", C.c_double),
                 ("true_relres", C.c_double), ("true_relres_dd", C.c_double),
@@ -65,6 +71,15 @@ IP = C.POINTER(C.c_int)
 I32P = C.POINTER(C.c_int32)
 DP = C.POINTER(C.c_double)
 PP = C.POINTER(C.c_void_p)
+
+# DDM shim arguments after n: nnd, offset, diaA (host pointers or, _G, devicemem handles),
+# num_neighbor_ranks, neighbor_ranks, margin, ndim, npe_dim, n_grids, offset_dim,
+# div_direc_th, ipreflag, addL, iflagAS, niter, rtolmax, reshistory, iovlflag,
+# precon_thblock, Neuman_itr, independ_nvec, nBlock (_DD: diaA_lo after diaA)
+_DDM_TAIL = [IP] * 12 + [DP, P] + [IP] * 5
+_DDM_H = [IP, I32P, P] + _DDM_TAIL
+_DDM_G = [IP, PP, PP] + _DDM_TAIL
+_DDM_DD = [IP, I32P, P, P] + _DDM_TAIL
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -133,6 +148,24 @@ SIGNATURES = {
                                  [IP] * 10),
     "parcel_ddgmres_dia_c_": (None, [IP, P, P, P, P, I32P, I32P, I32P, P, P, P, I32P] + [IP] * 5 + [DP, P] +
                               [IP] * 11),
+    "parcel_b_solve_ddm": (C.c_int, [C.POINTER(Input), C.POINTER(Ddm), P, P, P, IP, IP]),
+    "parcel_b_ddsolve_ddm": (C.c_int, [C.POINTER(Input), C.POINTER(Ddm), P, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       P, P, P, P, P, IP, IP]),
+    "parcel_b_ddm_order": (C.c_int, [C.POINTER(Ddm), C.c_int, I32P, I32P, I32P]),
+    # DDM shims: n (padded cells), nnd, offset, diaA, the decomposition and the solver arguments
+    "parcel_dcg_ddm_c_": (None, [IP, P, P, I32P] + _DDM_H + [IP]),
+    "parcel_dbicgstab_ddm_c_": (None, [IP, P, P, I32P] + _DDM_H + [IP]),
+    "parcel_dgmres_ddm_c_": (None, [IP, P, P, I32P] + _DDM_H + [IP] * 3),
+    "parcel_dcagmres_ddm_c_": (None, [IP, P, P, I32P] + _DDM_H + [IP] * 5),
+    "parcel_ddcg_ddm_c_": (None, [IP, P, P, P, P, I32P] + _DDM_DD + [IP] * 5),
+    "parcel_ddbicgstab_ddm_c_": (None, [IP, P, P, P, P, I32P] + _DDM_DD + [IP] * 5),
+    "parcel_ddgmres_ddm_c_": (None, [IP, P, P, P, P, I32P] + _DDM_DD + [IP] * 7),
+    "parcel_dcg_ddm_gpu_c_": (None, [IP, PP, PP, I32P] + _DDM_G + [IP]),
+    "parcel_dbicgstab_ddm_gpu_c_": (None, [IP, PP, PP, I32P] + _DDM_G + [IP]),
+    "parcel_dgmres_ddm_gpu_c_": (None, [IP, PP, PP, I32P] + _DDM_G + [IP] * 3),
+    "parcel_dcagmres_ddm_gpu_c_": (None, [IP, PP, PP, I32P] + _DDM_G + [IP] * 5),
+    "parcel_b_local_create_blocks": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, C.c_int, I32P,
+                                               C.POINTER(P)]),
     "parcel_b_bench_kernels": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, DP, DP]),
     "parcel_b_local_create": (C.c_int, [C.POINTER(Input), C.POINTER(Crs), C.c_int, C.POINTER(P)]),
     "parcel_b_local_spmv": (C.c_int, [P, P, P]),

@@ -38,6 +38,16 @@ def parse_errors(path: str):
     return out
 
 
+def parse_ddm_history(path: str):
+    """main_ddm.f90 prints `i reshistory(i)` for the iterations used, then the timings."""
+    h = []
+    for line in open(path):
+        m = re.match(r"\s*(\d+)\s+(\S+)\s*$", line)
+        if m:
+            h.append(float(m.group(2).replace("D", "E")))
+    return h
+
+
 def parse_qr(path: str):
     return [line.rstrip("\n") for line in open(path)]
 
@@ -70,12 +80,29 @@ def main(ref: str) -> None:
         "history_dd": dd[:half], "history_double": dbl[:half],
         **parse_errors(os.path.join(ex, "template_cpu", "STDOUT_run_dd")),
     }
+    ddm = "make_poisson_3D_DDM 160x160x160 on npe = (1, 4, 1), RHS of the example, x0 = 0"
+    fx["cpu_ddm_cg_slabs"] = {
+        "source": "src/example/template_cpu/STDOUT_run_ddm", "problem": ddm, "solver": "CG", "ipreflag": 2,
+        "npe": [1, 4, 1], "div_direc_th": 1, "threads": 20,
+        "blocks_note": "4 processes x 20 OpenMP threads: D-ILU on 80 boxes of 8 x 40 x 160 cells",
+        "rtolmax": 1e-9, "history": parse_ddm_history(os.path.join(ex, "template_cpu", "STDOUT_run_ddm")),
+    }
+    fx["gpu_ddm_cg_cubes"] = {
+        "source": "src/example/template_gpu/STDOUT_run_ddm", "problem": ddm, "solver": "CG", "ipreflag": 2,
+        "npe": [1, 4, 1], "blocks_note": "CUDA build (DDM_CUDA_BJ): D-ILU on 4 x 4 x 4 boxes",
+        "rtolmax": 1e-9, "history": parse_ddm_history(os.path.join(ex, "template_gpu", "STDOUT_run_ddm")),
+    }
+    fx["cpu_ddm_ddcg_slabs"] = {
+        "source": "src/example/template_cpu/STDOUT_run_ddm_dd", "problem": ddm, "solver": "ddCG", "ipreflag": 2,
+        "npe": [1, 4, 1], "div_direc_th": 1, "threads": 20, "precision": [2, 2, 2, 2],
+        "rtolmax": 1e-9, "history": parse_ddm_history(os.path.join(ex, "template_cpu", "STDOUT_run_ddm_dd")),
+    }
     fx["cpu_qr"] = {"source": "src/example/template_cpu/STDOUT_run_qr",
                     "lines": parse_qr(os.path.join(ex, "template_cpu", "STDOUT_run_qr"))}
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_templates.json")
     with open(out, "w") as f:
         json.dump(fx, f, indent=1)
-    print("wrote", out, {k: len(v.get("history_crs", v.get("history_dd", []))) for k, v in fx.items()})
+    print("wrote", out, {k: len(v.get("history_crs", v.get("history_dd", v.get("history", [])))) for k, v in fx.items()})
 
 
 if __name__ == "__main__":

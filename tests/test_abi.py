@@ -54,6 +54,29 @@ def test_struct_layouts_match_c(tmp_path):
     assert [int(v) for v in out] == want
 
 
+def test_ddm_struct_layout_matches_c(tmp_path):
+    src = tmp_path / "ddm.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "parcel_b.h"\n'
+                   'int main(){printf("%zu %zu %zu %zu %zu\\n", sizeof(parcel_b_ddm), offsetof(parcel_b_ddm, m), '
+                   'offsetof(parcel_b_ddm, offset), offsetof(parcel_b_ddm, val), offsetof(parcel_b_ddm, boxes));'
+                   'return 0;}\n')
+    exe = tmp_path / "ddm"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    D = _lib.Ddm
+    assert [int(v) for v in out] == [C.sizeof(D), D.m.offset, D.offset.offset, D.val.offset, D.boxes.offset]
+
+
+def test_ddm_shim_signatures_count_the_reference_arguments():
+    """parcel_dcg_ddm_c takes 27 arguments (c2fortran_kernel.f90:2964-2983), the dd form 34
+    (3272-3295)."""
+    decl = _c_declarations()
+    assert len(decl["parcel_dcg_ddm_c_"][1]) == 27 == len(_lib.SIGNATURES["parcel_dcg_ddm_c_"][1])
+    assert len(decl["parcel_dgmres_ddm_c_"][1]) == 29 == len(_lib.SIGNATURES["parcel_dgmres_ddm_c_"][1])
+    assert len(decl["parcel_ddcg_ddm_c_"][1]) == 34 == len(_lib.SIGNATURES["parcel_ddcg_ddm_c_"][1])
+    assert len(decl["parcel_dcagmres_ddm_gpu_c_"][1]) == 31 == len(_lib.SIGNATURES["parcel_dcagmres_ddm_gpu_c_"][1])
+
+
 def test_input_defaults_are_minus_one():
     p = _lib.new_input()
     for f in ("ipreflag", "ILU_method", "solver", "GMRES_m", "itrmax", "precon_thblock", "independ_nvec"):

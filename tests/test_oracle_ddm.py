@@ -1,0 +1,116 @@
+"""Pins the oracle's DDM restatement (oracle/ddm.py).
+
+  * the example's DDM generator (make_poisson_3D_DDM) on one process is the CRS example
+    problem, and on several processes their union is;
+  * the D-ILU applied cell by cell on each process's padded box (as_ddm_init and
+    ilu_ddm_case_{x,y,z}div, or the CUDA build's 4^3 boxes) equals the CRS block-Jacobi D-ILU
+    of the matrix renumbered process by process, box by box, with the boxes as the blocks
+    (1e-13 relative): slabs along x, y and z with uneven splits, uneven cubes, 1 and 4
+    processes;
+  * with that renumbering the CRS oracle reproduces the reference's stored DDM outputs
+    (src/example/template_cpu/STDOUT_run_ddm: 4 processes x 20 x-slabs, CG, 261 iterations;
+    template_gpu/STDOUT_run_ddm: 4^3 boxes, 345; template_cpu/STDOUT_run_ddm_dd: the
+    double-double CG, 261), iteration counts exact, histories within 1e-6 relative (the
+    reference sums its dot products per thread and process in another order).
+"""
+import numpy as np
+import pytest
+
+import ddm
+import oracle
+from conftest import golden
+from parcel_b import problems
+from parcel_b.problems import CRS
+
+
+def _slabs(axis, nth):
+    return lambda n: ddm.thread_boxes(n, axis, nth)
+
+
+def _system(gn, npe, boxes_of):
+    parts = [ddm.poisson3d_ddm(gn, npe, r) for r in range(int(np.prod(npe)))]
+    return parts, ddm.global_system(parts, npe, boxes_of)
+
+
+def _crs(G):
+    return CRS(n=G["n"], rowptr=G["rowptr"], col=G["col"], val=G["val"])
+
+
+@pytest.mark.parametrize("npe", [(1, 1, 1), (2, 2, 1), (1, 4, 1)])
+def test_generator_is_the_crs_example_problem(npe):
+    gn = (8, 8, 6)
+    parts, G = _system(gn, npe, lambda n: [((0, n[0]), (0, n[1]), (0, n[2]))])
+    A, b, xe = problems.poisson3d_reference(*gn)
+    S = A.to_scipy().tocsr()
+    # the global rows are the natural cells in another order: compare through the padded ids
+    nat = np.zeros(G["n"], dtype=np.int64)
+    for r, p in enumerate(parts):
+        sel = G["rank"] == r
+        j = G["padded"][sel]
+        mx, my, _ = p["pad"]
+        x, y, z = j % mx - 1, (j // mx) % my - 1, j // (mx * my) - 1
+        nat[sel] = (x + p["start"][0]) + gn[0] * ((y + p["start"][1]) + gn[1] * (z + p["start"][2]))
+    assert np.array_equal(np.sort(nat), np.arange(A.n))
+    P = S[nat][:, nat].tocsr()
+    P.sort_indices()
+    assert np.array_equal(P.indptr + 1, G["rowptr"]) and np.array_equal(P.indices + 1, G["col"])
+    assert np.array_equal(P.data, G["val"])
+    assert np.array_equal(b[nat], G["b"]) and np.allclose(xe[nat], G["x_exact"], rtol=1e-15, atol=0)
+
+
+@pytest.mark.parametrize("boxes,axis", [(_slabs(1, 3), 0), (_slabs(2, 2), 1), (_slabs(3, 4), 2),
+                                        (ddm.cube_boxes, None)])
+@pytest.mark.parametrize("npe", [(1, 1, 1), (2, 2, 1), (1, 2, 2)])
+def test_box_dilu_is_the_renumbered_crs_dilu(boxes, axis, npe):
+    parts, G = _system((9, 8, 7), npe, boxes)
+    rng = np.random.default_rng(5)
+    r = rng.standard_normal(G["n"])
+    zc = oracle.precon_apply(_crs(G), r, ipreflag=2, ILU_method=1, blocks=G["starts"])
+    zd = np.zeros(G["n"])
+    for k, p in enumerate(parts):
+        sel = G["rank"] == k
+        rp = np.zeros(p["m"])
+        rp[G["padded"][sel]] = r[sel]
+        zd[sel] = ddm.dilu_apply(p, boxes(p["n"]), rp, split_axis=axis)[G["padded"][sel]]
+    assert np.abs(zc - zd).max() <= 1e-13 * np.abs(zc).max()
+
+
+def test_box_shapes_follow_the_reference_splits():
+    # set_region_for_threads: 10 cells over 4 threads -> 2, 2, 2, 4
+    assert [b[0] for b in ddm.thread_boxes((10, 3, 3), 1, 4)] == [(0, 2), (2, 4), (4, 6), (6, 10)]
+    # more threads than cells: every slab but the last is empty
+    assert [b[1] for b in ddm.thread_boxes((3, 2, 3), 2, 5)] == [(0, 2)]
+    # init_DILU_DDM: n = 18 -> 4 divisions of ceil(18 / 4) = 5 -> 5, 5, 5, 3; n = 3 -> one box
+    assert sorted({b[0] for b in ddm.cube_boxes((18, 3, 4))}) == [(0, 5), (5, 10), (10, 15), (15, 18)]
+    assert {b[1] for b in ddm.cube_boxes((18, 3, 4))} == {(0, 3)}
+
+
+def _template(case, boxes_of, **kw):
+    fx = golden()[case]
+    parts, G = _system((160, 160, 160), tuple(fx["npe"]), boxes_of)
+    g = np.array(fx["history"])
+    if kw.pop("dd", False):
+        xh, xl, h, niter, iret = oracle.ddcg(_crs(G), G["b"], ipreflag=2, ILU_method=1, itrmax=2000, rtolmax=1e-9,
+                                             blocks=G["starts"])
+    else:
+        x, h, niter, iret = oracle.solve(_crs(G), G["b"], solver=1, ipreflag=2, ILU_method=1, itrmax=2000,
+                                         rtolmax=1e-9, blocks=G["starts"])
+    assert iret == 0 and niter == len(g), (niter, len(g))
+    rel = np.abs(h - g) / g
+    assert rel.max() <= 1e-6, rel.max()
+    return rel.max()
+
+
+@pytest.mark.slow
+def test_cpu_ddm_template_slabs():
+    _template("cpu_ddm_cg_slabs", _slabs(1, 20))
+
+
+@pytest.mark.slow
+def test_gpu_ddm_template_cubes():
+    _template("gpu_ddm_cg_cubes", ddm.cube_boxes)
+
+
+@pytest.mark.slow
+def test_cpu_ddm_dd_template_slabs():
+    _template("cpu_ddm_ddcg_slabs", _slabs(1, 20), dd=True)
