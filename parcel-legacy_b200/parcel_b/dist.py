@@ -115,7 +115,9 @@ class CudaLocal:
         self._L = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("the distributed solve runs on the GPU library: no CUDA device")
-        p = new_input(**options)
+        # blocks: explicit block-Jacobi row starts of this process (a DDM process's boxes)
+        starts = options.get("blocks")
+        p = new_input(**{k: v for k, v in options.items() if k != "blocks"})
         rp = np.ascontiguousarray(layout.rowptr, np.int32)
         ci = np.ascontiguousarray(layout.local_col, np.int32)
         va = np.ascontiguousarray(val, np.float64)
@@ -123,7 +125,13 @@ class CudaLocal:
         S.n, S.gn, S.nnz, S.istart = layout.n, layout.n, int(ci.shape[0]), 1
         S.rowptr, S.col, S.val = rp.ctypes.data, ci.ctypes.data, va.ctypes.data
         h = C.c_void_p()
-        if self._L.parcel_b_local_create(C.byref(p), C.byref(S), layout.n_ext, C.byref(h)) != 0:
+        if starts is None:
+            rc = self._L.parcel_b_local_create(C.byref(p), C.byref(S), layout.n_ext, C.byref(h))
+        else:
+            st = np.ascontiguousarray(starts, np.int32)
+            rc = self._L.parcel_b_local_create_blocks(C.byref(p), C.byref(S), layout.n_ext, len(st) - 1,
+                                                      st.ctypes.data_as(_lib.I32P), C.byref(h))
+        if rc != 0:
             raise RuntimeError(f"parcel_b_local_create failed: {_lib.last_error()}")
         self.h = h
 
@@ -275,7 +283,8 @@ def solve(layout: Layout, val, b: torch.Tensor, x: torch.Tensor, backend=None, *
     (float64 tensors on the backend's device; x is the initial guess and the result).
     options: the parcel_b_input fields (solver 1 = CG, 3 = GMRES; ipreflag, ILU_method,
     precon_thblock = block-Jacobi blocks of this process, itrmax, rtolmax, GMRES_m,
-    GMRES_GSflag).  Returns (niter, iret, reshistory)."""
+    GMRES_GSflag) and, for the default backend, blocks = explicit block-Jacobi row starts of
+    this process.  Returns (niter, iret, reshistory)."""
     solver = int(options.get("solver", 3))
     itrmax = int(options.get("itrmax", 100))
     rtol = float(options.get("rtolmax", 1e-8))
