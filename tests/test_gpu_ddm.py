@@ -69,7 +69,7 @@ def test_ddm_solve_matches_oracle(solver, name, opt, boxes_of):
     x = g["x"]
     assert np.max(np.abs(x[G["padded"]] - xo)) <= 1e-8 * np.max(np.abs(xo))
     assert np.all(x[margin] == 7.0)
-    assert g["stats"].ilu_nblocks == len(boxes_of(p["n"]))
+    assert g["stats"]["ilu_nblocks"] == len(boxes_of(p["n"]))
 
 
 @pytest.mark.parametrize("ipreflag", [0, 1])
