@@ -339,6 +339,15 @@ def configs_summary():
     x = r["x_hi"].cpu().numpy() + r["x_lo"].cpu().numpy()
     out["ddgmres128"] = {"s": sec, "iterations": r["niter"], "iret": r["iret"],
                          "true_relres": oracle.true_relres(A, b, x)}
+    import ddm as oddm
+    from parcel_b import ddm
+    p = oddm.poisson3d_ddm((160, 160, 160), (1, 1, 1), 0)
+    val, off, bd = t(p["val"]), t(p["offset"]), t(p["b"])
+    sec, r = timed(lambda: ddm.solve(val, off, p["offset_dim"], p["n"], bd, boxes=ddm.BOXES_CUBES, solver=1,
+                                     ipreflag=2, itrmax=2000, rtolmax=1e-9))
+    x = r["x"].cpu().numpy()
+    out["ddm160"] = {"s": sec, "iterations": r["niter"], "iret": r["iret"], "template_iterations": 345,
+                     "max_rel_error": float(np.abs(x - p["x_exact"]).max() / np.abs(p["x_exact"]).max())}
     return out
 
 
@@ -1082,6 +1091,142 @@ def run_reference_config(args):
     print(json.dumps(out))
 
 
+DDM_METRIC = "DDM CG solve time (s), 160^3 Poisson, block-Jacobi D-ILU on 4^3 boxes, rtol 1e-9"
+
+
+def _ddm_problem():
+    import ddm as oddm
+    return oddm.poisson3d_ddm((160, 160, 160), (1, 1, 1), 0)
+
+
+def run_ddm(args):
+    """The reference's DDM example as its CUDA build runs it (src/example/main_ddm.f90,
+    make_poisson_3D_DDM 160^3, CG, block-Jacobi D-ILU on 4^3 boxes (DDM_CUDA_BJ), rtol 1e-9,
+    x0 = 0; template_gpu/STDOUT_run_ddm: 345 iterations and a printed solve time of 0.617 s
+    with 4 processes of a y-split, whose boxes are the same 4^3 boxes).  One process holds
+    the whole grid here.  value: the whole parcel_b_solve_ddm call (renumbering, set-up and
+    solve, as the reference's timer brackets parcel_dcg_ddm) with the arrays in HBM, CUDA
+    events on the library stream; e2e: the same call with pinned host arrays (copies inside
+    the timed region); cpu_baseline: the oracle on the renumbered matrix (oracle/ddm.py), one
+    full solve on all host cores; rooflines: the SpMV and the D-ILU sweep of the renumbered
+    system (parcel_b_bench_kernels_ddm), with the byte models of the default line."""
+    import torch
+    from parcel_b import _lib, ddm
+    L = _lib.load()
+    p = _ddm_problem()
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    val, off, bd = t(p["val"]), t(p["offset"]), t(p["b"])
+    stream = torch.cuda.ExternalStream(L.parcel_b_get_stream(), device=dev)
+    kw = dict(boxes=ddm.BOXES_CUBES, solver=1, ipreflag=2, itrmax=2000, rtolmax=1e-9)
+
+    def solve_dev():
+        return ddm.solve(val, off, p["offset_dim"], p["n"], bd, **kw)
+
+    for _ in range(args.warmup):
+        res = solve_dev()
+    torch.cuda.synchronize()
+    clk = Clocks(0)
+    clk.started()
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = solve_dev()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    clocks = clk.stop()
+    x = res["x"].cpu().numpy()
+    err = float(np.abs(x - p["x_exact"]).max() / np.abs(p["x_exact"]).max())
+    hist_dev = res["reshistory"]
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "reference_templates.json")) as f:
+            g = np.array(json.load(f)["gpu_ddm_cg_cubes"]["history"])
+        k = min(len(g), len(hist_dev))
+        parity = {"template_iterations": len(g), "max_rel_history_diff": float(np.max(np.abs(hist_dev[:k] - g[:k]) / g[:k]))}
+    except (OSError, KeyError):
+        parity = None
+    # end to end: the same call with pinned host arrays
+    hp = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    h_val, h_off, h_b = hp(p["val"]), hp(p["offset"]), hp(p["b"])
+    e2e = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        ddm.solve(h_val, h_off, p["offset_dim"], p["n"], h_b, **kw)
+        e2e.append(time.perf_counter() - t0)
+    # kernel rooflines on the renumbered system
+    prm = _lib.new_input(solver=1, ipreflag=2)
+    D = ddm.ddm_struct(val, off, p["offset_dim"], p["n"], boxes=ddm.BOXES_CUBES)
+    ms_spmv, ms_pre = C.c_double(0), C.c_double(0)
+    rc = L.parcel_b_bench_kernels_ddm(C.byref(prm), C.byref(D), 50, C.byref(ms_spmv), C.byref(ms_pre))
+    if rc != 0:
+        raise RuntimeError(f"parcel_b_bench_kernels_ddm failed: {_lib.last_error()}")
+    n = int(np.prod(p["n"]))
+    nnz = int(np.count_nonzero(p["val"]))
+    hbm, peak_kind = peaks()
+    spmv_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
+    ilu_bytes = 12 * nnz + 8 * (n + 1) + 32 * n
+    sp_ach = spmv_bytes / (ms_spmv.value * 1e-3) / 1e9
+    il_ach = ilu_bytes / (ms_pre.value * 1e-3) / 1e9
+    m = p["m"]
+    out = {"metric": DDM_METRIC, "value": sum(times) / len(times), "unit": "s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "DDM 160^3 Poisson (make_poisson_3D_DDM), CG + block-Jacobi D-ILU on 4^3 boxes, "
+                                  "rtol 1e-9, one process", "n": n, "padded_cells": m, "nnz": nnz,
+                      "l2": "inputs larger than L2 (the 7 x 4.4M-cell DIA values are 245 MB)"},
+           "iterations": res["niter"], "iret": res["iret"], "max_rel_error": err, "parity": parity,
+           "setup_s": res["stats"]["setup_s"], "solve_s": res["stats"]["solve_s"],
+           "step_times_s": [round(v, 6) for v in times],
+           "e2e": {"value": sum(e2e) / len(e2e), "unit": "s", "h2d_bytes_per_step": int(h_val.nbytes + h_off.nbytes + 2 * m * 8),
+                   "d2h_bytes_per_step": int(m * 8 + res["niter"] * 8)},
+           "roofline": {"bound": "hbm", "kernel": "k_spmv_sell<double,double> on the renumbered system",
+                        "achieved": sp_ach, "peak": hbm, "unit": "GB/s", "frac": sp_ach / hbm, "peak_kind": peak_kind,
+                        "traffic": None, "algorithmic_bytes": int(spmv_bytes), "us_per_launch": ms_spmv.value * 1e3},
+           "roofline_dominant": {"bound": "hbm", "kernel": "block-Jacobi D-ILU sweep over the 64,000 boxes",
+                                 "achieved": il_ach, "peak": hbm, "unit": "GB/s", "frac": il_ach / hbm,
+                                 "peak_kind": peak_kind, "algorithmic_bytes": int(ilu_bytes),
+                                 "us_per_launch": ms_pre.value * 1e3},
+           "reference_printed_solve_s": {"cuda_build_4_processes": 0.617148808203638,
+                                         "cpu_build_4x20_threads_x_slabs": 1.58943619503407},
+           "clocks": clocks, "gpu_launches": int(res["stats"]["kernel_launches"]) * args.steps}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = _ddm_oracle_run()
+    print(json.dumps(out))
+
+
+def _ddm_oracle_run():
+    """The oracle's CG on the renumbered DDM system (all host threads): one full solve."""
+    import ddm as oddm
+    import oracle
+    from parcel_b.problems import CRS
+    p = _ddm_problem()
+    G = oddm.global_system([p], (1, 1, 1), oddm.cube_boxes)
+    A = CRS(n=G["n"], rowptr=G["rowptr"], col=G["col"], val=G["val"])
+    t0 = time.perf_counter()
+    _, h, niter, iret = oracle.solve(A, G["b"], solver=1, ipreflag=2, ILU_method=1, itrmax=2000, rtolmax=1e-9,
+                                     blocks=G["starts"])
+    return {"value": time.perf_counter() - t0, "unit": "s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"one full oracle solve of the renumbered system ({niter} iterations, iret {iret})"}
+
+
+def run_reference_ddm(args):
+    """Reference arm of the DDM line: the oracle's CPU restatement, one full solve per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    vals = [_ddm_oracle_run() for _ in range(max(1, args.steps))]
+    v = sum(c["value"] for c in vals) / len(vals)
+    out = {"impl": "reference", "metric": DDM_METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": 0, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "DDM 160^3 Poisson (make_poisson_3D_DDM), CG + block-Jacobi D-ILU on 4^3 boxes, "
+                                  "rtol 1e-9, one process"},
+           "cpu_baseline": dict(vals[-1], value=v),
+           "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1101,7 +1246,7 @@ def main():
     ap.add_argument("--ilu-method", type=int, default=0)
     ap.add_argument("--workload", default="convdiff128",
                     choices=["convdiff128", "vardiff", "ddcg160", "ddgmres128", "poisson2d256", "aniso192",
-                             "banded4m"],
+                             "banded4m", "ddm160"],
                     help="vardiff: the learned-preconditioner comparison; ddcg160: the double-double CG "
                          "configuration of the reference's dd example; ddgmres128: the double-double GMRES "
                          "on the default line's matrix (none of them is the default line)")
@@ -1119,7 +1264,9 @@ def main():
     ap.add_argument("--target-train-rhs", type=int, default=2)
     ap.add_argument("--target-train-steps", type=int, default=400)
     args = ap.parse_args()
-    if args.impl == "reference" and args.workload in ("ddcg160", "ddgmres128"):
+    if args.workload == "ddm160":
+        run_reference_ddm(args) if args.impl == "reference" else run_ddm(args)
+    elif args.impl == "reference" and args.workload in ("ddcg160", "ddgmres128"):
         run_reference_dd(args)
     elif args.impl == "reference" and args.workload == "vardiff":
         print(json.dumps({"impl": "reference", "unavailable": "the learned preconditioner has no counterpart in "

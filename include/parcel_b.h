@@ -554,6 +554,10 @@ int parcel_b_ddgmres(const parcel_b_input* prm, const parcel_b_crs* A, const dou
  * prm->inner_precision = 1 it times the FP32 system of the mixed-precision path. */
 int parcel_b_bench_kernels(const parcel_b_input* prm, const parcel_b_crs* A, int reps,
                            double* ms_spmv, double* ms_precon);
+/* As parcel_b_bench_kernels for a DDM box: the renumbered system and its boxes as the
+ * block-Jacobi blocks, as parcel_b_solve_ddm builds them. */
+int parcel_b_bench_kernels_ddm(const parcel_b_input* prm, const parcel_b_ddm* A, int reps, double* ms_spmv,
+                               double* ms_precon);
 
 /* ---- one process's share of a row-distributed system ---------------------------------
  * The GPU side of the multi-process solve (parcel_b/dist.py), which mirrors the reference's

@@ -461,6 +461,21 @@ extern "C" int parcel_b_ddsolve_ddm(const parcel_b_input* prm, const parcel_b_dd
   return rc < 0 ? rc : rc2;
 }
 
+extern "C" int parcel_b_bench_kernels_ddm(const parcel_b_input* prm, const parcel_b_ddm* A, int reps,
+                                          double* ms_spmv, double* ms_precon) {
+  DdmCrs C;
+  parcel_b_input p;
+  const int rc = guarded([&]() -> int {
+    ensure_init();
+    p = ddm_input(prm);
+    ddm_build(A, p.precon_thblock, nullptr, C);
+    return 0;
+  });
+  if (rc < 0) return rc;
+  ScopedBlockStarts blocks(&C.starts);
+  return parcel_b_bench_kernels(&p, &C.crs, reps, ms_spmv, ms_precon);
+}
+
 // ---- drop-in shims (src/example/c2fortran_kernel.f90:2964-3691) --------------------------
 namespace {
 

@@ -152,6 +152,7 @@ SIGNATURES = {
     "parcel_b_ddsolve_ddm": (C.c_int, [C.POINTER(Input), C.POINTER(Ddm), P, C.c_int, C.c_int, C.c_int, C.c_int,
                                        P, P, P, P, P, IP, IP]),
     "parcel_b_ddm_order": (C.c_int, [C.POINTER(Ddm), C.c_int, I32P, I32P, I32P]),
+    "parcel_b_bench_kernels_ddm": (C.c_int, [C.POINTER(Input), C.POINTER(Ddm), C.c_int, DP, DP]),
     # DDM shims: n (padded cells), nnd, offset, diaA, the decomposition and the solver arguments
     "parcel_dcg_ddm_c_": (None, [IP, P, P, I32P] + _DDM_H + [IP]),
     "parcel_dbicgstab_ddm_c_": (None, [IP, P, P, I32P] + _DDM_H + [IP]),
