@@ -157,6 +157,7 @@ void ilu_build_plan(const HostCSR& A, const BlockSplit& blocks, IluPlan& P, int*
       ku[gl] = std::max(ku[gl], cU[i]);
     }
   P.lvl_start.assign(totlev, 0);
+  P.lvl_end.assign(totlev, 0);
   int cursor = 0, maxw = 0;
   for (int b = 0; b < nb; ++b)
     for (int l = 0; l < nlev[b]; ++l) {
@@ -164,6 +165,7 @@ void ilu_build_plan(const HostCSR& A, const BlockSplit& blocks, IluPlan& P, int*
       cursor = align4(cursor);
       P.lvl_start[gl] = cursor;
       cursor += width[gl];
+      P.lvl_end[gl] = cursor;
       maxw = std::max(maxw, width[gl]);
     }
   P.np = align4(cursor);
@@ -1055,6 +1057,110 @@ __global__ void __launch_bounds__(kIluThreads, 1) k_ilu_solve(IluSolveArgs<T> a)
   }
 }
 
+// ------------------------------------------------------------------ many small blocks
+// A block of a few dozen rows (the 4^3 boxes of a stencil-format matrix: 64 rows on 10
+// levels) gives the grouped sweep's one CTA per block too little work for its set-up and
+// its 20 dependent level steps; with tens of thousands of blocks the CTAs then run one after
+// another.  Here one warp sweeps one block: the rows of a level on the lanes (the levels are
+// contiguous in the iteration layout), __syncwarp between levels (it orders the warp's global
+// writes before the next level's reads).  The records sit in the iteration layout, K entries
+// per row: forward the strictly lower in-block couplings in increasing column, backward the
+// strictly upper ones (ILU(0) increasing, D-ILU decreasing column), so each row sums in the
+// order of the grouped sweep, with the same expressions.
+constexpr int kSmallMaxRows = 1024;   // largest block the warp sweep takes
+constexpr int kSmallThreads = 256;
+
+template <class T>
+__global__ void k_ilu_small_pack(int n, int nb, const int* __restrict__ blk_lo, const int* __restrict__ blk_hi,
+                                 const int* __restrict__ pos, const int* __restrict__ rp, const int* __restrict__ ci,
+                                 int rbase, int cbase, const double* __restrict__ vL, const double* __restrict__ vU,
+                                 const double* __restrict__ Dinv, int dilu, int K, int* __restrict__ cF,
+                                 T* __restrict__ vF, T* __restrict__ dF, int* __restrict__ cB, T* __restrict__ vB,
+                                 T* __restrict__ dB) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int a = 0, z = nb - 1;   // block of row i: the last b with blk_lo[b] <= i
+    while (a < z) {
+      const int mid = (a + z + 1) >> 1;
+      if (blk_lo[mid] <= i) a = mid; else z = mid - 1;
+    }
+    int ia, iz, idg;
+    inblock_range(rp, ci, rbase, cbase, i, blk_lo[a], blk_hi[a], &ia, &iz, &idg);
+    const int64_t p = pos[i];
+    int k = 0;
+    for (int j = ia; j < idg; ++j, ++k) {
+      cF[p * K + k] = pos[ci[j] - cbase];
+      vF[p * K + k] = (T)vL[j];
+    }
+    for (; k < K; ++k) { cF[p * K + k] = -1; vF[p * K + k] = T(0); }
+    dF[p] = dilu ? (T)Dinv[i] : T(1);
+    k = 0;
+    if (!dilu) {
+      for (int j = idg + 1; j < iz; ++j, ++k) {
+        cB[p * K + k] = pos[ci[j] - cbase];
+        vB[p * K + k] = (T)vU[j];
+      }
+      dB[p] = (T)(1.0 / vU[idg]);
+    } else {
+      for (int j = iz - 1; j > idg; --j, ++k) {
+        cB[p * K + k] = pos[ci[j] - cbase];
+        vB[p * K + k] = (T)vU[j];
+      }
+      dB[p] = (T)Dinv[i];
+    }
+    for (; k < K; ++k) { cB[p * K + k] = -1; vB[p * K + k] = T(0); }
+  }
+}
+
+// y and s are written and re-read across levels: no __restrict__ on them.
+template <class T, bool DILU, int K>
+__global__ void __launch_bounds__(kSmallThreads) k_ilu_small(int nb, const int* __restrict__ blvl,
+                                                             const int* __restrict__ lo, const int* __restrict__ hi,
+                                                             const int* __restrict__ cF, const T* __restrict__ vF,
+                                                             const T* __restrict__ dF, const int* __restrict__ cB,
+                                                             const T* __restrict__ vB, const T* __restrict__ dB,
+                                                             const T* __restrict__ r, T* y, T* s, const int* gate) {
+  if (gated(gate)) return;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += nwarps) {
+    const int l0 = blvl[b], l1 = blvl[b + 1];
+    for (int l = l0; l < l1; ++l) {
+      const int e = hi[l];
+      for (int p = lo[l] + lane; p < e; p += 32) {
+        int c[K];
+        T v[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) { c[k] = cF[(int64_t)p * K + k]; v[k] = vF[(int64_t)p * K + k]; }
+        T acc = r[p];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          if (c[k] >= 0) acc = acc - v[k] * y[c[k]];
+        y[p] = DILU ? dF[p] * acc : acc;
+      }
+      __syncwarp();
+    }
+    for (int l = l1 - 1; l >= l0; --l) {
+      const int e = hi[l];
+      for (int p = lo[l] + lane; p < e; p += 32) {
+        int c[K];
+        T v[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) { c[k] = cB[(int64_t)p * K + k]; v[k] = vB[(int64_t)p * K + k]; }
+        const T yp = y[p];
+        T acc = DILU ? T(0) : yp;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          if (c[k] >= 0) {
+            if (DILU) acc = acc + s[c[k]] * v[k];
+            else acc = acc - s[c[k]] * v[k];
+          }
+        s[p] = DILU ? yp - dB[p] * acc : acc * dB[p];
+      }
+      __syncwarp();
+    }
+  }
+}
+
 // ------------------------------------------------------------------ host side
 template <class T>
 int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
@@ -1239,6 +1345,29 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
         dp<unsigned char>(D.packF), dp<unsigned char>(D.packB));
   }
   PB_CUDA(cudaGetLastError());
+  // many small blocks: the warp-per-block records as well (the packed ones serve the
+  // accumulating apply)
+  int max_rows = 0;
+  for (int b = 0; b < P.nb; ++b) max_rows = std::max(max_rows, P.blk_hi[b] - P.blk_lo[b]);
+  D.small = max_rows <= kSmallMaxRows && P.nb >= 8 * num_sms() && D.K <= 8;
+  if (D.small) {
+    const size_t rk = (size_t)P.np * D.K;
+    D.s_cF.alloc(sizeof(int) * rk); D.s_vF.alloc(sizeof(T) * rk); D.s_dF.alloc(sizeof(T) * P.np);
+    D.s_cB.alloc(sizeof(int) * rk); D.s_vB.alloc(sizeof(T) * rk); D.s_dB.alloc(sizeof(T) * P.np);
+    const int totlev = (int)P.lvl_start.size();
+    D.s_blvl.alloc(sizeof(int) * (P.nb + 1));
+    D.s_lo.alloc(sizeof(int) * std::max(totlev, 1));
+    D.s_hi.alloc(sizeof(int) * std::max(totlev, 1));
+    h2d(D.s_blvl.p, P.blk_lvl.data(), sizeof(int) * (P.nb + 1));
+    h2d(D.s_lo.p, P.lvl_start.data(), sizeof(int) * totlev);
+    h2d(D.s_hi.p, P.lvl_end.data(), sizeof(int) * totlev);
+    const int g = (int)std::min<int64_t>(((int64_t)P.n + 255) / 256, 8LL * num_sms());
+    k_ilu_small_pack<T><<<std::max(g, 1), 256, 0, st>>>(
+        P.n, P.nb, dp<int>(blo), dp<int>(bhi), d_pos, A.rowptr, A.col, A.rbase, A.cbase, vL, vU,
+        D.dilu ? dp<double>(Di) : nullptr, D.dilu ? 1 : 0, D.K, dp<int>(D.s_cF), dp<T>(D.s_vF), dp<T>(D.s_dF),
+        dp<int>(D.s_cB), dp<T>(D.s_vB), dp<T>(D.s_dB));
+    PB_CUDA(cudaGetLastError());
+  }
   D.ytmp.alloc(sizeof(T) * (P.np + 4));
   PB_CUDA(cudaMemsetAsync(D.ytmp.p, 0, sizeof(T) * (P.np + 4), st));
   D.err.alloc(sizeof(int));
@@ -1271,8 +1400,30 @@ static void launch_grp(const IluDev<T>& D, const GrpArgs<T>& a, cudaStream_t st)
   kern<<<D.nb, NC + 32, D.smem_bytes, st>>>(a);
 }
 
+template <class T, bool DILU, int K>
+static void launch_small(const IluDev<T>& D, const T* r, T* s, const int* gate, cudaStream_t st) {
+  const int grid = (int)std::min<int64_t>(((int64_t)D.nb * 32 + kSmallThreads - 1) / kSmallThreads,
+                                          16LL * num_sms());
+  k_ilu_small<T, DILU, K><<<grid, kSmallThreads, 0, st>>>(
+      D.nb, dp<int>(D.s_blvl), dp<int>(D.s_lo), dp<int>(D.s_hi), dp<int>(D.s_cF), dp<T>(D.s_vF), dp<T>(D.s_dF),
+      dp<int>(D.s_cB), dp<T>(D.s_vB), dp<T>(D.s_dB), r, dp<T>(D.ytmp), s, gate);
+}
+
 template <class T>
 void ilu_apply(const IluDev<T>& D, const T* r, T* s, T* accum, const int* gate, cudaStream_t st) {
+  if (D.small && !accum) {
+#define SMALL(K_)                                                                                  \
+  case K_:                                                                                         \
+    if (D.dilu) launch_small<T, true, K_>(D, r, s, gate, st); else launch_small<T, false, K_>(D, r, s, gate, st); \
+    break;
+    switch (D.K) {
+      SMALL(1) SMALL(2) SMALL(3) SMALL(4) SMALL(6) SMALL(8)
+      default: PB_CHECK(false, PARCEL_B_E_ARG, "unsupported coupling count %d", D.K);
+    }
+#undef SMALL
+    PB_CUDA(cudaGetLastError());
+    return;
+  }
   if (D.grp && !accum) {
     GrpArgs<T> g;
     g.tabF = dp<GrpDesc>(D.tabF);

@@ -85,6 +85,7 @@ struct IluPlan {
   std::vector<int> blk_chunk;   // nb + 1
   std::vector<int> blk_lo, blk_hi;   // natural row ranges [lo, hi)
   std::vector<int> lvl_start;   // per block-level (global index) permuted start
+  std::vector<int> lvl_end;     // per block-level permuted end (start + width)
   std::vector<int> blk_lvl;     // nb + 1 index into lvl_start
 };
 
@@ -110,6 +111,12 @@ struct IluDev {
   int64_t packF_bytes = 0, packB_bytes = 0;
   DBuf ytmp;        // forward result, np + 1 entries
   DBuf err;         // int error flag
+  // Many small blocks (k_ilu_small): one warp per block, per-row records in the iteration
+  // layout: K coupled entries (permuted column or -1, value) and a diagonal factor for each
+  // sweep, forward (F) and backward (B).
+  bool small = false;
+  DBuf s_blvl, s_lo, s_hi;                  // block -> first level (nb + 1); level -> [lo, hi)
+  DBuf s_cF, s_vF, s_dF, s_cB, s_vB, s_dB;
 };
 
 // Sparsity structure of the natural matrix on the host (for the wavefront plan).

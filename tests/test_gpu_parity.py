@@ -230,6 +230,30 @@ def test_wide_levels_precon_matches_oracle(blocks, ilu):
     assert _rel(s, s_ref) < 1e-11
 
 
+@pytest.mark.parametrize("ilu", [0, 1, 2])
+@pytest.mark.parametrize("blocks", [2000, 5000])
+def test_many_small_blocks_precon_matches_oracle(blocks, ilu):
+    """Thousands of blocks of a few rows each (more than eight per SM, at most 1024 rows)
+    take the warp-per-block sweep; uneven blocks (divide_region) and a nonsymmetric matrix."""
+    A = problems.convdiff3d_upwind(24)
+    pre = dict(ipreflag=2, ILU_method=ilu, precon_thblock=blocks)
+    r = np.random.default_rng(4).standard_normal(A.n)
+    s_ref = oracle.precon_apply(A, r, **pre)
+    s = np.zeros(A.n)
+    p = _lib.new_input(**pre)
+    rc = _lib.load().parcel_b_precon_apply(C.byref(p), C.byref(api.crs_struct(A)), r.ctypes.data, s.ctypes.data)
+    assert rc == 0, _lib.last_error()
+    assert _rel(s, s_ref) < 1e-11
+    # and a solve through it
+    b = problems.rhs_normal(A.n, 6)
+    kw = dict(solver=3, itrmax=2000, rtolmax=1e-10, GMRES_m=20, GMRES_GSflag=1, **pre)
+    (xo, ho, no, io), res = _solve_both(A, b, **kw)
+    assert io == 0 and res["iret"] == 0 and abs(res["niter"] - no) <= 2
+    k = min(len(ho), len(res["reshistory"]))
+    m = ho[:k] > 1e-8
+    assert np.all(np.abs(res["reshistory"][:k][m] - ho[:k][m]) / ho[:k][m] < 1e-6)
+
+
 def test_diagonal_copy_spmv_path_matches_oracle():
     """Point Jacobi keeps the natural layout, where a stencil matrix's product runs on its
     diagonal copy (statistics: spmv_diagonals); CG and GMRES histories against the oracle at
