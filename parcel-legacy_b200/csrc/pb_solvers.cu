@@ -174,6 +174,8 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
     cudaEvent_t ev[kPieces] = {};
     std::vector<int> piece_of(nb, 0);
     std::atomic<int> copy_failed{0};
+    std::atomic<int> piece_done[kPieces];
+    for (auto& d : piece_done) d.store(0);
     std::function<void(int)> ready;
     auto destroy_events = [&] {
       for (auto& e : ev)
@@ -200,9 +202,13 @@ void build_system(const Options& o, const parcel_b_crs& A, bool dev, System<T>& 
           PB_CUDA(e);
         }
       }
-      // called from the plan's parallel loop: no exception may leave it
+      // called from the plan's parallel loop: no exception may leave it.  A piece is waited
+      // for once (with tens of thousands of blocks a wait per block costs more than the plan).
       ready = [&](int b) {
-        if (cudaEventSynchronize(ev[piece_of[b]]) != cudaSuccess) copy_failed = 1;
+        const int k = piece_of[b];
+        if (piece_done[k].load(std::memory_order_acquire)) return;
+        if (cudaEventSynchronize(ev[k]) != cudaSuccess) copy_failed = 1;
+        piece_done[k].store(1, std::memory_order_release);
       };
     }
     HostCSR H;
