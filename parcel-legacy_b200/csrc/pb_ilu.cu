@@ -1111,52 +1111,107 @@ __global__ void k_ilu_small_pack(int n, int nb, const int* __restrict__ blk_lo, 
   }
 }
 
-// y and s are written and re-read across levels: no __restrict__ on them.
-template <class T, bool DILU, int K>
-__global__ void __launch_bounds__(kSmallThreads) k_ilu_small(int nb, const int* __restrict__ blvl,
+// One row's record of one sweep.
+template <class T, int K>
+struct SmallRec {
+  int p;        // permuted row, -1: none
+  int c[K];
+  T v[K];
+  T x, d;       // r (forward) or y (backward), and the diagonal factor
+};
+
+template <class T, int K>
+__device__ __forceinline__ void small_load(SmallRec<T, K>& o, int p, const int* __restrict__ cc,
+                                           const T* __restrict__ vv, const T* __restrict__ dd, const T* x) {
+  o.p = p;
+  if (p < 0) return;
+#pragma unroll
+  for (int k = 0; k < K; ++k) { o.c[k] = cc[(int64_t)p * K + k]; o.v[k] = vv[(int64_t)p * K + k]; }
+  o.x = x[p];
+  o.d = dd[p];
+}
+
+// LPB lanes per block, 32 / LPB blocks per warp; y and s are written and re-read across
+// levels (no __restrict__ on them).  Each lane loads its next level's record before it
+// gathers the current level's coupled values, so a level costs one dependent round trip.
+template <class T, bool DILU, int K, int LPB>
+__global__ void __launch_bounds__(kSmallThreads, K <= 3 ? 3 : (K <= 4 ? 2 : 1)) k_ilu_small(int nb, const int* __restrict__ blvl,
                                                              const int* __restrict__ lo, const int* __restrict__ hi,
                                                              const int* __restrict__ cF, const T* __restrict__ vF,
                                                              const T* __restrict__ dF, const int* __restrict__ cB,
                                                              const T* __restrict__ vB, const T* __restrict__ dB,
                                                              const T* __restrict__ r, T* y, T* s, const int* gate) {
   if (gated(gate)) return;
-  const int lane = threadIdx.x & 31;
+  constexpr int BPW = 32 / LPB;
+  const int lane = threadIdx.x & 31, sub = lane / LPB, li = lane % LPB;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += nwarps) {
-    const int l0 = blvl[b], l1 = blvl[b + 1];
-    for (int l = l0; l < l1; ++l) {
-      const int e = hi[l];
-      for (int p = lo[l] + lane; p < e; p += 32) {
-        int c[K];
-        T v[K];
+  const int ngroups = (nb + BPW - 1) / BPW;
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < ngroups; w += nwarps) {
+    const int b = w * BPW + sub;
+    const int l0 = b < nb ? blvl[b] : 0, l1 = b < nb ? blvl[b + 1] : 0;
+    int nlev = l1 - l0, maxlev = nlev;
 #pragma unroll
-        for (int k = 0; k < K; ++k) { c[k] = cF[(int64_t)p * K + k]; v[k] = vF[(int64_t)p * K + k]; }
-        T acc = r[p];
+    for (int o = 16; o > 0; o >>= 1) maxlev = max(maxlev, __shfl_xor_sync(0xffffffffu, maxlev, o));
+    auto first_row = [&](int t, bool fwd) -> int {   // this lane's first row of step t, or -1
+      if (t >= nlev) return -1;
+      const int l = fwd ? l0 + t : l1 - 1 - t;
+      const int p = lo[l] + li;
+      return p < hi[l] ? p : -1;
+    };
+    // forward
+    SmallRec<T, K> cur, nxt;
+    small_load<T, K>(cur, first_row(0, true), cF, vF, dF, r);
+    for (int t = 0; t < maxlev; ++t) {
+      small_load<T, K>(nxt, first_row(t + 1, true), cF, vF, dF, r);
+      if (cur.p >= 0) {
+        T acc = cur.x;
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          if (c[k] >= 0) acc = acc - v[k] * y[c[k]];
-        y[p] = DILU ? dF[p] * acc : acc;
+          if (cur.c[k] >= 0) acc = acc - cur.v[k] * y[cur.c[k]];
+        y[cur.p] = DILU ? cur.d * acc : acc;
+        const int l = l0 + t;
+        for (int p = cur.p + LPB; p < hi[l]; p += LPB) {   // levels wider than LPB
+          SmallRec<T, K> o;
+          small_load<T, K>(o, p, cF, vF, dF, r);
+          T a2 = o.x;
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            if (o.c[k] >= 0) a2 = a2 - o.v[k] * y[o.c[k]];
+          y[p] = DILU ? o.d * a2 : a2;
+        }
       }
       __syncwarp();
+      cur = nxt;
     }
-    for (int l = l1 - 1; l >= l0; --l) {
-      const int e = hi[l];
-      for (int p = lo[l] + lane; p < e; p += 32) {
-        int c[K];
-        T v[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) { c[k] = cB[(int64_t)p * K + k]; v[k] = vB[(int64_t)p * K + k]; }
-        const T yp = y[p];
-        T acc = DILU ? T(0) : yp;
+    // backward (the forward result y is the input)
+    small_load<T, K>(cur, first_row(0, false), cB, vB, dB, y);
+    for (int t = 0; t < maxlev; ++t) {
+      small_load<T, K>(nxt, first_row(t + 1, false), cB, vB, dB, y);
+      if (cur.p >= 0) {
+        T acc = DILU ? T(0) : cur.x;
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          if (c[k] >= 0) {
-            if (DILU) acc = acc + s[c[k]] * v[k];
-            else acc = acc - s[c[k]] * v[k];
+          if (cur.c[k] >= 0) {
+            if (DILU) acc = acc + s[cur.c[k]] * cur.v[k];
+            else acc = acc - s[cur.c[k]] * cur.v[k];
           }
-        s[p] = DILU ? yp - dB[p] * acc : acc * dB[p];
+        s[cur.p] = DILU ? cur.x - cur.d * acc : acc * cur.d;
+        const int l = l1 - 1 - t;
+        for (int p = cur.p + LPB; p < hi[l]; p += LPB) {
+          SmallRec<T, K> o;
+          small_load<T, K>(o, p, cB, vB, dB, y);
+          T a2 = DILU ? T(0) : o.x;
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            if (o.c[k] >= 0) {
+              if (DILU) a2 = a2 + s[o.c[k]] * o.v[k];
+              else a2 = a2 - s[o.c[k]] * o.v[k];
+            }
+          s[p] = DILU ? o.x - o.d * a2 : a2 * o.d;
+        }
       }
       __syncwarp();
+      cur = nxt;
     }
   }
 }
@@ -1351,6 +1406,9 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   for (int b = 0; b < P.nb; ++b) max_rows = std::max(max_rows, P.blk_hi[b] - P.blk_lo[b]);
   D.small = max_rows <= kSmallMaxRows && P.nb >= 8 * num_sms() && D.K <= 8;
   if (D.small) {
+    // lanes per block: the widest level, rounded up to 8, 16 or 32 (wider levels take
+    // several rows per lane)
+    D.s_lpb = maxw <= 8 ? 8 : (maxw <= 16 ? 16 : 32);
     const size_t rk = (size_t)P.np * D.K;
     D.s_cF.alloc(sizeof(int) * rk); D.s_vF.alloc(sizeof(T) * rk); D.s_dF.alloc(sizeof(T) * P.np);
     D.s_cB.alloc(sizeof(int) * rk); D.s_vB.alloc(sizeof(T) * rk); D.s_dB.alloc(sizeof(T) * P.np);
@@ -1400,13 +1458,20 @@ static void launch_grp(const IluDev<T>& D, const GrpArgs<T>& a, cudaStream_t st)
   kern<<<D.nb, NC + 32, D.smem_bytes, st>>>(a);
 }
 
-template <class T, bool DILU, int K>
-static void launch_small(const IluDev<T>& D, const T* r, T* s, const int* gate, cudaStream_t st) {
-  const int grid = (int)std::min<int64_t>(((int64_t)D.nb * 32 + kSmallThreads - 1) / kSmallThreads,
-                                          16LL * num_sms());
-  k_ilu_small<T, DILU, K><<<grid, kSmallThreads, 0, st>>>(
+template <class T, bool DILU, int K, int LPB>
+static void launch_small_lpb(const IluDev<T>& D, const T* r, T* s, const int* gate, cudaStream_t st) {
+  const int64_t warps = ((int64_t)D.nb + 32 / LPB - 1) / (32 / LPB);
+  const int grid = (int)std::min<int64_t>((warps * 32 + kSmallThreads - 1) / kSmallThreads, 16LL * num_sms());
+  k_ilu_small<T, DILU, K, LPB><<<grid, kSmallThreads, 0, st>>>(
       D.nb, dp<int>(D.s_blvl), dp<int>(D.s_lo), dp<int>(D.s_hi), dp<int>(D.s_cF), dp<T>(D.s_vF), dp<T>(D.s_dF),
       dp<int>(D.s_cB), dp<T>(D.s_vB), dp<T>(D.s_dB), r, dp<T>(D.ytmp), s, gate);
+}
+
+template <class T, bool DILU, int K>
+static void launch_small(const IluDev<T>& D, const T* r, T* s, const int* gate, cudaStream_t st) {
+  if (D.s_lpb == 8) launch_small_lpb<T, DILU, K, 8>(D, r, s, gate, st);
+  else if (D.s_lpb == 16) launch_small_lpb<T, DILU, K, 16>(D, r, s, gate, st);
+  else launch_small_lpb<T, DILU, K, 32>(D, r, s, gate, st);
 }
 
 template <class T>

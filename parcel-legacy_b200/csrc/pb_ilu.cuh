@@ -115,6 +115,7 @@ struct IluDev {
   // layout: K coupled entries (permuted column or -1, value) and a diagonal factor for each
   // sweep, forward (F) and backward (B).
   bool small = false;
+  int s_lpb = 32;                           // lanes per block (8, 16 or 32)
   DBuf s_blvl, s_lo, s_hi;                  // block -> first level (nb + 1); level -> [lo, hi)
   DBuf s_cF, s_vF, s_dF, s_cB, s_vB, s_dB;
 };
