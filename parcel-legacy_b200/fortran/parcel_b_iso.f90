@@ -849,3 +849,286 @@ contains
          CAGMRES_basis, CAGMRES_QRflag, iret)
   end subroutine parcel_dcagmres_dev
 end module PARCEL_wrapper
+
+! Module ddm_wrapper: the DDM stencil-format solvers under the argument lists of the
+! reference's CPU build (src/src_DDM/ddm_kernel.f90:1906-3279, used by
+! src/example/main_ddm.f90 through `use ddm_wrapper`).  x and b are the process's padded box
+! (nrow = m cells); the block-Jacobi D-ILU runs on precon_thblock slabs along div_direc_th,
+! as the CPU build's OpenMP threads cut them.  One process: ndiv_grids all 1 and no
+! neighbour ranks (a box split over processes runs through the Python package's
+! parcel_b.ddm on torch.distributed); anything else returns iret = -5.
+module ddm_wrapper
+  use iso_c_binding
+  implicit none
+  private
+  public :: parcel_dcg_ddm, parcel_dbicgstab_ddm, parcel_dgmres_ddm, parcel_dcagmres_ddm, parcel_ddcg_ddm, parcel_ddbicgstab_ddm, parcel_ddgmres_ddm
+
+  interface
+     subroutine c_parcel_dcg_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, &
+          num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, &
+          ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, &
+          iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, iret) &
+          bind(c, name="parcel_dcg_ddm_c_")
+       import :: c_int, c_int32_t, c_double
+       integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+            ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+            independ_nvec, nBlock, iret
+       integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+       integer(c_int32_t) :: nrow
+       integer(c_int32_t) :: ioff_dia(*)
+       real(c_double) :: x(*), b(*), val_dia(*), reshistory(*)
+       real(c_double) :: rtolmax
+     end subroutine c_parcel_dcg_ddm
+     subroutine c_parcel_dbicgstab_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, &
+          num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, &
+          ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, &
+          iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, iret) &
+          bind(c, name="parcel_dbicgstab_ddm_c_")
+       import :: c_int, c_int32_t, c_double
+       integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+            ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+            independ_nvec, nBlock, iret
+       integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+       integer(c_int32_t) :: nrow
+       integer(c_int32_t) :: ioff_dia(*)
+       real(c_double) :: x(*), b(*), val_dia(*), reshistory(*)
+       real(c_double) :: rtolmax
+     end subroutine c_parcel_dbicgstab_ddm
+     subroutine c_parcel_dgmres_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, &
+          num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, &
+          ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, &
+          iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, GMRES_m, &
+          GMRES_GSflag, iret) &
+          bind(c, name="parcel_dgmres_ddm_c_")
+       import :: c_int, c_int32_t, c_double
+       integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+            ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+            independ_nvec, nBlock, GMRES_m, GMRES_GSflag, iret
+       integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+       integer(c_int32_t) :: nrow
+       integer(c_int32_t) :: ioff_dia(*)
+       real(c_double) :: x(*), b(*), val_dia(*), reshistory(*)
+       real(c_double) :: rtolmax
+     end subroutine c_parcel_dgmres_ddm
+     subroutine c_parcel_dcagmres_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, &
+          num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, &
+          ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, &
+          iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, CAGMRES_sstep, &
+          CAGMRES_tstep, CAGMRES_basis, CAGMRES_QRflag, iret) &
+          bind(c, name="parcel_dcagmres_ddm_c_")
+       import :: c_int, c_int32_t, c_double
+       integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+            ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+            independ_nvec, nBlock, CAGMRES_sstep, CAGMRES_tstep, CAGMRES_basis, &
+            CAGMRES_QRflag, iret
+       integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+       integer(c_int32_t) :: nrow
+       integer(c_int32_t) :: ioff_dia(*)
+       real(c_double) :: x(*), b(*), val_dia(*), reshistory(*)
+       real(c_double) :: rtolmax
+     end subroutine c_parcel_dcagmres_ddm
+     subroutine c_parcel_ddcg_ddm(icomm, x, x_lo, b, b_lo, nrow, nnd, ioff_dia, val_dia, &
+          val_dia_lo, num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, &
+          num_grids, ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, &
+          reshistory, iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, &
+          PRECISION_A, PRECISION_b, PRECISION_x, PRECISION_PRECONDITION, iret) &
+          bind(c, name="parcel_ddcg_ddm_c_")
+       import :: c_int, c_int32_t, c_double
+       integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+            ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+            independ_nvec, nBlock, PRECISION_A, PRECISION_b, PRECISION_x, &
+            PRECISION_PRECONDITION, iret
+       integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+       integer(c_int32_t) :: nrow
+       integer(c_int32_t) :: ioff_dia(*)
+       real(c_double) :: x(*), b(*), val_dia(*), reshistory(*), x_lo(*), b_lo(*), &
+            val_dia_lo(*)
+       real(c_double) :: rtolmax
+     end subroutine c_parcel_ddcg_ddm
+     subroutine c_parcel_ddbicgstab_ddm(icomm, x, x_lo, b, b_lo, nrow, nnd, ioff_dia, &
+          val_dia, val_dia_lo, num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, &
+          ndiv_grids, num_grids, ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, &
+          rtolmax, reshistory, iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, &
+          PRECISION_A, PRECISION_b, PRECISION_x, PRECISION_PRECONDITION, iret) &
+          bind(c, name="parcel_ddbicgstab_ddm_c_")
+       import :: c_int, c_int32_t, c_double
+       integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+            ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+            independ_nvec, nBlock, PRECISION_A, PRECISION_b, PRECISION_x, &
+            PRECISION_PRECONDITION, iret
+       integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+       integer(c_int32_t) :: nrow
+       integer(c_int32_t) :: ioff_dia(*)
+       real(c_double) :: x(*), b(*), val_dia(*), reshistory(*), x_lo(*), b_lo(*), &
+            val_dia_lo(*)
+       real(c_double) :: rtolmax
+     end subroutine c_parcel_ddbicgstab_ddm
+     subroutine c_parcel_ddgmres_ddm(icomm, x, x_lo, b, b_lo, nrow, nnd, ioff_dia, val_dia, &
+          val_dia_lo, num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, &
+          num_grids, ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, &
+          reshistory, iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, GMRES_m, &
+          GMRES_GSflag, PRECISION_A, PRECISION_b, PRECISION_x, PRECISION_PRECONDITION, iret) &
+          bind(c, name="parcel_ddgmres_ddm_c_")
+       import :: c_int, c_int32_t, c_double
+       integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+            ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+            independ_nvec, nBlock, GMRES_m, GMRES_GSflag, PRECISION_A, PRECISION_b, &
+            PRECISION_x, PRECISION_PRECONDITION, iret
+       integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+       integer(c_int32_t) :: nrow
+       integer(c_int32_t) :: ioff_dia(*)
+       real(c_double) :: x(*), b(*), val_dia(*), reshistory(*), x_lo(*), b_lo(*), &
+            val_dia_lo(*)
+       real(c_double) :: rtolmax
+     end subroutine c_parcel_ddgmres_ddm
+  end interface
+
+contains
+
+  ! parcel_dcg_ddm (src/src_DDM/ddm_kernel.f90:2893-2986), CPU build: host arrays, one process
+  subroutine parcel_dcg_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, num_neighbor_ranks, &
+       neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, ioff_grids, div_direc_th, &
+       ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag, precon_thblock, &
+       Neuman_itr, independ_nvec, nBlock, iret)
+    integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+         ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+         independ_nvec, nBlock, iret
+    integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+    integer(c_int32_t) :: nrow
+    integer(c_int32_t) :: ioff_dia(*)
+    real(c_double) :: x(*), b(*), val_dia(*), reshistory(*)
+    real(c_double) :: rtolmax
+    call c_parcel_dcg_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, num_neighbor_ranks, &
+         neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, ioff_grids, &
+         div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag, &
+         precon_thblock, Neuman_itr, independ_nvec, nBlock, iret)
+  end subroutine parcel_dcg_ddm
+
+  ! parcel_dbicgstab_ddm (src/src_DDM/ddm_kernel.f90:2988-3080), CPU build: host arrays, one process
+  subroutine parcel_dbicgstab_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, &
+       num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, &
+       ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, &
+       iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, iret)
+    integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+         ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+         independ_nvec, nBlock, iret
+    integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+    integer(c_int32_t) :: nrow
+    integer(c_int32_t) :: ioff_dia(*)
+    real(c_double) :: x(*), b(*), val_dia(*), reshistory(*)
+    real(c_double) :: rtolmax
+    call c_parcel_dbicgstab_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, &
+         num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, &
+         ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, &
+         iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, iret)
+  end subroutine parcel_dbicgstab_ddm
+
+  ! parcel_dgmres_ddm (src/src_DDM/ddm_kernel.f90:3082-3178), CPU build: host arrays, one process
+  subroutine parcel_dgmres_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, &
+       num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, &
+       ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, &
+       iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, GMRES_m, GMRES_GSflag, &
+       iret)
+    integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+         ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+         independ_nvec, nBlock, GMRES_m, GMRES_GSflag, iret
+    integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+    integer(c_int32_t) :: nrow
+    integer(c_int32_t) :: ioff_dia(*)
+    real(c_double) :: x(*), b(*), val_dia(*), reshistory(*)
+    real(c_double) :: rtolmax
+    call c_parcel_dgmres_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, num_neighbor_ranks, &
+         neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, ioff_grids, &
+         div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, iovlflag, &
+         precon_thblock, Neuman_itr, independ_nvec, nBlock, GMRES_m, GMRES_GSflag, iret)
+  end subroutine parcel_dgmres_ddm
+
+  ! parcel_dcagmres_ddm (src/src_DDM/ddm_kernel.f90:3180-3279), CPU build: host arrays, one process
+  subroutine parcel_dcagmres_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, &
+       num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, &
+       ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, &
+       iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, CAGMRES_sstep, &
+       CAGMRES_tstep, CAGMRES_basis, CAGMRES_QRflag, iret)
+    integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+         ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+         independ_nvec, nBlock, CAGMRES_sstep, CAGMRES_tstep, CAGMRES_basis, CAGMRES_QRflag, &
+         iret
+    integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+    integer(c_int32_t) :: nrow
+    integer(c_int32_t) :: ioff_dia(*)
+    real(c_double) :: x(*), b(*), val_dia(*), reshistory(*)
+    real(c_double) :: rtolmax
+    call c_parcel_dcagmres_ddm(icomm, x, b, nrow, nnd, ioff_dia, val_dia, &
+         num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, num_grids, &
+         ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory, &
+         iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, CAGMRES_sstep, &
+         CAGMRES_tstep, CAGMRES_basis, CAGMRES_QRflag, iret)
+  end subroutine parcel_dcagmres_ddm
+
+  ! parcel_ddcg_ddm (src/src_DDM/ddm_kernel.f90:1906-2023), CPU build: host arrays, one process
+  subroutine parcel_ddcg_ddm(icomm, x, x_lo, b, b_lo, nrow, nnd, ioff_dia, val_dia, &
+       val_dia_lo, num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, &
+       num_grids, ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, &
+       reshistory, iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, PRECISION_A, &
+       PRECISION_b, PRECISION_x, PRECISION_PRECONDITION, iret)
+    integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+         ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+         independ_nvec, nBlock, PRECISION_A, PRECISION_b, PRECISION_x, &
+         PRECISION_PRECONDITION, iret
+    integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+    integer(c_int32_t) :: nrow
+    integer(c_int32_t) :: ioff_dia(*)
+    real(c_double) :: x(*), b(*), val_dia(*), reshistory(*), x_lo(*), b_lo(*), val_dia_lo(*)
+    real(c_double) :: rtolmax
+    call c_parcel_ddcg_ddm(icomm, x, x_lo, b, b_lo, nrow, nnd, ioff_dia, val_dia, &
+         val_dia_lo, num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, &
+         num_grids, ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, &
+         reshistory, iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, &
+         PRECISION_A, PRECISION_b, PRECISION_x, PRECISION_PRECONDITION, iret)
+  end subroutine parcel_ddcg_ddm
+
+  ! parcel_ddbicgstab_ddm (src/src_DDM/ddm_kernel.f90:2025-2141), CPU build: host arrays, one process
+  subroutine parcel_ddbicgstab_ddm(icomm, x, x_lo, b, b_lo, nrow, nnd, ioff_dia, val_dia, &
+       val_dia_lo, num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, &
+       num_grids, ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, &
+       reshistory, iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, PRECISION_A, &
+       PRECISION_b, PRECISION_x, PRECISION_PRECONDITION, iret)
+    integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+         ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+         independ_nvec, nBlock, PRECISION_A, PRECISION_b, PRECISION_x, &
+         PRECISION_PRECONDITION, iret
+    integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+    integer(c_int32_t) :: nrow
+    integer(c_int32_t) :: ioff_dia(*)
+    real(c_double) :: x(*), b(*), val_dia(*), reshistory(*), x_lo(*), b_lo(*), val_dia_lo(*)
+    real(c_double) :: rtolmax
+    call c_parcel_ddbicgstab_ddm(icomm, x, x_lo, b, b_lo, nrow, nnd, ioff_dia, val_dia, &
+         val_dia_lo, num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, &
+         num_grids, ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, &
+         reshistory, iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, &
+         PRECISION_A, PRECISION_b, PRECISION_x, PRECISION_PRECONDITION, iret)
+  end subroutine parcel_ddbicgstab_ddm
+
+  ! parcel_ddgmres_ddm (src/src_DDM/ddm_kernel.f90:2143-2263), CPU build: host arrays, one process
+  subroutine parcel_ddgmres_ddm(icomm, x, x_lo, b, b_lo, nrow, nnd, ioff_dia, val_dia, &
+       val_dia_lo, num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, &
+       num_grids, ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, &
+       reshistory, iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, GMRES_m, &
+       GMRES_GSflag, PRECISION_A, PRECISION_b, PRECISION_x, PRECISION_PRECONDITION, iret)
+    integer(c_int) :: icomm, nnd, num_neighbor_ranks, margin, ncomp_grids, div_direc_th, &
+         ipreflag, addL, iflagAS, itrmax, iovlflag, precon_thblock, Neuman_itr, &
+         independ_nvec, nBlock, GMRES_m, GMRES_GSflag, PRECISION_A, PRECISION_b, &
+         PRECISION_x, PRECISION_PRECONDITION, iret
+    integer(c_int) :: ioff_grids(*), ndiv_grids(*), neighbor_ranks(*), num_grids(*)
+    integer(c_int32_t) :: nrow
+    integer(c_int32_t) :: ioff_dia(*)
+    real(c_double) :: x(*), b(*), val_dia(*), reshistory(*), x_lo(*), b_lo(*), val_dia_lo(*)
+    real(c_double) :: rtolmax
+    call c_parcel_ddgmres_ddm(icomm, x, x_lo, b, b_lo, nrow, nnd, ioff_dia, val_dia, &
+         val_dia_lo, num_neighbor_ranks, neighbor_ranks, margin, ncomp_grids, ndiv_grids, &
+         num_grids, ioff_grids, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, &
+         reshistory, iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, GMRES_m, &
+         GMRES_GSflag, PRECISION_A, PRECISION_b, PRECISION_x, PRECISION_PRECONDITION, iret)
+  end subroutine parcel_ddgmres_ddm
+
+end module ddm_wrapper

@@ -225,3 +225,16 @@ def test_python_api_rejects_mistyped_arrays_before_calling_the_library():
         api.ddcg(A, b, val_lo=np.zeros(A.nnz + 1))
     with pytest.raises(TypeError, match="b_lo must be float64"):
         api.ddgmres(A, b, b_lo=np.zeros(A.n, dtype=np.float32))
+
+
+def test_fortran_ddm_wrapper_module_exports_the_reference_names():
+    """src/example/main_ddm.f90 uses module ddm_wrapper's parcel_d*_ddm routines."""
+    src = _fortran_source()
+    m = re.search(r"module ddm_wrapper(.*?)end module ddm_wrapper", src, flags=re.S)
+    assert m
+    public = re.search(r"public\s*::\s*([^\n]*)", m.group(1)).group(1)
+    names = {n.strip() for n in public.split(",")}
+    assert names == {"parcel_dcg_ddm", "parcel_dbicgstab_ddm", "parcel_dgmres_ddm", "parcel_dcagmres_ddm",
+                     "parcel_ddcg_ddm", "parcel_ddbicgstab_ddm", "parcel_ddgmres_ddm"}
+    for n in names:
+        assert re.search(r"subroutine %s\s*\(" % n, m.group(1)) and re.search(r"call c_%s\s*\(" % n, m.group(1))
