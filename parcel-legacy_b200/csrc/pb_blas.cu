@@ -65,7 +65,7 @@ __global__ void k_lincomb(int64_t n, T* __restrict__ out, const T* __restrict__ 
 // Same as k_lincomb, fused with up to three dot products of the result or inputs.
 // dot pairs select from {0: out, 1: x0, 2: x1, 3: x2, 4: d0, 5: d1}.
 template <class T, int ND>
-__global__ void __launch_bounds__(kRedThreads) k_lincomb_dot(int64_t n, T* __restrict__ out,
+__global__ void __launch_bounds__(kRedThreads, 4) k_lincomb_dot(int64_t n, T* __restrict__ out,
                                                              const T* __restrict__ x0,
                                                              const T* __restrict__ x1,
                                                              const T* __restrict__ x2, Coef c0,
@@ -77,10 +77,14 @@ __global__ void __launch_bounds__(kRedThreads) k_lincomb_dot(int64_t n, T* __res
   double acc[ND > 0 ? ND : 1];
 #pragma unroll
   for (int k = 0; k < ND; ++k) acc[k] = 0.0;
-  GRID_LOOP_U(i0, st, n) {
-    T s0[kU], s1[kU], s2[kU], s4[kU], s5[kU];
+  // three elements per thread and step (a thread still visits its elements in increasing
+  // order): four CTAs of 256 threads per SM then fit the registers without spilling
+  constexpr int kUD = 3;
+  const int64_t st = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += kUD * st) {
+    T s0[kUD], s1[kUD], s2[kUD], s4[kUD], s5[kUD];
 #pragma unroll
-    for (int u = 0; u < kU; ++u) {
+    for (int u = 0; u < kUD; ++u) {
       const int64_t i = i0 + u * st;
       const bool ok = i < n;
       s0[u] = (ok && x0) ? x0[i] : T(0);
@@ -90,7 +94,7 @@ __global__ void __launch_bounds__(kRedThreads) k_lincomb_dot(int64_t n, T* __res
       s5[u] = (ok && d1) ? d1[i] : T(0);
     }
 #pragma unroll
-    for (int u = 0; u < kU; ++u) {
+    for (int u = 0; u < kUD; ++u) {
       const int64_t i = i0 + u * st;
       if (i >= n) continue;
       T v = T(0);
@@ -100,9 +104,14 @@ __global__ void __launch_bounds__(kRedThreads) k_lincomb_dot(int64_t n, T* __res
         if (x2) v = v + a2 * s2[u];
         out[i] = v;
       }
-      T src[6] = {v, s0[u], s1[u], s2[u], s4[u], s5[u]};
+      // operand s of a dot: 0 the result, 1-3 the summands, 4-5 the extra vectors (a
+      // select chain on the uniform selector keeps the operands in registers; an array
+      // indexed by it would live in local memory)
+      auto pick = [&](int sidx) -> T {
+        return sidx == 0 ? v : sidx == 1 ? s0[u] : sidx == 2 ? s1[u] : sidx == 3 ? s2[u] : sidx == 4 ? s4[u] : s5[u];
+      };
 #pragma unroll
-      for (int k = 0; k < ND; ++k) acc[k] += (double)(src[sel.a[k]] * src[sel.b[k]]);
+      for (int k = 0; k < ND; ++k) acc[k] += (double)(pick(sel.a[k]) * pick(sel.b[k]));
     }
   }
   reduce_and_finish<ND>(acc, red);
