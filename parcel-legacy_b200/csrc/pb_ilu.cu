@@ -1111,36 +1111,55 @@ __global__ void k_ilu_small_pack(int n, int nb, const int* __restrict__ blk_lo, 
   }
 }
 
-// One row's record of one sweep.
-template <class T, int K>
-struct SmallRec {
+// The columns of one row's record (what its gathers wait for), loaded a level ahead.
+template <int K>
+struct SmallCols {
   int p;        // permuted row, -1: none
   int c[K];
-  T v[K];
-  T x, d;       // r (forward) or y (backward), and the diagonal factor
 };
 
-template <class T, int K>
-__device__ __forceinline__ void small_load(SmallRec<T, K>& o, int p, const int* __restrict__ cc,
-                                           const T* __restrict__ vv, const T* __restrict__ dd, const T* x) {
+template <int K>
+__device__ __forceinline__ void small_cols(SmallCols<K>& o, int p, const int* __restrict__ cc) {
   o.p = p;
   if (p < 0) return;
 #pragma unroll
-  for (int k = 0; k < K; ++k) { o.c[k] = cc[(int64_t)p * K + k]; o.v[k] = vv[(int64_t)p * K + k]; }
-  o.x = x[p];
-  o.d = dd[p];
+  for (int k = 0; k < K; ++k) o.c[k] = cc[(int64_t)p * K + k];
+}
+
+// Row p of one sweep: its values, its input x[p] (r forward, y backward) and its diagonal
+// factor load beside the gathers of the coupled values, so the row costs one round trip.
+template <class T, bool DILU, bool FWD, int K>
+__device__ __forceinline__ void small_row(const SmallCols<K>& o, const T* __restrict__ vv, const T* __restrict__ dd,
+                                          const T* x, const T* g, T* out) {
+  const int p = o.p;
+  T v[K], gv[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    v[k] = vv[(int64_t)p * K + k];
+    gv[k] = o.c[k] >= 0 ? g[o.c[k]] : T(0);
+  }
+  const T xp = x[p], dp_ = dd[p];
+  T acc = (FWD || !DILU) ? xp : T(0);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (o.c[k] >= 0) {
+      if (FWD) acc = acc - v[k] * gv[k];
+      else if (DILU) acc = acc + gv[k] * v[k];
+      else acc = acc - gv[k] * v[k];
+    }
+  if (FWD) out[p] = DILU ? dp_ * acc : acc;
+  else out[p] = DILU ? xp - dp_ * acc : acc * dp_;
 }
 
 // LPB lanes per block, 32 / LPB blocks per warp; y and s are written and re-read across
-// levels (no __restrict__ on them).  Each lane loads its next level's record before it
-// gathers the current level's coupled values, so a level costs one dependent round trip.
+// levels (no __restrict__ on them).  Each lane loads its next level's columns before it
+// works on the current level, so a level costs one dependent round trip.
 template <class T, bool DILU, int K, int LPB>
-__global__ void __launch_bounds__(kSmallThreads, K <= 3 ? 3 : (K <= 4 ? 2 : 1)) k_ilu_small(int nb, const int* __restrict__ blvl,
-                                                             const int* __restrict__ lo, const int* __restrict__ hi,
-                                                             const int* __restrict__ cF, const T* __restrict__ vF,
-                                                             const T* __restrict__ dF, const int* __restrict__ cB,
-                                                             const T* __restrict__ vB, const T* __restrict__ dB,
-                                                             const T* __restrict__ r, T* y, T* s, const int* gate) {
+__global__ void __launch_bounds__(kSmallThreads, K <= 3 ? 4 : (K <= 4 ? 3 : 2))
+k_ilu_small(int nb, const int* __restrict__ blvl, const int* __restrict__ lo, const int* __restrict__ hi,
+            const int* __restrict__ cF, const T* __restrict__ vF, const T* __restrict__ dF,
+            const int* __restrict__ cB, const T* __restrict__ vB, const T* __restrict__ dB,
+            const T* __restrict__ r, T* y, T* s, const int* gate) {
   if (gated(gate)) return;
   constexpr int BPW = 32 / LPB;
   const int lane = threadIdx.x & 31, sub = lane / LPB, li = lane % LPB;
@@ -1149,7 +1168,8 @@ __global__ void __launch_bounds__(kSmallThreads, K <= 3 ? 3 : (K <= 4 ? 2 : 1)) 
   for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < ngroups; w += nwarps) {
     const int b = w * BPW + sub;
     const int l0 = b < nb ? blvl[b] : 0, l1 = b < nb ? blvl[b + 1] : 0;
-    int nlev = l1 - l0, maxlev = nlev;
+    const int nlev = l1 - l0;
+    int maxlev = nlev;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) maxlev = max(maxlev, __shfl_xor_sync(0xffffffffu, maxlev, o));
     auto first_row = [&](int t, bool fwd) -> int {   // this lane's first row of step t, or -1
@@ -1158,56 +1178,34 @@ __global__ void __launch_bounds__(kSmallThreads, K <= 3 ? 3 : (K <= 4 ? 2 : 1)) 
       const int p = lo[l] + li;
       return p < hi[l] ? p : -1;
     };
-    // forward
-    SmallRec<T, K> cur, nxt;
-    small_load<T, K>(cur, first_row(0, true), cF, vF, dF, r);
+    SmallCols<K> cur, nxt;
+    // forward: y = D^-1 (r - L y) (D-ILU) or r - L y (ILU(0), unit L)
+    small_cols<K>(cur, first_row(0, true), cF);
     for (int t = 0; t < maxlev; ++t) {
-      small_load<T, K>(nxt, first_row(t + 1, true), cF, vF, dF, r);
+      small_cols<K>(nxt, first_row(t + 1, true), cF);
       if (cur.p >= 0) {
-        T acc = cur.x;
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-          if (cur.c[k] >= 0) acc = acc - cur.v[k] * y[cur.c[k]];
-        y[cur.p] = DILU ? cur.d * acc : acc;
-        const int l = l0 + t;
-        for (int p = cur.p + LPB; p < hi[l]; p += LPB) {   // levels wider than LPB
-          SmallRec<T, K> o;
-          small_load<T, K>(o, p, cF, vF, dF, r);
-          T a2 = o.x;
-#pragma unroll
-          for (int k = 0; k < K; ++k)
-            if (o.c[k] >= 0) a2 = a2 - o.v[k] * y[o.c[k]];
-          y[p] = DILU ? o.d * a2 : a2;
+        small_row<T, DILU, true, K>(cur, vF, dF, r, y, y);
+        const int e = hi[l0 + t];
+        for (int p = cur.p + LPB; p < e; p += LPB) {   // levels wider than LPB
+          SmallCols<K> o;
+          small_cols<K>(o, p, cF);
+          small_row<T, DILU, true, K>(o, vF, dF, r, y, y);
         }
       }
       __syncwarp();
       cur = nxt;
     }
-    // backward (the forward result y is the input)
-    small_load<T, K>(cur, first_row(0, false), cB, vB, dB, y);
+    // backward from the forward result y
+    small_cols<K>(cur, first_row(0, false), cB);
     for (int t = 0; t < maxlev; ++t) {
-      small_load<T, K>(nxt, first_row(t + 1, false), cB, vB, dB, y);
+      small_cols<K>(nxt, first_row(t + 1, false), cB);
       if (cur.p >= 0) {
-        T acc = DILU ? T(0) : cur.x;
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-          if (cur.c[k] >= 0) {
-            if (DILU) acc = acc + s[cur.c[k]] * cur.v[k];
-            else acc = acc - s[cur.c[k]] * cur.v[k];
-          }
-        s[cur.p] = DILU ? cur.x - cur.d * acc : acc * cur.d;
-        const int l = l1 - 1 - t;
-        for (int p = cur.p + LPB; p < hi[l]; p += LPB) {
-          SmallRec<T, K> o;
-          small_load<T, K>(o, p, cB, vB, dB, y);
-          T a2 = DILU ? T(0) : o.x;
-#pragma unroll
-          for (int k = 0; k < K; ++k)
-            if (o.c[k] >= 0) {
-              if (DILU) a2 = a2 + s[o.c[k]] * o.v[k];
-              else a2 = a2 - s[o.c[k]] * o.v[k];
-            }
-          s[p] = DILU ? o.x - o.d * a2 : a2 * o.d;
+        small_row<T, DILU, false, K>(cur, vB, dB, y, s, s);
+        const int e = hi[l1 - 1 - t];
+        for (int p = cur.p + LPB; p < e; p += LPB) {
+          SmallCols<K> o;
+          small_cols<K>(o, p, cB);
+          small_row<T, DILU, false, K>(o, vB, dB, y, s, s);
         }
       }
       __syncwarp();
