@@ -67,6 +67,7 @@ class Layout:
         local[own] = col[own] - lo + 1
         local[~own] = self.n + 1 + np.searchsorted(ghost, col[~own])
         self.local_col = local.astype(np.int32)
+        self.global_col = (col + 0).astype(np.int64)   # 1-based global columns, as given
         self.rowptr = np.asarray(rowptr, dtype=np.int32)
         need = {int(q): ghost[owner == q].tolist() for q in np.unique(owner)}
         needs = [None] * self.world
@@ -278,6 +279,28 @@ def _pgmres(lay, op, b, x, itrmax, rtol, hist, m, mgs):
     return min(itrmax, itr + inner), (1 if itrmax <= itr else 0)
 
 
+def cuda_block_precon(n, rowptr, col, val, starts, options):
+    """The library's block-Jacobi operator of an n-row matrix without halo columns (1-based
+    local rowptr / col), with explicit blocks `starts`: precon(r, z) on CUDA tensors."""
+    import types
+    lay = types.SimpleNamespace(n=int(n), n_ext=int(n), rowptr=np.asarray(rowptr, np.int32),
+                                local_col=np.asarray(col, np.int32))
+    return CudaLocal(lay, val, dict(options, blocks=starts))
+
+
+class _Composed:
+    """The product of one local operator and the preconditioner of another."""
+
+    def __init__(self, spmv_op, precon_op):
+        self.s, self.p = spmv_op, precon_op
+
+    def spmv(self, x_ext, y):
+        self.s.spmv(x_ext, y)
+
+    def precon(self, r, z):
+        self.p.precon(r, z)
+
+
 def solve(layout: Layout, val, b: torch.Tensor, x: torch.Tensor, backend=None, **options):
     """Distributed solve of the rows this process owns.  b, x: this process's parts
     (float64 tensors on the backend's device; x is the initial guess and the result).
@@ -288,7 +311,20 @@ def solve(layout: Layout, val, b: torch.Tensor, x: torch.Tensor, backend=None, *
     solver = int(options.get("solver", 3))
     itrmax = int(options.get("itrmax", 100))
     rtol = float(options.get("rtolmax", 1e-8))
-    op = backend if backend is not None else CudaLocal(layout, val, options)
+    if backend is not None:
+        op = backend
+    elif int(options.get("ipreflag", 0)) == 3 and layout.world > 1:
+        # additive Schwarz with overlap (parcel_b/schwarz.py): the product from a local operator
+        # without preconditioner, the preconditioner from the overlapped regions
+        from .schwarz import Schwarz
+        base = CudaLocal(layout, val, dict(options, ipreflag=0))
+        ilu = int(options.get("ILU_method", 1))
+        prec = Schwarz(layout, layout.rowptr, layout.global_col, val, int(options.get("precon_thblock", 1)),
+                       int(options.get("addL", 0)), int(options.get("iflagAS", 1)), ilu if ilu > 0 else 1,
+                       cuda_block_precon, {k: v for k, v in options.items() if k not in ("addL", "iflagAS")})
+        op = _Composed(base, prec)
+    else:
+        op = CudaLocal(layout, val, options)
     hist = np.zeros(max(itrmax, 1))
     if solver == 1:
         niter, iret = _pcg(layout, op, b, x, itrmax, rtol, hist)
@@ -307,6 +343,7 @@ def parcel_dcg(x, b, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU
     distributed matrix; returns (niter, iret)."""
     lay = Layout(n, gn, istart, crsRow_ptr, np.asarray(crsCol)[:nnz], group=group)
     niter, iret, h = solve(lay, np.asarray(crsA)[:nnz], b, x, solver=1, ipreflag=ipreflag, ILU_method=ILU_method,
+                           addL=addL, iflagAS=iflagAS,
                            itrmax=itrmax, rtolmax=rtolmax, **extra)
     reshistory[:len(h)] = h
     return niter, iret
@@ -318,6 +355,7 @@ def parcel_dgmres(x, b, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, 
     distributed matrix; returns (niter, iret)."""
     lay = Layout(n, gn, istart, crsRow_ptr, np.asarray(crsCol)[:nnz], group=group)
     niter, iret, h = solve(lay, np.asarray(crsA)[:nnz], b, x, solver=3, ipreflag=ipreflag, ILU_method=ILU_method,
+                           addL=addL, iflagAS=iflagAS,
                            itrmax=itrmax, rtolmax=rtolmax, GMRES_m=GMRES_m, GMRES_GSflag=GMRES_GSflag, **extra)
     reshistory[:len(h)] = h
     return niter, iret
