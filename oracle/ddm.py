@@ -136,7 +136,11 @@ def dilu_apply(dd, boxes, r, split_axis=None):
     vec2(j) = Dinv(j) (r(j) - sum_lower a vec2), backward vec2(j) -= Dinv(j) sum_upper a vec2,
     vec2 zero on the margin.  split_axis (0, 1, 2) restates the CPU build's slab sweeps, which
     test only that axis against the slab bounds (other axes reach the margin, where vec2 is
-    zero); None tests every axis (the CUDA build's boxes)."""
+    zero); None drops every coupling that leaves the box (the CUDA build's boxes, and the
+    block-Jacobi form the product follows).  The two agree for stencils along the
+    axes; with diagonal points the split-axis test lets a lower coupling reach into the next
+    slab, a cell that another OpenMP thread of the reference is writing at the same time (a
+    race there), so the box-restricted form is the one the product follows."""
     val, off, m = dd["val"], dd["offset"], dd["m"]
     nnd = len(off)
     od = np.asarray(dd["offset_dim"]).reshape(3, nnd).T
@@ -169,8 +173,9 @@ def dilu_apply(dd, boxes, r, split_axis=None):
                 Dinv[k] = Dinv[k] - val[ip * m + j] * val[ipp * m + k] * Dinv[j]
 
         def outside(c, d_lo_hi):
-            axes = range(3) if split_axis is None else (split_axis,)
-            return any(d_lo_hi(c, d) for d in axes)
+            if split_axis is None:   # the box: both bounds on every axis
+                return any(c[d] < lo[d] or c[d] > hi[d] - 1 for d in range(3))
+            return d_lo_hi(c, split_axis)
 
         for (x, y, z) in cells:
             j = pidx(x, y, z)
@@ -196,7 +201,8 @@ def dilu_apply(dd, boxes, r, split_axis=None):
 def global_system(parts, npe, boxes_of):
     """The global matrix of a DDM decomposition, numbered process by process (rank order), box
     by box, lexicographically inside a box.  parts[rank]: the process's DDM dict (as
-    poisson3d_ddm returns, with 'n', 'start', 'pad', 'margin', 'val', 'offset_dim');
+    poisson3d_ddm returns, with 'n', 'start', 'pad', 'margin', 'val', 'offset_dim'; optional
+    'margins' per axis, 0 past ndim, with offset_dim then holding ndim columns);
     boxes_of(n) -> that process's boxes.  Couplings to cells outside the global grid and
     zero values are left out.  Returns (rowptr, col (1-based, sorted), val, b, x_exact,
     starts of every box, the padded index of each row, the rank of each row)."""
@@ -225,12 +231,14 @@ def global_system(parts, npe, boxes_of):
     prank = np.zeros(N, dtype=np.int64)
     for r, p in enumerate(parts):
         (sx, sy, sz), (nx, ny, nz) = p["start"], p["n"]
-        mg, (mx, my, _), m = p["margin"], p["pad"], p["m"]
+        (mx, my, _), m = p["pad"], p["m"]
+        mgx, mgy, mgz = p.get("margins", (p["margin"],) * 3)   # per axis (0 past ndim)
         nnd = len(p["offset"])
-        od = np.asarray(p["offset_dim"]).reshape(3, nnd).T
+        od = np.asarray(p["offset_dim"]).reshape(-1, nnd).T
+        od = np.concatenate([od, np.zeros((nnd, 3 - od.shape[1]), od.dtype)], axis=1)
         zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
         row = base[r] + idx[r]
-        j = (xx + mg) + mx * ((yy + mg) + my * (zz + mg))
+        j = (xx + mgx) + mx * ((yy + mgy) + my * (zz + mgz))
         b[row.ravel()] = p["b"][j.ravel()]
         xe[row.ravel()] = p["x_exact"][j.ravel()]
         pj[row.ravel()] = j.ravel()

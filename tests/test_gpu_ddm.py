@@ -199,3 +199,36 @@ def test_ddm_over_processes_on_the_gpu_backend():
     m = ho[:k] > 1e-8 * ho[0]
     assert np.max(np.abs(hist[:k][m] - ho[:k][m]) / ho[:k][m]) < 1e-6
     assert np.max(np.abs(x[G["padded"]] - xo)) <= 1e-8 * np.max(np.abs(xo))
+
+
+GENERAL = [
+    ("star13-margin2-xslabs", (12, 10, 8), 2, "star", dict(boxes=ddm.BOXES_THREADS, div_direc_th=1, precon_thblock=3),
+     lambda n: oddm.thread_boxes(n, 1, 3)),
+    ("star13-margin2-cubes", (12, 10, 8), 2, "star", dict(boxes=ddm.BOXES_CUBES), oddm.cube_boxes),
+    ("box27-zslabs", (10, 9, 8), 1, "box", dict(boxes=ddm.BOXES_THREADS, div_direc_th=3, precon_thblock=2),
+     lambda n: oddm.thread_boxes(n, 3, 2)),
+    ("2d-box9-yslabs", (40, 30), 1, "box", dict(boxes=ddm.BOXES_THREADS, div_direc_th=2, precon_thblock=4),
+     lambda n: oddm.thread_boxes(n, 2, 4)),
+    ("2d-box9-cubes", (40, 30), 1, "box", dict(boxes=ddm.BOXES_CUBES), oddm.cube_boxes),
+]
+
+
+@pytest.mark.parametrize("solver", [2, 3], ids=["bicgstab", "gmres"])
+@pytest.mark.parametrize("name,n,margin,kind,opt,boxes_of", GENERAL, ids=[g[0] for g in GENERAL])
+def test_ddm_general_stencils_match_oracle(solver, name, n, margin, kind, opt, boxes_of):
+    """Boxes the reference's example does not make: a 13-point star reaching two cells (margin
+    2), the 27-point box (13 couplings per row and sweep, the general sweep) and a 2D box,
+    with random nonsymmetric couplings; against the oracle's solve of the renumbered system
+    with the boxes as blocks (every coupling that leaves a box dropped)."""
+    import ddm_cases
+    pts = ddm_cases.star(len(n), 2) if kind == "star" else ddm_cases.box(len(n))
+    p = ddm_cases.stencil_box(n, margin, pts, seed=11)
+    kw = dict(solver=solver, ipreflag=2, itrmax=800, rtolmax=1e-10, GMRES_m=15, GMRES_GSflag=1)
+    G, (xo, ho, no, io) = _oracle(p, boxes_of, ILU_method=1, **kw)
+    g = ddm.solve(p["val"], p["offset"], p["offset_dim"], n, p["b"], margin=margin, **opt, **kw)
+    assert g["iret"] == io == 0 and abs(g["niter"] - no) <= 2, (g["niter"], no)
+    k = min(g["niter"], no)
+    m = ho[:k] > (1e-6 if solver == 2 else 1e-8) * ho[0]
+    assert np.max(np.abs(g["reshistory"][:k][m] - ho[:k][m]) / ho[:k][m]) < 1e-6
+    assert np.max(np.abs(g["x"][G["padded"]] - xo)) <= 1e-7 * np.max(np.abs(xo))
+    assert g["stats"]["ilu_nblocks"] == len(boxes_of(p["n"]))

@@ -114,3 +114,24 @@ def test_gpu_ddm_template_cubes():
 @pytest.mark.slow
 def test_cpu_ddm_dd_template_slabs():
     _template("cpu_ddm_ddcg_slabs", _slabs(1, 20), dd=True)
+
+
+@pytest.mark.parametrize("pts,margin", [("star2", 2), ("box27", 1)])
+@pytest.mark.parametrize("boxes,axis", [(_slabs(1, 3), 0), (ddm.cube_boxes, None)])
+def test_box_dilu_general_stencils(pts, margin, boxes, axis):
+    """The padded-box D-ILU equals the renumbered CRS D-ILU for a 13-point star reaching two
+    cells (margin 2) and the 27-point box, not only for the example's 7 points.  A slab sweep
+    of the reference tests only the split axis against the slab, which for a stencil with
+    diagonal points (the 27-point box) lets a lower coupling reach the next slab, a cell
+    another thread is writing; the box-restricted form (every coupling that leaves the box
+    dropped) is the block Jacobi the diagonal recurrence assumes, and it is the one compared
+    for such stencils.  Axis-aligned stencils give the same result either way."""
+    import ddm_cases
+    p = ddm_cases.stencil_box((9, 8, 7), margin, ddm_cases.star(3, 2) if pts == "star2" else ddm_cases.box(3), 3)
+    G = ddm.global_system([p], (1, 1, 1), boxes)
+    r = np.random.default_rng(5).standard_normal(G["n"])
+    zc = oracle.precon_apply(_crs(G), r, ipreflag=2, ILU_method=1, blocks=G["starts"])
+    rp = np.zeros(p["m"])
+    rp[G["padded"]] = r
+    zd = ddm.dilu_apply(p, boxes(p["n"]), rp, split_axis=axis if pts == "star2" else None)[G["padded"]]
+    assert np.abs(zc - zd).max() <= 1e-13 * np.abs(zc).max()
