@@ -6,7 +6,9 @@ This mirrors the reference's MPI decomposition, which has no counterpart on one 
   * before every product a process receives the halo values it references from the
     processes that own them (src/comm.f90:153-403, 528-597);
   * block-Jacobi blocks stay inside each process (src/matrix.f90:8074-8134), so the
-    preconditioner needs no communication;
+    preconditioner needs no communication; additive Schwarz with overlap (ipreflag 3,
+    addL > 0) extends every block into its neighbours and exchanges addL rows with each
+    neighbouring process per application (parcel_b/schwarz.py);
   * an inner product is a local partial followed by one all-gather of the partials,
     summed in rank order, so every process takes the same branch and the result does not
     depend on message timing.
