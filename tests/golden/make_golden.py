@@ -7,8 +7,10 @@ output files; nothing here executes reference code):
 
 Writes tests/golden/reference_templates.json.  The fixtures are the reference's only
 known-answer outputs for this path (src/example/template_cpu/STDOUT_run,
-template_gpu/STDOUT_run, template_cpu/STDOUT_run_dd, template_cpu/STDOUT_run_qr), all
-for the 160^3 Poisson problem of src/example/problem.f90 with rtolmax = 1e-9.
+template_gpu/STDOUT_run, template_cpu/STDOUT_run_dd, template_cpu/STDOUT_run_qr, and the
+DDM ones template_cpu/STDOUT_run_ddm, template_gpu/STDOUT_run_ddm,
+template_cpu/STDOUT_run_ddm_dd), all for the 160^3 Poisson problem of the examples with
+rtolmax = 1e-9.
 """
 from __future__ import annotations
 
