@@ -58,3 +58,41 @@ def stencil_box(n, margin, pts, seed=0):
     return dict(val=val, offset=offset, offset_dim=np.asfortranarray(od).ravel(order="F").astype(np.int32),
                 b=b, x_exact=np.zeros(m), n=n3, nd=list(n), start=[0, 0, 0], pad=pad3, m=m, margin=margin,
                 margins=tuple([margin] * ndim + [0] * (3 - ndim)), rxyz=(0, 0, 0), nnd=nnd)
+
+
+def split_stencil(gn, npe, rank, margin, pts, seed=0):
+    """Process `rank`'s box (set_rank_xyz, set_grids_decompostion) of one global random
+    stencil matrix on the grid gn: the same couplings as stencil_box would give the whole grid,
+    each process holding its interior rows (couplings into other processes kept, into the
+    outside of the grid zero)."""
+    import ddm as oddm
+    rxyz = oddm.rank_xyz(rank, npe)
+    n, start, pad, m = oddm.grids_decomposition(gn, npe, rxyz, margin)
+    nnd = len(pts)
+    od = np.array(pts, dtype=np.int32)
+    stride = [1, pad[0], pad[0] * pad[1]]
+    offset = (od * np.array(stride)).sum(axis=1).astype(np.int32)
+    rng = np.random.default_rng(seed)
+    G = int(np.prod(gn))
+    gval = -rng.uniform(0.1, 1.0, (nnd, G))              # coupling of global cell g along point k
+    kd = [k for k in range(nnd) if not od[k].any()][0]
+    zz, yy, xx = np.meshgrid(*[np.arange(v) for v in reversed(gn)], indexing="ij")
+    gx, gy, gz = xx.ravel(), yy.ravel(), zz.ravel()
+    inside = np.ones((nnd, G), bool)
+    for k in range(nnd):
+        for d, c in enumerate((gx, gy, gz)):
+            inside[k] &= (c + od[k, d] >= 0) & (c + od[k, d] < gn[d])
+    gval = np.where(inside, gval, 0.0)
+    gval[kd] = 1.0 + np.abs(np.delete(gval, kd, axis=0)).sum(axis=0) * rng.uniform(1.0, 1.3, G)
+    gb = rng.standard_normal(G)
+    jz, jy, jx = np.meshgrid(*[np.arange(v) for v in reversed(n)], indexing="ij")
+    jx, jy, jz = jx.ravel(), jy.ravel(), jz.ravel()
+    g = (jx + start[0]) + gn[0] * ((jy + start[1]) + gn[1] * (jz + start[2]))
+    j = (jx + margin) + pad[0] * ((jy + margin) + pad[1] * (jz + margin))
+    val = np.zeros(nnd * m)
+    for k in range(nnd):
+        val[k * m + j] = gval[k, g]
+    b = np.zeros(m)
+    b[j] = gb[g]
+    return dict(val=val, offset=offset, offset_dim=np.asfortranarray(od).ravel(order="F").astype(np.int32),
+                b=b, x_exact=np.zeros(m), n=n, start=start, pad=pad, m=m, margin=margin, rxyz=rxyz, nnd=nnd)

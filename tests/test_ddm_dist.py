@@ -9,8 +9,10 @@ the boxes as blocks); the histories must reproduce the oracle's single-process s
 same global system (oracle/ddm.py: the rows numbered process by process, box by box) with
 the same iteration counts, within 1e-8 relative while the residual is above 1e-8 of its
 start (rank-ordered partial sums), and x must land in the interior cells of each box.
-The library's host-side box numbering (parcel_b_ddm_order) is checked against the
-oracle's here too (it needs no GPU)."""
+Eight processes (npe = (2, 2, 2)) carry a 27-point stencil with random nonsymmetric
+couplings cut from one global field, so each process couples to its face, edge and corner
+neighbours (all 7 others) through its margin cells.  The library's host-side box numbering
+(parcel_b_ddm_order) is checked against the oracle's here too (it needs no GPU)."""
 import multiprocessing as mp
 import os
 import socket
@@ -60,19 +62,26 @@ class OracleLocal:
         z.copy_(self.torch.from_numpy(np.asarray(self.M(r.numpy().copy()), dtype=np.float64)))
 
 
-def _worker(rank, world, port, npe, solver, boxes, q):
+def _part(gn, npe, rank, stencil):
+    import ddm as oddm
+    import ddm_cases
+    if stencil == "7":
+        return oddm.poisson3d_ddm(gn, npe, rank)
+    return ddm_cases.split_stencil(gn, npe, rank, 1, ddm_cases.box(3), seed=5)
+
+
+def _worker(rank, world, port, npe, solver, boxes, q, gn=GN, stencil="7"):
     try:
-        sys.path[:0] = [os.path.join(ROOT, "parcel-legacy_b200"), os.path.join(ROOT, "oracle")]
+        sys.path[:0] = [os.path.join(ROOT, "parcel-legacy_b200"), os.path.join(ROOT, "oracle"), HERE]
         import torch
         import torch.distributed as dist
 
-        import ddm as oddm
         from parcel_b import ddm
         dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
-        p = oddm.poisson3d_ddm(GN, npe, rank)
+        p = _part(gn, npe, rank, stencil)
         x = np.zeros(p["m"])
         hist = np.zeros(500)
-        args = (x, p["b"], p["m"], 7, p["offset"], p["val"], 0, np.zeros(0, np.int32), 1, 3, np.array(npe),
+        args = (x, p["b"], p["m"], p["nnd"], p["offset"], p["val"], 0, np.zeros(0, np.int32), 1, 3, np.array(npe),
                 np.array(p["n"]), p["offset_dim"], 1, 2, 2, 1, 500, 1e-10, hist, 0, 2, 1, -1, 0)
         kw = dict(boxes=boxes, backend=OracleLocal)
         if solver == 1:
@@ -155,3 +164,38 @@ def test_decomposition_rejects_inconsistent_stencils():
         assert dec.layout.n_ext == dec.n_int == 120 and dec.gn == 120
     finally:
         dist.destroy_process_group()
+
+
+def test_27_point_stencil_over_eight_processes():
+    """A 27-point stencil with random nonsymmetric couplings on a 2 x 2 x 2 process split:
+    every process couples to its face, edge and corner neighbours, so the margin cells reach
+    all 7 other processes; GMRES against the oracle's global solve."""
+    import ddm as oddm
+    import oracle
+    from parcel_b.problems import CRS
+    gn, npe, world = (10, 8, 8), (2, 2, 2), 8
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, npe, 3, 0, q, gn, "27")) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=300) for _ in range(world)], key=lambda o: o[0])
+    for p in procs:
+        p.join(timeout=60)
+    for o in out:
+        assert o[1] != "error", o[2]
+    parts = [_part(gn, npe, r, "27") for r in range(world)]
+    G = oddm.global_system(parts, npe, lambda n: oddm.thread_boxes(n, 1, 2))
+    xo, ho, no, io = oracle.solve(CRS(n=G["n"], rowptr=G["rowptr"], col=G["col"], val=G["val"]), G["b"],
+                                  blocks=G["starts"], solver=3, ipreflag=2, ILU_method=1, itrmax=500,
+                                  rtolmax=1e-10, GMRES_m=10, GMRES_GSflag=1)
+    for rank, niter, iret, hist, x in out:
+        assert (niter, iret) == (no, io), (rank, niter, iret, no, io)
+        msk = ho[:niter] > 1e-8 * ho[0]
+        assert np.max(np.abs(hist[msk] - ho[:niter][msk]) / ho[:niter][msk]) < 1e-8
+        sel = G["rank"] == rank
+        assert np.max(np.abs(x[G["padded"][sel]] - xo[sel])) <= 1e-8 * np.max(np.abs(xo))
+        interior = np.zeros(len(x), bool)
+        interior[G["padded"][sel]] = True
+        assert not x[~interior].any()
