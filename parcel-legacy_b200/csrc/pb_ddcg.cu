@@ -861,7 +861,7 @@ void dd_setup_precon(const Options& o, const parcel_b_crs& A, const DdSystem& S,
   k_dd_ranges<<<grid_for(A.n), kDdThreads, 0, st>>>(A.n, plan.nb, dp<int>(blo), dp<int>(bhi), dp<int>(bof), S.rp,
                                                      S.ci, S.cbase, dp<int4>(P.rng));
   DBuf Dh(sizeof(double) * A.n), Dl(sizeof(double) * A.n);
-  k_dd_dilu_diag<<<plan.nb, kDdThreads, 0, st>>>(dp<IluChunk>(P.chunks), dp<int>(P.blk_chunk), dp<int>(blo),
+  k_dd_dilu_diag<<<plan.nb, ilu_factor_threads(plan.maxWp), 0, st>>>(dp<IluChunk>(P.chunks), dp<int>(P.blk_chunk), dp<int>(blo),
                                                  dp<int>(bhi), dp<int>(P.rowAt), S.rp, S.ci, S.ah, S.al, S.cbase,
                                                  o.ilu_method == 2 ? 1 : 0, dp<double>(Dh), dp<double>(Dl),
                                                  dp<double>(P.dih), dp<double>(P.dil));

@@ -200,6 +200,29 @@ __global__ void k_ddm_rowptr(int64_t n1, int* __restrict__ a) {
     a[i] += 1;
 }
 
+// perm[r] = padded index of interior cell r and inv[perm[r]] = r (inv holds -1 elsewhere,
+// set before).  Box b's cells are rows starts[b] .. starts[b + 1] - 1, x fastest inside the
+// box; bx holds each box's lo[3], hi[3].  Boxes are never empty, so starts is strictly
+// increasing and the search finds the one box that holds r.
+__global__ void k_ddm_perm(int nint, int nb, const int* __restrict__ starts, const int* __restrict__ bx, int mg0,
+                           int mg1, int mg2, int64_t s1, int64_t s2, int* __restrict__ perm, int* __restrict__ inv) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nint; r += (int64_t)gridDim.x * blockDim.x) {
+    int a = 0, z = nb;   // starts[a] <= r < starts[z]
+    while (z - a > 1) {
+      const int h = (a + z) >> 1;
+      if (starts[h] <= r) a = h;
+      else z = h;
+    }
+    const int* B = bx + 6 * (int64_t)a;
+    const int ex = B[3] - B[0], ey = B[4] - B[1];
+    const int loc = (int)r - starts[a];
+    const int x = B[0] + loc % ex, y = B[1] + (loc / ex) % ey, zc = B[2] + loc / (ex * ey);
+    const int64_t j = (int64_t)(x + mg0) + (int64_t)(y + mg1) * s1 + (int64_t)(zc + mg2) * s2;
+    perm[r] = (int)j;
+    inv[j] = (int)r;
+  }
+}
+
 // dst[r] = src[perm[r]] (to the renumbered order) or dst[perm[r]] = src[r] (back).
 __global__ void k_ddm_move(int nint, const int* __restrict__ perm, const double* __restrict__ src,
                            double* __restrict__ dst, int to_box) {
@@ -243,19 +266,30 @@ void ddm_build(const parcel_b_ddm* A, int precon_thblock, const double* val_lo, 
       PB_CHECK(off[k2] != off[k], PARCEL_B_E_ARG, "offset %d appears twice", off[k]);
   }
   const std::vector<Box> boxes = ddm_boxes(g, A->boxes, A->div_direc_th, precon_thblock);
-  std::vector<int> perm;
-  ddm_order(g, boxes, &perm, out.starts);
-  std::vector<int> inv((size_t)g.m, -1);
-  for (int64_t r = 0; r < g.nint; ++r) inv[perm[r]] = (int)r;
+  ddm_order(g, boxes, nullptr, out.starts);
+  const int nbox = (int)boxes.size();
+  std::vector<int> bx((size_t)6 * nbox);
+  for (int b = 0; b < nbox; ++b)
+    for (int e = 0; e < 3; ++e) {
+      bx[(size_t)6 * b + e] = boxes[b].lo[e];
+      bx[(size_t)6 * b + 3 + e] = boxes[b].hi[e];
+    }
 
   cudaStream_t st = stream();
   const int nint = (int)g.nint;
   const size_t nv = (size_t)nnd * (size_t)g.m;
+  // the numbering and its inverse, built on the device from the boxes
   out.perm.alloc(sizeof(int) * (size_t)nint);
-  h2d(out.perm.p, perm.data(), sizeof(int) * (size_t)nint);
-  DBuf dinv(sizeof(int) * (size_t)g.m), doff(sizeof(int) * nnd);
-  h2d(dinv.p, inv.data(), sizeof(int) * (size_t)g.m);
+  DBuf dinv(sizeof(int) * (size_t)g.m), doff(sizeof(int) * nnd), dbx(sizeof(int) * bx.size()),
+      dst(sizeof(int) * out.starts.size());
+  h2d(dbx.p, bx.data(), sizeof(int) * bx.size());
+  h2d(dst.p, out.starts.data(), sizeof(int) * out.starts.size());
   h2d(doff.p, off.data(), sizeof(int) * nnd);
+  PB_CUDA(cudaMemsetAsync(dinv.p, 0xFF, sizeof(int) * (size_t)g.m, st));   // -1: margin cells
+  k_ddm_perm<<<ddm_grid(nint), kDdmThreads, 0, st>>>(nint, nbox, dp<int>(dst), dp<int>(dbx), g.mg[0], g.mg[1],
+                                                     g.mg[2], g.stride[1], g.stride[2], dp<int>(out.perm),
+                                                     dp<int>(dinv));
+  PB_CUDA(cudaGetLastError());
   DBuf hv, lv;
   const double* vh = A->val;
   const double* vl = val_lo;

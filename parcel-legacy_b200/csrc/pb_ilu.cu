@@ -24,6 +24,7 @@
 #include <omp.h>
 #include <climits>
 #include <cmath>
+#include <memory>
 #include <numeric>
 
 #include "pb_device.cuh"
@@ -82,7 +83,9 @@ void ilu_build_plan(const HostCSR& A, const BlockSplit& blocks, IluPlan& P, int*
   P.blk_hi.resize(nb);
   for (int b = 0; b < nb; ++b) blocks.rows(b, n, &P.blk_lo[b], &P.blk_hi[b]);
   std::vector<int> nlev(nb, 0), gap(nb, 0), missing_diag(nb, 0);
-  std::vector<int> cL(n, 0), cU(n, 0);
+  // per-row coupling counts, written for every row by the level pass (no zero fill: first
+  // touched by the threads that use them)
+  std::unique_ptr<int[]> cL(new int[std::max(n, 1)]), cU(new int[std::max(n, 1)]);
   const int* rp = A.rowptr;
   const int* ci = A.col;
   const int cb = A.istart;
@@ -90,52 +93,61 @@ void ilu_build_plan(const HostCSR& A, const BlockSplit& blocks, IluPlan& P, int*
   // one core is left to the caller's other threads: a plan thread that the scheduler
   // pre-empts for a time slice would hold up the whole loop
   const int nthr = std::max(1, omp_get_num_procs() - 1);
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthr)
-  for (int b = 0; b < nb; ++b) {
-    if (block_ready) block_ready(b);
-    const int lo = P.blk_lo[b], hi = P.blk_hi[b];
-    std::vector<int> lb(hi - lo, 0), lsrc(hi - lo, INT_MAX);
-    int maxlev = 0, g = 0;
-    for (int i = lo; i < hi; ++i) {
-      // columns are sorted: the lower entries come first, so the row's level is final at
-      // its first upper entry and one walk over the row suffices
-      int L = lb[i - lo];
-      int nl = 0, nu = 0, lmin = lsrc[i - lo];
-      bool diag = false, fixed = false, unsorted = false;
-      for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
-        const int c = ci[j] - cb;
-        if (c < lo || c >= hi) continue;
-        if (c < i) {
-          unsorted |= fixed;
-          L = std::max(L, lev[c] + 1);
-          lmin = std::min(lmin, lev[c]);
-          ++nl;
-        } else if (c == i) {
-          diag = true;
-        } else {
-          fixed = true;
-          // an upper entry (i, c) makes c wait for i in the backward sweep order as well
-          lb[c - lo] = std::max(lb[c - lo], L + 1);
-          lsrc[c - lo] = std::min(lsrc[c - lo], L);
-          ++nu;
-        }
-      }
-      if (unsorted)   // a lower entry after an upper one: redo the upper entries with the final level
+  // blocks are handed out in runs: one at a time when there are few (large) blocks, about
+  // 32 runs per thread when there are tens of thousands of small ones, so that the
+  // per-level counters of neighbouring blocks are mostly written by one thread
+  const int grain = std::max(1, nb / (32 * nthr));
+#pragma omp parallel num_threads(nthr)
+  {
+    std::vector<int> lb, lsrc;   // this thread's scratch, reused across its blocks
+#pragma omp for schedule(dynamic, grain)
+    for (int b = 0; b < nb; ++b) {
+      if (block_ready) block_ready(b);
+      const int lo = P.blk_lo[b], hi = P.blk_hi[b];
+      lb.assign(hi - lo, 0);
+      lsrc.assign(hi - lo, INT_MAX);
+      int maxlev = 0, g = 0;
+      for (int i = lo; i < hi; ++i) {
+        // columns are sorted: the lower entries come first, so the row's level is final at
+        // its first upper entry and one walk over the row suffices
+        int L = lb[i - lo];
+        int nl = 0, nu = 0, lmin = lsrc[i - lo];
+        bool diag = false, fixed = false, unsorted = false;
         for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
           const int c = ci[j] - cb;
-          if (c > i && c < hi) {
+          if (c < lo || c >= hi) continue;
+          if (c < i) {
+            unsorted |= fixed;
+            L = std::max(L, lev[c] + 1);
+            lmin = std::min(lmin, lev[c]);
+            ++nl;
+          } else if (c == i) {
+            diag = true;
+          } else {
+            fixed = true;
+            // an upper entry (i, c) makes c wait for i in the backward sweep order as well
             lb[c - lo] = std::max(lb[c - lo], L + 1);
-            lsrc[c - lo] = std::min(lsrc[c - lo], L);   // an earlier, smaller L only widens W
+            lsrc[c - lo] = std::min(lsrc[c - lo], L);
+            ++nu;
           }
         }
-      if (!diag) missing_diag[b] = 1;
-      lev[i] = L;
-      cL[i] = nl; cU[i] = nu;
-      maxlev = std::max(maxlev, L);
-      if (lmin != INT_MAX) g = std::max(g, L - lmin);
+        if (unsorted)   // a lower entry after an upper one: redo the upper entries with the final level
+          for (int j = rp[i] - 1; j < rp[i + 1] - 1; ++j) {
+            const int c = ci[j] - cb;
+            if (c > i && c < hi) {
+              lb[c - lo] = std::max(lb[c - lo], L + 1);
+              lsrc[c - lo] = std::min(lsrc[c - lo], L);   // an earlier, smaller L only widens W
+            }
+          }
+        if (!diag) missing_diag[b] = 1;
+        lev[i] = L;
+        cL[i] = nl; cU[i] = nu;
+        maxlev = std::max(maxlev, L);
+        if (lmin != INT_MAX) g = std::max(g, L - lmin);
+      }
+      nlev[b] = maxlev + 1;
+      gap[b] = g;
     }
-    nlev[b] = maxlev + 1;
-    gap[b] = g;
   }
   for (int b = 0; b < nb; ++b)
     if (missing_diag[b]) {
@@ -143,68 +155,84 @@ void ilu_build_plan(const HostCSR& A, const BlockSplit& blocks, IluPlan& P, int*
                      "block-Jacobi block %d has a row without an in-block diagonal entry", b);
       throw Error{PARCEL_B_E_ZERO_PIVOT, "missing diagonal"};
     }
-  // level widths and coupling counts; permuted layout, block by block, level by level
+  // level widths and coupling counts
   P.blk_lvl.assign(nb + 1, 0);
   for (int b = 0; b < nb; ++b) P.blk_lvl[b + 1] = P.blk_lvl[b] + nlev[b];
   const int totlev = P.blk_lvl[nb];
-  std::vector<int> width(totlev, 0), kl(totlev, 0), ku(totlev, 0);
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthr)
-  for (int b = 0; b < nb; ++b)   // blocks own disjoint level ranges
+  std::unique_ptr<int[]> width(new int[std::max(totlev, 1)]), kl(new int[std::max(totlev, 1)]),
+      ku(new int[std::max(totlev, 1)]);   // zeroed block by block below
+  // per block: its span in the permuted layout (every level starts on a multiple of 4, so a
+  // block that starts on one spans the sum of its rounded-up widths) and its chunks (a level
+  // split at kIluChunk rows)
+  std::vector<int64_t> span(nb + 1, 0);
+  std::vector<int> nchunk(nb + 1, 0);
+#pragma omp parallel for schedule(dynamic, grain) num_threads(nthr)
+  for (int b = 0; b < nb; ++b) {   // blocks own disjoint level ranges
+    const int l0 = P.blk_lvl[b];
+    for (int l = 0; l < nlev[b]; ++l) width[l0 + l] = kl[l0 + l] = ku[l0 + l] = 0;
     for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) {
-      const int gl = P.blk_lvl[b] + lev[i];
+      const int gl = l0 + lev[i];
       width[gl]++;
       kl[gl] = std::max(kl[gl], cL[i]);
       ku[gl] = std::max(ku[gl], cU[i]);
     }
+    int64_t sp = 0;
+    int nc = 0;
+    for (int l = 0; l < nlev[b]; ++l) {
+      sp += align4(width[l0 + l]);
+      nc += (width[l0 + l] + kIluChunk - 1) / kIluChunk;
+    }
+    span[b + 1] = sp;
+    nchunk[b + 1] = nc;
+  }
+  for (int b = 0; b < nb; ++b) {
+    span[b + 1] += span[b];
+    nchunk[b + 1] += nchunk[b];
+  }
+  PB_CHECK(span[nb] <= INT_MAX - 3, PARCEL_B_E_ARG, "the permuted layout of %d rows exceeds 2^31 entries", n);
   P.lvl_start.assign(totlev, 0);
   P.lvl_end.assign(totlev, 0);
-  int cursor = 0, maxw = 0;
-  for (int b = 0; b < nb; ++b)
-    for (int l = 0; l < nlev[b]; ++l) {
-      int gl = P.blk_lvl[b] + l;
-      cursor = align4(cursor);
-      P.lvl_start[gl] = cursor;
-      cursor += width[gl];
-      P.lvl_end[gl] = cursor;
-      maxw = std::max(maxw, width[gl]);
-    }
-  P.np = align4(cursor);
-  P.maxWp = align4(maxw);
-  P.max_levels = *std::max_element(nlev.begin(), nlev.end());
-  P.W = *std::max_element(gap.begin(), gap.end()) + 1;
-  // positions, stable by natural index within a level
-  std::vector<int> fill(totlev, 0);
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthr)
-  for (int b = 0; b < nb; ++b)
-    for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) {
-      const int gl = P.blk_lvl[b] + lev[i];
-      pos_out[i] = P.lvl_start[gl] + fill[gl]++;
-    }
-  // chunks (a level split at kIluChunk rows carries its level's coupling maxima), in
-  // block order
-  P.chunks.clear();
-  P.blk_chunk.assign(nb + 1, 0);
+  P.blk_chunk.assign(nchunk.begin(), nchunk.end());
+  P.chunks.resize(nchunk[nb]);
+  int maxw = 0;
+  // level starts, positions (stable by natural index within a level) and chunks, in block
+  // order
+#pragma omp parallel for schedule(dynamic, grain) num_threads(nthr) reduction(max : maxw)
   for (int b = 0; b < nb; ++b) {
-    P.blk_chunk[b] = (int)P.chunks.size();
+    const int l0 = P.blk_lvl[b];
+    int cursor = (int)span[b];
+    int c = P.blk_chunk[b];
     for (int l = 0; l < nlev[b]; ++l) {
-      const int gl = P.blk_lvl[b] + l;
-      for (int o = 0; o < width[gl]; o += kIluChunk) {
-        IluChunk c;
-        c.start = P.lvl_start[gl] + o;
-        c.w = std::min(kIluChunk, width[gl] - o);
-        c.wpad = align4(c.w);
-        c.KL = kl[gl];
-        c.KU = ku[gl];
-        c.lvl = l;
-        c.off_in_level = o;
-        c.blk = b;
-        c.offF = 0;
-        c.offB = 0;
-        P.chunks.push_back(c);
+      const int gl = l0 + l, w = width[gl];
+      P.lvl_start[gl] = cursor;
+      P.lvl_end[gl] = cursor + w;
+      maxw = std::max(maxw, w);
+      for (int o = 0; o < w; o += kIluChunk) {
+        IluChunk& C = P.chunks[c++];
+        C.start = cursor + o;
+        C.w = std::min(kIluChunk, w - o);
+        C.wpad = align4(C.w);
+        C.KL = kl[gl];
+        C.KU = ku[gl];
+        C.lvl = l;
+        C.off_in_level = o;
+        C.blk = b;
+        C.offF = 0;
+        C.offB = 0;
       }
+      cursor = align4(cursor + w);
+    }
+    for (int l = 0; l < nlev[b]; ++l) width[l0 + l] = 0;   // reused as the fill counters
+    for (int i = P.blk_lo[b]; i < P.blk_hi[b]; ++i) {
+      const int gl = l0 + lev[i];
+      pos_out[i] = P.lvl_start[gl] + width[gl]++;
     }
   }
-  P.blk_chunk[nb] = (int)P.chunks.size();
+  // the last level of the last block is not padded at its end
+  P.np = nb > 0 ? align4(P.lvl_end[totlev - 1]) : 0;
+  P.maxWp = align4(maxw);
+  P.max_levels = nb > 0 ? *std::max_element(nlev.begin(), nlev.end()) : 0;
+  P.W = (nb > 0 ? *std::max_element(gap.begin(), gap.end()) : 0) + 1;
 }
 
 
@@ -1366,7 +1394,7 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   if (!D.dilu) {
     lu.alloc(sizeof(double) * nnz);
     d2d(lu.p, A.val, sizeof(double) * nnz);
-    k_ilu0_factor<<<P.nb, 256, 0, st>>>(dp<IluChunk>(D.chunks), dp<int>(D.blk_chunk), dp<int>(blo),
+    k_ilu0_factor<<<P.nb, ilu_factor_threads(P.maxWp), 0, st>>>(dp<IluChunk>(D.chunks), dp<int>(D.blk_chunk), dp<int>(blo),
                                         dp<int>(bhi), d_rowAt, A.rowptr, A.col, A.rbase, A.cbase,
                                         dp<double>(lu));
     PB_CUDA(cudaGetLastError());
@@ -1375,7 +1403,7 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
   } else {
     Dd.alloc(sizeof(double) * P.n);
     Di.alloc(sizeof(double) * P.n);
-    k_dilu_diag<<<P.nb, 256, 0, st>>>(dp<IluChunk>(D.chunks), dp<int>(D.blk_chunk), dp<int>(blo),
+    k_dilu_diag<<<P.nb, ilu_factor_threads(P.maxWp), 0, st>>>(dp<IluChunk>(D.chunks), dp<int>(D.blk_chunk), dp<int>(blo),
                                       dp<int>(bhi), d_rowAt, A.rowptr, A.col, A.val, A.rbase, A.cbase,
                                       ilu_method == 2 ? 1 : 0, dp<double>(Dd), dp<double>(Di));
     PB_CUDA(cudaGetLastError());

@@ -67,6 +67,9 @@ struct IluChunk {
   int off_in_level;  // position of the chunk's first row within its level
   int blk;           // block-Jacobi block
   int64_t offF, offB;   // byte offsets of the packed forward / backward data
+  // left uninitialised: the plan writes every field, and a plan of tens of thousands of
+  // small blocks holds hundreds of thousands of chunks
+  __host__ __device__ IluChunk() {}
 };
 constexpr int kIluChunk = 512;      // rows per chunk (multiple of 4)
 constexpr int kIluHeader = 32;      // bytes of the per-chunk header in the packed data
@@ -144,6 +147,11 @@ struct BlockSplit {
     *hi = starts[b + 1];
   }
 };
+// Threads of the one-CTA-per-block factorisation kernels: the widest level rounded up to a
+// warp, at most 256 (a CTA walks its block's levels with a stride of its size, so any size
+// gives the same result; small blocks with narrow levels then fit many more CTAs per SM).
+inline int ilu_factor_threads(int maxWp) { return std::min(256, std::max(32, (maxWp + 31) & ~31)); }
+
 // rowAt[pos[i]] = i for i < n (entries not hit keep their value).
 void scatter_positions(int n, const int* pos, int* rowAt, cudaStream_t st);
 
