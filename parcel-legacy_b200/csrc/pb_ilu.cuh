@@ -121,6 +121,11 @@ struct IluDev {
   int s_lpb = 32;                           // lanes per block (8, 16 or 32)
   DBuf s_blvl, s_lo, s_hi;                  // block -> first level (nb + 1); level -> [lo, hi)
   DBuf s_cF, s_vF, s_dF, s_cB, s_vB, s_dB;
+  // staged variant (k_ilu_small_staged): per block its first iteration-layout position and
+  // its stretch rounded up to 4 positions; the largest stretch and level count; the shared
+  // memory of one warp (0: the stretches are too long, the unstaged sweep runs)
+  DBuf s_box;
+  int s_span = 0, s_levcap = 0, s_warp_bytes = 0;
 };
 
 // Sparsity structure of the natural matrix on the host (for the wavefront plan).

@@ -121,6 +121,9 @@ void Precon<T>::apply(int64_t np, const T* r, T* s, const int* gate, cudaStream_
       scale<T>(np, s, dp<T>(dinv), r, gate, st);
       break;
     case PARCEL_B_PRECON_BLOCKJACOBI:
+      // the sweeps may read r over the whole padded iteration layout
+      PB_CHECK(np >= ilu.np, PARCEL_B_E_ARG, "vector of %lld entries, the iteration layout has %d", (long long)np,
+               ilu.np);
       ilu_apply<T>(ilu, r, s, nullptr, gate, st);
       break;
   }

@@ -254,6 +254,31 @@ def test_many_small_blocks_precon_matches_oracle(blocks, ilu):
     assert np.all(np.abs(res["reshistory"][:k][m] - ho[:k][m]) / ho[:k][m] < 1e-6)
 
 
+@pytest.mark.parametrize("ilu", [0, 1])
+def test_small_block_sweeps_staged_and_unstaged_match_oracle(ilu):
+    """Many small blocks take one of two warp-per-block sweeps: a block whose stretch of the
+    iteration layout (records, factors and right-hand side) fits 12 KB of shared memory per
+    warp is staged there; longer ones read global memory.  On 64^3 rows, 1,200 blocks of about
+    218 rows (66 levels, each padded to 4 positions) take the second, 20,000 blocks of
+    about 13 rows the first; both against the oracle.  And the FP32 inner sweep of the
+    mixed-precision solve through the staged one."""
+    A = problems.convdiff3d_upwind(64)
+    r = np.random.default_rng(7).standard_normal(A.n)
+    for blocks in (1200, 20000):
+        pre = dict(ipreflag=2, ILU_method=ilu, precon_thblock=blocks)
+        s_ref = oracle.precon_apply(A, r, **pre)
+        s = np.zeros(A.n)
+        p = _lib.new_input(**pre)
+        rc = _lib.load().parcel_b_precon_apply(C.byref(p), C.byref(api.crs_struct(A)), r.ctypes.data, s.ctypes.data)
+        assert rc == 0, _lib.last_error()
+        assert _rel(s, s_ref) < 1e-11, blocks
+    P, bp, _ = problems.poisson3d_reference(24, 24, 24)
+    res = api.solve(P, bp, solver=1, ipreflag=2, ILU_method=ilu, precon_thblock=2000, itrmax=4000, rtolmax=1e-12,
+                    inner_precision=1, residual_dd=1, inner_rtol=1e-4, max_refine=40)
+    assert res["iret"] == 0, res["stats"]
+    assert oracle.true_relres(P, bp, res["x"]) < 1e-12
+
+
 def test_diagonal_copy_spmv_path_matches_oracle():
     """Point Jacobi keeps the natural layout, where a stencil matrix's product runs on its
     diagonal copy (statistics: spmv_diagonals); CG and GMRES histories against the oracle at
