@@ -1244,14 +1244,15 @@ k_ilu_small(int nb, const int* __restrict__ blvl, const int* __restrict__ lo, co
 
 // The same sweep with a block's data staged in shared memory.  A block's rows occupy one
 // stretch [P0, P0 + S) of the iteration layout (its levels one after another, each starting
-// on a multiple of 4), so a warp copies the stretch's right-hand side, records and diagonal
-// factors into its own shared memory with 16-byte asynchronous copies, all in flight at
-// once (the backward records as a second group, which lands while the forward sweep runs).
+// on a multiple of 4), so the block's lanes copy the stretch's right-hand side, records and
+// diagonal factors into the block's own area of shared memory with 16-byte asynchronous
+// copies, all in flight at once (the backward records as a second group, which lands while
+// the forward sweep runs).
 // Both sweeps then run on shared memory, the solution overwriting the right-hand side in
 // place (a level reads only rows of other levels, which are final), and each row of s is
 // stored as it is finished.  Same records, same expressions, same order as k_ilu_small.
 constexpr int kStageWarps = 4;
-constexpr int kStageWarpBytes = 12 * 1024;
+constexpr int kStageBoxBytes = 12 * 1024;
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
@@ -1260,26 +1261,30 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// The warp's lanes copy `bytes` (a multiple of 16; both addresses 16-byte aligned).
-__device__ __forceinline__ void warp_stage(void* dst, const void* src, int bytes, int lane) {
+// The lanes of a group copy `bytes` (a multiple of 16; both addresses 16-byte aligned).
+__device__ __forceinline__ void group_stage(void* dst, const void* src, int bytes, int li, int lanes) {
   char* d = static_cast<char*>(dst);
   const char* g = static_cast<const char*>(src);
-  for (int o = lane * 16; o < bytes; o += 32 * 16) cp_async16(d + o, g + o);
+  for (int o = li * 16; o < bytes; o += lanes * 16) cp_async16(d + o, g + o);
 }
 
-template <class T, bool DILU, int K>
+// LPB lanes per block, 32 / LPB blocks per warp (as k_ilu_small), each block with its own
+// area of box_bytes; blockDim.x / 32 warps per CTA.
+template <class T, bool DILU, int K, int LPB>
 __global__ void __launch_bounds__(kStageWarps * 32)
 k_ilu_small_staged(int nb, const int2* __restrict__ box, const int* __restrict__ blvl, const int* __restrict__ lo,
                    const int* __restrict__ hi, const int* __restrict__ cF, const T* __restrict__ vF,
                    const T* __restrict__ dF, const int* __restrict__ cB, const T* __restrict__ vB,
                    const T* __restrict__ dB, const T* __restrict__ r, T* __restrict__ s, const int* gate, int span,
-                   int levcap, int warp_bytes) {
+                   int levcap, int box_bytes) {
   if (gated(gate)) return;
+  constexpr int BPW = 32 / LPB;
   extern __shared__ __align__(16) unsigned char stage_smem[];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  // this warp's area: T arrays first (each a multiple of 16 bytes, span being a multiple of
+  const int lane = threadIdx.x & 31, sub = lane / LPB, li = lane % LPB;
+  const int wib = threadIdx.x >> 5, wpc = blockDim.x >> 5;
+  // this block's area: T arrays first (each a multiple of 16 bytes, span being a multiple of
   // 4), then the int arrays
-  T* X = reinterpret_cast<T*>(stage_smem + (size_t)wib * warp_bytes);
+  T* X = reinterpret_cast<T*>(stage_smem + ((size_t)wib * BPW + sub) * box_bytes);
   T* Fv = X + span;
   T* Fd = Fv + (size_t)span * K;
   T* Bv = Fd + span;
@@ -1288,59 +1293,78 @@ k_ilu_small_staged(int nb, const int2* __restrict__ box, const int* __restrict__
   int* Bc = Fc + (size_t)span * K;
   int* Lo = Bc + (size_t)span * K;
   int* Hi = Lo + levcap;
-  const int nwarps = gridDim.x * kStageWarps;
-  for (int b = blockIdx.x * kStageWarps + wib; b < nb; b += nwarps) {
-    const int2 bx = box[b];   // stretch: first position, length (host-checked: <= span)
-    const int P0 = bx.x, S = bx.y;
-    const int l0 = blvl[b], nlev = blvl[b + 1] - l0;   // host-checked: <= levcap
-    warp_stage(X, r + P0, S * (int)sizeof(T), lane);
-    warp_stage(Fv, vF + (int64_t)P0 * K, S * K * (int)sizeof(T), lane);
-    warp_stage(Fd, dF + P0, S * (int)sizeof(T), lane);
-    warp_stage(Fc, cF + (int64_t)P0 * K, S * K * 4, lane);
-    cp_async_commit();
-    warp_stage(Bv, vB + (int64_t)P0 * K, S * K * (int)sizeof(T), lane);
-    if (!DILU) warp_stage(Bd, dB + P0, S * (int)sizeof(T), lane);
-    warp_stage(Bc, cB + (int64_t)P0 * K, S * K * 4, lane);
-    cp_async_commit();
-    for (int t = lane; t < nlev; t += 32) {
-      Lo[t] = lo[l0 + t] - P0;
-      Hi[t] = hi[l0 + t] - P0;
+  const int nwarps = gridDim.x * wpc;
+  const int ngroups = (nb + BPW - 1) / BPW;
+  for (int w = blockIdx.x * wpc + wib; w < ngroups; w += nwarps) {
+    const int b = w * BPW + sub;
+    int P0 = 0, S = 0, l0 = 0, nlev = 0;
+    if (b < nb) {
+      const int2 bx = box[b];   // stretch: first position, length (host-checked: <= span)
+      P0 = bx.x;
+      S = bx.y;
+      l0 = blvl[b];
+      nlev = blvl[b + 1] - l0;  // host-checked: <= levcap
     }
+    int maxlev = nlev;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxlev = max(maxlev, __shfl_xor_sync(0xffffffffu, maxlev, o));
+    if (b < nb) {
+      group_stage(X, r + P0, S * (int)sizeof(T), li, LPB);
+      group_stage(Fv, vF + (int64_t)P0 * K, S * K * (int)sizeof(T), li, LPB);
+      group_stage(Fd, dF + P0, S * (int)sizeof(T), li, LPB);
+      group_stage(Fc, cF + (int64_t)P0 * K, S * K * 4, li, LPB);
+    }
+    cp_async_commit();
+    if (b < nb) {
+      group_stage(Bv, vB + (int64_t)P0 * K, S * K * (int)sizeof(T), li, LPB);
+      if (!DILU) group_stage(Bd, dB + P0, S * (int)sizeof(T), li, LPB);
+      group_stage(Bc, cB + (int64_t)P0 * K, S * K * 4, li, LPB);
+      for (int t = li; t < nlev; t += LPB) {
+        Lo[t] = lo[l0 + t] - P0;
+        Hi[t] = hi[l0 + t] - P0;
+      }
+    }
+    cp_async_commit();
     cp_async_wait<1>();   // this lane's forward copies
     __syncwarp();         // and everyone's
     // forward: y = D^-1 (r - L y) (D-ILU) or r - L y (ILU(0), unit L)
-    for (int t = 0; t < nlev; ++t) {
-      const int e = Hi[t];
-      for (int q = Lo[t] + lane; q < e; q += 32) {
-        T acc = X[q];
+    for (int t = 0; t < maxlev; ++t) {
+      if (t < nlev) {
+        const int e = Hi[t];
+        for (int q = Lo[t] + li; q < e; q += LPB) {
+          T acc = X[q];
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const int c = Fc[q * K + k] - P0;   // -1 (no entry) falls outside [0, S)
-          if ((unsigned)c < (unsigned)S) acc = acc - Fv[q * K + k] * X[c];
+          for (int k = 0; k < K; ++k) {
+            const int c = Fc[q * K + k] - P0;   // -1 (no entry) falls outside [0, S)
+            if ((unsigned)c < (unsigned)S) acc = acc - Fv[q * K + k] * X[c];
+          }
+          X[q] = DILU ? Fd[q] * acc : acc;
         }
-        X[q] = DILU ? Fd[q] * acc : acc;
       }
       __syncwarp();
     }
     cp_async_wait<0>();
     __syncwarp();
     // backward from the forward result
-    for (int t = nlev - 1; t >= 0; --t) {
-      const int e = Hi[t];
-      for (int q = Lo[t] + lane; q < e; q += 32) {
-        const T xp = X[q], d = Bd[q];
-        T acc = DILU ? T(0) : xp;
+    for (int t = 0; t < maxlev; ++t) {
+      if (t < nlev) {
+        const int tl = nlev - 1 - t;
+        const int e = Hi[tl];
+        for (int q = Lo[tl] + li; q < e; q += LPB) {
+          const T xp = X[q], d = Bd[q];
+          T acc = DILU ? T(0) : xp;
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const int c = Bc[q * K + k] - P0;
-          if ((unsigned)c < (unsigned)S) {
-            if (DILU) acc = acc + X[c] * Bv[q * K + k];
-            else acc = acc - X[c] * Bv[q * K + k];
+          for (int k = 0; k < K; ++k) {
+            const int c = Bc[q * K + k] - P0;
+            if ((unsigned)c < (unsigned)S) {
+              if (DILU) acc = acc + X[c] * Bv[q * K + k];
+              else acc = acc - X[c] * Bv[q * K + k];
+            }
           }
+          const T o = DILU ? xp - d * acc : acc * d;
+          X[q] = o;
+          s[P0 + q] = o;
         }
-        const T o = DILU ? xp - d * acc : acc * d;
-        X[q] = o;
-        s[P0 + q] = o;
       }
       __syncwarp();
     }
@@ -1569,11 +1593,11 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
     const int levcap = align4(std::max(P.max_levels, 1));
     const int64_t tb = (int64_t)span * (1 + 2 * D.K + (D.dilu ? 1 : 2)) * (int64_t)sizeof(T) +
                        (int64_t)span * 2 * D.K * 4 + 2LL * levcap * 4;
-    D.s_warp_bytes = 0;
-    if (tb <= kStageWarpBytes) {   // four warps' areas within the default 48 KB of a CTA
+    D.s_box_bytes = 0;
+    if (tb <= kStageBoxBytes) {   // a warp's blocks (at most 4) within the default 48 KB of a CTA
       D.s_span = span;
       D.s_levcap = levcap;
-      D.s_warp_bytes = (int)tb;
+      D.s_box_bytes = (int)tb;
       D.s_box.alloc(sizeof(int2) * P.nb);
       h2d(D.s_box.p, bxs.data(), sizeof(int2) * P.nb);
     }
@@ -1619,14 +1643,25 @@ static void launch_small_lpb(const IluDev<T>& D, const T* r, T* s, const int* ga
       dp<int>(D.s_cB), dp<T>(D.s_vB), dp<T>(D.s_dB), r, dp<T>(D.ytmp), s, gate);
 }
 
+template <class T, bool DILU, int K, int LPB>
+static void launch_staged(const IluDev<T>& D, const T* r, T* s, const int* gate, cudaStream_t st) {
+  constexpr int BPW = 32 / LPB;
+  const int warp_bytes = BPW * D.s_box_bytes;
+  const int wpc = std::max(1, std::min(kStageWarps, 48 * 1024 / warp_bytes));
+  const int64_t groups = ((int64_t)D.nb + BPW - 1) / BPW;
+  const int grid = (int)std::min<int64_t>((groups + wpc - 1) / wpc, 32LL * num_sms());
+  k_ilu_small_staged<T, DILU, K, LPB><<<grid, wpc * 32, (size_t)wpc * warp_bytes, st>>>(
+      D.nb, dp<int2>(D.s_box), dp<int>(D.s_blvl), dp<int>(D.s_lo), dp<int>(D.s_hi), dp<int>(D.s_cF),
+      dp<T>(D.s_vF), dp<T>(D.s_dF), dp<int>(D.s_cB), dp<T>(D.s_vB), dp<T>(D.s_dB), r, s, gate, D.s_span,
+      D.s_levcap, D.s_box_bytes);
+}
+
 template <class T, bool DILU, int K>
 static void launch_small(const IluDev<T>& D, const T* r, T* s, const int* gate, cudaStream_t st) {
-  if (D.s_warp_bytes > 0 && (reinterpret_cast<uintptr_t>(r) & 15) == 0) {
-    const int grid = (int)std::min<int64_t>(((int64_t)D.nb + kStageWarps - 1) / kStageWarps, 32LL * num_sms());
-    k_ilu_small_staged<T, DILU, K><<<grid, kStageWarps * 32, kStageWarps * D.s_warp_bytes, st>>>(
-        D.nb, dp<int2>(D.s_box), dp<int>(D.s_blvl), dp<int>(D.s_lo), dp<int>(D.s_hi), dp<int>(D.s_cF),
-        dp<T>(D.s_vF), dp<T>(D.s_dF), dp<int>(D.s_cB), dp<T>(D.s_vB), dp<T>(D.s_dB), r, s, gate, D.s_span,
-        D.s_levcap, D.s_warp_bytes);
+  if (D.s_box_bytes > 0 && (reinterpret_cast<uintptr_t>(r) & 15) == 0) {
+    if (D.s_lpb == 8) launch_staged<T, DILU, K, 8>(D, r, s, gate, st);
+    else if (D.s_lpb == 16) launch_staged<T, DILU, K, 16>(D, r, s, gate, st);
+    else launch_staged<T, DILU, K, 32>(D, r, s, gate, st);
     return;
   }
   if (D.s_lpb == 8) launch_small_lpb<T, DILU, K, 8>(D, r, s, gate, st);

@@ -123,9 +123,9 @@ struct IluDev {
   DBuf s_cF, s_vF, s_dF, s_cB, s_vB, s_dB;
   // staged variant (k_ilu_small_staged): per block its first iteration-layout position and
   // its stretch rounded up to 4 positions; the largest stretch and level count; the shared
-  // memory of one warp (0: the stretches are too long, the unstaged sweep runs)
+  // memory of one block (0: the stretches are too long, the unstaged sweep runs)
   DBuf s_box;
-  int s_span = 0, s_levcap = 0, s_warp_bytes = 0;
+  int s_span = 0, s_levcap = 0, s_box_bytes = 0;
 };
 
 // Sparsity structure of the natural matrix on the host (for the wavefront plan).
