@@ -1147,14 +1147,17 @@ def run_ddm(args):
         parity = {"template_iterations": len(g), "max_rel_history_diff": float(np.max(np.abs(hist_dev[:k] - g[:k]) / g[:k]))}
     except (OSError, KeyError):
         parity = None
-    # end to end: the same call with pinned host arrays
+    # end to end: the same call with pinned host arrays (x too: zero initial guess in, the
+    # solution out, in place)
     hp = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-    h_val, h_off, h_b = hp(p["val"]), hp(p["offset"]), hp(p["b"])
+    h_val, h_off, h_b, h_x = hp(p["val"]), hp(p["offset"]), hp(p["b"]), hp(np.zeros_like(p["b"]))
     e2e = []
     for _ in range(max(1, min(args.steps, 3))):
+        h_x[:] = 0.0
         t0 = time.perf_counter()
-        ddm.solve(h_val, h_off, p["offset_dim"], p["n"], h_b, **kw)
+        ddm.solve(h_val, h_off, p["offset_dim"], p["n"], h_b, out=h_x, **kw)
         e2e.append(time.perf_counter() - t0)
+    e2e_err = float(np.abs(h_x - p["x_exact"]).max() / np.abs(p["x_exact"]).max())
     # kernel rooflines on the renumbered system
     prm = _lib.new_input(solver=1, ipreflag=2)
     D = ddm.ddm_struct(val, off, p["offset_dim"], p["n"], boxes=ddm.BOXES_CUBES)
@@ -1180,7 +1183,7 @@ def run_ddm(args):
            "setup_s": res["stats"]["setup_s"], "solve_s": res["stats"]["solve_s"],
            "step_times_s": [round(v, 6) for v in times],
            "e2e": {"value": sum(e2e) / len(e2e), "unit": "s", "h2d_bytes_per_step": int(h_val.nbytes + h_off.nbytes + 2 * m * 8),
-                   "d2h_bytes_per_step": int(m * 8 + res["niter"] * 8)},
+                   "d2h_bytes_per_step": int(m * 8 + res["niter"] * 8), "max_rel_error": e2e_err},
            "roofline": {"bound": "hbm", "kernel": "k_spmv_sell<double,double> on the renumbered system",
                         "achieved": sp_ach, "peak": hbm, "unit": "GB/s", "frac": sp_ach / hbm, "peak_kind": peak_kind,
                         "traffic": None, "algorithmic_bytes": int(spmv_bytes), "us_per_launch": ms_spmv.value * 1e3},

@@ -73,18 +73,29 @@ def _m_of(n_grids, margin):
 
 
 def solve(val, offset, offset_dim, n_grids, b, x0=None, *, margin=1, div_direc_th=1, boxes=BOXES_THREADS,
-          **options):
+          out=None, **options):
     """parcel_ddm_main on one process: the Krylov solver and preconditioner of the options
     (solver 1-4, ipreflag 0-2, precon_thblock, itrmax, rtolmax, GMRES_m, ...) on the interior
-    cells.  Returns {x, reshistory, niter, iret, stats}; x's margin entries are x0's."""
+    cells.  Returns {x, reshistory, niter, iret, stats}; x's margin entries are x0's.
+
+    out: an array of m float64 (host, or a device tensor when b is one) that holds the initial
+    guess on entry and receives x in place, as the reference's x argument does; x0 must then
+    be None.  A caller that keeps out in page-locked memory gets full-speed copies."""
     m = _m_of(n_grids, margin)
     _check("offset", offset, "int32")
     _check("offset_dim", offset_dim, "int32", len(offset) * len(n_grids))
     _check("val", val, "float64", len(offset) * m)
     _check("b", b, "float64", m)
     _check("x0", x0, "float64", m)
+    _check("out", out, "float64", m)
     on_dev = hasattr(b, "is_cuda") and b.is_cuda
-    if x0 is None:
+    if out is not None:
+        if x0 is not None:
+            raise ValueError("give the initial guess in out, not in x0, when out is given")
+        if on_dev != (hasattr(out, "is_cuda") and out.is_cuda):
+            raise ValueError("out must be on the device when b is, and on the host when b is")
+        x = out
+    elif x0 is None:
         if on_dev:
             import torch
             x = torch.zeros_like(b)

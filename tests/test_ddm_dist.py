@@ -199,3 +199,17 @@ def test_27_point_stencil_over_eight_processes():
         interior = np.zeros(len(x), bool)
         interior[G["padded"][sel]] = True
         assert not x[~interior].any()
+
+
+def test_solve_out_argument_is_checked_before_the_library():
+    """out must be float64 with m entries, on the side b is on, and excludes x0."""
+    import ddm as oddm
+    from parcel_b import ddm
+    p = oddm.poisson3d_ddm((6, 5, 4), (1, 1, 1), 0)
+    args = (p["val"], p["offset"], p["offset_dim"], p["n"], p["b"])
+    with pytest.raises(ValueError):
+        ddm.solve(*args, np.zeros(p["m"]), out=np.zeros(p["m"]))
+    with pytest.raises((TypeError, ValueError)):
+        ddm.solve(*args, out=np.zeros(p["m"], np.float32))
+    with pytest.raises((TypeError, ValueError)):
+        ddm.solve(*args, out=np.zeros(p["m"] - 1))

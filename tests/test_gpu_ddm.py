@@ -74,6 +74,25 @@ def test_ddm_solve_matches_oracle(solver, name, opt, boxes_of):
     assert g["stats"]["ilu_nblocks"] == len(boxes_of(p["n"]))
 
 
+def test_ddm_solve_into_out_in_place():
+    """out= holds the initial guess and receives x in place (page-locked host memory and a
+    device tensor); the same result as the x0 form, bit for bit."""
+    import torch
+    p = oddm.poisson3d_ddm(GN, (1, 1, 1), 0)
+    kw = dict(solver=1, ipreflag=2, itrmax=600, rtolmax=1e-10, boxes=ddm.BOXES_CUBES)
+    x0 = np.zeros(p["m"])
+    x0[0] = 3.0                              # a margin cell: must come back untouched
+    g = ddm.solve(p["val"], p["offset"], p["offset_dim"], p["n"], p["b"], x0, **kw)
+    h = torch.from_numpy(x0.copy()).pin_memory().numpy()
+    r = ddm.solve(p["val"], p["offset"], p["offset_dim"], p["n"], p["b"], out=h, **kw)
+    assert r["x"] is h and np.array_equal(h, g["x"]) and h[0] == 3.0
+    assert r["niter"] == g["niter"] and np.array_equal(r["reshistory"], g["reshistory"])
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    d = t(x0)
+    r = ddm.solve(t(p["val"]), t(p["offset"]), t(p["offset_dim"]), p["n"], t(p["b"]), out=d, **kw)
+    assert np.array_equal(d.cpu().numpy(), g["x"])
+
+
 @pytest.mark.parametrize("ipreflag", [0, 1])
 def test_ddm_point_jacobi_and_none_match_oracle(ipreflag):
     p = oddm.poisson3d_ddm(GN, (1, 1, 1), 0)
