@@ -1246,11 +1246,12 @@ k_ilu_small(int nb, const int* __restrict__ blvl, const int* __restrict__ lo, co
 // stretch [P0, P0 + S) of the iteration layout (its levels one after another, each starting
 // on a multiple of 4), so the block's lanes copy the stretch's right-hand side, records and
 // diagonal factors into the block's own area of shared memory with 16-byte asynchronous
-// copies, all in flight at once (the backward records as a second group, which lands while
-// the forward sweep runs).
-// Both sweeps then run on shared memory, the solution overwriting the right-hand side in
-// place (a level reads only rows of other levels, which are final), and each row of s is
-// stored as it is finished.  Same records, same expressions, same order as k_ilu_small.
+// copies, all in flight at once.  Both sweeps run on shared memory, the solution overwriting
+// the right-hand side in place (a level reads only rows of other levels, which are final),
+// and each row of s is stored as it is finished.  The backward records are copied over the
+// forward ones once the forward sweep is done: a smaller area per block lets more blocks be
+// in flight on an SM, which is what the sweep waits on.  Same records, same expressions, same
+// order as k_ilu_small.
 constexpr int kStageWarps = 4;
 constexpr int kStageBoxBytes = 12 * 1024;
 
@@ -1283,15 +1284,13 @@ k_ilu_small_staged(int nb, const int2* __restrict__ box, const int* __restrict__
   const int lane = threadIdx.x & 31, sub = lane / LPB, li = lane % LPB;
   const int wib = threadIdx.x >> 5, wpc = blockDim.x >> 5;
   // this block's area: T arrays first (each a multiple of 16 bytes, span being a multiple of
-  // 4), then the int arrays
+  // 4), then the int arrays; V and Cc hold the forward records, then the backward ones
   T* X = reinterpret_cast<T*>(stage_smem + ((size_t)wib * BPW + sub) * box_bytes);
-  T* Fv = X + span;
-  T* Fd = Fv + (size_t)span * K;
-  T* Bv = Fd + span;
-  T* Bd = DILU ? Fd : Bv + (size_t)span * K;   // D-ILU: both sweeps scale by the same D^-1
-  int* Fc = reinterpret_cast<int*>(DILU ? Bv + (size_t)span * K : Bd + span);
-  int* Bc = Fc + (size_t)span * K;
-  int* Lo = Bc + (size_t)span * K;
+  T* Fd = X + span;
+  T* Bd = DILU ? Fd : Fd + span;   // D-ILU: both sweeps scale by the same D^-1
+  T* V = Fd + span + (DILU ? 0 : span);   // after Fd (D-ILU) or after Bd (ILU(0))
+  int* Cc = reinterpret_cast<int*>(V + (size_t)span * K);
+  int* Lo = Cc + (size_t)span * K;
   int* Hi = Lo + levcap;
   const int nwarps = gridDim.x * wpc;
   const int ngroups = (nb + BPW - 1) / BPW;
@@ -1310,22 +1309,17 @@ k_ilu_small_staged(int nb, const int2* __restrict__ box, const int* __restrict__
     for (int o = 16; o > 0; o >>= 1) maxlev = max(maxlev, __shfl_xor_sync(0xffffffffu, maxlev, o));
     if (b < nb) {
       group_stage(X, r + P0, S * (int)sizeof(T), li, LPB);
-      group_stage(Fv, vF + (int64_t)P0 * K, S * K * (int)sizeof(T), li, LPB);
+      group_stage(V, vF + (int64_t)P0 * K, S * K * (int)sizeof(T), li, LPB);
       group_stage(Fd, dF + P0, S * (int)sizeof(T), li, LPB);
-      group_stage(Fc, cF + (int64_t)P0 * K, S * K * 4, li, LPB);
-    }
-    cp_async_commit();
-    if (b < nb) {
-      group_stage(Bv, vB + (int64_t)P0 * K, S * K * (int)sizeof(T), li, LPB);
+      group_stage(Cc, cF + (int64_t)P0 * K, S * K * 4, li, LPB);
       if (!DILU) group_stage(Bd, dB + P0, S * (int)sizeof(T), li, LPB);
-      group_stage(Bc, cB + (int64_t)P0 * K, S * K * 4, li, LPB);
       for (int t = li; t < nlev; t += LPB) {
         Lo[t] = lo[l0 + t] - P0;
         Hi[t] = hi[l0 + t] - P0;
       }
     }
     cp_async_commit();
-    cp_async_wait<1>();   // this lane's forward copies
+    cp_async_wait<0>();   // this lane's copies
     __syncwarp();         // and everyone's
     // forward: y = D^-1 (r - L y) (D-ILU) or r - L y (ILU(0), unit L)
     for (int t = 0; t < maxlev; ++t) {
@@ -1335,14 +1329,20 @@ k_ilu_small_staged(int nb, const int2* __restrict__ box, const int* __restrict__
           T acc = X[q];
 #pragma unroll
           for (int k = 0; k < K; ++k) {
-            const int c = Fc[q * K + k] - P0;   // -1 (no entry) falls outside [0, S)
-            if ((unsigned)c < (unsigned)S) acc = acc - Fv[q * K + k] * X[c];
+            const int c = Cc[q * K + k] - P0;   // -1 (no entry) falls outside [0, S)
+            if ((unsigned)c < (unsigned)S) acc = acc - V[q * K + k] * X[c];
           }
           X[q] = DILU ? Fd[q] * acc : acc;
         }
       }
       __syncwarp();
     }
+    // the forward records are no longer read (the barrier above): the backward ones replace them
+    if (b < nb) {
+      group_stage(V, vB + (int64_t)P0 * K, S * K * (int)sizeof(T), li, LPB);
+      group_stage(Cc, cB + (int64_t)P0 * K, S * K * 4, li, LPB);
+    }
+    cp_async_commit();
     cp_async_wait<0>();
     __syncwarp();
     // backward from the forward result
@@ -1355,10 +1355,10 @@ k_ilu_small_staged(int nb, const int2* __restrict__ box, const int* __restrict__
           T acc = DILU ? T(0) : xp;
 #pragma unroll
           for (int k = 0; k < K; ++k) {
-            const int c = Bc[q * K + k] - P0;
+            const int c = Cc[q * K + k] - P0;
             if ((unsigned)c < (unsigned)S) {
-              if (DILU) acc = acc + X[c] * Bv[q * K + k];
-              else acc = acc - X[c] * Bv[q * K + k];
+              if (DILU) acc = acc + X[c] * V[q * K + k];
+              else acc = acc - X[c] * V[q * K + k];
             }
           }
           const T o = DILU ? xp - d * acc : acc * d;
@@ -1591,8 +1591,8 @@ int ilu_setup_device(const IluPlan& P, const DevMat<double>& A, int ilu_method,
       span = std::max(span, p1 - p0);
     }
     const int levcap = align4(std::max(P.max_levels, 1));
-    const int64_t tb = (int64_t)span * (1 + 2 * D.K + (D.dilu ? 1 : 2)) * (int64_t)sizeof(T) +
-                       (int64_t)span * 2 * D.K * 4 + 2LL * levcap * 4;
+    const int64_t tb = (int64_t)span * (2 + D.K + (D.dilu ? 0 : 1)) * (int64_t)sizeof(T) +
+                       (int64_t)span * D.K * 4 + 2LL * levcap * 4;
     D.s_box_bytes = 0;
     if (tb <= kStageBoxBytes) {   // a warp's blocks (at most 4) within the default 48 KB of a CTA
       D.s_span = span;
