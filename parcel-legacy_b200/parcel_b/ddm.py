@@ -8,8 +8,9 @@ cells carry the unknowns.
 
 * ``solve`` / ``ddsolve``: one process's whole grid through parcel_b_solve_ddm /
   parcel_b_ddsolve_ddm (the GPU library), numpy arrays or CUDA tensors.
-* ``parcel_dcg_ddm`` / ``parcel_dgmres_ddm``: the argument lists of the reference's
-  parcel_dcg_ddm / parcel_dgmres_ddm (src/src_DDM/ddm_kernel.f90:2893-2986, 3082-3178) for a
+* ``parcel_dcg_ddm`` / ``parcel_dbicgstab_ddm`` / ``parcel_dgmres_ddm``: the argument lists of
+  the reference's parcel_dcg_ddm / parcel_dbicgstab_ddm / parcel_dgmres_ddm
+  (src/src_DDM/ddm_kernel.f90:2893-2986, 2988-3080, 3082-3178) for a
   box that is one of several processes' (torch.distributed, one process per GPU, ranks laid
   out as set_rank_xyz lays them out, src/example/ddm_setup.f90:52-60).  Every process
   numbers its interior cells box by box after the lower ranks' cells; a margin cell it
@@ -311,6 +312,15 @@ def parcel_dcg_ddm(x, b, m, nnd, offset, diaA, num_neighbor_ranks, neighbor_rank
     given, makes the local operator (parcel_b.dist's spmv / precon interface); the default is
     the GPU library with the process's boxes as its blocks."""
     return _distributed(1, x, b, m, nnd, offset, diaA, margin, ndim, npe_dim, n_grids, offset_dim, div_direc_th,
+                        ipreflag, itrmax, rtolmax, reshistory, precon_thblock, independ_nvec, group, boxes, backend)
+
+
+def parcel_dbicgstab_ddm(x, b, m, nnd, offset, diaA, num_neighbor_ranks, neighbor_ranks, margin, ndim, npe_dim,
+                         n_grids, offset_dim, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory,
+                         iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, *, group=None,
+                         boxes=BOXES_THREADS, backend=None):
+    """parcel_dbicgstab_ddm's argument list (ddm_kernel.f90:2988-3080) on torch.distributed."""
+    return _distributed(2, x, b, m, nnd, offset, diaA, margin, ndim, npe_dim, n_grids, offset_dim, div_direc_th,
                         ipreflag, itrmax, rtolmax, reshistory, precon_thblock, independ_nvec, group, boxes, backend)
 
 

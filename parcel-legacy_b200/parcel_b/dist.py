@@ -13,9 +13,10 @@ This mirrors the reference's MPI decomposition, which has no counterpart on one 
     summed in rank order, so every process takes the same branch and the result does not
     depend on message timing.
 
-The recurrences are those of KSP_pCG (src/pcg.f90:224-892) and KSP_pGMRES
-(src/pgmres.f90:62-525), including their iteration-count and return-code conventions,
-with every reduction replaced by the distributed dot.
+The recurrences are those of KSP_pCG (src/pcg.f90:224-892), KSP_pBiCG
+(src/pbicg.f90:280-698) and KSP_pGMRES (src/pgmres.f90:62-525), including their
+iteration-count and return-code conventions, with every reduction replaced by the
+distributed dot.
 
 Local operations (the product with halo values, the preconditioner) come from a backend
 with two methods, ``spmv(x_ext, y)`` and ``precon(r, z)``; the default, ``CudaLocal``, is
@@ -190,6 +191,47 @@ def _pcg(lay, op, b, x, itrmax, rtol, hist):
     return min(itrmax, itr), (1 if itrmax <= itr else 0)
 
 
+def _pbicg(lay, op, b, x, itrmax, rtol, hist):
+    """KSP_pBiCG (src/pbicg.f90:280-698): right-preconditioned BiCGStab, two products and two
+    preconditioner applications per iteration, every inner product a distributed dot."""
+    n = lay.n
+    xe = torch.zeros(lay.n_ext, dtype=torch.float64, device=b.device)
+    r = torch.empty_like(b)
+    q, pp, e, pe, v = (torch.zeros_like(b) for _ in range(5))
+    xe[:n] = x
+    lay.exchange(xe)
+    op.spmv(xe, q)
+    torch.sub(b, q, out=r)                     # calc_res
+    bnorm = math.sqrt(lay.dot(b, b))
+    rnorm = math.sqrt(lay.dot(r, r))
+    r0, p = r.clone(), r.clone()
+    c1 = lay.dot(r0, r0)
+    itr = 0
+    for itr in range(1, itrmax + 1):
+        hist[itr - 1] = rnorm / bnorm
+        op.precon(p, pp)                       # pp = M^-1 p
+        xe[:n] = pp
+        lay.exchange(xe)
+        op.spmv(xe, q)                         # q = A pp
+        c2 = lay.dot(r0, q)
+        alpha = c1 / c2
+        torch.add(r, q, alpha=-alpha, out=e)   # e = r - alpha q
+        op.precon(e, pe)                       # pe = M^-1 e
+        xe[:n] = pe
+        lay.exchange(xe)
+        op.spmv(xe, v)                         # v = A pe
+        c3 = lay.dot(e, v) / lay.dot(v, v)
+        x.add_(pp, alpha=alpha).add_(pe, alpha=c3)
+        torch.add(e, v, alpha=-c3, out=r)      # r = e - c3 v
+        c1 = lay.dot(r, r0)
+        rnorm = math.sqrt(lay.dot(r, r))
+        if rnorm / bnorm < rtol:
+            break
+        beta = c1 / (c3 * c2)
+        p.mul_(beta).add_(q, alpha=-beta * c3).add_(r)   # p = r - beta c3 q + beta p
+    return min(itrmax, itr), (1 if itrmax <= itr else 0)
+
+
 def _givens(m, h, i, c, s, e):
     """GivensRotations (src/pcagmres.f90:190-242) on column i (1-based) of h[(m+1) x m],
     with the reference's zero-diagonal guard h/1.0d0-300 (Fortran: (h/1) - 300)."""
@@ -306,7 +348,7 @@ class _Composed:
 def solve(layout: Layout, val, b: torch.Tensor, x: torch.Tensor, backend=None, **options):
     """Distributed solve of the rows this process owns.  b, x: this process's parts
     (float64 tensors on the backend's device; x is the initial guess and the result).
-    options: the parcel_b_input fields (solver 1 = CG, 3 = GMRES; ipreflag, ILU_method,
+    options: the parcel_b_input fields (solver 1 = CG, 2 = BiCGStab, 3 = GMRES; ipreflag, ILU_method,
     precon_thblock = block-Jacobi blocks of this process, itrmax, rtolmax, GMRES_m,
     GMRES_GSflag) and, for the default backend, blocks = explicit block-Jacobi row starts of
     this process.  Returns (niter, iret, reshistory)."""
@@ -330,12 +372,14 @@ def solve(layout: Layout, val, b: torch.Tensor, x: torch.Tensor, backend=None, *
     hist = np.zeros(max(itrmax, 1))
     if solver == 1:
         niter, iret = _pcg(layout, op, b, x, itrmax, rtol, hist)
+    elif solver == 2:
+        niter, iret = _pbicg(layout, op, b, x, itrmax, rtol, hist)
     elif solver == 3:
         m = int(options.get("GMRES_m", 4))
         m = m if m > 0 else 4
         niter, iret = _pgmres(layout, op, b, x, itrmax, rtol, hist, m, int(options.get("GMRES_GSflag", 1)) != 2)
     else:
-        raise ValueError(f"solver {solver}: the distributed path provides CG (1) and GMRES (3)")
+        raise ValueError(f"solver {solver}: the distributed path provides CG (1), BiCGStab (2) and GMRES (3)")
     return niter, iret, hist[:niter].copy()
 
 
@@ -345,6 +389,18 @@ def parcel_dcg(x, b, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU
     distributed matrix; returns (niter, iret)."""
     lay = Layout(n, gn, istart, crsRow_ptr, np.asarray(crsCol)[:nnz], group=group)
     niter, iret, h = solve(lay, np.asarray(crsA)[:nnz], b, x, solver=1, ipreflag=ipreflag, ILU_method=ILU_method,
+                           addL=addL, iflagAS=iflagAS,
+                           itrmax=itrmax, rtolmax=rtolmax, **extra)
+    reshistory[:len(h)] = h
+    return niter, iret
+
+
+def parcel_dbicgstab(x, b, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU_method, addL, iflagAS,
+                     itrmax, rtolmax, reshistory, group=None, **extra):
+    """parcel_dbicgstab's argument list (src/wrapper.f90:1813) for one process's rows of a
+    distributed matrix; returns (niter, iret)."""
+    lay = Layout(n, gn, istart, crsRow_ptr, np.asarray(crsCol)[:nnz], group=group)
+    niter, iret, h = solve(lay, np.asarray(crsA)[:nnz], b, x, solver=2, ipreflag=ipreflag, ILU_method=ILU_method,
                            addL=addL, iflagAS=iflagAS,
                            itrmax=itrmax, rtolmax=rtolmax, **extra)
     reshistory[:len(h)] = h

@@ -86,6 +86,8 @@ def _worker(rank, world, port, npe, solver, boxes, q, gn=GN, stencil="7"):
         kw = dict(boxes=boxes, backend=OracleLocal)
         if solver == 1:
             niter, iret = ddm.parcel_dcg_ddm(*args, **kw)
+        elif solver == 2:
+            niter, iret = ddm.parcel_dbicgstab_ddm(*args, **kw)
         else:
             niter, iret = ddm.parcel_dgmres_ddm(*args, 10, 1, **kw)
         q.put((rank, niter, iret, hist[:niter].copy(), x))
@@ -95,7 +97,8 @@ def _worker(rank, world, port, npe, solver, boxes, q, gn=GN, stencil="7"):
         q.put((rank, "error", traceback.format_exc(), None, None))
 
 
-@pytest.mark.parametrize("npe,solver,boxes", [((1, 2, 2), 1, 0), ((2, 2, 1), 3, 0), ((1, 2, 2), 1, 1)])
+@pytest.mark.parametrize("npe,solver,boxes", [((1, 2, 2), 1, 0), ((2, 2, 1), 3, 0), ((1, 2, 2), 1, 1),
+                                               ((2, 1, 2), 2, 1)])
 def test_ddm_over_processes_reproduces_the_global_solve(npe, solver, boxes):
     import ddm as oddm
     import oracle

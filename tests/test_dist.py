@@ -1,4 +1,5 @@
-"""The row-distributed solve (parcel_b/dist.py) on CPU processes over gloo.
+"""The row-distributed solve (parcel_b/dist.py) on CPU processes over gloo: CG, BiCGStab
+and GMRES.
 
 Two (and three) processes split the rows of a matrix contiguously at block-Jacobi block
 boundaries; each runs the distributed recurrences with a test backend: its local product
@@ -64,6 +65,8 @@ def _problem(kind):
         return A, b, dict(solver=1, itrmax=500, rtolmax=1e-9)
     A = problems.convdiff3d_upwind(12)
     b = problems.rhs_normal(A.n, 3)
+    if kind == "bicgstab":
+        return A, b, dict(solver=2, itrmax=500, rtolmax=1e-10)
     return A, b, dict(solver=3, itrmax=500, rtolmax=1e-10, GMRES_m=10, GMRES_GSflag=1)
 
 
@@ -106,7 +109,7 @@ def _run(kind, world, nblocks):
     return sorted(out, key=lambda o: o[0])
 
 
-@pytest.mark.parametrize("kind,world", [("cg", 2), ("gmres", 2), ("gmres", 3)])
+@pytest.mark.parametrize("kind,world", [("cg", 2), ("bicgstab", 2), ("bicgstab", 3), ("gmres", 2), ("gmres", 3)])
 def test_distributed_solve_reproduces_single_process_history(kind, world):
     import oracle
     nblocks = 2 * world

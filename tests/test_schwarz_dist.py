@@ -7,9 +7,9 @@ block-Jacobi operator of the expanded matrix from the oracle.  Checked against t
 global restatement (oracle/schwarz.py):
   * the application, for BASIC, RESTRICT, INTERPOLATE and NONE, ILUD and MLUD, to 1e-12
     relative (a row is covered by at most two regions, so the sums agree to rounding);
-  * CG and GMRES through it: the same iteration counts and histories (1e-8 relative while the
-    residual is above 1e-8 of its start) as the same recurrences on one process with the
-    oracle's global preconditioner;
+  * CG, BiCGStab and GMRES through it: the same iteration counts and histories (1e-8
+    relative while the residual is above 1e-8 of its start) as the same recurrences on one
+    process with the oracle's global preconditioner;
   * the reference's fallbacks: block Jacobi on one process, and for every process when a
     block is shorter than 2 addL rows."""
 import multiprocessing as mp
@@ -69,6 +69,9 @@ class ScipySpmv:
         y.copy_(self.torch.from_numpy(self.A @ x_ext.numpy()))
 
 
+SOLVER = {"cg": 1, "bicgstab": 2, "gmres": 3}
+
+
 def _split(n, world):
     per = n // world
     return [(r * per, per if r < world - 1 else n - per * (world - 1)) for r in range(world)]
@@ -99,7 +102,7 @@ def _worker(rank, world, port, kind, nb, addL, iflag, ilu, solve, q):
         if solve:
             x = torch.zeros(n, dtype=torch.float64)
             be = pdist._Composed(ScipySpmv(lay, val), P)
-            kw = dict(solver=1 if kind == "cg" else 3, itrmax=400, rtolmax=1e-10, GMRES_m=10, GMRES_GSflag=1)
+            kw = dict(solver=SOLVER[kind], itrmax=400, rtolmax=1e-10, GMRES_m=10, GMRES_GSflag=1)
             niter, iret, hist = pdist.solve(lay, val, torch.from_numpy(b[lo:lo + n].copy()), x, backend=be, **kw)
             out.update(niter=niter, iret=iret, hist=hist, x=x.numpy())
         q.put((rank, out))
@@ -175,7 +178,7 @@ class _GlobalSchwarz:
         z.copy_(self.torch.from_numpy(schwarz.apply(A, ranges, nb, addL, iflag, r.numpy(), ILU_method=self.ilu)))
 
 
-@pytest.mark.parametrize("kind,world,iflag", [("cg", 2, 1), ("gmres", 3, 2), ("gmres", 2, 3)])
+@pytest.mark.parametrize("kind,world,iflag", [("cg", 2, 1), ("gmres", 3, 2), ("gmres", 2, 3), ("bicgstab", 2, 4)])
 def test_distributed_schwarz_solves_reproduce_the_global_recurrences(kind, world, iflag):
     import torch
     import torch.distributed as dist
@@ -189,7 +192,7 @@ def test_distributed_schwarz_solves_reproduce_the_global_recurrences(kind, world
         lay = pdist.Layout(A.n, A.n, 1, A.rowptr, A.col)
         x = torch.zeros(A.n, dtype=torch.float64)
         be = _GlobalSchwarz(A, _split(A.n, world), nb, addL, iflag, 1)
-        kw = dict(solver=1 if kind == "cg" else 3, itrmax=400, rtolmax=1e-10, GMRES_m=10, GMRES_GSflag=1)
+        kw = dict(solver=SOLVER[kind], itrmax=400, rtolmax=1e-10, GMRES_m=10, GMRES_GSflag=1)
         no, io, ho = pdist.solve(lay, A.val, torch.from_numpy(b.copy()), x, backend=be, **kw)
     finally:
         dist.destroy_process_group()
