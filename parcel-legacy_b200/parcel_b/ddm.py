@@ -8,9 +8,9 @@ cells carry the unknowns.
 
 * ``solve`` / ``ddsolve``: one process's whole grid through parcel_b_solve_ddm /
   parcel_b_ddsolve_ddm (the GPU library), numpy arrays or CUDA tensors.
-* ``parcel_dcg_ddm`` / ``parcel_dbicgstab_ddm`` / ``parcel_dgmres_ddm``: the argument lists of
-  the reference's parcel_dcg_ddm / parcel_dbicgstab_ddm / parcel_dgmres_ddm
-  (src/src_DDM/ddm_kernel.f90:2893-2986, 2988-3080, 3082-3178) for a
+* ``parcel_dcg_ddm`` / ``parcel_dbicgstab_ddm`` / ``parcel_dgmres_ddm`` /
+  ``parcel_dcagmres_ddm``: the argument lists of the reference's functions of those names
+  (src/src_DDM/ddm_kernel.f90:2893-2986, 2988-3080, 3082-3178, 3180-3279) for a
   box that is one of several processes' (torch.distributed, one process per GPU, ranks laid
   out as set_rank_xyz lays them out, src/example/ddm_setup.f90:52-60).  Every process
   numbers its interior cells box by box after the lower ranks' cells; a margin cell it
@@ -332,3 +332,14 @@ def parcel_dgmres_ddm(x, b, m, nnd, offset, diaA, num_neighbor_ranks, neighbor_r
     return _distributed(3, x, b, m, nnd, offset, diaA, margin, ndim, npe_dim, n_grids, offset_dim, div_direc_th,
                         ipreflag, itrmax, rtolmax, reshistory, precon_thblock, independ_nvec, group, boxes, backend,
                         GMRES_m=restart, GMRES_GSflag=GMRES_GSflag)
+
+
+def parcel_dcagmres_ddm(x, b, m, nnd, offset, diaA, num_neighbor_ranks, neighbor_ranks, margin, ndim, npe_dim,
+                        n_grids, offset_dim, div_direc_th, ipreflag, addL, iflagAS, itrmax, rtolmax, reshistory,
+                        iovlflag, precon_thblock, Neuman_itr, independ_nvec, nBlock, CAGMRES_sstep, CAGMRES_tstep,
+                        CAGMRES_basis, CAGMRES_QRflag, *, group=None, boxes=BOXES_THREADS, backend=None):
+    """parcel_dcagmres_ddm's argument list (ddm_kernel.f90:3180-3279) on torch.distributed."""
+    return _distributed(4, x, b, m, nnd, offset, diaA, margin, ndim, npe_dim, n_grids, offset_dim, div_direc_th,
+                        ipreflag, itrmax, rtolmax, reshistory, precon_thblock, independ_nvec, group, boxes, backend,
+                        CAGMRES_sstep=CAGMRES_sstep, CAGMRES_tstep=CAGMRES_tstep, CAGMRES_basis=CAGMRES_basis,
+                        CAGMRES_QRflag=CAGMRES_QRflag)

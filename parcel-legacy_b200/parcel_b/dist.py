@@ -14,9 +14,10 @@ This mirrors the reference's MPI decomposition, which has no counterpart on one 
     depend on message timing.
 
 The recurrences are those of KSP_pCG (src/pcg.f90:224-892), KSP_pBiCG
-(src/pbicg.f90:280-698) and KSP_pGMRES (src/pgmres.f90:62-525), including their
-iteration-count and return-code conventions, with every reduction replaced by the
-distributed dot.
+(src/pbicg.f90:280-698), KSP_pGMRES (src/pgmres.f90:62-525) and KSP_pCAGMRES
+(src/pcagmres.f90:1557-2518), including their iteration-count and return-code conventions,
+with every reduction replaced by a distributed one (CA-GMRES reduces a block's Gram and
+projection matrices in one message).
 
 Local operations (the product with halo values, the preconditioner) come from a backend
 with two methods, ``spmv(x_ext, y)`` and ``precon(r, z)``; the default, ``CudaLocal``, is
@@ -348,7 +349,8 @@ class _Composed:
 def solve(layout: Layout, val, b: torch.Tensor, x: torch.Tensor, backend=None, **options):
     """Distributed solve of the rows this process owns.  b, x: this process's parts
     (float64 tensors on the backend's device; x is the initial guess and the result).
-    options: the parcel_b_input fields (solver 1 = CG, 2 = BiCGStab, 3 = GMRES; ipreflag, ILU_method,
+    options: the parcel_b_input fields (solver 1 = CG, 2 = BiCGStab, 3 = GMRES, 4 = CA-GMRES with
+    CAGMRES_sstep / tstep / basis / QRflag; ipreflag, ILU_method,
     precon_thblock = block-Jacobi blocks of this process, itrmax, rtolmax, GMRES_m,
     GMRES_GSflag) and, for the default backend, blocks = explicit block-Jacobi row starts of
     this process.  Returns (niter, iret, reshistory)."""
@@ -369,18 +371,280 @@ def solve(layout: Layout, val, b: torch.Tensor, x: torch.Tensor, backend=None, *
         op = _Composed(base, prec)
     else:
         op = CudaLocal(layout, val, options)
-    hist = np.zeros(max(itrmax, 1))
+    hist = np.zeros(max(itrmax, 1) + 2)
     if solver == 1:
         niter, iret = _pcg(layout, op, b, x, itrmax, rtol, hist)
     elif solver == 2:
         niter, iret = _pbicg(layout, op, b, x, itrmax, rtol, hist)
+    elif solver == 4:
+        def opt(name, default, lo):
+            v = int(options.get(name, -1))
+            return v if v >= lo else default
+        niter, iret = _pcagmres(layout, op, b, x, itrmax, rtol, hist, opt("CAGMRES_sstep", 4, 1),
+                                opt("CAGMRES_tstep", 1, 1), opt("CAGMRES_basis", BASIS_MONOMIAL, 0),
+                                opt("CAGMRES_QRflag", QR_CHOLQR, 1))
     elif solver == 3:
         m = int(options.get("GMRES_m", 4))
         m = m if m > 0 else 4
         niter, iret = _pgmres(layout, op, b, x, itrmax, rtol, hist, m, int(options.get("GMRES_GSflag", 1)) != 2)
     else:
-        raise ValueError(f"solver {solver}: the distributed path provides CG (1), BiCGStab (2) and GMRES (3)")
+        raise ValueError(f"solver {solver}: the distributed path provides CG (1), BiCGStab (2), GMRES (3) and "
+                         "CA-GMRES (4)")
     return niter, iret, hist[:niter].copy()
+
+
+# ---------------------------------------------------------------- CA-GMRES(s, t)
+QR_MGS, QR_CGS, QR_TSQR, QR_CHOLQR, QR_CHOLQR2 = 1, 2, 3, 4, 5
+BASIS_MONOMIAL, BASIS_NEWTON = 0, 1
+
+
+def _sum_ranks(lay, loc: torch.Tensor) -> np.ndarray:
+    """A small local array summed over the processes, elementwise, in rank order."""
+    loc = loc.reshape(-1).to(torch.float64).contiguous()
+    parts = [torch.empty_like(loc) for _ in range(lay.world)]
+    dist.all_gather(parts, loc, group=lay.group)
+    out = np.zeros(loc.numel())
+    for t in parts:
+        out = out + t.cpu().numpy()
+    return out
+
+
+def _gram(lay, A: torch.Tensor, B: torch.Tensor) -> np.ndarray:
+    """A B^T over the global rows (the panels hold one vector per row): the block inner
+    products of calc_gemm_dot (src/pcagmres.f90:1052-1080)."""
+    return _sum_ranks(lay, A @ B.T).reshape(A.shape[0], B.shape[0])
+
+
+def _chol_upper(G):
+    """Upper Cholesky factor R (G = R^T R), or None when G is not numerically positive definite."""
+    try:
+        return np.linalg.cholesky(G).T
+    except np.linalg.LinAlgError:
+        return None
+
+
+def _trinv_upper(R):
+    return np.triu(np.linalg.inv(np.triu(R)))
+
+
+def _times_rinv(W: torch.Tensor, Rinv) -> torch.Tensor:
+    """The panel W R^-1 (calcQ_VRinv_), one vector per row."""
+    return torch.from_numpy(np.ascontiguousarray(Rinv.T)).to(W) @ W
+
+
+def _qr_r(lay, W: torch.Tensor, flag: int):
+    """R-only QR of the global panel W (QRDecomposition_, src/QRDecomposition.f90:1331-1552):
+    Cholesky QR or Cholesky QR2 from the distributed Gram matrix, falling back to TSQR when it
+    is not numerically positive definite; TSQR (also for the MGS / CGS flags, as on one
+    process) as the R of every process's local R factors stacked in rank order, the rows
+    signed to a positive diagonal (TSQR_Ronly_)."""
+    c = W.shape[0]
+    if flag in (QR_CHOLQR, QR_CHOLQR2):
+        R1 = _chol_upper(_gram(lay, W, W))
+        if R1 is not None:
+            if flag == QR_CHOLQR:
+                return R1
+            Q1 = _times_rinv(W, _trinv_upper(R1))
+            R2 = _chol_upper(_gram(lay, Q1, Q1))
+            if R2 is not None:
+                return R2 @ R1
+    loc = torch.linalg.qr(W.T, mode="r").R
+    Rl = torch.zeros((c, c), dtype=torch.float64, device=W.device)
+    Rl[:loc.shape[0]] = loc
+    parts = [torch.empty_like(Rl) for _ in range(lay.world)]
+    dist.all_gather(parts, Rl.contiguous(), group=lay.group)
+    R = np.linalg.qr(np.concatenate([t.cpu().numpy() for t in parts]), mode="r")
+    return R * np.where(np.diag(R) < 0.0, -1.0, 1.0)[:, None]
+
+
+def _newton_basis(s, B1, er, ei):
+    """calc_NewtonBasis (src/pcagmres.f90:586-611): the shifts on B1's diagonal; a complex
+    pair (real, +-imaginary) as a 2 x 2 real block."""
+    i = 1
+    while i <= s:
+        B1[i - 1, i - 1] = er[i - 1]
+        if i < s and ei[i - 1] != 0.0:
+            B1[i, i] = er[i - 1]
+            B1[i - 1, i] = -ei[i - 1] * ei[i - 1]
+            i += 1
+        i += 1
+
+
+def _leja(er, ei):
+    """modified_leja_ordering (src/LejaOrdering.f90:100-322): the Ritz values sorted by
+    decreasing modulus, then picked one by one (a complex pair together) to maximise the
+    product of distances to those already picked, the values rescaled at every step by the
+    growth of that product (the capacity estimate C) and scaled back at the end."""
+    n = len(er)
+    er, ei = [float(v) for v in er], [float(v) for v in ei]
+    mod = lambda j: math.sqrt(er[j] ** 2 + ei[j] ** 2)
+    for i in range(1, n):                        # stable insertion sort, largest modulus first
+        j = i
+        while j > 0 and mod(j - 1) < mod(j):
+            er[j], er[j - 1], ei[j], ei[j - 1] = er[j - 1], er[j], ei[j - 1], ei[j]
+            j -= 1
+    mu = [1.0] * n
+    ptmp = [1.0] * n
+    tr, ti, picked = [0.0] * n, [0.0] * n, [0] * n
+    if ei[0] > 0.0:
+        tr[0], ti[0], tr[1], ti[1] = er[0], ei[0], er[1], ei[1]
+        picked[0], picked[1] = 0, 1
+        L = 2
+    else:
+        tr[0], ti[0], picked[0] = er[0], 0.0, 0
+        L = 1
+    C = 1.0
+    while L < n:
+        c_old = C
+        for j in range(L - 1):
+            ptmp[j + 1] = math.sqrt((tr[L - 1] - tr[j]) ** 2 + (ti[L - 1] - ti[j]) ** 2) ** (mu[picked[j]] / L)
+        C = 1.0
+        for v in ptmp:
+            C = C * v
+        f = C / c_old
+        for j in range(n):
+            er[j], ei[j], tr[j], ti[j] = er[j] / f, ei[j] / f, tr[j] / f, ti[j] / f
+        score = [0.0] * n
+        for j in range(n):
+            if j not in picked[:L]:
+                dists = [math.sqrt((er[j] - tr[q]) ** 2 + (ei[j] - ti[q]) ** 2) ** mu[picked[q]] for q in range(L - 1)]
+                prod = 1.0
+                for v in dists:
+                    prod = prod * v
+                score[j] = prod
+        k = max(range(n), key=lambda j: (abs(score[j]), -j))
+        if abs(ei[k]) > 0.0:
+            a, z = (k - 1, k) if ei[k] < 0.0 else (k, k + 1)
+            tr[L], ti[L], tr[L + 1], ti[L + 1] = er[a], ei[a], er[z], ei[z]
+            picked[L], picked[L + 1] = a, z
+            L += 2
+        else:
+            tr[L], ti[L], picked[L] = er[k], 0.0, k
+            L += 1
+    return np.array([v * C for v in tr]), np.array([v * C for v in ti])
+
+
+def _hessenberg_update(s, k, B1, H, R1, Rk, BRup, hk_pre):
+    """calc_HessenbergMatrix (src/pcagmres.f90:879-1052): block k's columns of H from its R
+    factor, the change-of-basis matrix B1 and the projections BRup on the earlier basis.
+    Returns the new subdiagonal entry hk."""
+    if k == 1:
+        H[: s + 1, :s] = (R1 @ B1) @ _trinv_upper(R1[:s, :s])
+        return H[s, s - 1]
+    s1 = s * (k - 1)
+    Rt = np.zeros((s + 1, s + 1))
+    Rt[0, :] = BRup[s1, :]
+    Rt[1:, 1:] = Rk
+    BRu, BR = BRup[:s1, :], BRup[:s1, :s]
+    Rinv = _trinv_upper(Rt[:s, :s])
+    H[:s1, s1:s1 + s] = (-(H[:s1, :s1] @ BR) + (BRu @ B1)) @ Rinv
+    bk = B1[s, s - 1]
+    hk = Rt[s, s] / Rt[s - 1, s - 1] * bk
+    H[s * k, s * k - 1] = hk
+    Hss = (Rt[:s, :s] @ B1[:s, :s]) @ Rinv
+    Hss[:, s - 1] = Hss[:, s - 1] + bk / Rt[s - 1, s - 1] * Rt[:s, s]
+    e1 = np.zeros((s, s))
+    e1[0, :] = BR[s1 - 1, :] * hk_pre
+    H[s1:s1 + s, s1:s1 + s] = Hss - e1 @ Rinv
+    return hk
+
+
+def _pcagmres(lay, op, b, x, itrmax, rtol, hist, s, t, basis, qrflag):
+    """KSP_pCAGMRES (src/pcagmres.f90:1557-2518): CA-GMRES(s, t), right preconditioned; per
+    block s preconditioned products (monomial, or Newton with Leja-ordered Ritz shifts from
+    the second block on), a block Gram-Schmidt against the earlier blocks and an R-only QR,
+    all inner products of a block in one distributed reduction."""
+    n = lay.n
+    st = s * t
+    xe = torch.zeros(lay.n_ext, dtype=torch.float64, device=b.device)
+    q, pv, w, z = (torch.empty_like(b) for _ in range(4))
+    B1 = np.zeros((s + 1, s))
+    for i in range(s):
+        B1[i + 1, i] = 1.0
+    er, ei = np.zeros(st), np.zeros(st)
+    bnorm = math.sqrt(lay.dot(b, b))
+    exit_now, newton_on = False, False
+    itr0, itr = 0, 1
+    while itr <= itrmax:
+        itr0 = itr
+        co, si, ze = np.zeros(st + 1), np.zeros(st + 1), np.zeros(st + 1)
+        H, Hg = np.zeros((st + 1, st)), np.zeros((st + 1, st))
+        hk_pre = 0.0
+        xe[:n] = x
+        lay.exchange(xe)
+        op.spmv(xe, q)
+        r = b - q
+        rnorm = math.sqrt(lay.dot(r, r))
+        if rnorm / bnorm < rtol:
+            break
+        if itr == 1:
+            hist[0] = rnorm / bnorm
+        ze[0] = -rnorm
+        V = torch.zeros((s + 1, n), dtype=torch.float64, device=b.device)
+        Q = torch.zeros((st + 1, n), dtype=torch.float64, device=b.device)
+        V[0] = (-1.0 / rnorm) * r
+        mm = 0
+        R1 = Rk = BRup = None
+        for k in range(1, t + 1):
+            if basis == BASIS_NEWTON and newton_on:
+                _newton_basis(s, B1, er, ei)
+            for i in range(1, s + 1):                  # the basis: V_i = (A M^-1 - shift) V_{i-1}
+                op.precon(V[i - 1], pv)
+                xe[:n] = pv
+                lay.exchange(xe)
+                op.spmv(xe, w)
+                if basis == BASIS_NEWTON and newton_on:     # calc_NewtonBasisVec (pcagmres.f90:1480-1552)
+                    if i != 1:
+                        w = (-B1[i - 1, i - 1]) * V[i - 1] + (-B1[i - 2, i - 1]) * V[i - 2] + w
+                    else:
+                        w = (-B1[i - 1, i - 1]) * V[i - 1] + w
+                V[i] = w
+            if k == 1:
+                R1 = _qr_r(lay, V, qrflag)
+                Q[: s + 1] = _times_rinv(V, _trinv_upper(R1))
+            else:
+                s1 = s * (k - 1) + 1
+                BRup = _gram(lay, Q[:s1], V)           # block Gram-Schmidt against the earlier Q
+                for c in range(1, s + 1):
+                    for j in range(s1):
+                        V[c] = V[c] - Q[j] * BRup[j, c]
+                Rk = _qr_r(lay, V[1:], qrflag)
+                Q[s1:s1 + s] = _times_rinv(V[1:], _trinv_upper(Rk))
+            hk_pre = _hessenberg_update(s, k, B1, H, R1, Rk, BRup, hk_pre)
+            if k != t:
+                V = torch.zeros((s + 1, n), dtype=torch.float64, device=b.device)
+                V[0] = Q[s * k]
+            Hg[:, s * (k - 1):s * k] = H[:, s * (k - 1):s * k]
+            for i in range(s * (k - 1) + 1, s * k + 1):
+                mm = i
+                _givens(st, Hg, i, co, si, ze)
+                rnorm = abs(ze[i])
+                itr0 = i + itr
+                hist[itr0 - 1] = rnorm / bnorm
+                if rnorm / bnorm < rtol or i + itr == itrmax:
+                    exit_now = True
+                    break
+            if exit_now:
+                break
+            if basis == BASIS_NEWTON:
+                newton_on = True
+                ev = np.linalg.eigvals(H[: s * k, : s * k])
+                er[: s * k], ei[: s * k] = _leja(ev.real, ev.imag)
+        # update_xVec: y = Hg^-1 ze over the mm columns, x += M^-1 Q y
+        y = np.zeros(mm)
+        for i in range(mm, 0, -1):
+            v = ze[i - 1]
+            for j in range(mm, i, -1):
+                v = v - Hg[i - 1, j - 1] * y[j - 1]
+            d = Hg[i - 1, i - 1]
+            y[i - 1] = v / 1.0e-300 if d == 0.0 else v / d
+        v0 = torch.from_numpy(y).to(Q) @ Q[:mm]
+        op.precon(v0, z)
+        x.add_(z)
+        if exit_now:
+            break
+        itr += st
+    return min(itrmax, itr0), (1 if itrmax <= itr else 0)
 
 
 def parcel_dcg(x, b, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU_method, addL, iflagAS, itrmax,
@@ -415,5 +679,19 @@ def parcel_dgmres(x, b, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, 
     niter, iret, h = solve(lay, np.asarray(crsA)[:nnz], b, x, solver=3, ipreflag=ipreflag, ILU_method=ILU_method,
                            addL=addL, iflagAS=iflagAS,
                            itrmax=itrmax, rtolmax=rtolmax, GMRES_m=GMRES_m, GMRES_GSflag=GMRES_GSflag, **extra)
+    reshistory[:len(h)] = h
+    return niter, iret
+
+
+def parcel_dcagmres(x, b, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag, ILU_method, addL, iflagAS,
+                    itrmax, rtolmax, reshistory, CAGMRES_sstep, CAGMRES_tstep, CAGMRES_basis, CAGMRES_QRflag,
+                    group=None, **extra):
+    """parcel_dcagmres's argument list (src/wrapper.f90:2807) for one process's rows of a
+    distributed matrix; returns (niter, iret)."""
+    lay = Layout(n, gn, istart, crsRow_ptr, np.asarray(crsCol)[:nnz], group=group)
+    niter, iret, h = solve(lay, np.asarray(crsA)[:nnz], b, x, solver=4, ipreflag=ipreflag, ILU_method=ILU_method,
+                           addL=addL, iflagAS=iflagAS, itrmax=itrmax, rtolmax=rtolmax, CAGMRES_sstep=CAGMRES_sstep,
+                           CAGMRES_tstep=CAGMRES_tstep, CAGMRES_basis=CAGMRES_basis, CAGMRES_QRflag=CAGMRES_QRflag,
+                           **extra)
     reshistory[:len(h)] = h
     return niter, iret

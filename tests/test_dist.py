@@ -67,6 +67,10 @@ def _problem(kind):
     b = problems.rhs_normal(A.n, 3)
     if kind == "bicgstab":
         return A, b, dict(solver=2, itrmax=500, rtolmax=1e-10)
+    if kind.startswith("cagmres"):   # cagmres-s-t-basis-qr
+        _, sst, tst, bas, qr = kind.split("-")
+        return A, b, dict(solver=4, itrmax=500, rtolmax=1e-10, CAGMRES_sstep=int(sst), CAGMRES_tstep=int(tst),
+                          CAGMRES_basis=int(bas), CAGMRES_QRflag=int(qr))
     return A, b, dict(solver=3, itrmax=500, rtolmax=1e-10, GMRES_m=10, GMRES_GSflag=1)
 
 
@@ -125,3 +129,29 @@ def test_distributed_solve_reproduces_single_process_history(kind, world):
         assert nhalo > 0
     x = np.concatenate([o[4] for o in out])
     assert np.max(np.abs(x - xo)) <= 1e-8 * np.max(np.abs(xo))
+
+
+@pytest.mark.parametrize("kind,world", [("cagmres-4-1-0-4", 2), ("cagmres-4-2-0-5", 3), ("cagmres-2-4-0-3", 2),
+                                        ("cagmres-4-3-1-5", 2), ("cagmres-8-2-1-3", 3)])
+def test_distributed_cagmres_reproduces_the_oracle(kind, world):
+    """CA-GMRES(s, t) over processes (monomial and Newton bases; Cholesky QR, Cholesky QR2 and
+    TSQR) against the oracle's CA-GMRES on one process, at its parity criteria: iterations
+    within 2, histories within 1e-6 above 1e-8, and the final true residual."""
+    import cagmres
+    import oracle
+    nblocks = 2 * world
+    A, b, kw = _problem(kind)
+    if A.n % world or (A.n // world) % (nblocks // world):
+        pytest.skip("rows do not split evenly")
+    xo, ho, no, io = cagmres.pcagmres(A, b, s=kw["CAGMRES_sstep"], t=kw["CAGMRES_tstep"], basis=kw["CAGMRES_basis"],
+                                      qrflag=kw["CAGMRES_QRflag"], itrmax=kw["itrmax"], rtolmax=kw["rtolmax"],
+                                      ipreflag=2, ILU_method=0, precon_thblock=nblocks)
+    out = _run(kind, world, nblocks)
+    x = np.concatenate([o[4] for o in out])
+    for rank, niter, iret, hist, _, nhalo in out:
+        assert iret == io == 0 and abs(niter - no) <= 2, (rank, niter, no)
+        k = min(len(ho), len(hist))
+        m = ho[:k] > 1e-8
+        assert np.max(np.abs(hist[:k][m] - ho[:k][m]) / ho[:k][m]) < 1e-6
+        assert nhalo > 0
+    assert oracle.true_relres(A, b, x) < 1e-9
