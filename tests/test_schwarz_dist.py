@@ -7,9 +7,9 @@ block-Jacobi operator of the expanded matrix from the oracle.  Checked against t
 global restatement (oracle/schwarz.py):
   * the application, for BASIC, RESTRICT, INTERPOLATE and NONE, ILUD and MLUD, to 1e-12
     relative (a row is covered by at most two regions, so the sums agree to rounding);
-  * CG, BiCGStab and GMRES through it: the same iteration counts and histories (1e-8
-    relative while the residual is above 1e-8 of its start) as the same recurrences on one
-    process with the oracle's global preconditioner;
+  * CG, BiCGStab, GMRES and CA-GMRES through it: the same iteration counts and histories
+    (1e-8 relative while the residual is above 1e-8 of its start) as the same recurrences on
+    one process with the oracle's global preconditioner;
   * the reference's fallbacks: block Jacobi on one process, and for every process when a
     block is shorter than 2 addL rows."""
 import multiprocessing as mp
@@ -69,7 +69,7 @@ class ScipySpmv:
         y.copy_(self.torch.from_numpy(self.A @ x_ext.numpy()))
 
 
-SOLVER = {"cg": 1, "bicgstab": 2, "gmres": 3}
+SOLVER = {"cg": 1, "bicgstab": 2, "gmres": 3, "cagmres": 4}   # CA-GMRES: s = 4, t = 1, Cholesky QR
 
 
 def _split(n, world):
@@ -178,7 +178,8 @@ class _GlobalSchwarz:
         z.copy_(self.torch.from_numpy(schwarz.apply(A, ranges, nb, addL, iflag, r.numpy(), ILU_method=self.ilu)))
 
 
-@pytest.mark.parametrize("kind,world,iflag", [("cg", 2, 1), ("gmres", 3, 2), ("gmres", 2, 3), ("bicgstab", 2, 4)])
+@pytest.mark.parametrize("kind,world,iflag", [("cg", 2, 1), ("gmres", 3, 2), ("gmres", 2, 3), ("bicgstab", 2, 4),
+                                               ("cagmres", 3, 1)])
 def test_distributed_schwarz_solves_reproduce_the_global_recurrences(kind, world, iflag):
     import torch
     import torch.distributed as dist
