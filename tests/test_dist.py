@@ -155,3 +155,37 @@ def test_distributed_cagmres_reproduces_the_oracle(kind, world):
         assert np.max(np.abs(hist[:k][m] - ho[:k][m]) / ho[:k][m]) < 1e-6
         assert nhalo > 0
     assert oracle.true_relres(A, b, x) < 1e-9
+
+
+def test_cagmres_dense_steps_match_the_oracle():
+    """The distributed CA-GMRES's host steps (Leja ordering of Ritz values with complex pairs,
+    Newton change-of-basis matrix, Hessenberg block update) against the oracle's on random
+    inputs."""
+    import cagmres
+
+    from parcel_b import dist as pdist
+    rng = np.random.default_rng(11)
+    for trial in range(20):
+        s = int(rng.integers(2, 9))
+        H = rng.standard_normal((s, s))
+        ev = np.linalg.eigvals(H)
+        a = pdist._leja(ev.real, ev.imag)
+        b = cagmres.leja(ev.real, ev.imag)
+        assert np.allclose(a[0], b[0], rtol=1e-13, atol=0) and np.allclose(a[1], b[1], rtol=1e-13, atol=0), trial
+        B1a, B1b = np.zeros((s + 1, s)), np.zeros((s + 1, s))
+        for i in range(s):
+            B1a[i + 1, i] = B1b[i + 1, i] = 1.0
+        pdist._newton_basis(s, B1a, a[0], a[1])
+        cagmres.newton_basis(s, B1b, b[0], b[1])
+        assert np.array_equal(B1a, B1b)
+        # Hessenberg blocks k = 1 and k = 2 from random triangular factors
+        t = 2
+        R1 = np.triu(rng.standard_normal((s + 1, s + 1))) + 3 * np.eye(s + 1)
+        Rk = np.triu(rng.standard_normal((s, s))) + 3 * np.eye(s)
+        BRup = rng.standard_normal((s + 1, s + 1))
+        Ha, Hb = np.zeros((s * t + 1, s * t)), np.zeros((s * t + 1, s * t))
+        ha = pdist._hessenberg_update(s, 1, B1a, Ha, R1, None, None, 0.0)
+        hb = cagmres.hessenberg_update(s, t, 1, B1b, Hb, R1, None, None, 0.0)
+        ha = pdist._hessenberg_update(s, 2, B1a, Ha, R1, Rk, BRup, ha)
+        hb = cagmres.hessenberg_update(s, t, 2, B1b, Hb, R1, Rk, BRup, hb)
+        assert np.allclose(Ha, Hb, rtol=1e-12, atol=1e-12 * np.abs(Hb).max()) and np.isclose(ha, hb, rtol=1e-13)
