@@ -695,3 +695,78 @@ def parcel_dcagmres(x, b, n, gn, nnz, istart, crsA, crsRow_ptr, crsCol, ipreflag
                            **extra)
     reshistory[:len(h)] = h
     return niter, iret
+
+
+# ---------------------------------------------------------------- DIA rows over processes
+def dia_rows(n, gn, istart, diaA, offset, nnd):
+    """This process's rows of a DIA matrix as CRS with 1-based global columns.
+
+    PARCEL_KSP_DIA's layout (src/wrapper.f90, src/krylov.f90:845-905): diaA(k + (j-1) n) is
+    the entry of global row istart + k - 1 in column row + offset(j); the matrix holds the
+    entries of magnitude above zero (get_nnz_dia / dia2crs, src/matrix.f90:7536-7607).  Each
+    row's columns come out ascending (the diagonals walked in ascending offset order), a
+    column owned by another process becomes a halo column, and a column outside 1..gn (which
+    no process owns) is left out.  Returns (rowptr 1-based, col, val)."""
+    off = np.asarray(_host_array(offset), dtype=np.int64)[:nnd]
+    if len(np.unique(off)) != len(off):
+        raise ValueError("a DIA offset appears twice")
+    D = np.asarray(_host_array(diaA), dtype=np.float64)[: nnd * n].reshape(nnd, n)
+    order = np.argsort(off, kind="stable")
+    rows = np.arange(n, dtype=np.int64) + int(istart)
+    cols = (rows[None, :] + off[order][:, None]).T            # (n, nnd): row k, ascending offset
+    vals = D[order].T
+    keep = (np.abs(vals) > 0.0) & (cols >= 1) & (cols <= gn)
+    rowptr = np.concatenate([[1], 1 + np.cumsum(keep.sum(axis=1))]).astype(np.int32)
+    return rowptr, cols[keep].astype(np.int32), vals[keep]
+
+
+def _host_array(a):
+    return a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)
+
+
+def _dia_solve(solver, x, b, n, gn, istart, diaA, offset, nnd, reshistory, group, options):
+    """options["backend"], when given, makes the local operator: backend(layout, val,
+    options) (the GPU library's by default)."""
+    rowptr, col, val = dia_rows(n, gn, istart, diaA, offset, nnd)
+    lay = Layout(n, gn, istart, rowptr, col, group=group)
+    make = options.pop("backend", None)
+    op = make(lay, val, options) if make is not None else None
+    niter, iret, h = solve(lay, val, b, x, backend=op, solver=solver, **options)
+    reshistory[:len(h)] = h
+    return niter, iret
+
+
+def parcel_dcg_dia(x, b, n, gn, istart, diaA, offset, nnd, ipreflag, ILU_method, addL, iflagAS, itrmax, rtolmax,
+                   reshistory, group=None, **extra):
+    """parcel_dcg_dia's argument list (src/wrapper.f90:635) for one process's rows of a
+    distributed DIA matrix; returns (niter, iret)."""
+    return _dia_solve(1, x, b, n, gn, istart, diaA, offset, nnd, reshistory, group,
+                      dict(extra, ipreflag=ipreflag, ILU_method=ILU_method, addL=addL, iflagAS=iflagAS,
+                           itrmax=itrmax, rtolmax=rtolmax))
+
+
+def parcel_dbicgstab_dia(x, b, n, gn, istart, diaA, offset, nnd, ipreflag, ILU_method, addL, iflagAS, itrmax,
+                         rtolmax, reshistory, group=None, **extra):
+    """parcel_dbicgstab_dia's argument list (src/wrapper.f90:454); returns (niter, iret)."""
+    return _dia_solve(2, x, b, n, gn, istart, diaA, offset, nnd, reshistory, group,
+                      dict(extra, ipreflag=ipreflag, ILU_method=ILU_method, addL=addL, iflagAS=iflagAS,
+                           itrmax=itrmax, rtolmax=rtolmax))
+
+
+def parcel_dgmres_dia(x, b, n, gn, istart, diaA, offset, nnd, ipreflag, ILU_method, addL, iflagAS, itrmax, rtolmax,
+                      reshistory, GMRES_m, GMRES_GSflag, group=None, **extra):
+    """parcel_dgmres_dia's argument list (src/wrapper.f90:821); returns (niter, iret)."""
+    return _dia_solve(3, x, b, n, gn, istart, diaA, offset, nnd, reshistory, group,
+                      dict(extra, ipreflag=ipreflag, ILU_method=ILU_method, addL=addL, iflagAS=iflagAS,
+                           itrmax=itrmax, rtolmax=rtolmax, GMRES_m=GMRES_m, GMRES_GSflag=GMRES_GSflag))
+
+
+def parcel_dcagmres_dia(x, b, n, gn, istart, diaA, offset, nnd, ipreflag, ILU_method, addL, iflagAS, itrmax,
+                        rtolmax, reshistory, CAGMRES_sstep, CAGMRES_tstep, CAGMRES_basis, CAGMRES_QRflag,
+                        group=None, **extra):
+    """parcel_dcagmres_dia's argument list (src/wrapper.f90:1457); returns (niter, iret)."""
+    return _dia_solve(4, x, b, n, gn, istart, diaA, offset, nnd, reshistory, group,
+                      dict(extra, ipreflag=ipreflag, ILU_method=ILU_method, addL=addL, iflagAS=iflagAS,
+                           itrmax=itrmax, rtolmax=rtolmax, CAGMRES_sstep=CAGMRES_sstep,
+                           CAGMRES_tstep=CAGMRES_tstep, CAGMRES_basis=CAGMRES_basis,
+                           CAGMRES_QRflag=CAGMRES_QRflag))

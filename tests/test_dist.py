@@ -189,3 +189,103 @@ def test_cagmres_dense_steps_match_the_oracle():
         ha = pdist._hessenberg_update(s, 2, B1a, Ha, R1, Rk, BRup, ha)
         hb = cagmres.hessenberg_update(s, t, 2, B1b, Hb, R1, Rk, BRup, hb)
         assert np.allclose(Ha, Hb, rtol=1e-12, atol=1e-12 * np.abs(Hb).max()) and np.isclose(ha, hb, rtol=1e-13)
+
+
+def _dia_worker(rank, world, port, kind, nblocks, q):
+    try:
+        sys.path[:0] = [os.path.join(ROOT, "parcel-legacy_b200"), os.path.join(ROOT, "oracle")]
+        import torch
+        import torch.distributed as dist
+
+        import oracle
+        from parcel_b import dist as pdist
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+        A, b, kw = _problem(kind[4:])
+        dia, off = oracle.crs_to_dia(A)
+        off = off[::-1].copy()                     # any offset order
+        dia = dia.reshape(len(off), A.n)[::-1]
+        per = A.n // world
+        lo, hi = rank * per, (rank + 1) * per
+        mine = np.ascontiguousarray(dia[:, lo:hi]).ravel()
+        x = torch.zeros(hi - lo, dtype=torch.float64)
+        hist = np.zeros(kw["itrmax"] + 2)
+        be = lambda lay, val, opts: NumpyLocal(lay, val, nblocks // world, 2)
+        common = dict(ipreflag=2, ILU_method=0, addL=0, iflagAS=1, itrmax=kw["itrmax"], rtolmax=kw["rtolmax"],
+                      reshistory=hist, backend=be)
+        args = (x, torch.from_numpy(b[lo:hi].copy()), hi - lo, A.n, lo + 1, mine, off, len(off))
+        if kw["solver"] == 1:
+            niter, iret = pdist.parcel_dcg_dia(*args, **common)
+        elif kw["solver"] == 2:
+            niter, iret = pdist.parcel_dbicgstab_dia(*args, **common)
+        elif kw["solver"] == 3:
+            niter, iret = pdist.parcel_dgmres_dia(*args, GMRES_m=kw["GMRES_m"], GMRES_GSflag=1, **common)
+        else:
+            niter, iret = pdist.parcel_dcagmres_dia(*args, CAGMRES_sstep=kw["CAGMRES_sstep"],
+                                                    CAGMRES_tstep=kw["CAGMRES_tstep"],
+                                                    CAGMRES_basis=kw["CAGMRES_basis"],
+                                                    CAGMRES_QRflag=kw["CAGMRES_QRflag"], **common)
+        q.put((rank, niter, iret, hist[:niter].copy(), x.numpy(), 0))
+        dist.destroy_process_group()
+    except Exception:  # pragma: no cover - reported to the parent
+        import traceback
+        q.put((rank, "error", traceback.format_exc(), None, None, None))
+
+
+@pytest.mark.parametrize("kind", ["dia-cg", "dia-bicgstab", "dia-gmres", "dia-cagmres-4-2-1-5"])
+def test_distributed_dia_rows_reproduce_the_crs_solve(kind):
+    """Each process passes its rows of a DIA matrix (the diagonals in reverse offset order);
+    the global columns (row + offset) reach the neighbouring process's rows through the halo
+    exchange.  The histories equal the oracle's CRS solve of the same matrix as in the CRS
+    tests (CA-GMRES at its own criteria)."""
+    import cagmres
+    import oracle
+    world, nblocks = 2, 4
+    A, b, kw = _problem(kind[4:])
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_dia_worker, args=(r, world, port, kind, nblocks, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=300) for _ in range(world)], key=lambda o: o[0])
+    for p in procs:
+        p.join(timeout=60)
+    for o in out:
+        assert o[1] != "error", o[2]
+    x = np.concatenate([o[4] for o in out])
+    if kw["solver"] == 4:
+        xo, ho, no, io = cagmres.pcagmres(A, b, s=kw["CAGMRES_sstep"], t=kw["CAGMRES_tstep"],
+                                          basis=kw["CAGMRES_basis"], qrflag=kw["CAGMRES_QRflag"],
+                                          itrmax=kw["itrmax"], rtolmax=kw["rtolmax"], ipreflag=2, ILU_method=0,
+                                          precon_thblock=nblocks)
+        for _, niter, iret, hist, _, _ in out:
+            assert iret == io == 0 and abs(niter - no) <= 2
+            k = min(niter, no)
+            m = ho[:k] > 1e-8
+            assert np.max(np.abs(hist[:k][m] - ho[:k][m]) / ho[:k][m]) < 1e-6
+        assert oracle.true_relres(A, b, x) < 1e-9
+        return
+    okw = {k: v for k, v in kw.items() if not k.startswith("CAGMRES")}
+    xo, ho, no, io = oracle.solve(A, b, ipreflag=2, ILU_method=0, precon_thblock=nblocks, **okw)
+    for _, niter, iret, hist, _, _ in out:
+        assert (niter, iret) == (no, io)
+        m = ho[:niter] > 1e-8 * ho[0]
+        assert np.max(np.abs(hist[m] - ho[:niter][m]) / ho[:niter][m]) < 1e-8
+    assert np.max(np.abs(x - xo)) <= 1e-8 * np.max(np.abs(xo))
+
+
+def test_dia_rows_global_columns_and_edges():
+    """Row istart + k - 1 couples column row + offset; zero entries and columns outside
+    1..gn are left out, each row's columns ascending; a repeated offset is refused."""
+    from parcel_b import dist as pdist
+    n, gn, istart = 3, 6, 3                        # rows 3, 4, 5 of 6
+    off = np.array([2, -3, 0], np.int32)
+    dia = np.array([[1.0, 2.0, 3.0],               # offset 2: columns 5, 6, 7 (7 is outside)
+                    [4.0, 0.0, 6.0],               # offset -3: columns 0 (outside), 1 (zero), 2
+                    [7.0, 8.0, 9.0]]).ravel()      # offset 0
+    rp, col, val = pdist.dia_rows(n, gn, istart, dia, off, 3)
+    assert rp.tolist() == [1, 3, 5, 7]
+    assert col.tolist() == [3, 5, 4, 6, 2, 5]
+    assert val.tolist() == [7.0, 1.0, 8.0, 2.0, 6.0, 9.0]
+    with pytest.raises(ValueError):
+        pdist.dia_rows(n, gn, istart, dia, np.array([0, 1, 0], np.int32), 3)
