@@ -67,6 +67,10 @@ def _problem(kind):
     b = problems.rhs_normal(A.n, 3)
     if kind == "bicgstab":
         return A, b, dict(solver=2, itrmax=500, rtolmax=1e-10)
+    if kind == "gmres-cgs":
+        return A, b, dict(solver=3, itrmax=500, rtolmax=1e-10, GMRES_m=10, GMRES_GSflag=2)
+    if kind == "gmres-pj":   # point Jacobi
+        return A, b, dict(solver=3, itrmax=800, rtolmax=1e-10, GMRES_m=10, GMRES_GSflag=1)
     if kind.startswith("cagmres"):   # cagmres-s-t-basis-qr
         _, sst, tst, bas, qr = kind.split("-")
         return A, b, dict(solver=4, itrmax=500, rtolmax=1e-10, CAGMRES_sstep=int(sst), CAGMRES_tstep=int(tst),
@@ -88,7 +92,7 @@ def _worker(rank, world, port, kind, nblocks, q):
         rp = A.rowptr[lo:hi + 1] - A.rowptr[lo] + 1
         k0, k1 = A.rowptr[lo] - 1, A.rowptr[hi] - 1
         lay = pdist.Layout(hi - lo, A.n, lo + 1, rp, A.col[k0:k1])
-        be = NumpyLocal(lay, A.val[k0:k1], nblocks // world, 2)
+        be = NumpyLocal(lay, A.val[k0:k1], nblocks // world, 1 if kind == "gmres-pj" else 2)
         x = torch.zeros(hi - lo, dtype=torch.float64)
         niter, iret, hist = pdist.solve(lay, A.val[k0:k1], torch.from_numpy(b[lo:hi].copy()), x, backend=be, **kw)
         q.put((rank, niter, iret, hist, x.numpy(), lay.n_ext - lay.n))
@@ -113,14 +117,16 @@ def _run(kind, world, nblocks):
     return sorted(out, key=lambda o: o[0])
 
 
-@pytest.mark.parametrize("kind,world", [("cg", 2), ("bicgstab", 2), ("bicgstab", 3), ("gmres", 2), ("gmres", 3)])
+@pytest.mark.parametrize("kind,world", [("cg", 2), ("bicgstab", 2), ("bicgstab", 3), ("gmres", 2), ("gmres", 3),
+                                        ("gmres-cgs", 2), ("gmres-pj", 3)])
 def test_distributed_solve_reproduces_single_process_history(kind, world):
     import oracle
     nblocks = 2 * world
     A, b, kw = _problem(kind)
     if A.n % world or (A.n // world) % (nblocks // world):
         pytest.skip("rows do not split evenly")
-    xo, ho, no, io = oracle.solve(A, b, ipreflag=2, ILU_method=0, precon_thblock=nblocks, **kw)
+    pre = dict(ipreflag=1) if kind == "gmres-pj" else dict(ipreflag=2, ILU_method=0, precon_thblock=nblocks)
+    xo, ho, no, io = oracle.solve(A, b, **pre, **kw)
     out = _run(kind, world, nblocks)
     for rank, niter, iret, hist, x, nhalo in out:
         assert (niter, iret) == (no, io), (rank, niter, iret, no, io)
